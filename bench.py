@@ -1,0 +1,457 @@
+"""Benchmark of the fused Dopri5 + features + 1-NN basin-stability pass on B200.
+
+Workload (default): forced Duffing x'' + 0.08x' + x^3 = 0.2 cos t, N = 100,000
+ICs uniform on x in [-1,1], x' in [-0.5,1] (seeded), t in [0,1000], 5000 save
+points on the window [900,1000], features max and std of x, 1-NN against the
+five reference templates, labels and basin-stability counts back on the host
+(case_studies/duffing_oscillator/setup_duffing_oscillator_system.py).
+
+One step = one pass of that workload.  Arms:
+
+* default  : the B200 pipeline (FP32 stages, FP64 time / error norm / control,
+             work queue), with the plain FP64 kernel, |dBS| against it and the
+             CPU oracle timed beside it;
+* --impl reference : the CPU reference path on the host cores (the FP64 oracle
+             port of the reference's native Dopri5 + the reference's 1-NN).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_DEFAULT = 100_000
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+DUFFING = dict(
+    params={"delta": 0.08, "k3": 1.0, "A": 0.2},
+    lo=(-1.0, -0.5),
+    hi=(1.0, 1.0),
+    t_span=(0.0, 1000.0),
+    t_eval=(900.0, 1000.0),
+    t_steps=5000,
+    time_steady=900.0,
+    features_per_state={0: {"maximum": None, "standard_deviation": None}},
+    templates=[[-0.21, 0.02], [1.05, 0.77], [-0.67, 0.02], [-0.46, 0.30], [-0.43, 0.12]],
+    labels=["y1", "y2", "y3", "y4", "y5"],
+    rtol=1e-8,
+    atol=1e-6,
+)
+
+# algorithmic flops per attempted step (S=2, Duffing): 71*S + 6*F_rhs with F_rhs = 7
+FLOP_PER_STEP = 71 * 2 + 6 * 7
+FLOP_PER_SAVE = 8 * 2
+
+
+def seeded_ics(n: int, seed: int) -> torch.Tensor:
+    torch.manual_seed(seed)
+    lo = torch.tensor(DUFFING["lo"], dtype=torch.float32)
+    hi = torch.tensor(DUFFING["hi"], dtype=torch.float32)
+    return torch.rand(n, 2) * (hi - lo) + lo
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc: subprocess.Popen | None = None
+        self.lines: list[str] = []
+        self._t: threading.Thread | None = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        assert self.proc is not None and self.proc.stdout is not None
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": mx,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ---------------------------------------------------------------------------
+# CPU reference path: FP64 oracle (port of the reference's native Dopri5) + 1-NN
+# ---------------------------------------------------------------------------
+def cpu_reference_pass(y0: np.ndarray, threads: int) -> tuple[np.ndarray, float]:
+    from oracle import oracle as O
+    from sklearn.neighbors import KNeighborsClassifier
+
+    save = torch.linspace(*DUFFING["t_eval"], DUFFING["t_steps"], dtype=torch.float32).double().numpy()
+    wb = int(np.nonzero(save >= DUFFING["time_steady"])[0][0])
+    feats = [(0, 5, 0.0), (0, 2, 0.0)]
+    p = np.array([list(DUFFING["params"].values())])
+    t0 = time.perf_counter()
+    r = O.solve_batch(O.SYS_DUFFING, y0, p, save, (0.0, float(save[-1])), DUFFING["rtol"], DUFFING["atol"],
+                      win_begin=wb, features=feats, n_threads=threads)
+    rt = O.solve_batch(O.SYS_DUFFING, np.array(DUFFING["templates"]), p, save, (0.0, float(save[-1])),
+                       DUFFING["rtol"], DUFFING["atol"], win_begin=wb, features=feats, n_threads=threads)
+    knn = KNeighborsClassifier(n_neighbors=1).fit(rt["features"].astype(np.float32), DUFFING["labels"])
+    labels = knn.predict(np.nan_to_num(r["features"], nan=1e10, posinf=1e10, neginf=-1e10).astype(np.float32))
+    return labels, time.perf_counter() - t0
+
+
+def cpu_sample_size(threads: int, target_s: float) -> tuple[int, float]:
+    """Pick a bounded sample so one CPU pass takes about target_s seconds."""
+    n0 = 256 * threads
+    y0 = seeded_ics(n0, 1234).double().numpy()
+    _, dt = cpu_reference_pass(y0, threads)
+    rate = n0 / dt
+    return int(min(N_DEFAULT, max(n0, rate * target_s))), rate
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n, _ = cpu_sample_size(threads, 8.0)
+    y0 = seeded_ics(n, 42).double().numpy()
+    for _ in range(args.warmup):
+        cpu_reference_pass(y0[: max(n // 16, 64)], threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_reference_pass(y0, threads)
+        times.append(dt)
+    ms = 1000.0 * statistics.mean(times)
+    value = n / (ms / 1000.0)
+    line = {
+        "metric": "labelled ICs/sec (Duffing, |dBS|<=0.005 vs FP64)",
+        "value": value,
+        "unit": "ICs/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded uniform ICs, reference sampler)",
+        "impl": "reference",
+        "config": {"workload": f"duffing forced, N={n} per pass (bounded sample of N=100000), t=[0,1000], "
+                               "window [900,1000] x 5000 saves, rtol 1e-8 atol 1e-6, 1-NN on 5 templates",
+                   "n_ic": n},
+        "cpu_baseline": {
+            "value": value,
+            "unit": "ICs/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"{n} seeded Duffing ICs per pass; FP64 oracle (restatement of the reference's native "
+                      "Dopri5, src/zigode/src/solver/dopri5_generic.zig) on OpenMP threads + sklearn 1-NN",
+        },
+        "e2e": {"value": value, "unit": "ICs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def make_pipeline(dev: torch.device, precision: str, schedule: str):
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+    from pybasin_b200.pipeline import BasinStabilityPipeline
+
+    fx = FusedFeatureExtractor(time_steady=DUFFING["time_steady"], features=None,
+                               features_per_state=DUFFING["features_per_state"], normalize=False)
+    solver = B200Dopri5Solver(t_span=DUFFING["t_span"], t_steps=DUFFING["t_steps"], t_eval=DUFFING["t_eval"],
+                              device=str(dev), rtol=DUFFING["rtol"], atol=DUFFING["atol"], precision=precision,
+                              feature_extractor=fx, schedule=schedule)
+    ode = DuffingODE(DUFFING["params"])
+    return BasinStabilityPipeline(ode, solver, DUFFING["templates"], DUFFING["labels"], device=dev)
+
+
+def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: torch.Tensor, dist_on: bool):
+    """Device-timed passes: per-step events around the pass and around the integrator
+    kernel, with an L2 flush (write of a 256 MB buffer) between steps."""
+    from pybasin_b200 import _lib as L
+    import ctypes
+
+    lib = L.load()
+    s = torch.cuda.current_stream()
+    for _ in range(warmup):
+        pipe.run_device(y0_dev)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_(i)
+        a, b, c = ev[i]
+        n = y0_dev.shape[0]
+        pipe.y0_buf[:n].copy_(y0_dev, non_blocking=True)
+        a.record(s)
+        L.check(lib.pb_solve_batch(ctypes.byref(pipe.args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
+        b.record(s)
+        feats = pipe.out.features
+        L.check(lib.pb_label_nearest(feats.data_ptr(), n, feats.shape[1], feats[n:].data_ptr(), pipe.n_tpl,
+                                     pipe.tpl_class.data_ptr(), pipe.n_classes, pipe.out.status.data_ptr(), None, 1,
+                                     pipe.labels.data_ptr(), pipe.counts.data_ptr(), ctypes.c_void_p(s.cuda_stream)),
+                "pb_label_nearest")
+        c.record(s)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    step_ms = [a.elapsed_time(c) for a, b, c in ev]
+    kern_ms = [a.elapsed_time(b) for a, b, c in ev]
+    return step_ms, kern_ms
+
+
+def fma_peak(dev: torch.device, precision: int) -> float:
+    """Measured FMA-pipe peak (FLOP/s) of this GPU for the given precision."""
+    from pybasin_b200 import _lib as L
+
+    lib = L.load()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks = sms * 8
+    sink = torch.empty(blocks * 256, dtype=torch.float32, device=dev)
+    iters = 20000 if precision == L.PREC_MIXED else 8000
+    s = torch.cuda.current_stream()
+    for _ in range(2):
+        L.check(lib.pb_probe_fma(precision, blocks, iters, sink.data_ptr(), s.cuda_stream), "pb_probe_fma")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    reps = 5
+    for _ in range(reps):
+        lib.pb_probe_fma(precision, blocks, iters, sink.data_ptr(), s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1000.0 / reps
+    return 2.0 * 8 * iters * blocks * 256 / sec
+
+
+def run_b200_arm(args) -> None:
+    from pybasin_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist_on = world > 1
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    if dist_on:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=dev)
+    n = args.n
+    y0_host = seeded_ics(n, 42 + rank)
+    y0_dev = y0_host.to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    pipe = make_pipeline(dev, "mixed", "queue")
+    pipe.run_device(y0_dev)
+    torch.cuda.synchronize()
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        step_ms, kern_ms = timed_passes(pipe, y0_dev, args.steps, args.warmup, flush, dist_on)
+    ms = statistics.mean(step_ms)
+    kms = statistics.mean(kern_ms)
+    if dist_on:
+        t = torch.tensor([ms, kms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, kms = float(t[0]), float(t[1])
+        counts = pipe.counts.clone()
+        torch.distributed.all_reduce(counts)
+    labels_mixed = pipe.labels.clone()
+    counts_mixed = pipe.counts.clone()
+    steps_mixed = pipe.out.steps[:n].clone()
+    value = n * world / (ms / 1000.0)
+
+    # plain FP64 kernel (the reference algorithm, one thread per trajectory) on the same ICs
+    pipe64 = make_pipeline(dev, "fp64", "plain")
+    pipe64.run_device(y0_dev)
+    torch.cuda.synchronize()
+    step64, kern64 = timed_passes(pipe64, y0_dev, max(1, min(args.steps, 3)), 1, flush, dist_on)
+    ms64 = statistics.mean(step64)
+    counts64 = pipe64.counts.clone()
+    agree = float((pipe64.labels == labels_mixed).float().mean())
+    dbs = (counts_mixed[0, :5].double() - counts64[0, :5].double()).abs().max().item() / n
+
+    # end to end through the public API: pinned host ICs in, labels out
+    y0_pinned = y0_host.pin_memory()
+    for _ in range(2):
+        pipe.run(y0_pinned, use_graph=True)
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lab, bs = pipe.run(y0_pinned, use_graph=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = statistics.mean(e2e_times)
+    if dist_on:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t[0])
+
+    # roofline of the integrator kernel: algorithmic FLOPs per launch / kernel time
+    mean_steps = float(steps_mixed.double().mean())
+    n_saves = DUFFING["t_steps"]
+    flop_per_ic = mean_steps * FLOP_PER_STEP + n_saves * FLOP_PER_SAVE
+    achieved = (n + len(DUFFING["templates"])) * flop_per_ic / (kms / 1000.0)
+    peak32 = fma_peak(dev, L.PREC_MIXED)
+    peak64 = fma_peak(dev, L.PREC_FP64)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        n_cpu, _ = cpu_sample_size(threads, 4.0)
+        _, dt = cpu_reference_pass(seeded_ics(n_cpu, 42).double().numpy(), threads)
+        cpu = {
+            "value": n_cpu / dt,
+            "unit": "ICs/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"{n_cpu} of the {n} seeded Duffing ICs; FP64 oracle (restatement of the reference's "
+                      "native Dopri5) at rtol 1e-8 atol 1e-6 on OpenMP threads + sklearn 1-NN",
+        }
+    if dist_on:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {
+            "metric": "labelled ICs/sec (Duffing, |dBS|<=0.005 vs FP64)",
+            "value": value,
+            "unit": "ICs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 stages / f64 time+error+control",
+            "data": "synthetic (seeded uniform ICs, reference sampler)",
+            "config": {
+                "workload": "duffing forced (delta 0.08, k3 1, A 0.2), N=100000 ICs per GPU, t=[0,1000], "
+                            "window [900,1000] x 5000 saves, features max+std of x, 1-NN on 5 templates",
+                "n_ic_per_gpu": n,
+                "rtol_atol": list(pipe.solver.effective_tolerances()),
+                "schedule": "queue",
+                "l2": "flushed between timed steps (256 MB write)",
+                "parallelism": f"ic-shard x{world}",
+            },
+            "delta_bs_vs_fp64": dbs,
+            "label_agreement_vs_fp64": agree,
+            "plain_fp64": {"value": n * world / (ms64 / 1000.0), "ms_per_step": ms64,
+                           "kernel_ms": statistics.mean(kern64), "rtol_atol": [DUFFING["rtol"], DUFFING["atol"]]},
+            "speedup_vs_plain_fp64": ms64 / ms,
+            "e2e": {
+                "value": n * world / (e2e_ms / 1000.0),
+                "unit": "ICs/s",
+                "h2d_bytes_per_step": int(y0_host.numel() * 4),
+                "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8),
+            },
+            "gpu_launches": pipe.kernel_launches_per_pass() * args.steps,
+            "roofline": {
+                "bound": "fp32-fma",
+                "achieved": achieved / 1e12,
+                "peak": peak32 / 1e12,
+                "unit": "TFLOP/s",
+                "frac": achieved / peak32,
+                "traffic": None,
+                "peak_source": "FP32 FMA probe kernel measured in this run (MEASURED_PEAKS.json holds only the "
+                               "HBM-copy and bf16-GEMM peaks, neither bounds this kernel)",
+                "fp64_fma_peak": peak64 / 1e12,
+                "kernel_ms": kms,
+                "mean_steps_per_ic": mean_steps,
+                "flop_per_ic": flop_per_ic,
+            },
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist_on:
+        torch.distributed.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

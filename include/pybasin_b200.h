@@ -1,0 +1,198 @@
+/*
+ * pybasin_b200 — C ABI of the B200 fused Dopri5 + steady-state-feature library.
+ *
+ * Every entry point takes plain pointers and sizes.  Array arguments marked
+ * "device" are CUDA device pointers on the current device; `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  No entry point
+ * allocates on the caller's behalf except where stated, none aborts, and every
+ * one returns a pb_status (0 = success, negative = error, the numbering of the
+ * reference's native solver ABI extended with a few codes).
+ *
+ * Reference interfaces replaced (paths relative to the pybasin project root):
+ *   pb_solve_batch      src/zigode/src/c_api.zig:193-314 (`solve_batch`) and the
+ *                       Python-level SolverProtocol.integrate it backs,
+ *                       src/pybasin/protocols.py:156-168,
+ *                       src/pybasin/solvers/torchdiffeq_solver.py:97-134;
+ *                       fused with TorchFeatureExtractor.extract_features,
+ *                       src/pybasin/ts_torch/torch_feature_extractor.py:192-287.
+ *   pb_label_nearest    the 1-NN classification + basin-stability count step,
+ *                       src/pybasin/basin_stability_estimator.py:426-446,586-598
+ *                       (sklearn KNeighborsClassifier(n_neighbors=1) predict).
+ *   pb_error_string     src/zigode/zig_solver.py:333-341 (error-code messages).
+ */
+#ifndef PYBASIN_B200_H
+#define PYBASIN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes (0/-1/-2/-3 as in src/zigode/src/c_api.zig:17-23) ---- */
+typedef enum {
+    PB_SUCCESS = 0,
+    PB_EINVALID_ODE = -1,   /* unknown system id / dimension combination */
+    PB_EALLOC = -2,         /* device allocation failed */
+    PB_ESOLVE = -3,         /* kernel launch or execution error */
+    PB_EINVAL = -5,         /* invalid argument (null pointer, bad size, bad layout) */
+    PB_ECUDA = -6,          /* other CUDA runtime error */
+    PB_EUNSUPPORTED = -7,   /* valid request this build does not support */
+    PB_ECOMPILE = -8        /* runtime (NVRTC) compilation of a user right-hand side failed */
+} pb_status;
+
+/* ---- built-in right-hand sides (templated device functors) ---- */
+typedef enum {
+    PB_SYS_LINEAR = 0,        /* dy/dt = p0*y, any dim 1..4; tests/unit/solvers/test_solver.py:16-21 */
+    PB_SYS_PENDULUM = 1,      /* case_studies/pendulum/pendulum_ode.py:23-40, p=[alpha,T,K] */
+    PB_SYS_DUFFING = 2,       /* case_studies/duffing_oscillator/duffing_ode.py:26-42, p=[delta,k3,A] */
+    PB_SYS_LORENZ = 3,        /* case_studies/lorenz/lorenz_jax_ode.py, p=[sigma,r,b] */
+    PB_SYS_LORENZ_MASKED = 4, /* case_studies/lorenz/lorenz_ode.py:28-64 (|y|>=200 freezes) */
+    PB_SYS_ROSSLER_NET = 5    /* case_studies/rossler_network/rossler_network_jax_ode.py:53-79 */
+} pb_system;
+
+/* ---- arithmetic of the integrator ---- */
+typedef enum {
+    PB_PREC_FP64 = 0,  /* plain: stages, state, time, error norm and control all FP64 */
+    PB_PREC_MIXED = 1  /* FP32 stages and state (Kahan-compensated accumulation),
+                          FP64 time, error norm and step-size control */
+} pb_precision;
+
+/* ---- how trajectories map to initial conditions and parameter rows ---- */
+typedef enum {
+    PB_LAYOUT_SINGLE = 0,  /* every trajectory uses params row 0; traj j uses y0 row j */
+    PB_LAYOUT_CROSS = 1,   /* IC-major product, src/pybasin/solvers/base.py:155-159:
+                              traj j = ic*P + p uses y0 row ic and params row p */
+    PB_LAYOUT_INDEXED = 2  /* traj j uses y0 row j and params row param_index[j] */
+} pb_layout;
+
+/* ---- fused window features (names of src/pybasin/ts_torch/settings.py) ---- */
+typedef enum {
+    PB_FEAT_MEDIAN = 0, PB_FEAT_MEAN = 1, PB_FEAT_STD = 2, PB_FEAT_VAR = 3, PB_FEAT_RMS = 4,
+    PB_FEAT_MAX = 5, PB_FEAT_ABSMAX = 6, PB_FEAT_MIN = 7, PB_FEAT_DELTA = 8,
+    PB_FEAT_LOG_DELTA = 9, PB_FEAT_AMPLITUDE = 10, PB_FEAT_CROSSINGS = 11, PB_FEAT_LAST = 12
+} pb_feature;
+
+/* ---- per-trajectory status written to status_out ---- */
+typedef enum {
+    PB_TRAJ_OK = 0,
+    PB_TRAJ_MAX_STEPS = 1,    /* max_steps attempted steps before t1 */
+    PB_TRAJ_DT_UNDERFLOW = 2, /* t + dt == t */
+    PB_TRAJ_UNBOUNDED = 3,    /* max|y| >= unbounded_threshold after an accepted step */
+    PB_TRAJ_NONFINITE = 4     /* non-finite error norm */
+} pb_traj_status;
+
+#define PB_MAX_FEATURES 32
+#define PB_MAX_CROSSING 4
+#define PB_MAX_PARAMS 8
+
+typedef enum { PB_DTYPE_F32 = 0, PB_DTYPE_F64 = 1 } pb_dtype;
+
+/* Work distribution of pb_solve_batch. */
+typedef enum {
+    PB_SCHED_PLAIN = 0,  /* one thread per trajectory, grid covers all trajectories */
+    PB_SCHED_QUEUE = 1   /* persistent lanes refilled from a global atomic queue with
+                            warp-aggregated fetches (needs `queue_counter`) */
+} pb_schedule;
+
+typedef struct pb_solve_args {
+    /* problem */
+    int32_t system;          /* pb_system */
+    int32_t dim;             /* state dimension S */
+    int32_t precision;       /* pb_precision */
+    int32_t schedule;        /* pb_schedule */
+    int32_t layout;          /* pb_layout */
+    int32_t y0_dtype;        /* pb_dtype of y0 */
+    int32_t n_params;        /* columns of params (<= PB_MAX_PARAMS) */
+    int32_t block_size;      /* threads per block (0 = library default) */
+    int32_t grid_blocks;     /* QUEUE: persistent blocks (0 = occupancy-derived) */
+    int32_t _pad0;
+    int64_t n_ic;            /* rows of y0 */
+    int64_t n_param_rows;    /* rows of params */
+    int64_t n_traj;          /* trajectories to integrate */
+    const void* y0;          /* device (n_ic, dim) */
+    const double* params;    /* device (n_param_rows, n_params) */
+    const int32_t* param_index; /* device (n_traj) for PB_LAYOUT_INDEXED, else NULL */
+    const int32_t* csr_row;  /* device, network systems only: (n_nodes+1) */
+    const int32_t* csr_col;  /* device, network systems only */
+    /* time grid */
+    double t0, t1;           /* integrate from t0 to t1 */
+    const double* save_ts;   /* device (n_save) ascending save instants */
+    int32_t n_save;
+    int32_t win_begin;       /* first save index of the feature window */
+    /* control */
+    double rtol, atol;
+    int64_t max_steps;       /* attempted steps per trajectory */
+    double unbounded_thr;    /* <= 0 disables the stop-on-|y| event */
+    /* features: output column c = feature feat_kind[c] of state feat_state[c] */
+    int32_t n_features;
+    int32_t _pad1;
+    int32_t feat_state[PB_MAX_FEATURES];
+    int32_t feat_kind[PB_MAX_FEATURES];
+    double feat_param[PB_MAX_FEATURES]; /* level m of PB_FEAT_CROSSINGS */
+    /* outputs (device; any may be NULL) */
+    double* features_out;    /* (n_traj, n_features) */
+    int32_t* status_out;     /* (n_traj) pb_traj_status */
+    void* y_final_out;       /* (n_traj, dim) state at t1 (or at the stop) */
+    void* y_full_out;        /* (n_save, n_traj, dim): every save point, reference layout */
+    int32_t y_out_dtype;     /* pb_dtype of y_final_out / y_full_out */
+    int32_t _pad2;
+    int64_t* steps_out;      /* (n_traj) attempted steps */
+    /* scratch (device) */
+    unsigned long long* queue_counter; /* QUEUE schedule: one zero-initialised counter
+                                          (the call resets it on `stream`) */
+    float* median_scratch;   /* (n_traj, n_median_states, n_save - win_begin) when any
+                                PB_FEAT_MEDIAN column is requested, else NULL */
+} pb_solve_args;
+
+/* Integrate n_traj trajectories with adaptive Dormand-Prince 5(4) and write the
+ * fused window features, statuses and (optionally) states.  Asynchronous on
+ * `stream`.  Replaces src/zigode/src/c_api.zig:193-314 (solve_batch) and
+ * src/pybasin/solvers/torchdiffeq_solver.py:97-134 + the minimal statistics of
+ * src/pybasin/ts_torch/calculators/torch_features_statistical.py. */
+int pb_solve_batch(const pb_solve_args* args, void* stream);
+
+/* Device bytes of scratch pb_solve_batch needs for `args` (median window). */
+int64_t pb_solve_scratch_bytes(const pb_solve_args* args);
+
+/* 1-NN labelling on the device (Euclidean, the reference's
+ * KNeighborsClassifier(n_neighbors=1), src/pybasin/basin_stability_estimator.py:426-446)
+ * followed by per-group label counts (src/pybasin/basin_stability_estimator.py:586-598).
+ *   features   device (n, n_features) double
+ *   templates  device (n_templates, n_features) double
+ *   tpl_label  device (n_templates) int32 class of each template (0..n_classes-1)
+ *   status     device (n) int32 or NULL; PB_TRAJ_UNBOUNDED rows get class n_classes
+ *   group_of   device (n) int32 or NULL (all rows group 0)
+ *   labels_out device (n) int32
+ *   counts_out device (n_groups, n_classes + 1) int64, zeroed by the call on `stream`
+ * Non-finite features are imputed first (+inf,NaN -> +1e10, -inf -> -1e10),
+ * src/pybasin/ts_torch/torch_feature_utilities.py:60-94. */
+int pb_label_nearest(const double* features, int64_t n, int32_t n_features,
+                     const double* templates, int32_t n_templates, const int32_t* tpl_label,
+                     int32_t n_classes, const int32_t* status, const int32_t* group_of,
+                     int32_t n_groups, int32_t* labels_out, int64_t* counts_out, void* stream);
+
+/* Occupancy helper for the autotuner: resident blocks per SM of the pb_solve_batch
+ * kernel selected by (system, dim, precision, schedule) at `block_size`. */
+int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule,
+                       int32_t block_size, int32_t* blocks_per_sm, int32_t* num_sms);
+
+/* Throughput probe for the roofline denominator of the integrator kernels, whose
+ * bound is the FP32 (mixed) or FP64 (plain) FMA pipe rather than HBM or the tensor
+ * cores: launches `blocks` x 256 threads, each running `iters` x 8 independent
+ * FMA chains in FP32 (precision PB_PREC_MIXED) or FP64 (PB_PREC_FP64), and writes
+ * one value per thread to `sink` (device, blocks*256 floats) so nothing is elided.
+ * The caller times it; flops = 2 * 8 * iters * blocks * 256.  No reference
+ * counterpart (measurement utility). */
+int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, void* stream);
+
+/* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
+const char* pb_error_string(int32_t status);
+
+/* ABI version (major*100 + minor). */
+int32_t pb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYBASIN_B200_H */

@@ -1,0 +1,381 @@
+/*
+ * FP64 CPU oracle for the fused Dopri5 + steady-state-feature hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA kernels in
+ * pybasin_b200/csrc are compared against (tests/, __graft_entry__.smoke() and
+ * the cpu_baseline / reference arm of bench.py).  It is never linked into the
+ * product library and the product never calls it.
+ *
+ * What it restates (reference paths are relative to the pybasin project root):
+ *   - Dormand-Prince 5(4) step, tableau, Shampine error coefficients and the
+ *     torchdiffeq-style 4th-order dense output:
+ *       src/zigode/src/solver/dopri5_generic.zig:16-56  (coefficients)
+ *       src/zigode/src/solver/dopri5_generic.zig:77-242 (solve_into main loop)
+ *       src/zigode/src/solver/dopri5_generic.zig:185-192 (RMS error norm)
+ *       src/zigode/src/solver/dopri5_generic.zig:197-218 (dense output)
+ *       src/zigode/src/solver/dopri5_generic.zig:228-235 (step-size control)
+ *       src/zigode/src/solver/dopri5_generic.zig:270-321 (initial step size)
+ *   - pthread batch over ICs: src/zigode/src/c_api.zig:193-314 (here: OpenMP).
+ *   - Right-hand sides: case_studies/pendulum/pendulum_ode.py:23-46,
+ *     case_studies/duffing_oscillator/duffing_ode.py:26-42,
+ *     case_studies/lorenz/lorenz_ode.py:28-64 (masked variant) and
+ *     case_studies/lorenz/lorenz_jax_ode.py (plain variant),
+ *     tests/unit/solvers/test_solver.py:16-21 (linear decay).
+ *   - Window statistics computed the way the reference's torch calculators do
+ *     (two-pass, over the stored samples):
+ *       src/pybasin/ts_torch/calculators/torch_features_statistical.py:30-110,307-318
+ *       src/pybasin/ts_torch/calculators/torch_features_pattern.py:56-60
+ *
+ * Extensions over the Zig solver (documented, shared with the CUDA kernels):
+ *   - per-trajectory status (ok / max_steps / dt underflow / unbounded / non-finite),
+ *   - an optional unbounded threshold that stops a trajectory once max|y| >= thr
+ *     after an accepted step (the diffrax Event used by JaxSolver,
+ *     src/pybasin/solvers/jax_solver.py:375-436 and
+ *     case_studies/lorenz/setup_lorenz_system.py:16-26), after which the
+ *     remaining save points are +inf.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "oracle.h"
+
+/* ---- Dormand-Prince tableau (published method constants) ---------------- */
+static const double A21 = 1.0 / 5.0;
+static const double A31 = 3.0 / 40.0, A32 = 9.0 / 40.0;
+static const double A41 = 44.0 / 45.0, A42 = -56.0 / 15.0, A43 = 32.0 / 9.0;
+static const double A51 = 19372.0 / 6561.0, A52 = -25360.0 / 2187.0, A53 = 64448.0 / 6561.0,
+                    A54 = -212.0 / 729.0;
+static const double A61 = 9017.0 / 3168.0, A62 = -355.0 / 33.0, A63 = 46732.0 / 5247.0,
+                    A64 = 49.0 / 176.0, A65 = -5103.0 / 18656.0;
+static const double B1 = 35.0 / 384.0, B3 = 500.0 / 1113.0, B4 = 125.0 / 192.0,
+                    B5 = -2187.0 / 6784.0, B6 = 11.0 / 84.0;
+static const double C2 = 1.0 / 5.0, C3 = 3.0 / 10.0, C4 = 4.0 / 5.0, C5 = 8.0 / 9.0;
+static const double E1 = 35.0 / 384.0 - 1951.0 / 21600.0;
+static const double E3 = 500.0 / 1113.0 - 22642.0 / 50085.0;
+static const double E4 = 125.0 / 192.0 - 451.0 / 720.0;
+static const double E5 = -2187.0 / 6784.0 - -12231.0 / 42400.0;
+static const double E6 = 11.0 / 84.0 - 649.0 / 6300.0;
+static const double E7 = -1.0 / 60.0;
+static const double M1 = 6025192743.0 / 30085553152.0 / 2.0;
+static const double M3 = 51252292925.0 / 65400821598.0 / 2.0;
+static const double M4 = -2691868925.0 / 45128329728.0 / 2.0;
+static const double M5 = 187940372067.0 / 1594534317056.0 / 2.0;
+static const double M6 = -1776094331.0 / 19743644256.0 / 2.0;
+static const double M7 = 11237099.0 / 235043384.0 / 2.0;
+
+static const double SAFETY = 0.9, MIN_FACTOR = 0.2, MAX_FACTOR = 10.0;
+
+/* ---- right-hand sides ---------------------------------------------------- */
+static void rhs(int sys, double t, const double *y, double *dy, const double *p, int dim,
+                const oracle_aux *aux)
+{
+    switch (sys) {
+    case ORACLE_SYS_LINEAR: /* dy/dt = p0 * y (every component) */
+        for (int i = 0; i < dim; ++i) dy[i] = p[0] * y[i];
+        break;
+    case ORACLE_SYS_PENDULUM: /* [alpha, T, K] */
+        dy[0] = y[1];
+        dy[1] = -p[0] * y[1] + p[1] - p[2] * sin(y[0]);
+        break;
+    case ORACLE_SYS_DUFFING: /* [delta, k3, A] */
+        dy[0] = y[1];
+        dy[1] = -p[0] * y[1] - p[1] * y[0] * y[0] * y[0] + p[2] * cos(t);
+        break;
+    case ORACLE_SYS_LORENZ: /* [sigma, r, b] */
+    case ORACLE_SYS_LORENZ_MASKED: {
+        double f0 = p[0] * (y[1] - y[0]);
+        double f1 = p[1] * y[0] - y[0] * y[2] - y[1];
+        double f2 = y[0] * y[1] - p[2] * y[2];
+        if (sys == ORACLE_SYS_LORENZ_MASKED) {
+            double m = fmax(fabs(y[0]), fmax(fabs(y[1]), fabs(y[2])));
+            if (!(m < 200.0)) f0 = f1 = f2 = 0.0;
+        }
+        dy[0] = f0; dy[1] = f1; dy[2] = f2;
+        break;
+    }
+    case ORACLE_SYS_ROSSLER_NET: { /* [a, b, c, K]; state = [x(0..n), y(0..n), z(0..n)] */
+        int n = dim / 3;
+        const double *x = y, *yy = y + n, *z = y + 2 * n;
+        for (int i = 0; i < n; ++i) {
+            double lap = 0.0;
+            for (int e = aux->row_ptr[i]; e < aux->row_ptr[i + 1]; ++e) lap += x[aux->col_idx[e]] - x[i];
+            dy[i] = -yy[i] - z[i] + p[3] * lap;
+            dy[n + i] = x[i] + p[0] * yy[i];
+            dy[2 * n + i] = p[1] + z[i] * (x[i] - p[2]);
+        }
+        break;
+    }
+    default:
+        for (int i = 0; i < dim; ++i) dy[i] = NAN;
+    }
+}
+
+/* ---- window statistics (two-pass over stored samples) -------------------- */
+static int cmp_double(const void *a, const void *b)
+{
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+static double window_feature(int feat, double param, const double *w, int n, double *scratch)
+{
+    if (n <= 0) return NAN;
+    double sum = 0.0, mx = -INFINITY, mn = INFINITY;
+    int any_nan = 0;
+    for (int i = 0; i < n; ++i) {
+        sum += w[i];
+        any_nan |= isnan(w[i]);
+        if (w[i] > mx) mx = w[i];
+        if (w[i] < mn) mn = w[i];
+    }
+    if (any_nan) mx = mn = NAN; /* torch.max / torch.min propagate NaN */
+    double mean = sum / n;
+    double m2 = 0.0, sq = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double d = w[i] - mean;
+        m2 += d * d;
+        sq += w[i] * w[i];
+    }
+    switch (feat) {
+    case ORACLE_F_MEDIAN: { /* torch.median: the lower of the two middle values, NaN if any */
+        if (any_nan) return NAN;
+        memcpy(scratch, w, sizeof(double) * (size_t)n);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double);
+        return scratch[(n - 1) / 2];
+    }
+    case ORACLE_F_MEAN: return mean;
+    case ORACLE_F_STD: return sqrt(m2 / n);
+    case ORACLE_F_VAR: return m2 / n;
+    case ORACLE_F_RMS: return sqrt(sq / n);
+    case ORACLE_F_MAX: return mx;
+    case ORACLE_F_ABSMAX: return fmax(fabs(mx), fabs(mn));
+    case ORACLE_F_MIN: return mn;
+    case ORACLE_F_DELTA: return fabs(mx - mean);
+    case ORACLE_F_LOG_DELTA: return log(fabs(mx - mean) + 1e-10);
+    case ORACLE_F_AMPLITUDE: return mx - mn;
+    case ORACLE_F_CROSSINGS: {
+        double c = 0.0;
+        for (int i = 1; i < n; ++i) c += ((w[i] > param) != (w[i - 1] > param));
+        return c;
+    }
+    case ORACLE_F_LAST: return w[n - 1];
+    default: return NAN;
+    }
+}
+
+/* ---- initial step (Hairer, Norsett & Wanner II.4) ------------------------ */
+static double initial_step(int sys, const double *p, const double *y0, const double *f0, int dim,
+                           double t0, double rtol, double atol, const oracle_aux *aux,
+                           double *ytmp, double *ftmp)
+{
+    double d0 = 0.0, d1 = 0.0;
+    for (int i = 0; i < dim; ++i) {
+        double sc = atol + fabs(y0[i]) * rtol;
+        double r0 = y0[i] / sc, r1 = f0[i] / sc;
+        d0 += r0 * r0;
+        d1 += r1 * r1;
+    }
+    d0 = sqrt(d0 / dim);
+    d1 = sqrt(d1 / dim);
+    double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+    for (int i = 0; i < dim; ++i) ytmp[i] = y0[i] + h0 * f0[i];
+    rhs(sys, t0 + h0, ytmp, ftmp, p, dim, aux);
+    double d2 = 0.0;
+    for (int i = 0; i < dim; ++i) {
+        double sc = atol + fabs(y0[i]) * rtol;
+        double r = (ftmp[i] - f0[i]) / sc;
+        d2 += r * r;
+    }
+    d2 = sqrt(d2 / dim) / h0;
+    double h1 = (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / fmax(d1, d2), 0.2);
+    return fmin(100.0 * h0, h1);
+}
+
+/* ---- one trajectory ------------------------------------------------------ */
+typedef struct {
+    double *y, *ynew, *ystage, *k[7], *ia, *ib, *ic, *win, *scratch, *ytmp, *ftmp;
+} work_t;
+
+static int solve_one(const oracle_problem *pb, const double *y0, const double *p, work_t *w,
+                     double *feat_out, double *y_final, double *y_full, int64_t traj,
+                     int64_t n_traj, int64_t *steps_out, int64_t *accepted_out)
+{
+    const int dim = pb->dim;
+    const int ns = pb->n_save;
+    const int wb = pb->win_begin;
+    const int nwin = ns - wb;
+    double *y = w->y, *yn = w->ynew, *ys = w->ystage;
+    int k1 = 0, k7 = 6;
+    int status = ORACLE_OK;
+    memcpy(y, y0, sizeof(double) * (size_t)dim);
+    double t = pb->t0;
+    int si = 0;
+    rhs(pb->system, t, y, w->k[k1], p, dim, pb->aux);
+    double dt = initial_step(pb->system, p, y0, w->k[k1], dim, t, pb->rtol, pb->atol, pb->aux,
+                             w->ytmp, w->ftmp);
+    int64_t steps = 0, accepted = 0;
+#define STORE_SAVE(idx, src)                                                                     \
+    do {                                                                                         \
+        if ((idx) >= wb) memcpy(w->win + (size_t)((idx) - wb) * dim, (src), sizeof(double) * dim); \
+        if (y_full)                                                                              \
+            memcpy(y_full + ((size_t)(idx) * (size_t)n_traj + (size_t)traj) * dim, (src),        \
+                   sizeof(double) * dim);                                                        \
+    } while (0)
+
+    while (t < pb->t1 && steps < pb->max_steps) {
+        steps++;
+        if (t + dt > pb->t1) dt = pb->t1 - t;
+        if (dt <= 0.0) break;
+        if (t + dt == t) { status = ORACLE_DT_UNDERFLOW; break; }
+        double *K1 = w->k[k1], *K2 = w->k[1], *K3 = w->k[2], *K4 = w->k[3], *K5 = w->k[4],
+               *K6 = w->k[5], *K7 = w->k[k7];
+        for (int i = 0; i < dim; ++i) ys[i] = y[i] + dt * A21 * K1[i];
+        rhs(pb->system, t + C2 * dt, ys, K2, p, dim, pb->aux);
+        for (int i = 0; i < dim; ++i) ys[i] = y[i] + dt * (A31 * K1[i] + A32 * K2[i]);
+        rhs(pb->system, t + C3 * dt, ys, K3, p, dim, pb->aux);
+        for (int i = 0; i < dim; ++i) ys[i] = y[i] + dt * (A41 * K1[i] + A42 * K2[i] + A43 * K3[i]);
+        rhs(pb->system, t + C4 * dt, ys, K4, p, dim, pb->aux);
+        for (int i = 0; i < dim; ++i)
+            ys[i] = y[i] + dt * (A51 * K1[i] + A52 * K2[i] + A53 * K3[i] + A54 * K4[i]);
+        rhs(pb->system, t + C5 * dt, ys, K5, p, dim, pb->aux);
+        for (int i = 0; i < dim; ++i)
+            ys[i] = y[i] + dt * (A61 * K1[i] + A62 * K2[i] + A63 * K3[i] + A64 * K4[i] + A65 * K5[i]);
+        rhs(pb->system, t + dt, ys, K6, p, dim, pb->aux);
+        for (int i = 0; i < dim; ++i)
+            yn[i] = y[i] + dt * (B1 * K1[i] + B3 * K3[i] + B4 * K4[i] + B5 * K5[i] + B6 * K6[i]);
+        rhs(pb->system, t + dt, yn, K7, p, dim, pb->aux);
+
+        double err = 0.0;
+        for (int i = 0; i < dim; ++i) {
+            double e = dt * (E1 * K1[i] + E3 * K3[i] + E4 * K4[i] + E5 * K5[i] + E6 * K6[i] + E7 * K7[i]);
+            double sc = pb->atol + pb->rtol * fmax(fabs(y[i]), fabs(yn[i]));
+            double r = e / sc;
+            err += r * r;
+        }
+        err = sqrt(err / dim);
+        if (!isfinite(err)) { status = ORACLE_NONFINITE; break; }
+
+        if (err <= 1.0) {
+            double tn = t + dt;
+            accepted++;
+            if (si < ns && pb->save_ts[si] <= tn + 1e-12) {
+                for (int i = 0; i < dim; ++i) {
+                    double ym = y[i] + dt * (M1 * K1[i] + M3 * K3[i] + M4 * K4[i] + M5 * K5[i] +
+                                             M6 * K6[i] + M7 * K7[i]);
+                    w->ia[i] = 2.0 * dt * (K7[i] - K1[i]) - 8.0 * (yn[i] + y[i]) + 16.0 * ym;
+                    w->ib[i] = dt * (5.0 * K1[i] - 3.0 * K7[i]) + 18.0 * y[i] + 14.0 * yn[i] - 32.0 * ym;
+                    w->ic[i] = dt * (K7[i] - 4.0 * K1[i]) - 11.0 * y[i] - 5.0 * yn[i] + 16.0 * ym;
+                }
+                while (si < ns && pb->save_ts[si] <= tn + 1e-12) {
+                    if (pb->save_ts[si] <= t + 1e-12) {
+                        STORE_SAVE(si, y);
+                    } else {
+                        double x = (pb->save_ts[si] - t) / dt;
+                        for (int i = 0; i < dim; ++i)
+                            w->ytmp[i] = y[i] + x * (dt * K1[i] + x * (w->ic[i] + x * (w->ib[i] + x * w->ia[i])));
+                        STORE_SAVE(si, w->ytmp);
+                    }
+                    si++;
+                }
+            }
+            memcpy(y, yn, sizeof(double) * (size_t)dim);
+            t = tn;
+            int tmp = k1; k1 = k7; k7 = tmp;
+            if (pb->unbounded_thr > 0.0) {
+                double m = 0.0;
+                for (int i = 0; i < dim; ++i) m = fmax(m, fabs(y[i]));
+                if (m >= pb->unbounded_thr) { status = ORACLE_UNBOUNDED; break; }
+            }
+        }
+        double dfac = (err <= 1.0) ? 1.0 : MIN_FACTOR;
+        double fac = (err == 0.0) ? MAX_FACTOR : fmin(MAX_FACTOR, fmax(dfac, SAFETY * pow(err, -0.2)));
+        dt *= fac;
+    }
+    if (status == ORACLE_OK && t < pb->t1 && steps >= pb->max_steps) status = ORACLE_MAX_STEPS;
+
+    /* remaining save points: last state (Zig semantics), +inf after a stop event */
+    for (; si < ns; ++si) {
+        if (status == ORACLE_UNBOUNDED) {
+            for (int i = 0; i < dim; ++i) w->ytmp[i] = INFINITY;
+            STORE_SAVE(si, w->ytmp);
+        } else {
+            STORE_SAVE(si, y);
+        }
+    }
+#undef STORE_SAVE
+    if (y_final) memcpy(y_final, y, sizeof(double) * (size_t)dim);
+    if (steps_out) *steps_out = steps;
+    if (accepted_out) *accepted_out = accepted;
+
+    for (int f = 0; feat_out && f < pb->n_features; ++f) {
+        int state = pb->feat_state[f];
+        for (int j = 0; j < nwin; ++j) w->scratch[nwin + j] = w->win[(size_t)j * dim + state];
+        feat_out[f] = window_feature(pb->feat_kind[f], pb->feat_param ? pb->feat_param[f] : 0.0,
+                                     w->scratch + nwin, nwin, w->scratch);
+    }
+    return status;
+}
+
+int oracle_solve_batch(const oracle_problem *pb, const double *y0s, int64_t n_traj,
+                       const double *params, const int32_t *param_index, double *features_out,
+                       int32_t *status_out, double *y_final, double *y_full, int64_t *steps_out,
+                       int64_t *accepted_out, int n_threads)
+{
+    if (!pb || pb->dim <= 0 || n_traj < 0 || pb->n_save < 0 || pb->win_begin < 0 ||
+        pb->win_begin > pb->n_save)
+        return ORACLE_EINVAL;
+    const int dim = pb->dim;
+    const int nwin = pb->n_save - pb->win_begin;
+    int err_flag = 0;
+#ifdef _OPENMP
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel num_threads(n_threads)
+#endif
+    {
+        work_t w;
+        size_t per = (size_t)dim;
+        double *buf = (double *)calloc(per * 18 + (size_t)nwin * dim + 2 * (size_t)nwin + 8, sizeof(double));
+        if (!buf) {
+#ifdef _OPENMP
+#pragma omp atomic write
+#endif
+            err_flag = 1;
+        } else {
+            double *q = buf;
+            w.y = q; q += per; w.ynew = q; q += per; w.ystage = q; q += per;
+            for (int s = 0; s < 7; ++s) { w.k[s] = q; q += per; }
+            w.ia = q; q += per; w.ib = q; q += per; w.ic = q; q += per;
+            w.ytmp = q; q += per; w.ftmp = q; q += per;
+            w.win = q; q += (size_t)nwin * dim;
+            w.scratch = q;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 16)
+#endif
+            for (int64_t j = 0; j < n_traj; ++j) {
+                int64_t prow = param_index ? param_index[j] : 0;
+                int st = solve_one(pb, y0s + (size_t)j * dim, params + (size_t)prow * pb->n_params, &w,
+                                   features_out ? features_out + (size_t)j * pb->n_features : NULL,
+                                   y_final ? y_final + (size_t)j * dim : NULL, y_full, j, n_traj,
+                                   steps_out ? steps_out + j : NULL, accepted_out ? accepted_out + j : NULL);
+                if (status_out) status_out[j] = st;
+            }
+            free(buf);
+        }
+    }
+    return err_flag ? ORACLE_ENOMEM : ORACLE_OK;
+}
+
+/* Feature of one stored window (used to pin the statistics against the reference's calculators). */
+double oracle_window_feature(int kind, double param, const double *w, int n)
+{
+    double *scratch = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    if (!scratch) return NAN;
+    double v = window_feature(kind, param, w, n, scratch);
+    free(scratch);
+    return v;
+}

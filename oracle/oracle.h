@@ -1,0 +1,53 @@
+/* FP64 CPU oracle: test infrastructure only (see dopri5_oracle.c). */
+#ifndef PB_ORACLE_H
+#define PB_ORACLE_H
+#include <stdint.h>
+
+enum {
+    ORACLE_SYS_LINEAR = 0,
+    ORACLE_SYS_PENDULUM = 1,
+    ORACLE_SYS_DUFFING = 2,
+    ORACLE_SYS_LORENZ = 3,
+    ORACLE_SYS_LORENZ_MASKED = 4,
+    ORACLE_SYS_ROSSLER_NET = 5,
+};
+
+/* feature kinds: same numbering as the CUDA library's PB_FEAT_* */
+enum {
+    ORACLE_F_MEDIAN = 0, ORACLE_F_MEAN = 1, ORACLE_F_STD = 2, ORACLE_F_VAR = 3, ORACLE_F_RMS = 4,
+    ORACLE_F_MAX = 5, ORACLE_F_ABSMAX = 6, ORACLE_F_MIN = 7, ORACLE_F_DELTA = 8,
+    ORACLE_F_LOG_DELTA = 9, ORACLE_F_AMPLITUDE = 10, ORACLE_F_CROSSINGS = 11, ORACLE_F_LAST = 12,
+};
+
+enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };
+enum { ORACLE_EINVAL = -5, ORACLE_ENOMEM = -2 };
+
+typedef struct {
+    const int32_t *row_ptr; /* CSR adjacency for network systems (n_nodes + 1) */
+    const int32_t *col_idx;
+} oracle_aux;
+
+typedef struct {
+    int32_t system;
+    int32_t dim;
+    int32_t n_params;
+    int32_t n_save;
+    int32_t win_begin;      /* first save index inside the feature window */
+    int32_t n_features;
+    double t0, t1;
+    const double *save_ts;  /* (n_save,) */
+    double rtol, atol;
+    int64_t max_steps;
+    double unbounded_thr;   /* <= 0: off */
+    const int32_t *feat_state; /* (n_features,) */
+    const int32_t *feat_kind;  /* (n_features,) */
+    const double *feat_param;  /* (n_features,) or NULL */
+    const oracle_aux *aux;
+} oracle_problem;
+
+int oracle_solve_batch(const oracle_problem *pb, const double *y0s, int64_t n_traj,
+                       const double *params, const int32_t *param_index, double *features_out,
+                       int32_t *status_out, double *y_final, double *y_full, int64_t *steps_out,
+                       int64_t *accepted_out, int n_threads);
+double oracle_window_feature(int kind, double param, const double *w, int n);
+#endif

@@ -1,0 +1,195 @@
+"""ctypes binding of the C ABI declared in ``include/pybasin_b200.h``.
+
+The library is built in-tree (``pybasin_b200/_lib/libpybasin_b200.so``).  There
+is no CPU fallback: if the library is missing or CUDA is unavailable, every
+compute entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+from pybasin_b200 import build as _build
+
+# ---- enums mirrored from include/pybasin_b200.h ---------------------------
+PB_SUCCESS = 0
+PB_EINVALID_ODE = -1
+PB_EALLOC = -2
+PB_ESOLVE = -3
+PB_EINVAL = -5
+PB_ECUDA = -6
+PB_EUNSUPPORTED = -7
+PB_ECOMPILE = -8
+
+SYS_LINEAR = 0
+SYS_PENDULUM = 1
+SYS_DUFFING = 2
+SYS_LORENZ = 3
+SYS_LORENZ_MASKED = 4
+SYS_ROSSLER_NET = 5
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+LAYOUT_SINGLE = 0
+LAYOUT_CROSS = 1
+LAYOUT_INDEXED = 2
+
+SCHED_PLAIN = 0
+SCHED_QUEUE = 1
+
+DTYPE_F32 = 0
+DTYPE_F64 = 1
+
+FEAT_MEDIAN = 0
+FEAT_MEAN = 1
+FEAT_STD = 2
+FEAT_VAR = 3
+FEAT_RMS = 4
+FEAT_MAX = 5
+FEAT_ABSMAX = 6
+FEAT_MIN = 7
+FEAT_DELTA = 8
+FEAT_LOG_DELTA = 9
+FEAT_AMPLITUDE = 10
+FEAT_CROSSINGS = 11
+FEAT_LAST = 12
+
+TRAJ_OK = 0
+TRAJ_MAX_STEPS = 1
+TRAJ_DT_UNDERFLOW = 2
+TRAJ_UNBOUNDED = 3
+TRAJ_NONFINITE = 4
+
+MAX_FEATURES = 32
+MAX_CROSSING = 4
+MAX_PARAMS = 8
+
+_c_i32 = ctypes.c_int32
+_c_i64 = ctypes.c_int64
+_c_dbl = ctypes.c_double
+_c_vp = ctypes.c_void_p
+
+
+class SolveArgs(ctypes.Structure):
+    """Mirror of ``pb_solve_args``."""
+
+    _fields_ = [
+        ("system", _c_i32),
+        ("dim", _c_i32),
+        ("precision", _c_i32),
+        ("schedule", _c_i32),
+        ("layout", _c_i32),
+        ("y0_dtype", _c_i32),
+        ("n_params", _c_i32),
+        ("block_size", _c_i32),
+        ("grid_blocks", _c_i32),
+        ("_pad0", _c_i32),
+        ("n_ic", _c_i64),
+        ("n_param_rows", _c_i64),
+        ("n_traj", _c_i64),
+        ("y0", _c_vp),
+        ("params", _c_vp),
+        ("param_index", _c_vp),
+        ("csr_row", _c_vp),
+        ("csr_col", _c_vp),
+        ("t0", _c_dbl),
+        ("t1", _c_dbl),
+        ("save_ts", _c_vp),
+        ("n_save", _c_i32),
+        ("win_begin", _c_i32),
+        ("rtol", _c_dbl),
+        ("atol", _c_dbl),
+        ("max_steps", _c_i64),
+        ("unbounded_thr", _c_dbl),
+        ("n_features", _c_i32),
+        ("_pad1", _c_i32),
+        ("feat_state", _c_i32 * MAX_FEATURES),
+        ("feat_kind", _c_i32 * MAX_FEATURES),
+        ("feat_param", _c_dbl * MAX_FEATURES),
+        ("features_out", _c_vp),
+        ("status_out", _c_vp),
+        ("y_final_out", _c_vp),
+        ("y_full_out", _c_vp),
+        ("y_out_dtype", _c_i32),
+        ("_pad2", _c_i32),
+        ("steps_out", _c_vp),
+        ("queue_counter", _c_vp),
+        ("median_scratch", _c_vp),
+    ]
+
+
+class PbError(RuntimeError):
+    """A pb_* entry point returned a non-zero status."""
+
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where} failed: {error_string(code)} (code {code})")
+
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+EXPORTED_SYMBOLS = (
+    "pb_solve_batch",
+    "pb_solve_scratch_bytes",
+    "pb_label_nearest",
+    "pb_query_occupancy",
+    "pb_error_string",
+    "pb_abi_version",
+    "pb_probe_fma",
+)
+
+
+def library_path() -> Path:
+    return _build.lib_path()
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Load (building first if needed) the CUDA library; raises if it cannot."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        if build_if_missing and _build.is_stale():
+            _build.build()
+        if not path.exists():
+            raise RuntimeError(
+                f"pybasin_b200 CUDA library not found at {path}; build it with `python -m pybasin_b200.build`"
+            )
+        lib = ctypes.CDLL(str(path))
+        lib.pb_solve_batch.restype = ctypes.c_int
+        lib.pb_solve_batch.argtypes = [ctypes.POINTER(SolveArgs), _c_vp]
+        lib.pb_solve_scratch_bytes.restype = _c_i64
+        lib.pb_solve_scratch_bytes.argtypes = [ctypes.POINTER(SolveArgs)]
+        lib.pb_label_nearest.restype = ctypes.c_int
+        lib.pb_label_nearest.argtypes = [
+            _c_vp, _c_i64, _c_i32, _c_vp, _c_i32, _c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp, _c_vp, _c_vp,
+        ]
+        lib.pb_query_occupancy.restype = ctypes.c_int
+        lib.pb_query_occupancy.argtypes = [
+            _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32),
+        ]
+        lib.pb_error_string.restype = ctypes.c_char_p
+        lib.pb_error_string.argtypes = [_c_i32]
+        lib.pb_probe_fma.restype = ctypes.c_int
+        lib.pb_probe_fma.argtypes = [_c_i32, _c_i32, _c_i32, _c_vp, _c_vp]
+        lib.pb_abi_version.restype = _c_i32
+        lib.pb_abi_version.argtypes = []
+        _lib = lib
+        return lib
+
+
+def error_string(code: int) -> str:
+    try:
+        return load(build_if_missing=False).pb_error_string(code).decode()
+    except Exception:  # library unavailable: still produce a message
+        return f"pb status {code}"
+
+
+def check(code: int, where: str) -> None:
+    if code != PB_SUCCESS:
+        raise PbError(code, where)

@@ -1,0 +1,372 @@
+// C ABI of the B200 fused Dopri5 + feature library: argument checks, kernel
+// selection (system x precision x schedule), the median pass and 1-NN labelling.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "pb_dopri5.cuh"
+#include "pybasin_b200.h"
+
+namespace pb {
+
+// ---------------------------------------------------------------------------
+// exact lower median of a window row (torch.median semantics: the lower of the
+// two middle values, NaN if the row holds a NaN), by 4-pass radix select on
+// order-preserving 32-bit keys.  One warp per (trajectory, median column).
+// ---------------------------------------------------------------------------
+struct MedianPlan {
+    int n_med;
+    int col[PB_MAX_FEATURES];
+};
+
+__device__ __forceinline__ uint32_t float_key(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k)
+{
+    const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+__global__ void __launch_bounds__(256) k_median(const float* __restrict__ win, int64_t n_traj, int nwin,
+                                                MedianPlan plan, double* __restrict__ out, int n_features)
+{
+    __shared__ unsigned hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
+    if (row >= n_traj * plan.n_med) return;  // warp-uniform
+    const float* x = win + row * nwin;
+    unsigned* h = hist[warp];
+    // NaN anywhere -> NaN
+    bool nan_seen = false;
+    for (int i = lane; i < nwin; i += 32) nan_seen |= isnan(x[i]);
+    const int64_t traj = row / plan.n_med;
+    const int col = plan.col[row - traj * plan.n_med];
+    if (__any_sync(0xffffffffu, nan_seen)) {
+        if (lane == 0) out[traj * n_features + col] = CUDART_NAN;
+        return;
+    }
+    unsigned k = static_cast<unsigned>((nwin - 1) / 2);  // rank of the lower median
+    uint32_t prefix = 0, prefix_mask = 0;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+        for (int b = lane; b < 256; b += 32) h[b] = 0;
+        __syncwarp();
+        for (int i = lane; i < nwin; i += 32) {
+            const uint32_t key = float_key(x[i]);
+            if ((key & prefix_mask) == prefix) atomicAdd(&h[(key >> shift) & 0xffu], 1u);
+        }
+        __syncwarp();
+        // lane 0 scans the 256 bins to find the bin holding rank k
+        unsigned sel = 0, before = 0;
+        if (lane == 0) {
+            unsigned acc = 0;
+            for (int b = 0; b < 256; ++b) {
+                if (acc + h[b] > k) {
+                    sel = static_cast<unsigned>(b);
+                    before = acc;
+                    break;
+                }
+                acc += h[b];
+            }
+        }
+        sel = __shfl_sync(0xffffffffu, sel, 0);
+        before = __shfl_sync(0xffffffffu, before, 0);
+        k -= before;
+        prefix |= sel << shift;
+        prefix_mask |= 0xffu << shift;
+        __syncwarp();
+    }
+    if (lane == 0) out[traj * n_features + col] = static_cast<double>(key_float(prefix));
+}
+
+// ---------------------------------------------------------------------------
+// 1-NN labelling + per-group counts.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double impute_extreme(double v)
+{
+    if (isnan(v)) return 1e10;
+    if (isinf(v)) return v > 0 ? 1e10 : -1e10;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_label_nearest(const double* __restrict__ feat, int64_t n, int nf,
+                                                       const double* __restrict__ tpl, int nt,
+                                                       const int32_t* __restrict__ tpl_label, int n_classes,
+                                                       const int32_t* __restrict__ status,
+                                                       const int32_t* __restrict__ group_of, int n_groups,
+                                                       int32_t* __restrict__ labels,
+                                                       unsigned long long* __restrict__ counts)
+{
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int cls;
+    if (status && status[i] == PB_TRAJ_UNBOUNDED) {
+        cls = n_classes;
+    } else {
+        double best = CUDART_INF;
+        int arg = 0;
+        for (int t = 0; t < nt; ++t) {
+            double d2 = 0.0;
+            for (int f = 0; f < nf; ++f) {
+                const double d = impute_extreme(feat[i * nf + f]) - impute_extreme(__ldg(tpl + t * nf + f));
+                d2 += d * d;
+            }
+            if (d2 < best) {  // first minimum wins on ties
+                best = d2;
+                arg = t;
+            }
+        }
+        cls = __ldg(tpl_label + arg);
+    }
+    labels[i] = cls;
+    const int g = group_of ? group_of[i] : 0;
+    if (g >= 0 && g < n_groups) atomicAdd(counts + static_cast<int64_t>(g) * (n_classes + 1) + cls, 1ull);
+}
+
+// ---------------------------------------------------------------------------
+// FMA-pipe throughput probe (roofline denominator for the integrator kernels)
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_probe_fma(int iters, float* __restrict__ sink)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    T a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = static_cast<T>(tid * 1e-7 + j * 1e-3);
+    const T m = static_cast<T>(0.9999999), c = static_cast<T>(1e-7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fma(a[j], m, c);
+    }
+    T acc = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc += a[j];
+    sink[tid] = static_cast<float>(acc);
+}
+
+// ---------------------------------------------------------------------------
+// kernel selection
+// ---------------------------------------------------------------------------
+using kernel_fn = void (*)(const pb_solve_args);
+
+template <class Sys>
+kernel_fn select_kernel(int precision, int schedule)
+{
+    if (precision == PB_PREC_FP64)
+        return schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, double, false> : k_solve_plain<Sys, double, false>;
+    return schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, float, true> : k_solve_plain<Sys, float, true>;
+}
+
+static kernel_fn find_kernel(int system, int dim, int precision, int schedule)
+{
+    if (precision != PB_PREC_FP64 && precision != PB_PREC_MIXED) return nullptr;
+    if (schedule != PB_SCHED_PLAIN && schedule != PB_SCHED_QUEUE) return nullptr;
+    switch (system) {
+        case PB_SYS_LINEAR:
+            switch (dim) {
+                case 1: return select_kernel<SysLinear<1>>(precision, schedule);
+                case 2: return select_kernel<SysLinear<2>>(precision, schedule);
+                case 3: return select_kernel<SysLinear<3>>(precision, schedule);
+                case 4: return select_kernel<SysLinear<4>>(precision, schedule);
+                default: return nullptr;
+            }
+        case PB_SYS_PENDULUM: return dim == 2 ? select_kernel<SysPendulum>(precision, schedule) : nullptr;
+        case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision, schedule) : nullptr;
+        case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision, schedule) : nullptr;
+        case PB_SYS_LORENZ_MASKED:
+            return dim == 3 ? select_kernel<SysLorenz<true>>(precision, schedule) : nullptr;
+        default: return nullptr;
+    }
+}
+
+static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
+{
+    int m = 0;
+    for (int c = 0; c < a.n_features; ++c)
+        if (a.feat_kind[c] == PB_FEAT_MEDIAN) {
+            if (plan) plan->col[m] = c;
+            ++m;
+        }
+    if (plan) plan->n_med = m;
+    return m;
+}
+
+static int map_cuda(cudaError_t e)
+{
+    if (e == cudaSuccess) return PB_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return PB_EALLOC;
+    if (e == cudaErrorLaunchFailure || e == cudaErrorLaunchOutOfResources || e == cudaErrorInvalidConfiguration)
+        return PB_ESOLVE;
+    return PB_ECUDA;
+}
+
+static int validate(const pb_solve_args* a)
+{
+    if (!a) return PB_EINVAL;
+    if (a->n_traj < 0 || a->n_ic < 0 || a->dim <= 0) return PB_EINVAL;
+    if (a->n_traj > 0 && (!a->y0 || !a->params || !a->save_ts)) return PB_EINVAL;
+    if (a->n_params < 0 || a->n_params > PB_MAX_PARAMS) return PB_EINVAL;
+    if (a->n_save < 1 || a->win_begin < 0 || a->win_begin >= a->n_save) return PB_EINVAL;
+    if (a->n_features < 0 || a->n_features > PB_MAX_FEATURES) return PB_EINVAL;
+    if (a->y0_dtype != PB_DTYPE_F32 && a->y0_dtype != PB_DTYPE_F64) return PB_EINVAL;
+    if (a->y_out_dtype != PB_DTYPE_F32 && a->y_out_dtype != PB_DTYPE_F64) return PB_EINVAL;
+    if (!(a->rtol >= 0.0) || !(a->atol >= 0.0) || !(a->rtol + a->atol > 0.0)) return PB_EINVAL;
+    if (!(a->t1 >= a->t0) || a->max_steps < 0) return PB_EINVAL;
+    int n_cross = 0;
+    for (int c = 0; c < a->n_features; ++c) {
+        if (a->feat_state[c] < 0 || a->feat_state[c] >= a->dim) return PB_EINVAL;
+        if (a->feat_kind[c] < PB_FEAT_MEDIAN || a->feat_kind[c] > PB_FEAT_LAST) return PB_EINVAL;
+        n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
+    }
+    if (n_cross > PB_MAX_CROSSING) return PB_EUNSUPPORTED;
+    if (a->n_features > 0 && !a->features_out) return PB_EINVAL;
+    if (count_median_cols(*a, nullptr) > 0 && !a->median_scratch) return PB_EINVAL;
+    switch (a->layout) {
+        case PB_LAYOUT_SINGLE:
+            if (a->n_ic < a->n_traj || a->n_param_rows < 1) return PB_EINVAL;
+            break;
+        case PB_LAYOUT_CROSS:
+            if (a->n_param_rows < 1 || a->n_ic * a->n_param_rows != a->n_traj) return PB_EINVAL;
+            break;
+        case PB_LAYOUT_INDEXED:
+            if (!a->param_index && a->n_traj > 0) return PB_EINVAL;
+            if (a->n_ic < a->n_traj || a->n_param_rows < 1) return PB_EINVAL;
+            break;
+        default: return PB_EINVAL;
+    }
+    if (a->schedule == PB_SCHED_QUEUE && !a->queue_counter) return PB_EINVAL;
+    if (a->block_size < 0 || (a->block_size % 32) != 0 || a->block_size > 256) return PB_EINVAL;
+    return PB_SUCCESS;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" {
+
+int32_t pb_abi_version(void) { return 100; }
+
+const char* pb_error_string(int32_t s)
+{
+    switch (s) {
+        case PB_SUCCESS: return "success";
+        case PB_EINVALID_ODE: return "invalid ODE: unknown system id / dimension";
+        case PB_EALLOC: return "device memory allocation failed";
+        case PB_ESOLVE: return "solver kernel failed to launch or run";
+        case PB_EINVAL: return "invalid argument";
+        case PB_ECUDA: return "CUDA runtime error";
+        case PB_EUNSUPPORTED: return "unsupported request";
+        case PB_ECOMPILE: return "runtime compilation of the right-hand side failed";
+        default: return "unknown error";
+    }
+}
+
+int64_t pb_solve_scratch_bytes(const pb_solve_args* a)
+{
+    if (!a) return -1;
+    const int m = count_median_cols(*a, nullptr);
+    if (m == 0) return 0;
+    return static_cast<int64_t>(a->n_traj) * m * (a->n_save - a->win_begin) * static_cast<int64_t>(sizeof(float));
+}
+
+int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule, int32_t block_size,
+                       int32_t* blocks_per_sm, int32_t* num_sms)
+{
+    kernel_fn k = find_kernel(system, dim, precision, schedule);
+    if (!k) return PB_EINVALID_ODE;
+    if (block_size <= 0 || block_size % 32 || block_size > 256) return PB_EINVAL;
+    int dev = 0, bps = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, block_size, 0);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (blocks_per_sm) *blocks_per_sm = bps;
+    if (num_sms) *num_sms = sms;
+    return PB_SUCCESS;
+}
+
+int pb_solve_batch(const pb_solve_args* args, void* stream)
+{
+    int v = validate(args);
+    if (v != PB_SUCCESS) return v;
+    const pb_solve_args& a = *args;
+    kernel_fn k = find_kernel(a.system, a.dim, a.precision, a.schedule);
+    if (!k) return PB_EINVALID_ODE;
+    if (a.n_traj == 0) return PB_SUCCESS;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int block = a.block_size > 0 ? a.block_size : 128;
+    int64_t grid;
+    if (a.schedule == PB_SCHED_QUEUE) {
+        if (a.grid_blocks > 0) {
+            grid = a.grid_blocks;
+        } else {
+            int dev = 0, sms = 0, bps = 0;
+            cudaError_t e = cudaGetDevice(&dev);
+            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, block, 0);
+            if (e != cudaSuccess) return map_cuda(e);
+            grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
+        }
+        const int64_t need = (a.n_traj + block - 1) / block;
+        if (grid > need) grid = need;
+        cudaError_t e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return map_cuda(e);
+    } else {
+        grid = (a.n_traj + block - 1) / block;
+    }
+    if (grid > 0x7fffffffLL) return PB_EINVAL;
+    k<<<static_cast<unsigned>(grid), block, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return map_cuda(e);
+    MedianPlan plan;
+    if (count_median_cols(a, &plan) > 0) {
+        const int64_t rows = a.n_traj * plan.n_med;
+        const int64_t blocks = (rows + 7) / 8;
+        if (blocks > 0x7fffffffLL) return PB_EINVAL;
+        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(a.median_scratch, a.n_traj, a.n_save - a.win_begin,
+                                                               plan, a.features_out, a.n_features);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return map_cuda(e);
+    }
+    return PB_SUCCESS;
+}
+
+int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, void* stream)
+{
+    if (blocks <= 0 || iters <= 0 || !sink) return PB_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (precision == PB_PREC_FP64)
+        k_probe_fma<double><<<blocks, 256, 0, st>>>(iters, sink);
+    else if (precision == PB_PREC_MIXED)
+        k_probe_fma<float><<<blocks, 256, 0, st>>>(iters, sink);
+    else
+        return PB_EINVAL;
+    return map_cuda(cudaGetLastError());
+}
+
+int pb_label_nearest(const double* features, int64_t n, int32_t n_features, const double* templates,
+                     int32_t n_templates, const int32_t* tpl_label, int32_t n_classes, const int32_t* status,
+                     const int32_t* group_of, int32_t n_groups, int32_t* labels_out, int64_t* counts_out,
+                     void* stream)
+{
+    if (n < 0 || n_features < 0 || n_templates < 1 || n_classes < 1 || n_groups < 1) return PB_EINVAL;
+    if (!templates || !tpl_label || !labels_out || !counts_out) return PB_EINVAL;
+    if (n > 0 && n_features > 0 && !features) return PB_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(counts_out, 0, sizeof(int64_t) * n_groups * (n_classes + 1), st);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (n == 0) return PB_SUCCESS;
+    const int64_t blocks = (n + 255) / 256;
+    if (blocks > 0x7fffffffLL) return PB_EINVAL;
+    k_label_nearest<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
+        features, n, n_features, templates, n_templates, tpl_label, n_classes, status, group_of, n_groups,
+        labels_out, reinterpret_cast<unsigned long long*>(counts_out));
+    e = cudaGetLastError();
+    return map_cuda(e);
+}
+
+}  // extern "C"

@@ -1,0 +1,208 @@
+"""Device-side driver of ``pb_solve_batch`` / ``pb_label_nearest``.
+
+Owns nothing global: every call allocates its outputs through PyTorch's caching
+allocator on the compute device and launches on the given CUDA stream, so
+concurrent calls from several host threads (the reference's estimator runs the
+main and template integrations in a 2-thread pool,
+src/pybasin/basin_stability_estimator.py:499-512) do not interfere.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from pybasin_b200 import _lib as L
+
+
+@dataclass(frozen=True)
+class FeatureColumn:
+    """One output column: feature ``kind`` (a ``pb_feature``) of state ``state``."""
+
+    state: int
+    kind: int
+    param: float = 0.0
+    name: str = ""
+
+
+@dataclass
+class SolveRequest:
+    system: int
+    dim: int
+    y0: torch.Tensor  # (n_ic, dim) f32/f64 on the compute device
+    params: torch.Tensor  # (n_rows, n_params) f64 on the compute device
+    save_ts: torch.Tensor  # (n_save,) f64 on the compute device
+    t_span: tuple[float, float]
+    rtol: float
+    atol: float
+    layout: int = L.LAYOUT_SINGLE
+    param_index: torch.Tensor | None = None  # (n_traj,) int32
+    n_traj: int | None = None
+    win_begin: int = 0
+    columns: list[FeatureColumn] = field(default_factory=list)
+    precision: int = L.PREC_FP64
+    schedule: int = L.SCHED_QUEUE
+    max_steps: int = 16**5
+    unbounded_thr: float = 0.0
+    keep_final: bool = True
+    keep_full: bool = False
+    out_dtype: torch.dtype = torch.float32
+    keep_steps: bool = False
+    block_size: int = 0
+    grid_blocks: int = 0
+
+
+@dataclass
+class SolveResult:
+    features: torch.Tensor | None  # (n_traj, F) f64
+    status: torch.Tensor  # (n_traj,) int32
+    y_final: torch.Tensor | None  # (n_traj, dim)
+    y_full: torch.Tensor | None  # (n_save, n_traj, dim)
+    steps: torch.Tensor | None  # (n_traj,) int64
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _dtype_code(dt: torch.dtype) -> int:
+    if dt == torch.float32:
+        return L.DTYPE_F32
+    if dt == torch.float64:
+        return L.DTYPE_F64
+    raise TypeError(f"unsupported dtype {dt}; expected float32 or float64")
+
+
+def build_args(req: SolveRequest, out: SolveResult, queue: torch.Tensor | None, median: torch.Tensor | None) -> L.SolveArgs:
+    a = L.SolveArgs()
+    n_traj = req.n_traj if req.n_traj is not None else _default_n_traj(req)
+    a.system = req.system
+    a.dim = req.dim
+    a.precision = req.precision
+    a.schedule = req.schedule
+    a.layout = req.layout
+    a.y0_dtype = _dtype_code(req.y0.dtype)
+    a.n_params = req.params.shape[1]
+    a.block_size = req.block_size
+    a.grid_blocks = req.grid_blocks
+    a.n_ic = req.y0.shape[0]
+    a.n_param_rows = req.params.shape[0]
+    a.n_traj = n_traj
+    a.y0 = _ptr(req.y0)
+    a.params = _ptr(req.params)
+    a.param_index = _ptr(req.param_index)
+    a.t0 = float(req.t_span[0])
+    a.t1 = float(req.t_span[1])
+    a.save_ts = _ptr(req.save_ts)
+    a.n_save = req.save_ts.shape[0]
+    a.win_begin = req.win_begin
+    a.rtol = float(req.rtol)
+    a.atol = float(req.atol)
+    a.max_steps = int(req.max_steps)
+    a.unbounded_thr = float(req.unbounded_thr)
+    if len(req.columns) > L.MAX_FEATURES:
+        raise ValueError(f"at most {L.MAX_FEATURES} fused feature columns are supported")
+    a.n_features = len(req.columns)
+    for i, c in enumerate(req.columns):
+        a.feat_state[i] = c.state
+        a.feat_kind[i] = c.kind
+        a.feat_param[i] = float(c.param)
+    a.features_out = _ptr(out.features)
+    a.status_out = _ptr(out.status)
+    a.y_final_out = _ptr(out.y_final)
+    a.y_full_out = _ptr(out.y_full)
+    a.y_out_dtype = _dtype_code(req.out_dtype)
+    a.steps_out = _ptr(out.steps)
+    a.queue_counter = _ptr(queue)
+    a.median_scratch = _ptr(median)
+    return a
+
+
+def _default_n_traj(req: SolveRequest) -> int:
+    if req.layout == L.LAYOUT_CROSS:
+        return req.y0.shape[0] * req.params.shape[0]
+    return req.y0.shape[0]
+
+
+def solve(req: SolveRequest, stream: torch.cuda.Stream | None = None) -> SolveResult:
+    """Launch one fused integration on ``stream`` (asynchronous)."""
+    lib = L.load()
+    dev = req.y0.device
+    if dev.type != "cuda":
+        raise RuntimeError("pybasin_b200 computes on a CUDA device only; y0 must be on cuda")
+    n_traj = req.n_traj if req.n_traj is not None else _default_n_traj(req)
+    req.n_traj = n_traj
+    F = len(req.columns)
+    out = SolveResult(
+        features=torch.empty((n_traj, F), dtype=torch.float64, device=dev) if F else None,
+        status=torch.empty((n_traj,), dtype=torch.int32, device=dev),
+        y_final=torch.empty((n_traj, req.dim), dtype=req.out_dtype, device=dev) if req.keep_final else None,
+        y_full=torch.empty((req.save_ts.shape[0], n_traj, req.dim), dtype=req.out_dtype, device=dev)
+        if req.keep_full
+        else None,
+        steps=torch.empty((n_traj,), dtype=torch.int64, device=dev) if req.keep_steps else None,
+    )
+    queue = torch.zeros((1,), dtype=torch.int64, device=dev) if req.schedule == L.SCHED_QUEUE else None
+    args = build_args(req, out, queue, None)
+    nbytes = lib.pb_solve_scratch_bytes(ctypes.byref(args))
+    median = None
+    if nbytes > 0:
+        median = torch.empty((nbytes // 4,), dtype=torch.float32, device=dev)
+        args.median_scratch = median.data_ptr()
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    L.check(lib.pb_solve_batch(ctypes.byref(args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
+    # keep scratch alive until the kernels using it are done
+    if queue is not None:
+        queue.record_stream(s)
+    if median is not None:
+        median.record_stream(s)
+    return out
+
+
+def label_nearest(
+    features: torch.Tensor,
+    templates: torch.Tensor,
+    template_class: torch.Tensor,
+    n_classes: int,
+    status: torch.Tensor | None = None,
+    group_of: torch.Tensor | None = None,
+    n_groups: int = 1,
+    stream: torch.cuda.Stream | None = None,
+) -> tuple[torch.Tensor, torch.Tensor]:
+    """1-NN labels (int32, class ``n_classes`` = unbounded) and per-group counts."""
+    lib = L.load()
+    dev = features.device
+    n, nf = features.shape
+    labels = torch.empty((n,), dtype=torch.int32, device=dev)
+    counts = torch.empty((n_groups, n_classes + 1), dtype=torch.int64, device=dev)
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    rc = lib.pb_label_nearest(
+        _ptr(features),
+        n,
+        nf,
+        _ptr(templates),
+        templates.shape[0],
+        _ptr(template_class),
+        n_classes,
+        _ptr(status),
+        _ptr(group_of),
+        n_groups,
+        _ptr(labels),
+        _ptr(counts),
+        ctypes.c_void_p(s.cuda_stream),
+    )
+    L.check(rc, "pb_label_nearest")
+    return labels, counts
+
+
+def occupancy(system: int, dim: int, precision: int, schedule: int, block: int) -> tuple[int, int]:
+    lib = L.load()
+    bps = ctypes.c_int32(0)
+    sms = ctypes.c_int32(0)
+    L.check(
+        lib.pb_query_occupancy(system, dim, precision, schedule, block, ctypes.byref(bps), ctypes.byref(sms)),
+        "pb_query_occupancy",
+    )
+    return bps.value, sms.value

@@ -1,0 +1,179 @@
+"""Fused steady-state features: configuration and the extractor side channel.
+
+``FusedFeatureExtractor`` takes the constructor arguments of the reference's
+``TorchFeatureExtractor`` (src/pybasin/ts_torch/torch_feature_extractor.py:86-127)
+and produces the same columns, names (``state_{i}__{feature}``,
+src/pybasin/feature_extractors/utils.py:34-73), imputation
+(src/pybasin/ts_torch/torch_feature_utilities.py:60-94) and optional z-score
+(torch_feature_extractor.py:269-285).  The statistics themselves are computed
+inside the integration kernel; the solver attaches them to the ``y`` tensor it
+returns and ``extract_features`` reads them back.
+"""
+
+from __future__ import annotations
+
+import threading
+from typing import Any
+
+import torch
+
+from pybasin_b200 import _lib as L
+from pybasin_b200.engine import FeatureColumn
+
+#: Feature names of src/pybasin/ts_torch/settings.py mapped to fused kernels.
+FEATURE_KINDS: dict[str, int] = {
+    "median": L.FEAT_MEDIAN,
+    "mean": L.FEAT_MEAN,
+    "standard_deviation": L.FEAT_STD,
+    "variance": L.FEAT_VAR,
+    "root_mean_square": L.FEAT_RMS,
+    "maximum": L.FEAT_MAX,
+    "absolute_maximum": L.FEAT_ABSMAX,
+    "minimum": L.FEAT_MIN,
+    "delta": L.FEAT_DELTA,
+    "log_delta": L.FEAT_LOG_DELTA,
+    "amplitude": L.FEAT_AMPLITUDE,
+    "number_crossing_m": L.FEAT_CROSSINGS,
+}
+
+#: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).
+MINIMAL_FEATURES: dict[str, Any] = dict.fromkeys(
+    [
+        "median",
+        "mean",
+        "standard_deviation",
+        "variance",
+        "root_mean_square",
+        "maximum",
+        "absolute_maximum",
+        "minimum",
+        "delta",
+        "log_delta",
+    ]
+)
+
+DEFAULT_STEADY_FRACTION = 0.85  # src/pybasin/constants.py
+
+
+def _format_name(base: str, params: dict[str, Any] | None, state: int) -> str:
+    parts = [base]
+    if params:
+        parts.append("__".join(f"{k}_{v}" for k, v in sorted(params.items())))
+    return f"state_{state}__" + "__".join(parts)
+
+
+def columns_for(config: dict[str, Any] | None, state: int) -> list[FeatureColumn]:
+    """Output columns for one state's FCParameters-style config, in config order."""
+    cols: list[FeatureColumn] = []
+    if not config:
+        return cols
+    for fname, plist in config.items():
+        if fname not in FEATURE_KINDS:
+            raise ValueError(
+                f"feature '{fname}' is not one of the fused statistics {sorted(FEATURE_KINDS)}; "
+                "use B200Dopri5Solver(output='full') with the reference TorchFeatureExtractor for other features"
+            )
+        kind = FEATURE_KINDS[fname]
+        if kind == L.FEAT_CROSSINGS:
+            for p in plist or [{"m": 0}]:
+                cols.append(FeatureColumn(state, kind, float(p["m"]), _format_name(fname, p, state)))
+        else:
+            if plist is not None:
+                raise ValueError(f"feature '{fname}' takes no parameters")
+            cols.append(FeatureColumn(state, kind, 0.0, _format_name(fname, None, state)))
+    return cols
+
+
+def impute_extreme(features: torch.Tensor, extreme_value: float = 1e10) -> torch.Tensor:
+    """+inf -> +extreme, -inf -> -extreme, NaN -> +extreme (torch_feature_utilities.py:60-94)."""
+    out = torch.nan_to_num(features, nan=extreme_value, posinf=extreme_value, neginf=-extreme_value)
+    return out
+
+
+class FusedFeatureExtractor:
+    """Reference ``TorchFeatureExtractor`` API over features fused into the solver kernel."""
+
+    def __init__(
+        self,
+        time_steady: float | None = None,
+        features: str | dict[str, Any] | None = "minimal",
+        features_per_state: dict[int, dict[str, Any] | None] | None = None,
+        normalize: bool = True,
+        device: str = "gpu",
+        n_jobs: int | None = None,
+        impute_method: str = "extreme",
+    ):
+        if impute_method != "extreme":
+            raise ValueError("FusedFeatureExtractor supports impute_method='extreme' only")
+        self.time_steady = time_steady
+        if features in ("minimal", "comprehensive"):
+            # 'comprehensive' spans FFT/entropy/... features that are not fused;
+            # the fused kernel offers the minimal set for it.
+            self.features: dict[str, Any] | None = dict(MINIMAL_FEATURES)
+        else:
+            self.features = features  # type: ignore[assignment]
+        self.features_per_state = features_per_state or {}
+        self.normalize = normalize
+        self.device = device
+        self.n_jobs = n_jobs
+        self.impute_method = impute_method
+        self._fit_lock = threading.Lock()
+        self._is_fitted = False
+        self._feature_mean: torch.Tensor | None = None
+        self._feature_std: torch.Tensor | None = None
+        self._extracted_feature_names: list[str] | None = None
+
+    # -- configuration consumed by the solver ---------------------------------
+    def columns(self, num_states: int) -> list[FeatureColumn]:
+        cols: list[FeatureColumn] = []
+        for s in range(num_states):
+            if s in self.features_per_state:
+                cfg = self.features_per_state[s]
+                if cfg is not None:
+                    cols += columns_for(cfg, s)
+            elif self.features is not None:
+                cols += columns_for(self.features, s)
+        return cols
+
+    def resolve_time_steady(self, save_ts: torch.Tensor) -> float:
+        if self.time_steady is not None:
+            return float(self.time_steady)
+        t0, t1 = float(save_ts[0]), float(save_ts[-1])
+        return t0 + DEFAULT_STEADY_FRACTION * (t1 - t0)
+
+    # -- reference FeatureExtractor API ---------------------------------------
+    def extract_features(self, solution: Any) -> torch.Tensor:
+        y = solution.y
+        feats: torch.Tensor | None = getattr(y, "_pb_features", None)
+        names: list[str] | None = getattr(y, "_pb_feature_names", None)
+        if feats is None or names is None:
+            raise RuntimeError(
+                "FusedFeatureExtractor reads features computed inside B200Dopri5Solver; construct the solver "
+                "with feature_extractor=<this extractor> and pass its output solution"
+            )
+        self._extracted_feature_names = list(names)
+        if feats.shape[1] == 0:
+            return feats
+        features = impute_extreme(feats)
+        if self.normalize:
+            with self._fit_lock:
+                if not self._is_fitted:
+                    self._feature_mean = features.mean(dim=0, keepdim=True)
+                    std = features.std(dim=0, keepdim=True)
+                    self._feature_std = torch.where(std == 0, torch.ones_like(std), std)
+                    self._is_fitted = True
+            assert self._feature_mean is not None and self._feature_std is not None
+            features = (features - self._feature_mean.to(features.device)) / self._feature_std.to(features.device)
+        return features
+
+    def reset_scaler(self) -> None:
+        with self._fit_lock:
+            self._feature_mean = None
+            self._feature_std = None
+            self._is_fitted = False
+
+    @property
+    def feature_names(self) -> list[str]:
+        if self._extracted_feature_names is None:
+            raise RuntimeError("Feature names not available. Call extract_features first.")
+        return self._extracted_feature_names

@@ -1,0 +1,197 @@
+"""GPU-resident basin-stability pass: ICs -> fused Dopri5 + features -> 1-NN labels -> counts.
+
+This is the hot path of the reference's ``BasinStabilityEstimator.run`` for a
+supervised 1-NN predictor (src/pybasin/basin_stability_estimator.py:230-361):
+integration of the main and template ICs (:488-517), feature extraction
+(:304-311), ``KNeighborsClassifier(n_neighbors=1)`` fit/predict (:426-446) and
+the basin-stability fractions (:586-598).  Here the template ICs ride in the
+same kernel launch as the main ICs (their own parameter row), the features never
+leave the GPU, labelling is one kernel, and only labels and counts come back.
+
+All buffers are allocated once per batch size so a pass can be captured into a
+CUDA graph and replayed (``use_graph=True``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Any
+
+import numpy as np
+import torch
+
+from pybasin_b200 import _lib as L
+from pybasin_b200.engine import SolveRequest, build_args, SolveResult
+from pybasin_b200.odes import resolve_system
+from pybasin_b200.solver import B200Dopri5Solver
+
+
+class BasinStabilityPipeline:
+    """Labelled ICs for one ODE system and template set on one GPU.
+
+    :param ode_system: reference-style ODE system (params mapping in TypedDict order).
+    :param solver: a ``B200Dopri5Solver`` with a ``FusedFeatureExtractor`` (normalize=False).
+    :param template_y0: template initial conditions (``TemplateIntegrator.template_y0``).
+    :param template_labels: class name of each template.
+    :param template_params: parameters for the templates (default: the system's).
+    """
+
+    def __init__(
+        self,
+        ode_system: Any,
+        solver: B200Dopri5Solver,
+        template_y0: list[list[float]],
+        template_labels: list[str],
+        template_params: dict[str, float] | None = None,
+        device: torch.device | str | None = None,
+    ):
+        fx = solver.feature_extractor
+        if fx is None:
+            raise ValueError("the pipeline needs a solver constructed with a FusedFeatureExtractor")
+        if fx.normalize:
+            raise ValueError("on-device 1-NN labelling uses raw features (FusedFeatureExtractor(normalize=False))")
+        self.solver = solver
+        self.dev = torch.device(device) if device is not None else solver.compute_device()
+        self.dim = len(template_y0[0])
+        self.spec = resolve_system(ode_system, self.dim)
+        self.classes = sorted(set(template_labels), key=template_labels.index)
+        self.n_classes = len(self.classes)
+        self.tpl_class = torch.tensor(
+            [self.classes.index(s) for s in template_labels], dtype=torch.int32, device=self.dev
+        )
+        tparams = (
+            np.asarray(list(template_params.values()), dtype=np.float64)
+            if template_params is not None
+            else self.spec.params
+        )
+        self.params = torch.tensor(np.stack([self.spec.params, tparams]), dtype=torch.float64, device=self.dev)
+        self.template_y0 = torch.tensor(template_y0, dtype=torch.float32, device=self.dev)
+        self.n_tpl = self.template_y0.shape[0]
+        save = solver.save_times(torch.float32)
+        self.save_ts = save.to(torch.float64).to(self.dev)
+        self.columns = fx.columns(self.dim)
+        ts = fx.resolve_time_steady(save)
+        idx = torch.nonzero(save >= ts)
+        self.win_begin = int(idx[0, 0]) if idx.numel() > 0 else 0
+        self.t_span = (float(solver.t_span[0]), float(save[-1]))
+        self._n: int | None = None
+        self._graph: torch.cuda.CUDAGraph | None = None
+        self.stream = torch.cuda.Stream(device=self.dev)
+
+    # -- buffers ---------------------------------------------------------------
+    def _allocate(self, n: int) -> None:
+        dev = self.dev
+        tot = n + self.n_tpl
+        F = len(self.columns)
+        self.y0_buf = torch.empty((tot, self.dim), dtype=torch.float32, device=dev)
+        self.y0_buf[n:] = self.template_y0
+        pidx = torch.zeros((tot,), dtype=torch.int32, device=dev)
+        pidx[n:] = 1
+        self.pidx = pidx
+        self.out = SolveResult(
+            features=torch.empty((tot, F), dtype=torch.float64, device=dev),
+            status=torch.empty((tot,), dtype=torch.int32, device=dev),
+            y_final=None,
+            y_full=None,
+            steps=torch.empty((tot,), dtype=torch.int64, device=dev),
+        )
+        self.queue = torch.zeros((1,), dtype=torch.int64, device=dev)
+        self.labels = torch.empty((n,), dtype=torch.int32, device=dev)
+        self.counts = torch.empty((1, self.n_classes + 1), dtype=torch.int64, device=dev)
+        rtol, atol = self.solver.effective_tolerances()
+        req = SolveRequest(
+            system=self.spec.system,
+            dim=self.dim,
+            y0=self.y0_buf,
+            params=self.params,
+            save_ts=self.save_ts,
+            t_span=self.t_span,
+            rtol=rtol,
+            atol=atol,
+            layout=L.LAYOUT_INDEXED,
+            param_index=self.pidx,
+            n_traj=tot,
+            win_begin=self.win_begin,
+            columns=self.columns,
+            precision=L.PREC_MIXED if self.solver.precision == "mixed" else L.PREC_FP64,
+            schedule=L.SCHED_QUEUE if self.solver.schedule == "queue" else L.SCHED_PLAIN,
+            max_steps=self.solver.max_steps,
+            unbounded_thr=float(self.solver.unbounded_threshold or 0.0),
+            keep_final=False,
+            block_size=self.solver.block_size,
+            grid_blocks=self.solver.grid_blocks,
+        )
+        self.args = build_args(req, self.out, self.queue, None)
+        lib = L.load()
+        if lib.pb_solve_scratch_bytes(ctypes.byref(self.args)) > 0:
+            raise ValueError("median is not supported in the pipeline (needs per-trajectory scratch)")
+        self._n = n
+        self._graph = None
+
+    # -- one pass ----------------------------------------------------------------
+    def _launch(self) -> None:
+        lib = L.load()
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        L.check(lib.pb_solve_batch(ctypes.byref(self.args), s), "pb_solve_batch")
+        n = self._n
+        assert n is not None
+        feats = self.out.features
+        rc = lib.pb_label_nearest(
+            feats.data_ptr(),
+            n,
+            feats.shape[1],
+            feats[n:].data_ptr(),
+            self.n_tpl,
+            self.tpl_class.data_ptr(),
+            self.n_classes,
+            self.out.status.data_ptr(),
+            None,
+            1,
+            self.labels.data_ptr(),
+            self.counts.data_ptr(),
+            s,
+        )
+        L.check(rc, "pb_label_nearest")
+
+    def kernel_launches_per_pass(self) -> int:
+        return 2
+
+    def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
+        """Label device-resident ``y0`` (N, S) on the current stream; asynchronous."""
+        n = y0.shape[0]
+        if self._n != n:
+            self._allocate(n)
+        self.y0_buf[:n].copy_(y0, non_blocking=True)
+        if use_graph:
+            if self._graph is None:
+                self._capture()
+            assert self._graph is not None
+            self._graph.replay()
+        else:
+            self._launch()
+        return self.labels, self.counts
+
+    def _capture(self) -> None:
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):
+            self._launch()  # warm-up outside capture (lazy module loading)
+        s.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            self._launch()
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        self._graph = g
+
+    def run(self, y0_host: torch.Tensor, use_graph: bool = False) -> tuple[np.ndarray, dict[str, float]]:
+        """Host ICs -> (labels as class names, basin stability per class)."""
+        with torch.cuda.device(self.dev):
+            y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
+            labels, counts = self.run_device(y0, use_graph=use_graph)
+            lab = labels.cpu().numpy()
+            cnt = counts.cpu().numpy()[0]
+        names = np.array(self.classes + ["unbounded"], dtype=object)
+        n = max(int(cnt.sum()), 1)
+        bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}
+        return names[lab], bs

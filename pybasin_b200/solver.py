@@ -1,0 +1,315 @@
+"""``B200Dopri5Solver``: the drop-in for the reference's ``TorchDiffEqSolver``.
+
+It satisfies the reference's ``SolverProtocol`` (src/pybasin/protocols.py:116-187):
+``device``, the constructor arguments (``t_span, t_steps, device, method, rtol,
+atol, cache_dir, t_eval``), ``integrate(ode_system, y0, params=None) -> (t, y)``
+and ``clone(*, device, t_steps_factor, cache_dir)``, with the base class's
+argument checks and IC-major parameter expansion
+(src/pybasin/solvers/base.py:36-183).  Integration is the per-trajectory
+Dopri5 kernel of the CUDA library; there is no CPU path.
+
+Two output modes:
+
+* ``output="full"`` returns ``y`` of shape ``(t_steps, B*P, S)`` exactly like the
+  reference solvers, so any reference feature extractor works on it.
+* ``output="fused"`` (the default when a ``FusedFeatureExtractor`` is given)
+  keeps no trajectory: the window statistics are computed inside the kernel,
+  ``y`` is the state at the end of the span with shape ``(1, B*P, S)``, and the
+  features ride on ``y`` for ``FusedFeatureExtractor.extract_features``.
+  Trajectories stopped by the unbounded event get ``inf`` rows (the diffrax
+  convention the reference relies on, basin_stability_estimator.py:519-527).
+"""
+
+from __future__ import annotations
+
+import logging
+import threading
+from typing import Any
+
+import numpy as np
+import torch
+
+from pybasin_b200 import _lib as L
+from pybasin_b200.engine import SolveRequest, solve
+from pybasin_b200.features import FusedFeatureExtractor
+from pybasin_b200.odes import resolve_system
+
+logger = logging.getLogger(__name__)
+
+_UNSET = object()
+
+#: reference default max_steps of the per-trajectory solvers (jax_solver.py:37)
+DEFAULT_MAX_STEPS = 16**5
+
+#: tolerance floor of the FP32-stage kernel: rtol below FP32 resolution makes the
+#: embedded error estimate pure rounding noise (the reference's own docs warn of
+#: stagnation, docs/user-guide/solvers.md:206-211)
+MIXED_RTOL_FLOOR = 1e-6
+
+
+class IntegrationResult(tuple):
+    """``(t, y)`` that also carries ``features``, ``feature_names`` and ``status``."""
+
+    features: torch.Tensor | None
+    feature_names: list[str]
+    status: torch.Tensor
+    steps: torch.Tensor | None
+
+    def __new__(cls, t: torch.Tensor, y: torch.Tensor, **extra: Any) -> "IntegrationResult":
+        obj = super().__new__(cls, (t, y))
+        for k, v in extra.items():
+            setattr(obj, k, v)
+        return obj
+
+
+_streams = threading.local()
+
+
+def _thread_stream(dev: torch.device) -> torch.cuda.Stream:
+    """One non-default stream per (host thread, device): concurrent integrate
+    calls from the estimator's thread pool overlap on the GPU."""
+    cache = getattr(_streams, "by_dev", None)
+    if cache is None:
+        cache = {}
+        _streams.by_dev = cache
+    s = cache.get(dev.index)
+    if s is None:
+        s = torch.cuda.Stream(device=dev)
+        cache[dev.index] = s
+    return s
+
+
+class B200Dopri5Solver:
+    """Adaptive Dormand-Prince 5(4) over many ICs on one B200, fused with features.
+
+    :param t_span: integration interval ``(t0, t1)``.
+    :param t_steps: number of save points in the save region.
+    :param device: device of the returned tensors ('cuda', 'cuda:N', 'cpu' or None).
+        Computation always runs on a CUDA device (``device`` if it is CUDA, else the
+        current CUDA device); a CPU ``device`` only means CPU output tensors, which is
+        what the reference's TemplateIntegrator asks for (template_integrator.py:80-86).
+    :param method: only ``"dopri5"``.
+    :param rtol: relative tolerance (the FP32-stage kernel uses ``max(rtol, mixed_rtol_floor)``).
+    :param atol: absolute tolerance.
+    :param cache_dir: accepted for signature compatibility; results are not cached.
+    :param t_eval: save region ``(save_start, save_end)`` within ``t_span``.
+    :param precision: ``"fp64"`` (plain FP64 kernel) or ``"mixed"`` (FP32 stages and
+        state, FP64 time, error norm and step control).
+    :param feature_extractor: a ``FusedFeatureExtractor`` whose statistics the kernel computes.
+    :param output: ``"fused"`` or ``"full"`` (default: fused iff a feature extractor is given).
+    :param max_steps: attempted steps per trajectory before giving up (status MAX_STEPS).
+    :param unbounded_threshold: stop a trajectory once max|y| >= this after an accepted
+        step (the reference's stop events, e.g. case_studies/lorenz/setup_lorenz_system.py:16-26).
+    :param schedule: ``"queue"`` (persistent lanes + work queue) or ``"plain"``.
+    """
+
+    def __init__(
+        self,
+        t_span: tuple[float, float] = (0, 1000),
+        t_steps: int = 1000,
+        device: str | None = None,
+        method: str = "dopri5",
+        rtol: float = 1e-8,
+        atol: float = 1e-6,
+        cache_dir: str | None = None,
+        t_eval: tuple[float, float] | None = None,
+        *,
+        precision: str = "fp64",
+        feature_extractor: FusedFeatureExtractor | None = None,
+        output: str | None = None,
+        max_steps: int = DEFAULT_MAX_STEPS,
+        unbounded_threshold: float | None = None,
+        schedule: str = "queue",
+        mixed_rtol_floor: float = MIXED_RTOL_FLOOR,
+        block_size: int = 0,
+        grid_blocks: int = 0,
+    ):
+        if t_eval is not None and (t_eval[0] < t_span[0] or t_eval[1] > t_span[1]):
+            raise ValueError(f"t_eval {t_eval} must be within t_span {t_span}.")
+        if method not in ("dopri5", None):
+            raise ValueError(f"B200Dopri5Solver implements method='dopri5' only, got {method!r}")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if output not in (None, "fused", "full"):
+            raise ValueError("output must be 'fused' or 'full'")
+        if schedule not in ("queue", "plain"):
+            raise ValueError("schedule must be 'queue' or 'plain'")
+        if t_steps < 1:
+            raise ValueError("t_steps must be >= 1")
+        self.t_span = t_span
+        self.t_eval = t_eval
+        self.t_steps = t_steps
+        self.method = "dopri5"
+        self.rtol = rtol
+        self.atol = atol
+        self.precision = precision
+        self.feature_extractor = feature_extractor
+        self.output = output or ("fused" if feature_extractor is not None else "full")
+        if self.output == "fused" and feature_extractor is None:
+            raise ValueError("output='fused' needs a FusedFeatureExtractor")
+        self.max_steps = int(max_steps)
+        self.unbounded_threshold = unbounded_threshold
+        self.schedule = schedule
+        self.mixed_rtol_floor = mixed_rtol_floor
+        self.block_size = block_size
+        self.grid_blocks = grid_blocks
+        self._cache_dir = cache_dir
+        self._set_device(device)
+
+    # -- reference Solver surface ---------------------------------------------
+    def _set_device(self, device: str | None) -> None:
+        # same normalisation as src/pybasin/solvers/base.py:73-97
+        self._device_str = device
+        if device is None:
+            self.device = torch.device("cuda:0" if torch.cuda.is_available() else "cpu")
+        else:
+            dev = torch.device(device)
+            if dev.type == "cuda":
+                self.device = torch.device(f"cuda:{dev.index if dev.index is not None else 0}")
+            else:
+                self.device = dev
+
+    def clone(
+        self,
+        *,
+        device: str | None = None,
+        t_steps_factor: int = 1,
+        cache_dir: str | None | object = _UNSET,
+    ) -> "B200Dopri5Solver":
+        """Copy with a new output device / resolution (protocols.py:170-187)."""
+        return B200Dopri5Solver(
+            t_span=self.t_span,
+            t_steps=self.t_steps * t_steps_factor,
+            device=device or self._device_str,
+            method=self.method,
+            rtol=self.rtol,
+            atol=self.atol,
+            cache_dir=self._cache_dir if cache_dir is _UNSET else cache_dir,  # type: ignore[arg-type]
+            t_eval=self.t_eval,
+            precision=self.precision,
+            feature_extractor=self.feature_extractor,
+            output=self.output,
+            max_steps=self.max_steps,
+            unbounded_threshold=self.unbounded_threshold,
+            schedule=self.schedule,
+            mixed_rtol_floor=self.mixed_rtol_floor,
+            block_size=self.block_size,
+            grid_blocks=self.grid_blocks,
+        )
+
+    def compute_device(self) -> torch.device:
+        if not torch.cuda.is_available():
+            raise RuntimeError("B200Dopri5Solver needs a CUDA device; there is no CPU fallback")
+        if self.device.type == "cuda":
+            return self.device
+        return torch.device(f"cuda:{torch.cuda.current_device()}")
+
+    def effective_tolerances(self) -> tuple[float, float]:
+        if self.precision == "mixed":
+            return max(self.rtol, self.mixed_rtol_floor), self.atol
+        return self.rtol, self.atol
+
+    def save_times(self, dtype: torch.dtype) -> torch.Tensor:
+        """Save instants as the reference builds them: linspace in y0's dtype (base.py:113-127)."""
+        s0, s1 = self.t_eval if self.t_eval is not None else self.t_span
+        return torch.linspace(s0, s1, self.t_steps, dtype=dtype)
+
+    def integrate(
+        self, ode_system: Any, y0: torch.Tensor, params: torch.Tensor | None = None
+    ) -> IntegrationResult:
+        """Integrate every row of ``y0`` (against every row of ``params`` if given).
+
+        Returns ``(t, y)``; ``y`` has shape ``(t_steps, B*P, S)`` in full mode and
+        ``(1, B*P, S)`` in fused mode, trajectory ``ic*P + p`` carrying
+        ``(y0[ic], params[p])`` (base.py:155-159).
+        """
+        if y0.ndim != 2:
+            raise ValueError(
+                f"y0 must be 2D with shape (batch, n_dims), got shape {tuple(y0.shape)}. "
+                f"For single initial condition, use y0.unsqueeze(0) or y0.reshape(1, -1)."
+            )
+        if y0.dtype not in (torch.float32, torch.float64):
+            raise TypeError(f"y0 must be float32 or float64, got {y0.dtype}")
+        B, S = y0.shape
+        spec = resolve_system(ode_system, S)
+        dev = self.compute_device()
+        stream = _thread_stream(dev)
+        save_host = self.save_times(y0.dtype)
+        save_f64 = save_host.to(torch.float64)
+        t0 = float(self.t_span[0])
+        t1 = float(save_f64[-1])
+        if params is not None:
+            if params.ndim != 2:
+                raise ValueError("params must be 2D with shape (P, n_params)")
+            p_rows = params.detach().to(torch.float64).cpu().numpy()
+            layout = L.LAYOUT_CROSS
+        else:
+            p_rows = spec.params[None, :]
+            layout = L.LAYOUT_SINGLE
+        P = p_rows.shape[0]
+        n_traj = B * P if params is not None else B
+        cols = self.feature_extractor.columns(S) if self.feature_extractor is not None else []
+        if cols:
+            ts = self.feature_extractor.resolve_time_steady(save_host)  # type: ignore[union-attr]
+            idx = torch.nonzero(save_host >= ts)
+            win_begin = int(idx[0, 0]) if idx.numel() > 0 else 0
+        else:
+            win_begin = 0
+        rtol, atol = self.effective_tolerances()
+        full = self.output == "full"
+        stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.device(dev), torch.cuda.stream(stream):
+            y0_dev = y0.detach().to(dev, non_blocking=False).contiguous()
+            params_dev = torch.as_tensor(np.ascontiguousarray(p_rows), device=dev)
+            save_dev = save_f64.to(dev)
+            req = SolveRequest(
+                system=spec.system,
+                dim=S,
+                y0=y0_dev,
+                params=params_dev,
+                save_ts=save_dev,
+                t_span=(t0, t1),
+                rtol=rtol,
+                atol=atol,
+                layout=layout,
+                n_traj=n_traj,
+                win_begin=win_begin,
+                columns=cols,
+                precision=L.PREC_MIXED if self.precision == "mixed" else L.PREC_FP64,
+                schedule=L.SCHED_QUEUE if self.schedule == "queue" else L.SCHED_PLAIN,
+                max_steps=self.max_steps,
+                unbounded_thr=float(self.unbounded_threshold or 0.0),
+                keep_final=not full,
+                keep_full=full,
+                out_dtype=y0.dtype,
+                block_size=self.block_size,
+                grid_blocks=self.grid_blocks,
+            )
+            res = solve(req, stream)
+            if full:
+                y = res.y_full
+                t = save_host.to(self.device)
+            else:
+                y = res.y_final.unsqueeze(0)  # type: ignore[union-attr]
+                t = save_host[-1:].to(self.device)
+            status = res.status
+            feats = res.features.to(y0.dtype) if res.features is not None else None
+            if not full:
+                unb = (status == L.TRAJ_UNBOUNDED).view(1, -1, 1)
+                y = torch.where(unb, torch.full_like(y, float("inf")), y)
+        stream.synchronize()
+        y = y.to(self.device)  # type: ignore[union-attr]
+        status = status.to(self.device)
+        if feats is not None:
+            feats = feats.to(self.device)
+        names = [c.name for c in cols]
+        if feats is None:
+            feats = torch.zeros((n_traj, 0), dtype=y0.dtype, device=self.device)
+        # side channel read by FusedFeatureExtractor.extract_features
+        y._pb_features = feats  # type: ignore[attr-defined]
+        y._pb_feature_names = names  # type: ignore[attr-defined]
+        y._pb_status = status  # type: ignore[attr-defined]
+        n_bad = int((status == L.TRAJ_MAX_STEPS).sum()) + int((status == L.TRAJ_NONFINITE).sum())
+        if n_bad:
+            logger.warning("B200Dopri5Solver: %d trajectories hit max_steps or went non-finite", n_bad)
+        return IntegrationResult(t, y, features=feats, feature_names=names, status=status, steps=None)

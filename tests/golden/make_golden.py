@@ -1,0 +1,157 @@
+"""Generate the golden fixtures under tests/golden/ from the pybasin reference.
+
+Run once in a container where the reference tree is present:
+
+    python tests/golden/make_golden.py /root/reference
+
+It imports the reference (with empty stand-in modules for the two imports that
+are not installed, ``torchdiffeq`` and ``matplotlib``; neither is on the paths
+used here) and writes:
+
+* ``labels_pendulum_case1.npz`` / ``labels_duffing_main.npz`` — the reference's
+  seeded label fixtures (tests/integration/pendulum/ground_truths/case1/
+  main_pendulum_case1.csv, tests/integration/duffing/ground_truths/main/
+  main_duffing.csv; seed 42, N=4000) as class indices plus class names, with the
+  basin-stability counts of main_pendulum_case1.json / main_duffing_supervised.json.
+* ``features_reference.npz`` — outputs of the reference's own feature
+  calculators (src/pybasin/ts_torch/calculators/torch_features_statistical.py,
+  torch_features_pattern.py) on seeded random windows, to pin the statistics.
+* ``scipy_reference.npz`` — the reference's ScipyParallelSolver
+  (src/pybasin/solvers/scipy_solver.py) on a few seeded pendulum and Duffing ICs
+  over a short horizon at tight tolerance, to pin trajectories.
+"""
+
+from __future__ import annotations
+
+import json
+import sys
+import tempfile
+import types
+from pathlib import Path
+
+import numpy as np
+import pandas as pd
+import torch
+
+OUT = Path(__file__).resolve().parent
+
+
+def _install_stubs() -> None:
+    tmp = Path(tempfile.mkdtemp(prefix="pb_stubs_"))
+    (tmp / "torchdiffeq").mkdir()
+    (tmp / "torchdiffeq" / "__init__.py").write_text(
+        "def odeint(*a, **k):\n    raise RuntimeError('torchdiffeq is not installed')\n"
+    )
+    mpl = tmp / "matplotlib"
+    mpl.mkdir()
+    (mpl / "__init__.py").write_text("def use(*a, **k):\n    pass\n")
+    (mpl / "pyplot.py").write_text("def __getattr__(name):\n    raise AttributeError(name)\n")
+    (mpl / "figure.py").write_text("class Figure: pass\n")
+    (mpl / "axes.py").write_text("class Axes: pass\n")
+    (mpl / "colors.py").write_text("def __getattr__(name):\n    raise AttributeError(name)\n")
+    sys.path.insert(0, str(tmp))
+
+
+def _labels(ref: Path, csv: str, js: str, classes: list[str], name: str) -> None:
+    df = pd.read_csv(ref / csv)
+    meta = json.loads((ref / js).read_text())
+    label_map = meta.get("label_map", {})
+    idx = {c: i for i, c in enumerate(classes)}
+    lab = np.array([idx[s] for s in df["label"].astype(str)], dtype=np.int8)
+    counts = {label_map.get(d["label"], d["label"]): int(d["absNumMembers"]) for d in meta["data"]}
+    np.savez_compressed(
+        OUT / name,
+        labels=lab,
+        classes=np.array(classes),
+        ics=df[["x1", "x2"]].to_numpy(np.float32),
+        counts=np.array([counts.get(c, 0) for c in classes], dtype=np.int64),
+    )
+
+
+def _features(ref: Path) -> None:
+    from pybasin.ts_torch.calculators import torch_features_pattern as pat
+    from pybasin.ts_torch.calculators import torch_features_statistical as st
+
+    g = torch.Generator().manual_seed(1234)
+    n_t, n_b = 257, 16
+    x = torch.randn(n_t, n_b, 2, generator=g, dtype=torch.float64) * 3.0 + 0.5
+    x[:, 3, 0] = 2.0  # constant row
+    x[::2, 5, 1] = -x[::2, 5, 1]  # sign flips for crossings
+    even = torch.randn(256, n_b, 2, generator=g, dtype=torch.float64)  # even length: lower median
+    res = {
+        "x": x.numpy(),
+        "x_even": even.numpy(),
+        "median": st.median(x).numpy(),
+        "median_even": st.median(even).numpy(),
+        "mean": st.mean(x).numpy(),
+        "standard_deviation": st.standard_deviation(x).numpy(),
+        "variance": st.variance(x).numpy(),
+        "root_mean_square": st.root_mean_square(x).numpy(),
+        "maximum": st.maximum(x).numpy(),
+        "absolute_maximum": st.absolute_maximum(x).numpy(),
+        "minimum": st.minimum(x).numpy(),
+        "delta": st.delta(x).numpy(),
+        "log_delta": st.log_delta(x).numpy(),
+        "amplitude": st.amplitude(x).numpy(),
+        "number_crossing_m_0": pat.number_crossing_m(x, 0).numpy(),
+        "number_crossing_m_1": pat.number_crossing_m(x, 1).numpy(),
+    }
+    np.savez_compressed(OUT / "features_reference.npz", **res)
+
+
+def _scipy(ref: Path) -> None:
+    sys.path.insert(0, str(ref))
+    from case_studies.duffing_oscillator.duffing_ode import DuffingODE  # noqa: F401  (torch variant)
+    from case_studies.pendulum.pendulum_ode import PendulumNumpyODE
+    from pybasin.solvers import ScipyParallelSolver
+    from pybasin.solvers.numpy_ode_system import NumpyODESystem
+
+    class DuffingNumpyODE(NumpyODESystem):  # the reference ships only torch/JAX Duffing variants
+        def ode(self, t, y, p):
+            return np.array([y[1], -p[0] * y[1] - p[1] * y[0] ** 3 + p[2] * np.cos(t)])
+
+    out = {}
+    torch.manual_seed(7)
+    for key, ode, lo, hi in (
+        ("pendulum", PendulumNumpyODE({"alpha": 0.1, "T": 0.5, "K": 1.0}), [-2.6, -10.0], [3.7, 10.0]),
+        ("duffing", DuffingNumpyODE({"delta": 0.08, "k3": 1.0, "A": 0.2}), [-1.0, -0.5], [1.0, 1.0]),
+    ):
+        lo_t, hi_t = torch.tensor(lo), torch.tensor(hi)
+        y0 = torch.rand(8, 2) * (hi_t - lo_t) + lo_t
+        solver = ScipyParallelSolver(
+            t_span=(0, 20), t_steps=41, n_jobs=1, rtol=1e-11, atol=1e-12, max_step=0.05, cache_dir=None
+        )
+        t, y = solver.integrate(ode, y0.double())
+        out[f"{key}_y0"] = y0.numpy()
+        out[f"{key}_t"] = t.double().numpy()
+        out[f"{key}_y"] = y.double().numpy()
+    np.savez_compressed(OUT / "scipy_reference.npz", **out)
+
+
+def main() -> None:
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    _install_stubs()
+    sys.path.insert(0, str(ref / "src"))
+    it = ref / "tests" / "integration"
+    _labels(
+        it,
+        "pendulum/ground_truths/case1/main_pendulum_case1.csv",
+        "pendulum/main_pendulum_case1.json",
+        ["FP", "LC"],
+        "labels_pendulum_case1.npz",
+    )
+    _labels(
+        it,
+        "duffing/ground_truths/main/main_duffing.csv",
+        "duffing/main_duffing_supervised.json",
+        [f"$\\bar{{y}}_{i}$" for i in range(1, 6)],
+        "labels_duffing_main.npz",
+    )
+    _features(ref)
+    _scipy(ref)
+    for p in sorted(OUT.glob("*.npz")):
+        print(p.name, p.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+"""Pin the FP64 CPU oracle to the reference's golden vectors (CPU only)."""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.helpers import (
+    DUFFING,
+    PENDULUM,
+    knn_labels,
+    oracle_case_features,
+    seeded_ics,
+)
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def test_seeded_ics_reproduce_reference_fixture():
+    """torch.manual_seed(42); torch.rand reproduces the fixture ICs (sampler.py:56-65)."""
+    for case, name in ((PENDULUM, "labels_pendulum_case1.npz"), (DUFFING, "labels_duffing_main.npz")):
+        g = np.load(GOLDEN / name)
+        y0 = seeded_ics(case, 4000, seed=42)
+        np.testing.assert_allclose(y0.numpy(), g["ics"], atol=1e-6)
+
+
+def test_oracle_pendulum_labels_match_reference_exactly():
+    """Pendulum case 1 (tests/integration/pendulum/test_pendulum.py:21-47): FP 602 / LC 3398."""
+    g = np.load(GOLDEN / "labels_pendulum_case1.npz")
+    y0 = seeded_ics(PENDULUM, 4000, seed=42).double().numpy()
+    feats, tfeats, _ = oracle_case_features(PENDULUM, y0)
+    pred = knn_labels(tfeats, feats)
+    assert (pred == g["labels"]).all()
+    np.testing.assert_array_equal(np.bincount(pred, minlength=2), g["counts"])
+
+
+def test_oracle_duffing_labels_match_reference():
+    """Duffing (tests/integration/duffing/test_duffing.py): MCC >= 0.95 and per-class counts
+    within 2 of the reference's FP32 JAX labels (the oracle is FP64)."""
+    from sklearn.metrics import matthews_corrcoef
+
+    g = np.load(GOLDEN / "labels_duffing_main.npz")
+    y0 = seeded_ics(DUFFING, 4000, seed=42).double().numpy()
+    feats, tfeats, _ = oracle_case_features(DUFFING, y0)
+    pred = knn_labels(tfeats, feats)
+    assert matthews_corrcoef(g["labels"], pred) >= 0.99
+    assert (pred != g["labels"]).sum() <= 8
+    assert np.abs(np.bincount(pred, minlength=5) - g["counts"]).max() <= 2
+
+
+def test_oracle_pendulum_n50_prefix():
+    """N=50 at seed 42 on the CPU generator: the first 50 fixture labels (9 FP / 41 LC).
+
+    The reference's test_n50 (tests/integration/pendulum/test_pendulum.py:109-124)
+    quotes FP 0.12 +- 0.05 from a run whose sampler drew on its setup device; the
+    CPU generator's first 50 ICs are the fixture's first 50 rows, which hold 9 FP."""
+    g = np.load(GOLDEN / "labels_pendulum_case1.npz")
+    y0 = seeded_ics(PENDULUM, 50, seed=42).double().numpy()
+    feats, tfeats, _ = oracle_case_features(PENDULUM, y0)
+    pred = knn_labels(tfeats, feats)
+    assert (pred == g["labels"][:50]).all()
+    assert np.bincount(pred, minlength=2).tolist() == [9, 41]
+
+
+def test_oracle_exponential_decay_known_answers():
+    """e^-1 and e^-2 at t=1 (tests/unit/solvers/test_solver.py:138,163,215-216)."""
+    save = np.linspace(0.0, 1.0, 11)
+    r = O.solve_batch(O.SYS_LINEAR, np.array([[1.0], [1.0]]), np.array([[-1.0], [-2.0]]), save, (0, 1), 1e-8, 1e-6,
+                      param_index=np.array([0, 1]), keep_full=True)
+    np.testing.assert_allclose(r["y"][-1, :, 0], [np.exp(-1), np.exp(-2)], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(r["y"][:, 0, 0], np.exp(-save), rtol=0, atol=1e-6)
+
+
+def test_oracle_matches_reference_scipy_trajectories():
+    """Short non-chaotic horizon vs the reference's ScipyParallelSolver (RK45, rtol 1e-11)."""
+    g = np.load(GOLDEN / "scipy_reference.npz")
+    for key, sys_id, p in (("pendulum", O.SYS_PENDULUM, [0.1, 0.5, 1.0]), ("duffing", O.SYS_DUFFING, [0.08, 1.0, 0.2])):
+        y0 = g[f"{key}_y0"].astype(np.float64)
+        t = g[f"{key}_t"]
+        r = O.solve_batch(sys_id, y0, np.array([p]), t, (0.0, float(t[-1])), 1e-11, 1e-12, keep_full=True)
+        np.testing.assert_allclose(r["y"], g[f"{key}_y"], rtol=2e-7, atol=2e-7)
+
+
+@pytest.mark.parametrize(
+    "name,kind,param",
+    [
+        ("median", 0, 0.0),
+        ("mean", 1, 0.0),
+        ("standard_deviation", 2, 0.0),
+        ("variance", 3, 0.0),
+        ("root_mean_square", 4, 0.0),
+        ("maximum", 5, 0.0),
+        ("absolute_maximum", 6, 0.0),
+        ("minimum", 7, 0.0),
+        ("delta", 8, 0.0),
+        ("log_delta", 9, 0.0),
+        ("amplitude", 10, 0.0),
+        ("number_crossing_m_0", 11, 0.0),
+        ("number_crossing_m_1", 11, 1.0),
+    ],
+)
+def test_oracle_window_features_match_reference_calculators(name, kind, param):
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g["x"]
+    want = g[name]
+    got = np.array([[O.window_feature(kind, param, x[:, b, s]) for s in range(x.shape[2])] for b in range(x.shape[1])])
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+
+
+def test_oracle_median_even_length_is_lower_median():
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g["x_even"]
+    got = np.array([[O.window_feature(0, 0.0, x[:, b, s]) for s in range(2)] for b in range(x.shape[1])])
+    np.testing.assert_array_equal(got, g["median_even"])
+
+
+def test_oracle_status_codes():
+    save = np.linspace(0.0, 10.0, 5)
+    # max_steps
+    r = O.solve_batch(O.SYS_PENDULUM, np.array([[0.1, 0.0]]), np.array([[0.1, 0.5, 1.0]]), save, (0, 10), 1e-8, 1e-6,
+                      max_steps=10)
+    assert r["status"][0] == O.STATUS_MAX_STEPS
+    # non-finite initial condition
+    r = O.solve_batch(O.SYS_PENDULUM, np.array([[np.nan, 0.0]]), np.array([[0.1, 0.5, 1.0]]), save, (0, 10), 1e-8, 1e-6)
+    assert r["status"][0] == O.STATUS_NONFINITE
+    # unbounded event on exponential growth
+    r = O.solve_batch(O.SYS_LINEAR, np.array([[1.0]]), np.array([[5.0]]), save, (0, 10), 1e-8, 1e-6, unbounded_thr=1e6,
+                      keep_full=True)
+    assert r["status"][0] == O.STATUS_UNBOUNDED
+    assert np.isinf(r["y"][-1, 0, 0])
+
+
+def test_oracle_cross_layout_equals_explicit_expansion():
+    """IC-major expansion (src/pybasin/solvers/base.py:155-159)."""
+    y0 = np.array([[0.5, 0.0], [2.0, 1.0]])
+    P = np.array([[0.1, 0.3, 1.0], [0.1, 0.7, 1.0], [0.2, 0.5, 1.0]])
+    save = np.linspace(0.0, 5.0, 6)
+    idx = np.tile(np.arange(3), 2)
+    r = O.solve_batch(O.SYS_PENDULUM, np.repeat(y0, 3, axis=0), P, save, (0, 5), 1e-9, 1e-9, param_index=idx,
+                      keep_full=True)
+    for ic in range(2):
+        for p in range(3):
+            one = O.solve_batch(O.SYS_PENDULUM, y0[ic : ic + 1], P[p : p + 1], save, (0, 5), 1e-9, 1e-9, keep_full=True)
+            np.testing.assert_array_equal(r["y"][:, ic * 3 + p], one["y"][:, 0])
+
+
+def test_torch_linspace_save_times_are_float32_rounded():
+    """The reference's save grid is linspace in y0's dtype (base.py:113-127)."""
+    s32 = torch.linspace(900, 1000, 5000, dtype=torch.float32).double()
+    s64 = torch.linspace(900, 1000, 5000, dtype=torch.float64)
+    assert (s32 - s64).abs().max() > 1e-6

@@ -1,0 +1,324 @@
+"""Parity of the CUDA kernels (through the C ABI) with the FP64 oracle and the golden fixtures.
+
+Tolerances:
+* FP64 kernel vs FP64 oracle, short horizon (non-chaotic): rtol 1e-9 on trajectories.
+* FP64 kernel vs oracle, full horizon: window features rtol 1e-6 / atol 1e-8 on
+  trajectories away from basin boundaries; labels identical on the fixtures.
+* Mixed kernel (FP32 stages, rtol 1e-6) vs FP64 oracle: |dBS| <= 0.005 and features
+  within 2e-3 relative on the attractors.
+"""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from pybasin_b200 import _lib as L
+from pybasin_b200.engine import FeatureColumn, SolveRequest, label_nearest, solve
+from tests.helpers import DUFFING, PENDULUM, Case, impute, knn_labels, oracle_case_features, seeded_ics
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+DEV = torch.device("cuda:0")
+
+SYS_OF = {
+    O.SYS_LINEAR: L.SYS_LINEAR,
+    O.SYS_PENDULUM: L.SYS_PENDULUM,
+    O.SYS_DUFFING: L.SYS_DUFFING,
+    O.SYS_LORENZ: L.SYS_LORENZ,
+    O.SYS_LORENZ_MASKED: L.SYS_LORENZ_MASKED,
+}
+
+
+def gpu_solve(
+    oracle_sys: int,
+    y0: np.ndarray,
+    params: np.ndarray,
+    save: np.ndarray,
+    t_span: tuple[float, float],
+    rtol: float,
+    atol: float,
+    *,
+    precision: int = L.PREC_FP64,
+    schedule: int = L.SCHED_QUEUE,
+    win_begin: int = 0,
+    features: list[tuple[int, int, float]] | None = None,
+    param_index: np.ndarray | None = None,
+    layout: int | None = None,
+    keep_full: bool = False,
+    max_steps: int = 16**5,
+    unbounded_thr: float = 0.0,
+    y0_dtype=torch.float64,
+    block_size: int = 0,
+    grid_blocks: int = 0,
+):
+    y0_t = torch.as_tensor(np.ascontiguousarray(y0), dtype=y0_dtype, device=DEV)
+    p_t = torch.as_tensor(np.ascontiguousarray(np.atleast_2d(params)), dtype=torch.float64, device=DEV)
+    if layout is None:
+        layout = L.LAYOUT_INDEXED if param_index is not None else L.LAYOUT_SINGLE
+    req = SolveRequest(
+        system=SYS_OF[oracle_sys],
+        dim=y0.shape[1],
+        y0=y0_t,
+        params=p_t,
+        save_ts=torch.as_tensor(save, dtype=torch.float64, device=DEV),
+        t_span=t_span,
+        rtol=rtol,
+        atol=atol,
+        layout=layout,
+        param_index=None if param_index is None else torch.as_tensor(param_index, dtype=torch.int32, device=DEV),
+        win_begin=win_begin,
+        columns=[FeatureColumn(s, k, p) for (s, k, p) in (features or [])],
+        precision=precision,
+        schedule=schedule,
+        max_steps=max_steps,
+        unbounded_thr=unbounded_thr,
+        keep_final=True,
+        keep_full=keep_full,
+        out_dtype=torch.float64,
+        keep_steps=True,
+        block_size=block_size,
+        grid_blocks=grid_blocks,
+    )
+    r = solve(req)
+    torch.cuda.synchronize()
+    out = {
+        "status": r.status.cpu().numpy(),
+        "y_final": r.y_final.cpu().numpy(),
+        "steps": r.steps.cpu().numpy(),
+    }
+    if r.features is not None:
+        out["features"] = r.features.cpu().numpy()
+    if r.y_full is not None:
+        out["y"] = r.y_full.cpu().numpy()
+    return out
+
+
+def case_gpu_features(case: Case, y0: np.ndarray, precision: int, rtol: float | None = None, schedule=L.SCHED_QUEUE):
+    save = case.save_ts().numpy()
+    feats = [(f[0], f[1], f[2]) for f in case.features]
+    kw = dict(precision=precision, schedule=schedule, win_begin=case.win_begin(), features=feats)
+    t_span = (case.t_span[0], float(save[-1]))
+    r = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, rtol or case.rtol, case.atol, **kw)
+    rt = gpu_solve(case.oracle_sys, np.array(case.templates), np.array([case.params]), save, t_span,
+                   rtol or case.rtol, case.atol, **kw)
+    return r["features"], rt["features"], r
+
+
+# ---------------------------------------------------------------------------
+# trajectories (short, non-chaotic horizon)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("schedule", [L.SCHED_PLAIN, L.SCHED_QUEUE])
+@pytest.mark.parametrize("case", [PENDULUM, DUFFING], ids=lambda c: c.name)
+def test_fp64_trajectories_match_oracle(case, schedule):
+    y0 = seeded_ics(case, 257, seed=3).double().numpy()
+    save = np.linspace(0.0, 30.0, 61)
+    want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), 1e-10, 1e-10, keep_full=True)
+    got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), 1e-10, 1e-10,
+                    schedule=schedule, keep_full=True)
+    assert (got["status"] == 0).all()
+    np.testing.assert_allclose(got["y"], want["y"], rtol=1e-8, atol=1e-9)
+    # same algorithm, same control: step counts agree up to a handful of rounding-level decisions
+    assert np.abs(got["steps"] - want["steps"]).max() <= 3
+
+
+def test_mixed_trajectories_track_fp64():
+    y0 = seeded_ics(DUFFING, 512, seed=5).double().numpy()
+    save = np.linspace(0.0, 30.0, 61)
+    want = O.solve_batch(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 30.0), 1e-10, 1e-10, keep_full=True)
+    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 30.0), 1e-6, 1e-6,
+                    precision=L.PREC_MIXED, keep_full=True)
+    np.testing.assert_allclose(got["y"], want["y"], rtol=0, atol=2e-4)
+
+
+def test_cross_layout_matches_oracle_expansion():
+    y0 = np.array([[0.5, 0.0], [2.0, 1.0], [-1.0, 3.0]])
+    P = np.array([[0.1, 0.3, 1.0], [0.1, 0.7, 1.0]])
+    save = np.linspace(0.0, 10.0, 21)
+    got = gpu_solve(O.SYS_PENDULUM, y0, P, save, (0.0, 10.0), 1e-10, 1e-10, layout=L.LAYOUT_CROSS, keep_full=True)
+    idx = np.tile(np.arange(2), 3)
+    want = O.solve_batch(O.SYS_PENDULUM, np.repeat(y0, 2, axis=0), P, save, (0.0, 10.0), 1e-10, 1e-10,
+                         param_index=idx, keep_full=True)
+    np.testing.assert_allclose(got["y"], want["y"], rtol=1e-9, atol=1e-10)
+
+
+# ---------------------------------------------------------------------------
+# fused features over the full horizon
+# ---------------------------------------------------------------------------
+ALL_FEATS = [(s, k, 0.0) for s in range(2) for k in range(0, 11)] + [(0, 11, 0.0), (1, 11, 0.5), (1, 12, 0.0)]
+
+
+@pytest.mark.parametrize("case", [PENDULUM, DUFFING], ids=lambda c: c.name)
+def test_all_fused_features_match_oracle(case):
+    y0 = seeded_ics(case, 300, seed=11).double().numpy()
+    save = case.save_ts().numpy()
+    t_span = (0.0, float(save[-1]))
+    wb = case.win_begin()
+    want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, t_span, 1e-8, 1e-6, win_begin=wb,
+                         features=ALL_FEATS)
+    got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, 1e-8, 1e-6, win_begin=wb,
+                    features=ALL_FEATS)
+    ok = (got["status"] == 0) & (want["status"] == 0)
+    assert ok.all()
+    # compare on trajectories whose final states agree (away from basin boundaries)
+    same = np.abs(got["y_final"] - want["y_final"]).max(axis=1) < 1e-5 * (1 + np.abs(want["y_final"]).max(axis=1))
+    assert same.mean() > 0.95
+    np.testing.assert_allclose(got["features"][same], want["features"][same], rtol=1e-6, atol=1e-7)
+
+
+def test_median_and_crossings_exact_on_identical_windows():
+    """Median and crossing counts are order statistics: on short horizons where the
+    kernel and oracle windows agree to ~1e-12 they must be equal."""
+    y0 = seeded_ics(PENDULUM, 64, seed=2).double().numpy()
+    save = np.linspace(0.0, 20.0, 401)
+    feats = [(0, 0, 0.0), (1, 0, 0.0), (0, 11, 0.0), (1, 11, 0.25), (1, 11, -0.25)]
+    want = O.solve_batch(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0.0, 20.0), 1e-10, 1e-10,
+                         win_begin=100, features=feats)
+    got = gpu_solve(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0.0, 20.0), 1e-10, 1e-10,
+                    win_begin=100, features=feats)
+    np.testing.assert_allclose(got["features"][:, :2], want["features"][:, :2], rtol=1e-6, atol=1e-7)
+    np.testing.assert_array_equal(got["features"][:, 2:], want["features"][:, 2:])
+
+
+# ---------------------------------------------------------------------------
+# golden label fixtures of the reference
+# ---------------------------------------------------------------------------
+def test_fp64_pendulum_labels_equal_reference_fixture():
+    g = np.load(GOLDEN / "labels_pendulum_case1.npz")
+    y0 = seeded_ics(PENDULUM, 4000, seed=42).double().numpy()
+    f, tf, r = case_gpu_features(PENDULUM, y0, L.PREC_FP64)
+    assert (r["status"] == 0).all()
+    pred = knn_labels(tf, f)
+    assert (pred == g["labels"]).all()
+    np.testing.assert_array_equal(np.bincount(pred, minlength=2), g["counts"])
+
+
+def test_fp64_duffing_labels_match_reference_fixture():
+    from sklearn.metrics import matthews_corrcoef
+
+    g = np.load(GOLDEN / "labels_duffing_main.npz")
+    y0 = seeded_ics(DUFFING, 4000, seed=42).double().numpy()
+    f, tf, _ = case_gpu_features(DUFFING, y0, L.PREC_FP64)
+    pred = knn_labels(tf, f)
+    assert matthews_corrcoef(g["labels"], pred) >= 0.99
+    assert np.abs(np.bincount(pred, minlength=5) - g["counts"]).max() <= 2
+
+
+@pytest.mark.parametrize("case", [PENDULUM, DUFFING], ids=lambda c: c.name)
+def test_mixed_labels_within_delta_bs_of_fp64_oracle(case):
+    y0 = seeded_ics(case, 4000, seed=42).double().numpy()
+    fo, tfo, _ = oracle_case_features(case, y0)
+    want = knn_labels(tfo, fo)
+    f, tf, r = case_gpu_features(case, y0, L.PREC_MIXED, rtol=1e-6)
+    assert (r["status"] == 0).all()
+    got = knn_labels(tf, f)
+    k = len(case.templates)
+    dbs = np.abs(np.bincount(got, minlength=k) - np.bincount(want, minlength=k)) / len(y0)
+    assert dbs.max() <= 0.005
+    assert (got == want).mean() >= 0.99
+
+
+# ---------------------------------------------------------------------------
+# device 1-NN labelling
+# ---------------------------------------------------------------------------
+def test_label_nearest_matches_sklearn():
+    rng = np.random.default_rng(0)
+    feats = rng.normal(size=(5000, 3))
+    feats[7, 1] = np.inf
+    feats[9, 0] = np.nan
+    tpl = rng.normal(size=(6, 3))
+    tpl_cls = np.array([0, 1, 2, 0, 3, 1], dtype=np.int32)
+    status = np.zeros(5000, dtype=np.int32)
+    status[11] = L.TRAJ_UNBOUNDED
+    groups = (np.arange(5000) % 3).astype(np.int32)
+    lab, cnt = label_nearest(
+        torch.as_tensor(feats, device=DEV),
+        torch.as_tensor(tpl, device=DEV),
+        torch.as_tensor(tpl_cls, device=DEV),
+        4,
+        status=torch.as_tensor(status, device=DEV),
+        group_of=torch.as_tensor(groups, device=DEV),
+        n_groups=3,
+    )
+    lab = lab.cpu().numpy()
+    from sklearn.neighbors import KNeighborsClassifier
+
+    knn = KNeighborsClassifier(n_neighbors=1).fit(impute(tpl), tpl_cls)
+    want = knn.predict(impute(feats))
+    want[11] = 4
+    assert (lab == want).all()
+    cnt = cnt.cpu().numpy()
+    for g in range(3):
+        np.testing.assert_array_equal(cnt[g], np.bincount(want[groups == g], minlength=5))
+
+
+# ---------------------------------------------------------------------------
+# edge cases: ragged sizes, statuses, failure paths
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [1, 31, 33, 4097])
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+def test_ragged_batch_sizes_queue(n, precision):
+    y0 = seeded_ics(PENDULUM, n, seed=9).double().numpy()
+    save = np.linspace(0.0, 20.0, 41)
+    feats = [(1, 1, 0.0), (0, 5, 0.0)]
+    want = O.solve_batch(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0, 20), 1e-8, 1e-8, win_begin=20,
+                         features=feats)
+    got = gpu_solve(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0, 20), 1e-8, 1e-8, win_begin=20,
+                    features=feats, precision=precision, grid_blocks=3, block_size=64)
+    tol = 1e-7 if precision == L.PREC_FP64 else 2e-4
+    np.testing.assert_allclose(got["features"], want["features"], rtol=tol, atol=tol)
+
+
+def test_status_codes_and_fill():
+    save = np.linspace(0.0, 10.0, 11)
+    # NaN IC -> non-finite; max_steps=10 -> max_steps
+    y0 = np.array([[np.nan, 0.0], [0.1, 0.0]])
+    r = gpu_solve(O.SYS_PENDULUM, y0[:1], np.array([PENDULUM.params]), save, (0, 10), 1e-8, 1e-6)
+    assert r["status"][0] == L.TRAJ_NONFINITE
+    r = gpu_solve(O.SYS_PENDULUM, y0[1:], np.array([PENDULUM.params]), save, (0, 10), 1e-8, 1e-6, max_steps=10)
+    assert r["status"][0] == L.TRAJ_MAX_STEPS and r["steps"][0] == 10
+    # unbounded event: exponential growth stops, remaining saves are +inf
+    r = gpu_solve(O.SYS_LINEAR, np.array([[1.0]]), np.array([[5.0]]), save, (0, 10), 1e-8, 1e-6,
+                  unbounded_thr=1e6, keep_full=True, features=[(0, 1, 0.0)])
+    want = O.solve_batch(O.SYS_LINEAR, np.array([[1.0]]), np.array([[5.0]]), save, (0, 10), 1e-8, 1e-6,
+                         unbounded_thr=1e6, keep_full=True)
+    assert r["status"][0] == L.TRAJ_UNBOUNDED
+    assert np.isinf(r["y"][-1, 0, 0])
+    np.testing.assert_array_equal(np.isinf(r["y"]), np.isinf(want["y"]))
+    assert np.isinf(r["features"][0, 0])
+
+
+def test_huge_initial_condition_does_not_hang():
+    save = np.linspace(0.0, 10.0, 11)
+    r = gpu_solve(O.SYS_DUFFING, np.array([[1e30, 0.0]]), np.array([DUFFING.params]), save, (0, 10), 1e-8, 1e-6,
+                  max_steps=1000)
+    assert r["status"][0] in (L.TRAJ_NONFINITE, L.TRAJ_MAX_STEPS, L.TRAJ_DT_UNDERFLOW)
+
+
+@pytest.mark.parametrize("oracle_sys", [O.SYS_LORENZ, O.SYS_LORENZ_MASKED])
+def test_lorenz_variants_match_oracle(oracle_sys):
+    rng = np.random.default_rng(1)
+    y0 = rng.uniform(-20, 20, size=(128, 3))
+    save = np.linspace(0.0, 5.0, 51)
+    p = np.array([[10.0, 28.0, 8.0 / 3.0]])
+    want = O.solve_batch(oracle_sys, y0, p, save, (0, 5), 1e-10, 1e-10, keep_full=True)
+    got = gpu_solve(oracle_sys, y0, p, save, (0, 5), 1e-10, 1e-10, keep_full=True)
+    np.testing.assert_allclose(got["y"], want["y"], rtol=1e-6, atol=1e-6)
+
+
+def test_broken_butterfly_unbounded_labels_match_oracle():
+    """Broken-butterfly Lorenz (case_studies/lorenz/setup_lorenz_system.py:28-60): stop at |y|>=200."""
+    rng = np.random.default_rng(4)
+    y0 = np.stack([rng.uniform(-10, 10, 512), rng.uniform(-20, 20, 512), np.zeros(512)], axis=1)
+    save = np.linspace(900.0, 1000.0, 101)
+    p = np.array([[0.12, 0.0, -0.6]])
+    want = O.solve_batch(O.SYS_LORENZ, y0, p, save, (0, 1000), 1e-8, 1e-6, unbounded_thr=200.0)
+    got = gpu_solve(O.SYS_LORENZ, y0, p, save, (0, 1000), 1e-8, 1e-6, unbounded_thr=200.0)
+    unb_w = want["status"] == L.TRAJ_UNBOUNDED
+    unb_g = got["status"] == L.TRAJ_UNBOUNDED
+    assert 0 < unb_w.sum() < len(y0)
+    assert (unb_w == unb_g).mean() >= 0.99
