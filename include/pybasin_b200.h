@@ -79,7 +79,8 @@ typedef enum {
     PB_TRAJ_MAX_STEPS = 1,    /* max_steps attempted steps before t1 */
     PB_TRAJ_DT_UNDERFLOW = 2, /* t + dt == t */
     PB_TRAJ_UNBOUNDED = 3,    /* max|y| >= unbounded_threshold after an accepted step */
-    PB_TRAJ_NONFINITE = 4     /* non-finite error norm */
+    PB_TRAJ_NONFINITE = 4,    /* non-finite error norm */
+    PB_TRAJ_BAD_INPUT = 5     /* param_index row outside [0, n_param_rows) */
 } pb_traj_status;
 
 #define PB_MAX_FEATURES 32

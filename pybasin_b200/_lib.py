@@ -62,6 +62,7 @@ TRAJ_MAX_STEPS = 1
 TRAJ_DT_UNDERFLOW = 2
 TRAJ_UNBOUNDED = 3
 TRAJ_NONFINITE = 4
+TRAJ_BAD_INPUT = 5
 
 MAX_FEATURES = 32
 MAX_CROSSING = 4

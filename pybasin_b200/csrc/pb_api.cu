@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) k_label_nearest(const double* __restrict_
     }
     labels[i] = cls;
     const int g = group_of ? group_of[i] : 0;
-    if (g >= 0 && g < n_groups) atomicAdd(counts + static_cast<int64_t>(g) * (n_classes + 1) + cls, 1ull);
+    if (g >= 0 && g < n_groups && cls >= 0 && cls <= n_classes) atomicAdd(counts + static_cast<int64_t>(g) * (n_classes + 1) + cls, 1ull);
 }
 
 // ---------------------------------------------------------------------------

@@ -168,6 +168,8 @@ struct Integrator {
         } else if (a.layout == PB_LAYOUT_INDEXED) {
             prow = __ldg(a.param_index + traj);
         }
+        const bool bad_row = prow < 0 || prow >= a.n_param_rows;
+        if (bad_row) prow = 0;
         double y0d[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -179,9 +181,9 @@ struct Integrator {
 #pragma unroll
         for (int q = 0; q < Sys::NP; ++q)
             L.p[q] = q < a.n_params ? static_cast<R>(__ldg(a.params + prow * a.n_params + q)) : R(0);
-        L.t = a.t0;
+        L.t = bad_row ? a.t1 : a.t0;  // a bad row finishes without stepping
         L.steps = 0;
-        L.status = PB_TRAJ_OK;
+        L.status = bad_row ? PB_TRAJ_BAD_INPUT : PB_TRAJ_OK;
         L.si = a.y_full_out ? 0 : a.win_begin;
         L.next_save = load_save(a, L.si);
         L.nsamp = 0;
