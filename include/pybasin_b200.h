@@ -144,6 +144,11 @@ typedef struct pb_solve_args {
                                           (the call resets it on `stream`) */
     float* median_scratch;   /* (n_traj, n_median_states, n_save - win_begin) when any
                                 PB_FEAT_MEDIAN column is requested, else NULL */
+    /* processing order (device, optional): queue position q integrates trajectory
+       order[q], a permutation of [0, n_traj).  Ordering ICs along a space-filling
+       curve puts trajectories with similar dynamics (and step counts) in the same
+       warp.  Outputs stay indexed by trajectory. */
+    const int32_t* order;
 } pb_solve_args;
 
 /* Integrate n_traj trajectories with adaptive Dormand-Prince 5(4) and write the

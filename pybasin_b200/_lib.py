@@ -119,6 +119,7 @@ class SolveArgs(ctypes.Structure):
         ("steps_out", _c_vp),
         ("queue_counter", _c_vp),
         ("median_scratch", _c_vp),
+        ("order", _c_vp),
     ]
 
 

@@ -152,18 +152,27 @@ __global__ void __launch_bounds__(256) k_probe_fma(int iters, float* __restrict_
 // ---------------------------------------------------------------------------
 using kernel_fn = void (*)(const pb_solve_args);
 
+struct KernelSel {
+    kernel_fn fn = nullptr;
+    int smem_per_thread = 0;  // dynamic shared memory: per-thread statistics slot
+};
+
 template <class Sys>
-kernel_fn select_kernel(int precision, int schedule)
+KernelSel select_kernel(int precision, int schedule)
 {
+    KernelSel k;
+    k.smem_per_thread = Stats<Sys::S>::kBytesPerThread;
     if (precision == PB_PREC_FP64)
-        return schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, double, false> : k_solve_plain<Sys, double, false>;
-    return schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, float, true> : k_solve_plain<Sys, float, true>;
+        k.fn = schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, double> : k_solve_plain<Sys, double>;
+    else
+        k.fn = schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, float> : k_solve_plain<Sys, float>;
+    return k;
 }
 
-static kernel_fn find_kernel(int system, int dim, int precision, int schedule)
+static KernelSel find_kernel(int system, int dim, int precision, int schedule)
 {
-    if (precision != PB_PREC_FP64 && precision != PB_PREC_MIXED) return nullptr;
-    if (schedule != PB_SCHED_PLAIN && schedule != PB_SCHED_QUEUE) return nullptr;
+    if (precision != PB_PREC_FP64 && precision != PB_PREC_MIXED) return {};
+    if (schedule != PB_SCHED_PLAIN && schedule != PB_SCHED_QUEUE) return {};
     switch (system) {
         case PB_SYS_LINEAR:
             switch (dim) {
@@ -171,15 +180,23 @@ static kernel_fn find_kernel(int system, int dim, int precision, int schedule)
                 case 2: return select_kernel<SysLinear<2>>(precision, schedule);
                 case 3: return select_kernel<SysLinear<3>>(precision, schedule);
                 case 4: return select_kernel<SysLinear<4>>(precision, schedule);
-                default: return nullptr;
+                default: return {};
             }
-        case PB_SYS_PENDULUM: return dim == 2 ? select_kernel<SysPendulum>(precision, schedule) : nullptr;
-        case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision, schedule) : nullptr;
-        case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision, schedule) : nullptr;
+        case PB_SYS_PENDULUM: return dim == 2 ? select_kernel<SysPendulum>(precision, schedule) : KernelSel{};
+        case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision, schedule) : KernelSel{};
+        case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision, schedule) : KernelSel{};
         case PB_SYS_LORENZ_MASKED:
-            return dim == 3 ? select_kernel<SysLorenz<true>>(precision, schedule) : nullptr;
-        default: return nullptr;
+            return dim == 3 ? select_kernel<SysLorenz<true>>(precision, schedule) : KernelSel{};
+        default: return {};
     }
+}
+
+// Dynamic shared memory above the 48 KB default needs an opt-in per kernel.
+static cudaError_t prepare_smem(const KernelSel& k, int block)
+{
+    const int bytes = k.smem_per_thread * block;
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
@@ -276,13 +293,15 @@ int64_t pb_solve_scratch_bytes(const pb_solve_args* a)
 int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule, int32_t block_size,
                        int32_t* blocks_per_sm, int32_t* num_sms)
 {
-    kernel_fn k = find_kernel(system, dim, precision, schedule);
-    if (!k) return PB_EINVALID_ODE;
+    KernelSel k = find_kernel(system, dim, precision, schedule);
+    if (!k.fn) return PB_EINVALID_ODE;
     if (block_size <= 0 || block_size % 32 || block_size > 256) return PB_EINVAL;
     int dev = 0, bps = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, block_size, 0);
+    if (e == cudaSuccess) e = prepare_smem(k, block_size);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, block_size, k.smem_per_thread * block_size);
     if (e != cudaSuccess) return map_cuda(e);
     if (blocks_per_sm) *blocks_per_sm = bps;
     if (num_sms) *num_sms = sms;
@@ -294,33 +313,36 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
     int v = validate(args);
     if (v != PB_SUCCESS) return v;
     const pb_solve_args& a = *args;
-    kernel_fn k = find_kernel(a.system, a.dim, a.precision, a.schedule);
-    if (!k) return PB_EINVALID_ODE;
+    KernelSel k = find_kernel(a.system, a.dim, a.precision, a.schedule);
+    if (!k.fn) return PB_EINVALID_ODE;
     if (a.n_traj == 0) return PB_SUCCESS;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int block = a.block_size > 0 ? a.block_size : 128;
+    const int smem = k.smem_per_thread * block;
+    cudaError_t e = prepare_smem(k, block);
+    if (e != cudaSuccess) return map_cuda(e);
     int64_t grid;
     if (a.schedule == PB_SCHED_QUEUE) {
         if (a.grid_blocks > 0) {
             grid = a.grid_blocks;
         } else {
             int dev = 0, sms = 0, bps = 0;
-            cudaError_t e = cudaGetDevice(&dev);
+            e = cudaGetDevice(&dev);
             if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, block, 0);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, block, smem);
             if (e != cudaSuccess) return map_cuda(e);
             grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
         }
         const int64_t need = (a.n_traj + block - 1) / block;
         if (grid > need) grid = need;
-        cudaError_t e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return map_cuda(e);
     } else {
         grid = (a.n_traj + block - 1) / block;
     }
     if (grid > 0x7fffffffLL) return PB_EINVAL;
-    k<<<static_cast<unsigned>(grid), block, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    k.fn<<<static_cast<unsigned>(grid), block, smem, st>>>(a);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return map_cuda(e);
     MedianPlan plan;
     if (count_median_cols(a, &plan) > 0) {

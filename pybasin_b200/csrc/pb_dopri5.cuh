@@ -1,10 +1,13 @@
 // Per-lane adaptive Dormand-Prince 5(4) integrator with dense output fused
 // into streaming window statistics.
 //
-// One CUDA thread owns one trajectory at a time; its state, stages and
-// statistics live in registers.  The algorithm (tableau, Shampine error
-// estimate, torchdiffeq-style control and 4th-order dense output) is the one
-// of the reference's native solver, src/zigode/src/solver/dopri5_generic.zig:
+// One CUDA thread owns one trajectory at a time; its state and stages live in
+// registers, its window statistics in a per-thread slot of shared memory (they
+// are touched only at save points, so keeping them out of the register file
+// lets every trajectory of a 100k-IC batch be resident at once).  The algorithm
+// (tableau, Shampine error estimate, torchdiffeq-style control, 4th-order dense
+// output) is the reference's native solver,
+// src/zigode/src/solver/dopri5_generic.zig:
 //   step and stages      :130-183
 //   RMS error norm       :185-192
 //   dense output         :194-221
@@ -13,13 +16,20 @@
 //   initial step size    :270-321 (Hairer, Norsett & Wanner II.4)
 //   tail fill            :238-241
 // Statistics follow src/pybasin/ts_torch/calculators/torch_features_statistical.py
-// (:30-110, :307-318) and torch_features_pattern.py:56-60, evaluated as
-// streaming (shifted-sum) reductions over the save points of the window
-// instead of over a stored (T, B, S) tensor.
+// (:30-110, :307-318) and torch_features_pattern.py:56-60, as streaming
+// shifted-sum reductions over the save points of the window.
+//
+// Precision: Integrator<Sys, double> is the plain FP64 kernel (every operation
+// in FP64, control identical to the reference).  Integrator<Sys, float> runs
+// stages, state and dense output in FP32 (state increments Kahan-compensated),
+// keeps time, step size and the error-norm accumulation in FP64, and evaluates
+// the step-size factor in FP32.
 #pragma once
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "pb_rhs.cuh"
 #include "pybasin_b200.h"
@@ -64,25 +74,81 @@ __device__ __forceinline__ T pick(const T (&arr)[N], int idx)
     return v;
 }
 
+// Block-wide plan derived once from the arguments (shared memory).
+struct Plan {
+    int n_cross;
+    int n_med;
+    int cross_state[PB_MAX_CROSSING];
+    double cross_level[PB_MAX_CROSSING];
+    int med_state[PB_MAX_FEATURES];
+};
+
+__device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
+{
+    int nc = 0, nm = 0;
+    for (int c = 0; c < a.n_features; ++c) {
+        if (a.feat_kind[c] == PB_FEAT_CROSSINGS && nc < PB_MAX_CROSSING) {
+            pl.cross_state[nc] = a.feat_state[c];
+            pl.cross_level[nc] = a.feat_param[c];
+            ++nc;
+        } else if (a.feat_kind[c] == PB_FEAT_MEDIAN) {
+            pl.med_state[nm++] = a.feat_state[c];
+        }
+    }
+    pl.n_cross = nc;
+    pl.n_med = nm;
+}
+
+// Per-thread window statistics in shared memory, structure-of-arrays
+// (consecutive threads hit consecutive words).  Layout of the dynamic segment:
+//   double [6*S][nthr]: shift, s1, s2, min, max, last (per state)
+//   int    [PB_MAX_CROSSING + 2][nthr]: crossing counts, nsamp, flags
+// flags: bits 0..7 = NaN seen per state, bits 8..11 = previous sample above level.
+template <int S>
+struct Stats {
+    double* d;
+    int* i;
+    int nthr, tid;
+    static constexpr int kBytesPerThread = 6 * S * 8 + (PB_MAX_CROSSING + 2) * 4;
+    __device__ __forceinline__ double& shift(int s) { return d[(0 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ double& s1(int s) { return d[(1 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ double& s2(int s) { return d[(2 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ double& mn(int s) { return d[(3 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ double& mx(int s) { return d[(4 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ double& last(int s) { return d[(5 * S + s) * nthr + tid]; }
+    __device__ __forceinline__ int& cross(int j) { return i[j * nthr + tid]; }
+    __device__ __forceinline__ int& nsamp() { return i[PB_MAX_CROSSING * nthr + tid]; }
+    __device__ __forceinline__ int& flags() { return i[(PB_MAX_CROSSING + 1) * nthr + tid]; }
+    __device__ __forceinline__ void reset()
+    {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            shift(s) = 0.0;
+            s1(s) = 0.0;
+            s2(s) = 0.0;
+            mn(s) = CUDART_INF;
+            mx(s) = -CUDART_INF;
+            last(s) = 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < PB_MAX_CROSSING; ++j) cross(j) = 0;
+        nsamp() = 0;
+        flags() = 0;
+    }
+};
+
 template <class Sys, class R>
 struct Lane {
     static constexpr int S = Sys::S;
     R y[S];
-    R yc[S];  // Kahan compensation of y (mixed precision only)
+    R yc[S];  // Kahan compensation of y (FP32 kernel only)
     R k1[S];
     R p[Sys::NP];
     double t, dt;
-    int64_t steps;
-    int si;            // next save index
     double next_save;  // save_ts[si] (or +inf past the end)
+    int si;            // next save index
+    int steps;
     int status;
-    // window statistics
-    int nsamp;
-    unsigned nan_mask;
-    double shift[S], s1[S], s2[S];
-    R mn[S], mx[S], last[S];
-    int cross_cnt[PB_MAX_CROSSING];
-    unsigned cross_prev;  // bit j: previous sample of crossing slot j was above its level
 };
 
 __device__ __forceinline__ double load_save(const pb_solve_args& a, int si)
@@ -90,76 +156,70 @@ __device__ __forceinline__ double load_save(const pb_solve_args& a, int si)
     return si < a.n_save ? __ldg(a.save_ts + si) : CUDART_INF;
 }
 
-template <class Sys, class R, bool MIXED>
+template <class Sys, class R>
 struct Integrator {
     static constexpr int S = Sys::S;
+    static constexpr bool MIXED = std::is_same<R, float>::value;
     using L_t = Lane<Sys, R>;
+    using St = Stats<S>;
 
-    // ---- one save point: window statistics, optional full output, median window
-    __device__ static void record(L_t& L, const R (&v)[S], int64_t traj, const pb_solve_args& a)
+    // ---- the save points inside (t, tn]: interpolate each and fold it into the
+    // shared-memory statistics (`interp` produces the sample at save instant ts).
+    template <class Interp>
+    __device__ static void record_run(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a,
+                                      double tn, const Interp& interp)
     {
-        if (L.si >= a.win_begin) {
-            const int n = L.nsamp;
+        const bool stats_on = a.n_features > 0;
+        const int64_t nwin = a.n_save - a.win_begin;
+        while (L.si < a.n_save && L.next_save <= tn + dp::save_slack) {
+            R v[S];
+            interp(L.next_save, v);
+            if (L.si >= a.win_begin && stats_on) {
+                const int n = st.nsamp();
+                int flg = st.flags();
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const double x = static_cast<double>(v[s]);
-                if (n == 0) {
-                    L.shift[s] = isfinite(x) ? x : 0.0;
-                    L.mn[s] = v[s];
-                    L.mx[s] = v[s];
+                for (int s = 0; s < S; ++s) {
+                    const double x = static_cast<double>(v[s]);
+                    if (n == 0) st.shift(s) = isfinite(x) ? x : 0.0;
+                    const double dd = x - st.shift(s);
+                    st.s1(s) += dd;
+                    st.s2(s) += dd * dd;
+                    st.mn(s) = fmin(st.mn(s), x);
+                    st.mx(s) = fmax(st.mx(s), x);
+                    st.last(s) = x;
+                    if (x != x) flg |= 1 << s;
                 }
-                const double d = x - L.shift[s];
-                L.s1[s] += d;
-                L.s2[s] += d * d;
-                L.mn[s] = fmin(L.mn[s], v[s]);
-                L.mx[s] = fmax(L.mx[s], v[s]);
-                if (isnan(x)) L.nan_mask |= 1u << s;
-                L.last[s] = v[s];
+                for (int j = 0; j < pl.n_cross; ++j) {
+                    const bool above = static_cast<double>(pick(v, pl.cross_state[j])) > pl.cross_level[j];
+                    const bool prev = (flg >> (8 + j)) & 1;
+                    if (n > 0 && above != prev) st.cross(j) += 1;
+                    flg = (flg & ~(1 << (8 + j))) | (static_cast<int>(above) << (8 + j));
+                }
+                for (int m = 0; m < pl.n_med; ++m)
+                    a.median_scratch[(traj * pl.n_med + m) * nwin + (L.si - a.win_begin)] =
+                        static_cast<float>(pick(v, pl.med_state[m]));
+                st.nsamp() = n + 1;
+                st.flags() = flg;
             }
-            int j = 0, med = 0;
-            for (int c = 0; c < a.n_features; ++c) {
-                const int kind = a.feat_kind[c];
-                if (kind == PB_FEAT_CROSSINGS && j < PB_MAX_CROSSING) {
-                    const bool above = static_cast<double>(pick(v, a.feat_state[c])) > a.feat_param[c];
-                    const bool prev = (L.cross_prev >> j) & 1u;
-                    if (n > 0 && above != prev) {
+            if (a.y_full_out) {
+                const int64_t base = ((int64_t)L.si * a.n_traj + traj) * S;
+                if (a.y_out_dtype == PB_DTYPE_F64) {
+                    double* o = static_cast<double*>(a.y_full_out) + base;
 #pragma unroll
-                        for (int q = 0; q < PB_MAX_CROSSING; ++q) L.cross_cnt[q] += (q == j);
-                    }
-                    L.cross_prev = (L.cross_prev & ~(1u << j)) | (static_cast<unsigned>(above) << j);
-                    ++j;
-                } else if (kind == PB_FEAT_MEDIAN) {
-                    const int64_t nwin = a.n_save - a.win_begin;
-                    a.median_scratch[(traj * count_median(a) + med) * nwin + (L.si - a.win_begin)] =
-                        static_cast<float>(pick(v, a.feat_state[c]));
-                    ++med;
+                    for (int s = 0; s < S; ++s) o[s] = static_cast<double>(v[s]);
+                } else {
+                    float* o = static_cast<float*>(a.y_full_out) + base;
+#pragma unroll
+                    for (int s = 0; s < S; ++s) o[s] = static_cast<float>(v[s]);
                 }
             }
-            L.nsamp = n + 1;
+            L.si++;
+            L.next_save = load_save(a, L.si);
         }
-        if (a.y_full_out) {
-            const int64_t base = ((int64_t)L.si * a.n_traj + traj) * S;
-            if (a.y_out_dtype == PB_DTYPE_F64) {
-                double* o = static_cast<double*>(a.y_full_out) + base;
-#pragma unroll
-                for (int s = 0; s < S; ++s) o[s] = static_cast<double>(v[s]);
-            } else {
-                float* o = static_cast<float*>(a.y_full_out) + base;
-#pragma unroll
-                for (int s = 0; s < S; ++s) o[s] = static_cast<float>(v[s]);
-            }
-        }
-    }
-
-    __device__ static int count_median(const pb_solve_args& a)
-    {
-        int m = 0;
-        for (int c = 0; c < a.n_features; ++c) m += (a.feat_kind[c] == PB_FEAT_MEDIAN);
-        return m;
     }
 
     // ---- start a trajectory: load y0/params, first derivative, initial step
-    __device__ static void begin(L_t& L, int64_t traj, const pb_solve_args& a)
+    __device__ static void begin(L_t& L, St& st, int64_t traj, const pb_solve_args& a)
     {
         int64_t ic = traj, prow = 0;
         if (a.layout == PB_LAYOUT_CROSS) {
@@ -173,8 +233,9 @@ struct Integrator {
         double y0d[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            y0d[s] = (a.y0_dtype == PB_DTYPE_F64) ? __ldg(static_cast<const double*>(a.y0) + ic * S + s)
-                                                  : static_cast<double>(__ldg(static_cast<const float*>(a.y0) + ic * S + s));
+            y0d[s] = (a.y0_dtype == PB_DTYPE_F64)
+                         ? __ldg(static_cast<const double*>(a.y0) + ic * S + s)
+                         : static_cast<double>(__ldg(static_cast<const float*>(a.y0) + ic * S + s));
             L.y[s] = static_cast<R>(y0d[s]);
             L.yc[s] = R(0);
         }
@@ -186,23 +247,14 @@ struct Integrator {
         L.status = bad_row ? PB_TRAJ_BAD_INPUT : PB_TRAJ_OK;
         L.si = a.y_full_out ? 0 : a.win_begin;
         L.next_save = load_save(a, L.si);
-        L.nsamp = 0;
-        L.nan_mask = 0;
-        L.cross_prev = 0;
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            L.shift[s] = 0.0;
-            L.s1[s] = 0.0;
-            L.s2[s] = 0.0;
-            L.mn[s] = R(0);
-            L.mx[s] = R(0);
-            L.last[s] = R(0);
-        }
-#pragma unroll
-        for (int j = 0; j < PB_MAX_CROSSING; ++j) L.cross_cnt[j] = 0;
+        st.reset();
 
-        Sys::f(L.t, L.y, L.k1, L.p);
-        // initial step size (dopri5_generic.zig:270-321); norms in FP64
+        // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
+        if (MIXED) {
+            Sys::f(ClockF32{reduce_two_pi(a.t0)}, L.y, L.k1, L.p);
+        } else {
+            Sys::f(ClockF64{a.t0}, L.y, L.k1, L.p);
+        }
         double d0 = 0.0, d1 = 0.0;
         double sc[S];
 #pragma unroll
@@ -218,7 +270,11 @@ struct Integrator {
         R ytmp[S], ftmp[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) ytmp[s] = static_cast<R>(y0d[s] + h0 * static_cast<double>(L.k1[s]));
-        Sys::f(L.t + h0, ytmp, ftmp, L.p);
+        if (MIXED) {
+            Sys::f(ClockF32{reduce_two_pi(a.t0 + h0)}, ytmp, ftmp, L.p);
+        } else {
+            Sys::f(ClockF64{a.t0 + h0}, ytmp, ftmp, L.p);
+        }
         double d2 = 0.0;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -226,15 +282,50 @@ struct Integrator {
             d2 += r * r;
         }
         d2 = sqrt(d2 / S) / h0;
-        const double h1 = (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / fmax(d1, d2), 0.2);
+        const double h1 =
+            (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / fmax(d1, d2), 0.2);
         L.dt = fmin(100.0 * h0, h1);
     }
 
-    // ---- one attempted step; returns true once the trajectory is finished
-    __device__ static bool step(L_t& L, int64_t traj, const pb_solve_args& a)
+    template <class TB>
+    __device__ __forceinline__ static void stages(const TB& tb, const L_t& L, R h, R (&k2)[S], R (&k3)[S],
+                                                  R (&k4)[S], R (&k5)[S], R (&k6)[S], R (&k7)[S], R (&d)[S],
+                                                  R (&yn)[S])
     {
-        if (!(L.t < a.t1)) return true;
-        if (L.steps >= a.max_steps) return true;
+        R ys[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a21) * L.k1[s]);
+        Sys::f(tb.at(dp::c2), ys, k2, L.p);
+#pragma unroll
+        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a31) * L.k1[s] + R(dp::a32) * k2[s]);
+        Sys::f(tb.at(dp::c3), ys, k3, L.p);
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            ys[s] = L.y[s] + h * (R(dp::a41) * L.k1[s] + R(dp::a42) * k2[s] + R(dp::a43) * k3[s]);
+        Sys::f(tb.at(dp::c4), ys, k4, L.p);
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            ys[s] = L.y[s] + h * (R(dp::a51) * L.k1[s] + R(dp::a52) * k2[s] + R(dp::a53) * k3[s] +
+                                  R(dp::a54) * k4[s]);
+        Sys::f(tb.at(dp::c5), ys, k5, L.p);
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            ys[s] = L.y[s] + h * (R(dp::a61) * L.k1[s] + R(dp::a62) * k2[s] + R(dp::a63) * k3[s] +
+                                  R(dp::a64) * k4[s] + R(dp::a65) * k5[s]);
+        Sys::f(tb.at(1.0), ys, k6, L.p);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            d[s] = h * (R(dp::b1) * L.k1[s] + R(dp::b3) * k3[s] + R(dp::b4) * k4[s] + R(dp::b5) * k5[s] +
+                        R(dp::b6) * k6[s]);
+            yn[s] = L.y[s] + d[s];
+        }
+        Sys::f(tb.at(1.0), yn, k7, L.p);
+    }
+
+    // ---- one attempted step; returns true once the trajectory is finished
+    __device__ static bool step(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
+    {
+        if (!(L.t < a.t1) || L.steps >= a.max_steps) return true;
         L.steps++;
         double dt = L.dt;
         if (L.t + dt > a.t1) dt = a.t1 - L.t;
@@ -245,81 +336,73 @@ struct Integrator {
         }
         const R h = static_cast<R>(dt);
         const double t = L.t;
-        R k2[S], k3[S], k4[S], k5[S], k6[S], k7[S], ys[S], d[S], yn[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a21) * L.k1[s]);
-        Sys::f(t + dp::c2 * dt, ys, k2, L.p);
-#pragma unroll
-        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a31) * L.k1[s] + R(dp::a32) * k2[s]);
-        Sys::f(t + dp::c3 * dt, ys, k3, L.p);
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a41) * L.k1[s] + R(dp::a42) * k2[s] + R(dp::a43) * k3[s]);
-        Sys::f(t + dp::c4 * dt, ys, k4, L.p);
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a51) * L.k1[s] + R(dp::a52) * k2[s] + R(dp::a53) * k3[s] +
-                                  R(dp::a54) * k4[s]);
-        Sys::f(t + dp::c5 * dt, ys, k5, L.p);
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a61) * L.k1[s] + R(dp::a62) * k2[s] + R(dp::a63) * k3[s] +
-                                  R(dp::a64) * k4[s] + R(dp::a65) * k5[s]);
-        Sys::f(t + dt, ys, k6, L.p);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            d[s] = h * (R(dp::b1) * L.k1[s] + R(dp::b3) * k3[s] + R(dp::b4) * k4[s] + R(dp::b5) * k5[s] +
-                        R(dp::b6) * k6[s]);
-            yn[s] = L.y[s] + d[s];
+        R k2[S], k3[S], k4[S], k5[S], k6[S], k7[S], d[S], yn[S];
+        if (MIXED) {
+            const float r0 = Sys::kTime ? reduce_two_pi(t) : 0.f;
+            stages(TimeBaseF32{r0, static_cast<float>(h)}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
+        } else {
+            stages(TimeBaseF64{t, dt}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
         }
-        Sys::f(t + dt, yn, k7, L.p);
 
-        // embedded error estimate; the norm is accumulated in FP64
-        double err = 0.0;
+        // embedded error estimate (RMS norm, dopri5_generic.zig:185-192)
+        double err2 = 0.0;
+        if (MIXED) {
+            const float rt = static_cast<float>(a.rtol), at = static_cast<float>(a.atol);
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const R e = h * (R(dp::e1) * L.k1[s] + R(dp::e3) * k3[s] + R(dp::e4) * k4[s] + R(dp::e5) * k5[s] +
-                             R(dp::e6) * k6[s] + R(dp::e7) * k7[s]);
-            const double sc =
-                a.atol + a.rtol * fmax(fabs(static_cast<double>(L.y[s])), fabs(static_cast<double>(yn[s])));
-            const double r = static_cast<double>(e) / sc;
-            err += r * r;
+            for (int s = 0; s < S; ++s) {
+                const float e = static_cast<float>(
+                    h * (R(dp::e1) * L.k1[s] + R(dp::e3) * k3[s] + R(dp::e4) * k4[s] + R(dp::e5) * k5[s] +
+                         R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
+                const float sc =
+                    fmaf(rt, fmaxf(fabsf(static_cast<float>(L.y[s])), fabsf(static_cast<float>(yn[s]))), at);
+                const double r = static_cast<double>(__fdividef(e, sc));
+                err2 = fma(r, r, err2);
+            }
+            err2 *= 1.0 / S;
+        } else {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const double e = static_cast<double>(
+                    h * (R(dp::e1) * L.k1[s] + R(dp::e3) * k3[s] + R(dp::e4) * k4[s] + R(dp::e5) * k5[s] +
+                         R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
+                const double sc =
+                    a.atol + a.rtol * fmax(fabs(static_cast<double>(L.y[s])), fabs(static_cast<double>(yn[s])));
+                const double r = e / sc;
+                err2 += r * r;
+            }
+            err2 /= S;
         }
-        err = sqrt(err / S);
-        if (!isfinite(err)) {
+        if (!isfinite(err2)) {
             L.status = PB_TRAJ_NONFINITE;
             return true;
         }
+        const bool accept = err2 <= 1.0;
+        const double tn = t + dt;
 
-        const bool accept = err <= 1.0;
-        if (accept) {
-            const double tn = t + dt;
-            if (L.next_save <= tn + dp::save_slack) {
-                R ia[S], ib[S], icf[S];
+        if (accept && L.next_save <= tn + dp::save_slack) {
+            // dense output (dopri5_generic.zig:194-221): 4th-order polynomial in x = (ts - t)/dt
+            R ia[S], ib[S], icf[S];
 #pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const R ym = L.y[s] + h * (R(dp::m1) * L.k1[s] + R(dp::m3) * k3[s] + R(dp::m4) * k4[s] +
-                                               R(dp::m5) * k5[s] + R(dp::m6) * k6[s] + R(dp::m7) * k7[s]);
-                    ia[s] = R(2) * h * (k7[s] - L.k1[s]) - R(8) * (yn[s] + L.y[s]) + R(16) * ym;
-                    ib[s] = h * (R(5) * L.k1[s] - R(3) * k7[s]) + R(18) * L.y[s] + R(14) * yn[s] - R(32) * ym;
-                    icf[s] = h * (k7[s] - R(4) * L.k1[s]) - R(11) * L.y[s] - R(5) * yn[s] + R(16) * ym;
-                }
-                while (L.si < a.n_save && L.next_save <= tn + dp::save_slack) {
-                    R v[S];
-                    if (L.next_save <= t + dp::save_slack) {
-#pragma unroll
-                        for (int s = 0; s < S; ++s) v[s] = L.y[s];
-                    } else {
-                        const R x = static_cast<R>((L.next_save - t) / dt);
-#pragma unroll
-                        for (int s = 0; s < S; ++s)
-                            v[s] = L.y[s] + x * (h * L.k1[s] + x * (icf[s] + x * (ib[s] + x * ia[s])));
-                    }
-                    record(L, v, traj, a);
-                    L.si++;
-                    L.next_save = load_save(a, L.si);
-                }
+            for (int s = 0; s < S; ++s) {
+                const R ym = L.y[s] + h * (R(dp::m1) * L.k1[s] + R(dp::m3) * k3[s] + R(dp::m4) * k4[s] +
+                                           R(dp::m5) * k5[s] + R(dp::m6) * k6[s] + R(dp::m7) * k7[s]);
+                ia[s] = R(2) * h * (k7[s] - L.k1[s]) - R(8) * (yn[s] + L.y[s]) + R(16) * ym;
+                ib[s] = h * (R(5) * L.k1[s] - R(3) * k7[s]) + R(18) * L.y[s] + R(14) * yn[s] - R(32) * ym;
+                icf[s] = h * (k7[s] - R(4) * L.k1[s]) - R(11) * L.y[s] - R(5) * yn[s] + R(16) * ym;
             }
+            record_run(L, st, pl, traj, a, tn, [&](double ts, R (&v)[S]) {
+                if (ts <= t + dp::save_slack) {
+#pragma unroll
+                    for (int s = 0; s < S; ++s) v[s] = L.y[s];
+                } else {
+                    const R x = static_cast<R>((ts - t) / dt);
+#pragma unroll
+                    for (int s = 0; s < S; ++s)
+                        v[s] = L.y[s] + x * (h * L.k1[s] + x * (icf[s] + x * (ib[s] + x * ia[s])));
+                }
+            });
+        }
+        if (accept) {
             if (MIXED) {
                 // compensated accumulation keeps the FP32 state from drifting over
                 // ~1e4 accepted steps (Kahan summation of the increments d)
@@ -347,43 +430,44 @@ struct Integrator {
                 }
             }
         }
+        // step-size control (dopri5_generic.zig:228-235)
         double fac;
-        if (err == 0.0) {
-            fac = dp::max_factor;
+        if (MIXED) {
+            const float e2f = static_cast<float>(err2);
+            const float g = 0.9f * exp2f(-0.1f * __log2f(e2f));  // 0.9 * err^-0.2 with err^2 = e2f
+            fac = (err2 == 0.0) ? dp::max_factor : static_cast<double>(fminf(10.f, fmaxf(accept ? 1.f : 0.2f, g)));
         } else {
-            double g;
-            if (MIXED) {
-                g = static_cast<double>(0.9f * exp2f(-0.2f * log2f(static_cast<float>(err))));
-            } else {
-                g = dp::safety * pow(err, -0.2);
-            }
-            fac = fmin(dp::max_factor, fmax(accept ? 1.0 : dp::min_factor, g));
+            const double err = sqrt(err2);
+            fac = (err == 0.0) ? dp::max_factor
+                               : fmin(dp::max_factor, fmax(accept ? 1.0 : dp::min_factor, dp::safety * pow(err, -0.2)));
         }
         L.dt = dt * fac;
         return !(L.t < a.t1);
     }
 
     // ---- tail fill, features, status and states of a finished trajectory
-    __device__ static void finish(L_t& L, int64_t traj, const pb_solve_args& a)
+    __device__ static void finish(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
     {
         if (L.status == PB_TRAJ_OK && L.t < a.t1 && L.steps >= a.max_steps) L.status = PB_TRAJ_MAX_STEPS;
         R fill[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) fill[s] = (L.status == PB_TRAJ_UNBOUNDED) ? R(CUDART_INF) : L.y[s];
-        while (L.si < a.n_save) {
-            record(L, fill, traj, a);
-            L.si++;
-        }
+        record_run(L, st, pl, traj, a, CUDART_INF, [&](double, R (&v)[S]) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fill[s];
+        });
         if (a.features_out) {
-            const double n = static_cast<double>(L.nsamp);
+            const int ns = st.nsamp();
+            const double n = static_cast<double>(ns);
+            const int flg = st.flags();
             int j = 0;
             for (int c = 0; c < a.n_features; ++c) {
                 const int kind = a.feat_kind[c];
-                const int st = a.feat_state[c];
-                const double sh = pick(L.shift, st), s1 = pick(L.s1, st), s2 = pick(L.s2, st);
-                const bool has_nan = (L.nan_mask >> st) & 1u;
-                double mx = has_nan ? CUDART_NAN : static_cast<double>(pick(L.mx, st));
-                double mn = has_nan ? CUDART_NAN : static_cast<double>(pick(L.mn, st));
+                const int sidx = a.feat_state[c];
+                const double sh = st.shift(sidx), s1 = st.s1(sidx), s2 = st.s2(sidx);
+                const bool has_nan = (flg >> sidx) & 1;
+                const double mx = has_nan ? CUDART_NAN : st.mx(sidx);
+                const double mn = has_nan ? CUDART_NAN : st.mn(sidx);
                 const double mean = sh + s1 / n;
                 const double var = fmax((s2 - s1 * (s1 / n)) / n, 0.0);
                 double v;
@@ -399,14 +483,14 @@ struct Integrator {
                     case PB_FEAT_LOG_DELTA: v = log(fabs(mx - mean) + 1e-10); break;
                     case PB_FEAT_AMPLITUDE: v = mx - mn; break;
                     case PB_FEAT_CROSSINGS:
-                        v = (j < PB_MAX_CROSSING) ? static_cast<double>(pick(L.cross_cnt, j)) : CUDART_NAN;
+                        v = (j < pl.n_cross) ? static_cast<double>(st.cross(j)) : CUDART_NAN;
                         ++j;
                         break;
-                    case PB_FEAT_LAST: v = static_cast<double>(pick(L.last, st)); break;
+                    case PB_FEAT_LAST: v = st.last(sidx); break;
                     case PB_FEAT_MEDIAN: continue;  // written by the median pass
                     default: v = CUDART_NAN;
                 }
-                if (L.nsamp == 0) v = CUDART_NAN;
+                if (ns == 0) v = CUDART_NAN;
                 a.features_out[traj * a.n_features + c] = v;
             }
         }
@@ -427,7 +511,7 @@ struct Integrator {
 };
 
 // Warp-aggregated fetch from the global work queue: one atomicAdd per warp for
-// all lanes in `mask`; returns this lane's trajectory index (valid if in mask).
+// all lanes in `mask`; returns this lane's queue position (valid if in mask).
 __device__ __forceinline__ int64_t warp_fetch(unsigned long long* q, unsigned mask, int lane)
 {
     const int leader = __ffs(mask) - 1;
@@ -438,52 +522,78 @@ __device__ __forceinline__ int64_t warp_fetch(unsigned long long* q, unsigned ma
     return static_cast<int64_t>(base) + rank;
 }
 
-// Plain schedule: one thread per trajectory, no queue (the FP64 baseline K1
-// when R = double).
-template <class Sys, class R, bool MIXED>
+__device__ __forceinline__ int64_t traj_at(const pb_solve_args& a, int64_t q)
+{
+    return a.order ? static_cast<int64_t>(__ldg(a.order + q)) : q;
+}
+
+template <class Sys>
+__device__ __forceinline__ Stats<Sys::S> stats_slot(unsigned char* smem)
+{
+    Stats<Sys::S> st;
+    st.nthr = blockDim.x;
+    st.tid = threadIdx.x;
+    st.d = reinterpret_cast<double*>(smem);
+    st.i = reinterpret_cast<int*>(smem + static_cast<size_t>(6 * Sys::S * 8) * blockDim.x);
+    return st;
+}
+
+// Plain schedule: one thread per trajectory, no queue (the FP64 baseline when
+// R = double).
+template <class Sys, class R>
 __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
 {
-    using I = Integrator<Sys, R, MIXED>;
-    const int64_t traj = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (traj >= a.n_traj) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ Plan pl;
+    if (threadIdx.x == 0) build_plan(pl, a);
+    __syncthreads();
+    using I = Integrator<Sys, R>;
+    const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= a.n_traj) return;
+    const int64_t traj = traj_at(a, q);
+    auto st = stats_slot<Sys>(smem);
     typename I::L_t L;
-    I::begin(L, traj, a);
-    while (!I::step(L, traj, a)) {
+    I::begin(L, st, traj, a);
+    while (!I::step(L, st, pl, traj, a)) {
     }
-    I::finish(L, traj, a);
+    I::finish(L, st, pl, traj, a);
 }
 
 // Queue schedule: persistent lanes; a lane whose trajectory finished takes the
 // next one from the global queue (warp-aggregated), so long trajectories do not
 // leave the rest of their warp idle.  Every loop is bounded: each trajectory
 // runs at most max_steps attempted steps and the queue holds n_traj entries.
-template <class Sys, class R, bool MIXED>
+template <class Sys, class R>
 __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
 {
-    using I = Integrator<Sys, R, MIXED>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ Plan pl;
+    if (threadIdx.x == 0) build_plan(pl, a);
+    __syncthreads();
+    using I = Integrator<Sys, R>;
     const int lane = threadIdx.x & 31;
+    auto st = stats_slot<Sys>(smem);
     typename I::L_t L;
-    int64_t traj = warp_fetch(a.queue_counter, 0xffffffffu, lane);
-    bool have = traj < a.n_traj;
+    int64_t q = warp_fetch(a.queue_counter, 0xffffffffu, lane);
+    bool have = q < a.n_traj;
     bool exhausted = !have;
-    if (have) I::begin(L, traj, a);
+    int64_t traj = have ? traj_at(a, q) : 0;
+    if (have) I::begin(L, st, traj, a);
     while (__any_sync(0xffffffffu, have)) {
-        if (have && I::step(L, traj, a)) {
-            I::finish(L, traj, a);
+        if (have && I::step(L, st, pl, traj, a)) {
+            I::finish(L, st, pl, traj, a);
             have = false;
         }
         const bool want = !have && !exhausted;
         const unsigned m = __ballot_sync(0xffffffffu, want);
-        if (m) {
-            if (want) {
-                const int64_t nt = warp_fetch(a.queue_counter, m, lane);
-                if (nt < a.n_traj) {
-                    traj = nt;
-                    have = true;
-                    I::begin(L, traj, a);
-                } else {
-                    exhausted = true;
-                }
+        if (m && want) {
+            q = warp_fetch(a.queue_counter, m, lane);
+            if (q < a.n_traj) {
+                traj = traj_at(a, q);
+                have = true;
+                I::begin(L, st, traj, a);
+            } else {
+                exhausted = true;
             }
         }
     }

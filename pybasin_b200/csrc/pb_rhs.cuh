@@ -1,33 +1,49 @@
 // Right-hand sides of the built-in systems as templated device functors.
 //
 // Each functor exposes S (state dimension), NP (parameter count) and
-//   template <class R> static void f(double t, const R* y, R* dy, const R* p)
+//   template <class R, class Clock> static void f(const Clock& c, const R* y, R* dy, const R* p)
 // where R is the stage arithmetic (double for the plain FP64 kernel, float for
-// the mixed kernel).  Time always arrives in FP64; functors that need t reduce
-// it in FP64 before handing a small argument to R arithmetic.
+// the mixed kernel) and `c` is the time of the stage.  Time is kept in FP64 by
+// the integrator; the FP32 clock carries it already reduced modulo 2*pi (one
+// FP64 reduction per step, stage offsets added in FP32), which is all a
+// periodically forced system needs.
 #pragma once
 #include <cuda_runtime.h>
 
 namespace pb {
 
+// time of one stage, FP64 kernel: the stage instant itself
+struct ClockF64 {
+    double t;
+};
+// time of one stage, FP32 kernel: the stage instant modulo 2*pi, in [-pi, pi + h]
+struct ClockF32 {
+    float phase;
+};
+
+__device__ __forceinline__ double clock_cos(const ClockF64& c) { return cos(c.t); }
+__device__ __forceinline__ float clock_cos(const ClockF32& c) { return cosf(c.phase); }
+
 __device__ __forceinline__ float r_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double r_sin(double x) { return sin(x); }
+__device__ __forceinline__ float r_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double r_abs(double x) { return fabs(x); }
 
-// cos(t) for t in FP64.  FP64 stages: plain cos.  FP32 stages: reduce t modulo
-// 2*pi in FP64 (|t| stays far below 2^40 here, so k*2pi is exact enough) and
-// evaluate cosf on the reduced argument in [-pi, pi].
-template <class R>
-__device__ __forceinline__ R cos_of_time(double t);
-template <>
-__device__ __forceinline__ double cos_of_time<double>(double t) { return cos(t); }
-template <>
-__device__ __forceinline__ float cos_of_time<float>(double t)
+// Per-step time base: t and dt in FP64; stage clocks derived from it.
+struct TimeBaseF64 {
+    double t, dt;
+    __device__ __forceinline__ ClockF64 at(double c) const { return ClockF64{t + c * dt}; }
+};
+struct TimeBaseF32 {
+    float r0, h;  // t mod 2*pi (FP64-reduced, then rounded), FP32 step
+    __device__ __forceinline__ ClockF32 at(double c) const { return ClockF32{r0 + static_cast<float>(c) * h}; }
+};
+__device__ __forceinline__ float reduce_two_pi(double t)
 {
     const double two_pi = 6.283185307179586476925286766559;
     const double inv_two_pi = 0.15915494309189533576888376337251;
-    double k = rint(t * inv_two_pi);
-    double r = fma(-k, two_pi, t);
-    return cosf(static_cast<float>(r));
+    const double k = rint(t * inv_two_pi);
+    return static_cast<float>(fma(-k, two_pi, t));
 }
 
 // dy/dt = p0 * y  (tests/unit/solvers/test_solver.py:16-21 of the reference)
@@ -35,8 +51,9 @@ template <int DIM>
 struct SysLinear {
     static constexpr int S = DIM;
     static constexpr int NP = 1;
-    template <class R>
-    __device__ __forceinline__ static void f(double, const R* y, R* dy, const R* p)
+    static constexpr bool kTime = false;
+    template <class R, class C>
+    __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
     {
 #pragma unroll
         for (int i = 0; i < S; ++i) dy[i] = p[0] * y[i];
@@ -48,8 +65,9 @@ struct SysLinear {
 struct SysPendulum {
     static constexpr int S = 2;
     static constexpr int NP = 3;
-    template <class R>
-    __device__ __forceinline__ static void f(double, const R* y, R* dy, const R* p)
+    static constexpr bool kTime = false;
+    template <class R, class C>
+    __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
     {
         dy[0] = y[1];
         dy[1] = -p[0] * y[1] + p[1] - p[2] * r_sin(y[0]);
@@ -61,12 +79,13 @@ struct SysPendulum {
 struct SysDuffing {
     static constexpr int S = 2;
     static constexpr int NP = 3;
-    template <class R>
-    __device__ __forceinline__ static void f(double t, const R* y, R* dy, const R* p)
+    static constexpr bool kTime = true;
+    template <class R, class C>
+    __device__ __forceinline__ static void f(const C& c, const R* y, R* dy, const R* p)
     {
         const R x = y[0];
         dy[0] = y[1];
-        dy[1] = -p[0] * y[1] - p[1] * x * x * x + p[2] * cos_of_time<R>(t);
+        dy[1] = -p[0] * y[1] - p[1] * x * x * x + p[2] * clock_cos(c);
     }
 };
 
@@ -77,14 +96,15 @@ template <bool MASKED>
 struct SysLorenz {
     static constexpr int S = 3;
     static constexpr int NP = 3;
-    template <class R>
-    __device__ __forceinline__ static void f(double, const R* y, R* dy, const R* p)
+    static constexpr bool kTime = false;
+    template <class R, class C>
+    __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
     {
         R f0 = p[0] * (y[1] - y[0]);
         R f1 = p[1] * y[0] - y[0] * y[2] - y[1];
         R f2 = y[0] * y[1] - p[2] * y[2];
         if (MASKED) {
-            R m = fmax(fabs(y[0]), fmax(fabs(y[1]), fabs(y[2])));
+            const R m = fmax(r_abs(y[0]), fmax(r_abs(y[1]), r_abs(y[2])));
             if (!(m < R(200))) f0 = f1 = f2 = R(0);
         }
         dy[0] = f0;

@@ -52,6 +52,7 @@ class SolveRequest:
     keep_steps: bool = False
     block_size: int = 0
     grid_blocks: int = 0
+    order: torch.Tensor | None = None  # (n_traj,) int32 processing order
 
 
 @dataclass
@@ -117,6 +118,7 @@ def build_args(req: SolveRequest, out: SolveResult, queue: torch.Tensor | None, 
     a.steps_out = _ptr(out.steps)
     a.queue_counter = _ptr(queue)
     a.median_scratch = _ptr(median)
+    a.order = _ptr(req.order)
     return a
 
 
@@ -206,3 +208,34 @@ def occupancy(system: int, dim: int, precision: int, schedule: int, block: int) 
         "pb_query_occupancy",
     )
     return bps.value, sms.value
+
+
+def _spread_bits(v: torch.Tensor, dims: int, bits: int) -> torch.Tensor:
+    """Place bit b of v at position b*dims (Morton interleave helper)."""
+    out = torch.zeros_like(v)
+    for b in range(bits):
+        out |= ((v >> b) & 1) << (b * dims)
+    return out
+
+
+def spatial_order(y0: torch.Tensor, bits: int | None = None) -> torch.Tensor:
+    """Permutation of the rows of ``y0`` along a Morton (Z-order) curve of its bounding box.
+
+    Neighbouring initial conditions mostly share an attractor and a step count, so
+    integrating them in the same warp keeps the warp's lanes busy together.
+    Returns int32 indices on y0's device.
+    """
+    n, dims = y0.shape
+    if n == 0:
+        return torch.zeros((0,), dtype=torch.int32, device=y0.device)
+    d = min(dims, 4)
+    bits = bits or max(1, 60 // d if d > 2 else 20)
+    bits = min(bits, 62 // d)
+    x = y0[:, :d].to(torch.float64)
+    lo = x.amin(dim=0, keepdim=True)
+    span = (x.amax(dim=0, keepdim=True) - lo).clamp_min(1e-300)
+    q = ((x - lo) / span * ((1 << bits) - 1)).nan_to_num(0.0).clamp(0, (1 << bits) - 1).to(torch.int64)
+    key = torch.zeros((n,), dtype=torch.int64, device=y0.device)
+    for k in range(d):
+        key |= _spread_bits(q[:, k], d, bits) << k
+    return torch.argsort(key).to(torch.int32)
