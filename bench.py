@@ -228,8 +228,10 @@ def make_pipeline(dev: torch.device, precision: str, schedule: str):
 def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: torch.Tensor, dist_on: bool):
     """Device-timed passes: per-step events around the pass and around the integrator
     kernel, with an L2 flush (write of a 256 MB buffer) between steps."""
-    from pybasin_b200 import _lib as L
     import ctypes
+
+    from pybasin_b200 import _lib as L
+    from pybasin_b200.engine import spatial_order
 
     lib = L.load()
     s = torch.cuda.current_stream()
@@ -239,14 +241,16 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
     if dist_on:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(4)) for _ in range(steps)]
     for i in range(steps):
         flush.fill_(i)
-        a, b, c = ev[i]
+        a, k0, b, c = ev[i]
         n = y0_dev.shape[0]
-        pipe.y0_buf[:n].copy_(y0_dev, non_blocking=True)
         a.record(s)
+        pipe.y0_buf[:n].copy_(y0_dev, non_blocking=True)
+        if pipe.solver.order == "morton":
+            pipe.order[:n].copy_(spatial_order(y0_dev))
+        k0.record(s)
         L.check(lib.pb_solve_batch(ctypes.byref(pipe.args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
         b.record(s)
         feats = pipe.out.features
@@ -258,8 +262,8 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
     torch.cuda.synchronize()
     if dist_on:
         torch.distributed.barrier()
-    step_ms = [a.elapsed_time(c) for a, b, c in ev]
-    kern_ms = [a.elapsed_time(b) for a, b, c in ev]
+    step_ms = [a.elapsed_time(c) for a, k0, b, c in ev]
+    kern_ms = [k0.elapsed_time(b) for a, k0, b, c in ev]
     return step_ms, kern_ms
 
 

@@ -35,7 +35,8 @@ def _inputs() -> list[Path]:
 
 
 def lib_path() -> Path:
-    return OUT_DIR / LIB_NAME
+    override = os.environ.get("PB_LIBRARY_PATH")
+    return Path(override) if override else OUT_DIR / LIB_NAME
 
 
 def is_stale() -> bool:
@@ -59,7 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         "-O3",
         "-lineinfo",
         "-std=c++17",
-        "--use_fast_math" if os.environ.get("PB_FAST_MATH") else "-DPB_PRECISE_MATH",
+        *os.environ.get("PB_NVCC_DEFINES", "").split(),
         "-Xcompiler",
         "-fPIC",
         "-shared",

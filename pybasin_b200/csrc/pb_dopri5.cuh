@@ -78,6 +78,7 @@ __device__ __forceinline__ T pick(const T (&arr)[N], int idx)
 struct Plan {
     int n_cross;
     int n_med;
+    unsigned stat_mask;  // states that any feature column reads
     int cross_state[PB_MAX_CROSSING];
     double cross_level[PB_MAX_CROSSING];
     int med_state[PB_MAX_FEATURES];
@@ -86,7 +87,9 @@ struct Plan {
 __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
 {
     int nc = 0, nm = 0;
+    unsigned mask = 0;
     for (int c = 0; c < a.n_features; ++c) {
+        mask |= 1u << a.feat_state[c];
         if (a.feat_kind[c] == PB_FEAT_CROSSINGS && nc < PB_MAX_CROSSING) {
             pl.cross_state[nc] = a.feat_state[c];
             pl.cross_level[nc] = a.feat_param[c];
@@ -97,6 +100,7 @@ __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
     }
     pl.n_cross = nc;
     pl.n_med = nm;
+    pl.stat_mask = mask;
 }
 
 // Per-thread window statistics in shared memory, structure-of-arrays
@@ -163,43 +167,58 @@ struct Integrator {
     using L_t = Lane<Sys, R>;
     using St = Stats<S>;
 
-    // ---- the save points inside (t, tn]: interpolate each and fold it into the
-    // shared-memory statistics (`interp` produces the sample at save instant ts).
+    // ---- the save points inside (t, tn]: interpolate each (`interp` produces the
+    // sample at save instant ts) and fold it into register partials of the window
+    // statistics, merged into the shared-memory slot once per run.  The next save
+    // instant is fetched one iteration ahead so its load latency overlaps the work.
     template <class Interp>
     __device__ static void record_run(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a,
                                       double tn, const Interp& interp)
     {
-        const bool stats_on = a.n_features > 0;
+        const bool stats_on = pl.stat_mask != 0;
         const int64_t nwin = a.n_save - a.win_begin;
-        while (L.si < a.n_save && L.next_save <= tn + dp::save_slack) {
+        const int n = st.nsamp();
+        int flg = st.flags();
+        R sh[S], ls1[S], ls2[S], lmn[S], lmx[S], llast[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            sh[s] = static_cast<R>(st.shift(s));
+            ls1[s] = R(0);
+            ls2[s] = R(0);
+            lmn[s] = R(CUDART_INF);
+            lmx[s] = R(-CUDART_INF);
+            llast[s] = R(0);
+        }
+        int cnt = 0;
+        double ts = L.next_save;
+        while (L.si < a.n_save && ts <= tn + dp::save_slack) {
+            const double ts_next = load_save(a, L.si + 1);
             R v[S];
-            interp(L.next_save, v);
+            interp(ts, v);
             if (L.si >= a.win_begin && stats_on) {
-                const int n = st.nsamp();
-                int flg = st.flags();
+                const bool first = (n + cnt) == 0;
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
-                    const double x = static_cast<double>(v[s]);
-                    if (n == 0) st.shift(s) = isfinite(x) ? x : 0.0;
-                    const double dd = x - st.shift(s);
-                    st.s1(s) += dd;
-                    st.s2(s) += dd * dd;
-                    st.mn(s) = fmin(st.mn(s), x);
-                    st.mx(s) = fmax(st.mx(s), x);
-                    st.last(s) = x;
-                    if (x != x) flg |= 1 << s;
+                    if (!((pl.stat_mask >> s) & 1)) continue;
+                    if (first) sh[s] = isfinite(v[s]) ? v[s] : R(0);
+                    const R dd = v[s] - sh[s];
+                    ls1[s] += dd;
+                    ls2[s] = fma(dd, dd, ls2[s]);
+                    lmn[s] = fmin(lmn[s], v[s]);
+                    lmx[s] = fmax(lmx[s], v[s]);
+                    llast[s] = v[s];
+                    if (v[s] != v[s]) flg |= 1 << s;
                 }
                 for (int j = 0; j < pl.n_cross; ++j) {
                     const bool above = static_cast<double>(pick(v, pl.cross_state[j])) > pl.cross_level[j];
                     const bool prev = (flg >> (8 + j)) & 1;
-                    if (n > 0 && above != prev) st.cross(j) += 1;
+                    if (!first && above != prev) st.cross(j) += 1;
                     flg = (flg & ~(1 << (8 + j))) | (static_cast<int>(above) << (8 + j));
                 }
                 for (int m = 0; m < pl.n_med; ++m)
                     a.median_scratch[(traj * pl.n_med + m) * nwin + (L.si - a.win_begin)] =
                         static_cast<float>(pick(v, pl.med_state[m]));
-                st.nsamp() = n + 1;
-                st.flags() = flg;
+                ++cnt;
             }
             if (a.y_full_out) {
                 const int64_t base = ((int64_t)L.si * a.n_traj + traj) * S;
@@ -214,7 +233,22 @@ struct Integrator {
                 }
             }
             L.si++;
-            L.next_save = load_save(a, L.si);
+            ts = ts_next;
+        }
+        L.next_save = ts;
+        if (cnt > 0) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                if (!((pl.stat_mask >> s) & 1)) continue;
+                if (n == 0) st.shift(s) = static_cast<double>(sh[s]);
+                st.s1(s) += static_cast<double>(ls1[s]);
+                st.s2(s) += static_cast<double>(ls2[s]);
+                st.mn(s) = fmin(st.mn(s), static_cast<double>(lmn[s]));
+                st.mx(s) = fmax(st.mx(s), static_cast<double>(lmx[s]));
+                st.last(s) = static_cast<double>(llast[s]);
+            }
+            st.nsamp() = n + cnt;
+            st.flags() = flg;
         }
     }
 
@@ -355,8 +389,13 @@ struct Integrator {
                          R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
                 const float sc =
                     fmaf(rt, fmaxf(fabsf(static_cast<float>(L.y[s])), fabsf(static_cast<float>(yn[s]))), at);
+#ifdef PB_ERRNORM_F32
+                const float r = __fdividef(e, sc);
+                err2 = static_cast<double>(fmaf(r, r, static_cast<float>(err2)));
+#else
                 const double r = static_cast<double>(__fdividef(e, sc));
                 err2 = fma(r, r, err2);
+#endif
             }
             err2 *= 1.0 / S;
         } else {
@@ -390,12 +429,13 @@ struct Integrator {
                 ib[s] = h * (R(5) * L.k1[s] - R(3) * k7[s]) + R(18) * L.y[s] + R(14) * yn[s] - R(32) * ym;
                 icf[s] = h * (k7[s] - R(4) * L.k1[s]) - R(11) * L.y[s] - R(5) * yn[s] + R(16) * ym;
             }
+            const double inv_dt = 1.0 / dt;
             record_run(L, st, pl, traj, a, tn, [&](double ts, R (&v)[S]) {
                 if (ts <= t + dp::save_slack) {
 #pragma unroll
                     for (int s = 0; s < S; ++s) v[s] = L.y[s];
                 } else {
-                    const R x = static_cast<R>((ts - t) / dt);
+                    const R x = static_cast<R>((ts - t) * inv_dt);
 #pragma unroll
                     for (int s = 0; s < S; ++s)
                         v[s] = L.y[s] + x * (h * L.k1[s] + x * (icf[s] + x * (ib[s] + x * ia[s])));
@@ -510,18 +550,6 @@ struct Integrator {
     }
 };
 
-// Warp-aggregated fetch from the global work queue: one atomicAdd per warp for
-// all lanes in `mask`; returns this lane's queue position (valid if in mask).
-__device__ __forceinline__ int64_t warp_fetch(unsigned long long* q, unsigned mask, int lane)
-{
-    const int leader = __ffs(mask) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(q, static_cast<unsigned long long>(__popc(mask)));
-    base = __shfl_sync(mask, base, leader);
-    const int rank = __popc(mask & ((1u << lane) - 1u));
-    return static_cast<int64_t>(base) + rank;
-}
-
 __device__ __forceinline__ int64_t traj_at(const pb_solve_args& a, int64_t q)
 {
     return a.order ? static_cast<int64_t>(__ldg(a.order + q)) : q;
@@ -559,10 +587,12 @@ __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
     I::finish(L, st, pl, traj, a);
 }
 
-// Queue schedule: persistent lanes; a lane whose trajectory finished takes the
-// next one from the global queue (warp-aggregated), so long trajectories do not
-// leave the rest of their warp idle.  Every loop is bounded: each trajectory
-// runs at most max_steps attempted steps and the queue holds n_traj entries.
+// Queue schedule: persistent warps take 32 consecutive queue positions at a time
+// (one atomicAdd per warp) and come back for the next 32 once all their lanes
+// are done.  Taking whole warps keeps the lanes of a warp on neighbouring
+// positions of the processing order (spatially coherent ICs), which a per-lane
+// refill would scatter.  Every loop is bounded: each trajectory runs at most
+// max_steps attempted steps and the queue holds n_traj entries.
 template <class Sys, class R>
 __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
 {
@@ -573,29 +603,21 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
     using I = Integrator<Sys, R>;
     const int lane = threadIdx.x & 31;
     auto st = stats_slot<Sys>(smem);
-    typename I::L_t L;
-    int64_t q = warp_fetch(a.queue_counter, 0xffffffffu, lane);
-    bool have = q < a.n_traj;
-    bool exhausted = !have;
-    int64_t traj = have ? traj_at(a, q) : 0;
-    if (have) I::begin(L, st, traj, a);
-    while (__any_sync(0xffffffffu, have)) {
-        if (have && I::step(L, st, pl, traj, a)) {
-            I::finish(L, st, pl, traj, a);
-            have = false;
-        }
-        const bool want = !have && !exhausted;
-        const unsigned m = __ballot_sync(0xffffffffu, want);
-        if (m && want) {
-            q = warp_fetch(a.queue_counter, m, lane);
-            if (q < a.n_traj) {
-                traj = traj_at(a, q);
-                have = true;
-                I::begin(L, st, traj, a);
-            } else {
-                exhausted = true;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.queue_counter, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (static_cast<int64_t>(base) >= a.n_traj) break;
+        const int64_t q = static_cast<int64_t>(base) + lane;
+        if (q < a.n_traj) {
+            const int64_t traj = traj_at(a, q);
+            typename I::L_t L;
+            I::begin(L, st, traj, a);
+            while (!I::step(L, st, pl, traj, a)) {
             }
+            I::finish(L, st, pl, traj, a);
         }
+        __syncwarp();
     }
 }
 

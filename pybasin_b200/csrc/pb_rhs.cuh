@@ -22,7 +22,19 @@ struct ClockF32 {
 };
 
 __device__ __forceinline__ double clock_cos(const ClockF64& c) { return cos(c.t); }
-__device__ __forceinline__ float clock_cos(const ClockF32& c) { return cosf(c.phase); }
+__device__ __forceinline__ float clock_cos(const ClockF32& c)
+{
+#ifndef PB_ACCURATE_COS
+    // phase lies in [-pi, pi + h]; fold it back into [-pi, pi], where the hardware
+    // cosine's absolute error is below 2^-21.4 (about 3.6e-7, below the FP32 stage
+    // resolution of a unit-scale state)
+    const float two_pi = 6.28318530717958647692f;
+    const float r = c.phase > 3.14159265358979323846f ? c.phase - two_pi : c.phase;
+    return __cosf(r);
+#else
+    return cosf(c.phase);
+#endif
+}
 
 __device__ __forceinline__ float r_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double r_sin(double x) { return sin(x); }

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import SolveRequest, build_args, SolveResult
+from pybasin_b200.engine import SolveRequest, SolveResult, build_args, spatial_order
 from pybasin_b200.odes import resolve_system
 from pybasin_b200.solver import B200Dopri5Solver
 
@@ -96,6 +96,7 @@ class BasinStabilityPipeline:
             steps=torch.empty((tot,), dtype=torch.int64, device=dev),
         )
         self.queue = torch.zeros((1,), dtype=torch.int64, device=dev)
+        self.order = torch.arange(tot, dtype=torch.int32, device=dev)
         self.labels = torch.empty((n,), dtype=torch.int32, device=dev)
         self.counts = torch.empty((1, self.n_classes + 1), dtype=torch.int64, device=dev)
         rtol, atol = self.solver.effective_tolerances()
@@ -120,6 +121,7 @@ class BasinStabilityPipeline:
             keep_final=False,
             block_size=self.solver.block_size,
             grid_blocks=self.solver.grid_blocks,
+            order=self.order if self.solver.order == "morton" else None,
         )
         self.args = build_args(req, self.out, self.queue, None)
         lib = L.load()
@@ -154,6 +156,8 @@ class BasinStabilityPipeline:
         L.check(rc, "pb_label_nearest")
 
     def kernel_launches_per_pass(self) -> int:
+        """Launches of this library's kernels per pass (integrator + labelling); the
+        Z-order key/argsort of the ICs runs as PyTorch ops before them."""
         return 2
 
     def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
@@ -162,6 +166,8 @@ class BasinStabilityPipeline:
         if self._n != n:
             self._allocate(n)
         self.y0_buf[:n].copy_(y0, non_blocking=True)
+        if self.solver.order == "morton" and n > 1:
+            self.order[:n].copy_(spatial_order(y0))
         if use_graph:
             if self._graph is None:
                 self._capture()

@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import SolveRequest, solve
+from pybasin_b200.engine import SolveRequest, solve, spatial_order
 from pybasin_b200.features import FusedFeatureExtractor
 from pybasin_b200.odes import resolve_system
 
@@ -100,7 +100,10 @@ class B200Dopri5Solver:
     :param max_steps: attempted steps per trajectory before giving up (status MAX_STEPS).
     :param unbounded_threshold: stop a trajectory once max|y| >= this after an accepted
         step (the reference's stop events, e.g. case_studies/lorenz/setup_lorenz_system.py:16-26).
-    :param schedule: ``"queue"`` (persistent lanes + work queue) or ``"plain"``.
+    :param schedule: ``"queue"`` (persistent warps + work queue) or ``"plain"``.
+    :param order: ``"morton"`` integrates the ICs in Z-order of their coordinates so each
+        warp holds neighbouring ICs (similar dynamics and step counts); ``"none"`` keeps
+        the input order.  Outputs are in input order either way.
     """
 
     def __init__(
@@ -123,6 +126,7 @@ class B200Dopri5Solver:
         mixed_rtol_floor: float = MIXED_RTOL_FLOOR,
         block_size: int = 0,
         grid_blocks: int = 0,
+        order: str = "morton",
     ):
         if t_eval is not None and (t_eval[0] < t_span[0] or t_eval[1] > t_span[1]):
             raise ValueError(f"t_eval {t_eval} must be within t_span {t_span}.")
@@ -136,6 +140,9 @@ class B200Dopri5Solver:
             raise ValueError("schedule must be 'queue' or 'plain'")
         if t_steps < 1:
             raise ValueError("t_steps must be >= 1")
+        if order not in ("morton", "none"):
+            raise ValueError("order must be 'morton' or 'none'")
+        self.order = order
         self.t_span = t_span
         self.t_eval = t_eval
         self.t_steps = t_steps
@@ -195,6 +202,7 @@ class B200Dopri5Solver:
             mixed_rtol_floor=self.mixed_rtol_floor,
             block_size=self.block_size,
             grid_blocks=self.grid_blocks,
+            order=self.order,
         )
 
     def compute_device(self) -> torch.device:
@@ -262,6 +270,14 @@ class B200Dopri5Solver:
             y0_dev = y0.detach().to(dev, non_blocking=False).contiguous()
             params_dev = torch.as_tensor(np.ascontiguousarray(p_rows), device=dev)
             save_dev = save_f64.to(dev)
+            order = None
+            if self.order == "morton" and B > 1:
+                ic_order = spatial_order(y0_dev)
+                if params is not None:
+                    order = (ic_order.to(torch.int64)[:, None] * P + torch.arange(P, device=dev)).reshape(-1)
+                    order = order.to(torch.int32)
+                else:
+                    order = ic_order
             req = SolveRequest(
                 system=spec.system,
                 dim=S,
@@ -284,6 +300,7 @@ class B200Dopri5Solver:
                 out_dtype=y0.dtype,
                 block_size=self.block_size,
                 grid_blocks=self.grid_blocks,
+                order=order,
             )
             res = solve(req, stream)
             if full:
