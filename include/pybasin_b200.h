@@ -140,16 +140,28 @@ typedef struct pb_solve_args {
     int32_t _pad2;
     int64_t* steps_out;      /* (n_traj) attempted steps */
     /* scratch (device) */
-    unsigned long long* queue_counter; /* QUEUE schedule: one zero-initialised counter
-                                          (the call resets it on `stream`) */
-    float* median_scratch;   /* (n_traj, n_median_states, n_save - win_begin) when any
-                                PB_FEAT_MEDIAN column is requested, else NULL */
+    unsigned long long* queue_counter; /* QUEUE schedule: one counter (the call resets it on `stream`) */
+    void* scratch;           /* pb_solve_scratch_bytes(args) bytes, 256-byte aligned; NULL when that is 0 */
     /* processing order (device, optional): queue position q integrates trajectory
        order[q], a permutation of [0, n_traj).  Ordering ICs along a space-filling
        curve puts trajectories with similar dynamics (and step counts) in the same
        warp.  Outputs stay indexed by trajectory. */
     const int32_t* order;
+    int32_t dense_mode;      /* pb_dense_mode */
+    int32_t window_record_cap; /* PB_DENSE_DEFERRED: step records per trajectory (0 = default) */
 } pb_solve_args;
+
+/* Where the save points of the feature window are evaluated. */
+typedef enum {
+    PB_DENSE_INLINE = 0,   /* by the integrating thread, right after each accepted step */
+    PB_DENSE_DEFERRED = 1  /* two passes: the integrator writes one record (step start, step
+                              size, interpolation coefficients of the feature states) per window
+                              step that holds save points; a sampling kernel then evaluates all
+                              save points of a trajectory across the lanes of one warp.  A
+                              trajectory whose window needs more than window_record_cap records
+                              is integrated again with the inline path.  Not combinable with
+                              y_full_out (which uses the inline path). */
+} pb_dense_mode;
 
 /* Integrate n_traj trajectories with adaptive Dormand-Prince 5(4) and write the
  * fused window features, statuses and (optionally) states.  Asynchronous on
@@ -158,7 +170,9 @@ typedef struct pb_solve_args {
  * src/pybasin/ts_torch/calculators/torch_features_statistical.py. */
 int pb_solve_batch(const pb_solve_args* args, void* stream);
 
-/* Device bytes of scratch pb_solve_batch needs for `args` (median window). */
+/* Device bytes of `scratch` that pb_solve_batch needs for `args`: the median
+ * windows (n_traj x median columns x window length floats) and, in
+ * PB_DENSE_DEFERRED mode, the step records and per-trajectory record counts. */
 int64_t pb_solve_scratch_bytes(const pb_solve_args* args);
 
 /* 1-NN labelling on the device (Euclidean, the reference's

@@ -40,6 +40,9 @@ LAYOUT_INDEXED = 2
 SCHED_PLAIN = 0
 SCHED_QUEUE = 1
 
+DENSE_INLINE = 0
+DENSE_DEFERRED = 1
+
 DTYPE_F32 = 0
 DTYPE_F64 = 1
 
@@ -118,8 +121,10 @@ class SolveArgs(ctypes.Structure):
         ("_pad2", _c_i32),
         ("steps_out", _c_vp),
         ("queue_counter", _c_vp),
-        ("median_scratch", _c_vp),
+        ("scratch", _c_vp),
         ("order", _c_vp),
+        ("dense_mode", _c_i32),
+        ("window_record_cap", _c_i32),
     ]
 
 

@@ -4,7 +4,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
-#include "pb_dopri5.cuh"
+#include "pb_sample.cuh"
 #include "pybasin_b200.h"
 
 namespace pb {
@@ -150,23 +150,35 @@ __global__ void __launch_bounds__(256) k_probe_fma(int iters, float* __restrict_
 // ---------------------------------------------------------------------------
 // kernel selection
 // ---------------------------------------------------------------------------
-using kernel_fn = void (*)(const pb_solve_args);
+using plain_fn = void (*)(const pb_solve_args);
+using queue_fn = void (*)(const pb_solve_args, int);
 
 struct KernelSel {
-    kernel_fn fn = nullptr;
-    int smem_per_thread = 0;  // dynamic shared memory: per-thread statistics slot
+    plain_fn plain = nullptr;        // inline dense output, one thread per trajectory
+    plain_fn plain_defer = nullptr;  // deferred pass 1
+    queue_fn queue = nullptr;        // inline dense output, persistent warps (also the redo pass)
+    queue_fn queue_defer = nullptr;  // deferred pass 1, persistent warps
+    plain_fn sample = nullptr;       // deferred pass 2
+    int smem_per_thread = 0;         // inline kernels: per-thread statistics slot
 };
 
-template <class Sys>
-KernelSel select_kernel(int precision, int schedule)
+template <class Sys, class R>
+KernelSel select_prec()
 {
     KernelSel k;
     k.smem_per_thread = Stats<Sys::S>::kBytesPerThread;
-    if (precision == PB_PREC_FP64)
-        k.fn = schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, double> : k_solve_plain<Sys, double>;
-    else
-        k.fn = schedule == PB_SCHED_QUEUE ? k_solve_queue<Sys, float> : k_solve_plain<Sys, float>;
+    k.plain = k_solve_plain<Sys, R, false>;
+    k.plain_defer = k_solve_plain<Sys, R, true>;
+    k.queue = k_solve_queue<Sys, R, false>;
+    k.queue_defer = k_solve_queue<Sys, R, true>;
+    k.sample = k_sample<R, Sys::S>;
     return k;
+}
+
+template <class Sys>
+KernelSel select_kernel(int precision)
+{
+    return precision == PB_PREC_FP64 ? select_prec<Sys, double>() : select_prec<Sys, float>();
 }
 
 static KernelSel find_kernel(int system, int dim, int precision, int schedule)
@@ -176,27 +188,45 @@ static KernelSel find_kernel(int system, int dim, int precision, int schedule)
     switch (system) {
         case PB_SYS_LINEAR:
             switch (dim) {
-                case 1: return select_kernel<SysLinear<1>>(precision, schedule);
-                case 2: return select_kernel<SysLinear<2>>(precision, schedule);
-                case 3: return select_kernel<SysLinear<3>>(precision, schedule);
-                case 4: return select_kernel<SysLinear<4>>(precision, schedule);
+                case 1: return select_kernel<SysLinear<1>>(precision);
+                case 2: return select_kernel<SysLinear<2>>(precision);
+                case 3: return select_kernel<SysLinear<3>>(precision);
+                case 4: return select_kernel<SysLinear<4>>(precision);
                 default: return {};
             }
-        case PB_SYS_PENDULUM: return dim == 2 ? select_kernel<SysPendulum>(precision, schedule) : KernelSel{};
-        case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision, schedule) : KernelSel{};
-        case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision, schedule) : KernelSel{};
-        case PB_SYS_LORENZ_MASKED:
-            return dim == 3 ? select_kernel<SysLorenz<true>>(precision, schedule) : KernelSel{};
+        case PB_SYS_PENDULUM: return dim == 2 ? select_kernel<SysPendulum>(precision) : KernelSel{};
+        case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision) : KernelSel{};
+        case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision) : KernelSel{};
+        case PB_SYS_LORENZ_MASKED: return dim == 3 ? select_kernel<SysLorenz<true>>(precision) : KernelSel{};
         default: return {};
     }
 }
 
 // Dynamic shared memory above the 48 KB default needs an opt-in per kernel.
-static cudaError_t prepare_smem(const KernelSel& k, int block)
+template <class F>
+static cudaError_t prepare_smem(F fn, int bytes)
 {
-    const int bytes = k.smem_per_thread * block;
     if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// Persistent grid for a queue kernel: resident blocks on every SM, capped by the work.
+template <class F>
+static cudaError_t persistent_grid(F fn, int block, int smem, int64_t n_traj, int requested, int64_t* grid)
+{
+    if (requested > 0) {
+        *grid = requested;
+    } else {
+        int dev = 0, sms = 0, bps = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, block, smem);
+        if (e != cudaSuccess) return e;
+        *grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
+    }
+    const int64_t need = (n_traj + block - 1) / block;
+    if (*grid > need) *grid = need;
+    return cudaSuccess;
 }
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
@@ -240,7 +270,10 @@ static int validate(const pb_solve_args* a)
     }
     if (n_cross > PB_MAX_CROSSING) return PB_EUNSUPPORTED;
     if (a->n_features > 0 && !a->features_out) return PB_EINVAL;
-    if (count_median_cols(*a, nullptr) > 0 && !a->median_scratch) return PB_EINVAL;
+    if (a->dense_mode != PB_DENSE_INLINE && a->dense_mode != PB_DENSE_DEFERRED) return PB_EINVAL;
+    if (a->window_record_cap < 0) return PB_EINVAL;
+    for (int c = 0; c < a->n_features; ++c)
+        if (a->feat_state[c] >= PB_MAX_STAT_STATES) return PB_EUNSUPPORTED;
     switch (a->layout) {
         case PB_LAYOUT_SINGLE:
             if (a->n_ic < a->n_traj || a->n_param_rows < 1) return PB_EINVAL;
@@ -284,24 +317,27 @@ const char* pb_error_string(int32_t s)
 
 int64_t pb_solve_scratch_bytes(const pb_solve_args* a)
 {
-    if (!a) return -1;
-    const int m = count_median_cols(*a, nullptr);
-    if (m == 0) return 0;
-    return static_cast<int64_t>(a->n_traj) * m * (a->n_save - a->win_begin) * static_cast<int64_t>(sizeof(float));
+    if (!a || a->n_traj < 0 || a->n_save < 1 || a->win_begin < 0 || a->win_begin >= a->n_save) return -1;
+    return scratch_layout(*a).total;
 }
 
 int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule, int32_t block_size,
                        int32_t* blocks_per_sm, int32_t* num_sms)
 {
     KernelSel k = find_kernel(system, dim, precision, schedule);
-    if (!k.fn) return PB_EINVALID_ODE;
+    if (!k.plain) return PB_EINVALID_ODE;
     if (block_size <= 0 || block_size % 32 || block_size > 256) return PB_EINVAL;
     int dev = 0, bps = 0, sms = 0;
+    const int smem = k.smem_per_thread * block_size;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = prepare_smem(k, block_size);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, block_size, k.smem_per_thread * block_size);
+    if (schedule == PB_SCHED_QUEUE) {
+        if (e == cudaSuccess) e = prepare_smem(k.queue, smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.queue, block_size, smem);
+    } else {
+        if (e == cudaSuccess) e = prepare_smem(k.plain, smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.plain, block_size, smem);
+    }
     if (e != cudaSuccess) return map_cuda(e);
     if (blocks_per_sm) *blocks_per_sm = bps;
     if (num_sms) *num_sms = sms;
@@ -314,34 +350,56 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
     if (v != PB_SUCCESS) return v;
     const pb_solve_args& a = *args;
     KernelSel k = find_kernel(a.system, a.dim, a.precision, a.schedule);
-    if (!k.fn) return PB_EINVALID_ODE;
+    if (!k.plain) return PB_EINVALID_ODE;
     if (a.n_traj == 0) return PB_SUCCESS;
+    const ScratchLayout sl = scratch_layout(a);
+    if (sl.total > 0 && !a.scratch) return PB_EINVAL;
+    if (sl.deferred && !a.queue_counter) return PB_EINVAL;  // the redo pass runs on the queue
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int block = a.block_size > 0 ? a.block_size : 128;
     const int smem = k.smem_per_thread * block;
-    cudaError_t e = prepare_smem(k, block);
-    if (e != cudaSuccess) return map_cuda(e);
-    int64_t grid;
-    if (a.schedule == PB_SCHED_QUEUE) {
-        if (a.grid_blocks > 0) {
-            grid = a.grid_blocks;
-        } else {
-            int dev = 0, sms = 0, bps = 0;
-            e = cudaGetDevice(&dev);
-            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, block, smem);
+    cudaError_t e = cudaSuccess;
+    const int64_t plain_grid = (a.n_traj + block - 1) / block;
+    if (plain_grid > 0x7fffffffLL) return PB_EINVAL;
+
+    if (sl.deferred) {
+        // pass 1: integrate, one record per window step holding save points
+        if (a.schedule == PB_SCHED_QUEUE) {
+            int64_t grid = 0;
+            e = persistent_grid(k.queue_defer, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
             if (e != cudaSuccess) return map_cuda(e);
-            grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
+            k.queue_defer<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
+        } else {
+            k.plain_defer<<<static_cast<unsigned>(plain_grid), block, 0, st>>>(a);
         }
-        const int64_t need = (a.n_traj + block - 1) / block;
-        if (grid > need) grid = need;
-        e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        e = cudaGetLastError();
         if (e != cudaSuccess) return map_cuda(e);
+        // pass 2: one warp per trajectory evaluates its save points and reduces the statistics
+        const int64_t sblocks = (a.n_traj + 7) / 8;
+        if (sblocks > 0x7fffffffLL) return PB_EINVAL;
+        k.sample<<<static_cast<unsigned>(sblocks), 256, 0, st>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return map_cuda(e);
+        // pass 3: trajectories that exceeded the record capacity, inline
+        int64_t grid = 0;
+        e = prepare_smem(k.queue, smem);
+        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return map_cuda(e);
+        k.queue<<<static_cast<unsigned>(grid), block, smem, st>>>(a, 1);
+    } else if (a.schedule == PB_SCHED_QUEUE) {
+        int64_t grid = 0;
+        e = prepare_smem(k.queue, smem);
+        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return map_cuda(e);
+        k.queue<<<static_cast<unsigned>(grid), block, smem, st>>>(a, 0);
     } else {
-        grid = (a.n_traj + block - 1) / block;
+        e = prepare_smem(k.plain, smem);
+        if (e != cudaSuccess) return map_cuda(e);
+        k.plain<<<static_cast<unsigned>(plain_grid), block, smem, st>>>(a);
     }
-    if (grid > 0x7fffffffLL) return PB_EINVAL;
-    k.fn<<<static_cast<unsigned>(grid), block, smem, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return map_cuda(e);
     MedianPlan plan;
@@ -349,8 +407,9 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
         const int64_t rows = a.n_traj * plan.n_med;
         const int64_t blocks = (rows + 7) / 8;
         if (blocks > 0x7fffffffLL) return PB_EINVAL;
-        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(a.median_scratch, a.n_traj, a.n_save - a.win_begin,
-                                                               plan, a.features_out, a.n_features);
+        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
+            reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), a.n_traj,
+            a.n_save - a.win_begin, plan, a.features_out, a.n_features);
         e = cudaGetLastError();
         if (e != cudaSuccess) return map_cuda(e);
     }

@@ -32,6 +32,7 @@
 #include <type_traits>
 
 #include "pb_rhs.cuh"
+#include "pb_scratch.cuh"
 #include "pybasin_b200.h"
 
 namespace pb {
@@ -79,9 +80,13 @@ struct Plan {
     int n_cross;
     int n_med;
     unsigned stat_mask;  // states that any feature column reads
+    int ns;              // number of such states ("slots", in state order)
+    int stat_state[PB_MAX_STAT_STATES];
+    int slot_of[PB_MAX_STAT_STATES];
     int cross_state[PB_MAX_CROSSING];
     double cross_level[PB_MAX_CROSSING];
     int med_state[PB_MAX_FEATURES];
+    ScratchLayout sl;
 };
 
 __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
@@ -101,6 +106,16 @@ __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
     pl.n_cross = nc;
     pl.n_med = nm;
     pl.stat_mask = mask;
+    int ns = 0;
+    for (int st = 0; st < PB_MAX_STAT_STATES; ++st) {
+        pl.slot_of[st] = -1;
+        if ((mask >> st) & 1u) {
+            pl.slot_of[st] = ns;
+            pl.stat_state[ns++] = st;
+        }
+    }
+    pl.ns = ns;
+    pl.sl = scratch_layout(a);
 }
 
 // Per-thread window statistics in shared memory, structure-of-arrays
@@ -153,6 +168,7 @@ struct Lane {
     int si;            // next save index
     int steps;
     int status;
+    int nrec;          // deferred dense output: records written (-1 = capacity exceeded)
 };
 
 __device__ __forceinline__ double load_save(const pb_solve_args& a, int si)
@@ -216,7 +232,7 @@ struct Integrator {
                     flg = (flg & ~(1 << (8 + j))) | (static_cast<int>(above) << (8 + j));
                 }
                 for (int m = 0; m < pl.n_med; ++m)
-                    a.median_scratch[(traj * pl.n_med + m) * nwin + (L.si - a.win_begin)] =
+                    median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (L.si - a.win_begin)] =
                         static_cast<float>(pick(v, pl.med_state[m]));
                 ++cnt;
             }
@@ -281,7 +297,8 @@ struct Integrator {
         L.status = bad_row ? PB_TRAJ_BAD_INPUT : PB_TRAJ_OK;
         L.si = a.y_full_out ? 0 : a.win_begin;
         L.next_save = load_save(a, L.si);
-        st.reset();
+        L.nrec = 0;
+        if (st.d) st.reset();
 
         // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
         if (MIXED) {
@@ -321,6 +338,45 @@ struct Integrator {
         L.dt = fmin(100.0 * h0, h1);
     }
 
+    // ---- deferred dense output: one record per accepted window step holding save
+    // points (step start, step size, first covered save, count, and for each
+    // statistics state y, h*k1 and the three higher polynomial coefficients)
+    __device__ static bool write_record(L_t& L, const Plan& pl, int64_t traj, const pb_solve_args& a, double t,
+                                        double dt, R h, const R (&ia)[S], const R (&ib)[S], const R (&icf)[S],
+                                        double tn)
+    {
+        if (L.nrec >= pl.sl.cap) return false;
+        unsigned char* rec = record_ptr(a, pl.sl, traj, L.nrec);
+        double* hd = reinterpret_cast<double*>(rec);
+        hd[0] = t;
+        hd[1] = dt;
+        int si = L.si;
+        double ts = L.next_save;
+        while (si < a.n_save && ts <= tn + dp::save_slack) {
+            ++si;
+            ts = load_save(a, si);
+        }
+        int* hi = reinterpret_cast<int*>(rec + 16);
+        hi[0] = L.si;
+        hi[1] = si - L.si;
+        R* c = reinterpret_cast<R*>(rec + kRecordHeader);
+        int j = 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (!((pl.stat_mask >> s) & 1)) continue;
+            c[5 * j + 0] = L.y[s];
+            c[5 * j + 1] = h * L.k1[s];
+            c[5 * j + 2] = icf[s];
+            c[5 * j + 3] = ib[s];
+            c[5 * j + 4] = ia[s];
+            ++j;
+        }
+        L.si = si;
+        L.next_save = ts;
+        L.nrec++;
+        return true;
+    }
+
     template <class TB>
     __device__ __forceinline__ static void stages(const TB& tb, const L_t& L, R h, R (&k2)[S], R (&k3)[S],
                                                   R (&k4)[S], R (&k5)[S], R (&k6)[S], R (&k7)[S], R (&d)[S],
@@ -357,6 +413,7 @@ struct Integrator {
     }
 
     // ---- one attempted step; returns true once the trajectory is finished
+    template <bool DEFER>
     __device__ static bool step(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
     {
         if (!(L.t < a.t1) || L.steps >= a.max_steps) return true;
@@ -429,6 +486,12 @@ struct Integrator {
                 ib[s] = h * (R(5) * L.k1[s] - R(3) * k7[s]) + R(18) * L.y[s] + R(14) * yn[s] - R(32) * ym;
                 icf[s] = h * (k7[s] - R(4) * L.k1[s]) - R(11) * L.y[s] - R(5) * yn[s] + R(16) * ym;
             }
+            if (DEFER) {
+                if (!write_record(L, pl, traj, a, t, dt, h, ia, ib, icf, tn)) {
+                    L.nrec = -1;  // capacity exceeded: the inline pass integrates it again
+                    return true;
+                }
+            } else {
             const double inv_dt = 1.0 / dt;
             record_run(L, st, pl, traj, a, tn, [&](double ts, R (&v)[S]) {
                 if (ts <= t + dp::save_slack) {
@@ -441,6 +504,7 @@ struct Integrator {
                         v[s] = L.y[s] + x * (h * L.k1[s] + x * (icf[s] + x * (ib[s] + x * ia[s])));
                 }
             });
+            }
         }
         if (accept) {
             if (MIXED) {
@@ -486,9 +550,23 @@ struct Integrator {
     }
 
     // ---- tail fill, features, status and states of a finished trajectory
+    template <bool DEFER>
     __device__ static void finish(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
     {
         if (L.status == PB_TRAJ_OK && L.t < a.t1 && L.steps >= a.max_steps) L.status = PB_TRAJ_MAX_STEPS;
+        if (DEFER) {
+            // the sampling pass evaluates the records and fills the uncovered tail
+            unsigned char* tl = tail_ptr(a, pl.sl, traj);
+            int* ti = reinterpret_cast<int*>(tl);
+            ti[0] = L.nrec;
+            ti[1] = L.si;
+            ti[2] = L.status;
+            double* fillv = reinterpret_cast<double*>(tl + 16);
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                fillv[s] = (L.status == PB_TRAJ_UNBOUNDED) ? CUDART_INF : static_cast<double>(L.y[s]);
+            if (L.nrec < 0) return;  // the inline pass writes this trajectory's outputs
+        } else {
         R fill[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) fill[s] = (L.status == PB_TRAJ_UNBOUNDED) ? R(CUDART_INF) : L.y[s];
@@ -534,6 +612,7 @@ struct Integrator {
                 a.features_out[traj * a.n_features + c] = v;
             }
         }
+        }
         if (a.status_out) a.status_out[traj] = L.status;
         if (a.steps_out) a.steps_out[traj] = L.steps;
         if (a.y_final_out) {
@@ -556,9 +635,16 @@ __device__ __forceinline__ int64_t traj_at(const pb_solve_args& a, int64_t q)
 }
 
 template <class Sys>
-__device__ __forceinline__ Stats<Sys::S> stats_slot(unsigned char* smem)
+__device__ __forceinline__ Stats<Sys::S> stats_slot(unsigned char* smem, bool with_stats)
 {
     Stats<Sys::S> st;
+    if (!with_stats) {
+        st.d = nullptr;
+        st.i = nullptr;
+        st.nthr = 0;
+        st.tid = 0;
+        return st;
+    }
     st.nthr = blockDim.x;
     st.tid = threadIdx.x;
     st.d = reinterpret_cast<double*>(smem);
@@ -567,8 +653,8 @@ __device__ __forceinline__ Stats<Sys::S> stats_slot(unsigned char* smem)
 }
 
 // Plain schedule: one thread per trajectory, no queue (the FP64 baseline when
-// R = double).
-template <class Sys, class R>
+// R = double).  DEFER selects the first pass of the deferred dense output.
+template <class Sys, class R, bool DEFER>
 __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -579,22 +665,24 @@ __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
     const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= a.n_traj) return;
     const int64_t traj = traj_at(a, q);
-    auto st = stats_slot<Sys>(smem);
+    auto st = stats_slot<Sys>(smem, !DEFER);
     typename I::L_t L;
     I::begin(L, st, traj, a);
-    while (!I::step(L, st, pl, traj, a)) {
+    while (!I::template step<DEFER>(L, st, pl, traj, a)) {
     }
-    I::finish(L, st, pl, traj, a);
+    I::template finish<DEFER>(L, st, pl, traj, a);
 }
 
 // Queue schedule: persistent warps take 32 consecutive queue positions at a time
 // (one atomicAdd per warp) and come back for the next 32 once all their lanes
 // are done.  Taking whole warps keeps the lanes of a warp on neighbouring
 // positions of the processing order (spatially coherent ICs), which a per-lane
-// refill would scatter.  Every loop is bounded: each trajectory runs at most
-// max_steps attempted steps and the queue holds n_traj entries.
-template <class Sys, class R>
-__global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
+// refill would scatter.  With `redo_only`, only trajectories whose deferred
+// records overflowed are integrated (inline).  Every loop is bounded: each
+// trajectory runs at most max_steps attempted steps and the queue holds n_traj
+// entries.
+template <class Sys, class R, bool DEFER>
+__global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int redo_only)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Plan pl;
@@ -602,7 +690,7 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
     __syncthreads();
     using I = Integrator<Sys, R>;
     const int lane = threadIdx.x & 31;
-    auto st = stats_slot<Sys>(smem);
+    auto st = stats_slot<Sys>(smem, !DEFER);
     while (true) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.queue_counter, 32ull);
@@ -611,11 +699,14 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a)
         const int64_t q = static_cast<int64_t>(base) + lane;
         if (q < a.n_traj) {
             const int64_t traj = traj_at(a, q);
-            typename I::L_t L;
-            I::begin(L, st, traj, a);
-            while (!I::step(L, st, pl, traj, a)) {
+            const bool skip = redo_only && reinterpret_cast<const int*>(tail_ptr(a, pl.sl, traj))[0] >= 0;
+            if (!skip) {
+                typename I::L_t L;
+                I::begin(L, st, traj, a);
+                while (!I::template step<DEFER>(L, st, pl, traj, a)) {
+                }
+                I::template finish<DEFER>(L, st, pl, traj, a);
             }
-            I::finish(L, st, pl, traj, a);
         }
         __syncwarp();
     }

@@ -53,6 +53,8 @@ class SolveRequest:
     block_size: int = 0
     grid_blocks: int = 0
     order: torch.Tensor | None = None  # (n_traj,) int32 processing order
+    dense_mode: int = L.DENSE_DEFERRED
+    window_record_cap: int = 0
 
 
 @dataclass
@@ -76,7 +78,9 @@ def _dtype_code(dt: torch.dtype) -> int:
     raise TypeError(f"unsupported dtype {dt}; expected float32 or float64")
 
 
-def build_args(req: SolveRequest, out: SolveResult, queue: torch.Tensor | None, median: torch.Tensor | None) -> L.SolveArgs:
+def build_args(
+    req: SolveRequest, out: SolveResult, queue: torch.Tensor | None, scratch: torch.Tensor | None
+) -> L.SolveArgs:
     a = L.SolveArgs()
     n_traj = req.n_traj if req.n_traj is not None else _default_n_traj(req)
     a.system = req.system
@@ -117,9 +121,32 @@ def build_args(req: SolveRequest, out: SolveResult, queue: torch.Tensor | None, 
     a.y_out_dtype = _dtype_code(req.out_dtype)
     a.steps_out = _ptr(out.steps)
     a.queue_counter = _ptr(queue)
-    a.median_scratch = _ptr(median)
+    a.scratch = _ptr(scratch)
     a.order = _ptr(req.order)
+    a.dense_mode = req.dense_mode
+    a.window_record_cap = req.window_record_cap
     return a
+
+
+def scratch_bytes(args: L.SolveArgs) -> int:
+    """Device scratch ``pb_solve_batch`` needs for ``args`` (median windows, step records)."""
+    n = L.load().pb_solve_scratch_bytes(ctypes.byref(args))
+    if n < 0:
+        raise ValueError("invalid solve arguments")
+    return int(n)
+
+
+def alloc_scratch(args: L.SolveArgs, device: torch.device) -> torch.Tensor | None:
+    """Allocate (and attach to ``args``) the scratch buffer, 256-byte aligned."""
+    n = scratch_bytes(args)
+    if n == 0:
+        args.scratch = None
+        return None
+    buf = torch.empty((n + 256,), dtype=torch.uint8, device=device)
+    off = (-buf.data_ptr()) % 256
+    view = buf[off : off + n]
+    args.scratch = view.data_ptr()
+    return view
 
 
 def _default_n_traj(req: SolveRequest) -> int:
@@ -146,20 +173,15 @@ def solve(req: SolveRequest, stream: torch.cuda.Stream | None = None) -> SolveRe
         else None,
         steps=torch.empty((n_traj,), dtype=torch.int64, device=dev) if req.keep_steps else None,
     )
-    queue = torch.zeros((1,), dtype=torch.int64, device=dev) if req.schedule == L.SCHED_QUEUE else None
-    args = build_args(req, out, queue, None)
-    nbytes = lib.pb_solve_scratch_bytes(ctypes.byref(args))
-    median = None
-    if nbytes > 0:
-        median = torch.empty((nbytes // 4,), dtype=torch.float32, device=dev)
-        args.median_scratch = median.data_ptr()
     s = stream if stream is not None else torch.cuda.current_stream(dev)
+    with torch.cuda.stream(s):
+        queue = torch.zeros((1,), dtype=torch.int64, device=dev)
+        args = build_args(req, out, queue, None)
+        scratch = alloc_scratch(args, dev)
     L.check(lib.pb_solve_batch(ctypes.byref(args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
-    # keep scratch alive until the kernels using it are done
-    if queue is not None:
-        queue.record_stream(s)
-    if median is not None:
-        median.record_stream(s)
+    # the scratch was allocated on `s`, so the caching allocator keeps it until the
+    # kernels queued there before its release have run
+    del scratch, queue
     return out
 
 

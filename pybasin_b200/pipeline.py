@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import SolveRequest, SolveResult, build_args, spatial_order
+from pybasin_b200.engine import SolveRequest, SolveResult, alloc_scratch, build_args, spatial_order
 from pybasin_b200.odes import resolve_system
 from pybasin_b200.solver import B200Dopri5Solver
 
@@ -124,9 +124,7 @@ class BasinStabilityPipeline:
             order=self.order if self.solver.order == "morton" else None,
         )
         self.args = build_args(req, self.out, self.queue, None)
-        lib = L.load()
-        if lib.pb_solve_scratch_bytes(ctypes.byref(self.args)) > 0:
-            raise ValueError("median is not supported in the pipeline (needs per-trajectory scratch)")
+        self.scratch = alloc_scratch(self.args, dev)
         self._n = n
         self._graph = None
 

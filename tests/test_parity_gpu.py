@@ -55,6 +55,8 @@ def gpu_solve(
     y0_dtype=torch.float64,
     block_size: int = 0,
     grid_blocks: int = 0,
+    dense_mode: int = L.DENSE_DEFERRED,
+    window_record_cap: int = 0,
 ):
     y0_t = torch.as_tensor(np.ascontiguousarray(y0), dtype=y0_dtype, device=DEV)
     p_t = torch.as_tensor(np.ascontiguousarray(np.atleast_2d(params)), dtype=torch.float64, device=DEV)
@@ -83,6 +85,8 @@ def gpu_solve(
         keep_steps=True,
         block_size=block_size,
         grid_blocks=grid_blocks,
+        dense_mode=dense_mode,
+        window_record_cap=window_record_cap,
     )
     r = solve(req)
     torch.cuda.synchronize()
@@ -154,8 +158,12 @@ def test_cross_layout_matches_oracle_expansion():
 ALL_FEATS = [(s, k, 0.0) for s in range(2) for k in range(0, 11)] + [(0, 11, 0.0), (1, 11, 0.5), (1, 12, 0.0)]
 
 
+DENSE = pytest.mark.parametrize("dense", [L.DENSE_INLINE, L.DENSE_DEFERRED], ids=["inline", "deferred"])
+
+
+@DENSE
 @pytest.mark.parametrize("case", [PENDULUM, DUFFING], ids=lambda c: c.name)
-def test_all_fused_features_match_oracle(case):
+def test_all_fused_features_match_oracle(case, dense):
     y0 = seeded_ics(case, 300, seed=11).double().numpy()
     save = case.save_ts().numpy()
     t_span = (0.0, float(save[-1]))
@@ -163,7 +171,7 @@ def test_all_fused_features_match_oracle(case):
     want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, t_span, 1e-8, 1e-6, win_begin=wb,
                          features=ALL_FEATS)
     got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, 1e-8, 1e-6, win_begin=wb,
-                    features=ALL_FEATS)
+                    features=ALL_FEATS, dense_mode=dense)
     ok = (got["status"] == 0) & (want["status"] == 0)
     assert ok.all()
     # compare on trajectories whose final states agree (away from basin boundaries)
@@ -175,7 +183,9 @@ def test_all_fused_features_match_oracle(case):
     np.testing.assert_allclose(got["features"][same], want["features"][same], rtol=2e-4, atol=1e-6)
 
 
-def test_median_and_crossings_exact_on_identical_windows():
+@DENSE
+@pytest.mark.parametrize("cap", [0, 3])
+def test_median_and_crossings_exact_on_identical_windows(dense, cap):
     """Median and crossing counts are order statistics: on short horizons where the
     kernel and oracle windows agree to ~1e-12 they must be equal."""
     y0 = seeded_ics(PENDULUM, 64, seed=2).double().numpy()
@@ -184,7 +194,7 @@ def test_median_and_crossings_exact_on_identical_windows():
     want = O.solve_batch(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0.0, 20.0), 1e-10, 1e-10,
                          win_begin=100, features=feats)
     got = gpu_solve(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0.0, 20.0), 1e-10, 1e-10,
-                    win_begin=100, features=feats)
+                    win_begin=100, features=feats, dense_mode=dense, window_record_cap=cap)
     np.testing.assert_allclose(got["features"][:, :2], want["features"][:, :2], rtol=1e-6, atol=1e-7)
     np.testing.assert_array_equal(got["features"][:, 2:], want["features"][:, 2:])
 
@@ -264,9 +274,10 @@ def test_label_nearest_matches_sklearn():
 # ---------------------------------------------------------------------------
 # edge cases: ragged sizes, statuses, failure paths
 # ---------------------------------------------------------------------------
+@DENSE
 @pytest.mark.parametrize("n", [1, 31, 33, 4097])
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
-def test_ragged_batch_sizes_queue(n, precision):
+def test_ragged_batch_sizes_queue(n, precision, dense):
     y0 = seeded_ics(PENDULUM, n, seed=9).double().numpy()
     save = np.linspace(0.0, 20.0, 41)
     feats = [(1, 1, 0.0), (0, 5, 0.0)]
@@ -274,7 +285,7 @@ def test_ragged_batch_sizes_queue(n, precision):
                          features=feats)
     if precision == L.PREC_FP64:
         got = gpu_solve(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0, 20), 1e-8, 1e-8, win_begin=20,
-                        features=feats, precision=precision, grid_blocks=3, block_size=64)
+                        features=feats, precision=precision, grid_blocks=3, block_size=64, dense_mode=dense)
         np.testing.assert_allclose(got["features"], want["features"], rtol=1e-7, atol=1e-7)
     else:
         # FP32 stages at their own tolerance (1e-6) against the oracle at the same tolerance;
@@ -283,7 +294,7 @@ def test_ragged_batch_sizes_queue(n, precision):
         want = O.solve_batch(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0, 20), 1e-6, 1e-8,
                              win_begin=20, features=feats)
         got = gpu_solve(O.SYS_PENDULUM, y0, np.array([PENDULUM.params]), save, (0, 20), 1e-6, 1e-8, win_begin=20,
-                        features=feats, precision=precision, grid_blocks=3, block_size=64)
+                        features=feats, precision=precision, grid_blocks=3, block_size=64, dense_mode=dense)
         close = np.isclose(got["features"], want["features"], rtol=1e-3, atol=1e-3)
         assert close.mean() >= 0.995
 
