@@ -346,31 +346,55 @@ struct Integrator {
                                         double tn)
     {
         if (L.nrec >= pl.sl.cap) return false;
-        unsigned char* rec = record_ptr(a, pl.sl, traj, L.nrec);
-        double* hd = reinterpret_cast<double*>(rec);
-        hd[0] = t;
-        hd[1] = dt;
         int si = L.si;
         double ts = L.next_save;
         while (si < a.n_save && ts <= tn + dp::save_slack) {
             ++si;
             ts = load_save(a, si);
         }
-        int* hi = reinterpret_cast<int*>(rec + 16);
-        hi[0] = L.si;
-        hi[1] = si - L.si;
-        R* c = reinterpret_cast<R*>(rec + kRecordHeader);
+        // assemble the record as 32-bit words, then store it with 16-byte vector stores
+        constexpr int RW = sizeof(R) / 4;
+        constexpr int kWords = (kRecordHeader + 5 * S * static_cast<int>(sizeof(R)) + 8 + 15) / 16 * 4;
+        unsigned w[kWords];
+#pragma unroll
+        for (int q = 0; q < kWords; ++q) w[q] = 0u;
+        w[0] = __double2loint(t);
+        w[1] = __double2hiint(t);
+        w[2] = __double2loint(dt);
+        w[3] = __double2hiint(dt);
         int j = 0;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             if (!((pl.stat_mask >> s) & 1)) continue;
-            c[5 * j + 0] = L.y[s];
-            c[5 * j + 1] = h * L.k1[s];
-            c[5 * j + 2] = icf[s];
-            c[5 * j + 3] = ib[s];
-            c[5 * j + 4] = ia[s];
+            const R vals[5] = {L.y[s], h * L.k1[s], icf[s], ib[s], ia[s]};
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const int base = 4 + (5 * j + q) * RW;
+                if (RW == 1) {
+                    const unsigned u = __float_as_uint(static_cast<float>(vals[q]));
+#pragma unroll
+                    for (int z = 0; z < kWords; ++z) w[z] = (z == base) ? u : w[z];
+                } else {
+                    const double dv = static_cast<double>(vals[q]);
+                    const unsigned lo = static_cast<unsigned>(__double2loint(dv));
+                    const unsigned hi = static_cast<unsigned>(__double2hiint(dv));
+#pragma unroll
+                    for (int z = 0; z < kWords; ++z) w[z] = (z == base) ? lo : ((z == base + 1) ? hi : w[z]);
+                }
+            }
             ++j;
         }
+        const int iw = 4 + 5 * pl.ns * RW;  // (first_save, n_saves)
+#pragma unroll
+        for (int z = 0; z < kWords; ++z) {
+            w[z] = (z == iw) ? static_cast<unsigned>(L.si) : w[z];
+            w[z] = (z == iw + 1) ? static_cast<unsigned>(si - L.si) : w[z];
+        }
+        uint4* dst = reinterpret_cast<uint4*>(record_ptr(a, pl.sl, traj, L.nrec));
+        const int n16 = pl.sl.rec_stride / 16;
+#pragma unroll
+        for (int z = 0; z < kWords / 4; ++z)
+            if (z < n16) dst[z] = make_uint4(w[4 * z], w[4 * z + 1], w[4 * z + 2], w[4 * z + 3]);
         L.si = si;
         L.next_save = ts;
         L.nrec++;

@@ -37,6 +37,65 @@ __device__ __forceinline__ double feature_value(int kind, double sh, double s1, 
     }
 }
 
+// Per-lane window statistics accumulated by the sampling pass.
+template <int S>
+struct SampleAcc {
+    double sh[S], s1[S], s2[S], mn[S], mx[S], last[S];
+    int nan_flags;
+    int cross_cnt[PB_MAX_CROSSING];
+    double carry[PB_MAX_CROSSING];  // previous sample of each crossing state (the one before lane 0's)
+    bool shift_set;
+};
+
+// Fold one batch of (up to 32) consecutive save points into the accumulators.
+// Lane l holds sample j = j0 + l (valid if l < nvalid).  Collective over the warp.
+template <int S>
+__device__ __forceinline__ void fold_samples(SampleAcc<S>& acc, const Plan& pl, const pb_solve_args& a, int64_t traj,
+                                             int64_t nwin, int j0, int nvalid, const double (&v)[S], int lane)
+{
+    const int ns = pl.ns;
+    const int j = j0 + lane;
+    const bool valid = lane < nvalid;
+    if (!acc.shift_set) {  // shift = first window sample (lane 0 of the first batch)
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            const double f = __shfl_sync(0xffffffffu, v[q], 0);
+            acc.sh[q] = isfinite(f) ? f : 0.0;
+        }
+        acc.shift_set = true;
+    }
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            if (q >= ns) continue;
+            const double d = v[q] - acc.sh[q];
+            acc.s1[q] += d;
+            acc.s2[q] = fma(d, d, acc.s2[q]);
+            acc.mn[q] = fmin(acc.mn[q], v[q]);
+            acc.mx[q] = fmax(acc.mx[q], v[q]);
+            if (v[q] != v[q]) acc.nan_flags |= 1 << q;
+            if (j == a.n_save - 1) acc.last[q] = v[q];
+        }
+        for (int m = 0; m < pl.n_med; ++m)
+            median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (j - a.win_begin)] =
+                static_cast<float>(pick(v, pl.slot_of[pl.med_state[m]]));
+    }
+    const int lastl = nvalid - 1;
+    for (int c = 0; c < pl.n_cross; ++c) {
+        const double cur = pick(v, pl.slot_of[pl.cross_state[c]]);
+        double prev = __shfl_up_sync(0xffffffffu, cur, 1);
+        if (lane == 0) prev = pick(acc.carry, c);
+        const bool changed = (cur > pl.cross_level[c]) != (prev > pl.cross_level[c]);
+        const int inc = (valid && j > a.win_begin && changed) ? 1 : 0;
+        const double nxt = __shfl_sync(0xffffffffu, cur, lastl);
+#pragma unroll
+        for (int q = 0; q < PB_MAX_CROSSING; ++q) {
+            acc.cross_cnt[q] += (q == c) ? inc : 0;
+            acc.carry[q] = (q == c) ? nxt : acc.carry[q];
+        }
+    }
+}
+
 template <class R, int S>
 __global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
 {
@@ -49,128 +108,109 @@ __global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
     const unsigned char* tl = tail_ptr(a, pl.sl, traj);
     const int nrec = reinterpret_cast<const int*>(tl)[0];
     if (nrec < 0) return;  // integrated again by the inline pass
+    const int si_end = reinterpret_cast<const int*>(tl)[1];
     const double* fill = reinterpret_cast<const double*>(tl + 16);
     const int ns = pl.ns;
     const int64_t nwin = a.n_save - a.win_begin;
+    const int iw = record_index_offset(ns, sizeof(R));
 
-    double sh[S], s1[S], s2[S], mn[S], mx[S], last[S];
+    SampleAcc<S> acc;
 #pragma unroll
-    for (int k = 0; k < S; ++k) {
-        sh[k] = 0.0;
-        s1[k] = 0.0;
-        s2[k] = 0.0;
-        mn[k] = CUDART_INF;
-        mx[k] = -CUDART_INF;
-        last[k] = 0.0;
+    for (int q = 0; q < S; ++q) {
+        acc.sh[q] = 0.0;
+        acc.s1[q] = 0.0;
+        acc.s2[q] = 0.0;
+        acc.mn[q] = CUDART_INF;
+        acc.mx[q] = -CUDART_INF;
+        acc.last[q] = 0.0;
     }
-    int nan_flags = 0;
-    int cross_cnt[PB_MAX_CROSSING] = {0, 0, 0, 0};
-    double carry[PB_MAX_CROSSING] = {0.0, 0.0, 0.0, 0.0};  // previous sample of each crossing state
+    acc.nan_flags = 0;
+#pragma unroll
+    for (int q = 0; q < PB_MAX_CROSSING; ++q) {
+        acc.cross_cnt[q] = 0;
+        acc.carry[q] = 0.0;
+    }
+    acc.shift_set = false;
 
-    int k = 0;           // record under this lane's save point
-    int loaded = -1;     // record whose data sits in registers
-    int rsi = 0, rns = 0;
-    double rt = 0.0, rdt = 1.0;
-    R co[5 * S];
-    if (nrec > 0) {
-        const int* hi = reinterpret_cast<const int*>(record_ptr(a, pl.sl, traj, 0) + 16);
-        rsi = hi[0];
-        rns = hi[1];
+    // records, 32 at a time: lane i holds record chunk+i (coalesced loads of
+    // consecutive records); the save points they cover are evaluated 32 at a time,
+    // each lane locating its record by a binary search over the lanes' first_save.
+    for (int chunk = 0; chunk < nrec; chunk += 32) {
+        const int k = chunk + lane;
+        const int hl = min(31, nrec - 1 - chunk);  // last lane holding a record
+        double rt = 0.0, rdt = 1.0;
+        R co[5 * S];
+        int rsi = 0x7fffffff, rn = 0;
+        if (k < nrec) {
+            const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
+            rt = reinterpret_cast<const double*>(rec)[0];
+            rdt = reinterpret_cast<const double*>(rec)[1];
+            const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
+#pragma unroll
+            for (int q = 0; q < 5 * S; ++q) {
+                co[q] = R(0);
+                if (q < 5 * ns) co[q] = c[q];
+            }
+            rsi = reinterpret_cast<const int*>(rec + iw)[0];
+            rn = reinterpret_cast<const int*>(rec + iw)[1];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5 * S; ++q) co[q] = R(0);
+        }
+        const int lo = __shfl_sync(0xffffffffu, rsi, 0);
+        const int hi = __shfl_sync(0xffffffffu, rsi + rn, hl);
+        for (int j0 = lo; j0 < hi; j0 += 32) {
+            const int j = j0 + lane;
+            const int nvalid = min(32, hi - j0);
+            // largest record lane r <= hl with first_save <= j
+            int r = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int cand = r + step;
+                const int sc = __shfl_sync(0xffffffffu, rsi, min(cand, 31));
+                if (cand <= hl && sc <= j) r = cand;
+            }
+            const double t_r = __shfl_sync(0xffffffffu, rt, r);
+            const double dt_r = __shfl_sync(0xffffffffu, rdt, r);
+            const double ts = lane < nvalid ? __ldg(a.save_ts + j) : t_r;
+            const R x = (ts <= t_r + dp::save_slack) ? R(0) : static_cast<R>((ts - t_r) / dt_r);
+            double v[S];
+#pragma unroll
+            for (int q = 0; q < S; ++q) {
+                R c5[5];
+#pragma unroll
+                for (int z = 0; z < 5; ++z) c5[z] = __shfl_sync(0xffffffffu, co[5 * q + z], r);
+                v[q] = static_cast<double>(c5[0] + x * (c5[1] + x * (c5[2] + x * (c5[3] + x * c5[4]))));
+            }
+            fold_samples(acc, pl, a, traj, nwin, j0, nvalid, v, lane);
+        }
     }
-    for (int64_t base = a.win_begin; base < a.n_save; base += 32) {
-        const int j = static_cast<int>(base) + lane;
-        const bool valid = j < a.n_save;
+    // save points after the last record: the trajectory stopped (or t1 was reached
+    // before them); they hold the fill value (+inf after an unbounded stop)
+    const int tail0 = max(si_end, static_cast<int>(a.win_begin));
+    for (int j0 = tail0; j0 < a.n_save; j0 += 32) {
+        const int nvalid = min(32, a.n_save - j0);
         double v[S];
 #pragma unroll
-        for (int q = 0; q < S; ++q) v[q] = 0.0;
-        if (valid) {
-            while (k < nrec && j >= rsi + rns) {
-                ++k;
-                if (k < nrec) {
-                    const int* hi = reinterpret_cast<const int*>(record_ptr(a, pl.sl, traj, k) + 16);
-                    rsi = hi[0];
-                    rns = hi[1];
-                }
-            }
-            if (k < nrec && j >= rsi) {
-                if (loaded != k) {
-                    const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
-                    rt = reinterpret_cast<const double*>(rec)[0];
-                    rdt = reinterpret_cast<const double*>(rec)[1];
-                    const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
-#pragma unroll
-                    for (int q = 0; q < 5 * S; ++q) {
-                        co[q] = R(0);
-                        if (q < 5 * ns) co[q] = c[q];
-                    }
-                    loaded = k;
-                }
-                const double ts = __ldg(a.save_ts + j);
-                const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) / rdt);
-#pragma unroll
-                for (int q = 0; q < S; ++q) {
-                    const R y = co[5 * q], hk = co[5 * q + 1], cc = co[5 * q + 2], bb = co[5 * q + 3],
-                            aa = co[5 * q + 4];
-                    v[q] = static_cast<double>(y + x * (hk + x * (cc + x * (bb + x * aa))));
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < S; ++q)
-                    if (q < ns) v[q] = fill[pl.stat_state[q]];
-            }
-        }
-        if (base == a.win_begin) {  // shift = first window sample (lane 0 holds it)
-#pragma unroll
-            for (int q = 0; q < S; ++q) {
-                const double f = __shfl_sync(0xffffffffu, v[q], 0);
-                sh[q] = isfinite(f) ? f : 0.0;
-            }
-        }
-        if (valid) {
-#pragma unroll
-            for (int q = 0; q < S; ++q) {
-                if (q >= ns) continue;
-                const double d = v[q] - sh[q];
-                s1[q] += d;
-                s2[q] = fma(d, d, s2[q]);
-                mn[q] = fmin(mn[q], v[q]);
-                mx[q] = fmax(mx[q], v[q]);
-                if (v[q] != v[q]) nan_flags |= 1 << q;
-                if (j == a.n_save - 1) last[q] = v[q];
-            }
-            for (int m = 0; m < pl.n_med; ++m)
-                median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (j - a.win_begin)] =
-                    static_cast<float>(pick(v, pl.slot_of[pl.med_state[m]]));
-        }
-        for (int c = 0; c < pl.n_cross; ++c) {
-            const double cur = pick(v, pl.slot_of[pl.cross_state[c]]);
-            double prev = __shfl_up_sync(0xffffffffu, cur, 1);
-            if (lane == 0) prev = carry[c];
-            const bool count_it = valid && j > a.win_begin;
-            const bool changed = (cur > pl.cross_level[c]) != (prev > pl.cross_level[c]);
-            const int inc = (count_it && changed) ? 1 : 0;
-#pragma unroll
-            for (int q = 0; q < PB_MAX_CROSSING; ++q) cross_cnt[q] += (q == c) ? inc : 0;
-            const double nxt = __shfl_sync(0xffffffffu, cur, 31);
-#pragma unroll
-            for (int q = 0; q < PB_MAX_CROSSING; ++q) carry[q] = (q == c) ? nxt : carry[q];
-        }
+        for (int q = 0; q < S; ++q) v[q] = q < ns ? fill[pl.stat_state[q < ns ? q : 0]] : 0.0;
+        fold_samples(acc, pl, a, traj, nwin, j0, nvalid, v, lane);
     }
     // warp reductions
 #pragma unroll
     for (int q = 0; q < S; ++q) {
         for (int o = 16; o > 0; o >>= 1) {
-            s1[q] += __shfl_xor_sync(0xffffffffu, s1[q], o);
-            s2[q] += __shfl_xor_sync(0xffffffffu, s2[q], o);
-            mn[q] = fmin(mn[q], __shfl_xor_sync(0xffffffffu, mn[q], o));
-            mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
-            last[q] += __shfl_xor_sync(0xffffffffu, last[q], o);  // one lane holds it, the rest 0
+            acc.s1[q] += __shfl_xor_sync(0xffffffffu, acc.s1[q], o);
+            acc.s2[q] += __shfl_xor_sync(0xffffffffu, acc.s2[q], o);
+            acc.mn[q] = fmin(acc.mn[q], __shfl_xor_sync(0xffffffffu, acc.mn[q], o));
+            acc.mx[q] = fmax(acc.mx[q], __shfl_xor_sync(0xffffffffu, acc.mx[q], o));
+            acc.last[q] += __shfl_xor_sync(0xffffffffu, acc.last[q], o);  // one lane holds it, the rest 0
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
-        nan_flags |= __shfl_xor_sync(0xffffffffu, nan_flags, o);
+        acc.nan_flags |= __shfl_xor_sync(0xffffffffu, acc.nan_flags, o);
 #pragma unroll
-        for (int q = 0; q < PB_MAX_CROSSING; ++q) cross_cnt[q] += __shfl_xor_sync(0xffffffffu, cross_cnt[q], o);
+        for (int q = 0; q < PB_MAX_CROSSING; ++q)
+            acc.cross_cnt[q] += __shfl_xor_sync(0xffffffffu, acc.cross_cnt[q], o);
     }
     if (lane != 0 || !a.features_out) return;
     const double n = static_cast<double>(nwin);
@@ -179,16 +219,15 @@ __global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
         const int kind = a.feat_kind[c];
         if (kind == PB_FEAT_MEDIAN) continue;  // written by the median pass
         const int slot = pl.slot_of[a.feat_state[c]];
-        const bool has_nan = (nan_flags >> slot) & 1;
+        const bool has_nan = (acc.nan_flags >> slot) & 1;
         double cr = CUDART_NAN;
         if (kind == PB_FEAT_CROSSINGS) {
-            cr = jc < pl.n_cross ? static_cast<double>(pick(cross_cnt, jc)) : CUDART_NAN;
+            cr = jc < pl.n_cross ? static_cast<double>(pick(acc.cross_cnt, jc)) : CUDART_NAN;
             ++jc;
         }
-        double v = feature_value(kind, pick(sh, slot), pick(s1, slot), pick(s2, slot),
-                                 has_nan ? CUDART_NAN : pick(mn, slot), has_nan ? CUDART_NAN : pick(mx, slot),
-                                 pick(last, slot), n, cr);
-        if (nwin <= 0) v = CUDART_NAN;
+        const double v = feature_value(kind, pick(acc.sh, slot), pick(acc.s1, slot), pick(acc.s2, slot),
+                                       has_nan ? CUDART_NAN : pick(acc.mn, slot),
+                                       has_nan ? CUDART_NAN : pick(acc.mx, slot), pick(acc.last, slot), n, cr);
         a.features_out[traj * a.n_features + c] = v;
     }
 }

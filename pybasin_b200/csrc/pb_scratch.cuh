@@ -4,9 +4,11 @@
 //   [step records]    n_traj x cap x record_stride bytes        (PB_DENSE_DEFERRED)
 //   [tails]           n_traj x tail_stride bytes                (PB_DENSE_DEFERRED)
 //
-// Each part starts on a 256-byte boundary.  A step record is
-//   double t, double dt, int32 first_save, int32 n_saves,
-//   then for each statistics state: y, h*k1, c, b, a   (stage precision)
+// Each part starts on a 256-byte boundary.  A step record (a multiple of 16 bytes,
+// written with 16-byte stores) is
+//   double t, double dt,
+//   for each statistics state: y, h*k1, c, b, a   (stage precision),
+//   int32 first_save, int32 n_saves, padding
 // and a tail is
 //   int32 n_records (-1 = capacity exceeded), int32 next_save, int32 status, int32 pad,
 //   double fill[dim]   (value of the save points after the last record)
@@ -18,7 +20,7 @@
 namespace pb {
 
 constexpr int PB_MAX_STAT_STATES = 8;
-constexpr int kRecordHeader = 24;
+constexpr int kRecordHeader = 16;  // t, dt
 constexpr int kDefaultRecordCap = 1024;
 
 struct ScratchLayout {
@@ -61,7 +63,7 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
     l.deferred = (a.dense_mode == PB_DENSE_DEFERRED && a.n_features > 0 && a.y_full_out == nullptr) ? 1 : 0;
     if (l.deferred) {
         const int rsize = a.precision == PB_PREC_FP64 ? 8 : 4;
-        l.rec_stride = static_cast<int32_t>(align_up(kRecordHeader + 5 * count_stat_states(a) * rsize, 8));
+        l.rec_stride = static_cast<int32_t>(align_up(kRecordHeader + 5 * count_stat_states(a) * rsize + 8, 16));
         int64_t cap = a.window_record_cap > 0 ? a.window_record_cap : kDefaultRecordCap;
         if (cap > nwin) cap = nwin;
         l.cap = static_cast<int32_t>(cap);
@@ -88,5 +90,8 @@ __device__ __forceinline__ unsigned char* tail_ptr(const pb_solve_args& a, const
 {
     return static_cast<unsigned char*>(a.scratch) + l.tail_off + traj * l.tail_stride;
 }
+
+// offset of (first_save, n_saves) inside a record
+__host__ __device__ inline int record_index_offset(int ns, int rsize) { return kRecordHeader + 5 * ns * rsize; }
 
 }  // namespace pb
