@@ -87,6 +87,7 @@ struct Plan {
     double cross_level[PB_MAX_CROSSING];
     int med_state[PB_MAX_FEATURES];
     ScratchLayout sl;
+    double inv_ds;  // 1 / mean spacing of the save grid (a hint for locating save points)
 };
 
 __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
@@ -116,6 +117,9 @@ __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
     }
     pl.ns = ns;
     pl.sl = scratch_layout(a);
+    pl.inv_ds = (a.n_save > 1 && a.save_ts[a.n_save - 1] > a.save_ts[0])
+                    ? (a.n_save - 1) / (a.save_ts[a.n_save - 1] - a.save_ts[0])
+                    : 0.0;
 }
 
 // Per-thread window statistics in shared memory, structure-of-arrays
@@ -346,12 +350,18 @@ struct Integrator {
                                         double tn)
     {
         if (L.nrec >= pl.sl.cap) return false;
+        // first save index after (t, tn]: probe where a uniform grid would put it,
+        // then correct (the grid is not assumed uniform, only used as a hint)
+        const double lim = tn + dp::save_slack;
         int si = L.si;
-        double ts = L.next_save;
-        while (si < a.n_save && ts <= tn + dp::save_slack) {
-            ++si;
-            ts = load_save(a, si);
+        {
+            const int guess = L.si + 1 + static_cast<int>(fmax(0.0, (lim - L.next_save) * pl.inv_ds));
+            int g = min(guess, a.n_save);
+            while (g > L.si + 1 && !(load_save(a, g - 1) <= lim)) --g;  // move down to a covered index
+            while (g < a.n_save && load_save(a, g) <= lim) ++g;         // move up past the covered run
+            si = g;
         }
+        const double ts = load_save(a, si);
         // assemble the record as 32-bit words, then store it with 16-byte vector stores
         constexpr int RW = sizeof(R) / 4;
         constexpr int kWords = (kRecordHeader + 5 * S * static_cast<int>(sizeof(R)) + 8 + 15) / 16 * 4;
@@ -360,8 +370,9 @@ struct Integrator {
         for (int q = 0; q < kWords; ++q) w[q] = 0u;
         w[0] = __double2loint(t);
         w[1] = __double2hiint(t);
-        w[2] = __double2loint(dt);
-        w[3] = __double2hiint(dt);
+        const double inv_dt = 1.0 / dt;
+        w[2] = __double2loint(inv_dt);
+        w[3] = __double2hiint(inv_dt);
         int j = 0;
 #pragma unroll
         for (int s = 0; s < S; ++s) {

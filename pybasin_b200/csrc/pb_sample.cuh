@@ -171,12 +171,14 @@ __global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
                 if (cand <= hl && sc <= j) r = cand;
             }
             const double t_r = __shfl_sync(0xffffffffu, rt, r);
-            const double dt_r = __shfl_sync(0xffffffffu, rdt, r);
+            const double idt_r = __shfl_sync(0xffffffffu, rdt, r);
             const double ts = lane < nvalid ? __ldg(a.save_ts + j) : t_r;
-            const R x = (ts <= t_r + dp::save_slack) ? R(0) : static_cast<R>((ts - t_r) / dt_r);
+            const R x = (ts <= t_r + dp::save_slack) ? R(0) : static_cast<R>((ts - t_r) * idt_r);
             double v[S];
 #pragma unroll
             for (int q = 0; q < S; ++q) {
+                v[q] = 0.0;
+                if (q >= ns) continue;  // uniform across the warp
                 R c5[5];
 #pragma unroll
                 for (int z = 0; z < 5; ++z) c5[z] = __shfl_sync(0xffffffffu, co[5 * q + z], r);

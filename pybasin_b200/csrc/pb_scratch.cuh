@@ -6,7 +6,7 @@
 //
 // Each part starts on a 256-byte boundary.  A step record (a multiple of 16 bytes,
 // written with 16-byte stores) is
-//   double t, double dt,
+//   double t, double 1/dt,
 //   for each statistics state: y, h*k1, c, b, a   (stage precision),
 //   int32 first_save, int32 n_saves, padding
 // and a tail is
@@ -20,7 +20,7 @@
 namespace pb {
 
 constexpr int PB_MAX_STAT_STATES = 8;
-constexpr int kRecordHeader = 16;  // t, dt
+constexpr int kRecordHeader = 16;  // t, 1/dt
 constexpr int kDefaultRecordCap = 1024;
 
 struct ScratchLayout {
