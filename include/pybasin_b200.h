@@ -38,7 +38,8 @@ typedef enum {
     PB_EINVAL = -5,         /* invalid argument (null pointer, bad size, bad layout) */
     PB_ECUDA = -6,          /* other CUDA runtime error */
     PB_EUNSUPPORTED = -7,   /* valid request this build does not support */
-    PB_ECOMPILE = -8        /* runtime (NVRTC) compilation of a user right-hand side failed */
+    PB_ECOMPILE = -8,       /* runtime (NVRTC) compilation of a user right-hand side failed */
+    PB_ESCRATCH_LIMIT = -9  /* pb_solve_batch_noalloc: request needs more than PB_NOALLOC_SCRATCH_BYTES */
 } pb_status;
 
 /* ---- built-in right-hand sides (templated device functors) ---- */
@@ -205,6 +206,23 @@ int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t s
  * The caller times it; flops = 2 * 8 * iters * blocks * 256.  No reference
  * counterpart (measurement utility). */
 int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, void* stream);
+
+/* Allocation-free variant of pb_solve_batch.  No counterpart in the reference:
+ * it exists for callers that may not allocate device memory themselves, such as
+ * plug-ins of a host application that owns all device memory under a fixed
+ * budget, or latency-critical loops that cannot afford cudaMalloc.  The caller
+ * still provides every input and output array; args->scratch and
+ * args->queue_counter are ignored and replaced by a fixed array of
+ * PB_NOALLOC_SCRATCH_BYTES bytes that this library reserves on every GPU it is
+ * loaded on (held until the process exits).  A request whose scratch
+ * (pb_solve_scratch_bytes + 256) exceeds that size returns PB_ESCRATCH_LIMIT and
+ * launches nothing.  The first call on a device looks up the array's device
+ * address (once per device); make that first call before any stream capture.
+ * All calls on a device share the one array: calls whose kernels may overlap on
+ * the GPU (different streams, or several host threads) race and must be
+ * serialised by the caller.  The call itself allocates nothing. */
+#define PB_NOALLOC_SCRATCH_BYTES (64ll * 1024ll * 1024ll)
+int pb_solve_batch_noalloc(const pb_solve_args* args, void* stream);
 
 /* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
 const char* pb_error_string(int32_t status);

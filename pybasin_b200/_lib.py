@@ -22,6 +22,8 @@ PB_EINVAL = -5
 PB_ECUDA = -6
 PB_EUNSUPPORTED = -7
 PB_ECOMPILE = -8
+PB_ESCRATCH_LIMIT = -9
+NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 SYS_LINEAR = 0
 SYS_PENDULUM = 1
@@ -147,6 +149,7 @@ EXPORTED_SYMBOLS = (
     "pb_error_string",
     "pb_abi_version",
     "pb_probe_fma",
+    "pb_solve_batch_noalloc",
 )
 
 
@@ -170,6 +173,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         lib = ctypes.CDLL(str(path))
         lib.pb_solve_batch.restype = ctypes.c_int
         lib.pb_solve_batch.argtypes = [ctypes.POINTER(SolveArgs), _c_vp]
+        lib.pb_solve_batch_noalloc.restype = ctypes.c_int
+        lib.pb_solve_batch_noalloc.argtypes = [ctypes.POINTER(SolveArgs), _c_vp]
         lib.pb_solve_scratch_bytes.restype = _c_i64
         lib.pb_solve_scratch_bytes.argtypes = [ctypes.POINTER(SolveArgs)]
         lib.pb_label_nearest.restype = ctypes.c_int

@@ -311,6 +311,7 @@ const char* pb_error_string(int32_t s)
         case PB_ECUDA: return "CUDA runtime error";
         case PB_EUNSUPPORTED: return "unsupported request";
         case PB_ECOMPILE: return "runtime compilation of the right-hand side failed";
+        case PB_ESCRATCH_LIMIT: return "request exceeds the fixed scratch of the allocation-free entry point";
         default: return "unknown error";
     }
 }
