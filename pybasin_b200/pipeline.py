@@ -122,6 +122,7 @@ class BasinStabilityPipeline:
             block_size=self.solver.block_size,
             grid_blocks=self.solver.grid_blocks,
             order=self.order if self.solver.order == "morton" else None,
+            dense_mode=L.DENSE_DEFERRED if self.solver.dense_mode == "deferred" else L.DENSE_INLINE,
         )
         self.args = build_args(req, self.out, self.queue, None)
         self.scratch = alloc_scratch(self.args, dev)
@@ -154,9 +155,11 @@ class BasinStabilityPipeline:
         L.check(rc, "pb_label_nearest")
 
     def kernel_launches_per_pass(self) -> int:
-        """Launches of this library's kernels per pass (integrator + labelling); the
-        Z-order key/argsort of the ICs runs as PyTorch ops before them."""
-        return 2
+        """Launches of this library's kernels per pass; the Z-order key/argsort of the
+        ICs runs as PyTorch ops before them.  Deferred dense output: integrate + sample
+        + redo of record overflows, then labelling; inline: integrate, labelling."""
+        deferred = self.solver.dense_mode == "deferred"
+        return 4 if deferred else 2
 
     def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
         """Label device-resident ``y0`` (N, S) on the current stream; asynchronous."""

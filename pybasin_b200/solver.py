@@ -101,6 +101,9 @@ class B200Dopri5Solver:
     :param unbounded_threshold: stop a trajectory once max|y| >= this after an accepted
         step (the reference's stop events, e.g. case_studies/lorenz/setup_lorenz_system.py:16-26).
     :param schedule: ``"queue"`` (persistent warps + work queue) or ``"plain"``.
+    :param dense_mode: ``"deferred"`` (the integrator writes one record per window step that
+        holds save points and a warp-parallel pass evaluates the save points) or ``"inline"``
+        (each thread evaluates its save points after its step); full output is always inline.
     :param order: ``"morton"`` integrates the ICs in Z-order of their coordinates so each
         warp holds neighbouring ICs (similar dynamics and step counts); ``"none"`` keeps
         the input order.  Outputs are in input order either way.
@@ -127,6 +130,7 @@ class B200Dopri5Solver:
         block_size: int = 0,
         grid_blocks: int = 0,
         order: str = "morton",
+        dense_mode: str = "deferred",
     ):
         if t_eval is not None and (t_eval[0] < t_span[0] or t_eval[1] > t_span[1]):
             raise ValueError(f"t_eval {t_eval} must be within t_span {t_span}.")
@@ -142,7 +146,10 @@ class B200Dopri5Solver:
             raise ValueError("t_steps must be >= 1")
         if order not in ("morton", "none"):
             raise ValueError("order must be 'morton' or 'none'")
+        if dense_mode not in ("deferred", "inline"):
+            raise ValueError("dense_mode must be 'deferred' or 'inline'")
         self.order = order
+        self.dense_mode = dense_mode
         self.t_span = t_span
         self.t_eval = t_eval
         self.t_steps = t_steps
@@ -203,6 +210,7 @@ class B200Dopri5Solver:
             block_size=self.block_size,
             grid_blocks=self.grid_blocks,
             order=self.order,
+            dense_mode=self.dense_mode,
         )
 
     def compute_device(self) -> torch.device:
@@ -301,6 +309,7 @@ class B200Dopri5Solver:
                 block_size=self.block_size,
                 grid_blocks=self.grid_blocks,
                 order=order,
+                dense_mode=L.DENSE_DEFERRED if self.dense_mode == "deferred" else L.DENSE_INLINE,
             )
             res = solve(req, stream)
             if full:
