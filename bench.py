@@ -231,7 +231,6 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
     import ctypes
 
     from pybasin_b200 import _lib as L
-    from pybasin_b200.engine import spatial_order
 
     lib = L.load()
     s = torch.cuda.current_stream()
@@ -247,9 +246,7 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
         a, k0, b, c = ev[i]
         n = y0_dev.shape[0]
         a.record(s)
-        pipe.y0_buf[:n].copy_(y0_dev, non_blocking=True)
-        if pipe.solver.order == "morton":
-            pipe.order[:n].copy_(spatial_order(y0_dev))
+        pipe.load_rows(y0_dev)
         k0.record(s)
         L.check(lib.pb_solve_batch(ctypes.byref(pipe.args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
         b.record(s)

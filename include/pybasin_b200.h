@@ -144,7 +144,7 @@ typedef struct pb_solve_args {
     unsigned long long* queue_counter; /* QUEUE schedule: one counter (the call resets it on `stream`) */
     void* scratch;           /* pb_solve_scratch_bytes(args) bytes, 256-byte aligned; NULL when that is 0 */
     /* processing order (device, optional): queue position q integrates trajectory
-       order[q], a permutation of [0, n_traj).  Ordering ICs along a space-filling
+       order[q], a permutation of [0, n_traj) (entries outside that range are skipped).  Ordering ICs along a space-filling
        curve puts trajectories with similar dynamics (and step counts) in the same
        warp.  Outputs stay indexed by trajectory. */
     const int32_t* order;
@@ -223,6 +223,50 @@ int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, 
  * serialised by the caller.  The call itself allocates nothing. */
 #define PB_NOALLOC_SCRATCH_BYTES (64ll * 1024ll * 1024ll)
 int pb_solve_batch_noalloc(const pb_solve_args* args, void* stream);
+
+/* ---- learned surrogate (no counterpart in the reference) -------------------
+ * A small MLP maps (initial condition, parameters) to attractor-class logits;
+ * it is trained on labels produced by pb_solve_batch + pb_label_nearest, and its
+ * low-confidence predictions (plus an audited random slice) are integrated.
+ * BF16 operands, FP32 accumulation (mma.sync m16n8k16), all arrays device. */
+
+/* C[m,n] = alpha * sum_k A(m,k) B(k,n) (+ bias[n]), optionally GELU; A(m,k) is
+ * A[m*sam + k*sak], B(k,n) is B[k*sbk + n*sbn] (BF16).  Outputs (row stride ldc):
+ * c_f32 (FP32), c_bf16 (BF16), z_pre (FP32 value before the activation); any may
+ * be NULL but not all. */
+int pb_mlp_gemm(const void* A, int64_t sam, int64_t sak, const void* B, int64_t sbk, int64_t sbn,
+                const float* bias, float alpha, int32_t M, int32_t N, int32_t K, int32_t gelu,
+                float* c_f32, void* c_bf16, float* z_pre, int64_t ldc, void* stream);
+/* dz = dy * GELU'(z) elementwise (BF16 and/or FP32 outputs). */
+int pb_mlp_gelu_backward(const float* dy, const float* z, int64_t n, void* dz_bf16, float* dz_f32, void* stream);
+/* Softmax cross-entropy of (M x C) logits against labels (NULL: no loss):
+ * dz = (softmax - onehot) * scale; loss_sum += sum of -log p[label];
+ * correct += number of rows whose argmax is the label. */
+int pb_mlp_softmax_xent(const float* logits, const int32_t* labels, int32_t M, int32_t C, float scale,
+                        void* dz_bf16, float* dz_f32, float* loss_sum, int32_t* correct, void* stream);
+/* db[n] = alpha * sum_m dz[m, n] for an (M x N) FP32 matrix. */
+int pb_mlp_bias_grad(const float* dz, int32_t M, int32_t N, float alpha, float* db, void* stream);
+/* AdamW step `step` (>= 1) on FP32 master weights; refreshes the BF16 copy if given. */
+int pb_mlp_adamw(float* w, const float* g, float* m1, float* m2, void* w_bf16, int64_t n, float lr,
+                 float beta1, float beta2, float eps, float weight_decay, int32_t step, void* stream);
+/* y = BF16(x). */
+int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream);
+/* Network inputs: row r = [(ic[r, :S] , params[:n_params]) - shift] * scale, zero
+ * padded to d_pad columns, as BF16. */
+int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
+                        const float* scale, int64_t n, int32_t d_pad, void* out_bf16, void* stream);
+/* Confidence gate: label = argmax, conf = max softmax probability; rows with
+ * conf < threshold or audit[i] != 0 are appended to route (n_route counts them,
+ * reset by the call). */
+int pb_surrogate_gate(const float* logits, int64_t n, int32_t C, float threshold, const uint8_t* audit,
+                      int32_t* label, float* conf, int32_t* route, int32_t* n_route, void* stream);
+/* y[k, :] = x[idx[k], :] for k < min(*n_idx, max_rows). */
+int pb_gather_rows(const float* x, int32_t width, const int32_t* idx, const int32_t* n_idx, int64_t max_rows,
+                   float* y, void* stream);
+/* label[idx[k]] = integrated[k] for k < min(*n_idx, max_rows); the surrogate's label of
+ * each routed row is kept in surrogate_label_of_routed[k] (may be NULL). */
+int pb_merge_labels(const int32_t* integrated, const int32_t* idx, const int32_t* n_idx, int64_t max_rows,
+                    int32_t* label, int32_t* surrogate_label_of_routed, void* stream);
 
 /* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
 const char* pb_error_string(int32_t status);

@@ -700,6 +700,7 @@ __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
     const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= a.n_traj) return;
     const int64_t traj = traj_at(a, q);
+    if (traj < 0 || traj >= a.n_traj) return;  // an order entry out of range is ignored
     auto st = stats_slot<Sys>(smem, !DEFER);
     typename I::L_t L;
     I::begin(L, st, traj, a);
@@ -734,7 +735,9 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
         const int64_t q = static_cast<int64_t>(base) + lane;
         if (q < a.n_traj) {
             const int64_t traj = traj_at(a, q);
-            const bool skip = redo_only && reinterpret_cast<const int*>(tail_ptr(a, pl.sl, traj))[0] >= 0;
+            const bool in_range = traj >= 0 && traj < a.n_traj;  // an order entry out of range is ignored
+            const bool skip = !in_range ||
+                              (redo_only && reinterpret_cast<const int*>(tail_ptr(a, pl.sl, traj))[0] >= 0);
             if (!skip) {
                 typename I::L_t L;
                 I::begin(L, st, traj, a);

@@ -1,0 +1,130 @@
+"""Surrogate-gated basin-stability pass.
+
+ICs -> surrogate logits -> confidence gate (threshold, seeded audit slice) ->
+the routed ICs (low confidence or audited) are integrated with the fused Dopri5
+pipeline together with the templates -> labels merged back -> counts.  Every
+label is either an integrator label or a confident surrogate label, and the
+audit slice measures how often a confident surrogate label disagrees with the
+integrator.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from pybasin_b200 import _lib as L
+from pybasin_b200.pipeline import BasinStabilityPipeline
+from pybasin_b200.surrogate import MLPSurrogate, TrainHistory, _bind, _p
+
+
+@dataclass
+class GateStats:
+    n: int
+    n_routed: int
+    n_audited: int
+    audit_confident: int  # audited rows the surrogate was confident about
+    audit_disagree: int  # ... of which the integrator gave another label
+
+    @property
+    def routed_fraction(self) -> float:
+        return self.n_routed / max(self.n, 1)
+
+    @property
+    def audit_error(self) -> float:
+        return self.audit_disagree / max(self.audit_confident, 1)
+
+
+class SurrogateGatedPipeline:
+    """Surrogate in front of a ``BasinStabilityPipeline`` for one ODE system and parameter row."""
+
+    def __init__(
+        self,
+        pipeline: BasinStabilityPipeline,
+        hidden: int = 256,
+        depth: int = 4,
+        threshold: float = 0.95,
+        audit_fraction: float = 0.01,
+        audit_seed: int = 123,
+        seed: int = 0,
+    ):
+        self.pipe = pipeline
+        self.dev = pipeline.dev
+        self.params = pipeline.params[0].to(torch.float64)  # the main parameter row
+        self.S = pipeline.dim
+        self.C = pipeline.n_classes + 1  # + unbounded
+        self.net = MLPSurrogate(self.S + self.params.numel(), self.C, hidden=hidden, depth=depth, seed=seed,
+                                device=self.dev)
+        self.threshold = threshold
+        self.audit_fraction = audit_fraction
+        self.audit_seed = audit_seed
+        self._audit: dict[int, torch.Tensor] = {}
+
+    # -- training ------------------------------------------------------------------
+    def _raw_inputs(self, y0: torch.Tensor) -> torch.Tensor:
+        p = self.params.to(torch.float32).expand(y0.shape[0], -1)
+        return torch.cat([y0.to(torch.float32), p], dim=1)
+
+    def train(self, y0_train: torch.Tensor, epochs: int = 30, batch: int = 1024, lr: float = 2e-3,
+              seed: int = 0) -> tuple[TrainHistory, dict[str, float]]:
+        """Label ``y0_train`` with the integrator, then fit the network on those labels."""
+        t0 = time.perf_counter()
+        labels, _ = self.pipe.run_device(y0_train.to(self.dev))
+        labels = labels.clone()
+        torch.cuda.synchronize(self.dev)
+        t1 = time.perf_counter()
+        self.net.fit_normalisation(self._raw_inputs(y0_train.to(self.dev)))
+        x = self.net.inputs(y0_train.to(self.dev), self.params)
+        hist = self.net.train(x, labels, epochs=epochs, batch=batch, lr=lr, seed=seed)
+        torch.cuda.synchronize(self.dev)
+        t2 = time.perf_counter()
+        return hist, {"label_s": t1 - t0, "train_s": t2 - t1, "n_train": int(y0_train.shape[0])}
+
+    # -- inference -------------------------------------------------------------------
+    def audit_mask(self, n: int) -> torch.Tensor:
+        m = self._audit.get(n)
+        if m is None:
+            rng = np.random.default_rng(self.audit_seed)
+            m = torch.as_tensor((rng.random(n) < self.audit_fraction).astype(np.uint8), device=self.dev)
+            self._audit[n] = m
+        return m
+
+    def run_device(self, y0: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor, GateStats]:
+        """Labels (int32, class n_classes = unbounded) and per-class counts for device ICs."""
+        lib = L.load()
+        _bind(lib)
+        s = torch.cuda.current_stream(self.dev).cuda_stream
+        n = y0.shape[0]
+        x = self.net.inputs(y0, self.params)
+        logits = self.net.logits(x)
+        audit = self.audit_mask(n)
+        label = torch.empty((n,), dtype=torch.int32, device=self.dev)
+        route = torch.empty((n,), dtype=torch.int32, device=self.dev)
+        n_route = torch.empty((1,), dtype=torch.int32, device=self.dev)
+        L.check(lib.pb_surrogate_gate(_p(logits), n, self.C, self.threshold, _p(audit), _p(label), None, _p(route),
+                                      _p(n_route), s), "pb_surrogate_gate")
+        k = int(n_route.item())  # the one host read of the pass: how many ICs to integrate
+        if k > 0:
+            routed = torch.empty((k, self.S), dtype=torch.float32, device=self.dev)
+            L.check(lib.pb_gather_rows(_p(y0.contiguous()), self.S, _p(route), _p(n_route), k, _p(routed), s),
+                    "pb_gather_rows")
+            integ, _ = self.pipe.run_device(routed)
+            sur_of_routed = torch.empty((k,), dtype=torch.int32, device=self.dev)
+            L.check(lib.pb_merge_labels(_p(integ), _p(route), _p(n_route), k, _p(label), _p(sur_of_routed), s),
+                    "pb_merge_labels")
+            idx = route[:k].long()
+            aud = audit[idx].bool()
+            # audited rows the surrogate was confident about (it would have kept their label)
+            pmax = torch.softmax(logits[idx], dim=1).amax(dim=1)
+            conf_aud = aud & (pmax >= self.threshold)
+            n_conf = int(conf_aud.sum())
+            n_dis = int((conf_aud & (sur_of_routed.long() != integ[:k].long())).sum())
+            n_aud = int(aud.sum())
+        else:
+            n_conf = n_dis = n_aud = 0
+        counts = torch.bincount(label.long(), minlength=self.C)
+        return label, counts, GateStats(n, k, n_aud, n_conf, n_dis)

@@ -79,15 +79,14 @@ class BasinStabilityPipeline:
         self.stream = torch.cuda.Stream(device=self.dev)
 
     # -- buffers ---------------------------------------------------------------
-    def _allocate(self, n: int) -> None:
+    def _allocate(self, capacity: int) -> None:
+        """Buffers for up to `capacity` ICs; rows [n, n + templates) hold the templates."""
         dev = self.dev
-        tot = n + self.n_tpl
+        tot = capacity + self.n_tpl
         F = len(self.columns)
+        self.capacity = capacity
         self.y0_buf = torch.empty((tot, self.dim), dtype=torch.float32, device=dev)
-        self.y0_buf[n:] = self.template_y0
-        pidx = torch.zeros((tot,), dtype=torch.int32, device=dev)
-        pidx[n:] = 1
-        self.pidx = pidx
+        self.pidx = torch.zeros((tot,), dtype=torch.int32, device=dev)
         self.out = SolveResult(
             features=torch.empty((tot, F), dtype=torch.float64, device=dev),
             status=torch.empty((tot,), dtype=torch.int32, device=dev),
@@ -97,7 +96,7 @@ class BasinStabilityPipeline:
         )
         self.queue = torch.zeros((1,), dtype=torch.int64, device=dev)
         self.order = torch.arange(tot, dtype=torch.int32, device=dev)
-        self.labels = torch.empty((n,), dtype=torch.int32, device=dev)
+        self.labels = torch.empty((capacity,), dtype=torch.int32, device=dev)
         self.counts = torch.empty((1, self.n_classes + 1), dtype=torch.int64, device=dev)
         rtol, atol = self.solver.effective_tolerances()
         req = SolveRequest(
@@ -125,9 +124,25 @@ class BasinStabilityPipeline:
             dense_mode=L.DENSE_DEFERRED if self.solver.dense_mode == "deferred" else L.DENSE_INLINE,
         )
         self.args = build_args(req, self.out, self.queue, None)
-        self.scratch = alloc_scratch(self.args, dev)
-        self._n = n
+        self.scratch = alloc_scratch(self.args, dev)  # sized for the full capacity
+        self._n = None
         self._graph = None
+
+    def _prepare(self, n: int) -> None:
+        """Place the templates after the first n rows and size the launch to n + templates."""
+        T = self.n_tpl
+        self.y0_buf[n : n + T] = self.template_y0
+        self.pidx.zero_()
+        self.pidx[n : n + T] = 1
+        if self.solver.order == "morton" and n > 1:
+            self.order[:n].copy_(spatial_order(self.y0_buf[:n]))
+        elif self.solver.order == "morton":
+            self.order[:n] = torch.arange(n, dtype=torch.int32, device=self.dev)
+        self.order[n : n + T] = torch.arange(n, n + T, dtype=torch.int32, device=self.dev)
+        self.args.n_traj = n + T
+        if self._n != n:
+            self._graph = None
+        self._n = n
 
     # -- one pass ----------------------------------------------------------------
     def _launch(self) -> None:
@@ -161,14 +176,18 @@ class BasinStabilityPipeline:
         deferred = self.solver.dense_mode == "deferred"
         return 4 if deferred else 2
 
-    def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
-        """Label device-resident ``y0`` (N, S) on the current stream; asynchronous."""
+    def load_rows(self, y0: torch.Tensor) -> int:
+        """Copy device ICs into the pipeline (growing it if needed); returns n."""
         n = y0.shape[0]
-        if self._n != n:
+        if getattr(self, "capacity", -1) < n:
             self._allocate(n)
         self.y0_buf[:n].copy_(y0, non_blocking=True)
-        if self.solver.order == "morton" and n > 1:
-            self.order[:n].copy_(spatial_order(y0))
+        self._prepare(n)
+        return n
+
+    def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
+        """Label device-resident ``y0`` (N, S) on the current stream; asynchronous."""
+        n = self.load_rows(y0)
         if use_graph:
             if self._graph is None:
                 self._capture()
@@ -176,7 +195,7 @@ class BasinStabilityPipeline:
             self._graph.replay()
         else:
             self._launch()
-        return self.labels, self.counts
+        return self.labels[:n], self.counts
 
     def _capture(self) -> None:
         torch.cuda.synchronize(self.dev)

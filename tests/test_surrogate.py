@@ -1,0 +1,160 @@
+"""Surrogate MLP: the FP64 NumPy oracle (CPU) and the BF16 tensor-core kernels against it (GPU).
+
+Tolerances: BF16 operands carry 8 mantissa bits, so GEMMs are compared to the
+FP64 product of the *same* BF16-rounded operands at 1e-4 relative (FP32
+accumulation only), and end-to-end gradients (which also round dZ and the
+activations to BF16) at 3e-2 relative to the largest gradient entry.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_oracle as MO
+
+
+def _bf16(a: np.ndarray) -> np.ndarray:
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(torch.float64).numpy()
+
+
+def _tiny_net(rng, d_in=3, hidden=32, depth=2, C=4):
+    dims = [d_in] + [hidden] * depth + [C]
+    Ws = [rng.uniform(-1, 1, (o, i)) / np.sqrt(i) for i, o in zip(dims[:-1], dims[1:])]
+    bs = [rng.uniform(-0.1, 0.1, o) for o in dims[1:]]
+    return Ws, bs
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    Ws, bs = _tiny_net(rng)
+    x = rng.normal(size=(16, 3))
+    y = rng.integers(0, 4, 16)
+
+    def loss_of():
+        z, _, _ = MO.forward(x, Ws, bs)
+        return MO.loss_and_grad(z, y)[0] / len(y)
+
+    z, acts, pres = MO.forward(x, Ws, bs)
+    _, d = MO.loss_and_grad(z, y)
+    gW, gb = MO.backward(d, acts, pres, Ws)
+    eps = 1e-6
+    for li in range(len(Ws)):
+        for idx in [(0, 0), (1, 2), (Ws[li].shape[0] - 1, Ws[li].shape[1] - 1)]:
+            Ws[li][idx] += eps
+            lp = loss_of()
+            Ws[li][idx] -= 2 * eps
+            lm = loss_of()
+            Ws[li][idx] += eps
+            assert abs((lp - lm) / (2 * eps) - gW[li][idx]) < 1e-6
+        bs[li][0] += eps
+        lp = loss_of()
+        bs[li][0] -= 2 * eps
+        lm = loss_of()
+        bs[li][0] += eps
+        assert abs((lp - lm) / (2 * eps) - gb[li][0]) < 1e-6
+
+
+# ---------------------------------------------------------------------------- GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,N,K", [(1, 5, 3), (64, 64, 32), (130, 257, 70), (1024, 256, 256)])
+def test_gemm_matches_fp64_product_of_bf16_operands(M, N, K):
+    from pybasin_b200.surrogate import gemm
+
+    rng = np.random.default_rng(M + N + K)
+    a = _bf16(rng.normal(size=(M, K)))
+    w = _bf16(rng.normal(size=(N, K)))
+    bias = rng.normal(size=N).astype(np.float32)
+    dev = torch.device("cuda:0")
+    A = torch.tensor(a, device=dev).to(torch.bfloat16)
+    W = torch.tensor(w, device=dev).to(torch.bfloat16)
+    out = torch.empty((M, N), dtype=torch.float32, device=dev)
+    zpre = torch.empty((M, N), dtype=torch.float32, device=dev)
+    gemm(A, K, 1, W, 1, K, M, N, K, bias=torch.tensor(bias, device=dev), gelu=True, c_f32=out, z_pre=zpre)
+    # transposed operand access: C^T = W A^T through strides
+    outT = torch.empty((N, M), dtype=torch.float32, device=dev)
+    gemm(W, K, 1, A, 1, K, N, M, K, c_f32=outT)
+    torch.cuda.synchronize()
+    z = a @ w.T + bias
+    scale = np.abs(z).max() + 1e-30
+    np.testing.assert_allclose(zpre.cpu().numpy(), z, rtol=0, atol=1e-4 * scale)
+    np.testing.assert_allclose(out.cpu().numpy(), MO.gelu(z), rtol=0, atol=1e-4 * scale)
+    np.testing.assert_allclose(outT.cpu().numpy(), (a @ w.T).T, rtol=0, atol=1e-4 * scale)
+
+
+@pytest.mark.gpu
+def test_backward_matches_oracle_gradients():
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(3, 4, hidden=64, depth=3, seed=1, device=dev)
+    rng = np.random.default_rng(2)
+    xb = _bf16(rng.normal(size=(256, 3)))
+    y = rng.integers(0, 4, 256)
+    x_t = torch.tensor(xb, device=dev).to(torch.bfloat16)
+    logits, acts, pres = net.forward(x_t, keep=True)
+    dzb, dzf, loss, _ = net.loss_grad(logits, torch.tensor(y, dtype=torch.int32, device=dev), 1.0 / 256)
+    gW, gb = net.backward(dzb, dzf, acts, pres)
+    torch.cuda.synchronize()
+    Ws = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
+    bs = [b.double().cpu().numpy() for b in net.b]
+    z, oacts, opres = MO.forward(xb, Ws, bs)
+    oloss, d = MO.loss_and_grad(z, y)
+    oW, ob = MO.backward(d, oacts, opres, Ws)
+    np.testing.assert_allclose(float(loss.item()), oloss, rtol=2e-2)
+    for li in range(len(Ws)):
+        sW = np.abs(oW[li]).max()
+        np.testing.assert_allclose(gW[li].cpu().numpy(), oW[li], rtol=0, atol=3e-2 * sW)
+        sb = np.abs(ob[li]).max()
+        np.testing.assert_allclose(gb[li].cpu().numpy(), ob[li], rtol=0, atol=3e-2 * sb)
+
+
+@pytest.mark.gpu
+def test_training_learns_a_separable_problem():
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    g = torch.Generator().manual_seed(0)
+    x = torch.rand(8192, 2, generator=g) * 2 - 1
+    y = ((x[:, 0] > 0).int() + 2 * (x[:, 0] ** 2 + x[:, 1] ** 2 < 0.3).int()).to(torch.int32)
+    net = MLPSurrogate(2, 4, hidden=128, depth=3, seed=0, device=dev)
+    net.fit_normalisation(x.to(dev))
+    xi = net.inputs(x.to(dev), None)
+    hist = net.train(xi, y.to(dev), epochs=15, batch=512, lr=3e-3)
+    assert hist.loss[-1] < 0.5 * hist.loss[0]
+    assert hist.accuracy[-1] > 0.95
+
+
+@pytest.mark.gpu
+def test_gated_pipeline_matches_integrator_labels_on_duffing():
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+    from pybasin_b200.gated import SurrogateGatedPipeline
+    from pybasin_b200.pipeline import BasinStabilityPipeline
+
+    dev = torch.device("cuda:0")
+    fx = FusedFeatureExtractor(time_steady=900.0, features=None,
+                               features_per_state={0: {"maximum": None, "standard_deviation": None}}, normalize=False)
+    solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=5000, t_eval=(900, 1000), device="cuda:0", precision="mixed",
+                              feature_extractor=fx)
+    tpl = [[-0.21, 0.02], [1.05, 0.77], [-0.67, 0.02], [-0.46, 0.30], [-0.43, 0.12]]
+    pipe = BasinStabilityPipeline(DuffingODE({"delta": 0.08, "k3": 1.0, "A": 0.2}), solver, tpl,
+                                  ["y1", "y2", "y3", "y4", "y5"], device=dev)
+    gated = SurrogateGatedPipeline(pipe, hidden=128, depth=3, threshold=0.95)
+
+    def ics(n, seed):
+        torch.manual_seed(seed)
+        return (torch.rand(n, 2) * torch.tensor([2.0, 1.5]) + torch.tensor([-1.0, -0.5])).to(dev)
+
+    hist, _ = gated.train(ics(20000, 1), epochs=20)
+    assert hist.accuracy[-1] > 0.8
+    y0 = ics(20000, 2)
+    ref_labels, _ = pipe.run_device(y0)
+    ref = ref_labels.clone()
+    label, counts, stats = gated.run_device(y0)
+    torch.cuda.synchronize()
+    assert stats.n_routed < stats.n  # the surrogate labels part of the ICs
+    assert stats.n_audited > 0
+    dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
+    assert float(dbs) <= 0.005
+    assert float((label == ref).double().mean()) >= 0.99
