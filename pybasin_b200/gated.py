@@ -128,3 +128,15 @@ class SurrogateGatedPipeline:
             n_conf = n_dis = n_aud = 0
         counts = torch.bincount(label.long(), minlength=self.C)
         return label, counts, GateStats(n, k, n_aud, n_conf, n_dis)
+
+    def run(self, y0_host: torch.Tensor) -> tuple[np.ndarray, dict[str, float], GateStats]:
+        """Host ICs -> (labels as class names, basin stability per class, gate statistics)."""
+        with torch.cuda.device(self.dev):
+            y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
+            label, counts, stats = self.run_device(y0)
+            lab = label.cpu().numpy()
+            cnt = counts.cpu().numpy()
+        names = np.array(self.pipe.classes + ["unbounded"], dtype=object)
+        n = max(int(cnt.sum()), 1)
+        bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}
+        return names[lab], bs, stats
