@@ -297,10 +297,9 @@ def max_over_ranks(vals: list[float], dev: torch.device, dist_on: bool) -> list[
 
 def global_counts(counts: torch.Tensor, dist_on: bool) -> torch.Tensor:
     """Per-class counts summed over the IC shards of all ranks (the global basin stability)."""
-    c = counts[0].clone()
-    if dist_on:
-        torch.distributed.all_reduce(c)
-    return c
+    from pybasin_b200.sharding import global_counts as reduce_counts
+
+    return reduce_counts(counts[0]) if dist_on else counts[0].clone()
 
 
 def run_b200_arm(args) -> None:

@@ -240,12 +240,13 @@ def _spread_bits(v: torch.Tensor, dims: int, bits: int) -> torch.Tensor:
     return out
 
 
-def spatial_order(y0: torch.Tensor, bits: int | None = None) -> torch.Tensor:
+def spatial_order(y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
     """Permutation of the rows of ``y0`` along a Morton (Z-order) curve of its bounding box.
 
     Neighbouring initial conditions mostly share an attractor and a step count, so
-    integrating them in the same warp keeps the warp's lanes busy together.
-    Returns int32 indices on y0's device.
+    integrating them in the same warp keeps the warp's lanes busy together.  With
+    ``groups`` (e.g. the parameter row of each IC) the order is group-major, so a
+    warp does not mix parameter points.  Returns int32 indices on y0's device.
     """
     n, dims = y0.shape
     if n == 0:
@@ -260,4 +261,7 @@ def spatial_order(y0: torch.Tensor, bits: int | None = None) -> torch.Tensor:
     key = torch.zeros((n,), dtype=torch.int64, device=y0.device)
     for k in range(d):
         key |= _spread_bits(q[:, k], d, bits) << k
+    if groups is not None:
+        # group-major: 20 bits of group id above 40 bits of (truncated) Morton key
+        key = (groups.to(torch.int64) << 40) | (key >> max(0, bits * d - 40))
     return torch.argsort(key).to(torch.int32)
