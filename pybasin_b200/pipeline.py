@@ -34,6 +34,10 @@ class BasinStabilityPipeline:
     :param template_y0: template initial conditions (``TemplateIntegrator.template_y0``).
     :param template_labels: class name of each template.
     :param template_params: parameters for the templates (default: the system's).
+    :param param_rows: parameter study: one row per parameter point, shape ``(P, n_params)``
+        (default: the system's parameters, P = 1).  ICs pass their point through
+        ``group`` in ``run_device``; counts come back per point.  As in the reference's
+        parameter study, the templates are integrated once, at ``template_params``.
     """
 
     def __init__(
@@ -44,6 +48,7 @@ class BasinStabilityPipeline:
         template_labels: list[str],
         template_params: dict[str, float] | None = None,
         device: torch.device | str | None = None,
+        param_rows: np.ndarray | None = None,
     ):
         fx = solver.feature_extractor
         if fx is None:
@@ -64,7 +69,12 @@ class BasinStabilityPipeline:
             if template_params is not None
             else self.spec.params
         )
-        self.params = torch.tensor(np.stack([self.spec.params, tparams]), dtype=torch.float64, device=self.dev)
+        rows = np.atleast_2d(np.asarray(param_rows, dtype=np.float64)) if param_rows is not None else self.spec.params[None]
+        if rows.shape[1] != self.spec.params.shape[0]:
+            raise ValueError(f"param_rows need {self.spec.params.shape[0]} columns")
+        self.n_groups = rows.shape[0]
+        # rows 0..P-1: parameter points; row P: the templates' parameters
+        self.params = torch.tensor(np.vstack([rows, tparams[None]]), dtype=torch.float64, device=self.dev)
         self.template_y0 = torch.tensor(template_y0, dtype=torch.float32, device=self.dev)
         self.n_tpl = self.template_y0.shape[0]
         save = solver.save_times(torch.float32)
@@ -97,7 +107,7 @@ class BasinStabilityPipeline:
         self.queue = torch.zeros((1,), dtype=torch.int64, device=dev)
         self.order = torch.arange(tot, dtype=torch.int32, device=dev)
         self.labels = torch.empty((capacity,), dtype=torch.int32, device=dev)
-        self.counts = torch.empty((1, self.n_classes + 1), dtype=torch.int64, device=dev)
+        self.counts = torch.empty((self.n_groups, self.n_classes + 1), dtype=torch.int64, device=dev)
         rtol, atol = self.solver.effective_tolerances()
         req = SolveRequest(
             system=self.spec.system,
@@ -128,14 +138,18 @@ class BasinStabilityPipeline:
         self._n = None
         self._graph = None
 
-    def _prepare(self, n: int) -> None:
+    def _prepare(self, n: int, group: torch.Tensor | None = None) -> None:
         """Place the templates after the first n rows and size the launch to n + templates."""
         T = self.n_tpl
         self.y0_buf[n : n + T] = self.template_y0
-        self.pidx.zero_()
-        self.pidx[n : n + T] = 1
+        if group is None:
+            self.pidx.zero_()
+        else:
+            self.pidx[:n].copy_(group.to(torch.int32), non_blocking=True)
+        self.pidx[n : n + T] = self.n_groups
         if self.solver.order == "morton" and n > 1:
-            self.order[:n].copy_(spatial_order(self.y0_buf[:n]))
+            grp = self.pidx[:n] if (group is not None and self.n_groups > 1) else None
+            self.order[:n].copy_(spatial_order(self.y0_buf[:n], groups=grp))
         elif self.solver.order == "morton":
             self.order[:n] = torch.arange(n, dtype=torch.int32, device=self.dev)
         self.order[n : n + T] = torch.arange(n, n + T, dtype=torch.int32, device=self.dev)
@@ -161,8 +175,8 @@ class BasinStabilityPipeline:
             self.tpl_class.data_ptr(),
             self.n_classes,
             self.out.status.data_ptr(),
-            None,
-            1,
+            self.pidx.data_ptr() if self.n_groups > 1 else None,
+            self.n_groups,
             self.labels.data_ptr(),
             self.counts.data_ptr(),
             s,
@@ -176,18 +190,27 @@ class BasinStabilityPipeline:
         deferred = self.solver.dense_mode == "deferred"
         return 4 if deferred else 2
 
-    def load_rows(self, y0: torch.Tensor) -> int:
-        """Copy device ICs into the pipeline (growing it if needed); returns n."""
+    def load_rows(self, y0: torch.Tensor, group: torch.Tensor | None = None) -> int:
+        """Copy device ICs (and their parameter points) into the pipeline, growing it if needed."""
         n = y0.shape[0]
+        if group is None and self.n_groups > 1:
+            raise ValueError("a parameter study needs the parameter point (group) of every IC")
+        if group is not None and group.shape[0] != n:
+            raise ValueError("group must hold one entry per IC")
         if getattr(self, "capacity", -1) < n:
             self._allocate(n)
         self.y0_buf[:n].copy_(y0, non_blocking=True)
-        self._prepare(n)
+        self._prepare(n, group)
         return n
 
-    def run_device(self, y0: torch.Tensor, use_graph: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
-        """Label device-resident ``y0`` (N, S) on the current stream; asynchronous."""
-        n = self.load_rows(y0)
+    def run_device(
+        self, y0: torch.Tensor, use_graph: bool = False, group: torch.Tensor | None = None
+    ) -> tuple[torch.Tensor, torch.Tensor]:
+        """Label device-resident ``y0`` (N, S) on the current stream; asynchronous.
+
+        Returns labels (N,) int32 and counts (P, n_classes + 1) int64 (last column:
+        unbounded).  With a parameter study, ``group`` (N,) gives each IC's point."""
+        n = self.load_rows(y0, group)
         if use_graph:
             if self._graph is None:
                 self._capture()
