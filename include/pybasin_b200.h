@@ -71,7 +71,11 @@ typedef enum {
 typedef enum {
     PB_FEAT_MEDIAN = 0, PB_FEAT_MEAN = 1, PB_FEAT_STD = 2, PB_FEAT_VAR = 3, PB_FEAT_RMS = 4,
     PB_FEAT_MAX = 5, PB_FEAT_ABSMAX = 6, PB_FEAT_MIN = 7, PB_FEAT_DELTA = 8,
-    PB_FEAT_LOG_DELTA = 9, PB_FEAT_AMPLITUDE = 10, PB_FEAT_CROSSINGS = 11, PB_FEAT_LAST = 12
+    PB_FEAT_LOG_DELTA = 9, PB_FEAT_AMPLITUDE = 10, PB_FEAT_CROSSINGS = 11, PB_FEAT_LAST = 12,
+    /* network systems: max - min over the nodes of block feat_state (0 x, 1 y, 2 z;
+       3 = the largest of the three) at t1, the synchronisation features of
+       case_studies/rossler_network/synchronization_feature_extractor.py:73-106 */
+    PB_FEAT_SYNC_DEV = 13
 } pb_feature;
 
 /* ---- per-trajectory status written to status_out ---- */

@@ -61,6 +61,7 @@ FEAT_LOG_DELTA = 9
 FEAT_AMPLITUDE = 10
 FEAT_CROSSINGS = 11
 FEAT_LAST = 12
+FEAT_SYNC_DEV = 13
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

@@ -4,6 +4,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include "pb_network.cuh"
 #include "pb_sample.cuh"
 #include "pybasin_b200.h"
 
@@ -265,7 +266,8 @@ static int validate(const pb_solve_args* a)
     int n_cross = 0;
     for (int c = 0; c < a->n_features; ++c) {
         if (a->feat_state[c] < 0 || a->feat_state[c] >= a->dim) return PB_EINVAL;
-        if (a->feat_kind[c] < PB_FEAT_MEDIAN || a->feat_kind[c] > PB_FEAT_LAST) return PB_EINVAL;
+        if (a->feat_kind[c] < PB_FEAT_MEDIAN || a->feat_kind[c] > PB_FEAT_SYNC_DEV) return PB_EINVAL;
+        if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }
     if (n_cross > PB_MAX_CROSSING) return PB_EUNSUPPORTED;
@@ -345,11 +347,33 @@ int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t s
     return PB_SUCCESS;
 }
 
+static int solve_network(const pb_solve_args& a, cudaStream_t st)
+{
+    if (a.dim % 3 != 0 || a.dim / 3 < 1 || a.dim / 3 > kNetMaxNodes) return PB_EINVALID_ODE;
+    if (!a.csr_row || !a.csr_col || a.n_params < 4 || !a.queue_counter) return PB_EINVAL;
+    if (a.y_full_out) return PB_EUNSUPPORTED;  // features come from the final state
+    if (a.n_traj == 0) return PB_SUCCESS;
+    const int n_nodes = a.dim / 3;
+    auto k = a.precision == PB_PREC_FP64 ? k_network<double, 4> : k_network<float, 4>;
+    int dev = 0, sms = 0, bps = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, 128, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return map_cuda(e);
+    int64_t grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
+    const int64_t need = (a.n_traj + 3) / 4;  // 4 warps (trajectories in flight) per block
+    if (grid > need) grid = need;
+    k<<<static_cast<unsigned>(grid), 128, 0, st>>>(a, n_nodes);
+    return map_cuda(cudaGetLastError());
+}
+
 int pb_solve_batch(const pb_solve_args* args, void* stream)
 {
     int v = validate(args);
     if (v != PB_SUCCESS) return v;
     const pb_solve_args& a = *args;
+    if (a.system == PB_SYS_ROSSLER_NET) return solve_network(a, static_cast<cudaStream_t>(stream));
     KernelSel k = find_kernel(a.system, a.dim, a.precision, a.schedule);
     if (!k.plain) return PB_EINVALID_ODE;
     if (a.n_traj == 0) return PB_SUCCESS;

@@ -60,6 +60,11 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
     int64_t off = 0;
     l.median_off = 0;
     off = align_up(a.n_traj * count_median_columns(a) * nwin * static_cast<int64_t>(sizeof(float)), 256);
+    const bool network = a.system == PB_SYS_ROSSLER_NET;  // features from the final state, no windows
+    if (network) {
+        l.total = 0;
+        return l;
+    }
     l.deferred = (a.dense_mode == PB_DENSE_DEFERRED && a.n_features > 0 && a.y_full_out == nullptr) ? 1 : 0;
     if (l.deferred) {
         const int rsize = a.precision == PB_PREC_FP64 ? 8 : 4;

@@ -55,6 +55,8 @@ class SolveRequest:
     order: torch.Tensor | None = None  # (n_traj,) int32 processing order
     dense_mode: int = L.DENSE_DEFERRED
     window_record_cap: int = 0
+    csr_row: torch.Tensor | None = None  # network systems: (n_nodes + 1,) int32
+    csr_col: torch.Tensor | None = None  # network systems: (2 * n_edges,) int32
 
 
 @dataclass
@@ -98,6 +100,8 @@ def build_args(
     a.y0 = _ptr(req.y0)
     a.params = _ptr(req.params)
     a.param_index = _ptr(req.param_index)
+    a.csr_row = _ptr(req.csr_row)
+    a.csr_col = _ptr(req.csr_col)
     a.t0 = float(req.t_span[0])
     a.t1 = float(req.t_span[1])
     a.save_ts = _ptr(req.save_ts)

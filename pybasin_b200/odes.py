@@ -31,6 +31,7 @@ SYSTEM_IDS: dict[str, int] = {
     "duffing": L.SYS_DUFFING,
     "lorenz": L.SYS_LORENZ,
     "lorenz_masked": L.SYS_LORENZ_MASKED,
+    "rossler_network": L.SYS_ROSSLER_NET,
 }
 
 # reference class name -> system (case_studies/*/*_ode.py, tests/unit/solvers/test_solver.py)
@@ -47,6 +48,8 @@ _CLASS_MAP: dict[str, str] = {
     "ExponentialDecayODE": "linear",
     "ExponentialDecayNumpyODE": "linear",
     "LinearODE": "linear",
+    "RosslerNetworkJaxODE": "rossler_network",
+    "RosslerNetworkODE": "rossler_network",
 }
 
 _DIMS: dict[int, tuple[int, ...]] = {
@@ -55,6 +58,7 @@ _DIMS: dict[int, tuple[int, ...]] = {
     L.SYS_DUFFING: (2,),
     L.SYS_LORENZ: (3,),
     L.SYS_LORENZ_MASKED: (3,),
+    L.SYS_ROSSLER_NET: tuple(3 * n for n in range(1, 129)),
 }
 
 

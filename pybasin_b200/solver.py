@@ -286,6 +286,13 @@ class B200Dopri5Solver:
                     order = order.to(torch.int32)
                 else:
                     order = ic_order
+            csr_row = csr_col = None
+            if spec.system == L.SYS_ROSSLER_NET:
+                from pybasin_b200.network import network_csr
+
+                row, col, _ = network_csr(ode_system)
+                csr_row = torch.as_tensor(row, dtype=torch.int32, device=dev)
+                csr_col = torch.as_tensor(col, dtype=torch.int32, device=dev)
             req = SolveRequest(
                 system=spec.system,
                 dim=S,
@@ -310,6 +317,8 @@ class B200Dopri5Solver:
                 grid_blocks=self.grid_blocks,
                 order=order,
                 dense_mode=L.DENSE_DEFERRED if self.dense_mode == "deferred" else L.DENSE_INLINE,
+                csr_row=csr_row,
+                csr_col=csr_col,
             )
             res = solve(req, stream)
             if full:

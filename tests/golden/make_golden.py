@@ -16,6 +16,10 @@ used here) and writes:
 * ``features_reference.npz`` — outputs of the reference's own feature
   calculators (src/pybasin/ts_torch/calculators/torch_features_statistical.py,
   torch_features_pattern.py) on seeded random windows, to pin the statistics.
+* ``rossler_network_reference.npz`` — the reference's 100-node / 400-edge graph
+  (case_studies/rossler_network/rossler_network_topology.py) and the paper's
+  basin-stability values per coupling K it tests against
+  (case_studies/rossler_network/setup_rossler_network_system.py).
 * ``scipy_reference.npz`` — the reference's ScipyParallelSolver
   (src/pybasin/solvers/scipy_solver.py) on a few seeded pendulum and Duffing ICs
   over a short horizon at tight tolerance, to pin trajectories.
@@ -128,6 +132,30 @@ def _scipy(ref: Path) -> None:
     np.savez_compressed(OUT / "scipy_reference.npz", **out)
 
 
+def _rossler(ref: Path) -> None:
+    """The reference's 100-node / 400-edge Rössler graph and the paper's S_B values,
+    read as literals from the case-study sources (their modules import JAX)."""
+    import ast
+
+    def literal(path: Path, name: str):
+        tree = ast.parse(path.read_text())
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == name for t in node.targets):
+                v = node.value
+                if isinstance(v, ast.Call):  # np.array([...])
+                    v = v.args[0]
+                return ast.literal_eval(v)
+        raise KeyError(name)
+
+    cs = ref / "case_studies" / "rossler_network"
+    edges_str = literal(cs / "rossler_network_topology.py", "EDGE_LIST_STR")
+    edges = np.array([[int(a), int(b)] for a, b in (e.split("-") for e in edges_str.split(", "))], dtype=np.int32)
+    k_vals = np.array(literal(cs / "setup_rossler_network_system.py", "K_VALUES_FROM_PAPER"), dtype=np.float64)
+    sb = np.array(literal(cs / "setup_rossler_network_system.py", "EXPECTED_SB_FROM_PAPER"), dtype=np.float64)
+    np.savez_compressed(OUT / "rossler_network_reference.npz", edges=edges, k_values=k_vals, expected_sb=sb,
+                        n_reference=np.int64(500))
+
+
 def main() -> None:
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     _install_stubs()
@@ -149,6 +177,7 @@ def main() -> None:
     )
     _features(ref)
     _scipy(ref)
+    _rossler(ref)
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)
 
