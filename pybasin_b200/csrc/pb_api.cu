@@ -159,7 +159,8 @@ struct KernelSel {
     plain_fn plain_defer = nullptr;  // deferred pass 1
     queue_fn queue = nullptr;        // inline dense output, persistent warps (also the redo pass)
     queue_fn queue_defer = nullptr;  // deferred pass 1, persistent warps
-    plain_fn sample = nullptr;       // deferred pass 2
+    plain_fn sample = nullptr;       // deferred pass 2 (no crossing columns)
+    plain_fn sample_cross = nullptr; // deferred pass 2 with crossing counts
     int smem_per_thread = 0;         // inline kernels: per-thread statistics slot
 };
 
@@ -172,7 +173,8 @@ KernelSel select_prec()
     k.plain_defer = k_solve_plain<Sys, R, true>;
     k.queue = k_solve_queue<Sys, R, false>;
     k.queue_defer = k_solve_queue<Sys, R, true>;
-    k.sample = k_sample<R, Sys::S>;
+    k.sample = k_sample<R, Sys::S, 0>;
+    k.sample_cross = k_sample<R, Sys::S, PB_MAX_CROSSING>;
     return k;
 }
 
@@ -401,9 +403,11 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
         e = cudaGetLastError();
         if (e != cudaSuccess) return map_cuda(e);
         // pass 2: one warp per trajectory evaluates its save points and reduces the statistics
-        const int64_t sblocks = (a.n_traj + 7) / 8;
+        const int64_t sblocks = (a.n_traj + 3) / 4;
         if (sblocks > 0x7fffffffLL) return PB_EINVAL;
-        k.sample<<<static_cast<unsigned>(sblocks), 256, 0, st>>>(a);
+        bool any_cross = false;
+        for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
+        (any_cross ? k.sample_cross : k.sample)<<<static_cast<unsigned>(sblocks), 128, 0, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) return map_cuda(e);
         // pass 3: trajectories that exceeded the record capacity, inline

@@ -1,11 +1,9 @@
 // Second pass of the deferred dense output: evaluate every save point of the
 // feature window from the step records and reduce the window statistics.
 //
-// One warp per trajectory; lane l evaluates save points win_begin + l,
-// win_begin + l + 32, ...  Each lane walks the (time-ordered) records of its
-// trajectory forward to the record that covers its save point, so all 32 lanes
-// stay busy on the same trajectory regardless of how many save points a step
-// covers.  The statistics match the inline path (torch_features_statistical.py
+// One warp per trajectory; lane l takes records l, l + 32, ... of its
+// trajectory and evaluates the save points each record's step covers (no search,
+// no shuffles inside the sample loop).  The statistics match the inline path (torch_features_statistical.py
 // :30-110,:307-318 and torch_features_pattern.py:56-60 of the reference): a
 // shifted sum and sum of squares (shift = first window sample), min, max, last
 // sample, NaN flags and level crossings between consecutive samples, reduced
@@ -96,8 +94,10 @@ __device__ __forceinline__ void fold_samples(SampleAcc<S>& acc, const Plan& pl, 
     }
 }
 
-template <class R, int S>
-__global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
+// NC = crossing states compiled in (0 when no column counts crossings, which
+// keeps the per-lane crossing registers out of the common case).
+template <class R, int S, int NC>
+__global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
 {
     __shared__ Plan pl;
     if (threadIdx.x == 0) build_plan(pl, a);
@@ -132,59 +132,108 @@ __global__ void __launch_bounds__(256) k_sample(const pb_solve_args a)
     }
     acc.shift_set = false;
 
-    // records, 32 at a time: lane i holds record chunk+i (coalesced loads of
-    // consecutive records); the save points they cover are evaluated 32 at a time,
-    // each lane locating its record by a binary search over the lanes' first_save.
+    // records, 32 at a time: lane i takes record chunk+i (coalesced loads of
+    // consecutive records) and evaluates the save points its step covers, in
+    // time order.  Every record covers at least one save point.  Per-record
+    // partial sums are kept in R and folded into the lane's FP64 sums once per
+    // record; crossings between the last sample of one lane and the first of the
+    // next are counted after the loop with one shuffle per crossing state.
     for (int chunk = 0; chunk < nrec; chunk += 32) {
         const int k = chunk + lane;
         const int hl = min(31, nrec - 1 - chunk);  // last lane holding a record
-        double rt = 0.0, rdt = 1.0;
+        const bool have = k < nrec;
+        double rt = 0.0, rdt = 0.0;
         R co[5 * S];
-        int rsi = 0x7fffffff, rn = 0;
-        if (k < nrec) {
+        int rsi = 0, rn = 0;
+#pragma unroll
+        for (int q = 0; q < 5 * S; ++q) co[q] = R(0);
+        if (have) {
             const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
             rt = reinterpret_cast<const double*>(rec)[0];
             rdt = reinterpret_cast<const double*>(rec)[1];
             const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
 #pragma unroll
-            for (int q = 0; q < 5 * S; ++q) {
-                co[q] = R(0);
+            for (int q = 0; q < 5 * S; ++q)
                 if (q < 5 * ns) co[q] = c[q];
-            }
             rsi = reinterpret_cast<const int*>(rec + iw)[0];
             rn = reinterpret_cast<const int*>(rec + iw)[1];
-        } else {
-#pragma unroll
-            for (int q = 0; q < 5 * S; ++q) co[q] = R(0);
         }
-        const int lo = __shfl_sync(0xffffffffu, rsi, 0);
-        const int hi = __shfl_sync(0xffffffffu, rsi + rn, hl);
-        for (int j0 = lo; j0 < hi; j0 += 32) {
-            const int j = j0 + lane;
-            const int nvalid = min(32, hi - j0);
-            // largest record lane r <= hl with first_save <= j
-            int r = 0;
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int cand = r + step;
-                const int sc = __shfl_sync(0xffffffffu, rsi, min(cand, 31));
-                if (cand <= hl && sc <= j) r = cand;
-            }
-            const double t_r = __shfl_sync(0xffffffffu, rt, r);
-            const double idt_r = __shfl_sync(0xffffffffu, rdt, r);
-            const double ts = lane < nvalid ? __ldg(a.save_ts + j) : t_r;
-            const R x = (ts <= t_r + dp::save_slack) ? R(0) : static_cast<R>((ts - t_r) * idt_r);
-            double v[S];
+        if (!acc.shift_set) {  // shift = first window sample = first save of record 0 (lane 0)
+            const double ts = __ldg(a.save_ts + rsi);
+            const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) * rdt);
 #pragma unroll
             for (int q = 0; q < S; ++q) {
-                v[q] = 0.0;
-                if (q >= ns) continue;  // uniform across the warp
-                R c5[5];
-#pragma unroll
-                for (int z = 0; z < 5; ++z) c5[z] = __shfl_sync(0xffffffffu, co[5 * q + z], r);
-                v[q] = static_cast<double>(c5[0] + x * (c5[1] + x * (c5[2] + x * (c5[3] + x * c5[4]))));
+                const R v = co[5 * q] + x * (co[5 * q + 1] + x * (co[5 * q + 2] + x * (co[5 * q + 3] + x * co[5 * q + 4])));
+                const double f = __shfl_sync(0xffffffffu, static_cast<double>(v), 0);
+                acc.sh[q] = isfinite(f) ? f : 0.0;
             }
-            fold_samples(acc, pl, a, traj, nwin, j0, nvalid, v, lane);
+            acc.shift_set = true;
+        }
+        R p1[S], p2[S], pmn[S], pmx[S], sh[S];
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            p1[q] = R(0);
+            p2[q] = R(0);
+            pmn[q] = R(CUDART_INF);
+            pmx[q] = R(-CUDART_INF);
+            sh[q] = static_cast<R>(acc.sh[q]);
+        }
+        double cfirst[NC > 0 ? NC : 1], cprev[NC > 0 ? NC : 1];
+        int ccnt[NC > 0 ? NC : 1];
+#pragma unroll
+        for (int c = 0; c < (NC > 0 ? NC : 1); ++c) {
+            cfirst[c] = 0.0;
+            cprev[c] = 0.0;
+            ccnt[c] = 0;
+        }
+        for (int i = 0; i < rn; ++i) {
+            const int j = rsi + i;
+            const double ts = __ldg(a.save_ts + j);
+            const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) * rdt);
+            R v[S];
+#pragma unroll
+            for (int q = 0; q < S; ++q) {
+                v[q] = R(0);
+                if (q >= ns) continue;  // uniform across the warp
+                v[q] = co[5 * q] + x * (co[5 * q + 1] + x * (co[5 * q + 2] + x * (co[5 * q + 3] + x * co[5 * q + 4])));
+                const R d = v[q] - sh[q];
+                p1[q] += d;
+                p2[q] = fma(d, d, p2[q]);
+                pmn[q] = fmin(pmn[q], v[q]);
+                pmx[q] = fmax(pmx[q], v[q]);
+                if (v[q] != v[q]) acc.nan_flags |= 1 << q;
+                if (j == a.n_save - 1) acc.last[q] = static_cast<double>(v[q]);
+            }
+            for (int m = 0; m < pl.n_med; ++m)
+                median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (j - a.win_begin)] =
+                    static_cast<float>(pick(v, pl.slot_of[pl.med_state[m]]));
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c >= pl.n_cross) break;
+                const double cur = static_cast<double>(pick(v, pl.slot_of[pl.cross_state[c]]));
+                const bool changed = (cur > pl.cross_level[c]) != (cprev[c] > pl.cross_level[c]);
+                ccnt[c] += (i > 0 && changed) ? 1 : 0;
+                cfirst[c] = (i == 0) ? cur : cfirst[c];
+                cprev[c] = cur;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+            acc.s1[q] += static_cast<double>(p1[q]);
+            acc.s2[q] += static_cast<double>(p2[q]);
+            acc.mn[q] = fmin(acc.mn[q], static_cast<double>(pmn[q]));
+            acc.mx[q] = fmax(acc.mx[q], static_cast<double>(pmx[q]));
+        }
+        // crossings across record boundaries: lane l's first sample against lane
+        // l-1's last (lane 0 against the carry from the previous chunk)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (c >= pl.n_cross) break;
+            double prev = __shfl_up_sync(0xffffffffu, cprev[c], 1);
+            if (lane == 0) prev = acc.carry[c];
+            const bool changed = (cfirst[c] > pl.cross_level[c]) != (prev > pl.cross_level[c]);
+            acc.cross_cnt[c] += ccnt[c] + ((have && rsi > a.win_begin && changed) ? 1 : 0);
+            acc.carry[c] = __shfl_sync(0xffffffffu, cprev[c], hl);
         }
     }
     // save points after the last record: the trajectory stopped (or t1 was reached

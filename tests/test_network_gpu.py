@@ -56,11 +56,18 @@ def _solve(y0, params, csr, t1, rtol, atol, precision, save=None, group=None, un
 
 def test_fp64_network_matches_oracle_short_horizon():
     csr, _ = _graph()
+    # ICs near the attractor (x, y in [-5, 5], z in [0, 2]); from the sampler's full box
+    # many trajectories blow up in finite time, which the unbounded test covers
     y0 = _ics(16, 1).double()
+    y0[:, : 2 * N_NODES] /= 3.0
+    y0[:, 2 * N_NODES :] = (y0[:, 2 * N_NODES :] + 5.0) / 20.0
     p = np.array([[0.2, 0.2, 7.0, 0.218]])
-    r = _solve(y0, p, csr, 5.0, 1e-9, 1e-9, L.PREC_FP64)
+    # threshold off: every trajectory runs to t1 and is compared in full
+    r = _solve(y0, p, csr, 5.0, 1e-9, 1e-9, L.PREC_FP64, unb=0.0)
     want = O.solve_batch(O.SYS_ROSSLER_NET, y0.numpy(), p, np.array([5.0]), (0.0, 5.0), 1e-9, 1e-9, csr=csr)
-    assert (r.status.cpu().numpy() == 0).all()
+    assert (r.status.cpu().numpy() == 0).all() and (want["status"] == 0).all()
+    # the warp-reduced error norm sums in another order: a marginal accept may flip
+    assert np.abs(r.steps.cpu().numpy() - want["steps"]).max() <= 2
     np.testing.assert_allclose(r.y_final.cpu().numpy(), want["y_final"], rtol=1e-7, atol=1e-7)
     # features: max - min over nodes at the final state
     yf = want["y_final"].reshape(16, 3, N_NODES)
@@ -68,6 +75,20 @@ def test_fp64_network_matches_oracle_short_horizon():
     f = r.features.cpu().numpy()
     np.testing.assert_allclose(f[:, :3], dev, rtol=1e-6, atol=1e-6)
     np.testing.assert_allclose(f[:, 3], dev.max(axis=1), rtol=1e-6, atol=1e-6)
+
+
+def test_unbounded_stop_matches_oracle():
+    csr, _ = _graph()
+    y0 = _ics(64, 5).double()
+    p = np.array([[0.2, 0.2, 7.0, 0.218]])
+    r = _solve(y0, p, csr, 20.0, 1e-8, 1e-8, L.PREC_FP64, unb=400.0)
+    want = O.solve_batch(O.SYS_ROSSLER_NET, y0.numpy(), p, np.array([20.0]), (0.0, 20.0), 1e-8, 1e-8, csr=csr,
+                         unbounded_thr=400.0)
+    st = r.status.cpu().numpy()
+    assert (st == L.TRAJ_UNBOUNDED).any() and (st == L.TRAJ_OK).any()
+    np.testing.assert_array_equal(st, want["status"])
+    f = r.features.cpu().numpy()
+    assert np.isinf(f[st == L.TRAJ_UNBOUNDED]).all() and np.isfinite(f[st == L.TRAJ_OK]).all()
 
 
 def test_mixed_network_labels_agree_with_fp64():
@@ -122,3 +143,31 @@ def test_invalid_graph_is_reported_not_read():
     bad_col[5] = 1000  # a neighbour outside the graph
     r = _solve(_ics(4, 3), np.array([[0.2, 0.2, 7.0, 0.2]]), (csr[0], bad_col), 1.0, 1e-3, 1e-6, L.PREC_MIXED)
     assert (r.status.cpu().numpy() == L.TRAJ_BAD_INPUT).all()
+
+
+def test_solver_drop_in_with_sync_extractor():
+    """B200Dopri5Solver.integrate on a network ODE object, features read by SyncFeatureExtractor."""
+    from pybasin_b200 import B200Dopri5Solver
+    from pybasin_b200.network import RosslerNetworkODE, SyncFeatureExtractor, sync_labels
+
+    csr, g = _graph()
+    ode = RosslerNetworkODE({"a": 0.2, "b": 0.2, "c": 7.0, "K": 0.218}, N_NODES, g["edges"])
+    ext = SyncFeatureExtractor(N_NODES)
+    solver = B200Dopri5Solver(t_span=(0, 200), t_steps=200, device="cuda", rtol=1e-3, atol=1e-6,
+                              precision="mixed", feature_extractor=ext, unbounded_threshold=400.0)
+    y0 = _ics(256, 9)
+    t, y = solver.integrate(ode, y0)
+    feats = ext.extract_features(types_ns(y))
+    assert feats.shape == (256, 4) and t.shape == (1,)
+    direct = _solve(y0, np.array([[0.2, 0.2, 7.0, 0.218]]), csr, 200.0, 1e-3, 1e-6, L.PREC_MIXED,
+                    save=np.linspace(0, 200, 200), keep_final=False)
+    # same kernel, same inputs: identical features and statuses (processing order does not matter)
+    np.testing.assert_array_equal(feats.cpu().numpy(), direct.features.float().cpu().numpy())
+    lab = sync_labels(feats, y._pb_status)
+    assert set(lab) <= {"synchronized", "desynchronized", "unbounded"}
+
+
+def types_ns(y):
+    from types import SimpleNamespace
+
+    return SimpleNamespace(y=y)
