@@ -351,29 +351,32 @@ def run_b200_arm(args) -> None:
     # 50,000 integrator labels of separately seeded ICs, then gated passes
     from pybasin_b200.gated import SurrogateGatedPipeline
 
-    gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01)
-    hist, tinfo = gated.train(seeded_ics(50_000, 1042 + rank).to(dev), epochs=80, batch=512, lr=2e-3)
-    for _ in range(args.warmup):
-        gated.run_device(y0_dev)
-    torch.cuda.synchronize()
-    if dist_on:
-        torch.distributed.barrier()
-    g_times, g_stats = [], []
-    for i in range(args.steps):
-        flush.fill_(i)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        lab_g, cnt_g, st_g = gated.run_device(y0_dev)
-        e1.record()
+    gated = None
+    if not args.no_surrogate:
+        gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01)
+        hist, tinfo = gated.train(seeded_ics(50_000, 1042 + rank).to(dev), epochs=80, batch=512, lr=2e-3)
+        for _ in range(args.warmup):
+            gated.run_device(y0_dev)
         torch.cuda.synchronize()
-        g_times.append(e0.elapsed_time(e1))
-        g_stats.append(st_g)
-    (ms_g,) = max_over_ranks([statistics.mean(g_times)], dev, dist_on)
-    counts_g = global_counts(cnt_g.view(1, -1), dist_on)
-    dbs_g = (counts_g[:5].double() - counts64[:5].double()).abs().max().item() / n_all
-    agree_g = float((lab_g == labels64).float().mean())
-    value_gated = n_all / (ms_g / 1000.0)
-    use_gate = dbs_g <= 0.005 and value_gated > value_fused
+        if dist_on:
+            torch.distributed.barrier()
+        g_times, g_stats = [], []
+        for i in range(args.steps):
+            flush.fill_(i)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            lab_g, cnt_g, st_g = gated.run_device(y0_dev)
+            e1.record()
+            torch.cuda.synchronize()
+            g_times.append(e0.elapsed_time(e1))
+            g_stats.append(st_g)
+        (ms_g,) = max_over_ranks([statistics.mean(g_times)], dev, dist_on)
+        counts_g = global_counts(cnt_g.view(1, -1), dist_on)
+        dbs_g = (counts_g[:5].double() - counts64[:5].double()).abs().max().item() / n_all
+        agree_g = float((lab_g == labels64).float().mean())
+        value_gated = n_all / (ms_g / 1000.0)
+
+    use_gate = gated is not None and dbs_g <= 0.005 and value_gated > value_fused
     value = value_gated if use_gate else value_fused
     ms_pass = ms_g if use_gate else ms
 
@@ -448,7 +451,7 @@ def run_b200_arm(args) -> None:
             "label_agreement_vs_fp64": agree_g if use_gate else agree,
             "fused_fp32": {"value": value_fused, "ms_per_step": ms, "delta_bs_vs_fp64": dbs,
                            "label_agreement_vs_fp64": agree},
-            "surrogate": {
+            "surrogate": None if gated is None else {
                 "value": value_gated,
                 "ms_per_step": ms_g,
                 "delta_bs_vs_fp64": dbs_g,
@@ -507,6 +510,7 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="time the fused integrator path alone")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

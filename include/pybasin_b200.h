@@ -197,6 +197,19 @@ int pb_label_nearest(const double* features, int64_t n, int32_t n_features,
                      int32_t n_classes, const int32_t* status, const int32_t* group_of,
                      int32_t n_groups, int32_t* labels_out, int64_t* counts_out, void* stream);
 
+/* Z-order (Morton) keys of the ICs over their bounding box: argsort of the keys
+ * is the processing order passed as pb_solve_args.order (neighbouring ICs mostly
+ * share an attractor and a step count, so a warp's lanes finish together).
+ * No reference counterpart: the reference integrates in batch order.
+ *   y0        device (n, dim) f32 or f64 (y0_dtype), row-major
+ *   bits      bits per coordinate of the first min(dim, 4) coordinates, bits*min(dim,4) <= 62
+ *   groups    optional device (n,) int32: keys become group-major (group << 40 | top 40 key bits)
+ *   bbox_work device scratch of 8 uint64, overwritten on `stream`
+ *   keys_out  device (n,) int64
+ * NaN coordinates do not widen the bounding box and quantise to 0. */
+int pb_morton_keys(const void* y0, int32_t y0_dtype, int64_t n, int32_t dim, int32_t bits,
+                   const int32_t* groups, uint64_t* bbox_work, int64_t* keys_out, void* stream);
+
 /* Occupancy helper for the autotuner: resident blocks per SM of the pb_solve_batch
  * kernel selected by (system, dim, precision, schedule) at `block_size`. */
 int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule,

@@ -151,6 +151,7 @@ EXPORTED_SYMBOLS = (
     "pb_abi_version",
     "pb_probe_fma",
     "pb_solve_batch_noalloc",
+    "pb_morton_keys",
 )
 
 
@@ -182,6 +183,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         lib.pb_label_nearest.argtypes = [
             _c_vp, _c_i64, _c_i32, _c_vp, _c_i32, _c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp, _c_vp, _c_vp,
         ]
+        lib.pb_morton_keys.restype = ctypes.c_int
+        lib.pb_morton_keys.argtypes = [_c_vp, _c_i32, _c_i64, _c_i32, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp]
         lib.pb_query_occupancy.restype = ctypes.c_int
         lib.pb_query_occupancy.argtypes = [
             _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32),

@@ -171,9 +171,19 @@ struct Lane {
     double next_save;  // save_ts[si] (or +inf past the end)
     int si;            // next save index
     int steps;
+    int max_steps;     // a.max_steps clamped to int range (a 32-bit compare per step)
     int status;
     int nrec;          // deferred dense output: records written (-1 = capacity exceeded)
 };
+
+// 2^x by the hardware approximation (ex2.approx.ftz.f32, relative error ~2^-22):
+// ample for a step-size factor that is clamped to [0.2, 10] afterwards
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 __device__ __forceinline__ double load_save(const pb_solve_args& a, int si)
 {
@@ -298,6 +308,7 @@ struct Integrator {
             L.p[q] = q < a.n_params ? static_cast<R>(__ldg(a.params + prow * a.n_params + q)) : R(0);
         L.t = bad_row ? a.t1 : a.t0;  // a bad row finishes without stepping
         L.steps = 0;
+        L.max_steps = static_cast<int>(a.max_steps < 0x7fffffffLL ? a.max_steps : 0x7fffffffLL);
         L.status = bad_row ? PB_TRAJ_BAD_INPUT : PB_TRAJ_OK;
         L.si = a.y_full_out ? 0 : a.win_begin;
         L.next_save = load_save(a, L.si);
@@ -451,11 +462,12 @@ struct Integrator {
     template <bool DEFER>
     __device__ static bool step(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
     {
-        if (!(L.t < a.t1) || L.steps >= a.max_steps) return true;
+        if (!(L.t < a.t1) || L.steps >= L.max_steps) return true;
         L.steps++;
         double dt = L.dt;
         if (L.t + dt > a.t1) dt = a.t1 - L.t;
-        if (dt <= 0.0) return true;
+        // dt > 0 here (t < t1, and the control keeps dt * fac with fac >= 0.2);
+        // a dt lost below t's resolution (including 0) ends the trajectory
         if (L.t + dt == L.t) {
             L.status = PB_TRAJ_DT_UNDERFLOW;
             return true;
@@ -573,7 +585,7 @@ struct Integrator {
         double fac;
         if (MIXED) {
             const float e2f = static_cast<float>(err2);
-            const float g = 0.9f * exp2f(-0.1f * __log2f(e2f));  // 0.9 * err^-0.2 with err^2 = e2f
+            const float g = 0.9f * ex2_approx(-0.1f * __log2f(e2f));  // 0.9 * err^-0.2 with err^2 = e2f
             fac = (err2 == 0.0) ? dp::max_factor : static_cast<double>(fminf(10.f, fmaxf(accept ? 1.f : 0.2f, g)));
         } else {
             const double err = sqrt(err2);
@@ -588,7 +600,7 @@ struct Integrator {
     template <bool DEFER>
     __device__ static void finish(L_t& L, St& st, const Plan& pl, int64_t traj, const pb_solve_args& a)
     {
-        if (L.status == PB_TRAJ_OK && L.t < a.t1 && L.steps >= a.max_steps) L.status = PB_TRAJ_MAX_STEPS;
+        if (L.status == PB_TRAJ_OK && L.t < a.t1 && L.steps >= L.max_steps) L.status = PB_TRAJ_MAX_STEPS;
         if (DEFER) {
             // the sampling pass evaluates the records and fills the uncovered tail
             unsigned char* tl = tail_ptr(a, pl.sl, traj);

@@ -244,17 +244,10 @@ def _spread_bits(v: torch.Tensor, dims: int, bits: int) -> torch.Tensor:
     return out
 
 
-def spatial_order(y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
-    """Permutation of the rows of ``y0`` along a Morton (Z-order) curve of its bounding box.
-
-    Neighbouring initial conditions mostly share an attractor and a step count, so
-    integrating them in the same warp keeps the warp's lanes busy together.  With
-    ``groups`` (e.g. the parameter row of each IC) the order is group-major, so a
-    warp does not mix parameter points.  Returns int32 indices on y0's device.
-    """
+def morton_keys(y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
+    """Z-order keys of the rows of ``y0`` over their bounding box (PyTorch ops; the
+    host-side statement of ``pb_morton_keys``, which is bit-identical on finite input)."""
     n, dims = y0.shape
-    if n == 0:
-        return torch.zeros((0,), dtype=torch.int32, device=y0.device)
     d = min(dims, 4)
     bits = bits or max(1, 60 // d if d > 2 else 20)
     bits = min(bits, 62 // d)
@@ -268,4 +261,53 @@ def spatial_order(y0: torch.Tensor, bits: int | None = None, groups: torch.Tenso
     if groups is not None:
         # group-major: 20 bits of group id above 40 bits of (truncated) Morton key
         key = (groups.to(torch.int64) << 40) | (key >> max(0, bits * d - 40))
-    return torch.argsort(key).to(torch.int32)
+    return key
+
+
+def spatial_order(y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
+    """Permutation of the rows of ``y0`` along a Morton (Z-order) curve of its bounding box.
+
+    Neighbouring initial conditions mostly share an attractor and a step count, so
+    integrating them in the same warp keeps the warp's lanes busy together.  With
+    ``groups`` (e.g. the parameter row of each IC) the order is group-major, so a
+    warp does not mix parameter points.  Returns int32 indices on y0's device.
+    On CUDA tensors :class:`MortonOrder` computes the same keys in two kernels.
+    """
+    if y0.shape[0] == 0:
+        return torch.zeros((0,), dtype=torch.int32, device=y0.device)
+    return torch.argsort(morton_keys(y0, bits, groups)).to(torch.int32)
+
+
+class MortonOrder:
+    """Device Z-order of the ICs (``pb_morton_keys`` + argsort), with its buffers
+    kept between calls; keys are bit-identical to :func:`spatial_order`'s."""
+
+    def __init__(self, device: torch.device):
+        self.dev = torch.device(device)
+        self.box = torch.empty((8,), dtype=torch.int64, device=self.dev)
+        self.keys = torch.empty((0,), dtype=torch.int64, device=self.dev)
+
+    def keys_of(self, y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
+        n, dims = y0.shape
+        d = min(dims, 4)
+        bits = bits or max(1, 60 // d if d > 2 else 20)
+        bits = min(bits, 62 // d)
+        if self.keys.shape[0] < n:
+            self.keys = torch.empty((n,), dtype=torch.int64, device=self.dev)
+        if y0.dtype not in (torch.float32, torch.float64) or not y0.is_contiguous():
+            y0 = y0.contiguous().to(torch.float64 if y0.dtype == torch.float64 else torch.float32)
+        g = None
+        if groups is not None:
+            g = groups.to(torch.int32).contiguous()
+        rc = L.load().pb_morton_keys(
+            y0.data_ptr(), L.DTYPE_F64 if y0.dtype == torch.float64 else L.DTYPE_F32, n, dims, bits,
+            g.data_ptr() if g is not None else None, self.box.data_ptr(), self.keys.data_ptr(),
+            torch.cuda.current_stream(self.dev).cuda_stream,
+        )
+        L.check(rc, "pb_morton_keys")
+        return self.keys[:n]
+
+    def __call__(self, y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
+        if y0.shape[0] == 0:
+            return torch.zeros((0,), dtype=torch.int32, device=self.dev)
+        return torch.argsort(self.keys_of(y0, bits, groups)).to(torch.int32)

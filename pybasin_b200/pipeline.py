@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import SolveRequest, SolveResult, alloc_scratch, build_args, spatial_order
+from pybasin_b200.engine import MortonOrder, SolveRequest, SolveResult, alloc_scratch, build_args
 from pybasin_b200.odes import resolve_system
 from pybasin_b200.solver import B200Dopri5Solver
 
@@ -76,6 +76,7 @@ class BasinStabilityPipeline:
         # rows 0..P-1: parameter points; row P: the templates' parameters
         self.params = torch.tensor(np.vstack([rows, tparams[None]]), dtype=torch.float64, device=self.dev)
         self.template_y0 = torch.tensor(template_y0, dtype=torch.float32, device=self.dev)
+        self.morton = MortonOrder(self.dev)
         self.n_tpl = self.template_y0.shape[0]
         save = solver.save_times(torch.float32)
         self.save_ts = save.to(torch.float64).to(self.dev)
@@ -149,7 +150,7 @@ class BasinStabilityPipeline:
         self.pidx[n : n + T] = self.n_groups
         if self.solver.order == "morton" and n > 1:
             grp = self.pidx[:n] if (group is not None and self.n_groups > 1) else None
-            self.order[:n].copy_(spatial_order(self.y0_buf[:n], groups=grp))
+            self.order[:n].copy_(self.morton(self.y0_buf[:n], groups=grp))
         elif self.solver.order == "morton":
             self.order[:n] = torch.arange(n, dtype=torch.int32, device=self.dev)
         self.order[n : n + T] = torch.arange(n, n + T, dtype=torch.int32, device=self.dev)

@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import SolveRequest, solve, spatial_order
+from pybasin_b200.engine import MortonOrder, SolveRequest, solve
 from pybasin_b200.features import FusedFeatureExtractor
 from pybasin_b200.odes import resolve_system
 
@@ -280,7 +280,7 @@ class B200Dopri5Solver:
             save_dev = save_f64.to(dev)
             order = None
             if self.order == "morton" and B > 1:
-                ic_order = spatial_order(y0_dev)
+                ic_order = MortonOrder(dev)(y0_dev)
                 if params is not None:
                     order = (ic_order.to(torch.int64)[:, None] * P + torch.arange(P, device=dev)).reshape(-1)
                     order = order.to(torch.int32)

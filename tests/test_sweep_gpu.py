@@ -115,3 +115,22 @@ def test_lorenz_rho_sweep_with_unbounded_threshold():
     # rho = 28 is chaotic: pointwise values decorrelate; the attractor's statistics agree
     chaos = group == 2
     assert abs(f[chaos][:, 1].mean() - want["features"][chaos][:, 1].mean()) < 0.5
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("dim", [1, 2, 3, 5])
+def test_device_morton_keys_match_host_statement(dtype, dim):
+    from pybasin_b200.engine import MortonOrder, morton_keys
+
+    g = torch.Generator().manual_seed(dim)
+    y0 = (torch.rand(20_011, dim, generator=g, dtype=torch.float64) * 7.0 - 3.0).to(dtype)
+    groups = torch.randint(0, 9, (20_011,), generator=g, dtype=torch.int32)
+    mo = MortonOrder(torch.device("cuda:0"))
+    for grp in (None, groups):
+        want = morton_keys(y0, groups=grp)
+        got = mo.keys_of(y0.cuda(), groups=None if grp is None else grp.cuda()).cpu()
+        assert torch.equal(got, want)
+    # a constant coordinate (zero span)
+    y1 = y0.clone()
+    y1[:, 0] = 1.5
+    assert torch.equal(mo.keys_of(y1.cuda()).cpu(), morton_keys(y1))
