@@ -317,7 +317,7 @@ struct Integrator {
 
         // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
         if (MIXED) {
-            Sys::f(ClockF32{reduce_two_pi(a.t0)}, L.y, L.k1, L.p);
+            Sys::f(ClockF32{reduce_two_pi(a.t0, 0.0)}, L.y, L.k1, L.p);
         } else {
             Sys::f(ClockF64{a.t0}, L.y, L.k1, L.p);
         }
@@ -337,7 +337,7 @@ struct Integrator {
 #pragma unroll
         for (int s = 0; s < S; ++s) ytmp[s] = static_cast<R>(y0d[s] + h0 * static_cast<double>(L.k1[s]));
         if (MIXED) {
-            Sys::f(ClockF32{reduce_two_pi(a.t0 + h0)}, ytmp, ftmp, L.p);
+            Sys::f(ClockF32{reduce_two_pi(a.t0 + h0, 0.0)}, ytmp, ftmp, L.p);
         } else {
             Sys::f(ClockF64{a.t0 + h0}, ytmp, ftmp, L.p);
         }
@@ -364,15 +364,24 @@ struct Integrator {
         // first save index after (t, tn]: probe where a uniform grid would put it,
         // then correct (the grid is not assumed uniform, only used as a hint)
         const double lim = tn + dp::save_slack;
-        int si = L.si;
+        int si;
+        double ts;
         {
-            const int guess = L.si + 1 + static_cast<int>(fmax(0.0, (lim - L.next_save) * pl.inv_ds));
-            int g = min(guess, a.n_save);
-            while (g > L.si + 1 && !(load_save(a, g - 1) <= lim)) --g;  // move down to a covered index
-            while (g < a.n_save && load_save(a, g) <= lim) ++g;         // move up past the covered run
-            si = g;
+            const int guess = min(L.si + 1 + static_cast<int>(fmax(0.0, (lim - L.next_save) * pl.inv_ds)), a.n_save);
+            // both neighbours of the guess in one round trip; exact for a uniform grid
+            const double below = guess > L.si + 1 ? load_save(a, guess - 1) : L.next_save;
+            const double above = load_save(a, guess);
+            if (below <= lim && !(above <= lim)) {
+                si = guess;
+                ts = above;
+            } else {
+                int g = guess;
+                while (g > L.si + 1 && !(load_save(a, g - 1) <= lim)) --g;  // move down to a covered index
+                while (g < a.n_save && load_save(a, g) <= lim) ++g;         // move up past the covered run
+                si = g;
+                ts = load_save(a, si);
+            }
         }
-        const double ts = load_save(a, si);
         // assemble the record as 32-bit words, then store it with 16-byte vector stores
         constexpr int RW = sizeof(R) / 4;
         constexpr int kWords = (kRecordHeader + 5 * S * static_cast<int>(sizeof(R)) + 8 + 15) / 16 * 4;
@@ -476,7 +485,7 @@ struct Integrator {
         const double t = L.t;
         R k2[S], k3[S], k4[S], k5[S], k6[S], k7[S], d[S], yn[S];
         if (MIXED) {
-            const float r0 = Sys::kTime ? reduce_two_pi(t) : 0.f;
+            const float r0 = Sys::kTime ? reduce_two_pi(t, dt) : 0.f;
             stages(TimeBaseF32{r0, static_cast<float>(h)}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
         } else {
             stages(TimeBaseF64{t, dt}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
@@ -493,13 +502,8 @@ struct Integrator {
                          R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
                 const float sc =
                     fmaf(rt, fmaxf(fabsf(static_cast<float>(L.y[s])), fabsf(static_cast<float>(yn[s]))), at);
-#ifdef PB_ERRNORM_F32
-                const float r = __fdividef(e, sc);
-                err2 = static_cast<double>(fmaf(r, r, static_cast<float>(err2)));
-#else
                 const double r = static_cast<double>(__fdividef(e, sc));
                 err2 = fma(r, r, err2);
-#endif
             }
             err2 *= 1.0 / S;
         } else {

@@ -25,12 +25,11 @@ __device__ __forceinline__ double clock_cos(const ClockF64& c) { return cos(c.t)
 __device__ __forceinline__ float clock_cos(const ClockF32& c)
 {
 #ifndef PB_ACCURATE_COS
-    // phase lies in [-pi, pi + h]; fold it back into [-pi, pi], where the hardware
-    // cosine's absolute error is below 2^-21.4 (about 3.6e-7, below the FP32 stage
-    // resolution of a unit-scale state)
-    const float two_pi = 6.28318530717958647692f;
-    const float r = c.phase > 3.14159265358979323846f ? c.phase - two_pi : c.phase;
-    return __cosf(r);
+    // the step's phases lie in [-pi - h/2, pi + h/2] (reduction centred on the step
+    // midpoint, TimeBaseF32); measured max |__cosf(x) - cos(x)| on B200 is 4.0e-7
+    // for |x| <= pi, 4.2e-7 for |x| <= pi + 1 (h <= 2) and 7.1e-7 for |x| <= 2 pi,
+    // at or below the FP32 stage resolution of a unit-scale state
+    return __cosf(c.phase);
 #else
     return cosf(c.phase);
 #endif
@@ -50,11 +49,13 @@ struct TimeBaseF32 {
     float r0, h;  // t mod 2*pi (FP64-reduced, then rounded), FP32 step
     __device__ __forceinline__ ClockF32 at(double c) const { return ClockF32{r0 + static_cast<float>(c) * h}; }
 };
-__device__ __forceinline__ float reduce_two_pi(double t)
+// t - 2*pi*k with k the nearest integer to (t + dt/2) / (2*pi): the stage phases
+// t + c*dt - 2*pi*k (0 <= c <= 1) then lie within pi + dt/2 of zero
+__device__ __forceinline__ float reduce_two_pi(double t, double dt)
 {
     const double two_pi = 6.283185307179586476925286766559;
     const double inv_two_pi = 0.15915494309189533576888376337251;
-    const double k = rint(t * inv_two_pi);
+    const double k = rint(fma(0.5, dt, t) * inv_two_pi);
     return static_cast<float>(fma(-k, two_pi, t));
 }
 
