@@ -97,8 +97,15 @@ typedef enum { PB_DTYPE_F32 = 0, PB_DTYPE_F64 = 1 } pb_dtype;
 /* Work distribution of pb_solve_batch. */
 typedef enum {
     PB_SCHED_PLAIN = 0,  /* one thread per trajectory, grid covers all trajectories */
-    PB_SCHED_QUEUE = 1   /* persistent lanes refilled from a global atomic queue with
+    PB_SCHED_QUEUE = 1,  /* persistent lanes refilled from a global atomic queue with
                             warp-aggregated fetches (needs `queue_counter`) */
+    PB_SCHED_PROBED = 2  /* the queue in predicted-cost order: every trajectory first
+                            integrates the first 5 % of [t0, t1] (its step count there
+                            predicts its total), the trajectories are sorted longest
+                            first (stably, so `order` is kept within equal counts) and
+                            resumed from their saved state; results are identical to
+                            PB_SCHED_QUEUE.  Applies with deferred dense output; other
+                            requests run as PB_SCHED_QUEUE.  Needs `queue_counter`. */
 } pb_schedule;
 
 typedef struct pb_solve_args {

@@ -41,6 +41,8 @@ LAYOUT_INDEXED = 2
 
 SCHED_PLAIN = 0
 SCHED_QUEUE = 1
+SCHED_PROBED = 2
+SCHEDULES = {"plain": SCHED_PLAIN, "queue": SCHED_QUEUE, "probed": SCHED_PROBED}
 
 DENSE_INLINE = 0
 DENSE_DEFERRED = 1

@@ -10,7 +10,9 @@ one full pass on the caller's own ICs and keeps the fastest:
   balancing: an SM whose tasks happen to be long finishes last); fewer blocks
   make warps come back to the queue, which balances the SMs at the price of
   fewer warps in flight;
-* ``dense_mode`` — deferred (step records + sampling pass) or inline.
+* ``dense_mode`` — deferred (step records + sampling pass) or inline;
+* ``schedule`` — the queue in processing order, or probed (a probe over the
+  first 5 % of the span orders the trajectories longest first).
 
 Tuning time is reported, never part of a timed pass.  Results are cached in
 memory and, with ``path``, in a JSON file.
@@ -34,6 +36,7 @@ class LaunchShape:
     block_size: int
     grid_blocks: int  # 0 = one block per block_size trajectories (every warp one task)
     dense_mode: str  # "deferred" | "inline"
+    schedule: str = "queue"  # "queue" | "probed"
 
 
 @dataclass
@@ -49,19 +52,27 @@ def sm_count(dev: torch.device) -> int:
     return torch.cuda.get_device_properties(dev).multi_processor_count
 
 
-def candidate_shapes(n_traj: int, sms: int, dense_modes: tuple[str, ...] = ("deferred",)) -> list[LaunchShape]:
+def candidate_shapes(
+    n_traj: int,
+    sms: int,
+    dense_modes: tuple[str, ...] = ("deferred",),
+    schedules: tuple[str, ...] = ("queue", "probed"),
+) -> list[LaunchShape]:
     """Block sizes 64/128/256 x grids from one task per warp down to ~1.5 SM-waves."""
     out: list[LaunchShape] = []
-    for mode in dense_modes:
-        for bs in (64, 128, 256):
-            need = math.ceil(n_traj / bs)
-            grids = {0}
-            for frac in (0.75, 0.5, 0.33, 0.25):
-                g = int(need * frac)
-                if g >= sms:
-                    grids.add(g)
-            for g in sorted(grids, reverse=True):
-                out.append(LaunchShape(bs, g, mode))
+    for sched in schedules:
+        for mode in dense_modes:
+            if sched == "probed" and mode != "deferred":
+                continue  # the probed schedule applies to deferred dense output
+            for bs in (64, 128, 256):
+                need = math.ceil(n_traj / bs)
+                grids = {0}
+                for frac in (0.75, 0.5, 0.33, 0.25):
+                    g = int(need * frac)
+                    if g >= sms:
+                        grids.add(g)
+                for g in sorted(grids, reverse=True):
+                    out.append(LaunchShape(bs, g, mode, sched))
     return out
 
 
@@ -87,9 +98,10 @@ def _load(path: Path | None) -> dict[str, dict]:
 def _apply(pipe: Any, shape: LaunchShape) -> None:
     pipe.solver.block_size = shape.block_size
     pipe.solver.grid_blocks = shape.grid_blocks
-    if pipe.solver.dense_mode != shape.dense_mode:
+    if pipe.solver.dense_mode != shape.dense_mode or pipe.solver.schedule != shape.schedule:
         pipe.solver.dense_mode = shape.dense_mode
-        pipe._allocate(pipe.capacity)  # scratch layout depends on the dense-output mode
+        pipe.solver.schedule = shape.schedule
+        pipe._allocate(pipe.capacity)  # the scratch layout depends on both
     pipe.args.block_size = shape.block_size
     pipe.args.grid_blocks = shape.grid_blocks
     pipe._graph = None
@@ -129,8 +141,8 @@ def tune_pipeline(
         best = LaunchShape(**ent["best"])
         _apply(pipe, best)
         return TuneResult(best, ent["best_ms"], [], 0.0, key)
-    if pipe.solver.schedule != "queue":
-        raise ValueError("launch-shape tuning applies to the queue schedule")
+    if pipe.solver.schedule not in ("queue", "probed"):
+        raise ValueError("launch-shape tuning applies to the queue and probed schedules")
     cands = candidates or candidate_shapes(pipe.args.n_traj, sm_count(pipe.dev))
     t0 = time.perf_counter()
     table: list[tuple[LaunchShape, float]] = []

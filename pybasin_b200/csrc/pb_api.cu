@@ -4,6 +4,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "pb_network.cuh"
 #include "pb_sample.cuh"
 #include "pybasin_b200.h"
@@ -159,6 +161,8 @@ struct KernelSel {
     plain_fn plain_defer = nullptr;  // deferred pass 1
     queue_fn queue = nullptr;        // inline dense output, persistent warps (also the redo pass)
     queue_fn queue_defer = nullptr;  // deferred pass 1, persistent warps
+    queue_fn queue_probe = nullptr;  // deferred pass 1, probed schedule: probe phase
+    queue_fn queue_main = nullptr;   // deferred pass 1, probed schedule: main phase
     plain_fn sample = nullptr;       // deferred pass 2 (no crossing columns)
     plain_fn sample_cross = nullptr; // deferred pass 2 with crossing counts
     int smem_per_thread = 0;         // inline kernels: per-thread statistics slot
@@ -173,6 +177,8 @@ KernelSel select_prec()
     k.plain_defer = k_solve_plain<Sys, R, true>;
     k.queue = k_solve_queue<Sys, R, false>;
     k.queue_defer = k_solve_queue<Sys, R, true>;
+    k.queue_probe = k_solve_queue<Sys, R, true, 1>;
+    k.queue_main = k_solve_queue<Sys, R, true, 2>;
     k.sample = k_sample<R, Sys::S, 0>;
     k.sample_cross = k_sample<R, Sys::S, PB_MAX_CROSSING>;
     return k;
@@ -187,7 +193,7 @@ KernelSel select_kernel(int precision)
 static KernelSel find_kernel(int system, int dim, int precision, int schedule)
 {
     if (precision != PB_PREC_FP64 && precision != PB_PREC_MIXED) return {};
-    if (schedule != PB_SCHED_PLAIN && schedule != PB_SCHED_QUEUE) return {};
+    if (schedule != PB_SCHED_PLAIN && schedule != PB_SCHED_QUEUE && schedule != PB_SCHED_PROBED) return {};
     switch (system) {
         case PB_SYS_LINEAR:
             switch (dim) {
@@ -230,6 +236,35 @@ static cudaError_t persistent_grid(F fn, int block, int smem, int64_t n_traj, in
     const int64_t need = (n_traj + block - 1) / block;
     if (*grid > need) *grid = need;
     return cudaSuccess;
+}
+
+// Radix-sort temporary storage for the probed schedule's longest-first order.
+static size_t sort_temp_bytes(int64_t n)
+{
+    size_t bytes = 0;
+    if (cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, static_cast<const unsigned*>(nullptr),
+                                                  static_cast<unsigned*>(nullptr),
+                                                  static_cast<const unsigned*>(nullptr),
+                                                  static_cast<unsigned*>(nullptr), static_cast<int>(n)) !=
+        cudaSuccess)
+        return 0;
+    return bytes;
+}
+
+// Stable descending sort of the probe-phase step counts: the main phase then
+// takes the longest predicted trajectories first, so they start on every SM in
+// the first wave and the short ones fill in at the end.
+static cudaError_t sort_by_probe(const pb_solve_args& a, const ScratchLayout& sl, cudaStream_t st)
+{
+    unsigned char* base = static_cast<unsigned char*>(a.scratch);
+    size_t bytes = sort_temp_bytes(a.n_traj);
+    if (bytes == 0) return cudaErrorInvalidValue;
+    int end_bit = 1;
+    while (end_bit < 32 && (static_cast<int64_t>(1) << end_bit) <= a.max_steps) ++end_bit;
+    return cub::DeviceRadixSort::SortPairsDescending(
+        base + sl.sort_tmp_off, bytes, reinterpret_cast<const unsigned*>(base + sl.key_in_off),
+        reinterpret_cast<unsigned*>(base + sl.key_out_off), reinterpret_cast<const unsigned*>(base + sl.val_in_off),
+        reinterpret_cast<unsigned*>(base + sl.val_out_off), static_cast<int>(a.n_traj), 0, end_bit, st);
 }
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
@@ -291,7 +326,8 @@ static int validate(const pb_solve_args* a)
             break;
         default: return PB_EINVAL;
     }
-    if (a->schedule == PB_SCHED_QUEUE && !a->queue_counter) return PB_EINVAL;
+    if ((a->schedule == PB_SCHED_QUEUE || a->schedule == PB_SCHED_PROBED) && !a->queue_counter) return PB_EINVAL;
+    if (a->schedule == PB_SCHED_PROBED && a->n_traj > 0x7fffffffLL) return PB_EINVAL;  // 32-bit sort values
     if (a->block_size < 0 || (a->block_size % 32) != 0 || a->block_size > 256) return PB_EINVAL;
     return PB_SUCCESS;
 }
@@ -323,7 +359,11 @@ const char* pb_error_string(int32_t s)
 int64_t pb_solve_scratch_bytes(const pb_solve_args* a)
 {
     if (!a || a->n_traj < 0 || a->n_save < 1 || a->win_begin < 0 || a->win_begin >= a->n_save) return -1;
-    return scratch_layout(*a).total;
+    const ScratchLayout sl = scratch_layout(*a);
+    if (!sl.probed) return sl.total;
+    if (a->n_traj > 0x7fffffffLL) return -1;
+    const size_t tmp = sort_temp_bytes(a->n_traj);
+    return tmp == 0 && a->n_traj > 0 ? -1 : align_up(sl.total + static_cast<int64_t>(tmp), 256);
 }
 
 int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t schedule, int32_t block_size,
@@ -336,7 +376,7 @@ int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t s
     const int smem = k.smem_per_thread * block_size;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (schedule == PB_SCHED_QUEUE) {
+    if (schedule != PB_SCHED_PLAIN) {
         if (e == cudaSuccess) e = prepare_smem(k.queue, smem);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.queue, block_size, smem);
     } else {
@@ -391,7 +431,20 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
 
     if (sl.deferred) {
         // pass 1: integrate, one record per window step holding save points
-        if (a.schedule == PB_SCHED_QUEUE) {
+        if (sl.probed) {
+            // probe phase, longest-first sort of its step counts, main phase
+            int64_t grid = 0;
+            e = persistent_grid(k.queue_probe, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return map_cuda(e);
+            k.queue_probe<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = sort_by_probe(a, sl, st);
+            if (e == cudaSuccess) e = persistent_grid(k.queue_main, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return map_cuda(e);
+            k.queue_main<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
+        } else if (a.schedule != PB_SCHED_PLAIN) {
             int64_t grid = 0;
             e = persistent_grid(k.queue_defer, block, 0, a.n_traj, a.grid_blocks, &grid);
             if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
@@ -417,7 +470,7 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
         if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return map_cuda(e);
         k.queue<<<static_cast<unsigned>(grid), block, smem, st>>>(a, 1);
-    } else if (a.schedule == PB_SCHED_QUEUE) {
+    } else if (a.schedule != PB_SCHED_PLAIN) {
         int64_t grid = 0;
         e = prepare_smem(k.queue, smem);
         if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);

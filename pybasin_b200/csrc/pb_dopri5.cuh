@@ -283,9 +283,11 @@ struct Integrator {
     }
 
     // ---- start a trajectory: load y0/params, first derivative, initial step
-    __device__ static void begin(L_t& L, St& st, int64_t traj, const pb_solve_args& a)
+    // (y0 row, parameter row) of a trajectory; false for a parameter row out of range
+    __device__ static bool rows_of(int64_t traj, const pb_solve_args& a, int64_t& ic, int64_t& prow)
     {
-        int64_t ic = traj, prow = 0;
+        ic = traj;
+        prow = 0;
         if (a.layout == PB_LAYOUT_CROSS) {
             ic = traj / a.n_param_rows;
             prow = traj - ic * a.n_param_rows;
@@ -294,6 +296,71 @@ struct Integrator {
         }
         const bool bad_row = prow < 0 || prow >= a.n_param_rows;
         if (bad_row) prow = 0;
+        return !bad_row;
+    }
+
+    __device__ static void load_params(L_t& L, int64_t prow, const pb_solve_args& a)
+    {
+#pragma unroll
+        for (int q = 0; q < Sys::NP; ++q)
+            L.p[q] = q < a.n_params ? static_cast<R>(__ldg(a.params + prow * a.n_params + q)) : R(0);
+    }
+
+    // ---- probed schedule: the state after the probe phase, and back
+    __device__ static void save(const L_t& L, const Plan& pl, int64_t traj, const pb_solve_args& a, int done)
+    {
+        unsigned char* b = state_ptr(a, pl.sl, traj);
+        R* r = reinterpret_cast<R*>(b);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            r[s] = L.y[s];
+            r[S + s] = L.yc[s];
+            r[2 * S + s] = L.k1[s];
+        }
+        double* d = reinterpret_cast<double*>(b + (3 * S * sizeof(R) + 7) / 8 * 8);
+        d[0] = L.t;
+        d[1] = L.dt;
+        d[2] = L.next_save;
+        int* i = reinterpret_cast<int*>(d + 3);
+        i[0] = L.si;
+        i[1] = L.steps;
+        i[2] = L.status;
+        i[3] = L.nrec;
+        i[4] = done;
+    }
+
+    // false if the trajectory already finished in the probe phase
+    __device__ static bool resume(L_t& L, const Plan& pl, int64_t traj, const pb_solve_args& a)
+    {
+        const unsigned char* b = state_ptr(a, pl.sl, traj);
+        const double* d = reinterpret_cast<const double*>(b + (3 * S * sizeof(R) + 7) / 8 * 8);
+        const int* i = reinterpret_cast<const int*>(d + 3);
+        if (i[4]) return false;
+        const R* r = reinterpret_cast<const R*>(b);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            L.y[s] = r[s];
+            L.yc[s] = r[S + s];
+            L.k1[s] = r[2 * S + s];
+        }
+        L.t = d[0];
+        L.dt = d[1];
+        L.next_save = d[2];
+        L.si = i[0];
+        L.steps = i[1];
+        L.status = i[2];
+        L.nrec = i[3];
+        L.max_steps = static_cast<int>(a.max_steps < 0x7fffffffLL ? a.max_steps : 0x7fffffffLL);
+        int64_t ic, prow;
+        rows_of(traj, a, ic, prow);
+        load_params(L, prow, a);
+        return true;
+    }
+
+    __device__ static void begin(L_t& L, St& st, int64_t traj, const pb_solve_args& a)
+    {
+        int64_t ic, prow;
+        const bool bad_row = !rows_of(traj, a, ic, prow);
         double y0d[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -303,9 +370,7 @@ struct Integrator {
             L.y[s] = static_cast<R>(y0d[s]);
             L.yc[s] = R(0);
         }
-#pragma unroll
-        for (int q = 0; q < Sys::NP; ++q)
-            L.p[q] = q < a.n_params ? static_cast<R>(__ldg(a.params + prow * a.n_params + q)) : R(0);
+        load_params(L, prow, a);
         L.t = bad_row ? a.t1 : a.t0;  // a bad row finishes without stepping
         L.steps = 0;
         L.max_steps = static_cast<int>(a.max_steps < 0x7fffffffLL ? a.max_steps : 0x7fffffffLL);
@@ -317,7 +382,7 @@ struct Integrator {
 
         // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
         if (MIXED) {
-            Sys::f(ClockF32{reduce_two_pi(a.t0, 0.0)}, L.y, L.k1, L.p);
+            Sys::f(ClockF32{reduce_two_pi(a.t0)}, L.y, L.k1, L.p);
         } else {
             Sys::f(ClockF64{a.t0}, L.y, L.k1, L.p);
         }
@@ -337,7 +402,7 @@ struct Integrator {
 #pragma unroll
         for (int s = 0; s < S; ++s) ytmp[s] = static_cast<R>(y0d[s] + h0 * static_cast<double>(L.k1[s]));
         if (MIXED) {
-            Sys::f(ClockF32{reduce_two_pi(a.t0 + h0, 0.0)}, ytmp, ftmp, L.p);
+            Sys::f(ClockF32{reduce_two_pi(a.t0 + h0)}, ytmp, ftmp, L.p);
         } else {
             Sys::f(ClockF64{a.t0 + h0}, ytmp, ftmp, L.p);
         }
@@ -437,34 +502,48 @@ struct Integrator {
                                                   R (&k4)[S], R (&k5)[S], R (&k6)[S], R (&k7)[S], R (&d)[S],
                                                   R (&yn)[S])
     {
+        // stage arguments y + h * sum_j a_ij k_j, the sum accumulated oldest stage
+        // first (the newest stage enters the last multiply-add)
         R ys[S];
 #pragma unroll
-        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a21) * L.k1[s]);
+        for (int s = 0; s < S; ++s) ys[s] = fmad(h, R(dp::a21) * L.k1[s], L.y[s]);
         Sys::f(tb.at(dp::c2), ys, k2, L.p);
 #pragma unroll
-        for (int s = 0; s < S; ++s) ys[s] = L.y[s] + h * (R(dp::a31) * L.k1[s] + R(dp::a32) * k2[s]);
+        for (int s = 0; s < S; ++s) ys[s] = fmad(h, fmad(R(dp::a32), k2[s], R(dp::a31) * L.k1[s]), L.y[s]);
         Sys::f(tb.at(dp::c3), ys, k3, L.p);
 #pragma unroll
         for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a41) * L.k1[s] + R(dp::a42) * k2[s] + R(dp::a43) * k3[s]);
+            ys[s] = fmad(h, fmad(R(dp::a43), k3[s], fmad(R(dp::a42), k2[s], R(dp::a41) * L.k1[s])), L.y[s]);
         Sys::f(tb.at(dp::c4), ys, k4, L.p);
 #pragma unroll
         for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a51) * L.k1[s] + R(dp::a52) * k2[s] + R(dp::a53) * k3[s] +
-                                  R(dp::a54) * k4[s]);
+            ys[s] = fmad(h,
+                         fmad(R(dp::a54), k4[s],
+                              fmad(R(dp::a53), k3[s], fmad(R(dp::a52), k2[s], R(dp::a51) * L.k1[s]))),
+                         L.y[s]);
         Sys::f(tb.at(dp::c5), ys, k5, L.p);
 #pragma unroll
         for (int s = 0; s < S; ++s)
-            ys[s] = L.y[s] + h * (R(dp::a61) * L.k1[s] + R(dp::a62) * k2[s] + R(dp::a63) * k3[s] +
-                                  R(dp::a64) * k4[s] + R(dp::a65) * k5[s]);
+            ys[s] = fmad(h,
+                         fmad(R(dp::a65), k5[s],
+                              fmad(R(dp::a64), k4[s],
+                                   fmad(R(dp::a63), k3[s], fmad(R(dp::a62), k2[s], R(dp::a61) * L.k1[s])))),
+                         L.y[s]);
         Sys::f(tb.at(1.0), ys, k6, L.p);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            d[s] = h * (R(dp::b1) * L.k1[s] + R(dp::b3) * k3[s] + R(dp::b4) * k4[s] + R(dp::b5) * k5[s] +
-                        R(dp::b6) * k6[s]);
+            d[s] = h * fmad(R(dp::b6), k6[s],
+                            fmad(R(dp::b5), k5[s], fmad(R(dp::b4), k4[s], fmad(R(dp::b3), k3[s], R(dp::b1) * L.k1[s]))));
             yn[s] = L.y[s] + d[s];
         }
         Sys::f(tb.at(1.0), yn, k7, L.p);
+    }
+
+    // h * sum_j e_j k_j, the embedded error estimate of one state
+    __device__ __forceinline__ static R err_est(R h, R k1, R k3, R k4, R k5, R k6, R k7)
+    {
+        return h * fmad(R(dp::e7), k7,
+                        fmad(R(dp::e6), k6, fmad(R(dp::e5), k5, fmad(R(dp::e4), k4, fmad(R(dp::e3), k3, R(dp::e1) * k1)))));
     }
 
     // ---- one attempted step; returns true once the trajectory is finished
@@ -473,19 +552,24 @@ struct Integrator {
     {
         if (!(L.t < a.t1) || L.steps >= L.max_steps) return true;
         L.steps++;
+        const double t = L.t;
+        // the stage phase base depends on t only, so it is reduced while the
+        // clipping and conversion of dt below are in flight
+        const float r0 = (MIXED && Sys::kTime) ? reduce_two_pi(t) : 0.f;
         double dt = L.dt;
-        if (L.t + dt > a.t1) dt = a.t1 - L.t;
+        R h = static_cast<R>(dt);
+        if (t + dt > a.t1) {
+            dt = a.t1 - t;
+            h = static_cast<R>(dt);
+        }
         // dt > 0 here (t < t1, and the control keeps dt * fac with fac >= 0.2);
         // a dt lost below t's resolution (including 0) ends the trajectory
-        if (L.t + dt == L.t) {
+        if (t + dt == t) {
             L.status = PB_TRAJ_DT_UNDERFLOW;
             return true;
         }
-        const R h = static_cast<R>(dt);
-        const double t = L.t;
         R k2[S], k3[S], k4[S], k5[S], k6[S], k7[S], d[S], yn[S];
         if (MIXED) {
-            const float r0 = Sys::kTime ? reduce_two_pi(t, dt) : 0.f;
             stages(TimeBaseF32{r0, static_cast<float>(h)}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
         } else {
             stages(TimeBaseF64{t, dt}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
@@ -493,25 +577,25 @@ struct Integrator {
 
         // embedded error estimate (RMS norm, dopri5_generic.zig:185-192)
         double err2 = 0.0;
+        float e2f = 0.f;  // the same sum in FP32, feeding only the step-size factor
         if (MIXED) {
             const float rt = static_cast<float>(a.rtol), at = static_cast<float>(a.atol);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const float e = static_cast<float>(
-                    h * (R(dp::e1) * L.k1[s] + R(dp::e3) * k3[s] + R(dp::e4) * k4[s] + R(dp::e5) * k5[s] +
-                         R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
+                const float e = static_cast<float>(err_est(h, L.k1[s], k3[s], k4[s], k5[s], k6[s], k7[s]));
                 const float sc =
                     fmaf(rt, fmaxf(fabsf(static_cast<float>(L.y[s])), fabsf(static_cast<float>(yn[s]))), at);
-                const double r = static_cast<double>(__fdividef(e, sc));
+                const float rf = __fdividef(e, sc);
+                const double r = static_cast<double>(rf);
                 err2 = fma(r, r, err2);
+                e2f = fmaf(rf, rf, e2f);
             }
             err2 *= 1.0 / S;
+            e2f *= 1.f / S;
         } else {
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const double e = static_cast<double>(
-                    h * (R(dp::e1) * L.k1[s] + R(dp::e3) * k3[s] + R(dp::e4) * k4[s] + R(dp::e5) * k5[s] +
-                         R(dp::e6) * k6[s] + R(dp::e7) * k7[s]));
+                const double e = static_cast<double>(err_est(h, L.k1[s], k3[s], k4[s], k5[s], k6[s], k7[s]));
                 const double sc =
                     a.atol + a.rtol * fmax(fabs(static_cast<double>(L.y[s])), fabs(static_cast<double>(yn[s])));
                 const double r = e / sc;
@@ -531,11 +615,15 @@ struct Integrator {
             R ia[S], ib[S], icf[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const R ym = L.y[s] + h * (R(dp::m1) * L.k1[s] + R(dp::m3) * k3[s] + R(dp::m4) * k4[s] +
-                                           R(dp::m5) * k5[s] + R(dp::m6) * k6[s] + R(dp::m7) * k7[s]);
-                ia[s] = R(2) * h * (k7[s] - L.k1[s]) - R(8) * (yn[s] + L.y[s]) + R(16) * ym;
-                ib[s] = h * (R(5) * L.k1[s] - R(3) * k7[s]) + R(18) * L.y[s] + R(14) * yn[s] - R(32) * ym;
-                icf[s] = h * (k7[s] - R(4) * L.k1[s]) - R(11) * L.y[s] - R(5) * yn[s] + R(16) * ym;
+                const R ym = fmad(
+                    h,
+                    fmad(R(dp::m7), k7[s],
+                         fmad(R(dp::m6), k6[s],
+                              fmad(R(dp::m5), k5[s], fmad(R(dp::m4), k4[s], fmad(R(dp::m3), k3[s], R(dp::m1) * L.k1[s]))))),
+                    L.y[s]);
+                ia[s] = fmad(R(16), ym, fmad(R(-8), yn[s] + L.y[s], (R(2) * h) * (k7[s] - L.k1[s])));
+                ib[s] = fmad(R(-32), ym, fmad(R(14), yn[s], fmad(R(18), L.y[s], h * fmad(R(5), L.k1[s], R(-3) * k7[s]))));
+                icf[s] = fmad(R(16), ym, fmad(R(-5), yn[s], fmad(R(-11), L.y[s], h * fmad(R(-4), L.k1[s], k7[s]))));
             }
             if (DEFER) {
                 if (!write_record(L, pl, traj, a, t, dt, h, ia, ib, icf, tn)) {
@@ -552,7 +640,7 @@ struct Integrator {
                     const R x = static_cast<R>((ts - t) * inv_dt);
 #pragma unroll
                     for (int s = 0; s < S; ++s)
-                        v[s] = L.y[s] + x * (h * L.k1[s] + x * (icf[s] + x * (ib[s] + x * ia[s])));
+                        v[s] = fmad(x, fmad(x, fmad(x, fmad(x, ia[s], ib[s]), icf[s]), h * L.k1[s]), L.y[s]);
                 }
             });
             }
@@ -588,9 +676,11 @@ struct Integrator {
         // step-size control (dopri5_generic.zig:228-235)
         double fac;
         if (MIXED) {
-            const float e2f = static_cast<float>(err2);
-            const float g = 0.9f * ex2_approx(-0.1f * __log2f(e2f));  // 0.9 * err^-0.2 with err^2 = e2f
-            fac = (err2 == 0.0) ? dp::max_factor : static_cast<double>(fminf(10.f, fmaxf(accept ? 1.f : 0.2f, g)));
+            // acceptance above used the FP64 norm; the factor 0.9 * err^-0.2 needs no
+            // more than FP32, and taking it from the FP32 sum keeps the FP64
+            // conversions off the step-to-step dependency chain
+            const float g = 0.9f * ex2_approx(-0.1f * __log2f(e2f));
+            fac = (e2f == 0.f) ? dp::max_factor : static_cast<double>(fminf(10.f, fmaxf(accept ? 1.f : 0.2f, g)));
         } else {
             const double err = sqrt(err2);
             fac = (err == 0.0) ? dp::max_factor
@@ -733,9 +823,19 @@ __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
 // records overflowed are integrated (inline).  Every loop is bounded: each
 // trajectory runs at most max_steps attempted steps and the queue holds n_traj
 // entries.
-template <class Sys, class R, bool DEFER>
+//
+// PHASE (deferred dense output only): 0 = whole span; 1 = probe phase, which
+// stops each trajectory at the first accepted or rejected step ending at or after
+// t0 + kProbeFraction (t1 - t0), saves its state and writes its step count as a
+// sort key; 2 = main phase, which takes trajectories in the sorted order and
+// resumes them.  The probe does not clip the step at its end, so the sequence of
+// steps, and every output, is the one of PHASE 0.
+constexpr double kProbeFraction = 0.05;
+
+template <class Sys, class R, bool DEFER, int PHASE = 0>
 __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int redo_only)
 {
+    static_assert(PHASE == 0 || DEFER, "the probed schedule saves no inline statistics");
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Plan pl;
     if (threadIdx.x == 0) build_plan(pl, a);
@@ -743,6 +843,7 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
     using I = Integrator<Sys, R>;
     const int lane = threadIdx.x & 31;
     auto st = stats_slot<Sys>(smem, !DEFER);
+    const double t_probe = a.t0 + kProbeFraction * (a.t1 - a.t0);
     while (true) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.queue_counter, 32ull);
@@ -750,16 +851,36 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
         if (static_cast<int64_t>(base) >= a.n_traj) break;
         const int64_t q = static_cast<int64_t>(base) + lane;
         if (q < a.n_traj) {
-            const int64_t traj = traj_at(a, q);
+            const int64_t traj = PHASE == 2 ? static_cast<int64_t>(sort_vec(a, pl.sl.val_out_off)[q]) : traj_at(a, q);
             const bool in_range = traj >= 0 && traj < a.n_traj;  // an order entry out of range is ignored
             const bool skip = !in_range ||
                               (redo_only && reinterpret_cast<const int*>(tail_ptr(a, pl.sl, traj))[0] >= 0);
+            unsigned key = 0;
             if (!skip) {
                 typename I::L_t L;
-                I::begin(L, st, traj, a);
-                while (!I::template step<DEFER>(L, st, pl, traj, a)) {
+                if (PHASE == 2) {
+                    if (I::resume(L, pl, traj, a)) {
+                        while (!I::template step<DEFER>(L, st, pl, traj, a)) {
+                        }
+                        I::template finish<DEFER>(L, st, pl, traj, a);
+                    }
+                } else if (PHASE == 1) {
+                    I::begin(L, st, traj, a);
+                    bool done = false;
+                    while (!done && L.t < t_probe) done = I::template step<DEFER>(L, st, pl, traj, a);
+                    if (done) I::template finish<DEFER>(L, st, pl, traj, a);
+                    I::save(L, pl, traj, a, done ? 1 : 0);
+                    key = done ? 0u : static_cast<unsigned>(L.steps);
+                } else {
+                    I::begin(L, st, traj, a);
+                    while (!I::template step<DEFER>(L, st, pl, traj, a)) {
+                    }
+                    I::template finish<DEFER>(L, st, pl, traj, a);
                 }
-                I::template finish<DEFER>(L, st, pl, traj, a);
+            }
+            if (PHASE == 1) {
+                sort_vec(a, pl.sl.key_in_off)[q] = key;
+                sort_vec(a, pl.sl.val_in_off)[q] = static_cast<unsigned>(traj);
             }
         }
         __syncwarp();

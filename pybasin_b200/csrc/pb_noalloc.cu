@@ -52,7 +52,8 @@ extern "C" int pb_solve_batch_noalloc(const pb_solve_args* args, void* stream)
     if (args->n_traj < 0 || args->n_save < 1 || args->win_begin < 0 || args->win_begin >= args->n_save)
         return PB_EINVAL;
     // scratch of pb_solve_batch followed by the work-queue counter (256-byte aligned)
-    const int64_t need = pb::scratch_layout(*args).total;
+    const int64_t need = pb_solve_scratch_bytes(args);
+    if (need < 0) return PB_EINVAL;
     const int64_t total = need + 256;
     if (total > static_cast<int64_t>(PB_NOALLOC_SCRATCH_BYTES)) return PB_ESCRATCH_LIMIT;
     void* base = nullptr;

@@ -10,6 +10,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace pb {
 
 // time of one stage, FP64 kernel: the stage instant itself
@@ -25,15 +27,23 @@ __device__ __forceinline__ double clock_cos(const ClockF64& c) { return cos(c.t)
 __device__ __forceinline__ float clock_cos(const ClockF32& c)
 {
 #ifndef PB_ACCURATE_COS
-    // the step's phases lie in [-pi - h/2, pi + h/2] (reduction centred on the step
-    // midpoint, TimeBaseF32); measured max |__cosf(x) - cos(x)| on B200 is 4.0e-7
-    // for |x| <= pi, 4.2e-7 for |x| <= pi + 1 (h <= 2) and 7.1e-7 for |x| <= 2 pi,
-    // at or below the FP32 stage resolution of a unit-scale state
+    // the step's phases lie in [-pi, pi + h] (base reduced into [-pi, pi] in FP64);
+    // measured max |__cosf(x) - cos(x)| on B200 is 4.0e-7 for |x| <= pi, 4.2e-7 for
+    // |x| <= pi + 1 and 7.1e-7 for |x| <= 2 pi, at or below the FP32 stage
+    // resolution of a unit-scale state
     return __cosf(c.phase);
 #else
     return cosf(c.phase);
 #endif
 }
+
+// Explicit fused multiply-add.  Every multiply-add with two product operands in
+// the integrator and the built-in right-hand sides is written with it, so the
+// rounding does not depend on which product the compiler contracts in a given
+// kernel: the queue, probed, plain and redo kernels produce bit-identical
+// trajectories.
+__device__ __forceinline__ float fmad(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmad(double a, double b, double c) { return fma(a, b, c); }
 
 __device__ __forceinline__ float r_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double r_sin(double x) { return sin(x); }
@@ -49,13 +59,12 @@ struct TimeBaseF32 {
     float r0, h;  // t mod 2*pi (FP64-reduced, then rounded), FP32 step
     __device__ __forceinline__ ClockF32 at(double c) const { return ClockF32{r0 + static_cast<float>(c) * h}; }
 };
-// t - 2*pi*k with k the nearest integer to (t + dt/2) / (2*pi): the stage phases
-// t + c*dt - 2*pi*k (0 <= c <= 1) then lie within pi + dt/2 of zero
-__device__ __forceinline__ float reduce_two_pi(double t, double dt)
+// t - 2*pi*k with k the nearest integer to t / (2*pi), in [-pi, pi]
+__device__ __forceinline__ float reduce_two_pi(double t)
 {
     const double two_pi = 6.283185307179586476925286766559;
     const double inv_two_pi = 0.15915494309189533576888376337251;
-    const double k = rint(fma(0.5, dt, t) * inv_two_pi);
+    const double k = rint(t * inv_two_pi);
     return static_cast<float>(fma(-k, two_pi, t));
 }
 
@@ -83,7 +92,7 @@ struct SysPendulum {
     __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
     {
         dy[0] = y[1];
-        dy[1] = -p[0] * y[1] + p[1] - p[2] * r_sin(y[0]);
+        dy[1] = fmad(-p[2], r_sin(y[0]), fmad(-p[0], y[1], p[1]));
     }
 };
 
@@ -96,9 +105,11 @@ struct SysDuffing {
     template <class R, class C>
     __device__ __forceinline__ static void f(const C& c, const R* y, R* dy, const R* p)
     {
+        // -delta*v - k3*x^3 + A*cos(t), grouped for a two-level dependency chain
         const R x = y[0];
         dy[0] = y[1];
-        dy[1] = -p[0] * y[1] - p[1] * x * x * x + p[2] * clock_cos(c);
+        const R forcing = p[2] * static_cast<R>(clock_cos(c));
+        dy[1] = fmad(-p[1] * x, x * x, fmad(-p[0], y[1], forcing));
     }
 };
 
@@ -114,8 +125,8 @@ struct SysLorenz {
     __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
     {
         R f0 = p[0] * (y[1] - y[0]);
-        R f1 = p[1] * y[0] - y[0] * y[2] - y[1];
-        R f2 = y[0] * y[1] - p[2] * y[2];
+        R f1 = fmad(p[1], y[0], fmad(-y[0], y[2], -y[1]));
+        R f2 = fmad(y[0], y[1], -p[2] * y[2]);
         if (MASKED) {
             const R m = fmax(r_abs(y[0]), fmax(r_abs(y[1]), r_abs(y[2])));
             if (!(m < R(200))) f0 = f1 = f2 = R(0);

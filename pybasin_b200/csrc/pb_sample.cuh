@@ -35,6 +35,13 @@ __device__ __forceinline__ double feature_value(int kind, double sh, double s1, 
     }
 }
 
+// y(t + x dt) from a record's coefficients [y, h*k1, c, b, a] (Horner form)
+template <class R>
+__device__ __forceinline__ R dense_value(const R* c, R x)
+{
+    return fmad(x, fmad(x, fmad(x, fmad(x, c[4], c[3]), c[2]), c[1]), c[0]);
+}
+
 // Per-lane window statistics accumulated by the sampling pass.
 template <int S>
 struct SampleAcc {
@@ -163,7 +170,7 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
             const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) * rdt);
 #pragma unroll
             for (int q = 0; q < S; ++q) {
-                const R v = co[5 * q] + x * (co[5 * q + 1] + x * (co[5 * q + 2] + x * (co[5 * q + 3] + x * co[5 * q + 4])));
+                const R v = dense_value(co + 5 * q, x);
                 const double f = __shfl_sync(0xffffffffu, static_cast<double>(v), 0);
                 acc.sh[q] = isfinite(f) ? f : 0.0;
             }
@@ -195,7 +202,7 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
             for (int q = 0; q < S; ++q) {
                 v[q] = R(0);
                 if (q >= ns) continue;  // uniform across the warp
-                v[q] = co[5 * q] + x * (co[5 * q + 1] + x * (co[5 * q + 2] + x * (co[5 * q + 3] + x * co[5 * q + 4])));
+                v[q] = dense_value(co + 5 * q, x);
                 const R d = v[q] - sh[q];
                 p1[q] += d;
                 p2[q] = fma(d, d, p2[q]);

@@ -3,6 +3,9 @@
 //   [median windows]  n_traj x n_median_columns x window floats (PB_FEAT_MEDIAN)
 //   [step records]    n_traj x cap x record_stride bytes        (PB_DENSE_DEFERRED)
 //   [tails]           n_traj x tail_stride bytes                (PB_DENSE_DEFERRED)
+//   [saved states]    n_traj x state_stride bytes               (PB_SCHED_PROBED)
+//   [sort keys/values] 4 x n_traj int32, then the radix-sort temporary storage
+//                     (PB_SCHED_PROBED; the temporary's size is added on the host)
 //
 // Each part starts on a 256-byte boundary.  A step record (a multiple of 16 bytes,
 // written with 16-byte stores) is
@@ -27,12 +30,27 @@ struct ScratchLayout {
     int64_t median_off;
     int64_t rec_off;
     int64_t tail_off;
-    int64_t total;
+    int64_t state_off;     // PB_SCHED_PROBED: integrator state saved after the probe phase
+    int64_t key_in_off;    // probe-phase step counts, in queue order
+    int64_t key_out_off;
+    int64_t val_in_off;    // trajectory ids, in queue order
+    int64_t val_out_off;   // trajectory ids, longest predicted first
+    int64_t sort_tmp_off;  // radix-sort temporary storage (last)
+    int64_t total;         // excluding the radix-sort temporary
     int32_t rec_stride;
     int32_t cap;
     int32_t tail_stride;
     int32_t deferred;
+    int32_t state_stride;
+    int32_t probed;
 };
+
+// Bytes of one saved integrator state: y, yc, k1 (stage precision), then t, dt,
+// next save time (double) and si, steps, status, n_records, done (int32).
+__host__ __device__ constexpr int saved_state_bytes(int dim, int rsize)
+{
+    return ((3 * dim * rsize + 7) / 8 * 8 + 3 * 8 + 5 * 4 + 15) / 16 * 16;
+}
 
 __host__ __device__ inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
@@ -77,6 +95,19 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
         l.tail_stride = static_cast<int32_t>(align_up(16 + 8 * a.dim, 16));
         l.tail_off = off;
         off = align_up(off + a.n_traj * l.tail_stride, 256);
+        l.probed = (a.schedule == PB_SCHED_PROBED) ? 1 : 0;
+        if (l.probed) {
+            l.state_stride = saved_state_bytes(a.dim, rsize);
+            l.state_off = off;
+            off = align_up(off + a.n_traj * l.state_stride, 256);
+            const int64_t vec = align_up(a.n_traj * 4, 256);
+            l.key_in_off = off;
+            l.key_out_off = off + vec;
+            l.val_in_off = off + 2 * vec;
+            l.val_out_off = off + 3 * vec;
+            off += 4 * vec;
+            l.sort_tmp_off = off;
+        }
     }
     l.total = off;
     return l;
@@ -94,6 +125,15 @@ __device__ __forceinline__ unsigned char* record_ptr(const pb_solve_args& a, con
 __device__ __forceinline__ unsigned char* tail_ptr(const pb_solve_args& a, const ScratchLayout& l, int64_t traj)
 {
     return static_cast<unsigned char*>(a.scratch) + l.tail_off + traj * l.tail_stride;
+}
+
+__device__ __forceinline__ unsigned char* state_ptr(const pb_solve_args& a, const ScratchLayout& l, int64_t traj)
+{
+    return static_cast<unsigned char*>(a.scratch) + l.state_off + traj * l.state_stride;
+}
+__device__ __forceinline__ unsigned* sort_vec(const pb_solve_args& a, int64_t off)
+{
+    return reinterpret_cast<unsigned*>(static_cast<unsigned char*>(a.scratch) + off);
 }
 
 // offset of (first_save, n_saves) inside a record

@@ -125,7 +125,7 @@ class BasinStabilityPipeline:
             win_begin=self.win_begin,
             columns=self.columns,
             precision=L.PREC_MIXED if self.solver.precision == "mixed" else L.PREC_FP64,
-            schedule=L.SCHED_QUEUE if self.solver.schedule == "queue" else L.SCHED_PLAIN,
+            schedule=L.SCHEDULES[self.solver.schedule],
             max_steps=self.solver.max_steps,
             unbounded_thr=float(self.solver.unbounded_threshold or 0.0),
             keep_final=False,

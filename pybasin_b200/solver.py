@@ -100,7 +100,9 @@ class B200Dopri5Solver:
     :param max_steps: attempted steps per trajectory before giving up (status MAX_STEPS).
     :param unbounded_threshold: stop a trajectory once max|y| >= this after an accepted
         step (the reference's stop events, e.g. case_studies/lorenz/setup_lorenz_system.py:16-26).
-    :param schedule: ``"queue"`` (persistent warps + work queue) or ``"plain"``.
+    :param schedule: ``"queue"`` (persistent warps + work queue), ``"probed"`` (the queue in
+        predicted-cost order: a probe over the first 5 % of the span orders the
+        trajectories longest first; identical results) or ``"plain"``.
     :param dense_mode: ``"deferred"`` (the integrator writes one record per window step that
         holds save points and a warp-parallel pass evaluates the save points) or ``"inline"``
         (each thread evaluates its save points after its step); full output is always inline.
@@ -140,8 +142,8 @@ class B200Dopri5Solver:
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if output not in (None, "fused", "full"):
             raise ValueError("output must be 'fused' or 'full'")
-        if schedule not in ("queue", "plain"):
-            raise ValueError("schedule must be 'queue' or 'plain'")
+        if schedule not in L.SCHEDULES:
+            raise ValueError(f"schedule must be one of {sorted(L.SCHEDULES)}")
         if t_steps < 1:
             raise ValueError("t_steps must be >= 1")
         if order not in ("morton", "none"):
@@ -307,7 +309,7 @@ class B200Dopri5Solver:
                 win_begin=win_begin,
                 columns=cols,
                 precision=L.PREC_MIXED if self.precision == "mixed" else L.PREC_FP64,
-                schedule=L.SCHED_QUEUE if self.schedule == "queue" else L.SCHED_PLAIN,
+                schedule=L.SCHEDULES[self.schedule],
                 max_steps=self.max_steps,
                 unbounded_thr=float(self.unbounded_threshold or 0.0),
                 keep_final=not full,

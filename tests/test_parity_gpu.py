@@ -348,3 +348,49 @@ def test_broken_butterfly_unbounded_labels_match_oracle():
     unb_g = got["status"] == L.TRAJ_UNBOUNDED
     assert 0 < unb_w.sum() < len(y0)
     assert (unb_w == unb_g).mean() >= 0.99
+
+
+# ---------------------------------------------------------------------------
+# probed schedule: same steps, same outputs as the queue in processing order
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("case", [PENDULUM, DUFFING], ids=lambda c: c.name)
+def test_probed_schedule_is_bit_identical_to_queue(case, precision):
+    y0 = seeded_ics(case, 3000, 11).double().numpy()
+    save = case.save_ts().numpy()
+    feats = [(0, L.FEAT_MAX, 0.0), (0, L.FEAT_STD, 0.0), (1, L.FEAT_MEAN, 0.0), (1, L.FEAT_CROSSINGS, 0.0),
+             (0, L.FEAT_MEDIAN, 0.0)]
+    kw = dict(precision=precision, win_begin=case.win_begin(), features=feats)
+    t_span = (case.t_span[0], float(save[-1]))
+    rtol = case.rtol if precision == L.PREC_FP64 else 1e-6
+    a = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, rtol, case.atol,
+                  schedule=L.SCHED_QUEUE, **kw)
+    for grid in (0, 37):
+        b = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, rtol, case.atol,
+                      schedule=L.SCHED_PROBED, grid_blocks=grid, **kw)
+        for k in ("status", "steps", "y_final", "features"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_probed_schedule_edge_cases():
+    """Stops inside the probe span (unbounded, max_steps, non-finite, bad parameter row),
+    record-capacity overflow (redo pass) and a window that starts inside the probe span."""
+    rng = np.random.default_rng(5)
+    y0 = np.stack([rng.uniform(-10, 10, 700), rng.uniform(-20, 20, 700), np.zeros(700)], axis=1)
+    y0[3] = [np.nan, 0.0, 0.0]
+    p = np.array([[0.12, 0.0, -0.6], [10.0, 28.0, 8.0 / 3.0]])
+    pidx = (np.arange(700) % 2).astype(np.int32)
+    pidx[7] = 5  # parameter row out of range
+    for save, cap, max_steps in ((np.linspace(900.0, 1000.0, 101), 0, 16**5),
+                                 (np.linspace(0.0, 1000.0, 2001), 64, 16**5),
+                                 (np.linspace(0.0, 1000.0, 501), 0, 2000)):
+        kw = dict(features=[(0, L.FEAT_MEAN, 0.0), (2, L.FEAT_MAX, 0.0)], param_index=pidx,
+                  unbounded_thr=200.0, window_record_cap=cap, max_steps=max_steps)
+        a = gpu_solve(O.SYS_LORENZ, y0, p, save, (0, 1000), 1e-8, 1e-6, schedule=L.SCHED_QUEUE, **kw)
+        b = gpu_solve(O.SYS_LORENZ, y0, p, save, (0, 1000), 1e-8, 1e-6, schedule=L.SCHED_PROBED, **kw)
+        for k in ("status", "steps", "y_final", "features"):
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        st = a["status"]
+        assert st[3] == L.TRAJ_NONFINITE and st[7] == L.TRAJ_BAD_INPUT
+        assert (st == L.TRAJ_UNBOUNDED).any()
+    assert (a["status"] == L.TRAJ_MAX_STEPS).any()
