@@ -321,7 +321,7 @@ def run_b200_arm(args) -> None:
     y0_dev = y0_host.to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
-    pipe = make_pipeline(dev, "mixed", "queue")
+    pipe = make_pipeline(dev, "mixed", "probed")
     pipe.run_device(y0_dev)
     torch.cuda.synchronize()
 
@@ -442,7 +442,7 @@ def run_b200_arm(args) -> None:
                             "window [900,1000] x 5000 saves, features max+std of x, 1-NN on 5 templates",
                 "n_ic_per_gpu": n,
                 "rtol_atol": list(pipe.solver.effective_tolerances()),
-                "schedule": "queue",
+                "schedule": "probed",
                 "l2": "flushed between timed steps (256 MB write)",
                 "parallelism": f"ic-shard x{world}",
             },

@@ -117,7 +117,7 @@ typedef struct pb_solve_args {
     int32_t layout;          /* pb_layout */
     int32_t y0_dtype;        /* pb_dtype of y0 */
     int32_t n_params;        /* columns of params (<= PB_MAX_PARAMS) */
-    int32_t block_size;      /* threads per block (0 = library default) */
+    int32_t block_size;      /* threads per block (0 = library default: 64 queue, 128 plain) */
     int32_t grid_blocks;     /* QUEUE: persistent blocks (0 = occupancy-derived) */
     int32_t _pad0;
     int64_t n_ic;            /* rows of y0 */

@@ -423,7 +423,8 @@ int pb_solve_batch(const pb_solve_args* args, void* stream)
     if (sl.total > 0 && !a.scratch) return PB_EINVAL;
     if (sl.deferred && !a.queue_counter) return PB_EINVAL;  // the redo pass runs on the queue
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int block = a.block_size > 0 ? a.block_size : 128;
+    // defaults from the launch-shape sweep: 64 for the queue schedules, 128 plain
+    const int block = a.block_size > 0 ? a.block_size : (a.schedule == PB_SCHED_PLAIN ? 128 : 64);
     const int smem = k.smem_per_thread * block;
     cudaError_t e = cudaSuccess;
     const int64_t plain_grid = (a.n_traj + block - 1) / block;

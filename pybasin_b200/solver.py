@@ -127,7 +127,7 @@ class B200Dopri5Solver:
         output: str | None = None,
         max_steps: int = DEFAULT_MAX_STEPS,
         unbounded_threshold: float | None = None,
-        schedule: str = "queue",
+        schedule: str = "probed",
         mixed_rtol_floor: float = MIXED_RTOL_FLOOR,
         block_size: int = 0,
         grid_blocks: int = 0,
