@@ -185,11 +185,15 @@ class BasinStabilityPipeline:
         L.check(rc, "pb_label_nearest")
 
     def kernel_launches_per_pass(self) -> int:
-        """Launches of this library's kernels per pass; the Z-order key/argsort of the
-        ICs runs as PyTorch ops before them.  Deferred dense output: integrate + sample
-        + redo of record overflows, then labelling; inline: integrate, labelling."""
+        """Launches of this library's kernels per pass: the Z-order keys (bounding box +
+        keys), then integrate (inline), or integrate + sample + redo of record
+        overflows (deferred; the probed schedule integrates in a probe and a main
+        launch, with a library radix sort between them), then labelling."""
         deferred = self.solver.dense_mode == "deferred"
-        return 4 if deferred else 2
+        n = 2 if self.solver.order == "morton" else 0
+        if not deferred:
+            return n + 2
+        return n + (5 if self.solver.schedule == "probed" else 4)
 
     def load_rows(self, y0: torch.Tensor, group: torch.Tensor | None = None) -> int:
         """Copy device ICs (and their parameter points) into the pipeline, growing it if needed."""
