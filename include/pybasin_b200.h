@@ -23,7 +23,9 @@
 #ifndef PYBASIN_B200_H
 #define PYBASIN_B200_H
 
-#include <stdint.h>
+#ifndef __CUDACC_RTC__
+#include <stdint.h> /* under NVRTC the including kernel header supplies the fixed-width types */
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -49,7 +51,9 @@ typedef enum {
     PB_SYS_DUFFING = 2,       /* case_studies/duffing_oscillator/duffing_ode.py:26-42, p=[delta,k3,A] */
     PB_SYS_LORENZ = 3,        /* case_studies/lorenz/lorenz_jax_ode.py, p=[sigma,r,b] */
     PB_SYS_LORENZ_MASKED = 4, /* case_studies/lorenz/lorenz_ode.py:28-64 (|y|>=200 freezes) */
-    PB_SYS_ROSSLER_NET = 5    /* case_studies/rossler_network/rossler_network_jax_ode.py:53-79 */
+    PB_SYS_ROSSLER_NET = 5,   /* case_studies/rossler_network/rossler_network_jax_ode.py:53-79 */
+    PB_SYS_USER = 64          /* a right-hand side compiled at run time (pb_rhs_compile),
+                                 solved with pb_solve_batch_rhs */
 } pb_system;
 
 /* ---- arithmetic of the integrator ---- */
@@ -247,6 +251,42 @@ int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, 
  * serialised by the caller.  The call itself allocates nothing. */
 #define PB_NOALLOC_SCRATCH_BYTES (64ll * 1024ll * 1024ll)
 int pb_solve_batch_noalloc(const pb_solve_args* args, void* stream);
+
+/* ---- right-hand sides compiled at run time (NVRTC) -------------------------
+ * Replaces the reference's SymPy-to-C path for user ODEs, src/zigode/sympy_ode.py
+ * :49-78 (C source from symbolic expressions, compiled into a library that the
+ * native solver loads, zig_solver.py:106-179).  Here the expressions become a
+ * device functor inside the same fused integrator templates, compiled for
+ * sm_100a by NVRTC (loaded with dlopen: libnvrtc.so.12 of the CUDA toolkit, or
+ * the path in PB_NVRTC_LIBRARY).
+ *   rhs          dim C expressions, dy[i]/dt = rhs[i], in terms of y[j] (state,
+ *                stage precision), p[k] (parameters, stage precision) and t (FP64);
+ *                math functions of CUDA device code (sin, cos, exp, pow, ...)
+ *   dim          1..PB_MAX_USER_DIM;  n_params 0..PB_MAX_PARAMS
+ *   preamble     optional device code placed before the functor (helper
+ *                __device__ functions), or NULL
+ *   precision    pb_precision of the kernels to build
+ *   include_dirs directories holding pb_sample.cuh and pybasin_b200.h; with
+ *                n_include_dirs = 0 they are found next to this library
+ *                (../csrc and ../../include relative to its file)
+ *   cache_dir    optional directory for compiled modules, keyed by a hash of the
+ *                generated source and the compile options, or NULL
+ *   out          receives the loaded program on the current device; with
+ *                out = NULL the call only compiles (and fills cache_dir), which
+ *                needs no GPU
+ *   log          optional buffer for the NVRTC log (PB_ECOMPILE on a failed compile)
+ * The program holds a module on the device that was current; release it with
+ * pb_rhs_release. */
+#define PB_MAX_USER_DIM 16
+typedef struct pb_rhs_program pb_rhs_program;
+int pb_rhs_compile(const char* const* rhs, int32_t dim, int32_t n_params, const char* preamble,
+                   int32_t precision, const char* const* include_dirs, int32_t n_include_dirs,
+                   const char* cache_dir, pb_rhs_program** out, char* log, int64_t log_bytes);
+/* pb_solve_batch for a compiled right-hand side: args->system = PB_SYS_USER,
+ * args->dim / precision / n_params equal to the program's; every other field as
+ * for pb_solve_batch (features on states < 8). */
+int pb_solve_batch_rhs(const pb_rhs_program* prog, const pb_solve_args* args, void* stream);
+int pb_rhs_release(pb_rhs_program* prog);
 
 /* ---- learned surrogate (no counterpart in the reference) -------------------
  * A small MLP maps (initial condition, parameters) to attractor-class logits;

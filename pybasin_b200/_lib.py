@@ -31,6 +31,7 @@ SYS_DUFFING = 2
 SYS_LORENZ = 3
 SYS_LORENZ_MASKED = 4
 SYS_ROSSLER_NET = 5
+SYS_USER = 64
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -75,6 +76,7 @@ TRAJ_BAD_INPUT = 5
 MAX_FEATURES = 32
 MAX_CROSSING = 4
 MAX_PARAMS = 8
+MAX_USER_DIM = 16
 
 _c_i32 = ctypes.c_int32
 _c_i64 = ctypes.c_int64
@@ -154,6 +156,9 @@ EXPORTED_SYMBOLS = (
     "pb_probe_fma",
     "pb_solve_batch_noalloc",
     "pb_morton_keys",
+    "pb_rhs_compile",
+    "pb_solve_batch_rhs",
+    "pb_rhs_release",
 )
 
 
@@ -185,6 +190,16 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         lib.pb_label_nearest.argtypes = [
             _c_vp, _c_i64, _c_i32, _c_vp, _c_i32, _c_vp, _c_i32, _c_vp, _c_vp, _c_i32, _c_vp, _c_vp, _c_vp,
         ]
+        lib.pb_rhs_compile.restype = ctypes.c_int
+        lib.pb_rhs_compile.argtypes = [
+            ctypes.POINTER(ctypes.c_char_p), _c_i32, _c_i32, ctypes.c_char_p, _c_i32,
+            ctypes.POINTER(ctypes.c_char_p), _c_i32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p),
+            ctypes.c_char_p, _c_i64,
+        ]
+        lib.pb_solve_batch_rhs.restype = ctypes.c_int
+        lib.pb_solve_batch_rhs.argtypes = [_c_vp, ctypes.POINTER(SolveArgs), _c_vp]
+        lib.pb_rhs_release.restype = ctypes.c_int
+        lib.pb_rhs_release.argtypes = [_c_vp]
         lib.pb_morton_keys.restype = ctypes.c_int
         lib.pb_morton_keys.argtypes = [_c_vp, _c_i32, _c_i64, _c_i32, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp]
         lib.pb_query_occupancy.restype = ctypes.c_int

@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB_NAME = "libpybasin_b200.so"
-SOURCES = ["pb_api.cu", "pb_noalloc.cu", "pb_mlp.cu", "pb_order.cu"]
+SOURCES = ["pb_api.cu", "pb_noalloc.cu", "pb_mlp.cu", "pb_order.cu", "pb_rtc.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,7 +30,7 @@ def nvcc_path() -> str:
 
 def _inputs() -> list[Path]:
     files = [CSRC / s for s in SOURCES]
-    files += sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
+    files += sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted((ROOT / "include").glob("*.h"))
     return files
 
 
@@ -71,6 +71,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         "-o",
         str(tmp),
         *[str(CSRC / s) for s in SOURCES],
+        "-ldl",
     ]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

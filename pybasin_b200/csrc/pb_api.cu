@@ -8,6 +8,7 @@
 
 #include "pb_network.cuh"
 #include "pb_sample.cuh"
+#include "pb_launch.h"
 #include "pybasin_b200.h"
 
 namespace pb {
@@ -153,34 +154,27 @@ __global__ void __launch_bounds__(256) k_probe_fma(int iters, float* __restrict_
 // ---------------------------------------------------------------------------
 // kernel selection
 // ---------------------------------------------------------------------------
-using plain_fn = void (*)(const pb_solve_args);
-using queue_fn = void (*)(const pb_solve_args, int);
-
-struct KernelSel {
-    plain_fn plain = nullptr;        // inline dense output, one thread per trajectory
-    plain_fn plain_defer = nullptr;  // deferred pass 1
-    queue_fn queue = nullptr;        // inline dense output, persistent warps (also the redo pass)
-    queue_fn queue_defer = nullptr;  // deferred pass 1, persistent warps
-    queue_fn queue_probe = nullptr;  // deferred pass 1, probed schedule: probe phase
-    queue_fn queue_main = nullptr;   // deferred pass 1, probed schedule: main phase
-    plain_fn sample = nullptr;       // deferred pass 2 (no crossing columns)
-    plain_fn sample_cross = nullptr; // deferred pass 2 with crossing counts
-    int smem_per_thread = 0;         // inline kernels: per-thread statistics slot
-};
+template <class F>
+static KFn rt_fn(F* f)
+{
+    KFn k;
+    k.rt = reinterpret_cast<const void*>(f);
+    return k;
+}
 
 template <class Sys, class R>
 KernelSel select_prec()
 {
     KernelSel k;
     k.smem_per_thread = Stats<Sys::S>::kBytesPerThread;
-    k.plain = k_solve_plain<Sys, R, false>;
-    k.plain_defer = k_solve_plain<Sys, R, true>;
-    k.queue = k_solve_queue<Sys, R, false>;
-    k.queue_defer = k_solve_queue<Sys, R, true>;
-    k.queue_probe = k_solve_queue<Sys, R, true, 1>;
-    k.queue_main = k_solve_queue<Sys, R, true, 2>;
-    k.sample = k_sample<R, Sys::S, 0>;
-    k.sample_cross = k_sample<R, Sys::S, PB_MAX_CROSSING>;
+    k.plain = rt_fn(k_solve_plain<Sys, R, false>);
+    k.plain_defer = rt_fn(k_solve_plain<Sys, R, true>);
+    k.queue = rt_fn(k_solve_queue<Sys, R, false>);
+    k.queue_defer = rt_fn(k_solve_queue<Sys, R, true>);
+    k.queue_probe = rt_fn(k_solve_queue<Sys, R, true, 1>);
+    k.queue_main = rt_fn(k_solve_queue<Sys, R, true, 2>);
+    k.sample = rt_fn(k_sample<R, Sys::S, 0>);
+    k.sample_cross = rt_fn(k_sample<R, Sys::S, PB_MAX_CROSSING>);
     return k;
 }
 
@@ -211,17 +205,35 @@ static KernelSel find_kernel(int system, int dim, int precision, int schedule)
     }
 }
 
+// launches of a kernel handle: (pb_solve_args) or (pb_solve_args, int) arguments
+static cudaError_t launch_fn(const KFn& f, int64_t grid, int block, int smem, cudaStream_t st,
+                             const pb_solve_args& a, const int* extra)
+{
+    if (grid <= 0 || grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    pb_solve_args copy = a;
+    int x = extra ? *extra : 0;
+    void* argv[2] = {&copy, &x};
+    if (f.rt) return cudaLaunchKernel(f.rt, dim3(static_cast<unsigned>(grid)), dim3(block), argv, smem, st);
+    if (f.drv) return drv_launch(f.drv, static_cast<unsigned>(grid), block, smem, st, argv);
+    return cudaErrorInvalidDeviceFunction;
+}
+
 // Dynamic shared memory above the 48 KB default needs an opt-in per kernel.
-template <class F>
-static cudaError_t prepare_smem(F fn, int bytes)
+static cudaError_t prepare_smem(const KFn& f, int bytes)
 {
     if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (f.rt) return cudaFuncSetAttribute(f.rt, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return drv_set_max_smem(f.drv, bytes);
+}
+
+static cudaError_t occupancy(const KFn& f, int block, int smem, int* bps)
+{
+    if (f.rt) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, f.rt, block, smem);
+    return drv_occupancy(f.drv, block, smem, bps);
 }
 
 // Persistent grid for a queue kernel: resident blocks on every SM, capped by the work.
-template <class F>
-static cudaError_t persistent_grid(F fn, int block, int smem, int64_t n_traj, int requested, int64_t* grid)
+static cudaError_t persistent_grid(const KFn& f, int block, int smem, int64_t n_traj, int requested, int64_t* grid)
 {
     if (requested > 0) {
         *grid = requested;
@@ -229,7 +241,7 @@ static cudaError_t persistent_grid(F fn, int block, int smem, int64_t n_traj, in
         int dev = 0, sms = 0, bps = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, block, smem);
+        if (e == cudaSuccess) e = occupancy(f, block, smem, &bps);
         if (e != cudaSuccess) return e;
         *grid = static_cast<int64_t>(sms) * (bps > 0 ? bps : 1);
     }
@@ -288,9 +300,10 @@ static int map_cuda(cudaError_t e)
     return PB_ECUDA;
 }
 
-static int validate(const pb_solve_args* a)
+int validate_args(const pb_solve_args* a, bool user_system)
 {
     if (!a) return PB_EINVAL;
+    if ((a->system == PB_SYS_USER) != user_system) return PB_EINVALID_ODE;
     if (a->n_traj < 0 || a->n_ic < 0 || a->dim <= 0) return PB_EINVAL;
     if (a->n_traj > 0 && (!a->y0 || !a->params || !a->save_ts)) return PB_EINVAL;
     if (a->n_params < 0 || a->n_params > PB_MAX_PARAMS) return PB_EINVAL;
@@ -332,6 +345,88 @@ static int validate(const pb_solve_args* a)
     return PB_SUCCESS;
 }
 
+// The passes of one solve: pass 1 (plain, queue or probe + sort + main), the
+// sampling pass and the redo of record overflows for deferred dense output, then
+// the median pass.  `a` has been validated.
+int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
+{
+    const int zero = 0, one = 1;
+    if (a.n_traj == 0) return PB_SUCCESS;
+    const ScratchLayout sl = scratch_layout(a);
+    if (sl.total > 0 && !a.scratch) return PB_EINVAL;
+    if (sl.deferred && !a.queue_counter) return PB_EINVAL;  // the redo pass runs on the queue
+    // defaults from the launch-shape sweep: 64 for the queue schedules, 128 plain
+    const int block = a.block_size > 0 ? a.block_size : (a.schedule == PB_SCHED_PLAIN ? 128 : 64);
+    const int smem = k.smem_per_thread * block;
+    cudaError_t e = cudaSuccess;
+    const int64_t plain_grid = (a.n_traj + block - 1) / block;
+    if (plain_grid > 0x7fffffffLL) return PB_EINVAL;
+
+    if (sl.deferred) {
+        // pass 1: integrate, one record per window step holding save points
+        if (sl.probed) {
+            // probe phase, longest-first sort of its step counts, main phase
+            int64_t grid = 0;
+            e = persistent_grid(k.queue_probe, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return map_cuda(e);
+            e = launch_fn(k.queue_probe, grid, block, 0, st, a, &zero);
+            if (e == cudaSuccess) e = sort_by_probe(a, sl, st);
+            if (e == cudaSuccess) e = persistent_grid(k.queue_main, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return map_cuda(e);
+            e = launch_fn(k.queue_main, grid, block, 0, st, a, &zero);
+        } else if (a.schedule != PB_SCHED_PLAIN) {
+            int64_t grid = 0;
+            e = persistent_grid(k.queue_defer, block, 0, a.n_traj, a.grid_blocks, &grid);
+            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return map_cuda(e);
+            e = launch_fn(k.queue_defer, grid, block, 0, st, a, &zero);
+        } else {
+            e = launch_fn(k.plain_defer, plain_grid, block, 0, st, a, nullptr);
+        }
+        if (e != cudaSuccess) return map_cuda(e);
+        // pass 2: one warp per trajectory evaluates its save points and reduces the statistics
+        const int64_t sblocks = (a.n_traj + 3) / 4;
+        if (sblocks > 0x7fffffffLL) return PB_EINVAL;
+        bool any_cross = false;
+        for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
+        e = launch_fn(any_cross ? k.sample_cross : k.sample, sblocks, 128, 0, st, a, nullptr);
+        if (e != cudaSuccess) return map_cuda(e);
+        // pass 3: trajectories that exceeded the record capacity, inline
+        int64_t grid = 0;
+        e = prepare_smem(k.queue, smem);
+        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return map_cuda(e);
+        e = launch_fn(k.queue, grid, block, smem, st, a, &one);
+    } else if (a.schedule != PB_SCHED_PLAIN) {
+        int64_t grid = 0;
+        e = prepare_smem(k.queue, smem);
+        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
+        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return map_cuda(e);
+        e = launch_fn(k.queue, grid, block, smem, st, a, &zero);
+    } else {
+        e = prepare_smem(k.plain, smem);
+        if (e != cudaSuccess) return map_cuda(e);
+        e = launch_fn(k.plain, plain_grid, block, smem, st, a, nullptr);
+    }
+    if (e != cudaSuccess) return map_cuda(e);
+    MedianPlan plan;
+    if (count_median_cols(a, &plan) > 0) {
+        const int64_t rows = a.n_traj * plan.n_med;
+        const int64_t blocks = (rows + 7) / 8;
+        if (blocks > 0x7fffffffLL) return PB_EINVAL;
+        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
+            reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), a.n_traj,
+            a.n_save - a.win_begin, plan, a.features_out, a.n_features);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return map_cuda(e);
+    }
+    return PB_SUCCESS;
+}
+
 }  // namespace pb
 
 using namespace pb;
@@ -370,19 +465,15 @@ int pb_query_occupancy(int32_t system, int32_t dim, int32_t precision, int32_t s
                        int32_t* blocks_per_sm, int32_t* num_sms)
 {
     KernelSel k = find_kernel(system, dim, precision, schedule);
-    if (!k.plain) return PB_EINVALID_ODE;
+    if (!k.plain.ok()) return PB_EINVALID_ODE;
     if (block_size <= 0 || block_size % 32 || block_size > 256) return PB_EINVAL;
     int dev = 0, bps = 0, sms = 0;
     const int smem = k.smem_per_thread * block_size;
+    const KFn& f = schedule != PB_SCHED_PLAIN ? k.queue : k.plain;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (schedule != PB_SCHED_PLAIN) {
-        if (e == cudaSuccess) e = prepare_smem(k.queue, smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.queue, block_size, smem);
-    } else {
-        if (e == cudaSuccess) e = prepare_smem(k.plain, smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.plain, block_size, smem);
-    }
+    if (e == cudaSuccess) e = prepare_smem(f, smem);
+    if (e == cudaSuccess) e = occupancy(f, block_size, smem, &bps);
     if (e != cudaSuccess) return map_cuda(e);
     if (blocks_per_sm) *blocks_per_sm = bps;
     if (num_sms) *num_sms = sms;
@@ -412,91 +503,13 @@ static int solve_network(const pb_solve_args& a, cudaStream_t st)
 
 int pb_solve_batch(const pb_solve_args* args, void* stream)
 {
-    int v = validate(args);
+    int v = validate_args(args, false);
     if (v != PB_SUCCESS) return v;
     const pb_solve_args& a = *args;
     if (a.system == PB_SYS_ROSSLER_NET) return solve_network(a, static_cast<cudaStream_t>(stream));
     KernelSel k = find_kernel(a.system, a.dim, a.precision, a.schedule);
-    if (!k.plain) return PB_EINVALID_ODE;
-    if (a.n_traj == 0) return PB_SUCCESS;
-    const ScratchLayout sl = scratch_layout(a);
-    if (sl.total > 0 && !a.scratch) return PB_EINVAL;
-    if (sl.deferred && !a.queue_counter) return PB_EINVAL;  // the redo pass runs on the queue
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // defaults from the launch-shape sweep: 64 for the queue schedules, 128 plain
-    const int block = a.block_size > 0 ? a.block_size : (a.schedule == PB_SCHED_PLAIN ? 128 : 64);
-    const int smem = k.smem_per_thread * block;
-    cudaError_t e = cudaSuccess;
-    const int64_t plain_grid = (a.n_traj + block - 1) / block;
-    if (plain_grid > 0x7fffffffLL) return PB_EINVAL;
-
-    if (sl.deferred) {
-        // pass 1: integrate, one record per window step holding save points
-        if (sl.probed) {
-            // probe phase, longest-first sort of its step counts, main phase
-            int64_t grid = 0;
-            e = persistent_grid(k.queue_probe, block, 0, a.n_traj, a.grid_blocks, &grid);
-            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
-            if (e != cudaSuccess) return map_cuda(e);
-            k.queue_probe<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
-            e = cudaGetLastError();
-            if (e == cudaSuccess) e = sort_by_probe(a, sl, st);
-            if (e == cudaSuccess) e = persistent_grid(k.queue_main, block, 0, a.n_traj, a.grid_blocks, &grid);
-            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
-            if (e != cudaSuccess) return map_cuda(e);
-            k.queue_main<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
-        } else if (a.schedule != PB_SCHED_PLAIN) {
-            int64_t grid = 0;
-            e = persistent_grid(k.queue_defer, block, 0, a.n_traj, a.grid_blocks, &grid);
-            if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
-            if (e != cudaSuccess) return map_cuda(e);
-            k.queue_defer<<<static_cast<unsigned>(grid), block, 0, st>>>(a, 0);
-        } else {
-            k.plain_defer<<<static_cast<unsigned>(plain_grid), block, 0, st>>>(a);
-        }
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return map_cuda(e);
-        // pass 2: one warp per trajectory evaluates its save points and reduces the statistics
-        const int64_t sblocks = (a.n_traj + 3) / 4;
-        if (sblocks > 0x7fffffffLL) return PB_EINVAL;
-        bool any_cross = false;
-        for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
-        (any_cross ? k.sample_cross : k.sample)<<<static_cast<unsigned>(sblocks), 128, 0, st>>>(a);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return map_cuda(e);
-        // pass 3: trajectories that exceeded the record capacity, inline
-        int64_t grid = 0;
-        e = prepare_smem(k.queue, smem);
-        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
-        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
-        if (e != cudaSuccess) return map_cuda(e);
-        k.queue<<<static_cast<unsigned>(grid), block, smem, st>>>(a, 1);
-    } else if (a.schedule != PB_SCHED_PLAIN) {
-        int64_t grid = 0;
-        e = prepare_smem(k.queue, smem);
-        if (e == cudaSuccess) e = persistent_grid(k.queue, block, smem, a.n_traj, a.grid_blocks, &grid);
-        if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
-        if (e != cudaSuccess) return map_cuda(e);
-        k.queue<<<static_cast<unsigned>(grid), block, smem, st>>>(a, 0);
-    } else {
-        e = prepare_smem(k.plain, smem);
-        if (e != cudaSuccess) return map_cuda(e);
-        k.plain<<<static_cast<unsigned>(plain_grid), block, smem, st>>>(a);
-    }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return map_cuda(e);
-    MedianPlan plan;
-    if (count_median_cols(a, &plan) > 0) {
-        const int64_t rows = a.n_traj * plan.n_med;
-        const int64_t blocks = (rows + 7) / 8;
-        if (blocks > 0x7fffffffLL) return PB_EINVAL;
-        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
-            reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), a.n_traj,
-            a.n_save - a.win_begin, plan, a.features_out, a.n_features);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return map_cuda(e);
-    }
-    return PB_SUCCESS;
+    if (!k.plain.ok()) return PB_EINVALID_ODE;
+    return solve_with(k, a, static_cast<cudaStream_t>(stream));
 }
 
 int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, void* stream)

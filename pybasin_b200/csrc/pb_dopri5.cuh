@@ -25,12 +25,8 @@
 // keeps time, step size and the error-norm accumulation in FP64, and evaluates
 // the step-size factor in FP32.
 #pragma once
-#include <cuda_runtime.h>
-#include <math_constants.h>
-#include <stdint.h>
 
-#include <type_traits>
-
+#include "pb_compat.cuh"
 #include "pb_rhs.cuh"
 #include "pb_scratch.cuh"
 #include "pybasin_b200.h"
@@ -193,7 +189,10 @@ __device__ __forceinline__ double load_save(const pb_solve_args& a, int si)
 template <class Sys, class R>
 struct Integrator {
     static constexpr int S = Sys::S;
-    static constexpr bool MIXED = std::is_same<R, float>::value;
+    static constexpr bool MIXED = same_type<R, float>::value;
+    // FP32 phase clock (t mod 2 pi) for the built-in periodically forced systems;
+    // a system that declares kExactTime gets t in FP64 at every stage instead
+    static constexpr bool F32_CLOCK = MIXED && !exact_time<Sys>::value;
     using L_t = Lane<Sys, R>;
     using St = Stats<S>;
 
@@ -381,7 +380,7 @@ struct Integrator {
         if (st.d) st.reset();
 
         // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
-        if (MIXED) {
+        if constexpr (F32_CLOCK) {
             Sys::f(ClockF32{reduce_two_pi(a.t0)}, L.y, L.k1, L.p);
         } else {
             Sys::f(ClockF64{a.t0}, L.y, L.k1, L.p);
@@ -401,7 +400,7 @@ struct Integrator {
         R ytmp[S], ftmp[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) ytmp[s] = static_cast<R>(y0d[s] + h0 * static_cast<double>(L.k1[s]));
-        if (MIXED) {
+        if constexpr (F32_CLOCK) {
             Sys::f(ClockF32{reduce_two_pi(a.t0 + h0)}, ytmp, ftmp, L.p);
         } else {
             Sys::f(ClockF64{a.t0 + h0}, ytmp, ftmp, L.p);
@@ -555,7 +554,7 @@ struct Integrator {
         const double t = L.t;
         // the stage phase base depends on t only, so it is reduced while the
         // clipping and conversion of dt below are in flight
-        const float r0 = (MIXED && Sys::kTime) ? reduce_two_pi(t) : 0.f;
+        const float r0 = (F32_CLOCK && Sys::kTime) ? reduce_two_pi(t) : 0.f;
         double dt = L.dt;
         R h = static_cast<R>(dt);
         if (t + dt > a.t1) {
@@ -569,7 +568,7 @@ struct Integrator {
             return true;
         }
         R k2[S], k3[S], k4[S], k5[S], k6[S], k7[S], d[S], yn[S];
-        if (MIXED) {
+        if constexpr (F32_CLOCK) {
             stages(TimeBaseF32{r0, static_cast<float>(h)}, L, h, k2, k3, k4, k5, k6, k7, d, yn);
         } else {
             stages(TimeBaseF64{t, dt}, L, h, k2, k3, k4, k5, k6, k7, d, yn);

@@ -8,9 +8,7 @@
 // FP64 reduction per step, stage offsets added in FP32), which is all a
 // periodically forced system needs.
 #pragma once
-#include <cuda_runtime.h>
-
-#include <type_traits>
+#include "pb_compat.cuh"
 
 namespace pb {
 
@@ -24,6 +22,19 @@ struct ClockF32 {
 };
 
 __device__ __forceinline__ double clock_cos(const ClockF64& c) { return cos(c.t); }
+// stage instant of an FP64 clock (right-hand sides that use t itself, kExactTime)
+__device__ __forceinline__ double clock_time(const ClockF64& c) { return c.t; }
+
+// Sys::kExactTime if the system declares it, else false (the built-in systems use
+// cos(t) only, through the FP32 phase clock in the mixed kernel)
+template <class Sys, class = void>
+struct exact_time {
+    static constexpr bool value = false;
+};
+template <class Sys>
+struct exact_time<Sys, decltype(void(Sys::kExactTime))> {
+    static constexpr bool value = Sys::kExactTime;
+};
 __device__ __forceinline__ float clock_cos(const ClockF32& c)
 {
 #ifndef PB_ACCURATE_COS

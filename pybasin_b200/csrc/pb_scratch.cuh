@@ -16,7 +16,7 @@
 //   int32 n_records (-1 = capacity exceeded), int32 next_save, int32 status, int32 pad,
 //   double fill[dim]   (value of the save points after the last record)
 #pragma once
-#include <stdint.h>
+#include "pb_compat.cuh"
 
 #include "pybasin_b200.h"
 

@@ -57,6 +57,7 @@ class SolveRequest:
     window_record_cap: int = 0
     csr_row: torch.Tensor | None = None  # network systems: (n_nodes + 1,) int32
     csr_col: torch.Tensor | None = None  # network systems: (2 * n_edges,) int32
+    program: object | None = None  # SYS_USER: the compiled right-hand side (rhs.CompiledRHS)
 
 
 @dataclass
@@ -159,6 +160,17 @@ def _default_n_traj(req: SolveRequest) -> int:
     return req.y0.shape[0]
 
 
+def launch_solve(lib, args: L.SolveArgs, program, stream_handle: int) -> None:
+    """``pb_solve_batch``, or ``pb_solve_batch_rhs`` for a compiled user right-hand side."""
+    if args.system == L.SYS_USER:
+        if program is None:
+            raise ValueError("a user system needs its compiled program (ExpressionODE.program)")
+        L.check(lib.pb_solve_batch_rhs(ctypes.c_void_p(program.handle), ctypes.byref(args),
+                                       ctypes.c_void_p(stream_handle)), "pb_solve_batch_rhs")
+    else:
+        L.check(lib.pb_solve_batch(ctypes.byref(args), ctypes.c_void_p(stream_handle)), "pb_solve_batch")
+
+
 def solve(req: SolveRequest, stream: torch.cuda.Stream | None = None) -> SolveResult:
     """Launch one fused integration on ``stream`` (asynchronous)."""
     lib = L.load()
@@ -182,7 +194,7 @@ def solve(req: SolveRequest, stream: torch.cuda.Stream | None = None) -> SolveRe
         queue = torch.zeros((1,), dtype=torch.int64, device=dev)
         args = build_args(req, out, queue, None)
         scratch = alloc_scratch(args, dev)
-    L.check(lib.pb_solve_batch(ctypes.byref(args), ctypes.c_void_p(s.cuda_stream)), "pb_solve_batch")
+    launch_solve(lib, args, req.program, s.cuda_stream)
     # the scratch was allocated on `s`, so the caching allocator keeps it until the
     # kernels queued there before its release have run
     del scratch, queue

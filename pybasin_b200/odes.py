@@ -11,6 +11,9 @@ templated device functor; which one is chosen by (in order):
    (``PendulumODE``/``PendulumJaxODE``/``PendulumNumpyODE``, ``DuffingODE``...),
 3. names registered with :func:`register_system`.
 
+An object with ``b200_system = "user"`` (``pybasin_b200.rhs.ExpressionODE``)
+carries its own right-hand side as C expressions, compiled at run time.
+
 The classes defined here are minimal ODE systems with the reference's
 interface for users who do not have pybasin installed.
 """
@@ -32,6 +35,7 @@ SYSTEM_IDS: dict[str, int] = {
     "lorenz": L.SYS_LORENZ,
     "lorenz_masked": L.SYS_LORENZ_MASKED,
     "rossler_network": L.SYS_ROSSLER_NET,
+    "user": L.SYS_USER,  # expressions compiled at run time (pybasin_b200.rhs.ExpressionODE)
 }
 
 # reference class name -> system (case_studies/*/*_ode.py, tests/unit/solvers/test_solver.py)
@@ -59,6 +63,7 @@ _DIMS: dict[int, tuple[int, ...]] = {
     L.SYS_LORENZ: (3,),
     L.SYS_LORENZ_MASKED: (3,),
     L.SYS_ROSSLER_NET: tuple(3 * n for n in range(1, 129)),
+    L.SYS_USER: tuple(range(1, L.MAX_USER_DIM + 1)),
 }
 
 
@@ -104,6 +109,8 @@ def resolve_system(ode_system: Any, dim: int) -> SystemSpec:
             f"or call pybasin_b200.register_system (built-ins: {sorted(SYSTEM_IDS)})"
         )
     sid = tag if isinstance(tag, int) else SYSTEM_IDS[str(tag)]
+    if sid == L.SYS_USER and len(getattr(ode_system, "b200_rhs", ())) != dim:
+        raise ValueError(f"{type(ode_system).__name__} defines no right-hand side for state dimension {dim}")
     if dim not in _DIMS.get(sid, ()):
         raise ValueError(f"system '{_name_of(sid)}' does not support state dimension {dim}")
     params = params_array(ode_system)

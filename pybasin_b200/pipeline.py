@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import MortonOrder, SolveRequest, SolveResult, alloc_scratch, build_args
+from pybasin_b200.engine import MortonOrder, SolveRequest, SolveResult, alloc_scratch, build_args, launch_solve
 from pybasin_b200.odes import resolve_system
 from pybasin_b200.solver import B200Dopri5Solver
 
@@ -75,6 +75,7 @@ class BasinStabilityPipeline:
         self.n_groups = rows.shape[0]
         # rows 0..P-1: parameter points; row P: the templates' parameters
         self.params = torch.tensor(np.vstack([rows, tparams[None]]), dtype=torch.float64, device=self.dev)
+        self.ode_system = ode_system
         self.template_y0 = torch.tensor(template_y0, dtype=torch.float32, device=self.dev)
         self.morton = MortonOrder(self.dev)
         self.n_tpl = self.template_y0.shape[0]
@@ -134,6 +135,10 @@ class BasinStabilityPipeline:
             order=self.order if self.solver.order == "morton" else None,
             dense_mode=L.DENSE_DEFERRED if self.solver.dense_mode == "deferred" else L.DENSE_INLINE,
         )
+        self.program = None
+        if self.spec.system == L.SYS_USER:
+            prec = L.PREC_MIXED if self.solver.precision == "mixed" else L.PREC_FP64
+            self.program = self.ode_system.program(prec, dev.index if dev.index is not None else None)
         self.args = build_args(req, self.out, self.queue, None)
         self.scratch = alloc_scratch(self.args, dev)  # sized for the full capacity
         self._n = None
@@ -163,7 +168,7 @@ class BasinStabilityPipeline:
     def _launch(self) -> None:
         lib = L.load()
         s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
-        L.check(lib.pb_solve_batch(ctypes.byref(self.args), s), "pb_solve_batch")
+        launch_solve(lib, self.args, self.program, s.value or 0)
         n = self._n
         assert n is not None
         feats = self.out.features

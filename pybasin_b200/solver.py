@@ -289,6 +289,10 @@ class B200Dopri5Solver:
                 else:
                     order = ic_order
             csr_row = csr_col = None
+            program = None
+            if spec.system == L.SYS_USER:
+                program = ode_system.program(L.PREC_MIXED if self.precision == "mixed" else L.PREC_FP64,
+                                             dev.index if dev.index is not None else torch.cuda.current_device())
             if spec.system == L.SYS_ROSSLER_NET:
                 from pybasin_b200.network import network_csr
 
@@ -321,6 +325,7 @@ class B200Dopri5Solver:
                 dense_mode=L.DENSE_DEFERRED if self.dense_mode == "deferred" else L.DENSE_INLINE,
                 csr_row=csr_row,
                 csr_col=csr_col,
+                program=program,
             )
             res = solve(req, stream)
             if full:
