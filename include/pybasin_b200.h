@@ -266,7 +266,7 @@ int pb_solve_batch_noalloc(const pb_solve_args* args, void* stream);
  *   preamble     optional device code placed before the functor (helper
  *                __device__ functions), or NULL
  *   precision    pb_precision of the kernels to build
- *   include_dirs directories holding pb_sample.cuh and pybasin_b200.h; with
+ *   include_dirs directories holding pb_dopri5.cuh and pybasin_b200.h; with
  *                n_include_dirs = 0 they are found next to this library
  *                (../csrc and ../../include relative to its file)
  *   cache_dir    optional directory for compiled modules, keyed by a hash of the

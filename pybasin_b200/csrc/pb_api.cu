@@ -173,8 +173,6 @@ KernelSel select_prec()
     k.queue_defer = rt_fn(k_solve_queue<Sys, R, true>);
     k.queue_probe = rt_fn(k_solve_queue<Sys, R, true, 1>);
     k.queue_main = rt_fn(k_solve_queue<Sys, R, true, 2>);
-    k.sample = rt_fn(k_sample<R, Sys::S, 0>);
-    k.sample_cross = rt_fn(k_sample<R, Sys::S, PB_MAX_CROSSING>);
     return k;
 }
 
@@ -203,6 +201,34 @@ static KernelSel find_kernel(int system, int dim, int precision, int schedule)
         case PB_SYS_LORENZ_MASKED: return dim == 3 ? select_kernel<SysLorenz<true>>(precision) : KernelSel{};
         default: return {};
     }
+}
+
+// Sampling pass for `ns` feature states (shared by every system)
+template <class R, int NS>
+static KFn sample_of(bool cross)
+{
+    return cross ? rt_fn(k_sample<R, NS, PB_MAX_CROSSING>) : rt_fn(k_sample<R, NS, 0>);
+}
+
+template <class R>
+static KFn sample_kernel_r(int ns, bool cross)
+{
+    switch (ns) {
+        case 1: return sample_of<R, 1>(cross);
+        case 2: return sample_of<R, 2>(cross);
+        case 3: return sample_of<R, 3>(cross);
+        case 4: return sample_of<R, 4>(cross);
+        case 5: return sample_of<R, 5>(cross);
+        case 6: return sample_of<R, 6>(cross);
+        case 7: return sample_of<R, 7>(cross);
+        case 8: return sample_of<R, 8>(cross);
+        default: return KFn{};
+    }
+}
+
+static KFn sample_kernel(int precision, int ns, bool cross)
+{
+    return precision == PB_PREC_FP64 ? sample_kernel_r<double>(ns, cross) : sample_kernel_r<float>(ns, cross);
 }
 
 // launches of a kernel handle: (pb_solve_args) or (pb_solve_args, int) arguments
@@ -391,7 +417,16 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
         if (sblocks > 0x7fffffffLL) return PB_EINVAL;
         bool any_cross = false;
         for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
-        e = launch_fn(any_cross ? k.sample_cross : k.sample, sblocks, 128, 0, st, a, nullptr);
+        const KFn sample = sample_kernel(a.precision, count_stat_states(a), any_cross);
+        if (!sample.ok()) return PB_EUNSUPPORTED;
+        if (a.precision != PB_PREC_FP64) {
+            k_split_saves<<<(a.n_save + 255) / 256, 256, 0, st>>>(
+                a.save_ts, a.n_save,
+                reinterpret_cast<float2*>(static_cast<unsigned char*>(a.scratch) + sl.split_off));
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return map_cuda(e);
+        }
+        e = launch_fn(sample, sblocks, 128, 0, st, a, nullptr);
         if (e != cudaSuccess) return map_cuda(e);
         // pass 3: trajectories that exceeded the record capacity, inline
         int64_t grid = 0;

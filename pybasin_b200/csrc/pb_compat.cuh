@@ -1,7 +1,7 @@
 // Lets the kernel headers compile both under nvcc and under NVRTC (the runtime
 // compilation of user right-hand sides, pb_rtc.cu), where no host headers exist:
-// the fixed-width integer types, the two CUDART constants the kernels use, and a
-// type-equality trait.
+// the fixed-width integer types, the two CUDART constants the kernels use, and
+// two type traits.
 #pragma once
 #ifdef __CUDACC_RTC__
 typedef signed char int8_t;
@@ -28,5 +28,13 @@ struct same_type {
 template <class A>
 struct same_type<A, A> {
     static constexpr bool value = true;
+};
+template <bool B, class T, class F>
+struct pick_type {
+    using type = T;
+};
+template <class T, class F>
+struct pick_type<false, T, F> {
+    using type = F;
 };
 }  // namespace pb

@@ -22,8 +22,6 @@ struct KernelSel {
     KFn queue_defer;   // deferred pass 1, persistent warps
     KFn queue_probe;   // deferred pass 1, probed schedule: probe phase
     KFn queue_main;    // deferred pass 1, probed schedule: main phase
-    KFn sample;        // deferred pass 2 (no crossing columns)
-    KFn sample_cross;  // deferred pass 2 with crossing counts
     int smem_per_thread = 0;  // inline kernels: per-thread statistics slot
 };
 

@@ -123,13 +123,11 @@ const Nvrtc& nvrtc()
 }
 
 // kernels of one program, in KernelSel order
-constexpr int kNumKernels = 8;
+constexpr int kNumKernels = 6;  // the sampling pass is shared with the built-in systems
 
-std::vector<std::string> kernel_names(int precision, int dim)
+std::vector<std::string> kernel_names(int precision)
 {
-    const char* R = precision == PB_PREC_FP64 ? "double" : "float";
-    const int slots = dim < 8 ? dim : 8;  // the sampling pass sizes its arrays by feature states (< 8)
-    const std::string s(R), sl = std::to_string(slots);
+    const std::string s(precision == PB_PREC_FP64 ? "double" : "float");
     return {
         "pb::k_solve_plain<pb::SysUser, " + s + ", false>",
         "pb::k_solve_plain<pb::SysUser, " + s + ", true>",
@@ -137,15 +135,13 @@ std::vector<std::string> kernel_names(int precision, int dim)
         "pb::k_solve_queue<pb::SysUser, " + s + ", true, 0>",
         "pb::k_solve_queue<pb::SysUser, " + s + ", true, 1>",
         "pb::k_solve_queue<pb::SysUser, " + s + ", true, 2>",
-        "pb::k_sample<" + s + ", " + sl + ", 0>",
-        "pb::k_sample<" + s + ", " + sl + ", " + std::to_string(PB_MAX_CROSSING) + ">",
     };
 }
 
 std::string generate_source(const char* const* rhs, int dim, int n_params, const char* preamble)
 {
     std::string src;
-    src += "// generated by pb_rhs_compile\n#include \"pb_sample.cuh\"\nnamespace pb {\n";
+    src += "// generated by pb_rhs_compile\n#include \"pb_dopri5.cuh\"\nnamespace pb {\n";
     if (preamble) src += std::string(preamble) + "\n";
     src += "struct SysUser {\n";
     src += "    static constexpr int S = " + std::to_string(dim) + ";\n";
@@ -187,16 +183,23 @@ std::string library_dir()
     return k == std::string::npos ? "." : p.substr(0, k);
 }
 
-// cache file: "PBRHS1\n", the lowered kernel names one per line, "\n", the cubin
-bool read_cache(const std::string& path, std::vector<std::string>& names, std::string& cubin)
+bool read_file(const std::string& path, std::string& out)
 {
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) return false;
-    std::string data;
+    out.clear();
     char buf[1 << 16];
     size_t r;
-    while ((r = std::fread(buf, 1, sizeof buf, f)) > 0) data.append(buf, r);
+    while ((r = std::fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, r);
     std::fclose(f);
+    return true;
+}
+
+// cache file: "PBRHS1\n", the lowered kernel names one per line, "\n", the cubin
+bool read_cache(const std::string& path, std::vector<std::string>& names, std::string& cubin)
+{
+    std::string data;
+    if (!read_file(path, data)) return false;
     size_t pos = data.find('\n');
     if (pos == std::string::npos || data.compare(0, pos, "PBRHS1") != 0) return false;
     names.clear();
@@ -287,16 +290,27 @@ int pb_rhs_compile(const char* const* rhs, int32_t dim, int32_t n_params, const 
         opts.push_back("-I" + lib + "/../csrc");
         opts.push_back("-I" + lib + "/../../include");
     }
-    const std::vector<std::string> wanted = kernel_names(precision, dim);
+    const std::vector<std::string> wanted = kernel_names(precision);
 
-    // the key covers the generated source, the options, the kernels (precision)
-    // and the NVRTC version
+    // the key covers the generated source, the options, the kernels (precision),
+    // the NVRTC version and the kernel headers
     const Nvrtc& nv = nvrtc();
     int vmaj = 0, vmin = 0;
     if (nv.ok) nv.version(&vmaj, &vmin);
     std::string keytext = src;
     for (const auto& o : opts) keytext += "\n" + o;
     for (const auto& w : wanted) keytext += "\n" + w;
+    // and the kernel headers the program includes, read from the include paths
+    for (const char* h : {"pb_dopri5.cuh", "pb_rhs.cuh", "pb_scratch.cuh", "pb_compat.cuh", "pybasin_b200.h"}) {
+        for (const auto& o : opts) {
+            if (o.compare(0, 2, "-I") != 0) continue;
+            std::string text;
+            if (read_file(o.substr(2) + "/" + h, text)) {
+                keytext += "\n" + text;
+                break;
+            }
+        }
+    }
     keytext += "\nnvrtc " + std::to_string(vmaj) + "." + std::to_string(vmin);
     char keyhex[32];
     std::snprintf(keyhex, sizeof keyhex, "%016llx", static_cast<unsigned long long>(fnv1a(keytext)));
@@ -363,8 +377,8 @@ int pb_rhs_compile(const char* const* rhs, int32_t dim, int32_t n_params, const 
     p->n_params = n_params;
     p->precision = precision;
     p->module = mod;
-    KFn* slots[kNumKernels] = {&p->k.plain,       &p->k.plain_defer, &p->k.queue,  &p->k.queue_defer,
-                               &p->k.queue_probe, &p->k.queue_main,  &p->k.sample, &p->k.sample_cross};
+    KFn* slots[kNumKernels] = {&p->k.plain,     &p->k.plain_defer, &p->k.queue,
+                               &p->k.queue_defer, &p->k.queue_probe, &p->k.queue_main};
     for (int i = 0; i < kNumKernels; ++i) slots[i]->drv = fns[i];
     p->k.smem_per_thread = 6 * dim * 8 + (PB_MAX_CROSSING + 2) * 4;  // Stats<S>::kBytesPerThread
     *out = p;

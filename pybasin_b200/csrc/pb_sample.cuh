@@ -3,11 +3,17 @@
 //
 // One warp per trajectory; lane l takes records l, l + 32, ... of its
 // trajectory and evaluates the save points each record's step covers (no search,
-// no shuffles inside the sample loop).  The statistics match the inline path (torch_features_statistical.py
-// :30-110,:307-318 and torch_features_pattern.py:56-60 of the reference): a
-// shifted sum and sum of squares (shift = first window sample), min, max, last
-// sample, NaN flags and level crossings between consecutive samples, reduced
-// across the warp with shuffles.
+// no shuffles inside the sample loop).  The statistics match the inline path
+// (torch_features_statistical.py:30-110,307-318 and torch_features_pattern.py
+// :56-60 of the reference): a shifted sum and sum of squares (shift = first
+// window sample), min, max, last sample, NaN flags and level crossings between
+// consecutive samples, reduced across the warp with shuffles.
+//
+// The kernels are templated on the number of feature states NS (not on the
+// system), so every system, built-in or compiled at run time, shares them.  In
+// the FP32 pass the offset of a save point from its step start, ts - t, comes
+// from a (hi, lo) float split of both times (exact to a few float ulps of the
+// offset), so the sample loop runs without FP64 arithmetic or conversions.
 #pragma once
 #include "pb_dopri5.cuh"
 
@@ -43,27 +49,28 @@ __device__ __forceinline__ R dense_value(const R* c, R x)
 }
 
 // Per-lane window statistics accumulated by the sampling pass.
-template <int S>
+template <int NS>
 struct SampleAcc {
-    double sh[S], s1[S], s2[S], mn[S], mx[S], last[S];
+    double sh[NS], s1[NS], s2[NS], mn[NS], mx[NS], last[NS];
     int nan_flags;
     int cross_cnt[PB_MAX_CROSSING];
     double carry[PB_MAX_CROSSING];  // previous sample of each crossing state (the one before lane 0's)
     bool shift_set;
 };
 
-// Fold one batch of (up to 32) consecutive save points into the accumulators.
-// Lane l holds sample j = j0 + l (valid if l < nvalid).  Collective over the warp.
-template <int S>
-__device__ __forceinline__ void fold_samples(SampleAcc<S>& acc, const Plan& pl, const pb_solve_args& a, int64_t traj,
-                                             int64_t nwin, int j0, int nvalid, const double (&v)[S], int lane)
+// Fold one batch of (up to 32) consecutive save points into the accumulators
+// (the fill values after a stop).  Lane l holds sample j = j0 + l (valid if
+// l < nvalid).  Collective over the warp.
+template <int NS>
+__device__ __forceinline__ void fold_samples(SampleAcc<NS>& acc, const Plan& pl, const pb_solve_args& a,
+                                             int64_t traj, int64_t nwin, int j0, int nvalid, const double (&v)[NS],
+                                             int lane)
 {
-    const int ns = pl.ns;
     const int j = j0 + lane;
     const bool valid = lane < nvalid;
     if (!acc.shift_set) {  // shift = first window sample (lane 0 of the first batch)
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
+        for (int q = 0; q < NS; ++q) {
             const double f = __shfl_sync(0xffffffffu, v[q], 0);
             acc.sh[q] = isfinite(f) ? f : 0.0;
         }
@@ -71,8 +78,7 @@ __device__ __forceinline__ void fold_samples(SampleAcc<S>& acc, const Plan& pl, 
     }
     if (valid) {
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
-            if (q >= ns) continue;
+        for (int q = 0; q < NS; ++q) {
             const double d = v[q] - acc.sh[q];
             acc.s1[q] += d;
             acc.s2[q] = fma(d, d, acc.s2[q]);
@@ -101,9 +107,65 @@ __device__ __forceinline__ void fold_samples(SampleAcc<S>& acc, const Plan& pl, 
     }
 }
 
+// (hi, lo) float split of the save grid, for the FP32 sampling pass
+__global__ void __launch_bounds__(256) k_split_saves(const double* __restrict__ ts, int n, float2* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t = ts[i];
+    const float hi = static_cast<float>(t);
+    out[i] = make_float2(hi, static_cast<float>(t - static_cast<double>(hi)));
+}
+
+// Step-local offset x = (ts - t) / dt of save point j in a record starting at t.
+// FP32: from the split grid and the split record start; FP64: directly.
+struct OffsetF32 {
+    const float2* grid;
+    float t_hi, t_lo, inv_dt;
+    __device__ __forceinline__ OffsetF32(const float2* g, double t, double idt) : grid(g)
+    {
+        t_hi = static_cast<float>(t);
+        t_lo = static_cast<float>(t - static_cast<double>(t_hi));
+        inv_dt = static_cast<float>(idt);
+    }
+    __device__ __forceinline__ float at(int j) const
+    {
+        const float2 s = grid[j];
+        const float d = (s.x - t_hi) + (s.y - t_lo);
+        return d <= 1e-12f ? 0.f : d * inv_dt;  // save slack of dopri5_generic.zig:197
+    }
+};
+struct OffsetF64 {
+    const double* grid;
+    double t, inv_dt;
+    __device__ __forceinline__ OffsetF64(const double* g, double t0, double idt) : grid(g), t(t0), inv_dt(idt) {}
+    __device__ __forceinline__ double at(int j) const
+    {
+        const double ts = __ldg(grid + j);
+        return ts <= t + dp::save_slack ? 0.0 : (ts - t) * inv_dt;
+    }
+};
+
+template <class R>
+struct OffsetOf {
+    using type = OffsetF64;
+    __device__ __forceinline__ static OffsetF64 make(const float2*, const double* ts, double t, double idt)
+    {
+        return OffsetF64(ts, t, idt);
+    }
+};
+template <>
+struct OffsetOf<float> {
+    using type = OffsetF32;
+    __device__ __forceinline__ static OffsetF32 make(const float2* split, const double*, double t, double idt)
+    {
+        return OffsetF32(split, t, idt);
+    }
+};
+
 // NC = crossing states compiled in (0 when no column counts crossings, which
 // keeps the per-lane crossing registers out of the common case).
-template <class R, int S, int NC>
+template <class R, int NS, int NC>
 __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
 {
     __shared__ Plan pl;
@@ -111,19 +173,19 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t traj = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
-    if (traj >= a.n_traj) return;  // warp-uniform
+    if (traj >= a.n_traj || pl.ns != NS) return;  // warp-uniform
     const unsigned char* tl = tail_ptr(a, pl.sl, traj);
     const int nrec = reinterpret_cast<const int*>(tl)[0];
     if (nrec < 0) return;  // integrated again by the inline pass
     const int si_end = reinterpret_cast<const int*>(tl)[1];
     const double* fill = reinterpret_cast<const double*>(tl + 16);
-    const int ns = pl.ns;
     const int64_t nwin = a.n_save - a.win_begin;
-    const int iw = record_index_offset(ns, sizeof(R));
+    const int iw = record_index_offset(NS, sizeof(R));
+    const float2* split = reinterpret_cast<const float2*>(static_cast<const unsigned char*>(a.scratch) + pl.sl.split_off);
 
-    SampleAcc<S> acc;
+    SampleAcc<NS> acc;
 #pragma unroll
-    for (int q = 0; q < S; ++q) {
+    for (int q = 0; q < NS; ++q) {
         acc.sh[q] = 0.0;
         acc.s1[q] = 0.0;
         acc.s2[q] = 0.0;
@@ -150,40 +212,39 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
         const int hl = min(31, nrec - 1 - chunk);  // last lane holding a record
         const bool have = k < nrec;
         double rt = 0.0, rdt = 0.0;
-        R co[5 * S];
+        R co[5 * NS];
         int rsi = 0, rn = 0;
 #pragma unroll
-        for (int q = 0; q < 5 * S; ++q) co[q] = R(0);
+        for (int q = 0; q < 5 * NS; ++q) co[q] = R(0);
         if (have) {
             const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
             rt = reinterpret_cast<const double*>(rec)[0];
             rdt = reinterpret_cast<const double*>(rec)[1];
             const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
 #pragma unroll
-            for (int q = 0; q < 5 * S; ++q)
-                if (q < 5 * ns) co[q] = c[q];
+            for (int q = 0; q < 5 * NS; ++q) co[q] = c[q];
             rsi = reinterpret_cast<const int*>(rec + iw)[0];
             rn = reinterpret_cast<const int*>(rec + iw)[1];
         }
+        const auto off = OffsetOf<R>::make(split, a.save_ts, rt, rdt);
         if (!acc.shift_set) {  // shift = first window sample = first save of record 0 (lane 0)
-            const double ts = __ldg(a.save_ts + rsi);
-            const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) * rdt);
+            const R x = static_cast<R>(off.at(rsi));
 #pragma unroll
-            for (int q = 0; q < S; ++q) {
-                const R v = dense_value(co + 5 * q, x);
-                const double f = __shfl_sync(0xffffffffu, static_cast<double>(v), 0);
+            for (int q = 0; q < NS; ++q) {
+                const double f = __shfl_sync(0xffffffffu, static_cast<double>(dense_value(co + 5 * q, x)), 0);
                 acc.sh[q] = isfinite(f) ? f : 0.0;
             }
             acc.shift_set = true;
         }
-        R p1[S], p2[S], pmn[S], pmx[S], sh[S];
+        R p1[NS], p2[NS], pmn[NS], pmx[NS], sh[NS], vlast[NS];
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
+        for (int q = 0; q < NS; ++q) {
             p1[q] = R(0);
             p2[q] = R(0);
             pmn[q] = R(CUDART_INF);
             pmx[q] = R(-CUDART_INF);
             sh[q] = static_cast<R>(acc.sh[q]);
+            vlast[q] = R(0);
         }
         double cfirst[NC > 0 ? NC : 1], cprev[NC > 0 ? NC : 1];
         int ccnt[NC > 0 ? NC : 1];
@@ -193,27 +254,25 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
             cprev[c] = 0.0;
             ccnt[c] = 0;
         }
+        const bool with_median = pl.n_med > 0;
         for (int i = 0; i < rn; ++i) {
             const int j = rsi + i;
-            const double ts = __ldg(a.save_ts + j);
-            const R x = (ts <= rt + dp::save_slack) ? R(0) : static_cast<R>((ts - rt) * rdt);
-            R v[S];
+            const R x = static_cast<R>(off.at(j));
+            R v[NS];
 #pragma unroll
-            for (int q = 0; q < S; ++q) {
-                v[q] = R(0);
-                if (q >= ns) continue;  // uniform across the warp
+            for (int q = 0; q < NS; ++q) {
                 v[q] = dense_value(co + 5 * q, x);
                 const R d = v[q] - sh[q];
                 p1[q] += d;
-                p2[q] = fma(d, d, p2[q]);
+                p2[q] = fmad(d, d, p2[q]);  // NaN here iff a sample is NaN (the shift is finite)
                 pmn[q] = fmin(pmn[q], v[q]);
                 pmx[q] = fmax(pmx[q], v[q]);
-                if (v[q] != v[q]) acc.nan_flags |= 1 << q;
-                if (j == a.n_save - 1) acc.last[q] = static_cast<double>(v[q]);
+                vlast[q] = v[q];
             }
-            for (int m = 0; m < pl.n_med; ++m)
-                median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (j - a.win_begin)] =
-                    static_cast<float>(pick(v, pl.slot_of[pl.med_state[m]]));
+            if (with_median)
+                for (int m = 0; m < pl.n_med; ++m)
+                    median_ptr(a, pl.sl)[(traj * pl.n_med + m) * nwin + (j - a.win_begin)] =
+                        static_cast<float>(pick(v, pl.slot_of[pl.med_state[m]]));
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 if (c >= pl.n_cross) break;
@@ -224,12 +283,15 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
                 cprev[c] = cur;
             }
         }
+        const bool holds_last = have && rsi + rn == a.n_save;
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
+        for (int q = 0; q < NS; ++q) {
             acc.s1[q] += static_cast<double>(p1[q]);
             acc.s2[q] += static_cast<double>(p2[q]);
             acc.mn[q] = fmin(acc.mn[q], static_cast<double>(pmn[q]));
             acc.mx[q] = fmax(acc.mx[q], static_cast<double>(pmx[q]));
+            if (p2[q] != p2[q]) acc.nan_flags |= 1 << q;
+            if (holds_last) acc.last[q] = static_cast<double>(vlast[q]);
         }
         // crossings across record boundaries: lane l's first sample against lane
         // l-1's last (lane 0 against the carry from the previous chunk)
@@ -248,14 +310,14 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
     const int tail0 = max(si_end, static_cast<int>(a.win_begin));
     for (int j0 = tail0; j0 < a.n_save; j0 += 32) {
         const int nvalid = min(32, a.n_save - j0);
-        double v[S];
+        double v[NS];
 #pragma unroll
-        for (int q = 0; q < S; ++q) v[q] = q < ns ? fill[pl.stat_state[q < ns ? q : 0]] : 0.0;
+        for (int q = 0; q < NS; ++q) v[q] = fill[pl.stat_state[q]];
         fold_samples(acc, pl, a, traj, nwin, j0, nvalid, v, lane);
     }
     // warp reductions
 #pragma unroll
-    for (int q = 0; q < S; ++q) {
+    for (int q = 0; q < NS; ++q) {
         for (int o = 16; o > 0; o >>= 1) {
             acc.s1[q] += __shfl_xor_sync(0xffffffffu, acc.s1[q], o);
             acc.s2[q] += __shfl_xor_sync(0xffffffffu, acc.s2[q], o);

@@ -3,6 +3,7 @@
 //   [median windows]  n_traj x n_median_columns x window floats (PB_FEAT_MEDIAN)
 //   [step records]    n_traj x cap x record_stride bytes        (PB_DENSE_DEFERRED)
 //   [tails]           n_traj x tail_stride bytes                (PB_DENSE_DEFERRED)
+//   [split save grid] n_save x (float hi, float lo)            (PB_DENSE_DEFERRED)
 //   [saved states]    n_traj x state_stride bytes               (PB_SCHED_PROBED)
 //   [sort keys/values] 4 x n_traj int32, then the radix-sort temporary storage
 //                     (PB_SCHED_PROBED; the temporary's size is added on the host)
@@ -36,6 +37,7 @@ struct ScratchLayout {
     int64_t val_in_off;    // trajectory ids, in queue order
     int64_t val_out_off;   // trajectory ids, longest predicted first
     int64_t sort_tmp_off;  // radix-sort temporary storage (last)
+    int64_t split_off;     // deferred dense output: (hi, lo) float split of the save grid
     int64_t total;         // excluding the radix-sort temporary
     int32_t rec_stride;
     int32_t cap;
@@ -95,6 +97,8 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
         l.tail_stride = static_cast<int32_t>(align_up(16 + 8 * a.dim, 16));
         l.tail_off = off;
         off = align_up(off + a.n_traj * l.tail_stride, 256);
+        l.split_off = off;
+        off = align_up(off + static_cast<int64_t>(a.n_save) * 8, 256);
         l.probed = (a.schedule == PB_SCHED_PROBED) ? 1 : 0;
         if (l.probed) {
             l.state_stride = saved_state_bytes(a.dim, rsize);
