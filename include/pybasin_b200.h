@@ -301,6 +301,22 @@ int pb_rhs_release(pb_rhs_program* prog);
 int pb_mlp_gemm(const void* A, int64_t sam, int64_t sak, const void* B, int64_t sbk, int64_t sbn,
                 const float* bias, float alpha, int32_t M, int32_t N, int32_t K, int32_t gelu,
                 float* c_f32, void* c_bf16, float* z_pre, int64_t ldc, void* stream);
+/* MLP inference on the 5th-generation tensor cores (tcgen05.mma, FP32
+ * accumulators in tensor memory): the whole network for 128 rows per CTA, the
+ * activations kept in shared memory between layers, GELU after every layer but
+ * the last.  x: device (n, d_in) BF16.  Layer l has n_pad[l] x k_pad[l] weights
+ * (multiples of 16, <= 256, k_pad[l] = n_pad[l-1], k_pad[0] >= d_in) packed in
+ * the MMA operand layout (8 x 8 BF16 core matrices, core (n/8, k/8) at
+ * ((n/8)*(k_pad/8) + k/8) * 128 bytes, rows of a core 16 bytes apart; zero
+ * padding), 16-byte aligned, and n_real[l] biases (FP32).  w_packed, bias,
+ * n_pad, k_pad, n_real are host arrays of n_layers entries (<= 8).  logits:
+ * device (n, n_classes) FP32.  error_flag (device int32, optional) is set to 1
+ * if a CTA gave up waiting on its tensor-core or copy completion. */
+int pb_mlp_infer_tc(const void* x_bf16, int64_t n, int32_t d_in, int32_t n_layers,
+                    const void* const* w_packed, const float* const* bias, const int32_t* n_pad,
+                    const int32_t* k_pad, const int32_t* n_real, float* logits, int32_t n_classes,
+                    int32_t* error_flag, void* stream);
+
 /* dz = dy * GELU'(z) elementwise (BF16 and/or FP32 outputs). */
 int pb_mlp_gelu_backward(const float* dy, const float* z, int64_t n, void* dz_bf16, float* dz_f32, void* stream);
 /* Softmax cross-entropy of (M x C) logits against labels (NULL: no loss):

@@ -13,6 +13,7 @@ audit.  There is no counterpart in the reference.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -39,7 +40,10 @@ def _bind(lib: ctypes.CDLL) -> None:
     lib.pb_surrogate_gate.argtypes = [vp, i64, i32, f32, vp, vp, vp, vp, vp, vp]
     lib.pb_gather_rows.argtypes = [vp, i32, vp, vp, i64, vp, vp]
     lib.pb_merge_labels.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    lib.pb_mlp_infer_tc.argtypes = [vp, i64, i32, i32, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                    ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, i32, vp, vp]
     for name in (
+        "pb_mlp_infer_tc",
         "pb_mlp_gemm",
         "pb_mlp_gelu_backward",
         "pb_mlp_softmax_xent",
@@ -53,6 +57,39 @@ def _bind(lib: ctypes.CDLL) -> None:
     ):
         getattr(lib, name).restype = ctypes.c_int
     lib._pb_mlp_bound = True
+
+
+def pack_tc_weights(W: torch.Tensor) -> torch.Tensor:
+    """BF16 weights (N, K) -> the tensor-core operand layout of ``pb_mlp_infer_tc``:
+    N and K padded to multiples of 16, 8x8 core matrices, core (n/8, k/8) at
+    ((n/8) * (K/8) + k/8) * 64 elements."""
+    N, K = W.shape
+    Np, Kp = -(-N // 16) * 16, -(-K // 16) * 16
+    Wp = torch.zeros((Np, Kp), dtype=torch.bfloat16, device=W.device)
+    Wp[:N, :K] = W.to(torch.bfloat16)
+    return Wp.view(Np // 8, 8, Kp // 8, 8).permute(0, 2, 1, 3).contiguous().view(-1)
+
+
+def infer_tc(x: torch.Tensor, packed: list[torch.Tensor], biases: list[torch.Tensor], shapes: list[tuple[int, int, int]],
+             n_classes: int, error: torch.Tensor | None = None) -> torch.Tensor:
+    """Logits (n, n_classes) of BF16 inputs x through ``pb_mlp_infer_tc``.
+
+    ``shapes[l] = (n_pad, k_pad, n_real)`` of layer l."""
+    lib = L.load()
+    _bind(lib)
+    n, d_in = x.shape
+    nl = len(packed)
+    out = torch.empty((n, n_classes), dtype=torch.float32, device=x.device)
+    vp = ctypes.c_void_p
+    w_arr = (vp * nl)(*[p.data_ptr() for p in packed])
+    b_arr = (vp * nl)(*[b.data_ptr() for b in biases])
+    n_pad = (ctypes.c_int32 * nl)(*[s[0] for s in shapes])
+    k_pad = (ctypes.c_int32 * nl)(*[s[1] for s in shapes])
+    n_real = (ctypes.c_int32 * nl)(*[s[2] for s in shapes])
+    xc = x.contiguous()
+    L.check(lib.pb_mlp_infer_tc(_p(xc), n, d_in, nl, w_arr, b_arr, n_pad, k_pad, n_real, _p(out), n_classes,
+                                _p(error), torch.cuda.current_stream(x.device).cuda_stream), "pb_mlp_infer_tc")
+    return out
 
 
 def gemm(
@@ -254,8 +291,30 @@ class MLPSurrogate:
         return hist
 
     # -- inference -----------------------------------------------------------------
+    def tc_supported(self) -> bool:
+        """The network fits the fused tensor-core kernel (all widths <= 256, <= 8 layers)."""
+        dims = [self.d_in] + [w.shape[0] for w in self.Wb]
+        return self.n_layers <= 8 and max(dims) <= 256 and os.environ.get("PB_MLP_TC", "1") != "0"
+
+    def packed_tc(self) -> tuple[list[torch.Tensor], list[tuple[int, int, int]]]:
+        """Weights in the tensor-core operand layout (rebuilt after every optimiser step)."""
+        if getattr(self, "_tc_step", None) != self._step:
+            packed, shapes = [], []
+            for li, W in enumerate(self.Wb):
+                N, K = W.shape
+                packed.append(pack_tc_weights(W))
+                shapes.append((-(-N // 16) * 16, -(-K // 16) * 16, N))
+            self._tc_cache = (packed, shapes)
+            self._tc_step = self._step
+        return self._tc_cache
+
     def logits(self, x_in: torch.Tensor, chunk: int = 1 << 20) -> torch.Tensor:
+        """Inference logits: the fused tensor-core kernel when the network fits it,
+        else the layer-by-layer GEMM path of training."""
         n = x_in.shape[0]
+        if self.tc_supported():
+            packed, shapes = self.packed_tc()
+            return infer_tc(x_in, packed, self.b, shapes, self.n_classes)
         out = torch.empty((n, self.n_classes), dtype=torch.float32, device=self.dev)
         for c0 in range(0, n, chunk):
             out[c0 : c0 + chunk] = self.forward(x_in[c0 : c0 + chunk])
@@ -272,5 +331,6 @@ class MLPSurrogate:
         self.W = [torch.tensor(d[f"W{i}"], device=self.dev) for i in range(self.n_layers)]
         self.b = [torch.tensor(d[f"b{i}"], device=self.dev) for i in range(self.n_layers)]
         self.Wb = [w.to(torch.bfloat16) for w in self.W]
+        self._tc_step = None  # repack the tensor-core weights
         self.shift = torch.tensor(d["shift"], device=self.dev)
         self.scale = torch.tensor(d["scale"], device=self.dev)

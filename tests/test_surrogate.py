@@ -158,3 +158,50 @@ def test_gated_pipeline_matches_integrator_labels_on_duffing():
     dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
     assert float(dbs) <= 0.005
     assert float((label == ref).double().mean()) >= 0.99
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,N,K,d_in", [(300, 256, 256, 256), (129, 80, 48, 40), (7, 16, 16, 5)])
+def test_tensor_core_layer_matches_fp64_product_of_bf16_operands(M, N, K, d_in):
+    """One layer (no activation) of the tcgen05 inference kernel: x W^T + b."""
+    from pybasin_b200.surrogate import infer_tc, pack_tc_weights
+
+    rng = np.random.default_rng(M + N)
+    x = _bf16(rng.normal(size=(M, d_in)))
+    w = _bf16(rng.normal(size=(N, d_in)))
+    bias = rng.normal(size=N).astype(np.float32)
+    dev = torch.device("cuda:0")
+    X = torch.tensor(x, device=dev).to(torch.bfloat16)
+    W = torch.tensor(w, device=dev).to(torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    out = infer_tc(X, [pack_tc_weights(W)], [torch.tensor(bias, device=dev)], [(N, K, N)], N, error=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    z = x @ w.T + bias
+    scale = np.abs(z).max()
+    np.testing.assert_allclose(out.cpu().numpy(), z, rtol=0, atol=1e-5 * scale)
+
+
+@pytest.mark.gpu
+def test_tensor_core_mlp_matches_layer_by_layer_forward():
+    """The fused tcgen05 network (activations kept in shared memory) against the
+    training forward (mma.sync GEMMs, activations through HBM): both round the
+    activations to BF16 after each layer; the FP32 sums differ in order only."""
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(5, 6, hidden=256, depth=4, seed=3, device=dev)
+    g = torch.Generator().manual_seed(0)
+    x = (torch.randn(1000, 5, generator=g) * 2).to(dev).to(torch.bfloat16)
+    ref = net.forward(x)
+    packed, shapes = net.packed_tc()
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    from pybasin_b200.surrogate import infer_tc
+
+    tc = infer_tc(x, packed, net.b, shapes, 6, error=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    scale = ref.abs().max().item()
+    assert (tc - ref).abs().max().item() <= 2e-2 * scale
+    assert (tc.argmax(1) == ref.argmax(1)).float().mean().item() >= 0.995
+    assert torch.equal(net.logits(x), tc)  # inference takes the tensor-core path
