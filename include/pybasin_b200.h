@@ -52,6 +52,7 @@ typedef enum {
     PB_SYS_LORENZ = 3,        /* case_studies/lorenz/lorenz_jax_ode.py, p=[sigma,r,b] */
     PB_SYS_LORENZ_MASKED = 4, /* case_studies/lorenz/lorenz_ode.py:28-64 (|y|>=200 freezes) */
     PB_SYS_ROSSLER_NET = 5,   /* case_studies/rossler_network/rossler_network_jax_ode.py:53-79 */
+    PB_SYS_FRICTION = 6,      /* case_studies/friction/friction_ode.py:32-75, p=[v_d,xi,musd,mud,muv,v0] */
     PB_SYS_USER = 64          /* a right-hand side compiled at run time (pb_rhs_compile),
                                  solved with pb_solve_batch_rhs */
 } pb_system;

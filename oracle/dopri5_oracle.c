@@ -110,6 +110,20 @@ static void rhs(int sys, double t, const double *y, double *dy, const double *p,
         }
         break;
     }
+    case ORACLE_SYS_FRICTION: { /* [v_d, xi, musd, mud, muv, v0]; case_studies/friction/friction_ode.py:32-75 */
+        const double vd = p[0], xi = p[1], musd = p[2], mud = p[3], muv = p[4], v0 = p[5];
+        const double disp = y[0], vel = y[1];
+        const double vrel = vel - vd, eta = 1e-4, k_smooth = 50.0;
+        const double f_fric = mud + mud * (musd - 1.0) * exp(-fabs(vrel) / v0) + muv * fabs(vrel) / v0;
+        const int slip = fabs(vrel) > eta;
+        const int trans = fabs(disp + 2.0 * xi * vel) > mud * musd;
+        const double slip_vel = -disp - 2.0 * xi * vel - tanh(k_smooth * vrel) * f_fric;
+        const double trans_vel = -disp - 2.0 * xi * vel + mud * musd * tanh(k_smooth * f_fric);
+        const double stick_vel = -(vel - vd);
+        dy[0] = (slip || trans) ? vel : vd;
+        dy[1] = slip ? slip_vel : (trans ? trans_vel : stick_vel);
+        break;
+    }
     default:
         for (int i = 0; i < dim; ++i) dy[i] = NAN;
     }

@@ -10,6 +10,7 @@ enum {
     ORACLE_SYS_LORENZ = 3,
     ORACLE_SYS_LORENZ_MASKED = 4,
     ORACLE_SYS_ROSSLER_NET = 5,
+    ORACLE_SYS_FRICTION = 6,
 };
 
 /* feature kinds: same numbering as the CUDA library's PB_FEAT_* */

@@ -23,6 +23,7 @@ SYS_DUFFING = 2
 SYS_LORENZ = 3
 SYS_LORENZ_MASKED = 4
 SYS_ROSSLER_NET = 5
+SYS_FRICTION = 6
 
 STATUS_OK = 0
 STATUS_MAX_STEPS = 1

@@ -4,11 +4,20 @@ Drop-in pieces for the reference's pipeline:
 
 * :class:`B200Dopri5Solver` — a ``SolverProtocol`` solver (replaces ``TorchDiffEqSolver``),
 * :class:`FusedFeatureExtractor` — the ``TorchFeatureExtractor`` API over in-kernel statistics,
-* :func:`register_system` — map an ODE class to a built-in device right-hand side.
+* :func:`register_system` — map an ODE class to a built-in device right-hand side,
+* :class:`pybasin_b200.rhs.ExpressionODE` — a user ODE compiled at run time.
 """
 
-from pybasin_b200.features import FusedFeatureExtractor, impute_extreme
-from pybasin_b200.odes import DuffingODE, LinearODE, LorenzODE, PendulumODE, register_system, resolve_system
+from pybasin_b200.features import FrictionFeatureExtractor, FusedFeatureExtractor, impute_extreme
+from pybasin_b200.odes import (
+    DuffingODE,
+    FrictionODE,
+    LinearODE,
+    LorenzODE,
+    PendulumODE,
+    register_system,
+    resolve_system,
+)
 from pybasin_b200.solver import B200Dopri5Solver, IntegrationResult
 
 __all__ = [
@@ -22,4 +31,6 @@ __all__ = [
     "DuffingODE",
     "LorenzODE",
     "LinearODE",
+    "FrictionODE",
+    "FrictionFeatureExtractor",
 ]

@@ -31,6 +31,7 @@ SYS_DUFFING = 2
 SYS_LORENZ = 3
 SYS_LORENZ_MASKED = 4
 SYS_ROSSLER_NET = 5
+SYS_FRICTION = 6
 SYS_USER = 64
 
 PREC_FP64 = 0

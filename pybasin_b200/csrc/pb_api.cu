@@ -199,6 +199,7 @@ static KernelSel find_kernel(int system, int dim, int precision, int schedule)
         case PB_SYS_DUFFING: return dim == 2 ? select_kernel<SysDuffing>(precision) : KernelSel{};
         case PB_SYS_LORENZ: return dim == 3 ? select_kernel<SysLorenz<false>>(precision) : KernelSel{};
         case PB_SYS_LORENZ_MASKED: return dim == 3 ? select_kernel<SysLorenz<true>>(precision) : KernelSel{};
+        case PB_SYS_FRICTION: return dim == 2 ? select_kernel<SysFriction>(precision) : KernelSel{};
         default: return {};
     }
 }

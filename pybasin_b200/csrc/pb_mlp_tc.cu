@@ -9,7 +9,9 @@
 // streamed from global memory / L2 into shared memory by bulk copies completing
 // on an mbarrier; the copy for layer l+1 starts as soon as the MMAs of layer l
 // have finished reading, overlapping the epilogue.  One thread issues the MMAs;
-// 4 warps (one per 32 TMEM lanes) run the epilogue.
+// 16 warps run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (the
+// lane quarter a warp may access) and every fourth 32-column chunk starting at
+// chunk w / 4, so the bias + GELU work is spread over 512 threads.
 //
 // Operand layout (K-major, no swizzle): 8-row x 16-byte core matrices, core
 // (row/8, k/8) at ((row/8) * (K/8) + k/8) * 128 bytes; in the shared-memory
@@ -29,7 +31,8 @@ namespace {
 constexpr int kRows = 128;      // rows per CTA = MMA M = TMEM lanes used
 constexpr int kMaxDim = 256;    // largest K and N of a layer
 constexpr int kMaxLayers = 8;
-constexpr int kThreads = 128;
+constexpr int kThreads = 512;
+constexpr int kColGroups = kThreads / 128;  // warps sharing one TMEM lane quarter
 constexpr uint32_t kTmemCols = 256;
 constexpr int kABytes = kRows * kMaxDim * 2;      // activations, 64 KB
 constexpr int kBBytes = kMaxDim * kMaxDim * 2;    // one layer's weights, 128 KB
@@ -165,10 +168,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_infer_tc(const MlpTcArgs p)
     uint8_t* Bs = smem + kABytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kABytes + kBBytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quarter = warp & 3, cgroup = warp >> 2;
+    const int trow = quarter * 32 + lane;  // this thread's row of the tile (its TMEM lane)
     const uint32_t bar_w = smem_u32(&bars[0]), bar_m = smem_u32(&bars[1]);
     const uint32_t a_smem = smem_u32(As), b_smem = smem_u32(Bs);
-    const int64_t row = static_cast<int64_t>(blockIdx.x) * kRows + tid;
+    const int64_t row0 = static_cast<int64_t>(blockIdx.x) * kRows;
+    const int64_t row = row0 + trow;
 
     if (tid == 0) {
         mbar_init(bar_w, 1);
@@ -187,14 +193,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_infer_tc(const MlpTcArgs p)
     const uint32_t tmem = *tmem_slot;
 
     if (tid == 0) load_weights(p, 0, b_smem, bar_w);
-    {  // layer-0 operand: row tid of the tile, zero beyond d_in and beyond n
+    {  // layer-0 operand, 8 columns of one row per step; zero beyond d_in and beyond n
         const int K = p.k_pad[0];
-        for (int k = 0; k < K; k += 8) {
+        for (int idx = tid; idx < kRows * (K >> 3); idx += kThreads) {
+            const int r = idx & (kRows - 1), k = (idx / kRows) * 8;
+            const int64_t gr = row0 + r;
             __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j)
-                h[j] = (row < p.n && k + j < p.d_in) ? p.x[row * p.d_in + k + j] : __float2bfloat16(0.f);
-            *reinterpret_cast<uint4*>(As + core_offset(tid, k, K)) = *reinterpret_cast<const uint4*>(h);
+                h[j] = (gr < p.n && k + j < p.d_in) ? p.x[gr * p.d_in + k + j] : __float2bfloat16(0.f);
+            *reinterpret_cast<uint4*>(As + core_offset(r, k, K)) = *reinterpret_cast<const uint4*>(h);
         }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -224,9 +232,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_infer_tc(const MlpTcArgs p)
         const bool last = l + 1 == p.n_layers;
         const float* bias = p.b[l];
         const int nr = p.n_real[l];
-        for (int c0 = 0; c0 < N; c0 += 32) {
+        for (int c0 = cgroup * 32; c0 < N; c0 += 32 * kColGroups) {
             uint32_t v[32];
-            tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), v);
+            tmem_ld32(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(c0), v);
             if (!last) {
                 for (int g = 0; g < 32 && c0 + g < N; g += 8) {
                     __align__(16) __nv_bfloat16 h[8];
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_infer_tc(const MlpTcArgs p)
                         const float z = __uint_as_float(v[g + j]) + (c < nr ? __ldg(bias + c) : 0.f);
                         h[j] = __float2bfloat16(c < nr ? gelu(z) : 0.f);
                     }
-                    *reinterpret_cast<uint4*>(As + core_offset(tid, c0 + g, N)) = *reinterpret_cast<const uint4*>(h);
+                    *reinterpret_cast<uint4*>(As + core_offset(trow, c0 + g, N)) = *reinterpret_cast<const uint4*>(h);
                 }
             } else if (row < p.n) {
 #pragma unroll

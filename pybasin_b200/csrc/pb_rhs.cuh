@@ -124,6 +124,37 @@ struct SysDuffing {
     }
 };
 
+// Friction oscillator with a smoothed stick-slip law, p = [v_d, xi, musd, mud,
+// muv, v0] (case_studies/friction/friction_ode.py:32-75): slip when
+// |v - v_d| > 1e-4, else a transition when |x + 2 xi v| > mud musd, else stick.
+__device__ __forceinline__ float r_exp(float x) { return expf(x); }
+__device__ __forceinline__ double r_exp(double x) { return exp(x); }
+__device__ __forceinline__ float r_tanh(float x) { return tanhf(x); }
+__device__ __forceinline__ double r_tanh(double x) { return tanh(x); }
+
+struct SysFriction {
+    static constexpr int S = 2;
+    static constexpr int NP = 6;
+    static constexpr bool kTime = false;
+    template <class R, class C>
+    __device__ __forceinline__ static void f(const C&, const R* y, R* dy, const R* p)
+    {
+        const R vd = p[0], xi = p[1], musd = p[2], mud = p[3], muv = p[4], v0 = p[5];
+        const R disp = y[0], vel = y[1];
+        const R vrel = vel - vd;
+        const R avr = r_abs(vrel) / v0;
+        const R f_fric = fmad(muv, avr, fmad(mud * (musd - R(1)), r_exp(-avr), mud));
+        const R base = fmad(R(-2) * xi, vel, -disp);  // -disp - 2 xi vel
+        const bool slip = r_abs(vrel) > R(1e-4);
+        const bool trans = r_abs(base) > mud * musd;
+        const R slip_vel = fmad(-r_tanh(R(50) * vrel), f_fric, base);
+        const R trans_vel = fmad(mud * musd, r_tanh(R(50) * f_fric), base);
+        const R stick_vel = vd - vel;
+        dy[0] = (slip || trans) ? vel : vd;
+        dy[1] = slip ? slip_vel : (trans ? trans_vel : stick_vel);
+    }
+};
+
 // Lorenz system, p = [sigma, r, b].  MASKED freezes the flow once max|y| >= 200
 // (case_studies/lorenz/lorenz_ode.py:28-64); the plain variant is the JAX one
 // used with a stop event (case_studies/lorenz/lorenz_jax_ode.py).

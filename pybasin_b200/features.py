@@ -177,3 +177,39 @@ class FusedFeatureExtractor:
         if self._extracted_feature_names is None:
             raise RuntimeError("Feature names not available. Call extract_features first.")
         return self._extracted_feature_names
+
+
+class FrictionFeatureExtractor:
+    """The friction case study's extractor (case_studies/friction/friction_feature_extractor.py
+    :17-41): one-hot [FP, LC] from max |y_1| over the window (FP if <= 0.2), with the
+    maximum computed inside the integrator (``PB_FEAT_ABSMAX``)."""
+
+    def __init__(self, time_steady: float | None = None, state: int = 1, threshold: float = 0.2,
+                 device: str | torch.device = "cpu"):
+        self.time_steady = time_steady
+        self.state = state
+        self.threshold = threshold
+        self.device = device
+        self.normalize = False
+
+    def columns(self, num_states: int) -> list[FeatureColumn]:
+        if not 0 <= self.state < num_states:
+            raise ValueError(f"state {self.state} outside the {num_states}-dim system")
+        return [FeatureColumn(self.state, L.FEAT_ABSMAX, 0.0, f"state_{self.state}__absolute_maximum")]
+
+    def resolve_time_steady(self, save_ts: torch.Tensor) -> float:
+        if self.time_steady is not None:
+            return float(self.time_steady)
+        t0, t1 = float(save_ts[0]), float(save_ts[-1])
+        return t0 + DEFAULT_STEADY_FRACTION * (t1 - t0)
+
+    def extract_features(self, solution: Any) -> torch.Tensor:
+        feats = getattr(solution.y, "_pb_features", None)
+        if feats is None:
+            raise RuntimeError("FrictionFeatureExtractor reads features computed inside B200Dopri5Solver")
+        lc = (feats[:, 0] > self.threshold).to(torch.float64)
+        return torch.stack([1.0 - lc, lc], dim=1)
+
+    @property
+    def feature_names(self) -> list[str]:
+        return ["FP", "LC"]

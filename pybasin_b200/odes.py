@@ -35,6 +35,7 @@ SYSTEM_IDS: dict[str, int] = {
     "lorenz": L.SYS_LORENZ,
     "lorenz_masked": L.SYS_LORENZ_MASKED,
     "rossler_network": L.SYS_ROSSLER_NET,
+    "friction": L.SYS_FRICTION,
     "user": L.SYS_USER,  # expressions compiled at run time (pybasin_b200.rhs.ExpressionODE)
 }
 
@@ -54,6 +55,8 @@ _CLASS_MAP: dict[str, str] = {
     "LinearODE": "linear",
     "RosslerNetworkJaxODE": "rossler_network",
     "RosslerNetworkODE": "rossler_network",
+    "FrictionODE": "friction",
+    "FrictionJaxODE": "friction",
 }
 
 _DIMS: dict[int, tuple[int, ...]] = {
@@ -63,6 +66,7 @@ _DIMS: dict[int, tuple[int, ...]] = {
     L.SYS_LORENZ: (3,),
     L.SYS_LORENZ_MASKED: (3,),
     L.SYS_ROSSLER_NET: tuple(3 * n for n in range(1, 129)),
+    L.SYS_FRICTION: (2,),
     L.SYS_USER: tuple(range(1, L.MAX_USER_DIM + 1)),
 }
 
@@ -186,3 +190,23 @@ class LorenzODE(ODESystem):
         s, r, b = p[..., 0], p[..., 1], p[..., 2]
         x, yy, z = y[..., 0], y[..., 1], y[..., 2]
         return torch.stack([s * (yy - x), r * x - x * z - yy, x * yy - b * z], dim=-1)
+
+
+class FrictionODE(ODESystem):
+    """Friction oscillator, params {v_d, xi, musd, mud, muv, v0}
+    (case_studies/friction/friction_ode.py:32-75)."""
+
+    b200_system = "friction"
+
+    def ode(self, t, y, p):
+        vd, xi, musd, mud, muv, v0 = (p[..., i] for i in range(6))
+        disp, vel = y[..., 0], y[..., 1]
+        vrel = vel - vd
+        f_fric = mud + mud * (musd - 1.0) * torch.exp(-torch.abs(vrel) / v0) + muv * torch.abs(vrel) / v0
+        slip = torch.abs(vrel) > 1e-4
+        trans = torch.abs(disp + 2 * xi * vel) > mud * musd
+        slip_vel = -disp - 2 * xi * vel - torch.tanh(50 * vrel) * f_fric
+        trans_vel = -disp - 2 * xi * vel + mud * musd * torch.tanh(50 * f_fric)
+        stick_vel = -(vel - vd)
+        return torch.stack([torch.where(slip | trans, vel, vd),
+                            torch.where(slip, slip_vel, torch.where(trans, trans_vel, stick_vel))], dim=-1)

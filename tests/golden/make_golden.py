@@ -8,11 +8,13 @@ It imports the reference (with empty stand-in modules for the two imports that
 are not installed, ``torchdiffeq`` and ``matplotlib``; neither is on the paths
 used here) and writes:
 
-* ``labels_pendulum_case1.npz`` / ``labels_duffing_main.npz`` — the reference's
-  seeded label fixtures (tests/integration/pendulum/ground_truths/case1/
-  main_pendulum_case1.csv, tests/integration/duffing/ground_truths/main/
-  main_duffing.csv; seed 42, N=4000) as class indices plus class names, with the
-  basin-stability counts of main_pendulum_case1.json / main_duffing_supervised.json.
+* ``labels_pendulum_case1.npz`` / ``labels_duffing_main.npz`` /
+  ``labels_friction_case1.npz`` — the reference's seeded label fixtures
+  (tests/integration/pendulum/ground_truths/case1/main_pendulum_case1.csv,
+  tests/integration/duffing/ground_truths/main/main_duffing.csv,
+  tests/integration/friction/ground_truths/main/main_friction.csv; seed 42,
+  N=4000) as class indices plus class names, with the basin-stability counts of
+  main_pendulum_case1.json / main_duffing_supervised.json / main_friction_case1.json.
 * ``features_reference.npz`` — outputs of the reference's own feature
   calculators (src/pybasin/ts_torch/calculators/torch_features_statistical.py,
   torch_features_pattern.py) on seeded random windows, to pin the statistics.
@@ -174,6 +176,13 @@ def main() -> None:
         "duffing/main_duffing_supervised.json",
         [f"$\\bar{{y}}_{i}$" for i in range(1, 6)],
         "labels_duffing_main.npz",
+    )
+    _labels(
+        it,
+        "friction/ground_truths/main/main_friction.csv",
+        "friction/main_friction_case1.json",
+        ["FP", "LC"],
+        "labels_friction_case1.npz",
     )
     _features(ref)
     _scipy(ref)

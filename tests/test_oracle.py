@@ -153,3 +153,17 @@ def test_torch_linspace_save_times_are_float32_rounded():
     s32 = torch.linspace(900, 1000, 5000, dtype=torch.float32).double()
     s64 = torch.linspace(900, 1000, 5000, dtype=torch.float64)
     assert (s32 - s64).abs().max() > 1e-6
+
+
+def test_friction_labels_equal_reference_fixture():
+    """Friction case 1 (tests/integration/friction/test_friction.py, seed 42, N = 4000):
+    max |v| over t in [400, 500] > 0.2 -> LC (friction_feature_extractor.py:17-41)."""
+    d = np.load(GOLDEN / "labels_friction_case1.npz")
+    save = torch.linspace(400, 500, 500, dtype=torch.float32).double().numpy()
+    p = np.array([[1.5, 0.05, 2.0, 0.5, 0.0, 0.5]])  # setup_friction_system.py:19-26
+    r = O.solve_batch(O.SYS_FRICTION, d["ics"].astype(np.float64), p, save, (0.0, 500.0), 1e-8, 1e-6,
+                      features=[(1, 6, 0.0)])
+    labels = (r["features"][:, 0] > 0.2).astype(np.int8)
+    assert (r["status"] == 0).all()
+    np.testing.assert_array_equal(labels, d["labels"])
+    assert np.bincount(labels).tolist() == d["counts"].tolist() == [1266, 2734]
