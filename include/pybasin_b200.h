@@ -80,8 +80,26 @@ typedef enum {
     /* network systems: max - min over the nodes of block feat_state (0 x, 1 y, 2 z;
        3 = the largest of the three) at t1, the synchronisation features of
        case_studies/rossler_network/synchronization_feature_extractor.py:73-106 */
-    PB_FEAT_SYNC_DEV = 13
+    PB_FEAT_SYNC_DEV = 13,
+    /* wider set, streaming (ts_torch/calculators/torch_features_statistical.py:20-27,
+       119-122,160-163 and :50-57 for length) */
+    PB_FEAT_SUM = 14, PB_FEAT_ABS_ENERGY = 15, PB_FEAT_LENGTH = 16, PB_FEAT_VARIATION_COEFF = 17,
+    /* wider set from the stored window (a second pass; feat_param as noted):
+       quantile (q, torch.quantile linear), kurtosis, skewness (statistical.py:125-156),
+       absolute_sum_of_changes, mean_abs_change, mean_change, mean_second_derivative_central
+       (torch_features_change.py:79-110), count_above_mean, count_below_mean, count_above (t),
+       count_below (t) (torch_features_count.py:11-33), number_peaks (n, pattern.py:64-110),
+       autocorrelation (lag, torch_features_autocorrelation.py:13-27),
+       ratio_beyond_r_sigma (r, statistical.py:176-182) */
+    PB_FEAT_QUANTILE = 18, PB_FEAT_KURTOSIS = 19, PB_FEAT_SKEWNESS = 20, PB_FEAT_ABS_SUM_CHANGES = 21,
+    PB_FEAT_MEAN_ABS_CHANGE = 22, PB_FEAT_MEAN_CHANGE = 23, PB_FEAT_MEAN_SECOND_DERIV = 24,
+    PB_FEAT_COUNT_ABOVE_MEAN = 25, PB_FEAT_COUNT_BELOW_MEAN = 26, PB_FEAT_COUNT_ABOVE = 27,
+    PB_FEAT_COUNT_BELOW = 28, PB_FEAT_NUMBER_PEAKS = 29, PB_FEAT_AUTOCORRELATION = 30,
+    PB_FEAT_RATIO_BEYOND_R_SIGMA = 31
 } pb_feature;
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..31): the
+   window costs n_traj x (n_save - win_begin) floats of scratch per such column */
+#define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_RATIO_BEYOND_R_SIGMA))
 
 /* ---- per-trajectory status written to status_out ---- */
 typedef enum {

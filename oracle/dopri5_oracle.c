@@ -178,6 +178,81 @@ static double window_feature(int feat, double param, const double *w, int n, dou
         return c;
     }
     case ORACLE_F_LAST: return w[n - 1];
+    /* wider set: ts_torch/calculators/torch_features_statistical.py:20-27,119-163,
+       torch_features_change.py:79-110, torch_features_count.py:11-33,
+       torch_features_pattern.py:64-110, torch_features_autocorrelation.py:13-27 */
+    case ORACLE_F_SUM: return sum;
+    case ORACLE_F_ABS_ENERGY: return sq;
+    case ORACLE_F_LENGTH: return (double)n;
+    case ORACLE_F_VARIATION_COEFF: return sqrt(m2 / n) / (fabs(mean) + 1e-10);
+    case ORACLE_F_QUANTILE: { /* torch.quantile, linear interpolation; NaN if any */
+        if (any_nan) return NAN;
+        memcpy(scratch, w, sizeof(double) * (size_t)n);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double);
+        const double pos = param * (n - 1);
+        const int lo = (int)floor(pos), hi = lo + 1 < n ? lo + 1 : n - 1;
+        return scratch[lo] + (scratch[hi] - scratch[lo]) * (pos - lo);
+    }
+    case ORACLE_F_KURTOSIS: case ORACLE_F_SKEWNESS: {
+        double c2 = 0.0, c3 = 0.0, c4 = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double d = w[i] - mean;
+            c2 += d * d;
+            c3 += d * d * d;
+            c4 += d * d * d * d;
+        }
+        c2 /= n;
+        c3 /= n;
+        c4 /= n;
+        if (feat == ORACLE_F_KURTOSIS) {
+            const double g2 = c4 / (c2 * c2 + 1e-10) - 3.0;
+            return ((n - 1.0) / ((n - 2.0) * (n - 3.0) + 1e-10)) * ((n + 1.0) * g2 + 6.0);
+        }
+        const double g1 = c3 / (pow(c2, 1.5) + 1e-10);
+        return g1 * sqrt((double)n * (n - 1.0)) / (n - 2.0 + 1e-10);
+    }
+    case ORACLE_F_ABS_SUM_CHANGES: case ORACLE_F_MEAN_ABS_CHANGE: {
+        double a = 0.0;
+        for (int i = 1; i < n; ++i) a += fabs(w[i] - w[i - 1]);
+        return feat == ORACLE_F_ABS_SUM_CHANGES ? a : a / (n - 1);
+    }
+    case ORACLE_F_MEAN_CHANGE: return (w[n - 1] - w[0]) / (n - 1);
+    case ORACLE_F_MEAN_SECOND_DERIV: return (w[n - 1] - w[n - 2] - w[1] + w[0]) / (2.0 * (n - 2));
+    case ORACLE_F_COUNT_ABOVE_MEAN: case ORACLE_F_COUNT_BELOW_MEAN: {
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += feat == ORACLE_F_COUNT_ABOVE_MEAN ? (w[i] > mean) : (w[i] < mean);
+        return c;
+    }
+    case ORACLE_F_COUNT_ABOVE: case ORACLE_F_COUNT_BELOW: {
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += feat == ORACLE_F_COUNT_ABOVE ? (w[i] > param) : (w[i] < param);
+        return c / n;
+    }
+    case ORACLE_F_NUMBER_PEAKS: { /* strict local maxima with support k on each side */
+        const int k = (int)param;
+        double c = 0.0;
+        if (2 * k >= n) return 0.0;
+        for (int i = k; i < n - k; ++i) {
+            int peak = 1;
+            for (int j = 1; j <= k && peak; ++j) peak = (w[i] > w[i - j]) && (w[i] > w[i + j]);
+            c += peak;
+        }
+        return c;
+    }
+    case ORACLE_F_AUTOCORRELATION: {
+        const int lag = (int)param;
+        if (lag == 0) return 1.0;
+        if (lag >= n) return 0.0;
+        double ac = 0.0;
+        for (int i = 0; i + lag < n; ++i) ac += (w[i] - mean) * (w[i + lag] - mean);
+        return ac / (m2 + 1e-10);
+    }
+    case ORACLE_F_RATIO_BEYOND_R_SIGMA: {
+        const double sd = sqrt(m2 / n);
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += fabs(w[i] - mean) > param * sd;
+        return c / n;
+    }
     default: return NAN;
     }
 }

@@ -18,6 +18,13 @@ enum {
     ORACLE_F_MEDIAN = 0, ORACLE_F_MEAN = 1, ORACLE_F_STD = 2, ORACLE_F_VAR = 3, ORACLE_F_RMS = 4,
     ORACLE_F_MAX = 5, ORACLE_F_ABSMAX = 6, ORACLE_F_MIN = 7, ORACLE_F_DELTA = 8,
     ORACLE_F_LOG_DELTA = 9, ORACLE_F_AMPLITUDE = 10, ORACLE_F_CROSSINGS = 11, ORACLE_F_LAST = 12,
+    /* 13 is the network-only synchronisation feature */
+    ORACLE_F_SUM = 14, ORACLE_F_ABS_ENERGY = 15, ORACLE_F_LENGTH = 16, ORACLE_F_VARIATION_COEFF = 17,
+    ORACLE_F_QUANTILE = 18, ORACLE_F_KURTOSIS = 19, ORACLE_F_SKEWNESS = 20, ORACLE_F_ABS_SUM_CHANGES = 21,
+    ORACLE_F_MEAN_ABS_CHANGE = 22, ORACLE_F_MEAN_CHANGE = 23, ORACLE_F_MEAN_SECOND_DERIV = 24,
+    ORACLE_F_COUNT_ABOVE_MEAN = 25, ORACLE_F_COUNT_BELOW_MEAN = 26, ORACLE_F_COUNT_ABOVE = 27,
+    ORACLE_F_COUNT_BELOW = 28, ORACLE_F_NUMBER_PEAKS = 29, ORACLE_F_AUTOCORRELATION = 30,
+    ORACLE_F_RATIO_BEYOND_R_SIGMA = 31,
 };
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };

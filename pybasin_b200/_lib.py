@@ -66,6 +66,24 @@ FEAT_AMPLITUDE = 10
 FEAT_CROSSINGS = 11
 FEAT_LAST = 12
 FEAT_SYNC_DEV = 13
+FEAT_SUM = 14
+FEAT_ABS_ENERGY = 15
+FEAT_LENGTH = 16
+FEAT_VARIATION_COEFF = 17
+FEAT_QUANTILE = 18
+FEAT_KURTOSIS = 19
+FEAT_SKEWNESS = 20
+FEAT_ABS_SUM_CHANGES = 21
+FEAT_MEAN_ABS_CHANGE = 22
+FEAT_MEAN_CHANGE = 23
+FEAT_MEAN_SECOND_DERIV = 24
+FEAT_COUNT_ABOVE_MEAN = 25
+FEAT_COUNT_BELOW_MEAN = 26
+FEAT_COUNT_ABOVE = 27
+FEAT_COUNT_BELOW = 28
+FEAT_NUMBER_PEAKS = 29
+FEAT_AUTOCORRELATION = 30
+FEAT_RATIO_BEYOND_R_SIGMA = 31
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

@@ -19,8 +19,10 @@ namespace pb {
 // order-preserving 32-bit keys.  One warp per (trajectory, median column).
 // ---------------------------------------------------------------------------
 struct MedianPlan {
-    int n_med;
-    int col[PB_MAX_FEATURES];
+    int n_med;                       // window columns
+    int col[PB_MAX_FEATURES];        // output column of window column m
+    int kind[PB_MAX_FEATURES];       // its feature kind
+    double param[PB_MAX_FEATURES];   // and parameter (q, t, n, lag, r)
 };
 
 __device__ __forceinline__ uint32_t float_key(float f)
@@ -34,25 +36,10 @@ __device__ __forceinline__ float key_float(uint32_t k)
     return __uint_as_float(u);
 }
 
-__global__ void __launch_bounds__(256) k_median(const float* __restrict__ win, int64_t n_traj, int nwin,
-                                                MedianPlan plan, double* __restrict__ out, int n_features)
+// k-th smallest (0-based) value of a NaN-free row, by a 4-pass 8-bit radix select
+// on order-preserving keys (warp-collective; h = 256 bins of this warp)
+__device__ float select_rank(const float* __restrict__ x, int nwin, unsigned k, unsigned* h, int lane)
 {
-    __shared__ unsigned hist[8][256];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
-    if (row >= n_traj * plan.n_med) return;  // warp-uniform
-    const float* x = win + row * nwin;
-    unsigned* h = hist[warp];
-    // NaN anywhere -> NaN
-    bool nan_seen = false;
-    for (int i = lane; i < nwin; i += 32) nan_seen |= isnan(x[i]);
-    const int64_t traj = row / plan.n_med;
-    const int col = plan.col[row - traj * plan.n_med];
-    if (__any_sync(0xffffffffu, nan_seen)) {
-        if (lane == 0) out[traj * n_features + col] = CUDART_NAN;
-        return;
-    }
-    unsigned k = static_cast<unsigned>((nwin - 1) / 2);  // rank of the lower median
     uint32_t prefix = 0, prefix_mask = 0;
     for (int pass = 0; pass < 4; ++pass) {
         const int shift = 24 - 8 * pass;
@@ -83,7 +70,139 @@ __global__ void __launch_bounds__(256) k_median(const float* __restrict__ win, i
         prefix_mask |= 0xffu << shift;
         __syncwarp();
     }
-    if (lane == 0) out[traj * n_features + col] = static_cast<double>(key_float(prefix));
+    return key_float(prefix);
+}
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Window pass: one warp per (trajectory, window column) computes the column's
+// feature from the stored window (torch semantics of the reference calculators:
+// median = lower middle value, quantile = linear interpolation, NaN in -> NaN out
+// for order statistics, comparisons with NaN false).
+__global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, int64_t n_traj, int nwin,
+                                                MedianPlan plan, double* __restrict__ out, int n_features)
+{
+    __shared__ unsigned hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
+    if (row >= n_traj * plan.n_med) return;  // warp-uniform
+    const float* x = win + row * nwin;
+    unsigned* h = hist[warp];
+    const int64_t traj = row / plan.n_med;
+    const int m = static_cast<int>(row - traj * plan.n_med);
+    const int col = plan.col[m], kind = plan.kind[m];
+    const double param = plan.param[m];
+    const double n = static_cast<double>(nwin);
+    double result = CUDART_NAN;
+    if (kind == PB_FEAT_MEDIAN || kind == PB_FEAT_QUANTILE) {
+        bool nan_seen = false;
+        for (int i = lane; i < nwin; i += 32) nan_seen |= isnan(x[i]);
+        if (!__any_sync(0xffffffffu, nan_seen)) {
+            if (kind == PB_FEAT_MEDIAN) {
+                result = select_rank(x, nwin, static_cast<unsigned>((nwin - 1) / 2), h, lane);
+            } else {
+                const double pos = param * (nwin - 1);
+                const int lo = static_cast<int>(floor(pos));
+                const int hi = lo + 1 < nwin ? lo + 1 : nwin - 1;
+                const double va = select_rank(x, nwin, static_cast<unsigned>(lo), h, lane);
+                const double vb = hi == lo ? va : select_rank(x, nwin, static_cast<unsigned>(hi), h, lane);
+                result = va + (vb - va) * (pos - lo);
+            }
+        }
+    } else {
+        double s = 0.0;
+        for (int i = lane; i < nwin; i += 32) s += static_cast<double>(x[i]);
+        const double mean = warp_sum_d(s) / n;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        switch (kind) {
+            case PB_FEAT_KURTOSIS:
+            case PB_FEAT_SKEWNESS:
+            case PB_FEAT_AUTOCORRELATION:
+            case PB_FEAT_RATIO_BEYOND_R_SIGMA: {
+                const int lag = static_cast<int>(param);
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                    if (kind == PB_FEAT_KURTOSIS || kind == PB_FEAT_SKEWNESS) {
+                        a1 += d * d * d;
+                        a2 += d * d * d * d;
+                    } else if (kind == PB_FEAT_AUTOCORRELATION && lag > 0 && i + lag < nwin) {
+                        a1 += d * (static_cast<double>(x[i + lag]) - mean);
+                    }
+                }
+                const double m2 = warp_sum_d(a0);
+                if (kind == PB_FEAT_KURTOSIS || kind == PB_FEAT_SKEWNESS) {
+                    const double c2 = m2 / n, c3 = warp_sum_d(a1) / n, c4 = warp_sum_d(a2) / n;
+                    if (kind == PB_FEAT_KURTOSIS) {
+                        const double g2 = c4 / (c2 * c2 + 1e-10) - 3.0;
+                        result = ((n - 1.0) / ((n - 2.0) * (n - 3.0) + 1e-10)) * ((n + 1.0) * g2 + 6.0);
+                    } else {
+                        const double g1 = c3 / (pow(c2, 1.5) + 1e-10);
+                        result = g1 * sqrt(n * (n - 1.0)) / (n - 2.0 + 1e-10);
+                    }
+                } else if (kind == PB_FEAT_AUTOCORRELATION) {
+                    const double ac = warp_sum_d(a1);
+                    result = lag == 0 ? 1.0 : (lag >= nwin ? 0.0 : ac / (m2 + 1e-10));
+                } else {
+                    const double sd = sqrt(m2 / n);
+                    double c = 0.0;
+                    for (int i = lane; i < nwin; i += 32) c += fabs(static_cast<double>(x[i]) - mean) > param * sd;
+                    result = warp_sum_d(c) / n;
+                }
+                break;
+            }
+            case PB_FEAT_ABS_SUM_CHANGES:
+            case PB_FEAT_MEAN_ABS_CHANGE: {
+                for (int i = lane + 1; i < nwin; i += 32) a0 += fabs(static_cast<double>(x[i]) - static_cast<double>(x[i - 1]));
+                const double tot = warp_sum_d(a0);
+                result = kind == PB_FEAT_ABS_SUM_CHANGES ? tot : tot / (n - 1.0);
+                break;
+            }
+            case PB_FEAT_MEAN_CHANGE:
+                result = (static_cast<double>(x[nwin - 1]) - static_cast<double>(x[0])) / (n - 1.0);
+                break;
+            case PB_FEAT_MEAN_SECOND_DERIV:
+                result = nwin < 3 ? CUDART_NAN
+                                  : (static_cast<double>(x[nwin - 1]) - static_cast<double>(x[nwin - 2]) -
+                                     static_cast<double>(x[1]) + static_cast<double>(x[0])) /
+                                        (2.0 * (n - 2.0));
+                break;
+            case PB_FEAT_COUNT_ABOVE_MEAN:
+            case PB_FEAT_COUNT_BELOW_MEAN:
+            case PB_FEAT_COUNT_ABOVE:
+            case PB_FEAT_COUNT_BELOW: {
+                const bool rel_mean = kind == PB_FEAT_COUNT_ABOVE_MEAN || kind == PB_FEAT_COUNT_BELOW_MEAN;
+                const bool above = kind == PB_FEAT_COUNT_ABOVE_MEAN || kind == PB_FEAT_COUNT_ABOVE;
+                const double level = rel_mean ? mean : param;
+                for (int i = lane; i < nwin; i += 32) {
+                    const double v = static_cast<double>(x[i]);
+                    a0 += above ? (v > level) : (v < level);
+                }
+                const double c = warp_sum_d(a0);
+                result = rel_mean ? c : c / n;
+                break;
+            }
+            case PB_FEAT_NUMBER_PEAKS: {  // strict local maxima with support k on each side
+                const int k = static_cast<int>(param);
+                if (2 * k < nwin) {
+                    for (int i = k + lane; i < nwin - k; i += 32) {
+                        const float c = x[i];
+                        bool peak = true;
+                        for (int j = 1; j <= k && peak; ++j) peak = (c > x[i - j]) && (c > x[i + j]);
+                        a0 += peak ? 1.0 : 0.0;
+                    }
+                }
+                result = warp_sum_d(a0);
+                break;
+            }
+            default: break;
+        }
+    }
+    if (lane == 0) out[traj * n_features + col] = result;
 }
 
 // ---------------------------------------------------------------------------
@@ -310,8 +429,12 @@ static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
 {
     int m = 0;
     for (int c = 0; c < a.n_features; ++c)
-        if (a.feat_kind[c] == PB_FEAT_MEDIAN) {
-            if (plan) plan->col[m] = c;
+        if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
+            if (plan) {
+                plan->col[m] = c;
+                plan->kind[m] = a.feat_kind[c];
+                plan->param[m] = a.feat_param[c];
+            }
             ++m;
         }
     if (plan) plan->n_med = m;
@@ -343,7 +466,13 @@ int validate_args(const pb_solve_args* a, bool user_system)
     int n_cross = 0;
     for (int c = 0; c < a->n_features; ++c) {
         if (a->feat_state[c] < 0 || a->feat_state[c] >= a->dim) return PB_EINVAL;
-        if (a->feat_kind[c] < PB_FEAT_MEDIAN || a->feat_kind[c] > PB_FEAT_SYNC_DEV) return PB_EINVAL;
+        const int kind = a->feat_kind[c];
+        const double prm = a->feat_param[c];
+        if (kind < PB_FEAT_MEDIAN || kind > PB_FEAT_RATIO_BEYOND_R_SIGMA) return PB_EINVAL;
+        if (kind == PB_FEAT_QUANTILE && !(prm >= 0.0 && prm <= 1.0)) return PB_EINVAL;
+        if ((kind == PB_FEAT_NUMBER_PEAKS || kind == PB_FEAT_AUTOCORRELATION) &&
+            !(prm >= 0.0 && prm <= 1e6 && prm == static_cast<double>(static_cast<int>(prm))))
+            return PB_EINVAL;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }
@@ -454,7 +583,7 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
         const int64_t rows = a.n_traj * plan.n_med;
         const int64_t blocks = (rows + 7) / 8;
         if (blocks > 0x7fffffffLL) return PB_EINVAL;
-        k_median<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
+        k_window<<<static_cast<unsigned>(blocks), 256, 0, st>>>(
             reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), a.n_traj,
             a.n_save - a.win_begin, plan, a.features_out, a.n_features);
         e = cudaGetLastError();

@@ -96,7 +96,7 @@ __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
             pl.cross_state[nc] = a.feat_state[c];
             pl.cross_level[nc] = a.feat_param[c];
             ++nc;
-        } else if (a.feat_kind[c] == PB_FEAT_MEDIAN) {
+        } else if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
             pl.med_state[nm++] = a.feat_state[c];
         }
     }
@@ -745,8 +745,13 @@ struct Integrator {
                         ++j;
                         break;
                     case PB_FEAT_LAST: v = st.last(sidx); break;
-                    case PB_FEAT_MEDIAN: continue;  // written by the median pass
-                    default: v = CUDART_NAN;
+                    case PB_FEAT_SUM: v = n * sh + s1; break;
+                    case PB_FEAT_ABS_ENERGY: v = s2 + sh * (2.0 * s1 + n * sh); break;
+                    case PB_FEAT_LENGTH: v = n; break;
+                    case PB_FEAT_VARIATION_COEFF: v = sqrt(var) / (fabs(mean) + 1e-10); break;
+                    default:
+                        if (PB_FEAT_IS_WINDOW(kind)) continue;  // written by the window pass
+                        v = CUDART_NAN;
                 }
                 if (ns == 0) v = CUDART_NAN;
                 a.features_out[traj * a.n_features + c] = v;

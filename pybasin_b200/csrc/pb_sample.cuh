@@ -37,6 +37,10 @@ __device__ __forceinline__ double feature_value(int kind, double sh, double s1, 
         case PB_FEAT_AMPLITUDE: return mx - mn;
         case PB_FEAT_CROSSINGS: return crossings;
         case PB_FEAT_LAST: return last;
+        case PB_FEAT_SUM: return n * sh + s1;
+        case PB_FEAT_ABS_ENERGY: return s2 + sh * (2.0 * s1 + n * sh);
+        case PB_FEAT_LENGTH: return n;
+        case PB_FEAT_VARIATION_COEFF: return sqrt(var) / (fabs(mean) + 1e-10);
         default: return CUDART_NAN;
     }
 }
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
     int jc = 0;
     for (int c = 0; c < a.n_features; ++c) {
         const int kind = a.feat_kind[c];
-        if (kind == PB_FEAT_MEDIAN) continue;  // written by the median pass
+        if (PB_FEAT_IS_WINDOW(kind)) continue;  // written by the window pass
         const int slot = pl.slot_of[a.feat_state[c]];
         const bool has_nan = (acc.nan_flags >> slot) & 1;
         double cr = CUDART_NAN;

@@ -1,6 +1,6 @@
 // Layout of the caller-provided scratch buffer of pb_solve_batch (host and device).
 //
-//   [median windows]  n_traj x n_median_columns x window floats (PB_FEAT_MEDIAN)
+//   [feature windows] n_traj x n_window_columns x window floats (PB_FEAT_IS_WINDOW kinds)
 //   [step records]    n_traj x cap x record_stride bytes        (PB_DENSE_DEFERRED)
 //   [tails]           n_traj x tail_stride bytes                (PB_DENSE_DEFERRED)
 //   [split save grid] n_save x (float hi, float lo)            (PB_DENSE_DEFERRED)
@@ -56,10 +56,11 @@ __host__ __device__ constexpr int saved_state_bytes(int dim, int rsize)
 
 __host__ __device__ inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
+// columns whose feature needs the stored window (median, quantiles, moments, ...)
 __host__ __device__ inline int count_median_columns(const pb_solve_args& a)
 {
     int m = 0;
-    for (int c = 0; c < a.n_features; ++c) m += (a.feat_kind[c] == PB_FEAT_MEDIAN);
+    for (int c = 0; c < a.n_features; ++c) m += PB_FEAT_IS_WINDOW(a.feat_kind[c]) ? 1 : 0;
     return m;
 }
 

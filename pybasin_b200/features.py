@@ -34,6 +34,35 @@ FEATURE_KINDS: dict[str, int] = {
     "log_delta": L.FEAT_LOG_DELTA,
     "amplitude": L.FEAT_AMPLITUDE,
     "number_crossing_m": L.FEAT_CROSSINGS,
+    "sum_values": L.FEAT_SUM,
+    "abs_energy": L.FEAT_ABS_ENERGY,
+    "length": L.FEAT_LENGTH,
+    "variation_coefficient": L.FEAT_VARIATION_COEFF,
+    "quantile": L.FEAT_QUANTILE,
+    "kurtosis": L.FEAT_KURTOSIS,
+    "skewness": L.FEAT_SKEWNESS,
+    "absolute_sum_of_changes": L.FEAT_ABS_SUM_CHANGES,
+    "mean_abs_change": L.FEAT_MEAN_ABS_CHANGE,
+    "mean_change": L.FEAT_MEAN_CHANGE,
+    "mean_second_derivative_central": L.FEAT_MEAN_SECOND_DERIV,
+    "count_above_mean": L.FEAT_COUNT_ABOVE_MEAN,
+    "count_below_mean": L.FEAT_COUNT_BELOW_MEAN,
+    "count_above": L.FEAT_COUNT_ABOVE,
+    "count_below": L.FEAT_COUNT_BELOW,
+    "number_peaks": L.FEAT_NUMBER_PEAKS,
+    "autocorrelation": L.FEAT_AUTOCORRELATION,
+    "ratio_beyond_r_sigma": L.FEAT_RATIO_BEYOND_R_SIGMA,
+}
+
+#: The parameter of each parameterised feature (its FCParameters key) and default.
+FEATURE_PARAM: dict[int, tuple[str, float]] = {
+    L.FEAT_CROSSINGS: ("m", 0.0),
+    L.FEAT_QUANTILE: ("q", 0.5),
+    L.FEAT_COUNT_ABOVE: ("t", 0.0),
+    L.FEAT_COUNT_BELOW: ("t", 0.0),
+    L.FEAT_NUMBER_PEAKS: ("n", 1.0),
+    L.FEAT_AUTOCORRELATION: ("lag", 1.0),
+    L.FEAT_RATIO_BEYOND_R_SIGMA: ("r", 1.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).
@@ -74,9 +103,10 @@ def columns_for(config: dict[str, Any] | None, state: int) -> list[FeatureColumn
                 "use B200Dopri5Solver(output='full') with the reference TorchFeatureExtractor for other features"
             )
         kind = FEATURE_KINDS[fname]
-        if kind == L.FEAT_CROSSINGS:
-            for p in plist or [{"m": 0}]:
-                cols.append(FeatureColumn(state, kind, float(p["m"]), _format_name(fname, p, state)))
+        if kind in FEATURE_PARAM:
+            key, default = FEATURE_PARAM[kind]
+            for p in plist or [{key: default}]:
+                cols.append(FeatureColumn(state, kind, float(p[key]), _format_name(fname, p, state)))
         else:
             if plist is not None:
                 raise ValueError(f"feature '{fname}' takes no parameters")

@@ -75,6 +75,9 @@ def _labels(ref: Path, csv: str, js: str, classes: list[str], name: str) -> None
 
 
 def _features(ref: Path) -> None:
+    from pybasin.ts_torch.calculators import torch_features_autocorrelation as ac
+    from pybasin.ts_torch.calculators import torch_features_change as ch
+    from pybasin.ts_torch.calculators import torch_features_count as cn
     from pybasin.ts_torch.calculators import torch_features_pattern as pat
     from pybasin.ts_torch.calculators import torch_features_statistical as st
 
@@ -101,6 +104,29 @@ def _features(ref: Path) -> None:
         "amplitude": st.amplitude(x).numpy(),
         "number_crossing_m_0": pat.number_crossing_m(x, 0).numpy(),
         "number_crossing_m_1": pat.number_crossing_m(x, 1).numpy(),
+        # wider set (window features)
+        "sum_values": st.sum_values(x).numpy(),
+        "abs_energy": st.abs_energy(x).numpy(),
+        "length": st.length(x).numpy(),
+        "variation_coefficient": st.variation_coefficient(x).numpy(),
+        "quantile_0.1": st.quantile(x, 0.1).numpy(),
+        "quantile_0.75": st.quantile(x, 0.75).numpy(),
+        "quantile_even_0.3": st.quantile(even, 0.3).numpy(),
+        "kurtosis": st.kurtosis(x).numpy(),
+        "skewness": st.skewness(x).numpy(),
+        "absolute_sum_of_changes": ch.absolute_sum_of_changes(x).numpy(),
+        "mean_abs_change": ch.mean_abs_change(x).numpy(),
+        "mean_change": ch.mean_change(x).numpy(),
+        "mean_second_derivative_central": ch.mean_second_derivative_central(x).numpy(),
+        "count_above_mean": cn.count_above_mean(x).numpy(),
+        "count_below_mean": cn.count_below_mean(x).numpy(),
+        "count_above_0": cn.count_above(x, 0).numpy(),
+        "count_below_0.5": cn.count_below(x, 0.5).numpy(),
+        "number_peaks_1": pat.number_peaks(x, 1).numpy(),
+        "number_peaks_3": pat.number_peaks(x, 3).numpy(),
+        "autocorrelation_1": ac.autocorrelation(x, 1).numpy(),
+        "autocorrelation_7": ac.autocorrelation(x, 7).numpy(),
+        "ratio_beyond_r_sigma_1": st.ratio_beyond_r_sigma(x, 1.0).numpy(),
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

@@ -101,6 +101,27 @@ def test_oracle_matches_reference_scipy_trajectories():
         ("amplitude", 10, 0.0),
         ("number_crossing_m_0", 11, 0.0),
         ("number_crossing_m_1", 11, 1.0),
+        ("sum_values", 14, 0.0),
+        ("abs_energy", 15, 0.0),
+        ("length", 16, 0.0),
+        ("variation_coefficient", 17, 0.0),
+        ("quantile_0.1", 18, 0.1),
+        ("quantile_0.75", 18, 0.75),
+        ("kurtosis", 19, 0.0),
+        ("skewness", 20, 0.0),
+        ("absolute_sum_of_changes", 21, 0.0),
+        ("mean_abs_change", 22, 0.0),
+        ("mean_change", 23, 0.0),
+        ("mean_second_derivative_central", 24, 0.0),
+        ("count_above_mean", 25, 0.0),
+        ("count_below_mean", 26, 0.0),
+        ("count_above_0", 27, 0.0),
+        ("count_below_0.5", 28, 0.5),
+        ("number_peaks_1", 29, 1.0),
+        ("number_peaks_3", 29, 3.0),
+        ("autocorrelation_1", 30, 1.0),
+        ("autocorrelation_7", 30, 7.0),
+        ("ratio_beyond_r_sigma_1", 31, 1.0),
     ],
 )
 def test_oracle_window_features_match_reference_calculators(name, kind, param):
@@ -108,7 +129,18 @@ def test_oracle_window_features_match_reference_calculators(name, kind, param):
     x = g["x"]
     want = g[name]
     got = np.array([[O.window_feature(kind, param, x[:, b, s]) for s in range(x.shape[2])] for b in range(x.shape[1])])
-    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+    # count_above / count_below / ratio_beyond_r_sigma: the reference averages a
+    # boolean mask in FP32 (.float().mean()), exact to FP32 rounding only
+    fp32_mean = name.startswith(("count_above_", "count_below_", "ratio_beyond"))
+    tol = 2e-7 if fp32_mean else 1e-12
+    np.testing.assert_allclose(got, want, rtol=tol, atol=1e-12)
+
+
+def test_oracle_quantile_even_length():
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g["x_even"]
+    got = np.array([[O.window_feature(18, 0.3, x[:, b, s]) for s in range(2)] for b in range(x.shape[1])])
+    np.testing.assert_allclose(got, g["quantile_even_0.3"], rtol=1e-12, atol=1e-12)
 
 
 def test_oracle_median_even_length_is_lower_median():

@@ -394,3 +394,66 @@ def test_probed_schedule_edge_cases():
         assert st[3] == L.TRAJ_NONFINITE and st[7] == L.TRAJ_BAD_INPUT
         assert (st == L.TRAJ_UNBOUNDED).any()
     assert (a["status"] == L.TRAJ_MAX_STEPS).any()
+
+
+# the wider feature set: streaming kinds (from the running sums) and window kinds
+# (second pass over the stored FP32 window), on one state
+WIDE_FEATS = [(0, k, 0.0) for k in (L.FEAT_SUM, L.FEAT_ABS_ENERGY, L.FEAT_LENGTH, L.FEAT_VARIATION_COEFF)] + [
+    (0, L.FEAT_QUANTILE, 0.1), (0, L.FEAT_QUANTILE, 0.75), (0, L.FEAT_KURTOSIS, 0.0), (0, L.FEAT_SKEWNESS, 0.0),
+    (0, L.FEAT_ABS_SUM_CHANGES, 0.0), (0, L.FEAT_MEAN_ABS_CHANGE, 0.0), (0, L.FEAT_MEAN_CHANGE, 0.0),
+    (0, L.FEAT_MEAN_SECOND_DERIV, 0.0), (0, L.FEAT_COUNT_ABOVE_MEAN, 0.0), (0, L.FEAT_COUNT_BELOW_MEAN, 0.0),
+    (0, L.FEAT_COUNT_ABOVE, 0.0), (0, L.FEAT_COUNT_BELOW, 0.5), (0, L.FEAT_NUMBER_PEAKS, 1.0),
+    (0, L.FEAT_NUMBER_PEAKS, 3.0), (0, L.FEAT_AUTOCORRELATION, 1.0), (0, L.FEAT_AUTOCORRELATION, 7.0),
+    (0, L.FEAT_RATIO_BEYOND_R_SIGMA, 1.0), (0, L.FEAT_MEDIAN, 0.0),
+]
+COUNT_KINDS = {L.FEAT_COUNT_ABOVE_MEAN, L.FEAT_COUNT_BELOW_MEAN, L.FEAT_NUMBER_PEAKS}
+FRACTION_KINDS = {L.FEAT_COUNT_ABOVE, L.FEAT_COUNT_BELOW, L.FEAT_RATIO_BEYOND_R_SIGMA}
+
+
+@DENSE
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+def test_wider_feature_set_matches_oracle(dense, precision):
+    """Short horizon (t in [0, 30], window [20, 30] x 500 saves) where kernel and oracle
+    trajectories agree to ~1e-8 (FP64) / ~1e-5 (mixed): continuous features to 2e-4
+    relative (the window kinds read FP32-stored samples); counts and fractions to a
+    sample or two (a sample within rounding of the mean or level may flip)."""
+    case = DUFFING
+    y0 = seeded_ics(case, 200, seed=13).double().numpy()
+    save = np.asarray(torch.linspace(0.0, 30.0, 1501, dtype=torch.float32).double())
+    wb = int(np.nonzero(save >= 20.0)[0][0])
+    n = len(save) - wb
+    rtol = case.rtol if precision == L.PREC_FP64 else 1e-6
+    want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), 1e-10, 1e-10,
+                         win_begin=wb, features=WIDE_FEATS)
+    got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), min(rtol, 1e-8), 1e-10,
+                    win_begin=wb, features=WIDE_FEATS, dense_mode=dense, precision=precision)
+    assert (got["status"] == 0).all()
+    g, w = got["features"], want["features"]
+    for c, (_, kind, _) in enumerate(WIDE_FEATS):
+        if kind in COUNT_KINDS:
+            assert np.abs(g[:, c] - w[:, c]).max() <= 2, (c, kind)
+        elif kind in FRACTION_KINDS:
+            assert np.abs(g[:, c] - w[:, c]).max() <= 2.0 / n, (c, kind)
+        else:
+            tol = 2e-4 if precision == L.PREC_FP64 else 2e-3
+            scale = np.abs(w[:, c]).max() + 1e-12
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=tol, atol=tol * 1e-3 * scale, err_msg=f"col {c} kind {kind}")
+
+
+def test_wider_features_through_the_extractor_names():
+    """FCParameters names and parameters as in the reference's settings (ts_torch/settings.py:223-355)."""
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+
+    cfg = {"quantile": [{"q": 0.1}, {"q": 0.9}], "kurtosis": None, "number_peaks": [{"n": 1}, {"n": 3}],
+           "autocorrelation": [{"lag": 2}], "count_above": [{"t": 0}], "sum_values": None}
+    fx = FusedFeatureExtractor(time_steady=900.0, features=None, features_per_state={0: cfg}, normalize=False)
+    solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=2000, t_eval=(900, 1000), device="cuda:0",
+                              precision="fp64", feature_extractor=fx)
+    y0 = seeded_ics(DUFFING, 64, seed=3).double()
+    t, y = solver.integrate(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0)
+    f = fx.extract_features(type("S", (), {"y": y})())
+    assert f.shape == (64, 8) and torch.isfinite(f).all()
+    names = fx.feature_names
+    assert names[0] == "state_0__quantile__q_0.1" and "state_0__number_peaks__n_3" in names
+    # ordering sanity: quantile 0.1 <= quantile 0.9 on every trajectory
+    assert (f[:, 0] <= f[:, 1]).all()
