@@ -184,6 +184,15 @@ typedef struct pb_solve_args {
     const int32_t* order;
     int32_t dense_mode;      /* pb_dense_mode */
     int32_t window_record_cap; /* PB_DENSE_DEFERRED: step records per trajectory (0 = default) */
+    /* orbit data (utils.py:254-303 extract_orbit_data, torch_features_pattern.py:113-150
+       extract_peak_values): for the p-th PB_FEAT_NUMBER_PEAKS column (in column
+       order; its state and support n), the values of the strict local maxima of the
+       window in time order, the first peak_cap of them, at
+       peaks_out[(traj * n_peak_columns + p) * peak_cap + i], NaN-padded; the column
+       itself holds the full count.  NULL = not written. */
+    double* peaks_out;
+    int32_t peak_cap;
+    int32_t _pad3;
 } pb_solve_args;
 
 /* Where the save points of the feature window are evaluated. */

@@ -198,3 +198,15 @@ def window_feature(kind: int, param: float, w: np.ndarray) -> float:
     lib = _load()
     w = np.ascontiguousarray(w, dtype=np.float64)
     return float(lib.oracle_window_feature(kind, param, w.ctypes.data, w.shape[0]))
+
+
+def peak_values(w: np.ndarray, n: int) -> np.ndarray:
+    """Values of the strict local maxima of window ``w`` with support ``n`` on each
+    side, in time order (find_peak_mask / extract_peak_values,
+    src/pybasin/ts_torch/calculators/torch_features_pattern.py:64-150)."""
+    w = np.asarray(w, dtype=np.float64)
+    out = []
+    for i in range(n, len(w) - n):
+        if all(w[i] > w[i - j] and w[i] > w[i + j] for j in range(1, n + 1)):
+            out.append(w[i])
+    return np.array(out)

@@ -151,6 +151,9 @@ class SolveArgs(ctypes.Structure):
         ("order", _c_vp),
         ("dense_mode", _c_i32),
         ("window_record_cap", _c_i32),
+        ("peaks_out", _c_vp),
+        ("peak_cap", _c_i32),
+        ("_pad3", _c_i32),
     ]
 
 

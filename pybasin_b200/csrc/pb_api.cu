@@ -23,6 +23,10 @@ struct MedianPlan {
     int col[PB_MAX_FEATURES];        // output column of window column m
     int kind[PB_MAX_FEATURES];       // its feature kind
     double param[PB_MAX_FEATURES];   // and parameter (q, t, n, lag, r)
+    int peak_idx[PB_MAX_FEATURES];   // NUMBER_PEAKS columns: index among them (orbit data), else -1
+    int n_peak_cols;
+    int peak_cap;
+    double* peaks_out;               // (n_traj, n_peak_cols, peak_cap) or NULL
 };
 
 __device__ __forceinline__ uint32_t float_key(float f)
@@ -187,16 +191,31 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 break;
             }
             case PB_FEAT_NUMBER_PEAKS: {  // strict local maxima with support k on each side
+                // consecutive indices per 32-wide batch, so the peak values of the
+                // orbit data can be written in time order (ballot + prefix count)
                 const int k = static_cast<int>(param);
+                const int pi = plan.peak_idx[m];
+                double* pk = (plan.peaks_out && pi >= 0)
+                                 ? plan.peaks_out + (traj * plan.n_peak_cols + pi) * static_cast<int64_t>(plan.peak_cap)
+                                 : nullptr;
+                int count = 0;
                 if (2 * k < nwin) {
-                    for (int i = k + lane; i < nwin - k; i += 32) {
-                        const float c = x[i];
-                        bool peak = true;
-                        for (int j = 1; j <= k && peak; ++j) peak = (c > x[i - j]) && (c > x[i + j]);
-                        a0 += peak ? 1.0 : 0.0;
+                    for (int i0 = k; i0 < nwin - k; i0 += 32) {
+                        const int i = i0 + lane;
+                        bool peak = i < nwin - k;
+                        if (peak) {
+                            const float c = x[i];
+                            for (int j = 1; j <= k && peak; ++j) peak = (c > x[i - j]) && (c > x[i + j]);
+                        }
+                        const unsigned mask = __ballot_sync(0xffffffffu, peak);
+                        const int pos = count + __popc(mask & ((1u << lane) - 1u));
+                        if (pk && peak && pos < plan.peak_cap) pk[pos] = static_cast<double>(x[i]);
+                        count += __popc(mask);
                     }
                 }
-                result = warp_sum_d(a0);
+                if (pk)
+                    for (int i = count + lane; i < plan.peak_cap; i += 32) pk[i] = CUDART_NAN;
+                result = static_cast<double>(count);
                 break;
             }
             default: break;
@@ -427,17 +446,24 @@ static cudaError_t sort_by_probe(const pb_solve_args& a, const ScratchLayout& sl
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
 {
-    int m = 0;
+    int m = 0, np = 0;
     for (int c = 0; c < a.n_features; ++c)
         if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
             if (plan) {
                 plan->col[m] = c;
                 plan->kind[m] = a.feat_kind[c];
                 plan->param[m] = a.feat_param[c];
+                plan->peak_idx[m] = a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS ? np : -1;
             }
+            np += a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS;
             ++m;
         }
-    if (plan) plan->n_med = m;
+    if (plan) {
+        plan->n_med = m;
+        plan->n_peak_cols = np;
+        plan->peak_cap = a.peak_cap;
+        plan->peaks_out = a.peak_cap > 0 ? a.peaks_out : nullptr;
+    }
     return m;
 }
 
@@ -480,6 +506,7 @@ int validate_args(const pb_solve_args* a, bool user_system)
     if (a->n_features > 0 && !a->features_out) return PB_EINVAL;
     if (a->dense_mode != PB_DENSE_INLINE && a->dense_mode != PB_DENSE_DEFERRED) return PB_EINVAL;
     if (a->window_record_cap < 0) return PB_EINVAL;
+    if (a->peak_cap < 0 || (a->peaks_out && a->peak_cap == 0)) return PB_EINVAL;
     for (int c = 0; c < a->n_features; ++c)
         if (a->feat_state[c] >= PB_MAX_STAT_STATES) return PB_EUNSUPPORTED;
     switch (a->layout) {

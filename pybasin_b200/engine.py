@@ -58,6 +58,7 @@ class SolveRequest:
     csr_row: torch.Tensor | None = None  # network systems: (n_nodes + 1,) int32
     csr_col: torch.Tensor | None = None  # network systems: (2 * n_edges,) int32
     program: object | None = None  # SYS_USER: the compiled right-hand side (rhs.CompiledRHS)
+    peak_cap: int = 0  # orbit data: peak values kept per NUMBER_PEAKS column and trajectory
 
 
 @dataclass
@@ -67,6 +68,7 @@ class SolveResult:
     y_final: torch.Tensor | None  # (n_traj, dim)
     y_full: torch.Tensor | None  # (n_save, n_traj, dim)
     steps: torch.Tensor | None  # (n_traj,) int64
+    peaks: torch.Tensor | None = None  # (n_traj, n_peak_columns, peak_cap) f64, NaN-padded
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -130,6 +132,8 @@ def build_args(
     a.order = _ptr(req.order)
     a.dense_mode = req.dense_mode
     a.window_record_cap = req.window_record_cap
+    a.peaks_out = _ptr(out.peaks)
+    a.peak_cap = req.peak_cap if out.peaks is not None else 0
     return a
 
 
@@ -189,6 +193,9 @@ def solve(req: SolveRequest, stream: torch.cuda.Stream | None = None) -> SolveRe
         else None,
         steps=torch.empty((n_traj,), dtype=torch.int64, device=dev) if req.keep_steps else None,
     )
+    n_peak_cols = sum(1 for c in req.columns if c.kind == L.FEAT_NUMBER_PEAKS)
+    if req.peak_cap > 0 and n_peak_cols > 0:
+        out.peaks = torch.empty((n_traj, n_peak_cols, req.peak_cap), dtype=torch.float64, device=dev)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
     with torch.cuda.stream(s):
         queue = torch.zeros((1,), dtype=torch.int64, device=dev)

@@ -24,13 +24,14 @@ from __future__ import annotations
 
 import logging
 import threading
+from dataclasses import dataclass
 from typing import Any
 
 import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.engine import MortonOrder, SolveRequest, solve
+from pybasin_b200.engine import FeatureColumn, MortonOrder, SolveRequest, solve
 from pybasin_b200.features import FusedFeatureExtractor
 from pybasin_b200.odes import resolve_system
 
@@ -60,6 +61,40 @@ class IntegrationResult(tuple):
         for k, v in extra.items():
             setattr(obj, k, v)
         return obj
+
+
+@dataclass
+class OrbitData:
+    """Field layout of the reference's ``OrbitData`` (src/pybasin/utils.py:228-251):
+    ``peak_values`` (max_peaks, B, D) NaN-padded, ``peak_counts`` (B, D)."""
+
+    peak_values: torch.Tensor
+    peak_counts: torch.Tensor
+    dof_indices: list[int]
+    time_steady: float
+
+
+class _OrbitColumns:
+    """Feature columns of an orbit-data solve: one peak count per state in ``dof``."""
+
+    def __init__(self, dof: list[int], support: int, time_steady: float | None):
+        self.dof, self.support, self.time_steady = dof, int(support), time_steady
+        self.resolved = 0.0
+        if self.support < 1:
+            raise ValueError("peak_support must be >= 1")
+
+    def columns(self, num_states: int) -> list[FeatureColumn]:
+        if any(not 0 <= d < num_states for d in self.dof):
+            raise ValueError(f"dof indices must lie in [0, {num_states})")
+        return [FeatureColumn(d, L.FEAT_NUMBER_PEAKS, float(self.support), f"state_{d}__peaks") for d in self.dof]
+
+    def resolve_time_steady(self, save_ts: torch.Tensor) -> float:
+        if self.time_steady is not None:
+            self.resolved = float(self.time_steady)
+        else:
+            t0, t1 = float(save_ts[0]), float(save_ts[-1])
+            self.resolved = t0 + 0.85 * (t1 - t0)  # DEFAULT_STEADY_FRACTION, src/pybasin/constants.py
+        return self.resolved
 
 
 _streams = threading.local()
@@ -241,6 +276,32 @@ class B200Dopri5Solver:
         ``(1, B*P, S)`` in fused mode, trajectory ``ic*P + p`` carrying
         ``(y0[ic], params[p])`` (base.py:155-159).
         """
+        return self._integrate(ode_system, y0, params, self.feature_extractor, 0)
+
+    def orbit_data(
+        self,
+        ode_system: Any,
+        y0: torch.Tensor,
+        dof: list[int],
+        time_steady: float | None = None,
+        peak_support: int = 1,
+        max_peaks: int = 256,
+        params: torch.Tensor | None = None,
+    ) -> "OrbitData":
+        """Peak amplitudes of the steady-state window for orbit diagrams, computed in the
+        solve (the reference's ``extract_orbit_data``, src/pybasin/utils.py:254-303:
+        strict local maxima with ``peak_support`` neighbours on each side, for every
+        state in ``dof``).  At most ``max_peaks`` values per trajectory and state are
+        kept; ``peak_counts`` holds the full counts."""
+        ext = _OrbitColumns(list(dof), peak_support, time_steady)
+        r = self._integrate(ode_system, y0, params, ext, max_peaks)
+        counts = r.features.to(torch.long)  # (B*P, D)
+        keep = int(min(max(int(counts.max()) if counts.numel() else 0, 0), max_peaks))
+        peaks = r.peaks[:, :, :keep].permute(2, 0, 1).contiguous()  # (max_peaks, B*P, D)
+        return OrbitData(peaks, counts, list(dof), ext.resolved)
+
+    def _integrate(self, ode_system: Any, y0: torch.Tensor, params: torch.Tensor | None, extractor: Any,
+                   peak_cap: int) -> IntegrationResult:
         if y0.ndim != 2:
             raise ValueError(
                 f"y0 must be 2D with shape (batch, n_dims), got shape {tuple(y0.shape)}. "
@@ -266,15 +327,15 @@ class B200Dopri5Solver:
             layout = L.LAYOUT_SINGLE
         P = p_rows.shape[0]
         n_traj = B * P if params is not None else B
-        cols = self.feature_extractor.columns(S) if self.feature_extractor is not None else []
+        cols = extractor.columns(S) if extractor is not None else []
         if cols:
-            ts = self.feature_extractor.resolve_time_steady(save_host)  # type: ignore[union-attr]
+            ts = extractor.resolve_time_steady(save_host)
             idx = torch.nonzero(save_host >= ts)
             win_begin = int(idx[0, 0]) if idx.numel() > 0 else 0
         else:
             win_begin = 0
         rtol, atol = self.effective_tolerances()
-        full = self.output == "full"
+        full = self.output == "full" and peak_cap == 0
         stream.wait_stream(torch.cuda.current_stream(dev))
         with torch.cuda.device(dev), torch.cuda.stream(stream):
             y0_dev = y0.detach().to(dev, non_blocking=False).contiguous()
@@ -326,6 +387,7 @@ class B200Dopri5Solver:
                 csr_row=csr_row,
                 csr_col=csr_col,
                 program=program,
+                peak_cap=peak_cap,
             )
             res = solve(req, stream)
             if full:
@@ -354,4 +416,5 @@ class B200Dopri5Solver:
         n_bad = int((status == L.TRAJ_MAX_STEPS).sum()) + int((status == L.TRAJ_NONFINITE).sum())
         if n_bad:
             logger.warning("B200Dopri5Solver: %d trajectories hit max_steps or went non-finite", n_bad)
-        return IntegrationResult(t, y, features=feats, feature_names=names, status=status, steps=None)
+        peaks = res.peaks.to(self.device) if res.peaks is not None else None
+        return IntegrationResult(t, y, features=feats, feature_names=names, status=status, steps=None, peaks=peaks)

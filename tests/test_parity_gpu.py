@@ -457,3 +457,27 @@ def test_wider_features_through_the_extractor_names():
     assert names[0] == "state_0__quantile__q_0.1" and "state_0__number_peaks__n_3" in names
     # ordering sanity: quantile 0.1 <= quantile 0.9 on every trajectory
     assert (f[:, 0] <= f[:, 1]).all()
+
+
+def test_orbit_data_peaks_match_oracle_trajectories():
+    """Orbit-diagram peaks (src/pybasin/utils.py:254-303) from the solve vs strict local
+    maxima of the oracle's sampled window (short horizon: FP64 trajectories agree to ~1e-8)."""
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE
+
+    y0 = seeded_ics(DUFFING, 48, seed=21).double()
+    solver = B200Dopri5Solver(t_span=(0, 60), t_steps=1201, device="cuda:0", rtol=1e-10, atol=1e-10,
+                              precision="fp64")
+    od = solver.orbit_data(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0, dof=[0, 1],
+                           time_steady=40.0, peak_support=2, max_peaks=64)
+    save = solver.save_times(torch.float64).numpy()
+    wb = int(np.nonzero(save >= 40.0)[0][0])
+    want = O.solve_batch(O.SYS_DUFFING, y0.numpy(), np.array([DUFFING.params]), save, (0.0, 60.0), 1e-10, 1e-10,
+                         keep_full=True)
+    assert od.peak_values.shape[1:] == (48, 2) and od.time_steady == 40.0
+    for b in range(48):
+        for d in range(2):
+            ref = O.peak_values(want["y"][wb:, b, d], 2)
+            assert int(od.peak_counts[b, d]) == len(ref)
+            got = od.peak_values[: len(ref), b, d].cpu().numpy()
+            np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
+            assert torch.isnan(od.peak_values[len(ref):, b, d]).all()
