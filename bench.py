@@ -20,6 +20,7 @@ Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -69,6 +70,10 @@ def seeded_ics(n: int, seed: int) -> torch.Tensor:
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 50 ms for the whole run; samples are
+    stamped with the host clock and the summary keeps those inside the timed windows
+    marked with ``timed()``."""
+
     QUERY = (
         "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -78,14 +83,15 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc: subprocess.Popen | None = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.windows: list[tuple[float, float]] = []
         self._t: threading.Thread | None = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"],
+                 "-lms", "50"],
                 stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL,
                 text=True,
@@ -99,7 +105,7 @@ class ClockSampler:
     def _read(self):
         assert self.proc is not None and self.proc.stdout is not None
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -111,10 +117,27 @@ class ClockSampler:
         if self._t is not None:
             self._t.join(timeout=2)
 
+    class _Window:
+        def __init__(self, owner):
+            self.owner = owner
+
+        def __enter__(self):
+            self.t0 = time.monotonic()
+
+        def __exit__(self, *exc):
+            self.owner.windows.append((self.t0, time.monotonic()))
+
+    def timed(self):
+        """Context marking a timed region (the device work is synchronised inside it)."""
+        return ClockSampler._Window(self)
+
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        slack = 0.06  # one sampling interval on either side of a window
+        for ts, ln in self.lines:
+            if self.windows and not any(a - slack <= ts <= b + slack for a, b in self.windows):
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -131,6 +154,7 @@ class ClockSampler:
             "sm_max_mhz": mx,
             "reasons": sorted(reasons),
             "samples": len(sm),
+            "timed_windows": len(self.windows),
         }
 
 
@@ -169,7 +193,7 @@ def run_reference_arm(args) -> None:
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    n, _ = cpu_sample_size(threads, 8.0)
+    n, _ = cpu_sample_size(threads, 3.0)
     y0 = seeded_ics(n, 42).double().numpy()
     for _ in range(args.warmup):
         cpu_reference_pass(y0[: max(n // 16, 64)], threads)
@@ -225,7 +249,8 @@ def make_pipeline(dev: torch.device, precision: str, schedule: str):
     return BasinStabilityPipeline(ode, solver, DUFFING["templates"], DUFFING["labels"], device=dev)
 
 
-def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: torch.Tensor, dist_on: bool):
+def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: torch.Tensor, dist_on: bool,
+                 clk: "ClockSampler | None" = None):
     """Device-timed passes: per-step events around the pass and around the integrator
     kernel, with an L2 flush (write of a 256 MB buffer) between steps."""
     import ctypes
@@ -241,6 +266,8 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
         torch.distributed.barrier()
     torch.cuda.synchronize()
     ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(4)) for _ in range(steps)]
+    window = clk.timed() if clk is not None else contextlib.nullcontext()
+    window.__enter__()
     for i in range(steps):
         flush.fill_(i)
         a, k0, b, c = ev[i]
@@ -257,6 +284,7 @@ def timed_passes(pipe, y0_dev: torch.Tensor, steps: int, warmup: int, flush: tor
                 "pb_label_nearest")
         c.record(s)
     torch.cuda.synchronize()
+    window.__exit__(None, None, None)
     if dist_on:
         torch.distributed.barrier()
     step_ms = [a.elapsed_time(c) for a, k0, b, c in ev]
@@ -325,8 +353,9 @@ def run_b200_arm(args) -> None:
     pipe.run_device(y0_dev)
     torch.cuda.synchronize()
 
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        step_ms, kern_ms = timed_passes(pipe, y0_dev, args.steps, args.warmup, flush, dist_on)
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.__enter__()
+    step_ms, kern_ms = timed_passes(pipe, y0_dev, args.steps, args.warmup, flush, dist_on, clk)
     ms = statistics.mean(step_ms)
     kms = statistics.mean(kern_ms)
     ms, kms = max_over_ranks([ms, kms], dev, dist_on)
@@ -361,15 +390,16 @@ def run_b200_arm(args) -> None:
         if dist_on:
             torch.distributed.barrier()
         g_times, g_stats = [], []
-        for i in range(args.steps):
-            flush.fill_(i)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            lab_g, cnt_g, st_g = gated.run_device(y0_dev)
-            e1.record()
-            torch.cuda.synchronize()
-            g_times.append(e0.elapsed_time(e1))
-            g_stats.append(st_g)
+        with clk.timed():
+            for i in range(args.steps):
+                flush.fill_(i)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                lab_g, cnt_g, st_g = gated.run_device(y0_dev)
+                e1.record()
+                torch.cuda.synchronize()
+                g_times.append(e0.elapsed_time(e1))
+                g_stats.append(st_g)
         (ms_g,) = max_over_ranks([statistics.mean(g_times)], dev, dist_on)
         counts_g = global_counts(cnt_g.view(1, -1), dist_on)
         dbs_g = (counts_g[:5].double() - counts64[:5].double()).abs().max().item() / n_all
@@ -389,15 +419,17 @@ def run_b200_arm(args) -> None:
     if dist_on:
         torch.distributed.barrier()
     e2e_times = []
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        run_e2e()
-        e1.record()
-        torch.cuda.synchronize()
-        e2e_times.append(e0.elapsed_time(e1))
+    with clk.timed():
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run_e2e()
+            e1.record()
+            torch.cuda.synchronize()
+            e2e_times.append(e0.elapsed_time(e1))
+    clk.__exit__(None, None, None)
     (e2e_ms,) = max_over_ranks([statistics.mean(e2e_times)], dev, dist_on)
 
     # roofline of the integrator kernel: algorithmic FLOPs per launch / kernel time
@@ -506,7 +538,7 @@ def run_b200_arm(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)

@@ -126,7 +126,12 @@ class B200Dopri5Solver:
     :param method: only ``"dopri5"``.
     :param rtol: relative tolerance (the FP32-stage kernel uses ``max(rtol, mixed_rtol_floor)``).
     :param atol: absolute tolerance.
-    :param cache_dir: accepted for signature compatibility; results are not cached.
+    :param cache_dir: directory of the result cache (``None`` = no cache).  A result is
+        stored as ``{t, y, features, status}`` in a safetensors file keyed by an MD5
+        of the system, its parameters, the ICs, the save grid and every setting that
+        changes the result (the reference's CacheManager key,
+        src/pybasin/cache_manager.py:27-68, here with the fused features and statuses
+        instead of the full trajectory in fused mode).
     :param t_eval: save region ``(save_start, save_end)`` within ``t_span``.
     :param precision: ``"fp64"`` (plain FP64 kernel) or ``"mixed"`` (FP32 stages and
         state, FP64 time, error norm and step control).
@@ -276,7 +281,11 @@ class B200Dopri5Solver:
         ``(1, B*P, S)`` in fused mode, trajectory ``ic*P + p`` carrying
         ``(y0[ic], params[p])`` (base.py:155-159).
         """
-        return self._integrate(ode_system, y0, params, self.feature_extractor, 0)
+        if self._cache_dir is None:
+            return self._integrate(ode_system, y0, params, self.feature_extractor, 0)
+        from pybasin_b200 import result_cache
+
+        return result_cache.cached_integrate(self, ode_system, y0, params)
 
     def orbit_data(
         self,

@@ -220,3 +220,32 @@ def test_unbounded_rows_are_inf_in_fused_mode():
     _, y = res
     assert torch.isinf(y[0, 0, 0]) and not torch.isinf(y[0, 1, 0])
     assert res.status.tolist() == [3, 0]
+
+
+@pytest.mark.gpu
+def test_result_cache_roundtrip():
+    """Second call with the same inputs is served from the safetensors cache
+    (src/pybasin/cache_manager.py:27-128); other inputs miss."""
+    import shutil
+    from pathlib import Path
+
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+
+    cache = Path(__file__).resolve().parent / "_cache_roundtrip"
+    shutil.rmtree(cache, ignore_errors=True)
+    try:
+        fx = FusedFeatureExtractor(time_steady=90.0, features=None,
+                                   features_per_state={0: {"maximum": None}}, normalize=False)
+        solver = B200Dopri5Solver(t_span=(0, 100), t_steps=200, device="cuda:0", precision="mixed",
+                                  feature_extractor=fx, cache_dir=str(cache))
+        ode = DuffingODE({"delta": 0.08, "k3": 1.0, "A": 0.2})
+        y0 = torch.rand(64, 2, generator=torch.Generator().manual_seed(1))
+        t1, y1 = solver.integrate(ode, y0)
+        files = list(cache.glob("*.safetensors"))
+        assert len(files) == 1
+        t2, y2 = solver.integrate(ode, y0)
+        assert torch.equal(y1.cpu(), y2.cpu()) and torch.equal(y1._pb_features.cpu(), y2._pb_features.cpu())
+        solver.integrate(ode, y0 + 0.01)
+        assert len(list(cache.glob("*.safetensors"))) == 2
+    finally:
+        shutil.rmtree(cache, ignore_errors=True)
