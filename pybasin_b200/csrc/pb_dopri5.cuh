@@ -165,6 +165,7 @@ struct Lane {
     R p[Sys::NP];
     double t, dt;
     double next_save;  // save_ts[si] (or +inf past the end)
+    float phase;       // FP32 clock: t mod 2 pi of the current t (kept across steps)
     int si;            // next save index
     int steps;
     int max_steps;     // a.max_steps clamped to int range (a 32-bit compare per step)
@@ -349,6 +350,7 @@ struct Integrator {
         L.steps = i[1];
         L.status = i[2];
         L.nrec = i[3];
+        L.phase = (F32_CLOCK && Sys::kTime) ? reduce_two_pi(L.t) : 0.f;
         L.max_steps = static_cast<int>(a.max_steps < 0x7fffffffLL ? a.max_steps : 0x7fffffffLL);
         int64_t ic, prow;
         rows_of(traj, a, ic, prow);
@@ -377,6 +379,7 @@ struct Integrator {
         L.si = a.y_full_out ? 0 : a.win_begin;
         L.next_save = load_save(a, L.si);
         L.nrec = 0;
+        L.phase = (F32_CLOCK && Sys::kTime) ? reduce_two_pi(L.t) : 0.f;
         if (st.d) st.reset();
 
         // first derivative and initial step size (dopri5_generic.zig:270-321), norms in FP64
@@ -552,9 +555,9 @@ struct Integrator {
         if (!(L.t < a.t1) || L.steps >= L.max_steps) return true;
         L.steps++;
         const double t = L.t;
-        // the stage phase base depends on t only, so it is reduced while the
-        // clipping and conversion of dt below are in flight
-        const float r0 = (F32_CLOCK && Sys::kTime) ? reduce_two_pi(t) : 0.f;
+        // the stage phase base of t was reduced during the previous step (from its
+        // end point, known as soon as its dt was), off this step's dependency chain
+        const float r0 = L.phase;
         double dt = L.dt;
         R h = static_cast<R>(dt);
         if (t + dt > a.t1) {
@@ -608,6 +611,8 @@ struct Integrator {
         }
         const bool accept = err2 <= 1.0;
         const double tn = t + dt;
+        // phase base for the next step if this one is accepted (depends on t and dt only)
+        const float phase_next = (F32_CLOCK && Sys::kTime) ? reduce_two_pi(tn) : 0.f;
 
         if (accept && L.next_save <= tn + dp::save_slack) {
             // dense output (dopri5_generic.zig:194-221): 4th-order polynomial in x = (ts - t)/dt
@@ -662,6 +667,7 @@ struct Integrator {
 #pragma unroll
             for (int s = 0; s < S; ++s) L.k1[s] = k7[s];
             L.t = tn;
+            L.phase = phase_next;
             if (a.unbounded_thr > 0.0) {
                 double m = 0.0;
 #pragma unroll
