@@ -515,10 +515,10 @@ def run_b200_arm(args) -> None:
                 "peak": peak32 / 1e12,
                 "unit": "TFLOP/s",
                 "frac": achieved / peak32,
-                "traffic": 1.729e9,
+                "traffic": 0.8132e9 * (n + len(DUFFING["templates"])) / 50005,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel "
-                                  "(main phase of the probed integrator) at this workload "
-                                  "(profiles/k_solve_queue_probed_duffing100k.md): the window's step records",
+                                  "(main phase of the probed integrator) at N=50,000, scaled by trajectories "
+                                  "(profiles/k_solve_queue_probed_duffing50k.md): the window's step records",
                 "peak_source": "FP32 FMA probe kernel measured in this run (MEASURED_PEAKS.json holds only the "
                                "HBM-copy and bf16-GEMM peaks, neither bounds this kernel)",
                 "fp64_fma_peak": peak64 / 1e12,
