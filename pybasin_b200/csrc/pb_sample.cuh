@@ -169,15 +169,10 @@ struct OffsetOf<float> {
 
 // NC = crossing states compiled in (0 when no column counts crossings, which
 // keeps the per-lane crossing registers out of the common case).
+// Sampling of one trajectory by the calling warp (all 32 lanes, warp-uniform traj).
 template <class R, int NS, int NC>
-__global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
+__device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const Plan& pl, int64_t traj, int lane)
 {
-    __shared__ Plan pl;
-    if (threadIdx.x == 0) build_plan(pl, a);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t traj = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
-    if (traj >= a.n_traj || pl.ns != NS) return;  // warp-uniform
     const unsigned char* tl = tail_ptr(a, pl.sl, traj);
     const int nrec = reinterpret_cast<const int*>(tl)[0];
     if (nrec < 0) return;  // integrated again by the inline pass
@@ -354,6 +349,18 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
                                        has_nan ? CUDART_NAN : pick(acc.mx, slot), pick(acc.last, slot), n, cr);
         a.features_out[traj * a.n_features + c] = v;
     }
+}
+
+template <class R, int NS, int NC>
+__global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
+{
+    __shared__ Plan pl;
+    if (threadIdx.x == 0) build_plan(pl, a);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t traj = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+    if (traj >= a.n_traj || pl.ns != NS) return;  // warp-uniform
+    sample_trajectory<R, NS, NC>(a, pl, traj, lane);
 }
 
 }  // namespace pb

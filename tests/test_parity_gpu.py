@@ -481,3 +481,26 @@ def test_orbit_data_peaks_match_oracle_trajectories():
             got = od.peak_values[: len(ref), b, d].cpu().numpy()
             np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
             assert torch.isnan(od.peak_values[len(ref):, b, d]).all()
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("feats", [[(0, L.FEAT_MAX, 0.0), (0, L.FEAT_STD, 0.0)],
+                                   [(0, L.FEAT_MEAN, 0.0), (1, L.FEAT_LOG_DELTA, 0.0), (1, L.FEAT_LAST, 0.0)]],
+                         ids=["one_state", "two_states"])
+def test_features_are_bit_identical_across_schedules(feats, precision):
+    """Plain, queue and probed schedules write the same step records (explicit FMAs,
+    same step sequence) and the sampling pass reduces them the same way: the
+    features are bit-identical whichever schedule ran."""
+    case = DUFFING
+    y0 = seeded_ics(case, 3000, 17).double().numpy()
+    save = case.save_ts().numpy()
+    t_span = (case.t_span[0], float(save[-1]))
+    rtol = case.rtol if precision == L.PREC_FP64 else 1e-6
+    kw = dict(precision=precision, win_begin=case.win_begin(), features=feats)
+    ref = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, rtol, case.atol,
+                    schedule=L.SCHED_PLAIN, **kw)
+    for sched in (L.SCHED_QUEUE, L.SCHED_PROBED):
+        got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, t_span, rtol, case.atol,
+                        schedule=sched, **kw)
+        np.testing.assert_array_equal(got["features"], ref["features"])
+        np.testing.assert_array_equal(got["status"], ref["status"])
