@@ -112,6 +112,7 @@ __device__ __forceinline__ void build_plan(Plan& pl, const pb_solve_args& a)
         }
     }
     pl.ns = ns;
+    for (int j = ns; j < PB_MAX_STAT_STATES; ++j) pl.stat_state[j] = 0;  // unused slots read state 0
     pl.sl = scratch_layout(a);
     pl.inv_ds = (a.n_save > 1 && a.save_ts[a.n_save - 1] > a.save_ts[0])
                     ? (a.n_save - 1) / (a.save_ts[a.n_save - 1] - a.save_ts[0])
@@ -449,50 +450,61 @@ struct Integrator {
                 ts = load_save(a, si);
             }
         }
-        // assemble the record as 32-bit words, then store it with 16-byte vector stores
-        constexpr int RW = sizeof(R) / 4;
-        constexpr int kWords = (kRecordHeader + 5 * S * static_cast<int>(sizeof(R)) + 8 + 15) / 16 * 4;
-        unsigned w[kWords];
+        unsigned char* rec = record_ptr(a, pl.sl, traj, L.nrec);
+        if constexpr (S <= 4) {
+            // every word at a compile-time position: slot j holds state stat_state[j]
+            // (picked by value), slots past ns land in padding or past the stride;
+            // then 16-byte vector stores of the record's stride
+            constexpr int RW = sizeof(R) / 4;
+            constexpr int kWords = (kRecordHeader + 5 * S * static_cast<int>(sizeof(R)) + 15) / 16 * 4;
+            unsigned w[kWords];
 #pragma unroll
-        for (int q = 0; q < kWords; ++q) w[q] = 0u;
-        w[0] = __double2loint(t);
-        w[1] = __double2hiint(t);
-        const double inv_dt = 1.0 / dt;
-        w[2] = __double2loint(inv_dt);
-        w[3] = __double2hiint(inv_dt);
-        int j = 0;
+            for (int q = 0; q < kWords; ++q) w[q] = 0u;
+            w[0] = __double2loint(t);
+            w[1] = __double2hiint(t);
+            w[2] = __double2loint(dt);
+            w[3] = __double2hiint(dt);
+            w[kRecordIndexOffset / 4] = static_cast<unsigned>(L.si);
+            w[kRecordIndexOffset / 4 + 1] = static_cast<unsigned>(si - L.si);
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            if (!((pl.stat_mask >> s) & 1)) continue;
-            const R vals[5] = {L.y[s], h * L.k1[s], icf[s], ib[s], ia[s]};
+            for (int j = 0; j < S; ++j) {
+                const int s = pl.stat_state[j];
+                const R vals[5] = {pick(L.y, s), h * pick(L.k1, s), pick(icf, s), pick(ib, s), pick(ia, s)};
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const int base = 4 + (5 * j + q) * RW;
-                if (RW == 1) {
-                    const unsigned u = __float_as_uint(static_cast<float>(vals[q]));
-#pragma unroll
-                    for (int z = 0; z < kWords; ++z) w[z] = (z == base) ? u : w[z];
-                } else {
-                    const double dv = static_cast<double>(vals[q]);
-                    const unsigned lo = static_cast<unsigned>(__double2loint(dv));
-                    const unsigned hi = static_cast<unsigned>(__double2hiint(dv));
-#pragma unroll
-                    for (int z = 0; z < kWords; ++z) w[z] = (z == base) ? lo : ((z == base + 1) ? hi : w[z]);
+                for (int q = 0; q < 5; ++q) {
+                    const int base = kRecordHeader / 4 + (5 * j + q) * RW;
+                    if constexpr (RW == 1) {
+                        w[base] = __float_as_uint(static_cast<float>(vals[q]));
+                    } else {
+                        const double dv = static_cast<double>(vals[q]);
+                        w[base] = static_cast<unsigned>(__double2loint(dv));
+                        w[base + 1] = static_cast<unsigned>(__double2hiint(dv));
+                    }
                 }
             }
-            ++j;
-        }
-        const int iw = 4 + 5 * pl.ns * RW;  // (first_save, n_saves)
+            uint4* dst = reinterpret_cast<uint4*>(rec);
+            const int n16 = pl.sl.rec_stride / 16;
 #pragma unroll
-        for (int z = 0; z < kWords; ++z) {
-            w[z] = (z == iw) ? static_cast<unsigned>(L.si) : w[z];
-            w[z] = (z == iw + 1) ? static_cast<unsigned>(si - L.si) : w[z];
-        }
-        uint4* dst = reinterpret_cast<uint4*>(record_ptr(a, pl.sl, traj, L.nrec));
-        const int n16 = pl.sl.rec_stride / 16;
+            for (int z = 0; z < kWords / 4; ++z)
+                if (z < n16) dst[z] = make_uint4(w[4 * z], w[4 * z + 1], w[4 * z + 2], w[4 * z + 3]);
+        } else {
+            // wider systems: scalar stores of the statistics states only
+            double* hd = reinterpret_cast<double*>(rec);
+            hd[0] = t;
+            hd[1] = dt;
+            reinterpret_cast<int2*>(rec + kRecordIndexOffset)[0] = make_int2(L.si, si - L.si);
+            R* c = reinterpret_cast<R*>(rec + kRecordHeader);
 #pragma unroll
-        for (int z = 0; z < kWords / 4; ++z)
-            if (z < n16) dst[z] = make_uint4(w[4 * z], w[4 * z + 1], w[4 * z + 2], w[4 * z + 3]);
+            for (int s = 0; s < S; ++s) {
+                if (!((pl.stat_mask >> s) & 1u)) continue;
+                c[0] = L.y[s];
+                c[1] = h * L.k1[s];
+                c[2] = icf[s];
+                c[3] = ib[s];
+                c[4] = ia[s];
+                c += 5;
+            }
+        }
         L.si = si;
         L.next_save = ts;
         L.nrec++;

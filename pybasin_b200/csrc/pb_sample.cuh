@@ -179,7 +179,6 @@ __device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const 
     const int si_end = reinterpret_cast<const int*>(tl)[1];
     const double* fill = reinterpret_cast<const double*>(tl + 16);
     const int64_t nwin = a.n_save - a.win_begin;
-    const int iw = record_index_offset(NS, sizeof(R));
     const float2* split = reinterpret_cast<const float2*>(static_cast<const unsigned char*>(a.scratch) + pl.sl.split_off);
 
     SampleAcc<NS> acc;
@@ -218,12 +217,13 @@ __device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const 
         if (have) {
             const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
             rt = reinterpret_cast<const double*>(rec)[0];
-            rdt = reinterpret_cast<const double*>(rec)[1];
+            rdt = 1.0 / reinterpret_cast<const double*>(rec)[1];
+            const int2 span = reinterpret_cast<const int2*>(rec + kRecordIndexOffset)[0];
+            rsi = span.x;
+            rn = span.y;
             const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
 #pragma unroll
             for (int q = 0; q < 5 * NS; ++q) co[q] = c[q];
-            rsi = reinterpret_cast<const int*>(rec + iw)[0];
-            rn = reinterpret_cast<const int*>(rec + iw)[1];
         }
         const auto off = OffsetOf<R>::make(split, a.save_ts, rt, rdt);
         if (!acc.shift_set) {  // shift = first window sample = first save of record 0 (lane 0)

@@ -24,7 +24,10 @@
 namespace pb {
 
 constexpr int PB_MAX_STAT_STATES = 8;
-constexpr int kRecordHeader = 16;  // t, 1/dt
+// record header: t (f64), dt (f64), first covered save index, number of covered
+// saves (i32 each); the statistics slots follow
+constexpr int kRecordHeader = 24;
+constexpr int kRecordIndexOffset = 16;
 constexpr int kDefaultRecordCap = 1024;
 
 struct ScratchLayout {
@@ -89,7 +92,7 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
     l.deferred = (a.dense_mode == PB_DENSE_DEFERRED && a.n_features > 0 && a.y_full_out == nullptr) ? 1 : 0;
     if (l.deferred) {
         const int rsize = a.precision == PB_PREC_FP64 ? 8 : 4;
-        l.rec_stride = static_cast<int32_t>(align_up(kRecordHeader + 5 * count_stat_states(a) * rsize + 8, 16));
+        l.rec_stride = static_cast<int32_t>(align_up(kRecordHeader + 5 * count_stat_states(a) * rsize, 16));
         int64_t cap = a.window_record_cap > 0 ? a.window_record_cap : kDefaultRecordCap;
         if (cap > nwin) cap = nwin;
         l.cap = static_cast<int32_t>(cap);
@@ -140,8 +143,5 @@ __device__ __forceinline__ unsigned* sort_vec(const pb_solve_args& a, int64_t of
 {
     return reinterpret_cast<unsigned*>(static_cast<unsigned char*>(a.scratch) + off);
 }
-
-// offset of (first_save, n_saves) inside a record
-__host__ __device__ inline int record_index_offset(int ns, int rsize) { return kRecordHeader + 5 * ns * rsize; }
 
 }  // namespace pb
