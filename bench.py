@@ -492,8 +492,12 @@ def run_b200_arm(args) -> None:
                 "audited": g_stats[-1].n_audited,
                 "audit_error_of_confident_labels": g_stats[-1].audit_error,
                 "threshold": 0.95,
-                "net": "MLP (IC, params) -> 4 x 256 GELU -> 6 logits, BF16 mma.sync, FP32 accumulate",
+                "net": ("MLP (z-scored IC and params, sin/cos of 64 random Fourier projections) -> 4 x 256 GELU "
+                        "-> 6 logits; inference on tcgen05 (TMEM accumulators), training on BF16 mma.sync, "
+                        "FP32 accumulate; softmax temperature fitted on held-out labels"),
                 "train_labels": tinfo["n_train"],
+                "calibration_labels": tinfo["n_calibration"],
+                "temperature": tinfo["temperature"],
                 "train_label_s": tinfo["label_s"],
                 "train_s": tinfo["train_s"],
                 "train_accuracy": hist.accuracy[-1],

@@ -359,10 +359,14 @@ int pb_mlp_adamw(float* w, const float* g, float* m1, float* m2, void* w_bf16, i
                  float beta1, float beta2, float eps, float weight_decay, int32_t step, void* stream);
 /* y = BF16(x). */
 int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream);
-/* Network inputs: row r = [(ic[r, :S] , params[:n_params]) - shift] * scale, zero
- * padded to d_pad columns, as BF16. */
+/* Network inputs, as BF16 rows zero padded to d_pad columns: z = [(ic[r, :S],
+ * params[:n_params]) - shift] * scale (d = S + n_params columns), then, for the
+ * n_freq rows f of freq (n_freq x d, cycles per unit of z), sin(2 pi f.z) for
+ * every f and cos(2 pi f.z) for every f (random Fourier features; n_freq = 0
+ * and freq = NULL for z alone).  d + 2 n_freq <= d_pad. */
 int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
-                        const float* scale, int64_t n, int32_t d_pad, void* out_bf16, void* stream);
+                        const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
+                        void* out_bf16, void* stream);
 /* Confidence gate: label = argmax, conf = max softmax probability; rows with
  * conf < threshold or audit[i] != 0 are appended to route (n_route counts them,
  * reset by the call). */

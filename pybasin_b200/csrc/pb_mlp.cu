@@ -199,22 +199,40 @@ __global__ void k_cast_bf16(const float* __restrict__ x, __nv_bfloat16* __restri
         y[i] = __float2bfloat16(x[i]);
 }
 
-// Inputs of the surrogate: (x - shift) * scale per column, from FP32 ICs and an
-// FP64 parameter row, written as BF16 (n x d_pad, zero padded).
+// Inputs of the surrogate: z = (x - shift) * scale per column of x = (IC, FP64
+// parameter row), then for each of the n_freq rows f of `freq` (cycles per unit
+// of z) the pair sin(2 pi f.z), cos(2 pi f.z) (random Fourier features, which let
+// a small MLP resolve finely interleaved basins); written as BF16 rows
+// [z, sin, cos] (n x d_pad, zero padded).
+__device__ __forceinline__ float z_column(const float* __restrict__ ic, int S, const double* __restrict__ prm, int np,
+                                          const float* __restrict__ shift, const float* __restrict__ scale, int64_t r,
+                                          int c)
+{
+    const float v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
+    return (v - shift[c]) * scale[c];
+}
+
 __global__ void k_features_in(const float* __restrict__ ic, int S, const double* __restrict__ prm, int np,
-                              const float* __restrict__ shift, const float* __restrict__ scale, int64_t n, int d_pad,
+                              const float* __restrict__ shift, const float* __restrict__ scale,
+                              const float* __restrict__ freq, int n_freq, int64_t n, int d_pad,
                               __nv_bfloat16* __restrict__ out)
 {
+    const int d = S + np;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * d_pad;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = i / d_pad;
         const int c = static_cast<int>(i - r * d_pad);
         float v = 0.f;
-        if (c < S)
-            v = ic[r * S + c];
-        else if (c < S + np)
-            v = static_cast<float>(prm[c - S]);
-        if (c < S + np) v = (v - shift[c]) * scale[c];
+        if (c < d) {
+            v = z_column(ic, S, prm, np, shift, scale, r, c);
+        } else if (c < d + 2 * n_freq) {
+            const int j = (c - d) % n_freq;
+            float turns = 0.f;
+            for (int q = 0; q < d; ++q) turns = fmaf(freq[j * d + q], z_column(ic, S, prm, np, shift, scale, r, q), turns);
+            float sn, cs;
+            sincospif(2.f * turns, &sn, &cs);
+            v = (c < d + n_freq) ? sn : cs;
+        }
         out[i] = __float2bfloat16(v);
     }
 }
@@ -354,14 +372,16 @@ int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream)
 }
 
 int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
-                        const float* scale, int64_t n, int32_t d_pad, void* out_bf16, void* stream)
+                        const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
+                        void* out_bf16, void* stream)
 {
-    if (!ic || !shift || !scale || !out_bf16 || S <= 0 || n_params < 0 || S + n_params > d_pad || n < 0)
+    if (!ic || !shift || !scale || !out_bf16 || S <= 0 || n_params < 0 || n_freq < 0 ||
+        S + n_params + 2 * n_freq > d_pad || n < 0)
         return PB_EINVAL;
-    if (n_params > 0 && !params) return PB_EINVAL;
+    if ((n_params > 0 && !params) || (n_freq > 0 && !freq)) return PB_EINVAL;
     if (n == 0) return PB_SUCCESS;
     k_features_in<<<grid_for(n * d_pad, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        ic, S, params, n_params, shift, scale, n, d_pad, static_cast<__nv_bfloat16*>(out_bf16));
+        ic, S, params, n_params, shift, scale, freq, n_freq, n, d_pad, static_cast<__nv_bfloat16*>(out_bf16));
     return map_err(cudaGetLastError());
 }
 

@@ -39,6 +39,21 @@ class GateStats:
         return self.audit_disagree / max(self.audit_confident, 1)
 
 
+def calibrate_temperature(logits: np.ndarray, labels: np.ndarray, grid: np.ndarray | None = None) -> float:
+    """Softmax temperature minimising the mean negative log-likelihood of ``labels``
+    under ``logits / T`` (a grid over [0.5, 4])."""
+    grid = np.linspace(0.5, 4.0, 71) if grid is None else grid
+    lab = labels.astype(np.int64)
+    best_t, best_nll = 1.0, np.inf
+    for T in grid:
+        z = logits / T
+        z = z - z.max(axis=1, keepdims=True)
+        nll = float(np.mean(np.log(np.exp(z).sum(axis=1)) - z[np.arange(len(lab)), lab]))
+        if nll < best_nll:
+            best_t, best_nll = float(T), nll
+    return best_t
+
+
 class SurrogateGatedPipeline:
     """Surrogate in front of a ``BasinStabilityPipeline`` for one ODE system and parameter row."""
 
@@ -51,6 +66,9 @@ class SurrogateGatedPipeline:
         audit_fraction: float = 0.01,
         audit_seed: int = 123,
         seed: int = 0,
+        n_freq: int = 64,
+        freq_scale: float = 0.3,
+        calib_fraction: float = 0.1,
     ):
         self.pipe = pipeline
         self.dev = pipeline.dev
@@ -58,7 +76,9 @@ class SurrogateGatedPipeline:
         self.S = pipeline.dim
         self.C = pipeline.n_classes + 1  # + unbounded
         self.net = MLPSurrogate(self.S + self.params.numel(), self.C, hidden=hidden, depth=depth, seed=seed,
-                                device=self.dev)
+                                device=self.dev, n_freq=n_freq, freq_scale=freq_scale)
+        self.calib_fraction = calib_fraction
+        self.temperature = 1.0
         self.threshold = threshold
         self.audit_fraction = audit_fraction
         self.audit_seed = audit_seed
@@ -71,18 +91,31 @@ class SurrogateGatedPipeline:
 
     def train(self, y0_train: torch.Tensor, epochs: int = 30, batch: int = 1024, lr: float = 2e-3,
               seed: int = 0) -> tuple[TrainHistory, dict[str, float]]:
-        """Label ``y0_train`` with the integrator, then fit the network on those labels."""
+        """Label ``y0_train`` with the integrator, fit the network on all but a
+        ``calib_fraction`` slice of those labels, then calibrate its confidence on
+        the held-out slice: the softmax temperature T minimising the held-out
+        negative log-likelihood, folded into the last layer, so that the gate's
+        threshold reads as a probability of the label being right."""
         t0 = time.perf_counter()
-        labels, _ = self.pipe.run_device(y0_train.to(self.dev))
+        y0_train = y0_train.to(self.dev)
+        labels, _ = self.pipe.run_device(y0_train)
         labels = labels.clone()
         torch.cuda.synchronize(self.dev)
         t1 = time.perf_counter()
-        self.net.fit_normalisation(self._raw_inputs(y0_train.to(self.dev)))
-        x = self.net.inputs(y0_train.to(self.dev), self.params)
-        hist = self.net.train(x, labels, epochs=epochs, batch=batch, lr=lr, seed=seed)
+        n = y0_train.shape[0]
+        n_cal = int(n * self.calib_fraction) if n >= 100 else 0
+        fit_ic, fit_lab = y0_train[n_cal:], labels[n_cal:]
+        self.net.fit_normalisation(self._raw_inputs(fit_ic))
+        x = self.net.inputs(fit_ic, self.params)
+        hist = self.net.train(x, fit_lab, epochs=epochs, batch=batch, lr=lr, seed=seed)
+        if n_cal > 0:
+            z = self.net.logits(self.net.inputs(y0_train[:n_cal], self.params)).double().cpu().numpy()
+            self.temperature = calibrate_temperature(z, labels[:n_cal].cpu().numpy())
+            self.net.fold_temperature(self.temperature)
         torch.cuda.synchronize(self.dev)
         t2 = time.perf_counter()
-        return hist, {"label_s": t1 - t0, "train_s": t2 - t1, "n_train": int(y0_train.shape[0])}
+        return hist, {"label_s": t1 - t0, "train_s": t2 - t1, "n_train": int(n - n_cal), "n_calibration": n_cal,
+                      "temperature": self.temperature}
 
     # -- inference -------------------------------------------------------------------
     def audit_mask(self, n: int) -> torch.Tensor:

@@ -36,7 +36,7 @@ def _bind(lib: ctypes.CDLL) -> None:
     lib.pb_mlp_bias_grad.argtypes = [vp, i32, i32, f32, vp, vp]
     lib.pb_mlp_adamw.argtypes = [vp, vp, vp, vp, vp, i64, f32, f32, f32, f32, f32, i32, vp]
     lib.pb_mlp_cast_bf16.argtypes = [vp, vp, i64, vp]
-    lib.pb_surrogate_inputs.argtypes = [vp, i32, vp, i32, vp, vp, i64, i32, vp, vp]
+    lib.pb_surrogate_inputs.argtypes = [vp, i32, vp, i32, vp, vp, vp, i32, i64, i32, vp, vp]
     lib.pb_surrogate_gate.argtypes = [vp, i64, i32, f32, vp, vp, vp, vp, vp, vp]
     lib.pb_gather_rows.argtypes = [vp, i32, vp, vp, i64, vp, vp]
     lib.pb_merge_labels.argtypes = [vp, vp, vp, i64, vp, vp, vp]
@@ -129,13 +129,23 @@ class TrainHistory:
 
 
 class MLPSurrogate:
-    """(IC, params) -> class logits; ``depth`` hidden layers of ``hidden`` units with GELU."""
+    """(IC, params) -> class logits; ``depth`` hidden layers of ``hidden`` units with GELU.
 
-    def __init__(self, d_in: int, n_classes: int, hidden: int = 256, depth: int = 4, seed: int = 0,
-                 device: torch.device | str = "cuda"):
+    ``d_raw`` columns (IC and parameters) are z-scored; with ``n_freq`` > 0 the
+    network also sees sin and cos of 2 pi f.z for ``n_freq`` fixed random
+    frequency vectors f ~ N(0, freq_scale^2) per column (random Fourier features:
+    a plain MLP on two inputs underfits basins that interleave finely), so
+    ``d_in = d_raw + 2 n_freq``."""
+
+    def __init__(self, d_raw: int, n_classes: int, hidden: int = 256, depth: int = 4, seed: int = 0,
+                 device: torch.device | str = "cuda", n_freq: int = 0, freq_scale: float = 0.3):
         self.dev = torch.device(device)
+        self.d_raw, self.n_freq = d_raw, n_freq
+        d_in = d_raw + 2 * n_freq
         self.d_in, self.n_classes, self.hidden, self.depth = d_in, n_classes, hidden, depth
         rng = np.random.default_rng(seed)
+        self.freq = torch.tensor(rng.normal(0.0, freq_scale, (max(n_freq, 1), d_raw)), dtype=torch.float32,
+                                 device=self.dev)
         dims = [d_in] + [hidden] * depth + [n_classes]
         self.W: list[torch.Tensor] = []
         self.b: list[torch.Tensor] = []
@@ -145,8 +155,8 @@ class MLPSurrogate:
                                        device=self.dev))
             self.b.append(torch.tensor(rng.uniform(-bound, bound, fan_out), dtype=torch.float32, device=self.dev))
         self.Wb = [w.to(torch.bfloat16) for w in self.W]
-        self.shift = torch.zeros(d_in, dtype=torch.float32, device=self.dev)
-        self.scale = torch.ones(d_in, dtype=torch.float32, device=self.dev)
+        self.shift = torch.zeros(d_raw, dtype=torch.float32, device=self.dev)
+        self.scale = torch.ones(d_raw, dtype=torch.float32, device=self.dev)
         self._adam: list[tuple[torch.Tensor, torch.Tensor]] | None = None
         self._step = 0
 
@@ -168,14 +178,15 @@ class MLPSurrogate:
         _bind(lib)
         n, S = ic.shape
         npar = 0 if params is None else int(params.numel())
-        if S + npar != self.d_in:
-            raise ValueError(f"surrogate expects {self.d_in} inputs, got {S}+{npar}")
+        if S + npar != self.d_raw:
+            raise ValueError(f"surrogate expects {self.d_raw} inputs, got {S}+{npar}")
         out = torch.empty((n, self.d_in), dtype=torch.bfloat16, device=self.dev)
         s = torch.cuda.current_stream(self.dev).cuda_stream
         icc = ic.to(self.dev, torch.float32).contiguous()
         prm = None if params is None else params.to(self.dev, torch.float64).contiguous()
-        L.check(lib.pb_surrogate_inputs(_p(icc), S, _p(prm), npar, _p(self.shift), _p(self.scale), n, self.d_in,
-                                        _p(out), s), "pb_surrogate_inputs")
+        freq = self.freq if self.n_freq > 0 else None
+        L.check(lib.pb_surrogate_inputs(_p(icc), S, _p(prm), npar, _p(self.shift), _p(self.scale), _p(freq),
+                                        self.n_freq, n, self.d_in, _p(out), s), "pb_surrogate_inputs")
         return out
 
     # -- forward / backward ----------------------------------------------------
@@ -325,6 +336,7 @@ class MLPSurrogate:
         d.update({f"b{i}": b.cpu().numpy() for i, b in enumerate(self.b)})
         d["shift"] = self.shift.cpu().numpy()
         d["scale"] = self.scale.cpu().numpy()
+        d["freq"] = self.freq.cpu().numpy()
         return d
 
     def load_state_dict(self, d: dict[str, np.ndarray]) -> None:
@@ -334,3 +346,13 @@ class MLPSurrogate:
         self._tc_step = None  # repack the tensor-core weights
         self.shift = torch.tensor(d["shift"], device=self.dev)
         self.scale = torch.tensor(d["scale"], device=self.dev)
+        if "freq" in d:
+            self.freq = torch.tensor(d["freq"], device=self.dev)
+
+    def fold_temperature(self, T: float) -> None:
+        """Divide the logits by T (folded into the last layer's weights and bias)."""
+        self.W[-1] = (self.W[-1] / T).contiguous()
+        self.b[-1] = (self.b[-1] / T).contiguous()
+        self.Wb[-1] = self.W[-1].to(torch.bfloat16)
+        self._adam = None  # the optimiser state no longer matches the weights
+        self._step += 1  # repack the tensor-core weights

@@ -205,3 +205,58 @@ def test_tensor_core_mlp_matches_layer_by_layer_forward():
     assert (tc - ref).abs().max().item() <= 2e-2 * scale
     assert (tc.argmax(1) == ref.argmax(1)).float().mean().item() >= 0.995
     assert torch.equal(net.logits(x), tc)  # inference takes the tensor-core path
+
+
+def test_temperature_calibration_recovers_the_generating_temperature():
+    """Labels drawn from softmax(z / 2): the held-out NLL is smallest near T = 2."""
+    from pybasin_b200.gated import calibrate_temperature
+
+    rng = np.random.default_rng(5)
+    z = rng.normal(0.0, 4.0, (20000, 6))
+    p = np.exp(z / 2.0 - (z / 2.0).max(axis=1, keepdims=True))
+    p /= p.sum(axis=1, keepdims=True)
+    labels = np.array([rng.choice(6, p=row) for row in p])
+    assert abs(calibrate_temperature(z, labels) - 2.0) <= 0.1
+    # confident logits that are always right: the sharpest temperature of the grid
+    assert calibrate_temperature(z, z.argmax(axis=1)) == 0.5
+
+
+@pytest.mark.gpu
+def test_fourier_inputs_match_fp32_reference():
+    """pb_surrogate_inputs against the same features in PyTorch FP32, both rounded to
+    BF16: z-scored columns, then sin and cos of 2 pi f.z (one BF16 step of 2^-7 at 1
+    covers the FP32 differences between the two sine evaluations)."""
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(5, 6, hidden=64, depth=2, seed=2, device=dev, n_freq=16, freq_scale=0.7)
+    g = torch.Generator().manual_seed(3)
+    ic = (torch.rand(3000, 2, generator=g) * 4 - 2).to(dev)
+    params = torch.tensor([0.08, 1.0, 0.2], dtype=torch.float64, device=dev)
+    raw = torch.cat([ic, params.float().expand(3000, -1)], dim=1)
+    net.fit_normalisation(raw)
+    x = net.inputs(ic, params).float()
+    assert x.shape == (3000, 5 + 32)
+    z = (raw - net.shift) * net.scale
+    ph = 2 * np.pi * (z.double() @ net.freq.double().T)
+    ref = torch.cat([z.double(), torch.sin(ph), torch.cos(ph)], dim=1).float().to(torch.bfloat16).float()
+    assert (x - ref).abs().max().item() <= 2.0 ** -7 + 1e-6
+    assert (x[:, 2:5] == 0).all()  # constant parameter columns (zero spread) carry nothing
+
+
+@pytest.mark.gpu
+def test_folded_temperature_divides_the_logits():
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(5, 6, hidden=128, depth=3, seed=4, device=dev, n_freq=8)
+    g = torch.Generator().manual_seed(1)
+    ic = torch.randn(2000, 2, generator=g).to(dev)
+    params = torch.tensor([0.08, 1.0, 0.2], dtype=torch.float64, device=dev)
+    x = net.inputs(ic, params)
+    before = net.logits(x)
+    net.fold_temperature(2.0)
+    after = net.logits(x)
+    torch.cuda.synchronize()
+    scale = before.abs().max().item()
+    assert (after - before / 2.0).abs().max().item() <= 1e-2 * scale
