@@ -512,7 +512,8 @@ def run_b200_arm(args) -> None:
                 "h2d_bytes_per_step": int(y0_host.numel() * 4),
                 "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8),
             },
-            "gpu_launches": (pipe.kernel_launches_per_pass() + (9 if use_gate else 0)) * args.steps,
+            # gated: input features, tensor-core MLP, gate, gather, merge, summary
+            "gpu_launches": (pipe.kernel_launches_per_pass() + (6 if use_gate else 0)) * args.steps,
             "roofline": {
                 "bound": "fp32-fma",
                 "achieved": achieved / 1e12,

@@ -248,6 +248,13 @@ int pb_label_nearest(const double* features, int64_t n, int32_t n_features,
  * NaN coordinates do not widen the bounding box and quantise to 0. */
 int pb_morton_keys(const void* y0, int32_t y0_dtype, int64_t n, int32_t dim, int32_t bits,
                    const int32_t* groups, uint64_t* bbox_work, int64_t* keys_out, void* stream);
+/* Processing order from keys: order_out (n int32) = the stable ascending argsort of
+ * keys[0..n) on bits [0, end_bit) (an LSD radix sort; keys is clobbered).  scratch
+ * holds pb_morton_order_scratch_bytes(n) bytes (256-byte aligned).  No reference
+ * counterpart (see pb_morton_keys). */
+int64_t pb_morton_order_scratch_bytes(int64_t n);
+int pb_morton_order(int64_t* keys, int64_t n, int32_t end_bit, void* scratch, int64_t scratch_bytes,
+                    int32_t* order_out, void* stream);
 
 /* Occupancy helper for the autotuner: resident blocks per SM of the pb_solve_batch
  * kernel selected by (system, dim, precision, schedule) at `block_size`. */
@@ -379,6 +386,17 @@ int pb_gather_rows(const float* x, int32_t width, const int32_t* idx, const int3
  * each routed row is kept in surrogate_label_of_routed[k] (may be NULL). */
 int pb_merge_labels(const int32_t* integrated, const int32_t* idx, const int32_t* n_idx, int64_t max_rows,
                     int32_t* label, int32_t* surrogate_label_of_routed, void* stream);
+/* Summary of a gated pass, without host round trips: counts[c] (int64, C <= 64)
+ * of the final labels, and over the routed rows (route[:min(*n_route, max_rows)];
+ * route may be NULL for none) the audit tally stats[0] = audited rows, stats[1] =
+ * those whose surrogate confidence conf[i] was >= threshold, stats[2] = those of
+ * them whose surrogate label (surrogate_label_of_routed[q]) differs from the
+ * integrator's (integrated[q]).  counts and stats are cleared by the call.  No
+ * counterpart in the reference (the surrogate gate is this library's own). */
+int pb_gate_summary(const int32_t* label, int64_t n, int32_t C, const int32_t* route, const int32_t* n_route,
+                    int64_t max_rows, const uint8_t* audit, const float* conf, float threshold,
+                    const int32_t* surrogate_label_of_routed, const int32_t* integrated, int64_t* counts,
+                    int32_t* stats, void* stream);
 
 /* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
 const char* pb_error_string(int32_t status);

@@ -178,6 +178,8 @@ EXPORTED_SYMBOLS = (
     "pb_probe_fma",
     "pb_solve_batch_noalloc",
     "pb_morton_keys",
+    "pb_morton_order_scratch_bytes",
+    "pb_morton_order",
     "pb_rhs_compile",
     "pb_solve_batch_rhs",
     "pb_rhs_release",
@@ -224,6 +226,10 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
         lib.pb_rhs_release.argtypes = [_c_vp]
         lib.pb_morton_keys.restype = ctypes.c_int
         lib.pb_morton_keys.argtypes = [_c_vp, _c_i32, _c_i64, _c_i32, _c_i32, _c_vp, _c_vp, _c_vp, _c_vp]
+        lib.pb_morton_order_scratch_bytes.restype = _c_i64
+        lib.pb_morton_order_scratch_bytes.argtypes = [_c_i64]
+        lib.pb_morton_order.restype = ctypes.c_int
+        lib.pb_morton_order.argtypes = [_c_vp, _c_i64, _c_i32, _c_vp, _c_i64, _c_vp, _c_vp]
         lib.pb_query_occupancy.restype = ctypes.c_int
         lib.pb_query_occupancy.argtypes = [
             _c_i32, _c_i32, _c_i32, _c_i32, _c_i32, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32),

@@ -311,6 +311,8 @@ KernelSel select_prec()
     k.queue_defer = rt_fn(k_solve_queue<Sys, R, true>);
     k.queue_probe = rt_fn(k_solve_queue<Sys, R, true, 1>);
     k.queue_main = rt_fn(k_solve_queue<Sys, R, true, 2>);
+    k.queue_main_s1 = rt_fn(k_solve_queue<Sys, R, true, 2, SampleDrain<R, 1>>);
+    k.queue_main_s2 = rt_fn(k_solve_queue<Sys, R, true, 2, SampleDrain<R, 2>>);
     return k;
 }
 
@@ -546,6 +548,16 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
     if (plain_grid > 0x7fffffffLL) return PB_EINVAL;
 
     if (sl.deferred) {
+        bool any_cross = false;
+        for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
+        const int ns = count_stat_states(a);
+        if (a.precision != PB_PREC_FP64) {  // FP32 offsets of the save grid, for the sampling
+            k_split_saves<<<(a.n_save + 255) / 256, 256, 0, st>>>(
+                a.save_ts, a.n_save,
+                reinterpret_cast<float2*>(static_cast<unsigned char*>(a.scratch) + sl.split_off));
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return map_cuda(e);
+        }
         // pass 1: integrate, one record per window step holding save points
         if (sl.probed) {
             // probe phase, longest-first sort of its step counts, main phase
@@ -555,10 +567,19 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
             if (e != cudaSuccess) return map_cuda(e);
             e = launch_fn(k.queue_probe, grid, block, 0, st, a, &zero);
             if (e == cudaSuccess) e = sort_by_probe(a, sl, st);
-            if (e == cudaSuccess) e = persistent_grid(k.queue_main, block, 0, a.n_traj, a.grid_blocks, &grid);
+            // main phase, with the sampling drained into it where a variant exists
+            // (1 or 2 feature states, no crossing counts); the pass below samples
+            // whatever it leaves
+            KFn main = k.queue_main;
+            if (!any_cross && ns == 1 && k.queue_main_s1.ok()) main = k.queue_main_s1;
+            if (!any_cross && ns == 2 && k.queue_main_s2.ok()) main = k.queue_main_s2;
+            if (e == cudaSuccess) e = persistent_grid(main, block, 0, a.n_traj, a.grid_blocks, &grid);
             if (e == cudaSuccess) e = cudaMemsetAsync(a.queue_counter, 0, sizeof(unsigned long long), st);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(static_cast<unsigned char*>(a.scratch) + sl.drain_off, 0,
+                                    static_cast<size_t>(drain_bytes(sl, a.n_traj)), st);
             if (e != cudaSuccess) return map_cuda(e);
-            e = launch_fn(k.queue_main, grid, block, 0, st, a, &zero);
+            e = launch_fn(main, grid, block, 0, st, a, &zero);
         } else if (a.schedule != PB_SCHED_PLAIN) {
             int64_t grid = 0;
             e = persistent_grid(k.queue_defer, block, 0, a.n_traj, a.grid_blocks, &grid);
@@ -572,17 +593,8 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
         // pass 2: one warp per trajectory evaluates its save points and reduces the statistics
         const int64_t sblocks = (a.n_traj + 3) / 4;
         if (sblocks > 0x7fffffffLL) return PB_EINVAL;
-        bool any_cross = false;
-        for (int c = 0; c < a.n_features; ++c) any_cross |= a.feat_kind[c] == PB_FEAT_CROSSINGS;
-        const KFn sample = sample_kernel(a.precision, count_stat_states(a), any_cross);
+        const KFn sample = sample_kernel(a.precision, ns, any_cross);
         if (!sample.ok()) return PB_EUNSUPPORTED;
-        if (a.precision != PB_PREC_FP64) {
-            k_split_saves<<<(a.n_save + 255) / 256, 256, 0, st>>>(
-                a.save_ts, a.n_save,
-                reinterpret_cast<float2*>(static_cast<unsigned char*>(a.scratch) + sl.split_off));
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return map_cuda(e);
-        }
         e = launch_fn(sample, sblocks, 128, 0, st, a, nullptr);
         if (e != cudaSuccess) return map_cuda(e);
         // pass 3: trajectories that exceeded the record capacity, inline

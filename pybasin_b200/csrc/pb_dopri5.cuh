@@ -854,7 +854,17 @@ __global__ void __launch_bounds__(256) k_solve_plain(const pb_solve_args a)
 // steps, and every output, is the one of PHASE 0.
 constexpr double kProbeFraction = 0.05;
 
-template <class Sys, class R, bool DEFER, int PHASE = 0>
+// Main phase without sampling: the window is sampled by the next launch.
+struct NoDrain {
+    static constexpr bool kOn = false;
+    __device__ static void publish(const pb_solve_args&, const Plan&, int64_t) {}
+    __device__ static void drain(const pb_solve_args&, const Plan&, int) {}
+};
+
+// Drain (PHASE 2): each finished trajectory is published (Drain::publish, per
+// lane); a warp that finds the queue empty samples published trajectories
+// (Drain::drain) while the longest ones are still integrating.
+template <class Sys, class R, bool DEFER, int PHASE = 0, class Drain = NoDrain>
 __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int redo_only)
 {
     static_assert(PHASE == 0 || DEFER, "the probed schedule saves no inline statistics");
@@ -870,7 +880,10 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.queue_counter, 32ull);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (static_cast<int64_t>(base) >= a.n_traj) break;
+        if (static_cast<int64_t>(base) >= a.n_traj) {
+            if constexpr (Drain::kOn) Drain::drain(a, pl, lane);
+            break;
+        }
         const int64_t q = static_cast<int64_t>(base) + lane;
         if (q < a.n_traj) {
             const int64_t traj = PHASE == 2 ? static_cast<int64_t>(sort_vec(a, pl.sl.val_out_off)[q]) : traj_at(a, q);
@@ -886,6 +899,7 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
                         }
                         I::template finish<DEFER>(L, st, pl, traj, a);
                     }
+                    if constexpr (Drain::kOn) Drain::publish(a, pl, traj);
                 } else if (PHASE == 1) {
                     I::begin(L, st, traj, a);
                     bool done = false;
@@ -900,6 +914,8 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
                     I::template finish<DEFER>(L, st, pl, traj, a);
                 }
             }
+            if constexpr (PHASE == 2 && Drain::kOn)
+                if (skip) Drain::publish(a, pl, -1);
             if (PHASE == 1) {
                 sort_vec(a, pl.sl.key_in_off)[q] = key;
                 sort_vec(a, pl.sl.val_in_off)[q] = static_cast<unsigned>(traj);

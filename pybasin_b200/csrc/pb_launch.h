@@ -22,6 +22,8 @@ struct KernelSel {
     KFn queue_defer;   // deferred pass 1, persistent warps
     KFn queue_probe;   // deferred pass 1, probed schedule: probe phase
     KFn queue_main;    // deferred pass 1, probed schedule: main phase
+    KFn queue_main_s1; // ... with the sampling of 1 (2) feature states drained into it
+    KFn queue_main_s2;
     int smem_per_thread = 0;  // inline kernels: per-thread statistics slot
 };
 

@@ -204,36 +204,46 @@ __global__ void k_cast_bf16(const float* __restrict__ x, __nv_bfloat16* __restri
 // of z) the pair sin(2 pi f.z), cos(2 pi f.z) (random Fourier features, which let
 // a small MLP resolve finely interleaved basins); written as BF16 rows
 // [z, sin, cos] (n x d_pad, zero padded).
-__device__ __forceinline__ float z_column(const float* __restrict__ ic, int S, const double* __restrict__ prm, int np,
-                                          const float* __restrict__ shift, const float* __restrict__ scale, int64_t r,
-                                          int c)
-{
-    const float v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
-    return (v - shift[c]) * scale[c];
-}
+constexpr int kMaxRawInputs = 16;
 
+// One thread per (row, frequency): the row's d z-scored columns in registers (d
+// cached loads), the frequency's sine-cosine pair, and every U-th z or padding
+// column from its own index on; neighbouring threads write neighbouring columns.
 __global__ void k_features_in(const float* __restrict__ ic, int S, const double* __restrict__ prm, int np,
                               const float* __restrict__ shift, const float* __restrict__ scale,
                               const float* __restrict__ freq, int n_freq, int64_t n, int d_pad,
                               __nv_bfloat16* __restrict__ out)
 {
     const int d = S + np;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * d_pad;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = i / d_pad;
-        const int c = static_cast<int>(i - r * d_pad);
-        float v = 0.f;
-        if (c < d) {
-            v = z_column(ic, S, prm, np, shift, scale, r, c);
-        } else if (c < d + 2 * n_freq) {
-            const int j = (c - d) % n_freq;
+    const int U = n_freq > 0 ? n_freq : 1;
+    const int n_zero = d_pad - d - 2 * n_freq;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * U; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = t / U;
+        const int j = static_cast<int>(t - r * U);
+        __nv_bfloat16* o = out + r * d_pad;
+        float z[kMaxRawInputs];
+#pragma unroll
+        for (int c = 0; c < kMaxRawInputs; ++c) {
+            z[c] = 0.f;
+            if (c < d) {
+                const float v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
+                z[c] = (v - shift[c]) * scale[c];
+            }
+        }
+        if (n_freq > 0) {
             float turns = 0.f;
-            for (int q = 0; q < d; ++q) turns = fmaf(freq[j * d + q], z_column(ic, S, prm, np, shift, scale, r, q), turns);
+#pragma unroll
+            for (int c = 0; c < kMaxRawInputs; ++c)
+                if (c < d) turns = fmaf(freq[j * d + c], z[c], turns);
             float sn, cs;
             sincospif(2.f * turns, &sn, &cs);
-            v = (c < d + n_freq) ? sn : cs;
+            o[d + j] = __float2bfloat16(sn);
+            o[d + n_freq + j] = __float2bfloat16(cs);
         }
-        out[i] = __float2bfloat16(v);
+#pragma unroll
+        for (int c = 0; c < kMaxRawInputs; ++c)
+            if (c < d && c % U == j) o[c] = __float2bfloat16(z[c]);
+        for (int c = j; c < n_zero; c += U) o[d + 2 * n_freq + c] = __float2bfloat16(0.f);
     }
 }
 
@@ -290,6 +300,48 @@ __global__ void k_merge_labels(const int32_t* __restrict__ integ, const int32_t*
         if (surrogate_label_of_routed) surrogate_label_of_routed[k] = label[i];
         label[i] = integ[k];
     }
+}
+
+// Per-class counts of the final labels, and the audit tally over the routed rows:
+// stats[0] audited rows, stats[1] of those the ones the surrogate was confident
+// about (conf >= threshold), stats[2] of those the ones the integrator labelled
+// differently.  counts and stats start at zero (cleared by the entry point).
+constexpr int kMaxSummaryClasses = 64;
+__global__ void k_gate_summary(const int32_t* __restrict__ label, int64_t n, int C, const int32_t* __restrict__ route,
+                               const int32_t* __restrict__ n_route, int64_t max_rows, const uint8_t* __restrict__ audit,
+                               const float* __restrict__ conf, float threshold, const int32_t* __restrict__ sur,
+                               const int32_t* __restrict__ integ, unsigned long long* __restrict__ counts,
+                               int32_t* __restrict__ stats)
+{
+    __shared__ unsigned int hist[kMaxSummaryClasses];
+    __shared__ int tally[3];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) hist[c] = 0u;
+    if (threadIdx.x < 3) tally[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int c = label[i];
+        if (c >= 0 && c < C) atomicAdd(&hist[c], 1u);
+    }
+    const int64_t k = route ? min(static_cast<int64_t>(*n_route), max_rows) : 0;
+    int na = 0, nc = 0, nd = 0;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < k; q += stride) {
+        const int i = route[q];
+        if (audit && audit[i]) {
+            ++na;
+            if (conf[i] >= threshold) {
+                ++nc;
+                nd += sur[q] != integ[q] ? 1 : 0;
+            }
+        }
+    }
+    if (na) atomicAdd(&tally[0], na);
+    if (nc) atomicAdd(&tally[1], nc);
+    if (nd) atomicAdd(&tally[2], nd);
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        if (hist[c]) atomicAdd(&counts[c], static_cast<unsigned long long>(hist[c]));
+    if (threadIdx.x < 3 && tally[threadIdx.x]) atomicAdd(&stats[threadIdx.x], tally[threadIdx.x]);
 }
 
 int grid_for(int64_t n, int block)
@@ -376,11 +428,11 @@ int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_
                         void* out_bf16, void* stream)
 {
     if (!ic || !shift || !scale || !out_bf16 || S <= 0 || n_params < 0 || n_freq < 0 ||
-        S + n_params + 2 * n_freq > d_pad || n < 0)
+        S + n_params > kMaxRawInputs || S + n_params + 2 * n_freq > d_pad || n < 0)
         return PB_EINVAL;
     if ((n_params > 0 && !params) || (n_freq > 0 && !freq)) return PB_EINVAL;
     if (n == 0) return PB_SUCCESS;
-    k_features_in<<<grid_for(n * d_pad, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_features_in<<<grid_for(n * (n_freq > 0 ? n_freq : 1), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         ic, S, params, n_params, shift, scale, freq, n_freq, n, d_pad, static_cast<__nv_bfloat16*>(out_bf16));
     return map_err(cudaGetLastError());
 }
@@ -405,6 +457,27 @@ int pb_gather_rows(const float* x, int32_t width, const int32_t* idx, const int3
     if (max_rows == 0) return PB_SUCCESS;
     k_gather_rows<<<grid_for(max_rows * width, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         x, width, idx, n_idx, max_rows, y);
+    return map_err(cudaGetLastError());
+}
+
+int pb_gate_summary(const int32_t* label, int64_t n, int32_t C, const int32_t* route, const int32_t* n_route,
+                    int64_t max_rows, const uint8_t* audit, const float* conf, float threshold,
+                    const int32_t* surrogate_label_of_routed, const int32_t* integrated, int64_t* counts,
+                    int32_t* stats, void* stream)
+{
+    if (!label || n < 0 || C <= 0 || C > kMaxSummaryClasses || !counts || !stats || max_rows < 0) return PB_EINVAL;
+    if (route && (!n_route || !conf || !surrogate_label_of_routed || !integrated)) return PB_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(counts, 0, sizeof(int64_t) * C, st) != cudaSuccess ||
+        cudaMemsetAsync(stats, 0, sizeof(int32_t) * 3, st) != cudaSuccess)
+        return PB_ECUDA;
+    const int64_t work = n > max_rows ? n : max_rows;
+    if (work == 0) return PB_SUCCESS;
+    int blocks = grid_for(work, 256);
+    if (blocks > 1184) blocks = 1184;  // 8 blocks per SM of a 148-SM part: one atomic flush each
+    k_gate_summary<<<blocks, 256, 0, st>>>(label, n, C, route, n_route, max_rows, audit, conf, threshold,
+                                           surrogate_label_of_routed, integrated,
+                                           reinterpret_cast<unsigned long long*>(counts), stats);
     return map_err(cudaGetLastError());
 }
 

@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "pybasin_b200.h"
 
 namespace pb {
@@ -94,9 +96,70 @@ __global__ void __launch_bounds__(256) k_morton(const T* __restrict__ y0, int64_
     keys[i] = static_cast<long long>(key);
 }
 
+__global__ void k_iota(int32_t* __restrict__ v, int64_t n)
+{
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = static_cast<int32_t>(i);
+}
+
+// scratch of pb_morton_order: alternate key buffer, alternate index buffer, then
+// the radix sort's temporary storage, each 256-byte aligned
+struct SortScratch {
+    size_t keys_alt, vals_alt, temp, temp_bytes, total;
+};
+
+inline size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+inline bool sort_scratch(int64_t n, SortScratch& l)
+{
+    l.temp_bytes = 0;
+    cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
+    cub::DoubleBuffer<int32_t> v(nullptr, nullptr);
+    if (cub::DeviceRadixSort::SortPairs(nullptr, l.temp_bytes, k, v, static_cast<int>(n)) != cudaSuccess)
+        return false;
+    l.keys_alt = 0;
+    l.vals_alt = align256(static_cast<size_t>(n) * sizeof(unsigned long long));
+    l.temp = l.vals_alt + align256(static_cast<size_t>(n) * sizeof(int32_t));
+    l.total = l.temp + align256(l.temp_bytes);
+    return true;
+}
+
 }  // namespace pb
 
 using namespace pb;
+
+extern "C" int64_t pb_morton_order_scratch_bytes(int64_t n)
+{
+    if (n < 0 || n > 0x7fffffffLL) return -1;
+    SortScratch l;
+    if (!sort_scratch(n < 1 ? 1 : n, l)) return -1;
+    return static_cast<int64_t>(l.total);
+}
+
+extern "C" int pb_morton_order(int64_t* keys, int64_t n, int32_t end_bit, void* scratch, int64_t scratch_bytes,
+                               int32_t* order_out, void* stream)
+{
+    if (n < 0 || n > 0x7fffffffLL || end_bit < 1 || end_bit > 64) return PB_EINVAL;
+    if (n == 0) return PB_SUCCESS;
+    if (!keys || !scratch || !order_out) return PB_EINVAL;
+    SortScratch l;
+    if (!sort_scratch(n, l)) return PB_ECUDA;
+    if (scratch_bytes < static_cast<int64_t>(l.total)) return PB_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(scratch);
+    k_iota<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(order_out, n);
+    cub::DoubleBuffer<unsigned long long> k(reinterpret_cast<unsigned long long*>(keys),
+                                            reinterpret_cast<unsigned long long*>(b + l.keys_alt));
+    cub::DoubleBuffer<int32_t> v(order_out, reinterpret_cast<int32_t*>(b + l.vals_alt));
+    size_t tb = l.temp_bytes;
+    if (cub::DeviceRadixSort::SortPairs(b + l.temp, tb, k, v, static_cast<int>(n), 0, end_bit, st) != cudaSuccess)
+        return PB_ECUDA;
+    if (v.Current() != order_out &&
+        cudaMemcpyAsync(order_out, v.Current(), static_cast<size_t>(n) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                        st) != cudaSuccess)
+        return PB_ECUDA;
+    return cudaGetLastError() == cudaSuccess ? PB_SUCCESS : PB_ECUDA;
+}
 
 extern "C" int pb_morton_keys(const void* y0, int32_t y0_dtype, int64_t n, int32_t dim, int32_t bits,
                               const int32_t* groups, uint64_t* bbox_work, int64_t* keys_out, void* stream)

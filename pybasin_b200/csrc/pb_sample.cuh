@@ -170,13 +170,15 @@ struct OffsetOf<float> {
 // NC = crossing states compiled in (0 when no column counts crossings, which
 // keeps the per-lane crossing registers out of the common case).
 // Sampling of one trajectory by the calling warp (all 32 lanes, warp-uniform traj).
+// What the integrator wrote (tail, records) is read through L2 (__ldcg): when the
+// sampling is drained into the main phase, another SM wrote it during this launch.
 template <class R, int NS, int NC>
 __device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const Plan& pl, int64_t traj, int lane)
 {
     const unsigned char* tl = tail_ptr(a, pl.sl, traj);
-    const int nrec = reinterpret_cast<const int*>(tl)[0];
+    const int nrec = __ldcg(reinterpret_cast<const int*>(tl));
     if (nrec < 0) return;  // integrated again by the inline pass
-    const int si_end = reinterpret_cast<const int*>(tl)[1];
+    const int si_end = __ldcg(reinterpret_cast<const int*>(tl) + 1);
     const double* fill = reinterpret_cast<const double*>(tl + 16);
     const int64_t nwin = a.n_save - a.win_begin;
     const float2* split = reinterpret_cast<const float2*>(static_cast<const unsigned char*>(a.scratch) + pl.sl.split_off);
@@ -216,14 +218,14 @@ __device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const 
         for (int q = 0; q < 5 * NS; ++q) co[q] = R(0);
         if (have) {
             const unsigned char* rec = record_ptr(a, pl.sl, traj, k);
-            rt = reinterpret_cast<const double*>(rec)[0];
-            rdt = 1.0 / reinterpret_cast<const double*>(rec)[1];
-            const int2 span = reinterpret_cast<const int2*>(rec + kRecordIndexOffset)[0];
+            rt = __ldcg(reinterpret_cast<const double*>(rec));
+            rdt = 1.0 / __ldcg(reinterpret_cast<const double*>(rec) + 1);
+            const int2 span = __ldcg(reinterpret_cast<const int2*>(rec + kRecordIndexOffset));
             rsi = span.x;
             rn = span.y;
             const R* c = reinterpret_cast<const R*>(rec + kRecordHeader);
 #pragma unroll
-            for (int q = 0; q < 5 * NS; ++q) co[q] = c[q];
+            for (int q = 0; q < 5 * NS; ++q) co[q] = __ldcg(c + q);
         }
         const auto off = OffsetOf<R>::make(split, a.save_ts, rt, rdt);
         if (!acc.shift_set) {  // shift = first window sample = first save of record 0 (lane 0)
@@ -311,7 +313,7 @@ __device__ __forceinline__ void sample_trajectory(const pb_solve_args& a, const 
         const int nvalid = min(32, a.n_save - j0);
         double v[NS];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) v[q] = fill[pl.stat_state[q]];
+        for (int q = 0; q < NS; ++q) v[q] = __ldcg(fill + pl.stat_state[q]);
         fold_samples(acc, pl, a, traj, nwin, j0, nvalid, v, lane);
     }
     // warp reductions
@@ -360,7 +362,62 @@ __global__ void __launch_bounds__(128) k_sample(const pb_solve_args a)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t traj = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
     if (traj >= a.n_traj || pl.ns != NS) return;  // warp-uniform
+    if (pl.sl.probed && drain_sampled(a, pl.sl, a.n_traj)[traj]) return;  // sampled by the main phase
     sample_trajectory<R, NS, NC>(a, pl, traj, lane);
 }
+
+// Sampling drained into the probed main phase (k_solve_queue's Drain).  A lane
+// that finishes a trajectory publishes it: after a fence (its records and tail
+// are visible device-wide), it takes the next slot of the published list and
+// stores the id + 1 there (a skipped queue position stores -1).  A
+// warp that finds the queue empty claims slots in order and samples each one's
+// trajectory once it is published, while the longest trajectories still
+// integrate.  Every wait is bounded: a warp that waits longer than kMaxPolls
+// polls for a slot stops draining, and the sampling pass after the launch takes
+// every trajectory whose sampled flag is not set.  Producers never wait, so no
+// lane depends on a waiting warp.
+constexpr int kMaxPolls = 1 << 17;
+
+template <class R, int NS>
+struct SampleDrain {
+    static constexpr bool kOn = true;
+    __device__ static void publish(const pb_solve_args& a, const Plan& pl, int64_t traj)
+    {
+        __threadfence();
+        unsigned long long* cnt = drain_counters(a, pl.sl);
+        const unsigned long long slot = atomicAdd(cnt, 1ull);
+        if (slot < static_cast<unsigned long long>(a.n_traj))
+            atomicExch(drain_list(a, pl.sl) + slot, traj >= 0 ? static_cast<int>(traj) + 1 : -1);
+    }
+    __device__ static void drain(const pb_solve_args& a, const Plan& pl, int lane)
+    {
+        if (pl.ns != NS || pl.n_cross > 0) return;  // warp-uniform: the sampling pass covers it
+        unsigned long long* cnt = drain_counters(a, pl.sl);
+        int* list = drain_list(a, pl.sl);
+        unsigned char* sampled = drain_sampled(a, pl.sl, a.n_traj);
+        while (true) {
+            unsigned long long slot = 0;
+            if (lane == 0) slot = atomicAdd(cnt + 1, 1ull);
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            if (slot >= static_cast<unsigned long long>(a.n_traj)) return;
+            int v = 0;
+            if (lane == 0) {
+                for (int poll = 0; poll < kMaxPolls; ++poll) {
+                    v = atomicAdd(list + slot, 0);
+                    if (v != 0) break;
+                    __nanosleep(256);
+                }
+            }
+            v = __shfl_sync(0xffffffffu, v, 0);
+            if (v == 0) return;  // gave up: the sampling pass takes what is left
+            __threadfence();
+            if (v > 0) {
+                sample_trajectory<R, NS, 0>(a, pl, v - 1, lane);
+                __syncwarp();
+                if (lane == 0) sampled[v - 1] = 1;
+            }
+        }
+    }
+};
 
 }  // namespace pb

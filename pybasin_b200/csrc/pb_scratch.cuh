@@ -39,6 +39,9 @@ struct ScratchLayout {
     int64_t key_out_off;
     int64_t val_in_off;    // trajectory ids, in queue order
     int64_t val_out_off;   // trajectory ids, longest predicted first
+    int64_t drain_off;     // main phase sampling drained into the integrator (probed): two
+                           // u64 counters (published, claimed), then the published
+                           // trajectory ids + 1 (int32, n_traj), then sampled flags (u8, n_traj)
     int64_t sort_tmp_off;  // radix-sort temporary storage (last)
     int64_t split_off;     // deferred dense output: (hi, lo) float split of the save grid
     int64_t total;         // excluding the radix-sort temporary
@@ -114,6 +117,8 @@ __host__ __device__ inline ScratchLayout scratch_layout(const pb_solve_args& a)
             l.val_in_off = off + 2 * vec;
             l.val_out_off = off + 3 * vec;
             off += 4 * vec;
+            l.drain_off = off;
+            off += 256 + vec + align_up(a.n_traj, 256);
             l.sort_tmp_off = off;
         }
     }
@@ -139,6 +144,24 @@ __device__ __forceinline__ unsigned char* state_ptr(const pb_solve_args& a, cons
 {
     return static_cast<unsigned char*>(a.scratch) + l.state_off + traj * l.state_stride;
 }
+// drain region of the probed schedule (see ScratchLayout::drain_off)
+__host__ __device__ inline int64_t drain_bytes(const ScratchLayout& l, int64_t n_traj)
+{
+    return l.probed ? 256 + align_up(n_traj * 4, 256) + align_up(n_traj, 256) : 0;
+}
+__device__ __forceinline__ unsigned long long* drain_counters(const pb_solve_args& a, const ScratchLayout& l)
+{
+    return reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(a.scratch) + l.drain_off);
+}
+__device__ __forceinline__ int* drain_list(const pb_solve_args& a, const ScratchLayout& l)
+{
+    return reinterpret_cast<int*>(static_cast<unsigned char*>(a.scratch) + l.drain_off + 256);
+}
+__device__ __forceinline__ unsigned char* drain_sampled(const pb_solve_args& a, const ScratchLayout& l, int64_t n)
+{
+    return static_cast<unsigned char*>(a.scratch) + l.drain_off + 256 + align_up(n * 4, 256);
+}
+
 __device__ __forceinline__ unsigned* sort_vec(const pb_solve_args& a, int64_t off)
 {
     return reinterpret_cast<unsigned*>(static_cast<unsigned char*>(a.scratch) + off);

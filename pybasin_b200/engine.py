@@ -326,7 +326,25 @@ class MortonOrder:
         L.check(rc, "pb_morton_keys")
         return self.keys[:n]
 
-    def __call__(self, y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None) -> torch.Tensor:
-        if y0.shape[0] == 0:
-            return torch.zeros((0,), dtype=torch.int32, device=self.dev)
-        return torch.argsort(self.keys_of(y0, bits, groups)).to(torch.int32)
+    def __call__(self, y0: torch.Tensor, bits: int | None = None, groups: torch.Tensor | None = None,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+        """int32 processing order: the stable argsort of the keys (``pb_morton_order``,
+        a radix sort over the key bits in use), written to ``out`` if given."""
+        n, dims = y0.shape
+        if out is None:
+            out = torch.empty((n,), dtype=torch.int32, device=self.dev)
+        if n == 0:
+            return out
+        d = min(dims, 4)
+        bits = min(bits or max(1, 60 // d if d > 2 else 20), 62 // d)
+        keys = self.keys_of(y0, bits, groups)
+        lib = L.load()
+        need = int(lib.pb_morton_order_scratch_bytes(n))
+        if need < 0:
+            raise RuntimeError("pb_morton_order_scratch_bytes failed")
+        if getattr(self, "_sort_scratch", None) is None or self._sort_scratch.numel() < need:
+            self._sort_scratch = torch.empty((need,), dtype=torch.uint8, device=self.dev)
+        end_bit = 64 if groups is not None else bits * d
+        L.check(lib.pb_morton_order(keys.data_ptr(), n, end_bit, self._sort_scratch.data_ptr(), need, out.data_ptr(),
+                                    torch.cuda.current_stream(self.dev).cuda_stream), "pb_morton_order")
+        return out

@@ -12,7 +12,6 @@ from __future__ import annotations
 
 import ctypes
 import time
-from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -22,13 +21,41 @@ from pybasin_b200.pipeline import BasinStabilityPipeline
 from pybasin_b200.surrogate import MLPSurrogate, TrainHistory, _bind, _p
 
 
-@dataclass
 class GateStats:
-    n: int
-    n_routed: int
-    n_audited: int
-    audit_confident: int  # audited rows the surrogate was confident about
-    audit_disagree: int  # ... of which the integrator gave another label
+    """Gate statistics of one pass; the audit tally stays on the device until read."""
+
+    def __init__(self, n: int, n_routed: int, tally: torch.Tensor | None):
+        self.n = n
+        self.n_routed = n_routed
+        self._tally = tally  # int32 (3,): audited, audited-and-confident, ... of which relabelled
+        self._host: list[int] | None = None
+
+    def _read(self) -> list[int]:
+        if self._host is None:
+            self._host = [0, 0, 0] if self._tally is None else [int(v) for v in self._tally.cpu().tolist()]
+        return self._host
+
+    @property
+    def n_audited(self) -> int:
+        return self._read()[0]
+
+    @property
+    def audit_confident(self) -> int:
+        """Audited rows the surrogate was confident about."""
+        return self._read()[1]
+
+    @property
+    def audit_disagree(self) -> int:
+        """... of which the integrator gave another label."""
+        return self._read()[2]
+
+    @property
+    def routed_fraction(self) -> float:
+        return self.n_routed / max(self.n, 1)
+
+    @property
+    def audit_error(self) -> float:
+        return self.audit_disagree / max(self.audit_confident, 1)
 
     @property
     def routed_fraction(self) -> float:
@@ -138,8 +165,9 @@ class SurrogateGatedPipeline:
         label = torch.empty((n,), dtype=torch.int32, device=self.dev)
         route = torch.empty((n,), dtype=torch.int32, device=self.dev)
         n_route = torch.empty((1,), dtype=torch.int32, device=self.dev)
-        L.check(lib.pb_surrogate_gate(_p(logits), n, self.C, self.threshold, _p(audit), _p(label), None, _p(route),
-                                      _p(n_route), s), "pb_surrogate_gate")
+        conf = torch.empty((n,), dtype=torch.float32, device=self.dev)
+        L.check(lib.pb_surrogate_gate(_p(logits), n, self.C, self.threshold, _p(audit), _p(label), _p(conf),
+                                      _p(route), _p(n_route), s), "pb_surrogate_gate")
         k = int(n_route.item())  # the one host read of the pass: how many ICs to integrate
         if k > 0:
             routed = torch.empty((k, self.S), dtype=torch.float32, device=self.dev)
@@ -149,18 +177,14 @@ class SurrogateGatedPipeline:
             sur_of_routed = torch.empty((k,), dtype=torch.int32, device=self.dev)
             L.check(lib.pb_merge_labels(_p(integ), _p(route), _p(n_route), k, _p(label), _p(sur_of_routed), s),
                     "pb_merge_labels")
-            idx = route[:k].long()
-            aud = audit[idx].bool()
-            # audited rows the surrogate was confident about (it would have kept their label)
-            pmax = torch.softmax(logits[idx], dim=1).amax(dim=1)
-            conf_aud = aud & (pmax >= self.threshold)
-            n_conf = int(conf_aud.sum())
-            n_dis = int((conf_aud & (sur_of_routed.long() != integ[:k].long())).sum())
-            n_aud = int(aud.sum())
         else:
-            n_conf = n_dis = n_aud = 0
-        counts = torch.bincount(label.long(), minlength=self.C)
-        return label, counts, GateStats(n, k, n_aud, n_conf, n_dis)
+            integ = sur_of_routed = None
+        counts = torch.empty((self.C,), dtype=torch.int64, device=self.dev)
+        tally = torch.empty((3,), dtype=torch.int32, device=self.dev)
+        L.check(lib.pb_gate_summary(_p(label), n, self.C, _p(route) if k > 0 else None, _p(n_route), k, _p(audit),
+                                    _p(conf), self.threshold, _p(sur_of_routed), _p(integ), _p(counts), _p(tally), s),
+                "pb_gate_summary")
+        return label, counts, GateStats(n, k, tally)
 
     def run(self, y0_host: torch.Tensor) -> tuple[np.ndarray, dict[str, float], GateStats]:
         """Host ICs -> (labels as class names, basin stability per class, gate statistics)."""

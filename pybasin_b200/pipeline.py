@@ -155,7 +155,7 @@ class BasinStabilityPipeline:
         self.pidx[n : n + T] = self.n_groups
         if self.solver.order == "morton" and n > 1:
             grp = self.pidx[:n] if (group is not None and self.n_groups > 1) else None
-            self.order[:n].copy_(self.morton(self.y0_buf[:n], groups=grp))
+            self.morton(self.y0_buf[:n], groups=grp, out=self.order[:n])
         elif self.solver.order == "morton":
             self.order[:n] = torch.arange(n, dtype=torch.int32, device=self.dev)
         self.order[n : n + T] = torch.arange(n, n + T, dtype=torch.int32, device=self.dev)
@@ -190,15 +190,17 @@ class BasinStabilityPipeline:
         L.check(rc, "pb_label_nearest")
 
     def kernel_launches_per_pass(self) -> int:
-        """Launches of this library's kernels per pass: the Z-order keys (bounding box +
-        keys), then integrate (inline), or integrate + sample + redo of record
-        overflows (deferred; the probed schedule integrates in a probe and a main
-        launch, with a library radix sort between them), then labelling."""
+        """Launches of this library's own kernels per pass (CUB radix-sort passes not
+        counted): the Z-order (bounding box, keys, index fill), then integrate
+        (inline), or integrate + sample + redo of record overflows (deferred, with
+        the FP32 split of the save grid in mixed precision; the probed schedule
+        integrates in a probe and a main launch), then labelling."""
         deferred = self.solver.dense_mode == "deferred"
-        n = 2 if self.solver.order == "morton" else 0
+        n = 3 if self.solver.order == "morton" else 0
         if not deferred:
             return n + 2
-        return n + (5 if self.solver.schedule == "probed" else 4)
+        split = 1 if self.solver.precision != "fp64" else 0
+        return n + split + (5 if self.solver.schedule == "probed" else 4)
 
     def load_rows(self, y0: torch.Tensor, group: torch.Tensor | None = None) -> int:
         """Copy device ICs (and their parameter points) into the pipeline, growing it if needed."""

@@ -40,6 +40,7 @@ def _bind(lib: ctypes.CDLL) -> None:
     lib.pb_surrogate_gate.argtypes = [vp, i64, i32, f32, vp, vp, vp, vp, vp, vp]
     lib.pb_gather_rows.argtypes = [vp, i32, vp, vp, i64, vp, vp]
     lib.pb_merge_labels.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    lib.pb_gate_summary.argtypes = [vp, i64, i32, vp, vp, i64, vp, vp, f32, vp, vp, vp, vp, vp]
     lib.pb_mlp_infer_tc.argtypes = [vp, i64, i32, i32, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                     ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, i32, vp, vp]
     for name in (
@@ -54,6 +55,7 @@ def _bind(lib: ctypes.CDLL) -> None:
         "pb_surrogate_gate",
         "pb_gather_rows",
         "pb_merge_labels",
+        "pb_gate_summary",
     ):
         getattr(lib, name).restype = ctypes.c_int
     lib._pb_mlp_bound = True

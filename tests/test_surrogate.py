@@ -155,6 +155,15 @@ def test_gated_pipeline_matches_integrator_labels_on_duffing():
     torch.cuda.synchronize()
     assert stats.n_routed < stats.n  # the surrogate labels part of the ICs
     assert stats.n_audited > 0
+    # the device summary against host arithmetic: counts of the final labels, and
+    # the audit tally (audited rows all routed; confident ones as the gate saw them)
+    assert torch.equal(counts.cpu(), torch.bincount(label.long().cpu(), minlength=6))
+    audit = gated.audit_mask(20000).bool()
+    conf = torch.softmax(gated.net.logits(gated.net.inputs(y0, gated.params)), dim=1).amax(dim=1)
+    assert stats.n_audited == int(audit.sum())
+    confident_audited = audit & (conf >= 0.95)
+    assert abs(stats.audit_confident - int(confident_audited.sum())) <= 2  # FP32 softmax vs the gate's __expf
+    assert stats.audit_disagree <= stats.audit_confident
     dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
     assert float(dbs) <= 0.005
     assert float((label == ref).double().mean()) >= 0.99

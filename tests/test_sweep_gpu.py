@@ -134,3 +134,24 @@ def test_device_morton_keys_match_host_statement(dtype, dim):
     y1 = y0.clone()
     y1[:, 0] = 1.5
     assert torch.equal(mo.keys_of(y1.cuda()).cpu(), morton_keys(y1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_device_order_is_the_stable_argsort_of_the_keys(dim):
+    """pb_morton_order (radix sort over the key bits in use) against torch's stable
+    argsort of the same keys, with and without groups, duplicate keys included."""
+    from pybasin_b200.engine import MortonOrder
+
+    g = torch.Generator().manual_seed(7 + dim)
+    y0 = torch.rand(30_001, dim, generator=g) * 4.0 - 2.0
+    y0[1000:1100] = y0[5]  # equal keys keep their index order
+    groups = torch.randint(0, 5, (30_001,), generator=g, dtype=torch.int32)
+    mo = MortonOrder(torch.device("cuda:0"))
+    for grp in (None, groups.cuda()):
+        keys = mo.keys_of(y0.cuda(), groups=grp).clone()
+        want = torch.argsort(keys, stable=True).to(torch.int32)
+        got = mo(y0.cuda(), groups=grp)
+        assert torch.equal(got, want)
+    out = torch.full((30_001,), -1, dtype=torch.int32, device="cuda:0")
+    assert mo(y0.cuda(), out=out) is out and torch.equal(out, torch.argsort(mo.keys_of(y0.cuda()).clone(), stable=True).to(torch.int32))
