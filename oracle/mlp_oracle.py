@@ -2,23 +2,26 @@
 
 TEST INFRASTRUCTURE ONLY: the checker for the BF16 tensor-core kernels of
 pybasin_b200/csrc/pb_mlp.cu (tests/test_surrogate.py).  Layers: h = GELU(x W^T + b)
-for the hidden layers (exact erf GELU), logits = h W^T + b for the last one.
+for the hidden layers (GELU in its tanh form, evaluated exactly in FP64),
+logits = h W^T + b for the last one.
 """
 
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
+
+_A = np.sqrt(2.0 / np.pi)
+_B = 0.044715
 
 
 def gelu(z: np.ndarray) -> np.ndarray:
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(_A * (z + _B * z**3)))
 
 
 def gelu_grad(z: np.ndarray) -> np.ndarray:
-    cdf = 0.5 * (1.0 + erf(z / np.sqrt(2.0)))
-    pdf = np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
-    return cdf + z * pdf
+    t = np.tanh(_A * (z + _B * z**3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _A * (1.0 + 3.0 * _B * z * z)
 
 
 def forward(x: np.ndarray, Ws: list[np.ndarray], bs: list[np.ndarray]):

@@ -16,6 +16,7 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include "pb_gelu.cuh"
 #include "pybasin_b200.h"
 
 namespace {
@@ -31,13 +32,8 @@ __device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const uint32_t (&a
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float x)
-{
-    const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
-    return cdf + x * pdf;
-}
+using pb::gelu;
+using pb::gelu_grad;
 
 template <int EPI>  // 0: none, 1: GELU
 __global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16* __restrict__ A, int64_t sam, int64_t sak,

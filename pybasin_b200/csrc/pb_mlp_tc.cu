@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pb_gelu.cuh"
 #include "pybasin_b200.h"
 
 namespace {
@@ -159,7 +160,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+using pb::gelu;
 
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_infer_tc(const MlpTcArgs p)
 {

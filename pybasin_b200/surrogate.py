@@ -1,6 +1,6 @@
 """Learned surrogate: an MLP from (initial condition, parameters) to attractor classes.
 
-The network (inputs -> 4 hidden layers of 256 with GELU -> class logits) is
+The network (inputs -> 4 hidden layers of 256 with GELU, tanh form -> class logits) is
 trained on labels produced by the integrator itself, with this library's BF16
 tensor-core GEMMs (FP32 accumulation), softmax cross-entropy, GELU backward and
 AdamW kernels; FP32 master weights, BF16 copies for the GEMMs.  At inference,
