@@ -123,8 +123,10 @@ class ClockSampler:
 
         def __enter__(self):
             self.t0 = time.monotonic()
+            torch.cuda.nvtx.range_push("timed")  # the launch list filters on this range
 
         def __exit__(self, *exc):
+            torch.cuda.nvtx.range_pop()
             self.owner.windows.append((self.t0, time.monotonic()))
 
     def timed(self):
@@ -520,10 +522,14 @@ def run_b200_arm(args) -> None:
                 "peak": peak32 / 1e12,
                 "unit": "TFLOP/s",
                 "frac": achieved / peak32,
-                "traffic": 0.8132e9 * (n + len(DUFFING["templates"])) / 50005,
+                "traffic": 1.6934e9 * (n + len(DUFFING["templates"])) / 50005,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel "
                                   "(main phase of the probed integrator) at N=50,000, scaled by trajectories "
-                                  "(profiles/k_solve_queue_probed_duffing50k.md): the window's step records",
+                                  "(profiles/k_solve_queue_probed_duffing50k.md): the window's step records, "
+                                  "written by the integrating lanes and read back by the warps that drain "
+                                  "the sampling into the same launch",
+                "note": "achieved counts the integration FLOPs only; the dominant kernel's time also holds "
+                        "the window sampling drained into it",
                 "peak_source": "FP32 FMA probe kernel measured in this run (MEASURED_PEAKS.json holds only the "
                                "HBM-copy and bf16-GEMM peaks, neither bounds this kernel)",
                 "fp64_fma_peak": peak64 / 1e12,
