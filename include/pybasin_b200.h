@@ -370,7 +370,8 @@ int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream);
  * params[:n_params]) - shift] * scale (d = S + n_params columns), then, for the
  * n_freq rows f of freq (n_freq x d, cycles per unit of z), sin(2 pi f.z) for
  * every f and cos(2 pi f.z) for every f (random Fourier features; n_freq = 0
- * and freq = NULL for z alone).  d + 2 n_freq <= d_pad. */
+ * and freq = NULL for z alone).  d = S + n_params <= 16, n_freq <= 128,
+ * d + 2 n_freq <= d_pad. */
 int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
                         const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
                         void* out_bf16, void* stream);

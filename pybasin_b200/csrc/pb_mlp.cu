@@ -202,43 +202,50 @@ __global__ void k_cast_bf16(const float* __restrict__ x, __nv_bfloat16* __restri
 // [z, sin, cos] (n x d_pad, zero padded).
 constexpr int kMaxRawInputs = 16;
 
-// One thread per (row, frequency): the row's d z-scored columns in registers (d
-// cached loads), the frequency's sine-cosine pair, and every U-th z or padding
-// column from its own index on; neighbouring threads write neighbouring columns.
-__global__ void k_features_in(const float* __restrict__ ic, int S, const double* __restrict__ prm, int np,
-                              const float* __restrict__ shift, const float* __restrict__ scale,
-                              const float* __restrict__ freq, int n_freq, int64_t n, int d_pad,
-                              __nv_bfloat16* __restrict__ out)
+// A block takes R = 256 / U rows at a time (U = max(n_freq, 1) threads per row):
+// the frequencies and the rows' z-scored columns are staged in shared memory, then
+// thread (r, j) writes frequency j's sine-cosine pair of row r and every U-th z or
+// padding column from j on, so neighbouring threads write neighbouring columns.
+// Dynamic shared memory: (n_freq + R) * d floats.
+__global__ void __launch_bounds__(256) k_features_in(const float* __restrict__ ic, int S,
+                                                     const double* __restrict__ prm, int np,
+                                                     const float* __restrict__ shift,
+                                                     const float* __restrict__ scale,
+                                                     const float* __restrict__ freq, int n_freq, int64_t n,
+                                                     int d_pad, __nv_bfloat16* __restrict__ out)
 {
+    extern __shared__ float fsm[];
     const int d = S + np;
     const int U = n_freq > 0 ? n_freq : 1;
+    const int R = 256 / U;
+    float* f_s = fsm;               // n_freq x d
+    float* z_s = fsm + n_freq * d;  // R x d
+    for (int i = threadIdx.x; i < n_freq * d; i += blockDim.x) f_s[i] = freq[i];
     const int n_zero = d_pad - d - 2 * n_freq;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * U; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = t / U;
-        const int j = static_cast<int>(t - r * U);
-        __nv_bfloat16* o = out + r * d_pad;
-        float z[kMaxRawInputs];
-#pragma unroll
-        for (int c = 0; c < kMaxRawInputs; ++c) {
-            z[c] = 0.f;
-            if (c < d) {
-                const float v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
-                z[c] = (v - shift[c]) * scale[c];
-            }
+    const int r_loc = threadIdx.x / U, j = threadIdx.x - r_loc * U;
+    for (int64_t r0 = static_cast<int64_t>(blockIdx.x) * R; r0 < n; r0 += static_cast<int64_t>(gridDim.x) * R) {
+        __syncthreads();  // the previous rows' z are consumed
+        for (int i = threadIdx.x; i < R * d; i += blockDim.x) {
+            const int rr = i / d, c = i - rr * d;
+            const int64_t r = r0 + rr;
+            float v = 0.f;
+            if (r < n) v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
+            z_s[i] = (v - shift[c]) * scale[c];
         }
+        __syncthreads();
+        const int64_t r = r0 + r_loc;
+        if (r_loc >= R || r >= n) continue;
+        const float* z = z_s + r_loc * d;
+        __nv_bfloat16* o = out + r * d_pad;
         if (n_freq > 0) {
             float turns = 0.f;
-#pragma unroll
-            for (int c = 0; c < kMaxRawInputs; ++c)
-                if (c < d) turns = fmaf(freq[j * d + c], z[c], turns);
+            for (int c = 0; c < d; ++c) turns = fmaf(f_s[j * d + c], z[c], turns);
             float sn, cs;
             sincospif(2.f * turns, &sn, &cs);
             o[d + j] = __float2bfloat16(sn);
             o[d + n_freq + j] = __float2bfloat16(cs);
         }
-#pragma unroll
-        for (int c = 0; c < kMaxRawInputs; ++c)
-            if (c < d && c % U == j) o[c] = __float2bfloat16(z[c]);
+        for (int c = j; c < d; c += U) o[c] = __float2bfloat16(z[c]);
         for (int c = j; c < n_zero; c += U) o[d + 2 * n_freq + c] = __float2bfloat16(0.f);
     }
 }
@@ -428,7 +435,10 @@ int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_
         return PB_EINVAL;
     if ((n_params > 0 && !params) || (n_freq > 0 && !freq)) return PB_EINVAL;
     if (n == 0) return PB_SUCCESS;
-    k_features_in<<<grid_for(n * (n_freq > 0 ? n_freq : 1), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    if (n_freq > 128) return PB_EINVAL;  // at least two rows per 256-thread block
+    const int U = n_freq > 0 ? n_freq : 1, R = 256 / U;
+    const size_t fsmem = static_cast<size_t>(n_freq + R) * (S + n_params) * sizeof(float);
+    k_features_in<<<grid_for((n + R - 1) / R, 1), 256, fsmem, static_cast<cudaStream_t>(stream)>>>(
         ic, S, params, n_params, shift, scale, freq, n_freq, n, d_pad, static_cast<__nv_bfloat16*>(out_bf16));
     return map_err(cudaGetLastError());
 }
