@@ -485,12 +485,15 @@ def test_orbit_data_peaks_match_oracle_trajectories():
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
 @pytest.mark.parametrize("feats", [[(0, L.FEAT_MAX, 0.0), (0, L.FEAT_STD, 0.0)],
-                                   [(0, L.FEAT_MEAN, 0.0), (1, L.FEAT_LOG_DELTA, 0.0), (1, L.FEAT_LAST, 0.0)]],
-                         ids=["one_state", "two_states"])
+                                   [(0, L.FEAT_MEAN, 0.0), (1, L.FEAT_LOG_DELTA, 0.0), (1, L.FEAT_LAST, 0.0)],
+                                   [(0, L.FEAT_CROSSINGS, 0.0), (0, L.FEAT_MAX, 0.0)]],
+                         ids=["one_state", "two_states", "crossings"])
 def test_features_are_bit_identical_across_schedules(feats, precision):
     """Plain, queue and probed schedules write the same step records (explicit FMAs,
-    same step sequence) and the sampling pass reduces them the same way: the
-    features are bit-identical whichever schedule ran."""
+    same step sequence) and sampling reduces them the same way: the features are
+    bit-identical whichever schedule ran.  With one or two feature states and no
+    crossing counts the probed main phase samples finished trajectories itself
+    (drained sampling); with crossings the sampling pass after it does."""
     case = DUFFING
     y0 = seeded_ics(case, 3000, 17).double().numpy()
     save = case.save_ts().numpy()
