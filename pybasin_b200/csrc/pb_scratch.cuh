@@ -5,14 +5,16 @@
 //   [tails]           n_traj x tail_stride bytes                (PB_DENSE_DEFERRED)
 //   [split save grid] n_save x (float hi, float lo)            (PB_DENSE_DEFERRED)
 //   [saved states]    n_traj x state_stride bytes               (PB_SCHED_PROBED)
-//   [sort keys/values] 4 x n_traj int32, then the radix-sort temporary storage
-//                     (PB_SCHED_PROBED; the temporary's size is added on the host)
+//   [sort keys/values] 4 x n_traj int32                         (PB_SCHED_PROBED)
+//   [drain]           2 x u64 counters, n_traj int32 published ids, n_traj u8
+//                     sampled flags                              (PB_SCHED_PROBED)
+//   [radix-sort temporary storage]                               (PB_SCHED_PROBED; its
+//                     size is added on the host)
 //
 // Each part starts on a 256-byte boundary.  A step record (a multiple of 16 bytes,
 // written with 16-byte stores) is
-//   double t, double 1/dt,
-//   for each statistics state: y, h*k1, c, b, a   (stage precision),
-//   int32 first_save, int32 n_saves, padding
+//   double t, double dt, int32 first_save, int32 n_saves,
+//   for each statistics state: y, h*k1, c, b, a   (stage precision), padding
 // and a tail is
 //   int32 n_records (-1 = capacity exceeded), int32 next_save, int32 status, int32 pad,
 //   double fill[dim]   (value of the save points after the last record)
