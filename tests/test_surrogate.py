@@ -269,3 +269,29 @@ def test_folded_temperature_divides_the_logits():
     torch.cuda.synchronize()
     scale = before.abs().max().item()
     assert (after - before / 2.0).abs().max().item() <= 1e-2 * scale
+
+
+@pytest.mark.gpu
+def test_gate_summary_counts_without_routed_rows():
+    """pb_gate_summary with no routed rows: class counts of the labels, a zero tally."""
+    from pybasin_b200 import _lib as L
+    from pybasin_b200.surrogate import _bind, _p
+
+    lib = L.load()
+    _bind(lib)
+    dev = torch.device("cuda:0")
+    g = torch.Generator().manual_seed(4)
+    label = torch.randint(0, 6, (50_001,), generator=g, dtype=torch.int32).to(dev)
+    counts = torch.full((6,), -1, dtype=torch.int64, device=dev)
+    tally = torch.full((3,), -1, dtype=torch.int32, device=dev)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    assert lib.pb_gate_summary(_p(label), 50_001, 6, None, None, 0, None, None, 0.95, None, None, _p(counts),
+                               _p(tally), s) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(counts.cpu(), torch.bincount(label.long().cpu(), minlength=6))
+    assert tally.cpu().tolist() == [0, 0, 0]
+    # invalid: more than 64 classes, or a route without its count
+    assert lib.pb_gate_summary(_p(label), 10, 65, None, None, 0, None, None, 0.95, None, None, _p(counts),
+                               _p(tally), s) != 0
+    assert lib.pb_gate_summary(_p(label), 10, 6, _p(label), None, 10, None, None, 0.95, None, None, _p(counts),
+                               _p(tally), s) != 0

@@ -155,3 +155,15 @@ def test_device_order_is_the_stable_argsort_of_the_keys(dim):
         assert torch.equal(got, want)
     out = torch.full((30_001,), -1, dtype=torch.int32, device="cuda:0")
     assert mo(y0.cuda(), out=out) is out and torch.equal(out, torch.argsort(mo.keys_of(y0.cuda()).clone(), stable=True).to(torch.int32))
+
+
+@pytest.mark.gpu
+def test_device_order_of_tiny_and_empty_inputs():
+    from pybasin_b200.engine import MortonOrder
+
+    mo = MortonOrder(torch.device("cuda:0"))
+    assert mo(torch.zeros((0, 2), device="cuda:0")).numel() == 0
+    one = mo(torch.tensor([[0.5, -0.25]], device="cuda:0"))
+    assert one.tolist() == [0]
+    same = mo(torch.ones((5, 3), device="cuda:0"))  # equal keys: the identity, in index order
+    assert same.tolist() == [0, 1, 2, 3, 4]
