@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from pybasin_b200 import _lib as L
-from pybasin_b200.pipeline import BasinStabilityPipeline
+from pybasin_b200.pipeline import BasinStabilityPipeline, to_host_pinned
 from pybasin_b200.surrogate import MLPSurrogate, TrainHistory, _bind, _p
 
 
@@ -191,8 +191,7 @@ class SurrogateGatedPipeline:
         with torch.cuda.device(self.dev):
             y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
             label, counts, stats = self.run_device(y0)
-            lab = label.cpu().numpy()
-            cnt = counts.cpu().numpy()
+            lab, cnt = to_host_pinned(self, label, counts)
         names = np.array(self.pipe.classes + ["unbounded"], dtype=object)
         n = max(int(cnt.sum()), 1)
         bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}

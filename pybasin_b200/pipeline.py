@@ -26,6 +26,23 @@ from pybasin_b200.odes import resolve_system
 from pybasin_b200.solver import B200Dopri5Solver
 
 
+def to_host_pinned(owner, label: torch.Tensor, counts: torch.Tensor) -> tuple[np.ndarray, np.ndarray]:
+    """Labels and counts into page-locked host buffers kept on ``owner`` (grown as
+    needed): two asynchronous copies and one stream synchronisation.  The arrays
+    returned are views of those buffers, valid until the owner's next call."""
+    n, c = label.numel(), counts.numel()
+    buf = getattr(owner, "_host_out", None)
+    if buf is None or buf[0].numel() < n or buf[1].numel() < c:
+        buf = (torch.empty((max(n, 1),), dtype=label.dtype, pin_memory=True),
+               torch.empty((max(c, 1),), dtype=counts.dtype, pin_memory=True))
+        owner._host_out = buf
+    hl, hc = buf[0][:n], buf[1][:c]
+    hl.copy_(label.view(-1), non_blocking=True)
+    hc.copy_(counts.view(-1), non_blocking=True)
+    torch.cuda.current_stream(label.device).synchronize()
+    return hl.numpy(), hc.numpy()
+
+
 class BasinStabilityPipeline:
     """Labelled ICs for one ODE system and template set on one GPU.
 
@@ -250,8 +267,8 @@ class BasinStabilityPipeline:
         with torch.cuda.device(self.dev):
             y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
             labels, counts = self.run_device(y0, use_graph=use_graph)
-            lab = labels.cpu().numpy()
-            cnt = counts.cpu().numpy()[0]
+            lab, cnt_all = to_host_pinned(self, labels, counts)
+            cnt = cnt_all.reshape(counts.shape)[0]
         names = np.array(self.classes + ["unbounded"], dtype=object)
         n = max(int(cnt.sum()), 1)
         bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}
