@@ -414,7 +414,10 @@ def run_b200_arm(args) -> None:
 
     # end to end through the public API: pinned host ICs in, labels out
     y0_pinned = y0_host.pin_memory()
-    run_e2e = (lambda: gated.run(y0_pinned)) if use_gate else (lambda: pipe.run(y0_pinned, use_graph=True))
+    # labels out as class indices (the class list alongside), the form a high-rate
+    # caller takes; run(..., names=True) adds one string object per IC on the host
+    run_e2e = ((lambda: gated.run(y0_pinned, names=False)) if use_gate
+               else (lambda: pipe.run(y0_pinned, use_graph=True, names=False)))
     for _ in range(2):
         run_e2e()
     torch.cuda.synchronize()
@@ -513,6 +516,7 @@ def run_b200_arm(args) -> None:
                 "unit": "ICs/s",
                 "h2d_bytes_per_step": int(y0_host.numel() * 4),
                 "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8),
+                "labels": "int32 class indices per IC and the per-class counts, in host memory",
             },
             # gated: input features, tensor-core MLP, gate, gather, merge, summary
             "gpu_launches": (pipe.kernel_launches_per_pass() + (6 if use_gate else 0)) * args.steps,

@@ -186,13 +186,15 @@ class SurrogateGatedPipeline:
                 "pb_gate_summary")
         return label, counts, GateStats(n, k, tally)
 
-    def run(self, y0_host: torch.Tensor) -> tuple[np.ndarray, dict[str, float], GateStats]:
-        """Host ICs -> (labels as class names, basin stability per class, gate statistics)."""
+    def run(self, y0_host: torch.Tensor, names: bool = True) -> tuple[np.ndarray, dict[str, float], GateStats]:
+        """Host ICs -> (labels, basin stability per class, gate statistics); labels as
+        class names, or with ``names=False`` as int32 indices into
+        ``pipe.classes + ["unbounded"]`` (no per-IC string objects to build)."""
         with torch.cuda.device(self.dev):
             y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
             label, counts, stats = self.run_device(y0)
             lab, cnt = to_host_pinned(self, label, counts)
-        names = np.array(self.pipe.classes + ["unbounded"], dtype=object)
+        classes = np.array(self.pipe.classes + ["unbounded"], dtype=object)
         n = max(int(cnt.sum()), 1)
-        bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}
-        return names[lab], bs, stats
+        bs = {classes[i]: float(cnt[i]) / n for i in range(len(classes)) if cnt[i] > 0}
+        return (classes[lab] if names else lab.copy()), bs, stats

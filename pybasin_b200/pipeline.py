@@ -262,14 +262,16 @@ class BasinStabilityPipeline:
         torch.cuda.current_stream(self.dev).wait_stream(s)
         self._graph = g
 
-    def run(self, y0_host: torch.Tensor, use_graph: bool = False) -> tuple[np.ndarray, dict[str, float]]:
-        """Host ICs -> (labels as class names, basin stability per class)."""
+    def run(self, y0_host: torch.Tensor, use_graph: bool = False, names: bool = True
+            ) -> tuple[np.ndarray, dict[str, float]]:
+        """Host ICs -> (labels, basin stability per class); labels as class names, or
+        with ``names=False`` as int32 indices into ``classes + ["unbounded"]``."""
         with torch.cuda.device(self.dev):
             y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
             labels, counts = self.run_device(y0, use_graph=use_graph)
             lab, cnt_all = to_host_pinned(self, labels, counts)
             cnt = cnt_all.reshape(counts.shape)[0]
-        names = np.array(self.classes + ["unbounded"], dtype=object)
+        classes = np.array(self.classes + ["unbounded"], dtype=object)
         n = max(int(cnt.sum()), 1)
-        bs = {names[i]: float(cnt[i]) / n for i in range(len(names)) if cnt[i] > 0}
-        return names[lab], bs
+        bs = {classes[i]: float(cnt[i]) / n for i in range(len(classes)) if cnt[i] > 0}
+        return (classes[lab] if names else lab.copy()), bs
