@@ -164,6 +164,12 @@ def test_gated_pipeline_matches_integrator_labels_on_duffing():
     confident_audited = audit & (conf >= 0.95)
     assert abs(stats.audit_confident - int(confident_audited.sum())) <= 2  # FP32 softmax vs the gate's __expf
     assert stats.audit_disagree <= stats.audit_confident
+    # host API: class names, or the same labels as indices into the class list
+    lab_names, bs, _ = gated.run(y0.cpu())
+    lab_idx, bs_idx, _ = gated.run(y0.cpu(), names=False)
+    classes = np.array(pipe.classes + ["unbounded"], dtype=object)
+    assert lab_idx.dtype == np.int32 and (classes[lab_idx] == lab_names).all()
+    assert bs == bs_idx and abs(sum(bs.values()) - 1.0) < 1e-12
     dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
     assert float(dbs) <= 0.005
     assert float((label == ref).double().mean()) >= 0.99
