@@ -4,7 +4,7 @@
 //
 // The surrogate maps (initial condition, parameters) to attractor-class
 // probabilities; it is trained on labels the integrator itself produced.  It
-// has no counterpart in the reference (BASELINE's learned component).
+// has no counterpart in the reference.
 //
 // GEMM: C[m,n] = alpha * sum_k A(m,k) B(k,n) (+ bias[n]) with an optional GELU,
 // A and B addressed through arbitrary element strides so the same kernel serves
