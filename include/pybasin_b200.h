@@ -39,7 +39,7 @@ typedef enum {
     PB_ESOLVE = -3,         /* kernel launch or execution error */
     PB_EINVAL = -5,         /* invalid argument (null pointer, bad size, bad layout) */
     PB_ECUDA = -6,          /* other CUDA runtime error */
-    PB_EUNSUPPORTED = -7,   /* valid request this build does not support */
+    PB_EUNSUPPORTED = -7,   /* valid request the library does not support (e.g. a kernel variant not compiled in) */
     PB_ECOMPILE = -8,       /* runtime (NVRTC) compilation of a user right-hand side failed */
     PB_ESCRATCH_LIMIT = -9  /* pb_solve_batch_noalloc: request needs more than PB_NOALLOC_SCRATCH_BYTES */
 } pb_status;
