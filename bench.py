@@ -238,6 +238,46 @@ def run_reference_arm(args) -> None:
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def bf16_peak() -> tuple[float, str]:
+    """Dense bf16 peak (FLOP/s) for the surrogate's roofline: MEASURED_PEAKS.json's
+    burst figure when the file is there, else the 1.59 PFLOP/s fallback measured
+    earlier on this pool's B200s."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        for key in ("bf16_tflops", "bf16_dense_tflops"):
+            if key in d:
+                return float(d[key]) * 1e12, f"MEASURED_PEAKS.json {key} (measured)"
+    except (OSError, ValueError):
+        pass
+    return 1.59e15, "fallback 1.59 PFLOP/s (MEASURED_PEAKS.json absent)"
+
+
+def mlp_roofline(gated, y0_dev: torch.Tensor) -> dict:
+    """Algorithmic FLOPs of the surrogate network per row (2 K N per layer, real
+    widths) x rows / CUDA-event time of the tensor-core inference kernel."""
+    net = gated.net
+    x = net.inputs(y0_dev, gated.params)
+    for _ in range(3):
+        net.logits(x)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        net.logits(x)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = statistics.median(ts)
+    flop_row = 2 * sum(int(w.shape[0]) * int(w.shape[1]) for w in net.W)
+    achieved = flop_row * x.shape[0] / (ms / 1000.0)
+    peak, src = bf16_peak()
+    return {"bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+            "frac": achieved / peak, "kernel_ms": ms, "flop_per_row": flop_row, "peak_source": src}
+
+
 def make_pipeline(dev: torch.device, precision: str, schedule: str):
     from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
     from pybasin_b200.pipeline import BasinStabilityPipeline
@@ -407,6 +447,7 @@ def run_b200_arm(args) -> None:
         dbs_g = (counts_g[:5].double() - counts64[:5].double()).abs().max().item() / n_all
         agree_g = float((lab_g == labels64).float().mean())
         value_gated = n_all / (ms_g / 1000.0)
+        mlp_roof = mlp_roofline(gated, y0_dev)
 
     use_gate = gated is not None and dbs_g <= 0.005 and value_gated > value_fused
     value = value_gated if use_gate else value_fused
@@ -497,6 +538,7 @@ def run_b200_arm(args) -> None:
                 "audited": g_stats[-1].n_audited,
                 "audit_error_of_confident_labels": g_stats[-1].audit_error,
                 "threshold": 0.95,
+                "mlp_roofline": mlp_roof,
                 "net": ("MLP (z-scored IC and params, sin/cos of 64 random Fourier projections) -> 4 x 256 GELU "
                         "-> 6 logits; inference on tcgen05 (TMEM accumulators), training on BF16 mma.sync, "
                         "FP32 accumulate; softmax temperature fitted on held-out labels"),
@@ -534,8 +576,9 @@ def run_b200_arm(args) -> None:
                                   "the sampling into the same launch",
                 "note": "achieved counts the integration FLOPs only; the dominant kernel's time also holds "
                         "the window sampling drained into it",
-                "peak_source": "FP32 FMA probe kernel measured in this run (MEASURED_PEAKS.json holds only the "
-                               "HBM-copy and bf16-GEMM peaks, neither bounds this kernel)",
+                "peak_source": "FP32 FMA probe kernel measured in this run (the measured-peaks file, when "
+                               "present, holds only HBM-copy and bf16-GEMM peaks, neither of which bounds "
+                               "this kernel)",
                 "fp64_fma_peak": peak64 / 1e12,
                 "kernel_ms": kms,
                 "mean_steps_per_ic": mean_steps,
