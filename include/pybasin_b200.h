@@ -95,11 +95,24 @@ typedef enum {
     PB_FEAT_MEAN_ABS_CHANGE = 22, PB_FEAT_MEAN_CHANGE = 23, PB_FEAT_MEAN_SECOND_DERIV = 24,
     PB_FEAT_COUNT_ABOVE_MEAN = 25, PB_FEAT_COUNT_BELOW_MEAN = 26, PB_FEAT_COUNT_ABOVE = 27,
     PB_FEAT_COUNT_BELOW = 28, PB_FEAT_NUMBER_PEAKS = 29, PB_FEAT_AUTOCORRELATION = 30,
-    PB_FEAT_RATIO_BEYOND_R_SIGMA = 31
+    PB_FEAT_RATIO_BEYOND_R_SIGMA = 31,
+    /* fft_coefficient (coeff = feat_param; the attribute in the kind: real, imag,
+       abs, angle; torch_features_frequency.py:11-29), linear_trend (the attribute
+       in the kind; torch_features_trend.py:11-51), first/last location of the
+       maximum/minimum (torch_features_location.py:11-49), cid_ce (normalize =
+       feat_param 0/1; torch_features_entropy_complexity.py:182-190), c3 (lag) and
+       time_reversal_asymmetry_statistic (lag) (torch_features_advanced.py:84-90,
+       109-118) */
+    PB_FEAT_FFT_REAL = 32, PB_FEAT_FFT_IMAG = 33, PB_FEAT_FFT_ABS = 34, PB_FEAT_FFT_ANGLE = 35,
+    PB_FEAT_TREND_SLOPE = 36, PB_FEAT_TREND_INTERCEPT = 37, PB_FEAT_TREND_RVALUE = 38,
+    PB_FEAT_TREND_PVALUE = 39, PB_FEAT_TREND_STDERR = 40,
+    PB_FEAT_FIRST_LOC_MAX = 41, PB_FEAT_FIRST_LOC_MIN = 42, PB_FEAT_LAST_LOC_MAX = 43,
+    PB_FEAT_LAST_LOC_MIN = 44, PB_FEAT_CID_CE = 45, PB_FEAT_C3 = 46, PB_FEAT_TIME_REVERSAL = 47
 } pb_feature;
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..31): the
+#define PB_FEAT_LAST_KIND PB_FEAT_TIME_REVERSAL
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..47): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
-#define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_RATIO_BEYOND_R_SIGMA))
+#define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 
 /* ---- per-trajectory status written to status_out ---- */
 typedef enum {

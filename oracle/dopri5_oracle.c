@@ -253,6 +253,75 @@ static double window_feature(int feat, double param, const double *w, int n, dou
         for (int i = 0; i < n; ++i) c += fabs(w[i] - mean) > param * sd;
         return c / n;
     }
+    /* torch_features_frequency.py:11-29: coefficient k of torch.fft.rfft, a direct
+       DFT sum with the phase k*i/n reduced in integers */
+    case ORACLE_F_FFT_REAL: case ORACLE_F_FFT_IMAG: case ORACLE_F_FFT_ABS: case ORACLE_F_FFT_ANGLE: {
+        const long k = (long)param;
+        if (k > n / 2) return 0.0;
+        double re = 0.0, im = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double ang = 6.283185307179586476925286766559 * (double)((k * i) % n) / n;
+            re += w[i] * cos(ang);
+            im -= w[i] * sin(ang);
+        }
+        if (feat == ORACLE_F_FFT_REAL) return re;
+        if (feat == ORACLE_F_FFT_IMAG) return im;
+        if (feat == ORACLE_F_FFT_ABS) return sqrt(re * re + im * im);
+        return atan2(im, re);
+    }
+    /* torch_features_trend.py:11-51 (with its pseudo p-value 1 / (1 + |t|)) */
+    case ORACLE_F_TREND_SLOPE: case ORACLE_F_TREND_INTERCEPT: case ORACLE_F_TREND_RVALUE:
+    case ORACLE_F_TREND_PVALUE: case ORACLE_F_TREND_STDERR: {
+        const double tm = 0.5 * (n - 1.0);
+        double ss_tt = 0.0, ss_tx = 0.0;
+        for (int i = 0; i < n; ++i) {
+            ss_tt += (i - tm) * (i - tm);
+            ss_tx += (i - tm) * (w[i] - mean);
+        }
+        const double slope = ss_tx / (ss_tt + 1e-10), intercept = mean - slope * tm;
+        const double r = ss_tx / (sqrt(ss_tt * m2) + 1e-10);
+        if (feat == ORACLE_F_TREND_SLOPE) return slope;
+        if (feat == ORACLE_F_TREND_INTERCEPT) return intercept;
+        if (feat == ORACLE_F_TREND_RVALUE) return r;
+        if (feat == ORACLE_F_TREND_PVALUE) return 1.0 / (1.0 + fabs(r * sqrt(n - 2.0) / (sqrt(1.0 - r * r) + 1e-10)));
+        double rss = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double e = w[i] - (slope * i + intercept);
+            rss += e * e;
+        }
+        return sqrt(rss / (n - 2.0) / (ss_tt + 1e-10));
+    }
+    /* torch_features_location.py:11-49: index of the first (last) extreme / n */
+    case ORACLE_F_FIRST_LOC_MAX: case ORACLE_F_FIRST_LOC_MIN: case ORACLE_F_LAST_LOC_MAX:
+    case ORACLE_F_LAST_LOC_MIN: {
+        if (any_nan) return NAN;
+        const int want_max = feat == ORACLE_F_FIRST_LOC_MAX || feat == ORACLE_F_LAST_LOC_MAX;
+        const int last = feat == ORACLE_F_LAST_LOC_MAX || feat == ORACLE_F_LAST_LOC_MIN;
+        const double target = want_max ? mx : mn;
+        int idx = -1;
+        for (int i = 0; i < n; ++i)
+            if (w[i] == target && (idx < 0 || last)) idx = i;
+        return (double)idx / n;
+    }
+    /* torch_features_entropy_complexity.py:182-190 */
+    case ORACLE_F_CID_CE: {
+        double ce = 0.0;
+        for (int i = 1; i < n; ++i) ce += (w[i] - w[i - 1]) * (w[i] - w[i - 1]);
+        ce = sqrt(ce);
+        return param != 0.0 ? ce / (sqrt(m2 / n) + 1e-10) : ce;
+    }
+    /* torch_features_advanced.py:84-90, 109-118 */
+    case ORACLE_F_C3: case ORACLE_F_TIME_REVERSAL: {
+        const int lag = (int)param;
+        if (2 * lag >= n) return 0.0;
+        const int m = n - 2 * lag;
+        double a = 0.0;
+        for (int i = 0; i < m; ++i) {
+            const double x0 = w[i], x1 = w[i + lag], x2 = w[i + 2 * lag];
+            a += feat == ORACLE_F_C3 ? x0 * x1 * x2 : x2 * x2 * x1 - x1 * x0 * x0;
+        }
+        return a / m;
+    }
     default: return NAN;
     }
 }

@@ -25,6 +25,14 @@ enum {
     ORACLE_F_COUNT_ABOVE_MEAN = 25, ORACLE_F_COUNT_BELOW_MEAN = 26, ORACLE_F_COUNT_ABOVE = 27,
     ORACLE_F_COUNT_BELOW = 28, ORACLE_F_NUMBER_PEAKS = 29, ORACLE_F_AUTOCORRELATION = 30,
     ORACLE_F_RATIO_BEYOND_R_SIGMA = 31,
+    /* fft_coefficient real/imag/abs/angle (coeff), linear_trend slope/intercept/
+       rvalue/pvalue/stderr, first/last location of max/min, cid_ce (normalize),
+       c3 (lag), time_reversal_asymmetry_statistic (lag) */
+    ORACLE_F_FFT_REAL = 32, ORACLE_F_FFT_IMAG = 33, ORACLE_F_FFT_ABS = 34, ORACLE_F_FFT_ANGLE = 35,
+    ORACLE_F_TREND_SLOPE = 36, ORACLE_F_TREND_INTERCEPT = 37, ORACLE_F_TREND_RVALUE = 38,
+    ORACLE_F_TREND_PVALUE = 39, ORACLE_F_TREND_STDERR = 40,
+    ORACLE_F_FIRST_LOC_MAX = 41, ORACLE_F_FIRST_LOC_MIN = 42, ORACLE_F_LAST_LOC_MAX = 43,
+    ORACLE_F_LAST_LOC_MIN = 44, ORACLE_F_CID_CE = 45, ORACLE_F_C3 = 46, ORACLE_F_TIME_REVERSAL = 47,
 };
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };

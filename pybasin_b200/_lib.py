@@ -84,6 +84,10 @@ FEAT_COUNT_BELOW = 28
 FEAT_NUMBER_PEAKS = 29
 FEAT_AUTOCORRELATION = 30
 FEAT_RATIO_BEYOND_R_SIGMA = 31
+FEAT_FFT_REAL, FEAT_FFT_IMAG, FEAT_FFT_ABS, FEAT_FFT_ANGLE = 32, 33, 34, 35
+FEAT_TREND_SLOPE, FEAT_TREND_INTERCEPT, FEAT_TREND_RVALUE, FEAT_TREND_PVALUE, FEAT_TREND_STDERR = 36, 37, 38, 39, 40
+FEAT_FIRST_LOC_MAX, FEAT_FIRST_LOC_MIN, FEAT_LAST_LOC_MAX, FEAT_LAST_LOC_MIN = 41, 42, 43, 44
+FEAT_CID_CE, FEAT_C3, FEAT_TIME_REVERSAL = 45, 46, 47
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

@@ -218,6 +218,127 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = static_cast<double>(count);
                 break;
             }
+            case PB_FEAT_FFT_REAL:
+            case PB_FEAT_FFT_IMAG:
+            case PB_FEAT_FFT_ABS:
+            case PB_FEAT_FFT_ANGLE: {  // coefficient k of the one-sided DFT (rfft)
+                const int k = static_cast<int>(param);
+                if (k > nwin / 2) {
+                    result = 0.0;  // past the last rfft coefficient
+                    break;
+                }
+                for (int i = lane; i < nwin; i += 32) {
+                    // phase k i / N in turns, reduced exactly in integers
+                    const int64_t r = (static_cast<int64_t>(k) * i) % nwin;
+                    double sn, cs;
+                    sincospi(2.0 * static_cast<double>(r) / n, &sn, &cs);
+                    const double v = static_cast<double>(x[i]);
+                    a0 = fma(v, cs, a0);
+                    a1 = fma(-v, sn, a1);
+                }
+                const double re = warp_sum_d(a0), im = warp_sum_d(a1);
+                result = kind == PB_FEAT_FFT_REAL   ? re
+                         : kind == PB_FEAT_FFT_IMAG ? im
+                         : kind == PB_FEAT_FFT_ABS  ? hypot(re, im)
+                                                    : atan2(im, re);
+                break;
+            }
+            case PB_FEAT_TREND_SLOPE:
+            case PB_FEAT_TREND_INTERCEPT:
+            case PB_FEAT_TREND_RVALUE:
+            case PB_FEAT_TREND_PVALUE:
+            case PB_FEAT_TREND_STDERR: {  // least squares of x on t = 0..N-1
+                const double tm = 0.5 * (n - 1.0);
+                for (int i = lane; i < nwin; i += 32) {
+                    const double dt = static_cast<double>(i) - tm, dx = static_cast<double>(x[i]) - mean;
+                    a0 += dt * dt;
+                    a1 += dt * dx;
+                    a2 += dx * dx;
+                }
+                const double ss_tt = warp_sum_d(a0), ss_tx = warp_sum_d(a1), ss_xx = warp_sum_d(a2);
+                const double slope = ss_tx / (ss_tt + 1e-10);
+                const double intercept = mean - slope * tm;
+                const double r = ss_tx / (sqrt(ss_tt * ss_xx) + 1e-10);
+                if (kind == PB_FEAT_TREND_SLOPE) {
+                    result = slope;
+                } else if (kind == PB_FEAT_TREND_INTERCEPT) {
+                    result = intercept;
+                } else if (kind == PB_FEAT_TREND_RVALUE) {
+                    result = r;
+                } else if (kind == PB_FEAT_TREND_PVALUE) {  // the reference's pseudo p-value
+                    const double tstat = r * sqrt(n - 2.0) / (sqrt(1.0 - r * r) + 1e-10);
+                    result = 1.0 / (1.0 + fabs(tstat));
+                } else {
+                    double rss = 0.0;
+                    for (int i = lane; i < nwin; i += 32) {
+                        const double e = static_cast<double>(x[i]) - (slope * static_cast<double>(i) + intercept);
+                        rss += e * e;
+                    }
+                    result = sqrt(warp_sum_d(rss) / (n - 2.0) / (ss_tt + 1e-10));
+                }
+                break;
+            }
+            case PB_FEAT_FIRST_LOC_MAX:
+            case PB_FEAT_FIRST_LOC_MIN:
+            case PB_FEAT_LAST_LOC_MAX:
+            case PB_FEAT_LAST_LOC_MIN: {  // index of the first (last) extreme / N
+                const bool want_max = kind == PB_FEAT_FIRST_LOC_MAX || kind == PB_FEAT_LAST_LOC_MAX;
+                const bool last = kind == PB_FEAT_LAST_LOC_MAX || kind == PB_FEAT_LAST_LOC_MIN;
+                float best = want_max ? -CUDART_INF_F : CUDART_INF_F;
+                int bi = -1;
+                bool nan_seen = false;
+                for (int i = lane; i < nwin; i += 32) {
+                    const float v = x[i];
+                    nan_seen |= isnan(v);
+                    const bool better = want_max ? (v > best || (last && v == best)) : (v < best || (last && v == best));
+                    if (bi < 0 || better) {
+                        best = v;
+                        bi = i;
+                    }
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float ov = __shfl_down_sync(0xffffffffu, best, off);
+                    const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                    const bool take = oi >= 0 && (bi < 0 || (want_max ? ov > best : ov < best) ||
+                                                  (ov == best && (last ? oi > bi : oi < bi)));
+                    if (take) {
+                        best = ov;
+                        bi = oi;
+                    }
+                }
+                bi = __shfl_sync(0xffffffffu, bi, 0);
+                result = __any_sync(0xffffffffu, nan_seen) ? CUDART_NAN : static_cast<double>(bi) / n;
+                break;
+            }
+            case PB_FEAT_CID_CE: {
+                for (int i = lane; i < nwin; i += 32) {
+                    const double dx = static_cast<double>(x[i]) - mean;
+                    a1 += dx * dx;
+                    if (i > 0) {
+                        const double d = static_cast<double>(x[i]) - static_cast<double>(x[i - 1]);
+                        a0 += d * d;
+                    }
+                }
+                const double ce = sqrt(warp_sum_d(a0));
+                const double sd = sqrt(warp_sum_d(a1) / n);
+                result = param != 0.0 ? ce / (sd + 1e-10) : ce;
+                break;
+            }
+            case PB_FEAT_C3:
+            case PB_FEAT_TIME_REVERSAL: {
+                const int lag = static_cast<int>(param);
+                if (2 * static_cast<int64_t>(lag) >= nwin) {
+                    result = 0.0;
+                    break;
+                }
+                const int m3 = nwin - 2 * lag;
+                for (int i = lane; i < m3; i += 32) {
+                    const double x0 = x[i], x1 = x[i + lag], x2 = x[i + 2 * lag];
+                    a0 += kind == PB_FEAT_C3 ? x0 * x1 * x2 : x2 * x2 * x1 - x1 * x0 * x0;
+                }
+                result = warp_sum_d(a0) / static_cast<double>(m3);
+                break;
+            }
             default: break;
         }
     }
@@ -496,11 +617,14 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (a->feat_state[c] < 0 || a->feat_state[c] >= a->dim) return PB_EINVAL;
         const int kind = a->feat_kind[c];
         const double prm = a->feat_param[c];
-        if (kind < PB_FEAT_MEDIAN || kind > PB_FEAT_RATIO_BEYOND_R_SIGMA) return PB_EINVAL;
+        if (kind < PB_FEAT_MEDIAN || kind > PB_FEAT_LAST_KIND) return PB_EINVAL;
         if (kind == PB_FEAT_QUANTILE && !(prm >= 0.0 && prm <= 1.0)) return PB_EINVAL;
-        if ((kind == PB_FEAT_NUMBER_PEAKS || kind == PB_FEAT_AUTOCORRELATION) &&
-            !(prm >= 0.0 && prm <= 1e6 && prm == static_cast<double>(static_cast<int>(prm))))
+        const bool int_param = kind == PB_FEAT_NUMBER_PEAKS || kind == PB_FEAT_AUTOCORRELATION ||
+                               (kind >= PB_FEAT_FFT_REAL && kind <= PB_FEAT_FFT_ANGLE) || kind == PB_FEAT_C3 ||
+                               kind == PB_FEAT_TIME_REVERSAL;
+        if (int_param && !(prm >= 0.0 && prm <= 1e6 && prm == static_cast<double>(static_cast<int>(prm))))
             return PB_EINVAL;
+        if (kind == PB_FEAT_CID_CE && !(prm == 0.0 || prm == 1.0)) return PB_EINVAL;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }

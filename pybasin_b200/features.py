@@ -52,6 +52,23 @@ FEATURE_KINDS: dict[str, int] = {
     "number_peaks": L.FEAT_NUMBER_PEAKS,
     "autocorrelation": L.FEAT_AUTOCORRELATION,
     "ratio_beyond_r_sigma": L.FEAT_RATIO_BEYOND_R_SIGMA,
+    "first_location_of_maximum": L.FEAT_FIRST_LOC_MAX,
+    "first_location_of_minimum": L.FEAT_FIRST_LOC_MIN,
+    "last_location_of_maximum": L.FEAT_LAST_LOC_MAX,
+    "last_location_of_minimum": L.FEAT_LAST_LOC_MIN,
+    "cid_ce": L.FEAT_CID_CE,
+    "c3": L.FEAT_C3,
+    "time_reversal_asymmetry_statistic": L.FEAT_TIME_REVERSAL,
+}
+
+#: Features whose ``attr`` parameter selects the kernel kind: name -> (kinds by
+#: attr, default attr, numeric parameter key or None, its default).
+FEATURE_ATTR: dict[str, tuple[dict[str, int], str, str | None, float]] = {
+    "fft_coefficient": ({"real": L.FEAT_FFT_REAL, "imag": L.FEAT_FFT_IMAG, "abs": L.FEAT_FFT_ABS,
+                         "angle": L.FEAT_FFT_ANGLE}, "abs", "coeff", 0.0),
+    "linear_trend": ({"slope": L.FEAT_TREND_SLOPE, "intercept": L.FEAT_TREND_INTERCEPT,
+                      "rvalue": L.FEAT_TREND_RVALUE, "pvalue": L.FEAT_TREND_PVALUE,
+                      "stderr": L.FEAT_TREND_STDERR}, "slope", None, 0.0),
 }
 
 #: The parameter of each parameterised feature (its FCParameters key) and default.
@@ -63,6 +80,9 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_NUMBER_PEAKS: ("n", 1.0),
     L.FEAT_AUTOCORRELATION: ("lag", 1.0),
     L.FEAT_RATIO_BEYOND_R_SIGMA: ("r", 1.0),
+    L.FEAT_CID_CE: ("normalize", 1.0),
+    L.FEAT_C3: ("lag", 1.0),
+    L.FEAT_TIME_REVERSAL: ("lag", 1.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).
@@ -97,16 +117,27 @@ def columns_for(config: dict[str, Any] | None, state: int) -> list[FeatureColumn
     if not config:
         return cols
     for fname, plist in config.items():
+        if fname in FEATURE_ATTR:
+            kinds, default_attr, key, default = FEATURE_ATTR[fname]
+            for p in plist or [{"attr": default_attr, **({key: default} if key else {})}]:
+                attr = p.get("attr", default_attr)
+                if attr not in kinds:
+                    raise ValueError(f"feature '{fname}': attr must be one of {sorted(kinds)}, got {attr!r}")
+                value = float(p[key]) if key and key in p else default
+                cols.append(FeatureColumn(state, kinds[attr], value, _format_name(fname, p, state)))
+            continue
         if fname not in FEATURE_KINDS:
             raise ValueError(
-                f"feature '{fname}' is not one of the fused statistics {sorted(FEATURE_KINDS)}; "
+                f"feature '{fname}' is not one of the fused statistics {sorted([*FEATURE_KINDS, *FEATURE_ATTR])}; "
                 "use B200Dopri5Solver(output='full') with the reference TorchFeatureExtractor for other features"
             )
         kind = FEATURE_KINDS[fname]
         if kind in FEATURE_PARAM:
             key, default = FEATURE_PARAM[kind]
             for p in plist or [{key: default}]:
-                cols.append(FeatureColumn(state, kind, float(p[key]), _format_name(fname, p, state)))
+                v = p[key]
+                cols.append(FeatureColumn(state, kind, float(bool(v)) if isinstance(v, bool) else float(v),
+                                          _format_name(fname, p, state)))
         else:
             if plist is not None:
                 raise ValueError(f"feature '{fname}' takes no parameters")

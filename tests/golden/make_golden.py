@@ -80,6 +80,11 @@ def _features(ref: Path) -> None:
     from pybasin.ts_torch.calculators import torch_features_count as cn
     from pybasin.ts_torch.calculators import torch_features_pattern as pat
     from pybasin.ts_torch.calculators import torch_features_statistical as st
+    from pybasin.ts_torch.calculators import torch_features_advanced as ad
+    from pybasin.ts_torch.calculators import torch_features_entropy_complexity as ec
+    from pybasin.ts_torch.calculators import torch_features_frequency as fq
+    from pybasin.ts_torch.calculators import torch_features_location as lo
+    from pybasin.ts_torch.calculators import torch_features_trend as tr
 
     g = torch.Generator().manual_seed(1234)
     n_t, n_b = 257, 16
@@ -127,6 +132,21 @@ def _features(ref: Path) -> None:
         "autocorrelation_1": ac.autocorrelation(x, 1).numpy(),
         "autocorrelation_7": ac.autocorrelation(x, 7).numpy(),
         "ratio_beyond_r_sigma_1": st.ratio_beyond_r_sigma(x, 1.0).numpy(),
+        # FFT coefficients, linear trend, extreme locations, cid_ce, c3, time reversal
+        **{f"fft_coefficient_{a}_{k}": fq.fft_coefficient(x, k, a).numpy()
+           for a in ("real", "imag", "abs", "angle") for k in (0, 1, 7, 128, 129)},
+        **{f"linear_trend_{a}": tr.linear_trend(x, a).numpy()
+           for a in ("slope", "intercept", "rvalue", "pvalue", "stderr")},
+        "first_location_of_maximum": lo.first_location_of_maximum(x).numpy(),
+        "first_location_of_minimum": lo.first_location_of_minimum(x).numpy(),
+        "last_location_of_maximum": lo.last_location_of_maximum(x).numpy(),
+        "last_location_of_minimum": lo.last_location_of_minimum(x).numpy(),
+        "cid_ce_true": ec.cid_ce(x, True).numpy(),
+        "cid_ce_false": ec.cid_ce(x, False).numpy(),
+        "c3_1": ad.c3(x, 1).numpy(),
+        "c3_5": ad.c3(x, 5).numpy(),
+        "c3_200": ad.c3(x, 200).numpy(),
+        "time_reversal_asymmetry_statistic_2": ad.time_reversal_asymmetry_statistic(x, 2).numpy(),
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

@@ -440,6 +440,64 @@ def test_wider_feature_set_matches_oracle(dense, precision):
             np.testing.assert_allclose(g[:, c], w[:, c], rtol=tol, atol=tol * 1e-3 * scale, err_msg=f"col {c} kind {kind}")
 
 
+MORE_FEATS = [(0, k, float(c)) for k in (L.FEAT_FFT_REAL, L.FEAT_FFT_IMAG, L.FEAT_FFT_ABS, L.FEAT_FFT_ANGLE)
+              for c in (1, 5, 250)] + [
+    (0, L.FEAT_FFT_ABS, 0.0), (0, L.FEAT_FFT_REAL, 251.0),
+    (0, L.FEAT_TREND_SLOPE, 0.0), (0, L.FEAT_TREND_INTERCEPT, 0.0), (0, L.FEAT_TREND_RVALUE, 0.0),
+    (0, L.FEAT_TREND_PVALUE, 0.0), (0, L.FEAT_TREND_STDERR, 0.0),
+    (1, L.FEAT_FIRST_LOC_MAX, 0.0), (1, L.FEAT_FIRST_LOC_MIN, 0.0), (1, L.FEAT_LAST_LOC_MAX, 0.0),
+    (1, L.FEAT_LAST_LOC_MIN, 0.0), (0, L.FEAT_CID_CE, 1.0), (0, L.FEAT_CID_CE, 0.0), (0, L.FEAT_C3, 2.0),
+    (0, L.FEAT_C3, 300.0), (1, L.FEAT_TIME_REVERSAL, 3.0),
+]
+LOCATION_KINDS = {L.FEAT_FIRST_LOC_MAX, L.FEAT_FIRST_LOC_MIN, L.FEAT_LAST_LOC_MAX, L.FEAT_LAST_LOC_MIN}
+
+
+@DENSE
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+def test_frequency_trend_location_features_match_oracle(dense, precision):
+    """FFT coefficients, linear trend, extreme locations, cid_ce, c3 and the time
+    reversal statistic from the window pass against the oracle (the short horizon
+    of the wider-set test): continuous features to 2e-4 relative (2e-3 mixed); the
+    location of an extreme within 2 samples (FP64) / 10 samples (mixed) of the
+    oracle's, since a flat extremum moves with the trajectory's last digits.  The
+    window pass reads FP32-stored samples, so a DFT coefficient carries up to
+    2^-24 * sum |x_n| (about 3e-5 here) of absolute error whatever its size: real,
+    imaginary part and magnitude get that absolute tolerance, and an angle is
+    compared on the unit circle where the magnitude resolves it."""
+    case = DUFFING
+    y0 = seeded_ics(case, 200, seed=13).double().numpy()
+    save = np.asarray(torch.linspace(0.0, 30.0, 1501, dtype=torch.float32).double())
+    wb = int(np.nonzero(save >= 20.0)[0][0])
+    n = len(save) - wb
+    rtol = case.rtol if precision == L.PREC_FP64 else 1e-6
+    want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), min(rtol, 1e-8), 1e-10,
+                         win_begin=wb, features=MORE_FEATS)
+    got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), min(rtol, 1e-8), 1e-10,
+                    win_begin=wb, features=MORE_FEATS, dense_mode=dense, precision=precision)
+    assert (got["status"] == 0).all()
+    g, w = got["features"], want["features"]
+    fft_atol = 3e-5 if precision == L.PREC_FP64 else 3e-3
+    abs_col = {prm: c for c, (_, kind, prm) in enumerate(MORE_FEATS) if kind == L.FEAT_FFT_ABS}
+    for c, (_, kind, prm) in enumerate(MORE_FEATS):
+        if kind == L.FEAT_FFT_ANGLE:
+            mag = w[:, abs_col[prm]]
+            keep = mag > 100 * fft_atol
+            chord = np.abs(np.exp(1j * g[keep, c]) - np.exp(1j * w[keep, c]))
+            assert chord.max(initial=0.0) <= 2e-2, (c, kind, prm)  # angle error <= fft_atol / |X| <= 1e-2
+        elif kind in (L.FEAT_FFT_REAL, L.FEAT_FFT_IMAG, L.FEAT_FFT_ABS) and prm != 251.0:
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=2e-4, atol=fft_atol, err_msg=f"col {c} kind {kind}")
+        elif kind in LOCATION_KINDS:
+            lim = (2.0 if precision == L.PREC_FP64 else 10.0) / n
+            assert np.abs(g[:, c] - w[:, c]).max() <= lim + 1e-12, (c, kind)
+        elif kind == L.FEAT_FFT_REAL and prm == 251.0 or kind == L.FEAT_C3 and prm == 300.0:
+            assert (g[:, c] == 0.0).all() and (w[:, c] == 0.0).all()  # past the last coefficient / lag
+        else:
+            tol = 2e-4 if precision == L.PREC_FP64 else 2e-3
+            scale = np.abs(w[:, c]).max() + 1e-12
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=tol, atol=tol * 1e-2 * scale,
+                                       err_msg=f"col {c} kind {kind}")
+
+
 def test_wider_features_through_the_extractor_names():
     """FCParameters names and parameters as in the reference's settings (ts_torch/settings.py:223-355)."""
     from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor

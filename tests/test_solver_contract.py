@@ -102,7 +102,14 @@ def test_feature_columns_and_names_follow_reference_order():
         "state_1__number_crossing_m__m_1",
     ]
     with pytest.raises(ValueError, match="fused statistics"):
-        FusedFeatureExtractor(features={"fft_coefficient": None}).columns(1)
+        FusedFeatureExtractor(features={"sample_entropy": None}).columns(1)
+    # attribute-selected kernels keep the reference's parameter names
+    fft = FusedFeatureExtractor(features={"fft_coefficient": [{"coeff": 2, "attr": "imag"}],
+                                          "linear_trend": [{"attr": "stderr"}]}).columns(1)
+    assert [c.name for c in fft] == ["state_0__fft_coefficient__attr_imag__coeff_2",
+                                     "state_0__linear_trend__attr_stderr"]
+    with pytest.raises(ValueError, match="attr"):
+        FusedFeatureExtractor(features={"linear_trend": [{"attr": "slop"}]}).columns(1)
 
 
 def test_y0_shape_validation_before_any_gpu_work(simple_ode):
