@@ -107,10 +107,17 @@ typedef enum {
     PB_FEAT_TREND_SLOPE = 36, PB_FEAT_TREND_INTERCEPT = 37, PB_FEAT_TREND_RVALUE = 38,
     PB_FEAT_TREND_PVALUE = 39, PB_FEAT_TREND_STDERR = 40,
     PB_FEAT_FIRST_LOC_MAX = 41, PB_FEAT_FIRST_LOC_MIN = 42, PB_FEAT_LAST_LOC_MAX = 43,
-    PB_FEAT_LAST_LOC_MIN = 44, PB_FEAT_CID_CE = 45, PB_FEAT_C3 = 46, PB_FEAT_TIME_REVERSAL = 47
+    PB_FEAT_LAST_LOC_MIN = 44, PB_FEAT_CID_CE = 45, PB_FEAT_C3 = 46, PB_FEAT_TIME_REVERSAL = 47,
+    /* spkt_welch_density (coeff; torch_features_frequency.py:57-65),
+       large_standard_deviation (r; torch_features_boolean.py:44-48), symmetry_looking
+       (r; torch_features_statistical.py:185-191), index_mass_quantile (q;
+       torch_features_location.py:52-65), longest_strike_above_mean /
+       longest_strike_below_mean (torch_features_pattern.py:10-53) */
+    PB_FEAT_SPKT_WELCH = 48, PB_FEAT_LARGE_STD = 49, PB_FEAT_SYMMETRY_LOOKING = 50,
+    PB_FEAT_INDEX_MASS_QUANTILE = 51, PB_FEAT_LONGEST_STRIKE_ABOVE = 52, PB_FEAT_LONGEST_STRIKE_BELOW = 53
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_TIME_REVERSAL
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..47): the
+#define PB_FEAT_LAST_KIND PB_FEAT_LONGEST_STRIKE_BELOW
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..53): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 

@@ -255,6 +255,7 @@ static double window_feature(int feat, double param, const double *w, int n, dou
     }
     /* torch_features_frequency.py:11-29: coefficient k of torch.fft.rfft, a direct
        DFT sum with the phase k*i/n reduced in integers */
+    case ORACLE_F_SPKT_WELCH: /* torch_features_frequency.py:57-65: |X_k|^2 / n */
     case ORACLE_F_FFT_REAL: case ORACLE_F_FFT_IMAG: case ORACLE_F_FFT_ABS: case ORACLE_F_FFT_ANGLE: {
         const long k = (long)param;
         if (k > n / 2) return 0.0;
@@ -267,7 +268,37 @@ static double window_feature(int feat, double param, const double *w, int n, dou
         if (feat == ORACLE_F_FFT_REAL) return re;
         if (feat == ORACLE_F_FFT_IMAG) return im;
         if (feat == ORACLE_F_FFT_ABS) return sqrt(re * re + im * im);
+        if (feat == ORACLE_F_SPKT_WELCH) return (re * re + im * im) / n;
         return atan2(im, re);
+    }
+    /* torch_features_boolean.py:44-48 */
+    case ORACLE_F_LARGE_STD: return sqrt(m2 / n) > param * (mx - mn) ? 1.0 : 0.0;
+    /* torch_features_statistical.py:185-191 (median as torch.median: the lower middle) */
+    case ORACLE_F_SYMMETRY_LOOKING: {
+        if (any_nan) return NAN;
+        memcpy(scratch, w, sizeof(double) * (size_t)n);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double);
+        return fabs(mean - scratch[(n - 1) / 2]) < param * (mx - mn) ? 1.0 : 0.0;
+    }
+    /* torch_features_location.py:52-65 */
+    case ORACLE_F_INDEX_MASS_QUANTILE: {
+        double tot = 0.0, c = 0.0;
+        for (int i = 0; i < n; ++i) tot += fabs(w[i]);
+        for (int i = 0; i < n; ++i) {
+            c += fabs(w[i]);
+            if (c >= param * tot) return (double)i / n;
+        }
+        return 0.0;
+    }
+    /* torch_features_pattern.py:10-53 */
+    case ORACLE_F_LONGEST_STRIKE_ABOVE: case ORACLE_F_LONGEST_STRIKE_BELOW: {
+        int run = 0, best = 0;
+        for (int i = 0; i < n; ++i) {
+            const int on = feat == ORACLE_F_LONGEST_STRIKE_ABOVE ? w[i] > mean : w[i] < mean;
+            run = on ? run + 1 : 0;
+            if (run > best) best = run;
+        }
+        return (double)best;
     }
     /* torch_features_trend.py:11-51 (with its pseudo p-value 1 / (1 + |t|)) */
     case ORACLE_F_TREND_SLOPE: case ORACLE_F_TREND_INTERCEPT: case ORACLE_F_TREND_RVALUE:

@@ -33,6 +33,10 @@ enum {
     ORACLE_F_TREND_PVALUE = 39, ORACLE_F_TREND_STDERR = 40,
     ORACLE_F_FIRST_LOC_MAX = 41, ORACLE_F_FIRST_LOC_MIN = 42, ORACLE_F_LAST_LOC_MAX = 43,
     ORACLE_F_LAST_LOC_MIN = 44, ORACLE_F_CID_CE = 45, ORACLE_F_C3 = 46, ORACLE_F_TIME_REVERSAL = 47,
+    /* spkt_welch_density (coeff), large_standard_deviation (r), symmetry_looking (r),
+       index_mass_quantile (q), longest_strike_above_mean, longest_strike_below_mean */
+    ORACLE_F_SPKT_WELCH = 48, ORACLE_F_LARGE_STD = 49, ORACLE_F_SYMMETRY_LOOKING = 50,
+    ORACLE_F_INDEX_MASS_QUANTILE = 51, ORACLE_F_LONGEST_STRIKE_ABOVE = 52, ORACLE_F_LONGEST_STRIKE_BELOW = 53,
 };
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };

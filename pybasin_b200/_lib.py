@@ -88,6 +88,8 @@ FEAT_FFT_REAL, FEAT_FFT_IMAG, FEAT_FFT_ABS, FEAT_FFT_ANGLE = 32, 33, 34, 35
 FEAT_TREND_SLOPE, FEAT_TREND_INTERCEPT, FEAT_TREND_RVALUE, FEAT_TREND_PVALUE, FEAT_TREND_STDERR = 36, 37, 38, 39, 40
 FEAT_FIRST_LOC_MAX, FEAT_FIRST_LOC_MIN, FEAT_LAST_LOC_MAX, FEAT_LAST_LOC_MIN = 41, 42, 43, 44
 FEAT_CID_CE, FEAT_C3, FEAT_TIME_REVERSAL = 45, 46, 47
+FEAT_SPKT_WELCH, FEAT_LARGE_STD, FEAT_SYMMETRY_LOOKING = 48, 49, 50
+FEAT_INDEX_MASS_QUANTILE, FEAT_LONGEST_STRIKE_ABOVE, FEAT_LONGEST_STRIKE_BELOW = 51, 52, 53
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

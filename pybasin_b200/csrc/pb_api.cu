@@ -102,11 +102,26 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
     const double param = plan.param[m];
     const double n = static_cast<double>(nwin);
     double result = CUDART_NAN;
-    if (kind == PB_FEAT_MEDIAN || kind == PB_FEAT_QUANTILE) {
+    if (kind == PB_FEAT_MEDIAN || kind == PB_FEAT_QUANTILE || kind == PB_FEAT_SYMMETRY_LOOKING) {
         bool nan_seen = false;
         for (int i = lane; i < nwin; i += 32) nan_seen |= isnan(x[i]);
         if (!__any_sync(0xffffffffu, nan_seen)) {
-            if (kind == PB_FEAT_MEDIAN) {
+            if (kind == PB_FEAT_SYMMETRY_LOOKING) {  // |mean - median| < r * range, as 1 / 0
+                double s = 0.0;
+                float mx = -CUDART_INF_F, mn = CUDART_INF_F;
+                for (int i = lane; i < nwin; i += 32) {
+                    s += static_cast<double>(x[i]);
+                    mx = fmaxf(mx, x[i]);
+                    mn = fminf(mn, x[i]);
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+                    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+                }
+                const double mean = warp_sum_d(s) / n;
+                const double med = select_rank(x, nwin, static_cast<unsigned>((nwin - 1) / 2), h, lane);
+                result = fabs(mean - med) < param * (static_cast<double>(mx) - static_cast<double>(mn)) ? 1.0 : 0.0;
+            } else if (kind == PB_FEAT_MEDIAN) {
                 result = select_rank(x, nwin, static_cast<unsigned>((nwin - 1) / 2), h, lane);
             } else {
                 const double pos = param * (nwin - 1);
@@ -218,6 +233,7 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = static_cast<double>(count);
                 break;
             }
+            case PB_FEAT_SPKT_WELCH:
             case PB_FEAT_FFT_REAL:
             case PB_FEAT_FFT_IMAG:
             case PB_FEAT_FFT_ABS:
@@ -240,7 +256,8 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = kind == PB_FEAT_FFT_REAL   ? re
                          : kind == PB_FEAT_FFT_IMAG ? im
                          : kind == PB_FEAT_FFT_ABS  ? hypot(re, im)
-                                                    : atan2(im, re);
+                         : kind == PB_FEAT_FFT_ANGLE ? atan2(im, re)
+                                                     : (re * re + im * im) / n;  // power / N
                 break;
             }
             case PB_FEAT_TREND_SLOPE:
@@ -322,6 +339,61 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 const double ce = sqrt(warp_sum_d(a0));
                 const double sd = sqrt(warp_sum_d(a1) / n);
                 result = param != 0.0 ? ce / (sd + 1e-10) : ce;
+                break;
+            }
+            case PB_FEAT_LARGE_STD: {  // population std > r * range, as 1 / 0
+                float mx = -CUDART_INF_F, mn = CUDART_INF_F;
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                    mx = fmaxf(mx, x[i]);
+                    mn = fminf(mn, x[i]);
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+                    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+                }
+                const double sd = sqrt(warp_sum_d(a0) / n);
+                result = sd > param * (static_cast<double>(mx) - static_cast<double>(mn)) ? 1.0 : 0.0;
+                break;
+            }
+            case PB_FEAT_INDEX_MASS_QUANTILE: {  // first index where cumsum |x| >= q * total, / N
+                for (int i = lane; i < nwin; i += 32) a0 += fabs(static_cast<double>(x[i]));
+                const double thr = param * warp_sum_d(a0);
+                double carry = 0.0;
+                int found = -1;
+                for (int i0 = 0; i0 < nwin && found < 0; i0 += 32) {
+                    const int i = i0 + lane;
+                    double c = i < nwin ? fabs(static_cast<double>(x[i])) : 0.0;
+                    for (int off = 1; off < 32; off <<= 1) {  // inclusive prefix sum
+                        const double o = __shfl_up_sync(0xffffffffu, c, off);
+                        if (lane >= off) c += o;
+                    }
+                    c += carry;
+                    const unsigned hit = __ballot_sync(0xffffffffu, i < nwin && c >= thr);
+                    if (hit) found = i0 + __ffs(hit) - 1;
+                    carry = __shfl_sync(0xffffffffu, c, 31);
+                }
+                result = static_cast<double>(found < 0 ? 0 : found) / n;
+                break;
+            }
+            case PB_FEAT_LONGEST_STRIKE_ABOVE:
+            case PB_FEAT_LONGEST_STRIKE_BELOW: {  // longest run of samples above (below) the mean
+                int run = 0, best = 0;  // run: length of the run ending at the previous chunk's end
+                for (int i0 = 0; i0 < nwin; i0 += 32) {
+                    const int i = i0 + lane;
+                    const double v = i < nwin ? static_cast<double>(x[i]) : mean;
+                    const bool on = i < nwin && (kind == PB_FEAT_LONGEST_STRIKE_ABOVE ? v > mean : v < mean);
+                    const unsigned m = __ballot_sync(0xffffffffu, on);
+                    // run ending at this lane: back to the last lane (at or below) that is off
+                    const unsigned off_mask = ~m & ((lane == 31) ? 0xffffffffu : ((1u << (lane + 1)) - 1u));
+                    const int here = !on ? 0 : (off_mask ? lane - (31 - __clz(off_mask)) : lane + 1 + run);
+                    int mx = here;
+                    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                    best = max(best, mx);
+                    run = __shfl_sync(0xffffffffu, here, 31);
+                }
+                result = static_cast<double>(best);
                 break;
             }
             case PB_FEAT_C3:
@@ -621,10 +693,11 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_QUANTILE && !(prm >= 0.0 && prm <= 1.0)) return PB_EINVAL;
         const bool int_param = kind == PB_FEAT_NUMBER_PEAKS || kind == PB_FEAT_AUTOCORRELATION ||
                                (kind >= PB_FEAT_FFT_REAL && kind <= PB_FEAT_FFT_ANGLE) || kind == PB_FEAT_C3 ||
-                               kind == PB_FEAT_TIME_REVERSAL;
+                               kind == PB_FEAT_TIME_REVERSAL || kind == PB_FEAT_SPKT_WELCH;
         if (int_param && !(prm >= 0.0 && prm <= 1e6 && prm == static_cast<double>(static_cast<int>(prm))))
             return PB_EINVAL;
         if (kind == PB_FEAT_CID_CE && !(prm == 0.0 || prm == 1.0)) return PB_EINVAL;
+        if (kind == PB_FEAT_INDEX_MASS_QUANTILE && !(prm >= 0.0 && prm <= 1.0)) return PB_EINVAL;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }

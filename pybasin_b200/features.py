@@ -59,6 +59,12 @@ FEATURE_KINDS: dict[str, int] = {
     "cid_ce": L.FEAT_CID_CE,
     "c3": L.FEAT_C3,
     "time_reversal_asymmetry_statistic": L.FEAT_TIME_REVERSAL,
+    "spkt_welch_density": L.FEAT_SPKT_WELCH,
+    "large_standard_deviation": L.FEAT_LARGE_STD,
+    "symmetry_looking": L.FEAT_SYMMETRY_LOOKING,
+    "index_mass_quantile": L.FEAT_INDEX_MASS_QUANTILE,
+    "longest_strike_above_mean": L.FEAT_LONGEST_STRIKE_ABOVE,
+    "longest_strike_below_mean": L.FEAT_LONGEST_STRIKE_BELOW,
 }
 
 #: Features whose ``attr`` parameter selects the kernel kind: name -> (kinds by
@@ -83,6 +89,10 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_CID_CE: ("normalize", 1.0),
     L.FEAT_C3: ("lag", 1.0),
     L.FEAT_TIME_REVERSAL: ("lag", 1.0),
+    L.FEAT_SPKT_WELCH: ("coeff", 2.0),
+    L.FEAT_LARGE_STD: ("r", 0.25),
+    L.FEAT_SYMMETRY_LOOKING: ("r", 0.1),
+    L.FEAT_INDEX_MASS_QUANTILE: ("q", 0.5),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).

@@ -81,6 +81,7 @@ def _features(ref: Path) -> None:
     from pybasin.ts_torch.calculators import torch_features_pattern as pat
     from pybasin.ts_torch.calculators import torch_features_statistical as st
     from pybasin.ts_torch.calculators import torch_features_advanced as ad
+    from pybasin.ts_torch.calculators import torch_features_boolean as bo
     from pybasin.ts_torch.calculators import torch_features_entropy_complexity as ec
     from pybasin.ts_torch.calculators import torch_features_frequency as fq
     from pybasin.ts_torch.calculators import torch_features_location as lo
@@ -147,6 +148,12 @@ def _features(ref: Path) -> None:
         "c3_5": ad.c3(x, 5).numpy(),
         "c3_200": ad.c3(x, 200).numpy(),
         "time_reversal_asymmetry_statistic_2": ad.time_reversal_asymmetry_statistic(x, 2).numpy(),
+        **{f"spkt_welch_density_{k}": fq.spkt_welch_density(x, k).numpy() for k in (2, 5, 128, 129)},
+        **{f"large_standard_deviation_{r}": bo.has_large_standard_deviation(x, r).numpy() for r in (0.1, 0.25, 0.3)},
+        **{f"symmetry_looking_{r}": st.symmetry_looking(x, r).numpy() for r in (0.05, 0.5)},
+        **{f"index_mass_quantile_{q}": lo.index_mass_quantile(x, q).numpy() for q in (0.1, 0.5, 0.9)},
+        "longest_strike_above_mean": pat.longest_strike_above_mean(x).numpy(),
+        "longest_strike_below_mean": pat.longest_strike_below_mean(x).numpy(),
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

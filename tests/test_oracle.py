@@ -135,6 +135,12 @@ def test_oracle_matches_reference_scipy_trajectories():
         ("c3_5", 46, 5.0),
         ("c3_200", 46, 200.0),
         ("time_reversal_asymmetry_statistic_2", 47, 2.0),
+        *[(f"spkt_welch_density_{k}", 48, float(k)) for k in (2, 5, 128, 129)],
+        *[(f"large_standard_deviation_{r}", 49, r) for r in (0.1, 0.25, 0.3)],
+        *[(f"symmetry_looking_{r}", 50, r) for r in (0.05, 0.5)],
+        *[(f"index_mass_quantile_{q}", 51, q) for q in (0.1, 0.5, 0.9)],
+        ("longest_strike_above_mean", 52, 0.0),
+        ("longest_strike_below_mean", 53, 0.0),
     ],
 )
 def test_oracle_window_features_match_reference_calculators(name, kind, param):
@@ -146,7 +152,8 @@ def test_oracle_window_features_match_reference_calculators(name, kind, param):
     # boolean mask in FP32 (.float().mean()), and divides the extreme locations
     # as FP32 (idx.float() / n): exact to FP32 rounding only.  The FFT coefficients
     # come from torch's FFT (another summation order): 1e-10 of the window's scale.
-    fp32 = name.startswith(("count_above_", "count_below_", "ratio_beyond", "first_location", "last_location"))
+    fp32 = name.startswith(("count_above_", "count_below_", "ratio_beyond", "first_location", "last_location",
+                            "index_mass_quantile"))
     tol = 2e-7 if fp32 else 1e-12
     atol = 1e-12
     if name.startswith("fft_coefficient_angle"):
@@ -156,7 +163,7 @@ def test_oracle_window_features_match_reference_calculators(name, kind, param):
         keep = mag > 1e-8 * np.abs(x).sum(axis=0)
         np.testing.assert_allclose(got[keep], want[keep], rtol=0.0, atol=1e-9)
         return
-    if name.startswith("fft_coefficient"):
+    if name.startswith(("fft_coefficient", "spkt_welch")):
         tol, atol = 1e-10, 1e-10 * np.abs(x).sum(axis=0).max()
     np.testing.assert_allclose(got, want, rtol=tol, atol=atol)
 

@@ -440,16 +440,22 @@ def test_wider_feature_set_matches_oracle(dense, precision):
             np.testing.assert_allclose(g[:, c], w[:, c], rtol=tol, atol=tol * 1e-3 * scale, err_msg=f"col {c} kind {kind}")
 
 
-MORE_FEATS = [(0, k, float(c)) for k in (L.FEAT_FFT_REAL, L.FEAT_FFT_IMAG, L.FEAT_FFT_ABS, L.FEAT_FFT_ANGLE)
-              for c in (1, 5, 250)] + [
+MORE_FEATS = [(0, k, float(c)) for k in (L.FEAT_FFT_REAL, L.FEAT_FFT_IMAG, L.FEAT_FFT_ANGLE) for c in (1, 250)] + [
+    (0, L.FEAT_FFT_ABS, 1.0), (0, L.FEAT_FFT_ABS, 250.0),
     (0, L.FEAT_FFT_ABS, 0.0), (0, L.FEAT_FFT_REAL, 251.0),
     (0, L.FEAT_TREND_SLOPE, 0.0), (0, L.FEAT_TREND_INTERCEPT, 0.0), (0, L.FEAT_TREND_RVALUE, 0.0),
     (0, L.FEAT_TREND_PVALUE, 0.0), (0, L.FEAT_TREND_STDERR, 0.0),
     (1, L.FEAT_FIRST_LOC_MAX, 0.0), (1, L.FEAT_FIRST_LOC_MIN, 0.0), (1, L.FEAT_LAST_LOC_MAX, 0.0),
     (1, L.FEAT_LAST_LOC_MIN, 0.0), (0, L.FEAT_CID_CE, 1.0), (0, L.FEAT_CID_CE, 0.0), (0, L.FEAT_C3, 2.0),
     (0, L.FEAT_C3, 300.0), (1, L.FEAT_TIME_REVERSAL, 3.0),
+    (0, L.FEAT_SPKT_WELCH, 5.0), (0, L.FEAT_LARGE_STD, 0.25), (1, L.FEAT_SYMMETRY_LOOKING, 0.1),
+    (0, L.FEAT_INDEX_MASS_QUANTILE, 0.5), (0, L.FEAT_LONGEST_STRIKE_ABOVE, 0.0),
+    (1, L.FEAT_LONGEST_STRIKE_BELOW, 0.0),
 ]
-LOCATION_KINDS = {L.FEAT_FIRST_LOC_MAX, L.FEAT_FIRST_LOC_MIN, L.FEAT_LAST_LOC_MAX, L.FEAT_LAST_LOC_MIN}
+LOCATION_KINDS = {L.FEAT_FIRST_LOC_MAX, L.FEAT_FIRST_LOC_MIN, L.FEAT_LAST_LOC_MAX, L.FEAT_LAST_LOC_MIN,
+                  L.FEAT_INDEX_MASS_QUANTILE}
+FLAG_KINDS = {L.FEAT_LARGE_STD, L.FEAT_SYMMETRY_LOOKING}  # 1 / 0 decisions on a threshold
+RUN_KINDS = {L.FEAT_LONGEST_STRIKE_ABOVE, L.FEAT_LONGEST_STRIKE_BELOW}
 
 
 @DENSE
@@ -489,6 +495,12 @@ def test_frequency_trend_location_features_match_oracle(dense, precision):
         elif kind in LOCATION_KINDS:
             lim = (2.0 if precision == L.PREC_FP64 else 10.0) / n
             assert np.abs(g[:, c] - w[:, c]).max() <= lim + 1e-12, (c, kind)
+        elif kind in FLAG_KINDS:  # a value within rounding of its threshold may flip
+            assert (g[:, c] != w[:, c]).sum() <= 2, (c, kind)
+        elif kind in RUN_KINDS:  # a sample within rounding of the mean may end a run
+            assert (g[:, c] != w[:, c]).mean() <= 0.05, (c, kind)
+        elif kind == L.FEAT_SPKT_WELCH:
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=2e-3, atol=fft_atol * 2e-2, err_msg=f"col {c}")
         elif kind == L.FEAT_FFT_REAL and prm == 251.0 or kind == L.FEAT_C3 and prm == 300.0:
             assert (g[:, c] == 0.0).all() and (w[:, c] == 0.0).all()  # past the last coefficient / lag
         else:
