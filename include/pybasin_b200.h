@@ -114,10 +114,16 @@ typedef enum {
        torch_features_location.py:52-65), longest_strike_above_mean /
        longest_strike_below_mean (torch_features_pattern.py:10-53) */
     PB_FEAT_SPKT_WELCH = 48, PB_FEAT_LARGE_STD = 49, PB_FEAT_SYMMETRY_LOOKING = 50,
-    PB_FEAT_INDEX_MASS_QUANTILE = 51, PB_FEAT_LONGEST_STRIKE_ABOVE = 52, PB_FEAT_LONGEST_STRIKE_BELOW = 53
+    PB_FEAT_INDEX_MASS_QUANTILE = 51, PB_FEAT_LONGEST_STRIKE_ABOVE = 52, PB_FEAT_LONGEST_STRIKE_BELOW = 53,
+    /* has_duplicate_max / has_duplicate_min (torch_features_boolean.py:23-34),
+       binned_entropy (max_bins <= 256; torch_features_entropy_complexity.py:58-100),
+       mean_n_absolute_max (number_of_maxima <= 64; torch_features_statistical.py:166-172),
+       benford_correlation (torch_features_advanced.py:21-81) */
+    PB_FEAT_HAS_DUP_MAX = 54, PB_FEAT_HAS_DUP_MIN = 55, PB_FEAT_BINNED_ENTROPY = 56,
+    PB_FEAT_MEAN_N_ABS_MAX = 57, PB_FEAT_BENFORD = 58
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_LONGEST_STRIKE_BELOW
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..53): the
+#define PB_FEAT_LAST_KIND PB_FEAT_BENFORD
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..58): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 

@@ -290,6 +290,72 @@ static double window_feature(int feat, double param, const double *w, int n, dou
         }
         return 0.0;
     }
+    /* torch_features_boolean.py:23-34 */
+    case ORACLE_F_HAS_DUP_MAX: case ORACLE_F_HAS_DUP_MIN: {
+        if (any_nan) return 0.0;
+        const double e = feat == ORACLE_F_HAS_DUP_MAX ? mx : mn;
+        int c = 0;
+        for (int i = 0; i < n; ++i) c += w[i] == e;
+        return c > 1 ? 1.0 : 0.0;
+    }
+    /* torch_features_entropy_complexity.py:58-100 */
+    case ORACLE_F_BINNED_ENTROPY: {
+        const int bins = (int)param;
+        double hb[256];
+        if (mx == mn) return 0.0;
+        if (bins < 1 || bins > 256) return NAN;
+        for (int b = 0; b < bins; ++b) hb[b] = 0.0;
+        for (int i = 0; i < n; ++i) {
+            long long b = (long long)((w[i] - mn) / (mx - mn + 1e-10) * (bins - 1e-6));
+            b = b < 0 ? 0 : (b > bins - 1 ? bins - 1 : b);
+            hb[b] += 1.0;
+        }
+        double e = 0.0;
+        for (int b = 0; b < bins; ++b)
+            if (hb[b] > 0.0) {
+                const double p = fmax(hb[b] / n, 1e-10);
+                e -= p * log(p);
+            }
+        return e;
+    }
+    /* torch_features_statistical.py:166-172: mean of the k largest |x| */
+    case ORACLE_F_MEAN_N_ABS_MAX: {
+        const int k = (int)param < n ? (int)param : n;
+        for (int i = 0; i < n; ++i) scratch[i] = fabs(w[i]);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double);
+        double t = 0.0;
+        for (int i = 0; i < k; ++i) t += scratch[n - 1 - i];
+        return t / k;
+    }
+    /* torch_features_advanced.py:21-81 */
+    case ORACLE_F_BENFORD: {
+        double f[9] = {0}, b[9], tot = 0.0, fm = 0.0, bm = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double v = fabs(w[i]);
+            if (!(v > 0.0)) continue;
+            const long long dg = (long long)floor(v / pow(10.0, floor(log10(v))));
+            if (dg >= 1 && dg <= 9) {
+                f[dg - 1] += 1.0;
+                tot += 1.0;
+            }
+        }
+        for (int d = 0; d < 9; ++d) {
+            f[d] /= tot + 1e-10;
+            fm += f[d];
+            b[d] = log10(1.0 + 1.0 / (d + 1));
+            bm += b[d];
+        }
+        fm /= 9.0;
+        bm /= 9.0;
+        double sfb = 0.0, sff = 0.0, sbb = 0.0;
+        for (int d = 0; d < 9; ++d) {
+            sfb += (f[d] - fm) * (b[d] - bm);
+            sff += (f[d] - fm) * (f[d] - fm);
+            sbb += (b[d] - bm) * (b[d] - bm);
+        }
+        const double corr = sfb / (sqrt(sff / 8.0) * sqrt(sbb / 8.0) * 9.0 + 1e-10);
+        return tot >= 10.0 ? corr : 0.0;
+    }
     /* torch_features_pattern.py:10-53 */
     case ORACLE_F_LONGEST_STRIKE_ABOVE: case ORACLE_F_LONGEST_STRIKE_BELOW: {
         int run = 0, best = 0;

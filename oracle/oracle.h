@@ -37,6 +37,10 @@ enum {
        index_mass_quantile (q), longest_strike_above_mean, longest_strike_below_mean */
     ORACLE_F_SPKT_WELCH = 48, ORACLE_F_LARGE_STD = 49, ORACLE_F_SYMMETRY_LOOKING = 50,
     ORACLE_F_INDEX_MASS_QUANTILE = 51, ORACLE_F_LONGEST_STRIKE_ABOVE = 52, ORACLE_F_LONGEST_STRIKE_BELOW = 53,
+    /* has_duplicate_max, has_duplicate_min, binned_entropy (max_bins),
+       mean_n_absolute_max (number_of_maxima), benford_correlation */
+    ORACLE_F_HAS_DUP_MAX = 54, ORACLE_F_HAS_DUP_MIN = 55, ORACLE_F_BINNED_ENTROPY = 56,
+    ORACLE_F_MEAN_N_ABS_MAX = 57, ORACLE_F_BENFORD = 58,
 };
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };

@@ -90,6 +90,7 @@ FEAT_FIRST_LOC_MAX, FEAT_FIRST_LOC_MIN, FEAT_LAST_LOC_MAX, FEAT_LAST_LOC_MIN = 4
 FEAT_CID_CE, FEAT_C3, FEAT_TIME_REVERSAL = 45, 46, 47
 FEAT_SPKT_WELCH, FEAT_LARGE_STD, FEAT_SYMMETRY_LOOKING = 48, 49, 50
 FEAT_INDEX_MASS_QUANTILE, FEAT_LONGEST_STRIKE_ABOVE, FEAT_LONGEST_STRIKE_BELOW = 51, 52, 53
+FEAT_HAS_DUP_MAX, FEAT_HAS_DUP_MIN, FEAT_BINNED_ENTROPY, FEAT_MEAN_N_ABS_MAX, FEAT_BENFORD = 54, 55, 56, 57, 58
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

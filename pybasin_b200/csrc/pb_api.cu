@@ -396,6 +396,137 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = static_cast<double>(best);
                 break;
             }
+            case PB_FEAT_HAS_DUP_MAX:
+            case PB_FEAT_HAS_DUP_MIN: {  // the extreme occurs more than once, as 1 / 0
+                const bool want_max = kind == PB_FEAT_HAS_DUP_MAX;
+                float e = want_max ? -CUDART_INF_F : CUDART_INF_F;
+                bool nan_seen = false;
+                for (int i = lane; i < nwin; i += 32) {
+                    nan_seen |= isnan(x[i]);
+                    e = want_max ? fmaxf(e, x[i]) : fminf(e, x[i]);
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float o = __shfl_xor_sync(0xffffffffu, e, off);
+                    e = want_max ? fmaxf(e, o) : fminf(e, o);
+                }
+                int cnt = 0;
+                for (int i = lane; i < nwin; i += 32) cnt += x[i] == e;
+                for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+                // torch.max propagates NaN, and NaN == NaN is false: no duplicate then
+                result = (!__any_sync(0xffffffffu, nan_seen) && cnt > 1) ? 1.0 : 0.0;
+                break;
+            }
+            case PB_FEAT_BINNED_ENTROPY: {  // entropy of max_bins equal-width bins over [min, max]
+                const int bins = static_cast<int>(param);
+                float mx = -CUDART_INF_F, mn = CUDART_INF_F;
+                for (int i = lane; i < nwin; i += 32) {
+                    mx = fmaxf(mx, x[i]);
+                    mn = fminf(mn, x[i]);
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+                    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+                }
+                if (mx == mn) {
+                    result = 0.0;  // a constant window
+                    break;
+                }
+                for (int b = lane; b < bins; b += 32) h[b] = 0u;
+                __syncwarp();
+                const double lo = mn, range = static_cast<double>(mx) - lo;
+                for (int i = lane; i < nwin; i += 32) {
+                    const double u = (static_cast<double>(x[i]) - lo) / (range + 1e-10) * (bins - 1e-6);
+                    long long b = static_cast<long long>(u);  // truncation, as .long()
+                    b = b < 0 ? 0 : (b > bins - 1 ? bins - 1 : b);
+                    atomicAdd(&h[b], 1u);
+                }
+                __syncwarp();
+                for (int b = lane; b < bins; b += 32) {
+                    if (h[b] > 0u) {
+                        const double p = fmax(static_cast<double>(h[b]) / n, 1e-10);
+                        a0 -= p * log(p);
+                    }
+                }
+                result = warp_sum_d(a0);
+                break;
+            }
+            case PB_FEAT_MEAN_N_ABS_MAX: {  // mean of the k largest |x| (ties by index, as topk)
+                const int k = min(static_cast<int>(param), nwin);
+                float prev = CUDART_INF_F;
+                int prev_i = -1;
+                double tot = 0.0;
+                for (int r = 0; r < k; ++r) {
+                    // the largest (|x|, -index) strictly below the previous pick
+                    float best = -1.f;
+                    int bi = -1;
+                    for (int i = lane; i < nwin; i += 32) {
+                        const float v = fabsf(x[i]);
+                        const bool below = v < prev || (v == prev && i > prev_i);
+                        if (below && (bi < 0 || v > best)) {
+                            best = v;
+                            bi = i;
+                        }
+                    }
+                    for (int off = 16; off > 0; off >>= 1) {
+                        const float ov = __shfl_down_sync(0xffffffffu, best, off);
+                        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                        if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
+                            best = ov;
+                            bi = oi;
+                        }
+                    }
+                    prev = __shfl_sync(0xffffffffu, best, 0);
+                    prev_i = __shfl_sync(0xffffffffu, bi, 0);
+                    tot += static_cast<double>(prev);
+                }
+                result = tot / k;
+                break;
+            }
+            case PB_FEAT_BENFORD: {  // Pearson correlation of first-digit frequencies with Benford's law
+                unsigned cnt[9];
+#pragma unroll
+                for (int dgt = 0; dgt < 9; ++dgt) cnt[dgt] = 0u;
+                for (int i = lane; i < nwin; i += 32) {
+                    const double v = fabs(static_cast<double>(x[i]));
+                    if (v > 0.0) {
+                        const double fl = floor(log10(v));
+                        const long long dg = static_cast<long long>(floor(v / pow(10.0, fl)));
+                        if (dg >= 1 && dg <= 9) {
+#pragma unroll
+                            for (int dgt = 0; dgt < 9; ++dgt) cnt[dgt] += (dg == dgt + 1) ? 1u : 0u;
+                        }
+                    }
+                }
+                double f[9], tot = 0.0;
+#pragma unroll
+                for (int dgt = 0; dgt < 9; ++dgt) {
+                    unsigned c = cnt[dgt];
+                    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+                    f[dgt] = static_cast<double>(c);
+                    tot += f[dgt];
+                }
+                double fm = 0.0, bm = 0.0, b[9];
+#pragma unroll
+                for (int dgt = 0; dgt < 9; ++dgt) {
+                    f[dgt] /= tot + 1e-10;
+                    fm += f[dgt];
+                    b[dgt] = log10(1.0 + 1.0 / (dgt + 1));
+                    bm += b[dgt];
+                }
+                fm /= 9.0;
+                bm /= 9.0;
+                double sfb = 0.0, sff = 0.0, sbb = 0.0;
+#pragma unroll
+                for (int dgt = 0; dgt < 9; ++dgt) {
+                    sfb += (f[dgt] - fm) * (b[dgt] - bm);
+                    sff += (f[dgt] - fm) * (f[dgt] - fm);
+                    sbb += (b[dgt] - bm) * (b[dgt] - bm);
+                }
+                // unbiased (n - 1 = 8) standard deviations, as torch.std
+                const double corr = sfb / (sqrt(sff / 8.0) * sqrt(sbb / 8.0) * 9.0 + 1e-10);
+                result = tot >= 10.0 ? corr : 0.0;
+                break;
+            }
             case PB_FEAT_C3:
             case PB_FEAT_TIME_REVERSAL: {
                 const int lag = static_cast<int>(param);
@@ -698,6 +829,10 @@ int validate_args(const pb_solve_args* a, bool user_system)
             return PB_EINVAL;
         if (kind == PB_FEAT_CID_CE && !(prm == 0.0 || prm == 1.0)) return PB_EINVAL;
         if (kind == PB_FEAT_INDEX_MASS_QUANTILE && !(prm >= 0.0 && prm <= 1.0)) return PB_EINVAL;
+        if (kind == PB_FEAT_BINNED_ENTROPY && !(prm >= 1.0 && prm <= 256.0 && prm == static_cast<double>(static_cast<int>(prm))))
+            return PB_EINVAL;
+        if (kind == PB_FEAT_MEAN_N_ABS_MAX && !(prm >= 1.0 && prm <= 64.0 && prm == static_cast<double>(static_cast<int>(prm))))
+            return PB_EINVAL;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }

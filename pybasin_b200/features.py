@@ -65,6 +65,11 @@ FEATURE_KINDS: dict[str, int] = {
     "index_mass_quantile": L.FEAT_INDEX_MASS_QUANTILE,
     "longest_strike_above_mean": L.FEAT_LONGEST_STRIKE_ABOVE,
     "longest_strike_below_mean": L.FEAT_LONGEST_STRIKE_BELOW,
+    "has_duplicate_max": L.FEAT_HAS_DUP_MAX,
+    "has_duplicate_min": L.FEAT_HAS_DUP_MIN,
+    "binned_entropy": L.FEAT_BINNED_ENTROPY,
+    "mean_n_absolute_max": L.FEAT_MEAN_N_ABS_MAX,
+    "benford_correlation": L.FEAT_BENFORD,
 }
 
 #: Features whose ``attr`` parameter selects the kernel kind: name -> (kinds by
@@ -93,6 +98,8 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_LARGE_STD: ("r", 0.25),
     L.FEAT_SYMMETRY_LOOKING: ("r", 0.1),
     L.FEAT_INDEX_MASS_QUANTILE: ("q", 0.5),
+    L.FEAT_BINNED_ENTROPY: ("max_bins", 10.0),
+    L.FEAT_MEAN_N_ABS_MAX: ("number_of_maxima", 1.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).

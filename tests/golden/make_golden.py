@@ -154,6 +154,11 @@ def _features(ref: Path) -> None:
         **{f"index_mass_quantile_{q}": lo.index_mass_quantile(x, q).numpy() for q in (0.1, 0.5, 0.9)},
         "longest_strike_above_mean": pat.longest_strike_above_mean(x).numpy(),
         "longest_strike_below_mean": pat.longest_strike_below_mean(x).numpy(),
+        "has_duplicate_max": bo.has_duplicate_max(x).numpy(),
+        "has_duplicate_min": bo.has_duplicate_min(x).numpy(),
+        **{f"binned_entropy_{b}": ec.binned_entropy(x, b).numpy() for b in (10, 37)},
+        **{f"mean_n_absolute_max_{k}": st.mean_n_absolute_max(x, k).numpy() for k in (1, 3, 7)},
+        "benford_correlation": ad.benford_correlation(x).numpy(),
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

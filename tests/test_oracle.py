@@ -141,6 +141,12 @@ def test_oracle_matches_reference_scipy_trajectories():
         *[(f"index_mass_quantile_{q}", 51, q) for q in (0.1, 0.5, 0.9)],
         ("longest_strike_above_mean", 52, 0.0),
         ("longest_strike_below_mean", 53, 0.0),
+        ("has_duplicate_max", 54, 0.0),
+        ("has_duplicate_min", 55, 0.0),
+        ("binned_entropy_10", 56, 10.0),
+        ("binned_entropy_37", 56, 37.0),
+        *[(f"mean_n_absolute_max_{k}", 57, float(k)) for k in (1, 3, 7)],
+        ("benford_correlation", 58, 0.0),
     ],
 )
 def test_oracle_window_features_match_reference_calculators(name, kind, param):
@@ -149,11 +155,12 @@ def test_oracle_window_features_match_reference_calculators(name, kind, param):
     want = g[name]
     got = np.array([[O.window_feature(kind, param, x[:, b, s]) for s in range(x.shape[2])] for b in range(x.shape[1])])
     # count_above / count_below / ratio_beyond_r_sigma: the reference averages a
-    # boolean mask in FP32 (.float().mean()), and divides the extreme locations
-    # as FP32 (idx.float() / n): exact to FP32 rounding only.  The FFT coefficients
+    # boolean mask in FP32 (.float().mean()), divides the extreme locations as FP32
+    # (idx.float() / n) and counts bins and digits in FP32 one-hot sums (binned
+    # entropy, Benford): exact to FP32 rounding only.  The FFT coefficients
     # come from torch's FFT (another summation order): 1e-10 of the window's scale.
     fp32 = name.startswith(("count_above_", "count_below_", "ratio_beyond", "first_location", "last_location",
-                            "index_mass_quantile"))
+                            "index_mass_quantile", "binned_entropy", "benford"))
     tol = 2e-7 if fp32 else 1e-12
     atol = 1e-12
     if name.startswith("fft_coefficient_angle"):

@@ -452,9 +452,13 @@ MORE_FEATS = [(0, k, float(c)) for k in (L.FEAT_FFT_REAL, L.FEAT_FFT_IMAG, L.FEA
     (0, L.FEAT_INDEX_MASS_QUANTILE, 0.5), (0, L.FEAT_LONGEST_STRIKE_ABOVE, 0.0),
     (1, L.FEAT_LONGEST_STRIKE_BELOW, 0.0),
 ]
+# fourth group (the window pass takes at most 32 columns per call)
+EXTRA_FEATS = [(0, L.FEAT_HAS_DUP_MAX, 0.0), (1, L.FEAT_HAS_DUP_MIN, 0.0), (0, L.FEAT_BINNED_ENTROPY, 10.0),
+               (1, L.FEAT_BINNED_ENTROPY, 37.0), (0, L.FEAT_MEAN_N_ABS_MAX, 1.0), (0, L.FEAT_MEAN_N_ABS_MAX, 7.0),
+               (0, L.FEAT_BENFORD, 0.0), (1, L.FEAT_BENFORD, 0.0)]
 LOCATION_KINDS = {L.FEAT_FIRST_LOC_MAX, L.FEAT_FIRST_LOC_MIN, L.FEAT_LAST_LOC_MAX, L.FEAT_LAST_LOC_MIN,
                   L.FEAT_INDEX_MASS_QUANTILE}
-FLAG_KINDS = {L.FEAT_LARGE_STD, L.FEAT_SYMMETRY_LOOKING}  # 1 / 0 decisions on a threshold
+FLAG_KINDS = {L.FEAT_LARGE_STD, L.FEAT_SYMMETRY_LOOKING, L.FEAT_HAS_DUP_MAX, L.FEAT_HAS_DUP_MIN}  # 1 / 0 decisions
 RUN_KINDS = {L.FEAT_LONGEST_STRIKE_ABOVE, L.FEAT_LONGEST_STRIKE_BELOW}
 
 
@@ -508,6 +512,35 @@ def test_frequency_trend_location_features_match_oracle(dense, precision):
             scale = np.abs(w[:, c]).max() + 1e-12
             np.testing.assert_allclose(g[:, c], w[:, c], rtol=tol, atol=tol * 1e-2 * scale,
                                        err_msg=f"col {c} kind {kind}")
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+def test_entropy_duplicate_benford_features_match_oracle(precision):
+    """Binned entropy, duplicate extremes, mean of the n largest |x| and the Benford
+    correlation from the window pass against the oracle (the short horizon of the
+    wider-set test).  Bin and first-digit counts can move by a sample whose value
+    sits within rounding of a bin edge or a power of ten, so entropy and Benford
+    compare to 1e-2; the duplicate flags are exact decisions on FP32-stored
+    samples (the oracle's FP64 trajectory rarely repeats a value)."""
+    case = DUFFING
+    y0 = seeded_ics(case, 200, seed=13).double().numpy()
+    save = np.asarray(torch.linspace(0.0, 30.0, 1501, dtype=torch.float32).double())
+    wb = int(np.nonzero(save >= 20.0)[0][0])
+    rtol = case.rtol if precision == L.PREC_FP64 else 1e-6
+    want = O.solve_batch(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), min(rtol, 1e-8), 1e-10,
+                         win_begin=wb, features=EXTRA_FEATS)
+    got = gpu_solve(case.oracle_sys, y0, np.array([case.params]), save, (0.0, 30.0), min(rtol, 1e-8), 1e-10,
+                    win_begin=wb, features=EXTRA_FEATS, precision=precision)
+    assert (got["status"] == 0).all()
+    g, w = got["features"], want["features"]
+    for c, (_, kind, _) in enumerate(EXTRA_FEATS):
+        if kind in (L.FEAT_HAS_DUP_MAX, L.FEAT_HAS_DUP_MIN):
+            assert set(np.unique(g[:, c])) <= {0.0, 1.0}
+            assert (g[:, c] != w[:, c]).mean() <= 0.1, (c, kind)
+        elif kind == L.FEAT_MEAN_N_ABS_MAX:
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=2e-4 if precision == L.PREC_FP64 else 2e-3)
+        else:
+            np.testing.assert_allclose(g[:, c], w[:, c], rtol=1e-2, atol=1e-2, err_msg=f"col {c} kind {kind}")
 
 
 def test_wider_features_through_the_extractor_names():
