@@ -120,12 +120,27 @@ typedef enum {
        mean_n_absolute_max (number_of_maxima <= 64; torch_features_statistical.py:166-172),
        benford_correlation (torch_features_advanced.py:21-81) */
     PB_FEAT_HAS_DUP_MAX = 54, PB_FEAT_HAS_DUP_MIN = 55, PB_FEAT_BINNED_ENTROPY = 56,
-    PB_FEAT_MEAN_N_ABS_MAX = 57, PB_FEAT_BENFORD = 58
+    PB_FEAT_MEAN_N_ABS_MAX = 57, PB_FEAT_BENFORD = 58,
+    /* repeated values over the whole window, from the sorted window (at most
+       PB_SORTED_WINDOW_MAX samples): has_duplicate (torch_features_boolean.py:11-20),
+       percentage_of_reoccurring_datapoints_to_all_datapoints, percentage_of_reoccurring_
+       values_to_all_values, sum_of_reoccurring_data_points, sum_of_reoccurring_values,
+       ratio_value_number_to_time_series_length (torch_features_reocurrance.py:10-163);
+       then has_variance_larger_than_standard_deviation (torch_features_boolean.py:37-41)
+       and count_value (value, compared in FP32 like the stored window;
+       torch_features_count.py:42-45) */
+    PB_FEAT_HAS_DUPLICATE = 59, PB_FEAT_PCT_REOCCURRING_POINTS = 60, PB_FEAT_PCT_REOCCURRING_VALUES = 61,
+    PB_FEAT_SUM_REOCCURRING_POINTS = 62, PB_FEAT_SUM_REOCCURRING_VALUES = 63, PB_FEAT_RATIO_UNIQUE_VALUES = 64,
+    PB_FEAT_VAR_LARGER_THAN_STD = 65, PB_FEAT_COUNT_VALUE = 66
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_BENFORD
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..58): the
+#define PB_FEAT_LAST_KIND PB_FEAT_COUNT_VALUE
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..66): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
+/* kinds 59..64 sort the window in shared memory: a request with more window
+   samples than this returns PB_EUNSUPPORTED */
+#define PB_FEAT_IS_SORTED(k) ((k) >= PB_FEAT_HAS_DUPLICATE && (k) <= PB_FEAT_RATIO_UNIQUE_VALUES)
+#define PB_SORTED_WINDOW_MAX 32768
 
 /* ---- per-trajectory status written to status_out ---- */
 typedef enum {

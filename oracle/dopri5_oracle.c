@@ -136,6 +136,14 @@ static int cmp_double(const void *a, const void *b)
     return (x > y) - (x < y);
 }
 
+/* ascending with every NaN after the numbers (the order of torch.sort) */
+static int cmp_double_nan_last(const void *a, const void *b)
+{
+    double x = *(const double *)a, y = *(const double *)b;
+    if (isnan(x) || isnan(y)) return (isnan(x) != 0) - (isnan(y) != 0);
+    return (x > y) - (x < y);
+}
+
 static double window_feature(int feat, double param, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
@@ -418,6 +426,45 @@ static double window_feature(int feat, double param, const double *w, int n, dou
             a += feat == ORACLE_F_C3 ? x0 * x1 * x2 : x2 * x2 * x1 - x1 * x0 * x0;
         }
         return a / m;
+    }
+    /* torch_features_boolean.py:11-20 and torch_features_reocurrance.py:10-163: the
+       window sorted ascending (NaN last, as torch.sort), then runs of equal
+       neighbours; NaN equals nothing, so each NaN is a value of its own */
+    case ORACLE_F_HAS_DUPLICATE: case ORACLE_F_PCT_REOCCURRING_POINTS: case ORACLE_F_PCT_REOCCURRING_VALUES:
+    case ORACLE_F_SUM_REOCCURRING_POINTS: case ORACLE_F_SUM_REOCCURRING_VALUES: case ORACLE_F_RATIO_UNIQUE_VALUES: {
+        memcpy(scratch, w, sizeof(double) * (size_t)n);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double_nan_last);
+        double dups = 0.0, in_runs = 0.0, run_starts = 0.0, sum_in_runs = 0.0, sum_run_starts = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const int eq_prev = i > 0 && scratch[i] == scratch[i - 1];
+            const int eq_next = i + 1 < n && scratch[i] == scratch[i + 1];
+            dups += eq_prev;
+            if (eq_prev || eq_next) {
+                in_runs += 1.0;
+                sum_in_runs += scratch[i];
+            }
+            if (eq_next && !eq_prev) {
+                run_starts += 1.0;
+                sum_run_starts += scratch[i];
+            }
+        }
+        switch (feat) {
+        case ORACLE_F_HAS_DUPLICATE: return dups > 0.0 ? 1.0 : 0.0;
+        case ORACLE_F_PCT_REOCCURRING_POINTS: return run_starts / ((n - dups) + 1e-10);
+        case ORACLE_F_PCT_REOCCURRING_VALUES: return n <= 1 ? 0.0 : in_runs / n;
+        /* the reference sums sorted values times a 0/1 mask: a NaN anywhere gives NaN */
+        case ORACLE_F_SUM_REOCCURRING_POINTS: return any_nan ? NAN : sum_in_runs;
+        case ORACLE_F_SUM_REOCCURRING_VALUES: return any_nan ? NAN : sum_run_starts;
+        default: return (n - dups) / n;
+        }
+    }
+    /* torch_features_boolean.py:37-41 */
+    case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
+    /* torch_features_count.py:42-45 */
+    case ORACLE_F_COUNT_VALUE: {
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += w[i] == param;
+        return c;
     }
     default: return NAN;
     }

@@ -41,6 +41,13 @@ enum {
        mean_n_absolute_max (number_of_maxima), benford_correlation */
     ORACLE_F_HAS_DUP_MAX = 54, ORACLE_F_HAS_DUP_MIN = 55, ORACLE_F_BINNED_ENTROPY = 56,
     ORACLE_F_MEAN_N_ABS_MAX = 57, ORACLE_F_BENFORD = 58,
+    /* has_duplicate, percentage_of_reoccurring_datapoints_to_all_datapoints,
+       percentage_of_reoccurring_values_to_all_values, sum_of_reoccurring_data_points,
+       sum_of_reoccurring_values, ratio_value_number_to_time_series_length,
+       has_variance_larger_than_standard_deviation, count_value (value) */
+    ORACLE_F_HAS_DUPLICATE = 59, ORACLE_F_PCT_REOCCURRING_POINTS = 60, ORACLE_F_PCT_REOCCURRING_VALUES = 61,
+    ORACLE_F_SUM_REOCCURRING_POINTS = 62, ORACLE_F_SUM_REOCCURRING_VALUES = 63, ORACLE_F_RATIO_UNIQUE_VALUES = 64,
+    ORACLE_F_VAR_LARGER_THAN_STD = 65, ORACLE_F_COUNT_VALUE = 66,
 };
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };

@@ -91,6 +91,10 @@ FEAT_CID_CE, FEAT_C3, FEAT_TIME_REVERSAL = 45, 46, 47
 FEAT_SPKT_WELCH, FEAT_LARGE_STD, FEAT_SYMMETRY_LOOKING = 48, 49, 50
 FEAT_INDEX_MASS_QUANTILE, FEAT_LONGEST_STRIKE_ABOVE, FEAT_LONGEST_STRIKE_BELOW = 51, 52, 53
 FEAT_HAS_DUP_MAX, FEAT_HAS_DUP_MIN, FEAT_BINNED_ENTROPY, FEAT_MEAN_N_ABS_MAX, FEAT_BENFORD = 54, 55, 56, 57, 58
+FEAT_HAS_DUPLICATE, FEAT_PCT_REOCCURRING_POINTS, FEAT_PCT_REOCCURRING_VALUES = 59, 60, 61
+FEAT_SUM_REOCCURRING_POINTS, FEAT_SUM_REOCCURRING_VALUES, FEAT_RATIO_UNIQUE_VALUES = 62, 63, 64
+FEAT_VAR_LARGER_THAN_STD, FEAT_COUNT_VALUE = 65, 66
+SORTED_WINDOW_MAX = 32768  # PB_SORTED_WINDOW_MAX: window samples of the sorted kinds 59..64
 
 TRAJ_OK = 0
 TRAJ_MAX_STEPS = 1

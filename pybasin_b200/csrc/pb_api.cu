@@ -27,6 +27,8 @@ struct MedianPlan {
     int n_peak_cols;
     int peak_cap;
     double* peaks_out;               // (n_traj, n_peak_cols, peak_cap) or NULL
+    int n_sorted;                    // window columns of the sorted kinds (PB_FEAT_IS_SORTED)
+    int sorted_m[PB_MAX_FEATURES];   // their window column indices m
 };
 
 __device__ __forceinline__ uint32_t float_key(float f)
@@ -99,6 +101,7 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
     const int64_t traj = row / plan.n_med;
     const int m = static_cast<int>(row - traj * plan.n_med);
     const int col = plan.col[m], kind = plan.kind[m];
+    if (PB_FEAT_IS_SORTED(kind)) return;  // warp-uniform; k_window_sorted writes these
     const double param = plan.param[m];
     const double n = static_cast<double>(nwin);
     double result = CUDART_NAN;
@@ -542,10 +545,122 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = warp_sum_d(a0) / static_cast<double>(m3);
                 break;
             }
+            case PB_FEAT_VAR_LARGER_THAN_STD: {  // population std > 1, as 1 / 0
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                }
+                result = sqrt(warp_sum_d(a0) / n) > 1.0 ? 1.0 : 0.0;
+                break;
+            }
+            case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
+                const float v = static_cast<float>(param);
+                for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
+                result = warp_sum_d(a0);
+                break;
+            }
             default: break;
         }
     }
     if (lane == 0) out[traj * n_features + col] = result;
+}
+
+// Repeated values over the whole window (kinds 59..64): one block per (trajectory,
+// sorted column) sorts that column's window in shared memory, as order-preserving
+// keys padded to a power of two with all-ones keys (after every number), by a
+// bitonic network, then counts runs of equal neighbours.  Equality is the float
+// comparison, so NaN equals nothing and -0 equals +0, as in torch; the block reads
+// only the first nwin sorted keys.
+__global__ void __launch_bounds__(256) k_window_sorted(const float* __restrict__ win, int nwin, int pow2,
+                                                       MedianPlan plan, double* __restrict__ out, int n_features)
+{
+    extern __shared__ uint32_t keys[];  // pow2 entries
+    __shared__ double red_d[2][8];
+    __shared__ unsigned red_u[3][8];
+    const int64_t blk = blockIdx.x;
+    const int64_t traj = blk / plan.n_sorted;
+    const int m = plan.sorted_m[blk - traj * plan.n_sorted];
+    const float* x = win + (traj * plan.n_med + m) * static_cast<int64_t>(nwin);
+    int nan_seen = 0;
+    for (int i = threadIdx.x; i < pow2; i += blockDim.x) {
+        uint32_t k = 0xffffffffu;
+        if (i < nwin) {
+            const float v = x[i];
+            nan_seen |= isnan(v) ? 1 : 0;
+            k = float_key(v);
+        }
+        keys[i] = k;
+    }
+    const int any_nan = __syncthreads_or(nan_seen);
+    const int half = pow2 >> 1;
+    for (int k = 2; k <= pow2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int p = threadIdx.x; p < half; p += blockDim.x) {
+                const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));  // bit j of i clear
+                const int l = i | j;
+                const uint32_t a = keys[i], c = keys[l];
+                if ((a > c) == ((i & k) == 0)) {
+                    keys[i] = c;
+                    keys[l] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    unsigned dups = 0, in_runs = 0, starts = 0;
+    double s_runs = 0.0, s_starts = 0.0;
+    for (int i = threadIdx.x; i < nwin; i += blockDim.x) {
+        const float v = key_float(keys[i]);
+        const bool eq_prev = i > 0 && key_float(keys[i - 1]) == v;
+        const bool eq_next = i + 1 < nwin && key_float(keys[i + 1]) == v;
+        dups += eq_prev ? 1u : 0u;
+        if (eq_prev || eq_next) {
+            ++in_runs;
+            s_runs += static_cast<double>(v);
+        }
+        if (eq_next && !eq_prev) {
+            ++starts;
+            s_starts += static_cast<double>(v);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        dups += __shfl_xor_sync(0xffffffffu, dups, off);
+        in_runs += __shfl_xor_sync(0xffffffffu, in_runs, off);
+        starts += __shfl_xor_sync(0xffffffffu, starts, off);
+        s_runs += __shfl_xor_sync(0xffffffffu, s_runs, off);
+        s_starts += __shfl_xor_sync(0xffffffffu, s_starts, off);
+    }
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red_u[0][warp] = dups;
+        red_u[1][warp] = in_runs;
+        red_u[2][warp] = starts;
+        red_d[0][warp] = s_runs;
+        red_d[1][warp] = s_starts;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const int nw = static_cast<int>(blockDim.x >> 5);
+    double d = 0.0, r = 0.0, st = 0.0, sr = 0.0, ss = 0.0;
+    for (int w = 0; w < nw; ++w) {
+        d += red_u[0][w];
+        r += red_u[1][w];
+        st += red_u[2][w];
+        sr += red_d[0][w];
+        ss += red_d[1][w];
+    }
+    const double n = static_cast<double>(nwin);
+    double result;
+    switch (plan.kind[m]) {
+        case PB_FEAT_HAS_DUPLICATE: result = d > 0.0 ? 1.0 : 0.0; break;
+        case PB_FEAT_PCT_REOCCURRING_POINTS: result = st / ((n - d) + 1e-10); break;  // repeated values / distinct
+        case PB_FEAT_PCT_REOCCURRING_VALUES: result = nwin <= 1 ? 0.0 : r / n; break;   // samples in runs / N
+        // the reference sums sorted values times a 0/1 mask: a NaN anywhere gives NaN
+        case PB_FEAT_SUM_REOCCURRING_POINTS: result = any_nan ? CUDART_NAN : sr; break;
+        case PB_FEAT_SUM_REOCCURRING_VALUES: result = any_nan ? CUDART_NAN : ss; break;
+        default: result = (n - d) / n; break;  // PB_FEAT_RATIO_UNIQUE_VALUES
+    }
+    out[traj * n_features + plan.col[m]] = result;
 }
 
 // ---------------------------------------------------------------------------
@@ -772,7 +887,7 @@ static cudaError_t sort_by_probe(const pb_solve_args& a, const ScratchLayout& sl
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
 {
-    int m = 0, np = 0;
+    int m = 0, np = 0, ns = 0;
     for (int c = 0; c < a.n_features; ++c)
         if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
             if (plan) {
@@ -782,9 +897,12 @@ static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
                 plan->peak_idx[m] = a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS ? np : -1;
             }
             np += a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS;
+            if (plan && PB_FEAT_IS_SORTED(a.feat_kind[c])) plan->sorted_m[ns] = m;
+            ns += PB_FEAT_IS_SORTED(a.feat_kind[c]) ? 1 : 0;
             ++m;
         }
     if (plan) {
+        plan->n_sorted = ns;
         plan->n_med = m;
         plan->n_peak_cols = np;
         plan->peak_cap = a.peak_cap;
@@ -833,6 +951,7 @@ int validate_args(const pb_solve_args* a, bool user_system)
             return PB_EINVAL;
         if (kind == PB_FEAT_MEAN_N_ABS_MAX && !(prm >= 1.0 && prm <= 64.0 && prm == static_cast<double>(static_cast<int>(prm))))
             return PB_EINVAL;
+        if (PB_FEAT_IS_SORTED(kind) && a->n_save - a->win_begin > PB_SORTED_WINDOW_MAX) return PB_EUNSUPPORTED;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }
@@ -959,6 +1078,23 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
             a.n_save - a.win_begin, plan, a.features_out, a.n_features);
         e = cudaGetLastError();
         if (e != cudaSuccess) return map_cuda(e);
+        if (plan.n_sorted > 0) {
+            const int nwin = a.n_save - a.win_begin;  // <= PB_SORTED_WINDOW_MAX (validated)
+            int pow2 = 1;
+            while (pow2 < nwin) pow2 <<= 1;
+            const int64_t sblocks = a.n_traj * plan.n_sorted;
+            if (sblocks > 0x7fffffffLL) return PB_EINVAL;
+            const size_t smem = static_cast<size_t>(pow2) * sizeof(uint32_t);
+            if (smem > 48 * 1024)
+                e = cudaFuncSetAttribute(k_window_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+            if (e != cudaSuccess) return map_cuda(e);
+            k_window_sorted<<<static_cast<unsigned>(sblocks), 256, smem, st>>>(
+                reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), nwin,
+                pow2, plan, a.features_out, a.n_features);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return map_cuda(e);
+        }
     }
     return PB_SUCCESS;
 }

@@ -70,6 +70,14 @@ FEATURE_KINDS: dict[str, int] = {
     "binned_entropy": L.FEAT_BINNED_ENTROPY,
     "mean_n_absolute_max": L.FEAT_MEAN_N_ABS_MAX,
     "benford_correlation": L.FEAT_BENFORD,
+    "has_duplicate": L.FEAT_HAS_DUPLICATE,
+    "percentage_of_reoccurring_datapoints_to_all_datapoints": L.FEAT_PCT_REOCCURRING_POINTS,
+    "percentage_of_reoccurring_values_to_all_values": L.FEAT_PCT_REOCCURRING_VALUES,
+    "sum_of_reoccurring_data_points": L.FEAT_SUM_REOCCURRING_POINTS,
+    "sum_of_reoccurring_values": L.FEAT_SUM_REOCCURRING_VALUES,
+    "ratio_value_number_to_time_series_length": L.FEAT_RATIO_UNIQUE_VALUES,
+    "has_variance_larger_than_standard_deviation": L.FEAT_VAR_LARGER_THAN_STD,
+    "count_value": L.FEAT_COUNT_VALUE,
 }
 
 #: Features whose ``attr`` parameter selects the kernel kind: name -> (kinds by
@@ -100,6 +108,7 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_INDEX_MASS_QUANTILE: ("q", 0.5),
     L.FEAT_BINNED_ENTROPY: ("max_bins", 10.0),
     L.FEAT_MEAN_N_ABS_MAX: ("number_of_maxima", 1.0),
+    L.FEAT_COUNT_VALUE: ("value", 0.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).

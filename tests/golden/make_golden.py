@@ -16,8 +16,8 @@ used here) and writes:
   N=4000) as class indices plus class names, with the basin-stability counts of
   main_pendulum_case1.json / main_duffing_supervised.json / main_friction_case1.json.
 * ``features_reference.npz`` — outputs of the reference's own feature
-  calculators (src/pybasin/ts_torch/calculators/torch_features_statistical.py,
-  torch_features_pattern.py) on seeded random windows, to pin the statistics.
+  calculators (src/pybasin/ts_torch/calculators/*.py) on seeded random windows
+  (and a copy rounded to a 0.5 grid, so that values repeat), to pin the statistics.
 * ``rossler_network_reference.npz`` — the reference's 100-node / 400-edge graph
   (case_studies/rossler_network/rossler_network_topology.py) and the paper's
   basin-stability values per coupling K it tests against
@@ -85,6 +85,7 @@ def _features(ref: Path) -> None:
     from pybasin.ts_torch.calculators import torch_features_entropy_complexity as ec
     from pybasin.ts_torch.calculators import torch_features_frequency as fq
     from pybasin.ts_torch.calculators import torch_features_location as lo
+    from pybasin.ts_torch.calculators import torch_features_reocurrance as re
     from pybasin.ts_torch.calculators import torch_features_trend as tr
 
     g = torch.Generator().manual_seed(1234)
@@ -93,6 +94,11 @@ def _features(ref: Path) -> None:
     x[:, 3, 0] = 2.0  # constant row
     x[::2, 5, 1] = -x[::2, 5, 1]  # sign flips for crossings
     even = torch.randn(256, n_b, 2, generator=g, dtype=torch.float64)  # even length: lower median
+    # a window on a 0.5 grid, so values repeat (duplicate and reoccurrence features),
+    # with one NaN sample; and a scaled copy whose standard deviations straddle 1
+    rep = torch.round(x * 2.0) / 2.0
+    rep[7, 2, 1] = float("nan")
+    scaled = x * 0.35
     res = {
         "x": x.numpy(),
         "x_even": even.numpy(),
@@ -159,6 +165,23 @@ def _features(ref: Path) -> None:
         **{f"binned_entropy_{b}": ec.binned_entropy(x, b).numpy() for b in (10, 37)},
         **{f"mean_n_absolute_max_{k}": st.mean_n_absolute_max(x, k).numpy() for k in (1, 3, 7)},
         "benford_correlation": ad.benford_correlation(x).numpy(),
+        # repeated values (torch_features_boolean.py, torch_features_reocurrance.py,
+        # torch_features_count.py)
+        "x_rep": rep.numpy(),
+        "x_scaled": scaled.numpy(),
+        "has_duplicate": bo.has_duplicate(x).numpy(),
+        "rep_has_duplicate": bo.has_duplicate(rep).numpy(),
+        "rep_percentage_of_reoccurring_datapoints_to_all_datapoints":
+            re.percentage_of_reoccurring_datapoints_to_all_datapoints(rep).numpy(),
+        "rep_percentage_of_reoccurring_values_to_all_values":
+            re.percentage_of_reoccurring_values_to_all_values(rep).numpy(),
+        "rep_sum_of_reoccurring_data_points": re.sum_of_reoccurring_data_points(rep).numpy(),
+        "rep_sum_of_reoccurring_values": re.sum_of_reoccurring_values(rep).numpy(),
+        "rep_ratio_value_number_to_time_series_length": re.ratio_value_number_to_time_series_length(rep).numpy(),
+        "ratio_value_number_to_time_series_length": re.ratio_value_number_to_time_series_length(x).numpy(),
+        **{f"rep_count_value_{v}": cn.count_value(rep, v).numpy() for v in (0.0, 0.5, -1.0)},
+        "scaled_has_variance_larger_than_standard_deviation":
+            bo.has_variance_larger_than_standard_deviation(scaled).numpy(),
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

@@ -175,6 +175,36 @@ def test_oracle_window_features_match_reference_calculators(name, kind, param):
     np.testing.assert_allclose(got, want, rtol=tol, atol=atol)
 
 
+@pytest.mark.parametrize(
+    "name, src, kind, param",
+    [
+        ("has_duplicate", "x", 59, 0.0),
+        ("rep_has_duplicate", "x_rep", 59, 0.0),
+        ("rep_percentage_of_reoccurring_datapoints_to_all_datapoints", "x_rep", 60, 0.0),
+        ("rep_percentage_of_reoccurring_values_to_all_values", "x_rep", 61, 0.0),
+        ("rep_sum_of_reoccurring_data_points", "x_rep", 62, 0.0),
+        ("rep_sum_of_reoccurring_values", "x_rep", 63, 0.0),
+        ("rep_ratio_value_number_to_time_series_length", "x_rep", 64, 0.0),
+        ("ratio_value_number_to_time_series_length", "x", 64, 0.0),
+        ("scaled_has_variance_larger_than_standard_deviation", "x_scaled", 65, 0.0),
+        *[(f"rep_count_value_{v}", "x_rep", 66, v) for v in (0.0, 0.5, -1.0)],
+    ],
+)
+def test_oracle_repeated_value_features_match_reference_calculators(name, src, kind, param):
+    """Duplicates and reoccurring values on a window rounded to a 0.5 grid (one
+    column holds a NaN, which equals nothing and turns both sums into NaN).  The
+    reference returns its counts and ratios in FP32 (.float() masks), so those
+    match to FP32 rounding; the sums run in the window's FP64."""
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g[src]
+    want = g[name]
+    got = np.array([[O.window_feature(kind, param, x[:, b, s]) for s in range(x.shape[2])] for b in range(x.shape[1])])
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)
+    if src == "x_rep":
+        assert np.isnan(want[2, 1]) == (kind in (62, 63))
+
+
 def test_oracle_quantile_even_length():
     g = np.load(GOLDEN / "features_reference.npz")
     x = g["x_even"]

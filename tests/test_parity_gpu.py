@@ -543,6 +543,60 @@ def test_entropy_duplicate_benford_features_match_oracle(precision):
             np.testing.assert_allclose(g[:, c], w[:, c], rtol=1e-2, atol=1e-2, err_msg=f"col {c} kind {kind}")
 
 
+SORTED_FEATS = [(0, L.FEAT_HAS_DUPLICATE, 0.0), (0, L.FEAT_PCT_REOCCURRING_POINTS, 0.0),
+                (0, L.FEAT_PCT_REOCCURRING_VALUES, 0.0), (0, L.FEAT_SUM_REOCCURRING_POINTS, 0.0),
+                (0, L.FEAT_SUM_REOCCURRING_VALUES, 0.0), (0, L.FEAT_RATIO_UNIQUE_VALUES, 0.0),
+                (0, L.FEAT_VAR_LARGER_THAN_STD, 0.0), (0, L.FEAT_COUNT_VALUE, 0.0)]
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("n_save", [2001, 20001])
+def test_repeated_value_features_on_identical_windows(precision, n_save):
+    """Duplicate and reoccurrence features from the sorted window pass against the
+    oracle evaluated on the kernel's own FP32 window (the save points written to
+    y_full are the samples the window holds, rounded to FP32 alike), so counts and
+    ratios must agree exactly and the sums to FP64 summation order.  Exponential
+    decay at four rates under relative error control: the slow one keeps distinct
+    normal floats (no repeats), the fast ones reach FP32 subnormals and then zero,
+    where values repeat in long runs.  20,001 saves put 16,001 samples in the window: a 64 KB sort in shared
+    memory."""
+    rng = np.random.default_rng(5)
+    n = 64
+    y0 = rng.uniform(0.5, 2.0, size=(n, 1))
+    rates = np.array([[-0.3], [-0.9], [-1.0], [-1.1]])
+    pidx = np.arange(n, dtype=np.int32) % 4
+    save = np.linspace(90.0, 140.0, n_save)
+    wb = int(np.nonzero(save >= 100.0)[0][0])
+    # relative error control all the way down (FP64: atol 0; the FP32 stages of the
+    # mixed kernel need a nonzero atol once the state underflows)
+    atol = 0.0 if precision == L.PREC_FP64 else 1e-30
+    got = gpu_solve(O.SYS_LINEAR, y0, rates, save, (0.0, 140.0), 1e-8, atol, precision=precision,
+                    win_begin=wb, features=SORTED_FEATS, param_index=pidx, keep_full=True)
+    assert (got["status"] == 0).all()
+    win = got["y"][wb:, :, 0].astype(np.float32).astype(np.float64)  # (n_win, n)
+    want = np.array([[O.window_feature(k, p, win[:, j]) for (_, k, p) in SORTED_FEATS] for j in range(n)])
+    g = got["features"]
+    sums = [c for c, (_, k, _) in enumerate(SORTED_FEATS)
+            if k in (L.FEAT_SUM_REOCCURRING_POINTS, L.FEAT_SUM_REOCCURRING_VALUES)]
+    exact = [c for c in range(len(SORTED_FEATS)) if c not in sums]
+    np.testing.assert_array_equal(g[:, exact], want[:, exact])
+    np.testing.assert_allclose(g[:, sums], want[:, sums], rtol=1e-12, atol=1e-300)
+    dup = g[:, 0]
+    # both regimes present (the mixed kernel's FP32 state settles into absolute-
+    # tolerance noise rather than underflowing, so fewer of its windows repeat)
+    assert (dup[pidx == 0] == 0.0).all()
+    assert (dup[pidx > 0] == 1.0).sum() >= (n // 4 if precision == L.PREC_FP64 else 1)
+
+
+def test_sorted_window_features_reject_oversized_windows():
+    """The sorted kinds hold the window in shared memory: more than 32,768 window
+    samples is refused before any launch."""
+    save = np.linspace(0.0, 1.0, L.SORTED_WINDOW_MAX + 2)
+    with pytest.raises(RuntimeError, match="unsupported"):
+        gpu_solve(O.SYS_LINEAR, np.ones((2, 1)), np.array([[-1.0]]), save, (0.0, 1.0), 1e-6, 1e-9,
+                  win_begin=0, features=[(0, L.FEAT_HAS_DUPLICATE, 0.0)])
+
+
 def test_wider_features_through_the_extractor_names():
     """FCParameters names and parameters as in the reference's settings (ts_torch/settings.py:223-355)."""
     from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
