@@ -131,10 +131,23 @@ typedef enum {
        torch_features_count.py:42-45) */
     PB_FEAT_HAS_DUPLICATE = 59, PB_FEAT_PCT_REOCCURRING_POINTS = 60, PB_FEAT_PCT_REOCCURRING_VALUES = 61,
     PB_FEAT_SUM_REOCCURRING_POINTS = 62, PB_FEAT_SUM_REOCCURRING_VALUES = 63, PB_FEAT_RATIO_UNIQUE_VALUES = 64,
-    PB_FEAT_VAR_LARGER_THAN_STD = 65, PB_FEAT_COUNT_VALUE = 66
+    PB_FEAT_VAR_LARGER_THAN_STD = 65, PB_FEAT_COUNT_VALUE = 66,
+    /* partial_autocorrelation (lag <= 64; Durbin-Levinson,
+       torch_features_autocorrelation.py:31-68), agg_autocorrelation over lags
+       1..maxlag (maxlag <= 128; f_agg mean / median / var in the kind,
+       torch_features_autocorrelation.py:72-97), energy_ratio_by_chunks
+       (num_segments, feat_param2 = segment_focus; torch_features_advanced.py:93-105),
+       count_in_range (min_val, feat_param2 = max_val, compared in FP32 like the
+       stored window; torch_features_count.py:37-39), change_quantiles (ql,
+       feat_param2 = qh; isabs and f_agg in the kind; torch_features_change.py:20-75,
+       113-140) */
+    PB_FEAT_PARTIAL_AUTOCORRELATION = 67, PB_FEAT_AGG_AUTOCORR_MEAN = 68, PB_FEAT_AGG_AUTOCORR_MEDIAN = 69,
+    PB_FEAT_AGG_AUTOCORR_VAR = 70, PB_FEAT_ENERGY_RATIO_BY_CHUNKS = 71, PB_FEAT_COUNT_IN_RANGE = 72,
+    PB_FEAT_CHANGE_QUANTILES_MEAN = 73, PB_FEAT_CHANGE_QUANTILES_VAR = 74,
+    PB_FEAT_CHANGE_QUANTILES_ABS_MEAN = 75, PB_FEAT_CHANGE_QUANTILES_ABS_VAR = 76
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_COUNT_VALUE
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..66): the
+#define PB_FEAT_LAST_KIND PB_FEAT_CHANGE_QUANTILES_ABS_VAR
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..76): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window
@@ -234,6 +247,8 @@ typedef struct pb_solve_args {
     double* peaks_out;
     int32_t peak_cap;
     int32_t _pad3;
+    /* second parameter of the two-parameter window kinds (segment_focus, max_val, qh) */
+    double feat_param2[PB_MAX_FEATURES];
 } pb_solve_args;
 
 /* Where the save points of the feature window are evaluated. */

@@ -144,7 +144,7 @@ static int cmp_double_nan_last(const void *a, const void *b)
     return (x > y) - (x < y);
 }
 
-static double window_feature(int feat, double param, const double *w, int n, double *scratch)
+static double window_feature(int feat, double param, double param2, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
     double sum = 0.0, mx = -INFINITY, mn = INFINITY;
@@ -458,6 +458,110 @@ static double window_feature(int feat, double param, const double *w, int n, dou
         default: return (n - dups) / n;
         }
     }
+    /* torch_features_autocorrelation.py:31-68: lag-k autocorrelations of the centred
+       window over its lag-0 sum (the reference's zero-padded FFT gives the same
+       linear sums), then the Durbin-Levinson recursion with its +1e-10 guard */
+    case ORACLE_F_PARTIAL_AUTOCORRELATION: {
+        const int lag = (int)param;
+        if (lag == 0) return 1.0;
+        const int maxlag = lag < n - 1 ? lag : n - 1;
+        if (maxlag < 1) return 0.0;
+        double acf[ORACLE_MAX_ACF_LAG + 1], phi[ORACLE_MAX_ACF_LAG + 1], prev[ORACLE_MAX_ACF_LAG + 1];
+        if (maxlag > ORACLE_MAX_ACF_LAG) return NAN;
+        for (int k = 1; k <= maxlag; ++k) {
+            double r = 0.0;
+            for (int i = 0; i + k < n; ++i) r += (w[i] - mean) * (w[i + k] - mean);
+            acf[k] = r / (m2 + 1e-10);
+        }
+        phi[1] = acf[1];
+        for (int k = 2; k <= maxlag; ++k) {
+            double num = acf[k], den = 1.0;
+            for (int j = 1; j < k; ++j) {
+                num -= phi[j] * acf[k - j];
+                den -= phi[j] * acf[j];
+            }
+            const double pk = num / (den + 1e-10);
+            for (int j = 1; j < k; ++j) prev[j] = phi[j];
+            for (int j = 1; j < k; ++j) phi[j] = prev[j] - pk * prev[k - j];
+            phi[k] = pk;
+        }
+        return lag <= maxlag ? phi[lag] : 0.0;
+    }
+    /* torch_features_autocorrelation.py:72-97: mean, lower median or population
+       variance of the autocorrelations at lags 1..maxlag */
+    case ORACLE_F_AGG_AUTOCORR_MEAN: case ORACLE_F_AGG_AUTOCORR_MEDIAN: case ORACLE_F_AGG_AUTOCORR_VAR: {
+        const int ml = (int)param < n - 1 ? (int)param : n - 1;
+        if (ml < 1 || ml > n) return NAN;
+        double am = 0.0;
+        for (int k = 1; k <= ml; ++k) {
+            double r = 0.0;
+            for (int i = 0; i + k < n; ++i) r += (w[i] - mean) * (w[i + k] - mean);
+            scratch[k - 1] = r / (m2 + 1e-10);
+            am += scratch[k - 1];
+        }
+        am /= ml;
+        if (feat == ORACLE_F_AGG_AUTOCORR_MEAN) return am;
+        if (feat == ORACLE_F_AGG_AUTOCORR_VAR) {
+            double v = 0.0;
+            for (int k = 0; k < ml; ++k) v += (scratch[k] - am) * (scratch[k] - am);
+            return v / ml;
+        }
+        qsort(scratch, (size_t)ml, sizeof(double), cmp_double_nan_last);
+        return scratch[(ml - 1) / 2];
+    }
+    /* torch_features_advanced.py:93-105 */
+    case ORACLE_F_ENERGY_RATIO_BY_CHUNKS: {
+        const int ns = (int)param, focus = (int)param2;
+        const int size = ns > 0 ? n / ns : 0;
+        if (size == 0) return 0.0;
+        const long start = (long)focus * size;
+        const long end = start + size < n ? start + size : n;
+        double seg = 0.0;
+        for (long i = start; i < end; ++i) seg += w[i] * w[i];
+        return seg / (sq + 1e-10);
+    }
+    /* torch_features_count.py:37-39 */
+    case ORACLE_F_COUNT_IN_RANGE: {
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += (w[i] >= param && w[i] <= param2);
+        return c;
+    }
+    /* torch_features_change.py:20-75,113-140: changes between neighbours that both
+       lie in the corridor [quantile ql, quantile qh], their mean or population
+       variance (0 when no change qualifies; NaN in the window gives no corridor) */
+    case ORACLE_F_CHANGE_QUANTILES_MEAN: case ORACLE_F_CHANGE_QUANTILES_VAR:
+    case ORACLE_F_CHANGE_QUANTILES_ABS_MEAN: case ORACLE_F_CHANGE_QUANTILES_ABS_VAR: {
+        if (any_nan) return 0.0;
+        memcpy(scratch, w, sizeof(double) * (size_t)n);
+        qsort(scratch, (size_t)n, sizeof(double), cmp_double);
+        double qv[2];
+        for (int e = 0; e < 2; ++e) {
+            const double pos = (e == 0 ? param : param2) * (n - 1);
+            const int lo = (int)floor(pos), hi = lo + 1 < n ? lo + 1 : n - 1;
+            qv[e] = scratch[lo] + (scratch[hi] - scratch[lo]) * (pos - lo);
+        }
+        const int isabs = feat == ORACLE_F_CHANGE_QUANTILES_ABS_MEAN || feat == ORACLE_F_CHANGE_QUANTILES_ABS_VAR;
+        const int is_var = feat == ORACLE_F_CHANGE_QUANTILES_VAR || feat == ORACLE_F_CHANGE_QUANTILES_ABS_VAR;
+        double s1 = 0.0, cnt = 0.0;
+        for (int i = 1; i < n; ++i) {
+            if (!(w[i - 1] >= qv[0] && w[i - 1] <= qv[1] && w[i] >= qv[0] && w[i] <= qv[1])) continue;
+            const double d = isabs ? fabs(w[i] - w[i - 1]) : w[i] - w[i - 1];
+            s1 += d;
+            cnt += 1.0;
+        }
+        /* the reference's +1e-10 guard is added to an FP32 count (.float().sum()),
+           where it vanishes: the divisor is the count itself */
+        if (cnt == 0.0) return 0.0;
+        const double mu = s1 / cnt;
+        if (!is_var) return mu;
+        double v = 0.0;
+        for (int i = 1; i < n; ++i) {
+            if (!(w[i - 1] >= qv[0] && w[i - 1] <= qv[1] && w[i] >= qv[0] && w[i] <= qv[1])) continue;
+            const double d = isabs ? fabs(w[i] - w[i - 1]) : w[i] - w[i - 1];
+            v += (d - mu) * (d - mu);
+        }
+        return v / cnt;
+    }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
     /* torch_features_count.py:42-45 */
@@ -618,7 +722,8 @@ static int solve_one(const oracle_problem *pb, const double *y0, const double *p
         int state = pb->feat_state[f];
         for (int j = 0; j < nwin; ++j) w->scratch[nwin + j] = w->win[(size_t)j * dim + state];
         feat_out[f] = window_feature(pb->feat_kind[f], pb->feat_param ? pb->feat_param[f] : 0.0,
-                                     w->scratch + nwin, nwin, w->scratch);
+                                     pb->feat_param2 ? pb->feat_param2[f] : 0.0, w->scratch + nwin, nwin,
+                                     w->scratch);
     }
     return status;
 }
@@ -675,9 +780,14 @@ int oracle_solve_batch(const oracle_problem *pb, const double *y0s, int64_t n_tr
 /* Feature of one stored window (used to pin the statistics against the reference's calculators). */
 double oracle_window_feature(int kind, double param, const double *w, int n)
 {
+    return oracle_window_feature2(kind, param, 0.0, w, n);
+}
+
+double oracle_window_feature2(int kind, double param, double param2, const double *w, int n)
+{
     double *scratch = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
     if (!scratch) return NAN;
-    double v = window_feature(kind, param, w, n, scratch);
+    double v = window_feature(kind, param, param2, w, n, scratch);
     free(scratch);
     return v;
 }

@@ -48,7 +48,15 @@ enum {
     ORACLE_F_HAS_DUPLICATE = 59, ORACLE_F_PCT_REOCCURRING_POINTS = 60, ORACLE_F_PCT_REOCCURRING_VALUES = 61,
     ORACLE_F_SUM_REOCCURRING_POINTS = 62, ORACLE_F_SUM_REOCCURRING_VALUES = 63, ORACLE_F_RATIO_UNIQUE_VALUES = 64,
     ORACLE_F_VAR_LARGER_THAN_STD = 65, ORACLE_F_COUNT_VALUE = 66,
+    /* partial_autocorrelation (lag), agg_autocorrelation (maxlag; mean, median, var),
+       energy_ratio_by_chunks (num_segments, segment_focus), count_in_range (min_val,
+       max_val), change_quantiles (ql, qh; isabs x f_agg mean / var) */
+    ORACLE_F_PARTIAL_AUTOCORRELATION = 67, ORACLE_F_AGG_AUTOCORR_MEAN = 68, ORACLE_F_AGG_AUTOCORR_MEDIAN = 69,
+    ORACLE_F_AGG_AUTOCORR_VAR = 70, ORACLE_F_ENERGY_RATIO_BY_CHUNKS = 71, ORACLE_F_COUNT_IN_RANGE = 72,
+    ORACLE_F_CHANGE_QUANTILES_MEAN = 73, ORACLE_F_CHANGE_QUANTILES_VAR = 74,
+    ORACLE_F_CHANGE_QUANTILES_ABS_MEAN = 75, ORACLE_F_CHANGE_QUANTILES_ABS_VAR = 76,
 };
+#define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 
 enum { ORACLE_OK = 0, ORACLE_MAX_STEPS = 1, ORACLE_DT_UNDERFLOW = 2, ORACLE_UNBOUNDED = 3, ORACLE_NONFINITE = 4 };
 enum { ORACLE_EINVAL = -5, ORACLE_ENOMEM = -2 };
@@ -74,6 +82,7 @@ typedef struct {
     const int32_t *feat_kind;  /* (n_features,) */
     const double *feat_param;  /* (n_features,) or NULL */
     const oracle_aux *aux;
+    const double *feat_param2; /* (n_features,) second parameter of the two-parameter kinds, or NULL */
 } oracle_problem;
 
 int oracle_solve_batch(const oracle_problem *pb, const double *y0s, int64_t n_traj,
@@ -81,4 +90,5 @@ int oracle_solve_batch(const oracle_problem *pb, const double *y0s, int64_t n_tr
                        int32_t *status_out, double *y_final, double *y_full, int64_t *steps_out,
                        int64_t *accepted_out, int n_threads);
 double oracle_window_feature(int kind, double param, const double *w, int n);
+double oracle_window_feature2(int kind, double param, double param2, const double *w, int n);
 #endif

@@ -55,6 +55,7 @@ class _Problem(ctypes.Structure):
         ("feat_kind", ctypes.POINTER(ctypes.c_int32)),
         ("feat_param", ctypes.POINTER(ctypes.c_double)),
         ("aux", ctypes.POINTER(_Aux)),
+        ("feat_param2", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -78,6 +79,9 @@ def _load() -> ctypes.CDLL:
         lib = ctypes.CDLL(str(_LIB_PATH))
         lib.oracle_window_feature.restype = ctypes.c_double
         lib.oracle_window_feature.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
+        lib.oracle_window_feature2.restype = ctypes.c_double
+        lib.oracle_window_feature2.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                               ctypes.c_int]
         lib.oracle_solve_batch.restype = ctypes.c_int
         lib.oracle_solve_batch.argtypes = [
             ctypes.POINTER(_Problem),
@@ -125,7 +129,8 @@ def solve_batch(
     :param y0: ``(n_traj, dim)`` initial conditions.
     :param params: ``(n_rows, n_params)`` parameter table.
     :param param_index: ``(n_traj,)`` row of ``params`` per trajectory (default row 0).
-    :param features: output columns ``(state, kind, param)`` in output order.
+    :param features: output columns ``(state, kind, param)`` or ``(state, kind, param,
+        param2)`` in output order.
     :return: dict with ``features (n,F)``, ``status (n,)``, ``y_final (n,dim)``,
         ``steps``/``accepted`` ``(n,)`` and, with ``keep_full``, ``y (n_save,n,dim)``.
     """
@@ -138,6 +143,7 @@ def solve_batch(
     fs = np.ascontiguousarray([f[0] for f in feats] or [0], dtype=np.int32)
     fk = np.ascontiguousarray([f[1] for f in feats] or [0], dtype=np.int32)
     fp = np.ascontiguousarray([f[2] for f in feats] or [0.0], dtype=np.float64)
+    fp2 = np.ascontiguousarray([f[3] if len(f) > 3 else 0.0 for f in feats] or [0.0], dtype=np.float64)
     pidx = None if param_index is None else np.ascontiguousarray(param_index, dtype=np.int32)
     aux = None
     keep: list[object] = []
@@ -164,6 +170,7 @@ def solve_batch(
         fk.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
         fp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
         ctypes.pointer(aux) if aux is not None else None,
+        fp2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
     )
     out_f = np.empty((n, max(len(feats), 1)), dtype=np.float64)
     status = np.empty(n, dtype=np.int32)
@@ -193,11 +200,12 @@ def solve_batch(
     return res
 
 
-def window_feature(kind: int, param: float, w: np.ndarray) -> float:
-    """Feature ``kind`` of one stored window ``w`` (two-pass, as the reference's calculators)."""
+def window_feature(kind: int, param: float, w: np.ndarray, param2: float = 0.0) -> float:
+    """Feature ``kind`` of one stored window ``w`` (two-pass, as the reference's
+    calculators); ``param2`` is the second parameter of the two-parameter kinds."""
     lib = _load()
     w = np.ascontiguousarray(w, dtype=np.float64)
-    return float(lib.oracle_window_feature(kind, param, w.ctypes.data, w.shape[0]))
+    return float(lib.oracle_window_feature2(kind, param, param2, w.ctypes.data, w.shape[0]))
 
 
 def peak_values(w: np.ndarray, n: int) -> np.ndarray:

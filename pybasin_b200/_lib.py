@@ -94,6 +94,10 @@ FEAT_HAS_DUP_MAX, FEAT_HAS_DUP_MIN, FEAT_BINNED_ENTROPY, FEAT_MEAN_N_ABS_MAX, FE
 FEAT_HAS_DUPLICATE, FEAT_PCT_REOCCURRING_POINTS, FEAT_PCT_REOCCURRING_VALUES = 59, 60, 61
 FEAT_SUM_REOCCURRING_POINTS, FEAT_SUM_REOCCURRING_VALUES, FEAT_RATIO_UNIQUE_VALUES = 62, 63, 64
 FEAT_VAR_LARGER_THAN_STD, FEAT_COUNT_VALUE = 65, 66
+FEAT_PARTIAL_AUTOCORRELATION, FEAT_AGG_AUTOCORR_MEAN, FEAT_AGG_AUTOCORR_MEDIAN, FEAT_AGG_AUTOCORR_VAR = 67, 68, 69, 70
+FEAT_ENERGY_RATIO_BY_CHUNKS, FEAT_COUNT_IN_RANGE = 71, 72
+FEAT_CHANGE_QUANTILES_MEAN, FEAT_CHANGE_QUANTILES_VAR = 73, 74
+FEAT_CHANGE_QUANTILES_ABS_MEAN, FEAT_CHANGE_QUANTILES_ABS_VAR = 75, 76
 SORTED_WINDOW_MAX = 32768  # PB_SORTED_WINDOW_MAX: window samples of the sorted kinds 59..64
 
 TRAJ_OK = 0
@@ -165,6 +169,7 @@ class SolveArgs(ctypes.Structure):
         ("peaks_out", _c_vp),
         ("peak_cap", _c_i32),
         ("_pad3", _c_i32),
+        ("feat_param2", _c_dbl * MAX_FEATURES),
     ]
 
 

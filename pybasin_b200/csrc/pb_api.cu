@@ -23,6 +23,7 @@ struct MedianPlan {
     int col[PB_MAX_FEATURES];        // output column of window column m
     int kind[PB_MAX_FEATURES];       // its feature kind
     double param[PB_MAX_FEATURES];   // and parameter (q, t, n, lag, r)
+    double param2[PB_MAX_FEATURES];  // second parameter of the two-parameter kinds
     int peak_idx[PB_MAX_FEATURES];   // NUMBER_PEAKS columns: index among them (orbit data), else -1
     int n_peak_cols;
     int peak_cap;
@@ -92,7 +93,7 @@ __device__ __forceinline__ double warp_sum_d(double v)
 __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, int64_t n_traj, int nwin,
                                                 MedianPlan plan, double* __restrict__ out, int n_features)
 {
-    __shared__ unsigned hist[8][256];
+    __shared__ __align__(16) unsigned hist[8][256];  // per warp: radix bins, or 128 doubles
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
     if (row >= n_traj * plan.n_med) return;  // warp-uniform
@@ -553,6 +554,164 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = sqrt(warp_sum_d(a0) / n) > 1.0 ? 1.0 : 0.0;
                 break;
             }
+            case PB_FEAT_PARTIAL_AUTOCORRELATION:
+            case PB_FEAT_AGG_AUTOCORR_MEAN:
+            case PB_FEAT_AGG_AUTOCORR_MEDIAN:
+            case PB_FEAT_AGG_AUTOCORR_VAR: {
+                // autocorrelations acf[k] = sum d_i d_(i+k) / (sum d_i^2 + 1e-10) for k = 1..ml,
+                // one warp reduction per lag, kept in this warp's shared doubles
+                const bool pacf = kind == PB_FEAT_PARTIAL_AUTOCORRELATION;
+                const int want = static_cast<int>(param);
+                if (pacf && want == 0) {
+                    result = 1.0;
+                    break;
+                }
+                const int ml = min(want, nwin - 1);
+                if (ml < 1) {
+                    result = pacf ? 0.0 : CUDART_NAN;
+                    break;
+                }
+                double* hd = reinterpret_cast<double*>(h);  // acf[k] at hd[k - 1]; phi[k] at hd[63 + k]
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                }
+                const double m2 = warp_sum_d(a0);
+                for (int k = 1; k <= ml; ++k) {
+                    double r = 0.0;
+                    for (int i = lane; i + k < nwin; i += 32)
+                        r += (static_cast<double>(x[i]) - mean) * (static_cast<double>(x[i + k]) - mean);
+                    r = warp_sum_d(r);
+                    if (lane == 0) hd[k - 1] = r / (m2 + 1e-10);
+                }
+                __syncwarp();
+                if (pacf) {  // Durbin-Levinson on lane 0 (ml <= 63), the update in place by pairs (j, k - j)
+                    if (lane == 0) {
+                        double* phi = hd + 63;
+                        phi[1] = hd[0];
+                        for (int k = 2; k <= ml; ++k) {
+                            double num = hd[k - 1], den = 1.0;
+                            for (int j = 1; j < k; ++j) {
+                                num -= phi[j] * hd[k - j - 1];
+                                den -= phi[j] * hd[j - 1];
+                            }
+                            const double pk = num / (den + 1e-10);
+                            for (int j = 1, l = k - 1; j <= l; ++j, --l) {
+                                const double pj = phi[j], pl = phi[l];
+                                phi[j] = pj - pk * pl;
+                                if (l != j) phi[l] = pl - pk * pj;
+                            }
+                            phi[k] = pk;
+                        }
+                        result = want <= ml ? phi[want] : 0.0;
+                    }
+                    __syncwarp();
+                    break;
+                }
+                double sa = 0.0;
+                for (int k = lane; k < ml; k += 32) sa += hd[k];
+                const double am = warp_sum_d(sa) / ml;
+                if (kind == PB_FEAT_AGG_AUTOCORR_MEAN) {
+                    result = am;
+                } else if (kind == PB_FEAT_AGG_AUTOCORR_VAR) {  // population variance
+                    double v = 0.0;
+                    for (int k = lane; k < ml; k += 32) v += (hd[k] - am) * (hd[k] - am);
+                    result = warp_sum_d(v) / ml;
+                } else {  // lower median: the value with at most (ml-1)/2 smaller and more not larger
+                    const int kk = (ml - 1) / 2;
+                    double med = CUDART_NAN;
+                    bool found = false;
+                    for (int c = lane; c < ml; c += 32) {
+                        const double v = hd[c];
+                        int less = 0, leq = 0;
+                        for (int q = 0; q < ml; ++q) {
+                            less += hd[q] < v ? 1 : 0;
+                            leq += hd[q] <= v ? 1 : 0;
+                        }
+                        if (less <= kk && kk < leq) {
+                            med = v;
+                            found = true;
+                        }
+                    }
+                    const unsigned b = __ballot_sync(0xffffffffu, found);
+                    med = __shfl_sync(0xffffffffu, med, b ? __ffs(b) - 1 : 0);
+                    result = b ? med : CUDART_NAN;
+                }
+                __syncwarp();
+                break;
+            }
+            case PB_FEAT_ENERGY_RATIO_BY_CHUNKS: {  // energy of chunk segment_focus of num_segments / total
+                const int ns = static_cast<int>(param);
+                const int size = nwin / ns;
+                if (size == 0) {
+                    result = 0.0;
+                    break;
+                }
+                const int64_t start = static_cast<int64_t>(plan.param2[m]) * size;
+                const int64_t end = min(start + size, static_cast<int64_t>(nwin));
+                for (int i = lane; i < nwin; i += 32) {
+                    const double v = static_cast<double>(x[i]);
+                    a0 += v * v;
+                    if (i >= start && i < end) a1 += v * v;
+                }
+                const double tot = warp_sum_d(a0);
+                result = warp_sum_d(a1) / (tot + 1e-10);
+                break;
+            }
+            case PB_FEAT_COUNT_IN_RANGE: {  // min_val <= x <= max_val, compared in the window's FP32
+                const float lo = static_cast<float>(param), hi = static_cast<float>(plan.param2[m]);
+                for (int i = lane; i < nwin; i += 32) a0 += (x[i] >= lo && x[i] <= hi) ? 1.0 : 0.0;
+                result = warp_sum_d(a0);
+                break;
+            }
+            case PB_FEAT_CHANGE_QUANTILES_MEAN:
+            case PB_FEAT_CHANGE_QUANTILES_VAR:
+            case PB_FEAT_CHANGE_QUANTILES_ABS_MEAN:
+            case PB_FEAT_CHANGE_QUANTILES_ABS_VAR: {
+                // changes between neighbours inside [quantile ql, quantile qh]: their mean or
+                // population variance over the count (0 if none; a NaN leaves no corridor)
+                bool nan_seen = false;
+                for (int i = lane; i < nwin; i += 32) nan_seen |= isnan(x[i]);
+                if (__any_sync(0xffffffffu, nan_seen)) {
+                    result = 0.0;
+                    break;
+                }
+                double qv[2];
+                for (int e = 0; e < 2; ++e) {
+                    const double pos = (e == 0 ? param : plan.param2[m]) * (nwin - 1);
+                    const int lo = static_cast<int>(floor(pos));
+                    const int hi = lo + 1 < nwin ? lo + 1 : nwin - 1;
+                    const double va = select_rank(x, nwin, static_cast<unsigned>(lo), h, lane);
+                    const double vb = hi == lo ? va : select_rank(x, nwin, static_cast<unsigned>(hi), h, lane);
+                    qv[e] = va + (vb - va) * (pos - lo);
+                }
+                const bool isabs = kind == PB_FEAT_CHANGE_QUANTILES_ABS_MEAN || kind == PB_FEAT_CHANGE_QUANTILES_ABS_VAR;
+                const bool is_var = kind == PB_FEAT_CHANGE_QUANTILES_VAR || kind == PB_FEAT_CHANGE_QUANTILES_ABS_VAR;
+                for (int i = lane + 1; i < nwin; i += 32) {
+                    const double p = static_cast<double>(x[i - 1]), c = static_cast<double>(x[i]);
+                    if (p >= qv[0] && p <= qv[1] && c >= qv[0] && c <= qv[1]) {
+                        a0 += isabs ? fabs(c - p) : c - p;
+                        a1 += 1.0;
+                    }
+                }
+                const double cnt = warp_sum_d(a1);
+                const double mu = warp_sum_d(a0) / cnt;
+                if (cnt == 0.0) {
+                    result = 0.0;
+                } else if (!is_var) {
+                    result = mu;
+                } else {
+                    for (int i = lane + 1; i < nwin; i += 32) {
+                        const double p = static_cast<double>(x[i - 1]), c = static_cast<double>(x[i]);
+                        if (p >= qv[0] && p <= qv[1] && c >= qv[0] && c <= qv[1]) {
+                            const double d = (isabs ? fabs(c - p) : c - p) - mu;
+                            a2 += d * d;
+                        }
+                    }
+                    result = warp_sum_d(a2) / cnt;
+                }
+                break;
+            }
             case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
                 const float v = static_cast<float>(param);
                 for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
@@ -894,6 +1053,7 @@ static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
                 plan->col[m] = c;
                 plan->kind[m] = a.feat_kind[c];
                 plan->param[m] = a.feat_param[c];
+                plan->param2[m] = a.feat_param2[c];
                 plan->peak_idx[m] = a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS ? np : -1;
             }
             np += a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS;
@@ -952,6 +1112,18 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_MEAN_N_ABS_MAX && !(prm >= 1.0 && prm <= 64.0 && prm == static_cast<double>(static_cast<int>(prm))))
             return PB_EINVAL;
         if (PB_FEAT_IS_SORTED(kind) && a->n_save - a->win_begin > PB_SORTED_WINDOW_MAX) return PB_EUNSUPPORTED;
+        const double prm2 = a->feat_param2[c];
+        const auto is_int = [](double v, double lo, double hi) {
+            return v >= lo && v <= hi && v == static_cast<double>(static_cast<int>(v));
+        };
+        if (kind == PB_FEAT_PARTIAL_AUTOCORRELATION && !is_int(prm, 0.0, 63.0)) return PB_EINVAL;
+        if (kind >= PB_FEAT_AGG_AUTOCORR_MEAN && kind <= PB_FEAT_AGG_AUTOCORR_VAR && !is_int(prm, 0.0, 128.0))
+            return PB_EINVAL;
+        if (kind == PB_FEAT_ENERGY_RATIO_BY_CHUNKS && !(is_int(prm, 1.0, 1e6) && is_int(prm2, 0.0, 1e6)))
+            return PB_EINVAL;
+        if (kind >= PB_FEAT_CHANGE_QUANTILES_MEAN && kind <= PB_FEAT_CHANGE_QUANTILES_ABS_VAR &&
+            !(prm >= 0.0 && prm <= 1.0 && prm2 >= 0.0 && prm2 <= 1.0))
+            return PB_EINVAL;
         if ((a->feat_kind[c] == PB_FEAT_SYNC_DEV) != (a->system == PB_SYS_ROSSLER_NET)) return PB_EUNSUPPORTED;
         n_cross += a->feat_kind[c] == PB_FEAT_CROSSINGS;
     }
@@ -1105,7 +1277,7 @@ using namespace pb;
 
 extern "C" {
 
-int32_t pb_abi_version(void) { return 100; }
+int32_t pb_abi_version(void) { return 101; }  // 101: pb_solve_args gained feat_param2
 
 const char* pb_error_string(int32_t s)
 {

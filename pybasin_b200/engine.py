@@ -25,6 +25,7 @@ class FeatureColumn:
     kind: int
     param: float = 0.0
     name: str = ""
+    param2: float = 0.0  # second parameter of the two-parameter window kinds
 
 
 @dataclass
@@ -121,6 +122,7 @@ def build_args(
         a.feat_state[i] = c.state
         a.feat_kind[i] = c.kind
         a.feat_param[i] = float(c.param)
+        a.feat_param2[i] = float(c.param2)
     a.features_out = _ptr(out.features)
     a.status_out = _ptr(out.status)
     a.y_final_out = _ptr(out.y_final)

@@ -78,7 +78,42 @@ FEATURE_KINDS: dict[str, int] = {
     "ratio_value_number_to_time_series_length": L.FEAT_RATIO_UNIQUE_VALUES,
     "has_variance_larger_than_standard_deviation": L.FEAT_VAR_LARGER_THAN_STD,
     "count_value": L.FEAT_COUNT_VALUE,
+    "partial_autocorrelation": L.FEAT_PARTIAL_AUTOCORRELATION,
 }
+
+#: Features with several parameters (FCParameters keys as in the reference's
+#: settings, src/pybasin/ts_torch/settings.py:263-346): name -> (defaults when
+#: the config gives None, or None if the parameters are required).
+FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
+    "agg_autocorrelation": [{"f_agg": "mean", "maxlag": 40}],
+    "energy_ratio_by_chunks": [{"num_segments": 10, "segment_focus": 0}],
+    "count_in_range": None,
+    "change_quantiles": None,
+}
+_AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
+                 "var": L.FEAT_AGG_AUTOCORR_VAR}
+_CHANGE_Q_KIND = {(False, "mean"): L.FEAT_CHANGE_QUANTILES_MEAN, (False, "var"): L.FEAT_CHANGE_QUANTILES_VAR,
+                  (True, "mean"): L.FEAT_CHANGE_QUANTILES_ABS_MEAN, (True, "var"): L.FEAT_CHANGE_QUANTILES_ABS_VAR}
+
+
+def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
+    """One column of a multi-parameter feature: its kind and the (param, param2) pair."""
+    name = _format_name(fname, p, state)
+    if fname == "agg_autocorrelation":  # torch_features_autocorrelation.py:72-97
+        f_agg = p.get("f_agg", "mean")
+        if f_agg not in _AGG_ACF_KIND:
+            raise ValueError(f"agg_autocorrelation: f_agg must be one of {sorted(_AGG_ACF_KIND)}, got {f_agg!r}")
+        return FeatureColumn(state, _AGG_ACF_KIND[f_agg], float(p.get("maxlag", 40)), name)
+    if fname == "energy_ratio_by_chunks":  # torch_features_advanced.py:93-105
+        return FeatureColumn(state, L.FEAT_ENERGY_RATIO_BY_CHUNKS, float(p.get("num_segments", 10)), name,
+                             float(p.get("segment_focus", 0)))
+    if fname == "count_in_range":  # torch_features_count.py:37-39
+        return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
+    # change_quantiles, torch_features_change.py:113-140
+    key = (bool(p.get("isabs", True)), p.get("f_agg", "mean"))
+    if key not in _CHANGE_Q_KIND:
+        raise ValueError(f"change_quantiles: f_agg must be 'mean' or 'var', got {key[1]!r}")
+    return FeatureColumn(state, _CHANGE_Q_KIND[key], float(p["ql"]), name, float(p["qh"]))
 
 #: Features whose ``attr`` parameter selects the kernel kind: name -> (kinds by
 #: attr, default attr, numeric parameter key or None, its default).
@@ -109,6 +144,7 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_BINNED_ENTROPY: ("max_bins", 10.0),
     L.FEAT_MEAN_N_ABS_MAX: ("number_of_maxima", 1.0),
     L.FEAT_COUNT_VALUE: ("value", 0.0),
+    L.FEAT_PARTIAL_AUTOCORRELATION: ("lag", 1.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).
@@ -143,6 +179,12 @@ def columns_for(config: dict[str, Any] | None, state: int) -> list[FeatureColumn
     if not config:
         return cols
     for fname, plist in config.items():
+        if fname in FEATURE_MULTI:
+            defaults = FEATURE_MULTI[fname]
+            if plist is None and defaults is None:
+                raise ValueError(f"feature '{fname}' needs its parameters")
+            cols.extend(_multi_column(fname, p, state) for p in (plist if plist is not None else defaults))
+            continue
         if fname in FEATURE_ATTR:
             kinds, default_attr, key, default = FEATURE_ATTR[fname]
             for p in plist or [{"attr": default_attr, **({key: default} if key else {})}]:
@@ -154,7 +196,8 @@ def columns_for(config: dict[str, Any] | None, state: int) -> list[FeatureColumn
             continue
         if fname not in FEATURE_KINDS:
             raise ValueError(
-                f"feature '{fname}' is not one of the fused statistics {sorted([*FEATURE_KINDS, *FEATURE_ATTR])}; "
+                f"feature '{fname}' is not one of the fused statistics "
+                f"{sorted([*FEATURE_KINDS, *FEATURE_ATTR, *FEATURE_MULTI])}; "
                 "use B200Dopri5Solver(output='full') with the reference TorchFeatureExtractor for other features"
             )
         kind = FEATURE_KINDS[fname]

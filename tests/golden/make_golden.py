@@ -182,6 +182,19 @@ def _features(ref: Path) -> None:
         **{f"rep_count_value_{v}": cn.count_value(rep, v).numpy() for v in (0.0, 0.5, -1.0)},
         "scaled_has_variance_larger_than_standard_deviation":
             bo.has_variance_larger_than_standard_deviation(scaled).numpy(),
+        # autocorrelation family and the two-parameter features
+        **{f"partial_autocorrelation_{k}": ac.partial_autocorrelation(x, k).numpy() for k in (0, 1, 2, 5, 9)},
+        **{f"agg_autocorrelation_{f}_{m}": ac.agg_autocorrelation(x, m, f).numpy()
+           for f in ("mean", "median", "var") for m in (7, 40)},
+        **{f"energy_ratio_by_chunks_{k}_{i}": ad.energy_ratio_by_chunks(x, k, i).numpy()
+           for (k, i) in ((10, 0), (10, 3), (10, 9), (3, 2), (300, 0))},
+        **{f"count_in_range_{lo}_{hi}": cn.count_in_range(x, lo, hi).numpy()
+           for (lo, hi) in ((-1.0, 1.0), (-1e12, 0.0), (0.0, 1e12))},
+        "rep_count_in_range_-1.0_1.0": cn.count_in_range(rep, -1.0, 1.0).numpy(),
+        **{f"change_quantiles_{ql}_{qh}_{b}_{f}": ch.change_quantiles(x, ql, qh, b, f).numpy()
+           for (ql, qh) in ((0.0, 0.2), (0.2, 0.8), (0.4, 1.0)) for b in (False, True) for f in ("mean", "var")},
+        **{f"rep_change_quantiles_0.2_0.8_{b}_{f}": ch.change_quantiles(rep, 0.2, 0.8, b, f).numpy()
+           for b in (False, True) for f in ("mean", "var")},
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

@@ -205,6 +205,43 @@ def test_oracle_repeated_value_features_match_reference_calculators(name, src, k
         assert np.isnan(want[2, 1]) == (kind in (62, 63))
 
 
+_CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, "var"): 76}
+
+
+@pytest.mark.parametrize(
+    "name, src, kind, param, param2",
+    [
+        *[(f"partial_autocorrelation_{k}", "x", 67, float(k), 0.0) for k in (0, 1, 2, 5, 9)],
+        *[(f"agg_autocorrelation_{f}_{m}", "x", 68 + i, float(m), 0.0)
+          for i, f in enumerate(("mean", "median", "var")) for m in (7, 40)],
+        *[(f"energy_ratio_by_chunks_{k}_{i}", "x", 71, float(k), float(i))
+          for (k, i) in ((10, 0), (10, 3), (10, 9), (3, 2), (300, 0))],
+        *[(f"count_in_range_{lo}_{hi}", "x", 72, lo, hi) for (lo, hi) in ((-1.0, 1.0), (-1e12, 0.0), (0.0, 1e12))],
+        ("rep_count_in_range_-1.0_1.0", "x_rep", 72, -1.0, 1.0),
+        *[(f"change_quantiles_{ql}_{qh}_{b}_{f}", "x", _CQ_KIND[(b, f)], ql, qh)
+          for (ql, qh) in ((0.0, 0.2), (0.2, 0.8), (0.4, 1.0)) for b in (False, True) for f in ("mean", "var")],
+        *[(f"rep_change_quantiles_0.2_0.8_{b}_{f}", "x_rep", _CQ_KIND[(b, f)], 0.2, 0.8)
+          for b in (False, True) for f in ("mean", "var")],
+    ],
+)
+def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name, src, kind, param, param2):
+    """Partial and aggregated autocorrelation, energy ratio of a chunk, count in a
+    range and change quantiles.  The reference's autocorrelations come from a
+    zero-padded FFT (another summation order than the oracle's direct lag sums):
+    1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
+    rest 1e-12 relative.  On the 0.5-grid copy the corridor bounds of change
+    quantiles are sample values, so ties at both bounds are inside."""
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g[src]
+    want = g[name]
+    got = np.array([[O.window_feature(kind, param, x[:, b, s], param2) for s in range(x.shape[2])]
+                    for b in range(x.shape[1])])
+    if 67 <= kind <= 70:
+        np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
+    else:
+        np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)
+
+
 def test_oracle_quantile_even_length():
     g = np.load(GOLDEN / "features_reference.npz")
     x = g["x_even"]

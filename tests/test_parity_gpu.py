@@ -74,7 +74,7 @@ def gpu_solve(
         layout=layout,
         param_index=None if param_index is None else torch.as_tensor(param_index, dtype=torch.int32, device=DEV),
         win_begin=win_begin,
-        columns=[FeatureColumn(s, k, p) for (s, k, p) in (features or [])],
+        columns=[FeatureColumn(f[0], f[1], f[2], "", f[3] if len(f) > 3 else 0.0) for f in (features or [])],
         precision=precision,
         schedule=schedule,
         max_steps=max_steps,
@@ -586,6 +586,67 @@ def test_repeated_value_features_on_identical_windows(precision, n_save):
     # tolerance noise rather than underflowing, so fewer of its windows repeat)
     assert (dup[pidx == 0] == 0.0).all()
     assert (dup[pidx > 0] == 1.0).sum() >= (n // 4 if precision == L.PREC_FP64 else 1)
+
+
+ACF_PAIR_FEATS = [(0, L.FEAT_PARTIAL_AUTOCORRELATION, 1.0), (0, L.FEAT_PARTIAL_AUTOCORRELATION, 7.0),
+                  (1, L.FEAT_PARTIAL_AUTOCORRELATION, 63.0), (0, L.FEAT_PARTIAL_AUTOCORRELATION, 0.0),
+                  (0, L.FEAT_AGG_AUTOCORR_MEAN, 40.0), (1, L.FEAT_AGG_AUTOCORR_MEDIAN, 40.0),
+                  (0, L.FEAT_AGG_AUTOCORR_MEDIAN, 7.0), (1, L.FEAT_AGG_AUTOCORR_VAR, 128.0),
+                  (0, L.FEAT_ENERGY_RATIO_BY_CHUNKS, 10.0, 0.0), (1, L.FEAT_ENERGY_RATIO_BY_CHUNKS, 10.0, 9.0),
+                  (0, L.FEAT_ENERGY_RATIO_BY_CHUNKS, 3.0, 5.0), (0, L.FEAT_COUNT_IN_RANGE, -1.0, 1.0),
+                  (1, L.FEAT_COUNT_IN_RANGE, 0.0, 1e12), (0, L.FEAT_CHANGE_QUANTILES_MEAN, 0.2, 0.8),
+                  (1, L.FEAT_CHANGE_QUANTILES_VAR, 0.0, 0.4), (0, L.FEAT_CHANGE_QUANTILES_ABS_MEAN, 0.4, 1.0),
+                  (1, L.FEAT_CHANGE_QUANTILES_ABS_VAR, 0.2, 0.8), (0, L.FEAT_CHANGE_QUANTILES_VAR, 0.5, 0.5)]
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+def test_acf_and_two_parameter_features_on_identical_windows(precision):
+    """Partial and aggregated autocorrelation, chunk energy ratio, count in range
+    and change quantiles from the window pass against the oracle evaluated on the
+    kernel's own FP32 window (y_full holds the samples the window stores).  Counts
+    are exact; the rest differ by summation order only: the autocorrelations (at
+    most 1 in size) to 1e-10 absolute, the others to 1e-9 relative."""
+    y0 = seeded_ics(DUFFING, 96, seed=21).double().numpy()
+    save = np.linspace(0.0, 40.0, 2001)
+    wb = int(np.nonzero(save >= 25.0)[0][0])
+    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 40.0), 1e-8, 1e-10,
+                    precision=precision, win_begin=wb, features=ACF_PAIR_FEATS, keep_full=True)
+    assert (got["status"] == 0).all()
+    win = got["y"][wb:].astype(np.float32).astype(np.float64)  # (n_win, n, 2)
+    want = np.array([[O.window_feature(f[1], f[2], win[:, j, f[0]], f[3] if len(f) > 3 else 0.0)
+                      for f in ACF_PAIR_FEATS] for j in range(len(y0))])
+    g = got["features"]
+    for c, f in enumerate(ACF_PAIR_FEATS):
+        if L.FEAT_PARTIAL_AUTOCORRELATION <= f[1] <= L.FEAT_AGG_AUTOCORR_VAR:
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=0.0, atol=1e-10, err_msg=f"col {c} {f}")
+        elif f[1] == L.FEAT_COUNT_IN_RANGE:
+            np.testing.assert_array_equal(g[:, c], want[:, c])
+        else:
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-15, err_msg=f"col {c} {f}")
+    assert (g[:, 3] == 1.0).all()  # lag 0
+    assert np.ptp(g[:, 11]) > 0 and (g[:, 13] != 0).any()  # non-trivial counts and corridors
+
+
+def test_two_parameter_features_through_the_extractor_names():
+    """FCParameters entries with several parameters (the reference's settings,
+    ts_torch/settings.py:263-346) become one fused column each, in config order."""
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+
+    cfg = {"agg_autocorrelation": [{"f_agg": s, "maxlag": 40} for s in ("mean", "median", "var")],
+           "partial_autocorrelation": [{"lag": 2}],
+           "change_quantiles": [{"ql": 0.2, "qh": 0.8, "isabs": True, "f_agg": "mean"}],
+           "count_in_range": [{"min_val": -1, "max_val": 1}],
+           "energy_ratio_by_chunks": [{"num_segments": 10, "segment_focus": i} for i in range(10)]}
+    fx = FusedFeatureExtractor(time_steady=900.0, features=None, features_per_state={0: cfg}, normalize=False)
+    solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=2000, t_eval=(900, 1000), device="cuda:0",
+                              precision="fp64", feature_extractor=fx)
+    y0 = seeded_ics(DUFFING, 32, seed=3).double()
+    t, y = solver.integrate(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0)
+    f = fx.extract_features(type("S", (), {"y": y})())
+    assert f.shape == (32, 16) and torch.isfinite(f).all()
+    assert fx.feature_names[0] == "state_0__agg_autocorrelation__f_agg_mean__maxlag_40"
+    # the ten chunk energy ratios partition the window's energy (200 samples per chunk)
+    np.testing.assert_allclose(f[:, 6:].sum(dim=1).cpu().numpy(), 1.0, rtol=1e-9)
 
 
 def test_sorted_window_features_reject_oversized_windows():
