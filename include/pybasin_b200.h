@@ -144,10 +144,14 @@ typedef enum {
     PB_FEAT_PARTIAL_AUTOCORRELATION = 67, PB_FEAT_AGG_AUTOCORR_MEAN = 68, PB_FEAT_AGG_AUTOCORR_MEDIAN = 69,
     PB_FEAT_AGG_AUTOCORR_VAR = 70, PB_FEAT_ENERGY_RATIO_BY_CHUNKS = 71, PB_FEAT_COUNT_IN_RANGE = 72,
     PB_FEAT_CHANGE_QUANTILES_MEAN = 73, PB_FEAT_CHANGE_QUANTILES_VAR = 74,
-    PB_FEAT_CHANGE_QUANTILES_ABS_MEAN = 75, PB_FEAT_CHANGE_QUANTILES_ABS_VAR = 76
+    PB_FEAT_CHANGE_QUANTILES_ABS_MEAN = 75, PB_FEAT_CHANGE_QUANTILES_ABS_VAR = 76,
+    /* autocorrelation_periodicity (min_lag, feat_param2 = peak_threshold; output
+       strength / period in the kind; torch_features_autocorrelation.py:268-329, peaks
+       as torch_feature_utilities.py:146-218) */
+    PB_FEAT_ACF_PERIOD_STRENGTH = 77, PB_FEAT_ACF_PERIOD_LAG = 78
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_CHANGE_QUANTILES_ABS_VAR
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..76): the
+#define PB_FEAT_LAST_KIND PB_FEAT_ACF_PERIOD_LAG
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..78): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window

@@ -562,6 +562,38 @@ static double window_feature(int feat, double param, double param2, const double
         }
         return v / cnt;
     }
+    /* torch_features_autocorrelation.py:268-329 with the peak rule of
+       torch_feature_utilities.py:146-218 (scipy's _local_maxima_1d): the window is
+       centred and divided by its unbiased standard deviation + 1e-10, acf[k] =
+       r_k / (r_0 + 1e-10) for k = 0..n-1, and a peak is the midpoint (rounded down)
+       of a maximal run of equal values entered from a smaller value and left to a
+       smaller one.  The first peak at index >= min_lag whose value exceeds
+       peak_threshold gives the strength (its value) and the period (its index);
+       none gives 0.  The lags are computed in order and the scan stops at that
+       peak. */
+    case ORACLE_F_ACF_PERIOD_STRENGTH: case ORACLE_F_ACF_PERIOD_LAG: {
+        if (n < 2) return 0.0;
+        const int min_lag = (int)param;
+        const double s = sqrt(m2 / (n - 1.0)) + 1e-10, ss = s * s;
+        const double r0 = m2 / ss, den = r0 + 1e-10;
+        double v_run = r0 / den; /* the run holding index 0 is never a peak */
+        int run_a = 0, rose = 0;
+        for (int k = 1; k < n; ++k) {
+            double r = 0.0;
+            for (int i = 0; i + k < n; ++i) r += (w[i] - mean) * (w[i + k] - mean);
+            const double v = (r / ss) / den;
+            if (v == v_run) continue;
+            if (rose && v < v_run) {
+                const int mid = (run_a + k - 1) / 2;
+                if (mid >= min_lag && v_run > param2)
+                    return feat == ORACLE_F_ACF_PERIOD_STRENGTH ? v_run : (double)mid;
+            }
+            rose = v_run < v;
+            run_a = k;
+            v_run = v;
+        }
+        return 0.0;
+    }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
     /* torch_features_count.py:42-45 */

@@ -55,6 +55,8 @@ enum {
     ORACLE_F_AGG_AUTOCORR_VAR = 70, ORACLE_F_ENERGY_RATIO_BY_CHUNKS = 71, ORACLE_F_COUNT_IN_RANGE = 72,
     ORACLE_F_CHANGE_QUANTILES_MEAN = 73, ORACLE_F_CHANGE_QUANTILES_VAR = 74,
     ORACLE_F_CHANGE_QUANTILES_ABS_MEAN = 75, ORACLE_F_CHANGE_QUANTILES_ABS_VAR = 76,
+    /* autocorrelation_periodicity (min_lag, peak_threshold; output strength / period) */
+    ORACLE_F_ACF_PERIOD_STRENGTH = 77, ORACLE_F_ACF_PERIOD_LAG = 78,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

@@ -98,6 +98,7 @@ FEAT_PARTIAL_AUTOCORRELATION, FEAT_AGG_AUTOCORR_MEAN, FEAT_AGG_AUTOCORR_MEDIAN, 
 FEAT_ENERGY_RATIO_BY_CHUNKS, FEAT_COUNT_IN_RANGE = 71, 72
 FEAT_CHANGE_QUANTILES_MEAN, FEAT_CHANGE_QUANTILES_VAR = 73, 74
 FEAT_CHANGE_QUANTILES_ABS_MEAN, FEAT_CHANGE_QUANTILES_ABS_VAR = 75, 76
+FEAT_ACF_PERIOD_STRENGTH, FEAT_ACF_PERIOD_LAG = 77, 78
 SORTED_WINDOW_MAX = 32768  # PB_SORTED_WINDOW_MAX: window samples of the sorted kinds 59..64
 
 TRAJ_OK = 0

@@ -712,6 +712,58 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 }
                 break;
             }
+            case PB_FEAT_ACF_PERIOD_STRENGTH:
+            case PB_FEAT_ACF_PERIOD_LAG: {
+                // first autocorrelation peak (midpoint of a maximal run of equal values
+                // entered from below and left downwards) at lag >= min_lag above the
+                // threshold: its value or its lag, else 0.  acf[k] = r_k / (r_0 + 1e-10)
+                // of the window centred and scaled by its unbiased std + 1e-10.  Lags
+                // are computed 32 at a time (one per lane, each a sequential sum) and
+                // scanned in order by every lane alike; the scan stops at the peak.
+                if (nwin < 2) {
+                    result = 0.0;
+                    break;
+                }
+                const int min_lag = static_cast<int>(param);
+                const double thr = plan.param2[m];
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                }
+                const double m2 = warp_sum_d(a0);
+                const double sd = sqrt(m2 / (n - 1.0)) + 1e-10, ss = sd * sd;
+                const double r0 = m2 / ss, den = r0 + 1e-10;
+                double v_run = r0 / den;  // the run holding lag 0 is never a peak
+                int run_a = 0;
+                bool rose = false, found = false;
+                double out_v = 0.0, out_lag = 0.0;
+                for (int k0 = 1; k0 < nwin && !found; k0 += 32) {
+                    const int k = k0 + lane;
+                    double r = 0.0;
+                    for (int i = 0; i + k < nwin; ++i)
+                        r += (static_cast<double>(x[i]) - mean) * (static_cast<double>(x[i + k]) - mean);
+                    const double val = (r / ss) / den;
+                    const int cnt = min(32, nwin - k0);
+                    for (int j = 0; j < cnt; ++j) {
+                        const double v = __shfl_sync(0xffffffffu, val, j);
+                        if (v == v_run) continue;
+                        if (rose && v < v_run) {
+                            const int mid = (run_a + k0 + j - 1) / 2;
+                            if (mid >= min_lag && v_run > thr) {
+                                found = true;
+                                out_v = v_run;
+                                out_lag = static_cast<double>(mid);
+                                break;
+                            }
+                        }
+                        rose = v_run < v;
+                        run_a = k0 + j;
+                        v_run = v;
+                    }
+                }
+                result = kind == PB_FEAT_ACF_PERIOD_STRENGTH ? out_v : out_lag;
+                break;
+            }
             case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
                 const float v = static_cast<float>(param);
                 for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
@@ -1117,6 +1169,8 @@ int validate_args(const pb_solve_args* a, bool user_system)
             return v >= lo && v <= hi && v == static_cast<double>(static_cast<int>(v));
         };
         if (kind == PB_FEAT_PARTIAL_AUTOCORRELATION && !is_int(prm, 0.0, 63.0)) return PB_EINVAL;
+        if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))
+            return PB_EINVAL;
         if (kind >= PB_FEAT_AGG_AUTOCORR_MEAN && kind <= PB_FEAT_AGG_AUTOCORR_VAR && !is_int(prm, 0.0, 128.0))
             return PB_EINVAL;
         if (kind == PB_FEAT_ENERGY_RATIO_BY_CHUNKS && !(is_int(prm, 1.0, 1e6) && is_int(prm2, 0.0, 1e6)))

@@ -82,13 +82,14 @@ FEATURE_KINDS: dict[str, int] = {
 }
 
 #: Features with several parameters (FCParameters keys as in the reference's
-#: settings, src/pybasin/ts_torch/settings.py:263-346): name -> (defaults when
+#: settings, src/pybasin/ts_torch/settings.py:263-346,407-417): name -> (defaults when
 #: the config gives None, or None if the parameters are required).
 FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "agg_autocorrelation": [{"f_agg": "mean", "maxlag": 40}],
     "energy_ratio_by_chunks": [{"num_segments": 10, "segment_focus": 0}],
     "count_in_range": None,
     "change_quantiles": None,
+    "autocorrelation_periodicity": [{"output": "strength"}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -107,6 +108,12 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
     if fname == "energy_ratio_by_chunks":  # torch_features_advanced.py:93-105
         return FeatureColumn(state, L.FEAT_ENERGY_RATIO_BY_CHUNKS, float(p.get("num_segments", 10)), name,
                              float(p.get("segment_focus", 0)))
+    if fname == "autocorrelation_periodicity":  # torch_features_autocorrelation.py:268-329
+        out = p.get("output", "strength")
+        kinds = {"strength": L.FEAT_ACF_PERIOD_STRENGTH, "period": L.FEAT_ACF_PERIOD_LAG}
+        if out not in kinds:
+            raise ValueError(f"autocorrelation_periodicity: output must be 'strength' or 'period', got {out!r}")
+        return FeatureColumn(state, kinds[out], float(p.get("min_lag", 2)), name, float(p.get("peak_threshold", 0.3)))
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140

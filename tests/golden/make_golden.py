@@ -99,6 +99,12 @@ def _features(ref: Path) -> None:
     rep = torch.round(x * 2.0) / 2.0
     rep[7, 2, 1] = float("nan")
     scaled = x * 0.35
+    # noisy sine waves of 16 periods (6.5 to 36.5 samples), for the periodicity features
+    tt = torch.arange(n_t, dtype=torch.float64)
+    per = torch.sin(2.0 * torch.pi * tt[:, None, None] / (6.5 + 2.0 * torch.arange(n_b, dtype=torch.float64))[None, :, None]
+                    + torch.tensor([0.0, 1.0], dtype=torch.float64)) + 0.3 * torch.randn(n_t, n_b, 2, generator=g,
+                                                                                          dtype=torch.float64)
+    per[:, 4, 1] = 0.25  # constant: no peak
     res = {
         "x": x.numpy(),
         "x_even": even.numpy(),
@@ -195,6 +201,12 @@ def _features(ref: Path) -> None:
            for (ql, qh) in ((0.0, 0.2), (0.2, 0.8), (0.4, 1.0)) for b in (False, True) for f in ("mean", "var")},
         **{f"rep_change_quantiles_0.2_0.8_{b}_{f}": ch.change_quantiles(rep, 0.2, 0.8, b, f).numpy()
            for b in (False, True) for f in ("mean", "var")},
+        "x_periodic": per.numpy(),
+        **{f"periodic_autocorrelation_periodicity_{o}_{m}_{t}":
+           ac.autocorrelation_periodicity(per, m, t, o).numpy()
+           for o in ("strength", "period") for (m, t) in ((2, 0.3), (10, 0.5), (2, 0.9))},
+        **{f"autocorrelation_periodicity_{o}": ac.autocorrelation_periodicity(x, output=o).numpy()
+           for o in ("strength", "period")},
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

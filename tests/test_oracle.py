@@ -222,11 +222,15 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
           for (ql, qh) in ((0.0, 0.2), (0.2, 0.8), (0.4, 1.0)) for b in (False, True) for f in ("mean", "var")],
         *[(f"rep_change_quantiles_0.2_0.8_{b}_{f}", "x_rep", _CQ_KIND[(b, f)], 0.2, 0.8)
           for b in (False, True) for f in ("mean", "var")],
+        *[(f"periodic_autocorrelation_periodicity_{o}_{m}_{t}", "x_periodic", 77 + i, float(m), t)
+          for i, o in enumerate(("strength", "period")) for (m, t) in ((2, 0.3), (10, 0.5), (2, 0.9))],
+        *[(f"autocorrelation_periodicity_{o}", "x", 77 + i, 2.0, 0.3) for i, o in enumerate(("strength", "period"))],
     ],
 )
 def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name, src, kind, param, param2):
-    """Partial and aggregated autocorrelation, energy ratio of a chunk, count in a
-    range and change quantiles.  The reference's autocorrelations come from a
+    """Partial and aggregated autocorrelation, autocorrelation periodicity (noisy
+    sine waves of 16 periods, one constant column), energy ratio of a chunk,
+    count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
     rest 1e-12 relative.  On the 0.5-grid copy the corridor bounds of change
@@ -236,7 +240,7 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
     want = g[name]
     got = np.array([[O.window_feature(kind, param, x[:, b, s], param2) for s in range(x.shape[2])]
                     for b in range(x.shape[1])])
-    if 67 <= kind <= 70:
+    if 67 <= kind <= 70 or kind == 77:
         np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
     else:
         np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)

@@ -596,16 +596,19 @@ ACF_PAIR_FEATS = [(0, L.FEAT_PARTIAL_AUTOCORRELATION, 1.0), (0, L.FEAT_PARTIAL_A
                   (0, L.FEAT_ENERGY_RATIO_BY_CHUNKS, 3.0, 5.0), (0, L.FEAT_COUNT_IN_RANGE, -1.0, 1.0),
                   (1, L.FEAT_COUNT_IN_RANGE, 0.0, 1e12), (0, L.FEAT_CHANGE_QUANTILES_MEAN, 0.2, 0.8),
                   (1, L.FEAT_CHANGE_QUANTILES_VAR, 0.0, 0.4), (0, L.FEAT_CHANGE_QUANTILES_ABS_MEAN, 0.4, 1.0),
-                  (1, L.FEAT_CHANGE_QUANTILES_ABS_VAR, 0.2, 0.8), (0, L.FEAT_CHANGE_QUANTILES_VAR, 0.5, 0.5)]
+                  (1, L.FEAT_CHANGE_QUANTILES_ABS_VAR, 0.2, 0.8), (0, L.FEAT_CHANGE_QUANTILES_VAR, 0.5, 0.5),
+                  (0, L.FEAT_ACF_PERIOD_STRENGTH, 2.0, 0.3), (0, L.FEAT_ACF_PERIOD_LAG, 2.0, 0.3),
+                  (1, L.FEAT_ACF_PERIOD_LAG, 50.0, 0.5), (1, L.FEAT_ACF_PERIOD_STRENGTH, 2.0, 0.99)]
 
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
 def test_acf_and_two_parameter_features_on_identical_windows(precision):
-    """Partial and aggregated autocorrelation, chunk energy ratio, count in range
-    and change quantiles from the window pass against the oracle evaluated on the
+    """Partial and aggregated autocorrelation, autocorrelation periodicity, chunk
+    energy ratio, count in range and change quantiles from the window pass against the oracle evaluated on the
     kernel's own FP32 window (y_full holds the samples the window stores).  Counts
-    are exact; the rest differ by summation order only: the autocorrelations (at
-    most 1 in size) to 1e-10 absolute, the others to 1e-9 relative."""
+    and periods are exact; the rest differ by summation order only: the
+    autocorrelations (at most 1 in size) to 1e-10 absolute, the others to 1e-9
+    relative."""
     y0 = seeded_ics(DUFFING, 96, seed=21).double().numpy()
     save = np.linspace(0.0, 40.0, 2001)
     wb = int(np.nonzero(save >= 25.0)[0][0])
@@ -617,14 +620,15 @@ def test_acf_and_two_parameter_features_on_identical_windows(precision):
                       for f in ACF_PAIR_FEATS] for j in range(len(y0))])
     g = got["features"]
     for c, f in enumerate(ACF_PAIR_FEATS):
-        if L.FEAT_PARTIAL_AUTOCORRELATION <= f[1] <= L.FEAT_AGG_AUTOCORR_VAR:
+        if L.FEAT_PARTIAL_AUTOCORRELATION <= f[1] <= L.FEAT_AGG_AUTOCORR_VAR or f[1] == L.FEAT_ACF_PERIOD_STRENGTH:
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=0.0, atol=1e-10, err_msg=f"col {c} {f}")
-        elif f[1] == L.FEAT_COUNT_IN_RANGE:
-            np.testing.assert_array_equal(g[:, c], want[:, c])
+        elif f[1] in (L.FEAT_COUNT_IN_RANGE, L.FEAT_ACF_PERIOD_LAG):
+            np.testing.assert_array_equal(g[:, c], want[:, c], err_msg=f"col {c} {f}")
         else:
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-15, err_msg=f"col {c} {f}")
     assert (g[:, 3] == 1.0).all()  # lag 0
     assert np.ptp(g[:, 11]) > 0 and (g[:, 13] != 0).any()  # non-trivial counts and corridors
+    assert (g[:, 19] > 0).mean() > 0.5  # most windows of the forced oscillation show a period
 
 
 def test_two_parameter_features_through_the_extractor_names():
