@@ -148,16 +148,26 @@ typedef enum {
     /* autocorrelation_periodicity (min_lag, feat_param2 = peak_threshold; output
        strength / period in the kind; torch_features_autocorrelation.py:268-329, peaks
        as torch_feature_utilities.py:146-218) */
-    PB_FEAT_ACF_PERIOD_STRENGTH = 77, PB_FEAT_ACF_PERIOD_LAG = 78
+    PB_FEAT_ACF_PERIOD_STRENGTH = 77, PB_FEAT_ACF_PERIOD_LAG = 78,
+    /* from the window's power spectrum (at most PB_SPECTRAL_WINDOW_MAX samples):
+       spectral_frequency_ratio (torch_features_frequency.py:390-441) and
+       fft_aggregated with aggtype centroid / variance / skew / kurtosis in the kind
+       (torch_features_frequency.py:32-54) */
+    PB_FEAT_SPECTRAL_FREQ_RATIO = 79, PB_FEAT_FFT_AGG_CENTROID = 80, PB_FEAT_FFT_AGG_VARIANCE = 81,
+    PB_FEAT_FFT_AGG_SKEW = 82, PB_FEAT_FFT_AGG_KURTOSIS = 83
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_ACF_PERIOD_LAG
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..78): the
+#define PB_FEAT_LAST_KIND PB_FEAT_FFT_AGG_KURTOSIS
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..83): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window
    samples than this returns PB_EUNSUPPORTED */
 #define PB_FEAT_IS_SORTED(k) ((k) >= PB_FEAT_HAS_DUPLICATE && (k) <= PB_FEAT_RATIO_UNIQUE_VALUES)
 #define PB_SORTED_WINDOW_MAX 32768
+/* kinds 79..83 hold the window's power spectrum in shared memory: a request with
+   more window samples than this returns PB_EUNSUPPORTED */
+#define PB_FEAT_IS_SPECTRAL(k) ((k) >= PB_FEAT_SPECTRAL_FREQ_RATIO && (k) <= PB_FEAT_FFT_AGG_KURTOSIS)
+#define PB_SPECTRAL_WINDOW_MAX 16384
 
 /* ---- per-trajectory status written to status_out ---- */
 typedef enum {

@@ -144,6 +144,25 @@ static int cmp_double_nan_last(const void *a, const void *b)
     return (x > y) - (x < y);
 }
 
+/* Power |X_k|^2 of the one-sided DFT (rfft, k = 0..n/2) of w - shift, by direct
+   sums with the phase k*i reduced exactly modulo n. */
+static void power_spectrum(const double *w, int n, double shift, double *psd)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int k = 0; k <= n / 2; ++k) {
+        double re = 0.0, im = 0.0;
+        long ph = 0;
+        for (int i = 0; i < n; ++i) {
+            const double ang = two_pi * (double)ph / n;
+            re += (w[i] - shift) * cos(ang);
+            im -= (w[i] - shift) * sin(ang);
+            ph += k;
+            if (ph >= n) ph -= n;
+        }
+        psd[k] = re * re + im * im;
+    }
+}
+
 static double window_feature(int feat, double param, double param2, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
@@ -593,6 +612,52 @@ static double window_feature(int feat, double param, double param2, const double
             v_run = v;
         }
         return 0.0;
+    }
+    /* torch_features_frequency.py:390-441: the two strongest bins of the centred
+       window's power spectrum (bin 0 zeroed) at least two bins apart, the ratio of
+       the second's index to the first's (ties to the lower index); 0 for a flat
+       spectrum (max < 1e-10) */
+    case ORACLE_F_SPECTRAL_FREQ_RATIO: {
+        const int nb = n / 2 + 1;
+        double *psd = (double *)malloc(sizeof(double) * (size_t)nb);
+        if (!psd) return NAN;
+        power_spectrum(w, n, mean, psd);
+        psd[0] = 0.0;
+        int first = 0;
+        for (int k = 1; k < nb; ++k)
+            if (psd[k] > psd[first]) first = k;
+        double res = 0.0;
+        if (!(psd[first] < 1e-10)) {
+            int second = -1;
+            for (int k = 0; k < nb; ++k)
+                if (abs(k - first) >= 2 && (second < 0 || psd[k] > psd[second])) second = k;
+            if (second >= 0 && first > 0) res = (double)second / first;
+        }
+        free(psd);
+        return res;
+    }
+    /* torch_features_frequency.py:32-54: moments of the bin index under the
+       normalised power spectrum of the (uncentred) window */
+    case ORACLE_F_FFT_AGG_CENTROID: case ORACLE_F_FFT_AGG_VARIANCE: case ORACLE_F_FFT_AGG_SKEW:
+    case ORACLE_F_FFT_AGG_KURTOSIS: {
+        const int nb = n / 2 + 1;
+        double *psd = (double *)malloc(sizeof(double) * (size_t)nb);
+        if (!psd) return NAN;
+        power_spectrum(w, n, 0.0, psd);
+        double tot = 0.0, c = 0.0, v = 0.0, m3 = 0.0, m4 = 0.0;
+        for (int k = 0; k < nb; ++k) tot += psd[k];
+        for (int k = 0; k < nb; ++k) c += k * (psd[k] / (tot + 1e-10));
+        for (int k = 0; k < nb; ++k) {
+            const double p = psd[k] / (tot + 1e-10), d = k - c;
+            v += d * d * p;
+            m3 += d * d * d * p;
+            m4 += d * d * d * d * p;
+        }
+        free(psd);
+        if (feat == ORACLE_F_FFT_AGG_CENTROID) return c;
+        if (feat == ORACLE_F_FFT_AGG_VARIANCE) return v;
+        if (feat == ORACLE_F_FFT_AGG_SKEW) return m3 / (pow(v, 1.5) + 1e-10);
+        return m4 / (v * v + 1e-10);
     }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;

@@ -57,6 +57,9 @@ enum {
     ORACLE_F_CHANGE_QUANTILES_ABS_MEAN = 75, ORACLE_F_CHANGE_QUANTILES_ABS_VAR = 76,
     /* autocorrelation_periodicity (min_lag, peak_threshold; output strength / period) */
     ORACLE_F_ACF_PERIOD_STRENGTH = 77, ORACLE_F_ACF_PERIOD_LAG = 78,
+    /* spectral_frequency_ratio, fft_aggregated (centroid, variance, skew, kurtosis) */
+    ORACLE_F_SPECTRAL_FREQ_RATIO = 79, ORACLE_F_FFT_AGG_CENTROID = 80, ORACLE_F_FFT_AGG_VARIANCE = 81,
+    ORACLE_F_FFT_AGG_SKEW = 82, ORACLE_F_FFT_AGG_KURTOSIS = 83,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

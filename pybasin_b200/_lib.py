@@ -99,6 +99,9 @@ FEAT_ENERGY_RATIO_BY_CHUNKS, FEAT_COUNT_IN_RANGE = 71, 72
 FEAT_CHANGE_QUANTILES_MEAN, FEAT_CHANGE_QUANTILES_VAR = 73, 74
 FEAT_CHANGE_QUANTILES_ABS_MEAN, FEAT_CHANGE_QUANTILES_ABS_VAR = 75, 76
 FEAT_ACF_PERIOD_STRENGTH, FEAT_ACF_PERIOD_LAG = 77, 78
+FEAT_SPECTRAL_FREQ_RATIO, FEAT_FFT_AGG_CENTROID, FEAT_FFT_AGG_VARIANCE = 79, 80, 81
+FEAT_FFT_AGG_SKEW, FEAT_FFT_AGG_KURTOSIS = 82, 83
+SPECTRAL_WINDOW_MAX = 16384  # PB_SPECTRAL_WINDOW_MAX: window samples of the spectral kinds 79..83
 SORTED_WINDOW_MAX = 32768  # PB_SORTED_WINDOW_MAX: window samples of the sorted kinds 59..64
 
 TRAJ_OK = 0

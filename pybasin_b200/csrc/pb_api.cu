@@ -30,6 +30,8 @@ struct MedianPlan {
     double* peaks_out;               // (n_traj, n_peak_cols, peak_cap) or NULL
     int n_sorted;                    // window columns of the sorted kinds (PB_FEAT_IS_SORTED)
     int sorted_m[PB_MAX_FEATURES];   // their window column indices m
+    int n_spectral;                  // window columns of the spectral kinds (PB_FEAT_IS_SPECTRAL)
+    int spectral_m[PB_MAX_FEATURES];
 };
 
 __device__ __forceinline__ uint32_t float_key(float f)
@@ -102,7 +104,8 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
     const int64_t traj = row / plan.n_med;
     const int m = static_cast<int>(row - traj * plan.n_med);
     const int col = plan.col[m], kind = plan.kind[m];
-    if (PB_FEAT_IS_SORTED(kind)) return;  // warp-uniform; k_window_sorted writes these
+    if (PB_FEAT_IS_SORTED(kind) || PB_FEAT_IS_SPECTRAL(kind)) return;  // warp-uniform; written by
+                                                                       // k_window_sorted / k_window_spectrum
     const double param = plan.param[m];
     const double n = static_cast<double>(nwin);
     double result = CUDART_NAN;
@@ -776,6 +779,140 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
     if (lane == 0) out[traj * n_features + col] = result;
 }
 
+// Block-wide FP64 sum over 256 threads (every thread gets the total).
+__device__ double block_sum_d(double v, double* red)
+{
+    v = warp_sum_d(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+// Block-wide argmax of psd[k] over k in [0, nb) with |k - skip| >= 2 (skip < 0:
+// none), ties to the lower index; every thread gets the index (-1 if none).
+__device__ int block_argmax(const double* psd, int nb, int skip, double* red, int* redi)
+{
+    double bv = -CUDART_INF;
+    int bi = -1;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        if (skip >= 0 && abs(k - skip) < 2) continue;
+        if (bi < 0 || psd[k] > bv) {
+            bv = psd[k];
+            bi = k;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (oi >= 0 && (bi < 0 || ov > bv || (ov == bv && oi < bi))) {
+            bv = ov;
+            bi = oi;
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = bv;
+        redi[threadIdx.x >> 5] = bi;
+    }
+    __syncthreads();
+    bv = -CUDART_INF;
+    bi = -1;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w)
+        if (redi[w] >= 0 && (bi < 0 || red[w] > bv || (red[w] == bv && redi[w] < bi))) {
+            bv = red[w];
+            bi = redi[w];
+        }
+    __syncthreads();
+    return bi;
+}
+
+// Power spectrum of the window (kinds 79..83): one 256-thread block per
+// (trajectory, spectral column).  |X_k|^2 of the one-sided DFT, k = 0..n/2, by
+// Goertzel recurrences in FP64 (four bins per thread per pass over the window,
+// which every thread reads alike), closed as X_k = s1 - e^(-i w) s2; the spectrum
+// stays in shared memory for the reductions: spectral_frequency_ratio (centred
+// window, bin 0 zeroed; the two strongest bins at least two apart, ties to the
+// lower index) and fft_aggregated (moments of the bin index under the normalised
+// spectrum of the uncentred window).
+__global__ void __launch_bounds__(256) k_window_spectrum(const float* __restrict__ win, int nwin, MedianPlan plan,
+                                                         double* __restrict__ out, int n_features)
+{
+    extern __shared__ double psd[];  // nwin / 2 + 1 entries
+    __shared__ double red[8];
+    __shared__ int redi[8];
+    const int64_t blk = blockIdx.x;
+    const int64_t traj = blk / plan.n_spectral;
+    const int m = plan.spectral_m[blk - traj * plan.n_spectral];
+    const int kind = plan.kind[m];
+    const float* x = win + (traj * plan.n_med + m) * static_cast<int64_t>(nwin);
+    const int nb = nwin / 2 + 1;
+    double sx = 0.0;
+    for (int i = threadIdx.x; i < nwin; i += blockDim.x) sx += static_cast<double>(x[i]);
+    const double shift = kind == PB_FEAT_SPECTRAL_FREQ_RATIO ? block_sum_d(sx, red) / nwin : 0.0;
+    for (int k0 = 4 * threadIdx.x; k0 < nb; k0 += 4 * blockDim.x) {
+        double c[4], sn[4], cs[4], s1[4], s2[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = min(k0 + j, nb - 1);
+            sincospi(2.0 * static_cast<double>(k) / nwin, &sn[j], &cs[j]);
+            c[j] = 2.0 * cs[j];
+            s1[j] = 0.0;
+            s2[j] = 0.0;
+        }
+        for (int i = 0; i < nwin; ++i) {
+            const double v = static_cast<double>(x[i]) - shift;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double t = fma(c[j], s1[j], v - s2[j]);
+                s2[j] = s1[j];
+                s1[j] = t;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (k0 + j >= nb) break;
+            const double re = s1[j] - cs[j] * s2[j], im = sn[j] * s2[j];
+            psd[k0 + j] = re * re + im * im;
+        }
+    }
+    __syncthreads();
+    double result;
+    if (kind == PB_FEAT_SPECTRAL_FREQ_RATIO) {
+        if (threadIdx.x == 0) psd[0] = 0.0;
+        __syncthreads();
+        const int first = block_argmax(psd, nb, -1, red, redi);
+        result = 0.0;
+        if (first >= 0 && !(psd[first] < 1e-10)) {
+            const int second = block_argmax(psd, nb, first, red, redi);
+            if (second >= 0 && first > 0) result = static_cast<double>(second) / first;
+        }
+    } else {
+        double a = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) a += psd[k];
+        const double tot = block_sum_d(a, red) + 1e-10;
+        a = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) a += k * (psd[k] / tot);
+        const double cen = block_sum_d(a, red);
+        double v2 = 0.0, v3 = 0.0, v4 = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+            const double p = psd[k] / tot, d = k - cen;
+            v2 += d * d * p;
+            v3 += d * d * d * p;
+            v4 += d * d * d * d * p;
+        }
+        const double var = block_sum_d(v2, red);
+        const double m3 = block_sum_d(v3, red);
+        const double m4 = block_sum_d(v4, red);
+        if (kind == PB_FEAT_FFT_AGG_CENTROID) result = cen;
+        else if (kind == PB_FEAT_FFT_AGG_VARIANCE) result = var;
+        else if (kind == PB_FEAT_FFT_AGG_SKEW) result = m3 / (pow(var, 1.5) + 1e-10);
+        else result = m4 / (var * var + 1e-10);
+    }
+    if (threadIdx.x == 0) out[traj * n_features + plan.col[m]] = result;
+}
+
 // Repeated values over the whole window (kinds 59..64): one block per (trajectory,
 // sorted column) sorts that column's window in shared memory, as order-preserving
 // keys padded to a power of two with all-ones keys (after every number), by a
@@ -1098,7 +1235,7 @@ static cudaError_t sort_by_probe(const pb_solve_args& a, const ScratchLayout& sl
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
 {
-    int m = 0, np = 0, ns = 0;
+    int m = 0, np = 0, ns = 0, nsp = 0;
     for (int c = 0; c < a.n_features; ++c)
         if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
             if (plan) {
@@ -1111,10 +1248,13 @@ static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
             np += a.feat_kind[c] == PB_FEAT_NUMBER_PEAKS;
             if (plan && PB_FEAT_IS_SORTED(a.feat_kind[c])) plan->sorted_m[ns] = m;
             ns += PB_FEAT_IS_SORTED(a.feat_kind[c]) ? 1 : 0;
+            if (plan && PB_FEAT_IS_SPECTRAL(a.feat_kind[c])) plan->spectral_m[nsp] = m;
+            nsp += PB_FEAT_IS_SPECTRAL(a.feat_kind[c]) ? 1 : 0;
             ++m;
         }
     if (plan) {
         plan->n_sorted = ns;
+        plan->n_spectral = nsp;
         plan->n_med = m;
         plan->n_peak_cols = np;
         plan->peak_cap = a.peak_cap;
@@ -1164,6 +1304,7 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_MEAN_N_ABS_MAX && !(prm >= 1.0 && prm <= 64.0 && prm == static_cast<double>(static_cast<int>(prm))))
             return PB_EINVAL;
         if (PB_FEAT_IS_SORTED(kind) && a->n_save - a->win_begin > PB_SORTED_WINDOW_MAX) return PB_EUNSUPPORTED;
+        if (PB_FEAT_IS_SPECTRAL(kind) && a->n_save - a->win_begin > PB_SPECTRAL_WINDOW_MAX) return PB_EUNSUPPORTED;
         const double prm2 = a->feat_param2[c];
         const auto is_int = [](double v, double lo, double hi) {
             return v >= lo && v <= hi && v == static_cast<double>(static_cast<int>(v));
@@ -1318,6 +1459,21 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
             k_window_sorted<<<static_cast<unsigned>(sblocks), 256, smem, st>>>(
                 reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), nwin,
                 pow2, plan, a.features_out, a.n_features);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return map_cuda(e);
+        }
+        if (plan.n_spectral > 0) {
+            const int nwin = a.n_save - a.win_begin;  // <= PB_SPECTRAL_WINDOW_MAX (validated)
+            const int64_t sblocks = a.n_traj * plan.n_spectral;
+            if (sblocks > 0x7fffffffLL) return PB_EINVAL;
+            const size_t smem = static_cast<size_t>(nwin / 2 + 1) * sizeof(double);
+            if (smem > 48 * 1024)
+                e = cudaFuncSetAttribute(k_window_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+            if (e != cudaSuccess) return map_cuda(e);
+            k_window_spectrum<<<static_cast<unsigned>(sblocks), 256, smem, st>>>(
+                reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), nwin,
+                plan, a.features_out, a.n_features);
             e = cudaGetLastError();
             if (e != cudaSuccess) return map_cuda(e);
         }

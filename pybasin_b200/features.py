@@ -79,6 +79,7 @@ FEATURE_KINDS: dict[str, int] = {
     "has_variance_larger_than_standard_deviation": L.FEAT_VAR_LARGER_THAN_STD,
     "count_value": L.FEAT_COUNT_VALUE,
     "partial_autocorrelation": L.FEAT_PARTIAL_AUTOCORRELATION,
+    "spectral_frequency_ratio": L.FEAT_SPECTRAL_FREQ_RATIO,
 }
 
 #: Features with several parameters (FCParameters keys as in the reference's
@@ -90,6 +91,7 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "count_in_range": None,
     "change_quantiles": None,
     "autocorrelation_periodicity": [{"output": "strength"}],
+    "fft_aggregated": [{"aggtype": "centroid"}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -114,6 +116,13 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
         if out not in kinds:
             raise ValueError(f"autocorrelation_periodicity: output must be 'strength' or 'period', got {out!r}")
         return FeatureColumn(state, kinds[out], float(p.get("min_lag", 2)), name, float(p.get("peak_threshold", 0.3)))
+    if fname == "fft_aggregated":  # torch_features_frequency.py:32-54
+        agg = p.get("aggtype", "centroid")
+        kinds = {"centroid": L.FEAT_FFT_AGG_CENTROID, "variance": L.FEAT_FFT_AGG_VARIANCE,
+                 "skew": L.FEAT_FFT_AGG_SKEW, "kurtosis": L.FEAT_FFT_AGG_KURTOSIS}
+        if agg not in kinds:
+            raise ValueError(f"fft_aggregated: aggtype must be one of {sorted(kinds)}, got {agg!r}")
+        return FeatureColumn(state, kinds[agg], 0.0, name)
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140

@@ -207,6 +207,12 @@ def _features(ref: Path) -> None:
            for o in ("strength", "period") for (m, t) in ((2, 0.3), (10, 0.5), (2, 0.9))},
         **{f"autocorrelation_periodicity_{o}": ac.autocorrelation_periodicity(x, output=o).numpy()
            for o in ("strength", "period")},
+        # spectra (odd and even lengths)
+        **{f"{src}_spectral_frequency_ratio": fq.spectral_frequency_ratio(v).numpy()
+           for src, v in (("x", x), ("periodic", per), ("even", even))},
+        **{f"{src}_fft_aggregated_{a}": fq.fft_aggregated(v, a).numpy()
+           for src, v in (("x", x), ("periodic", per), ("even", even))
+           for a in ("centroid", "variance", "skew", "kurtosis")},
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

@@ -225,11 +225,17 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
         *[(f"periodic_autocorrelation_periodicity_{o}_{m}_{t}", "x_periodic", 77 + i, float(m), t)
           for i, o in enumerate(("strength", "period")) for (m, t) in ((2, 0.3), (10, 0.5), (2, 0.9))],
         *[(f"autocorrelation_periodicity_{o}", "x", 77 + i, 2.0, 0.3) for i, o in enumerate(("strength", "period"))],
+        *[(f"{tag}_{name}", src, kind, 0.0, 0.0)
+          for tag, src in (("x", "x"), ("periodic", "x_periodic"), ("even", "x_even"))
+          for name, kind in (("spectral_frequency_ratio", 79), ("fft_aggregated_centroid", 80),
+                             ("fft_aggregated_variance", 81), ("fft_aggregated_skew", 82),
+                             ("fft_aggregated_kurtosis", 83))],
     ],
 )
 def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name, src, kind, param, param2):
     """Partial and aggregated autocorrelation, autocorrelation periodicity (noisy
-    sine waves of 16 periods, one constant column), energy ratio of a chunk,
+    sine waves of 16 periods, one constant column), spectral frequency ratio and
+    aggregated spectrum moments (odd and even lengths), energy ratio of a chunk,
     count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
@@ -242,6 +248,8 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
                     for b in range(x.shape[1])])
     if 67 <= kind <= 70 or kind == 77:
         np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
+    elif 80 <= kind <= 83:  # torch's FFT against the oracle's direct sums
+        np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12)
     else:
         np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)
 

@@ -640,17 +640,57 @@ def test_two_parameter_features_through_the_extractor_names():
            "partial_autocorrelation": [{"lag": 2}],
            "change_quantiles": [{"ql": 0.2, "qh": 0.8, "isabs": True, "f_agg": "mean"}],
            "count_in_range": [{"min_val": -1, "max_val": 1}],
-           "energy_ratio_by_chunks": [{"num_segments": 10, "segment_focus": i} for i in range(10)]}
+           "energy_ratio_by_chunks": [{"num_segments": 10, "segment_focus": i} for i in range(10)],
+           "autocorrelation_periodicity": [{"output": "strength"}, {"output": "period"}],
+           "spectral_frequency_ratio": None, "fft_aggregated": [{"aggtype": "kurtosis"}]}
     fx = FusedFeatureExtractor(time_steady=900.0, features=None, features_per_state={0: cfg}, normalize=False)
     solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=2000, t_eval=(900, 1000), device="cuda:0",
                               precision="fp64", feature_extractor=fx)
     y0 = seeded_ics(DUFFING, 32, seed=3).double()
     t, y = solver.integrate(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0)
     f = fx.extract_features(type("S", (), {"y": y})())
-    assert f.shape == (32, 16) and torch.isfinite(f).all()
+    assert f.shape == (32, 20) and torch.isfinite(f).all()
     assert fx.feature_names[0] == "state_0__agg_autocorrelation__f_agg_mean__maxlag_40"
+    assert fx.feature_names[-1] == "state_0__fft_aggregated__aggtype_kurtosis"
     # the ten chunk energy ratios partition the window's energy (200 samples per chunk)
-    np.testing.assert_allclose(f[:, 6:].sum(dim=1).cpu().numpy(), 1.0, rtol=1e-9)
+    np.testing.assert_allclose(f[:, 6:16].sum(dim=1).cpu().numpy(), 1.0, rtol=1e-9)
+
+
+SPECTRAL_FEATS = [(0, L.FEAT_SPECTRAL_FREQ_RATIO, 0.0), (1, L.FEAT_SPECTRAL_FREQ_RATIO, 0.0),
+                  (0, L.FEAT_FFT_AGG_CENTROID, 0.0), (1, L.FEAT_FFT_AGG_VARIANCE, 0.0),
+                  (0, L.FEAT_FFT_AGG_SKEW, 0.0), (1, L.FEAT_FFT_AGG_KURTOSIS, 0.0)]
+
+
+@pytest.mark.parametrize("n_save", [2001, 2002])
+def test_spectral_features_on_identical_windows(n_save):
+    """spectral_frequency_ratio and fft_aggregated from the spectrum pass (FP64
+    Goertzel recurrences) against the oracle's direct DFT on the kernel's own FP32
+    window, odd and even window lengths: the spectrum moments to 1e-8 relative; the
+    frequency ratio picks bins by rank, so it is equal wherever the competing bins'
+    powers differ by more than the two methods' rounding (all but a few windows)."""
+    y0 = seeded_ics(DUFFING, 128, seed=23).double().numpy()
+    save = np.linspace(0.0, 60.0, n_save)
+    wb = int(np.nonzero(save >= 20.0)[0][0])
+    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 60.0), 1e-8, 1e-10,
+                    win_begin=wb, features=SPECTRAL_FEATS, keep_full=True)
+    assert (got["status"] == 0).all()
+    win = got["y"][wb:].astype(np.float32).astype(np.float64)
+    want = np.array([[O.window_feature(k, p, win[:, j, st]) for (st, k, p) in SPECTRAL_FEATS] for j in range(len(y0))])
+    g = got["features"]
+    for c, (_, k, _) in enumerate(SPECTRAL_FEATS):
+        if k == L.FEAT_SPECTRAL_FREQ_RATIO:
+            assert (g[:, c] == want[:, c]).mean() >= 0.97, c
+            assert (g[:, c] > 0).all()
+        else:
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-8, atol=1e-12, err_msg=f"col {c}")
+
+
+def test_spectral_features_reject_oversized_windows():
+    """The spectrum sits in shared memory: more than 16,384 window samples is refused."""
+    save = np.linspace(0.0, 1.0, L.SPECTRAL_WINDOW_MAX + 1)
+    with pytest.raises(RuntimeError, match="unsupported"):
+        gpu_solve(O.SYS_LINEAR, np.ones((2, 1)), np.array([[-1.0]]), save, (0.0, 1.0), 1e-6, 1e-9,
+                  win_begin=0, features=[(0, L.FEAT_FFT_AGG_CENTROID, 0.0)])
 
 
 def test_sorted_window_features_reject_oversized_windows():
