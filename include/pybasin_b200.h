@@ -154,20 +154,28 @@ typedef enum {
        fft_aggregated with aggtype centroid / variance / skew / kurtosis in the kind
        (torch_features_frequency.py:32-54) */
     PB_FEAT_SPECTRAL_FREQ_RATIO = 79, PB_FEAT_FFT_AGG_CENTROID = 80, PB_FEAT_FFT_AGG_VARIANCE = 81,
-    PB_FEAT_FFT_AGG_SKEW = 82, PB_FEAT_FFT_AGG_KURTOSIS = 83
+    PB_FEAT_FFT_AGG_SKEW = 82, PB_FEAT_FFT_AGG_KURTOSIS = 83,
+    /* fourier_entropy (bins, unused as in the reference; a spectral kind;
+       torch_features_entropy_complexity.py:97-110), permutation_entropy (tau,
+       feat_param2 = dimension <= 7; :13-54), lempel_ziv_complexity (bins <= 255, at
+       most PB_SYMBOLIC_WINDOW_MAX window samples; :141-178) */
+    PB_FEAT_FOURIER_ENTROPY = 84, PB_FEAT_PERMUTATION_ENTROPY = 85, PB_FEAT_LEMPEL_ZIV = 86
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_FFT_AGG_KURTOSIS
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..83): the
+#define PB_FEAT_LAST_KIND PB_FEAT_LEMPEL_ZIV
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..86): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window
    samples than this returns PB_EUNSUPPORTED */
 #define PB_FEAT_IS_SORTED(k) ((k) >= PB_FEAT_HAS_DUPLICATE && (k) <= PB_FEAT_RATIO_UNIQUE_VALUES)
 #define PB_SORTED_WINDOW_MAX 32768
-/* kinds 79..83 hold the window's power spectrum in shared memory: a request with
+/* kinds 79..84 hold the window's power spectrum in shared memory: a request with
    more window samples than this returns PB_EUNSUPPORTED */
-#define PB_FEAT_IS_SPECTRAL(k) ((k) >= PB_FEAT_SPECTRAL_FREQ_RATIO && (k) <= PB_FEAT_FFT_AGG_KURTOSIS)
+#define PB_FEAT_IS_SPECTRAL(k) ((k) >= PB_FEAT_SPECTRAL_FREQ_RATIO && (k) <= PB_FEAT_FOURIER_ENTROPY)
 #define PB_SPECTRAL_WINDOW_MAX 16384
+/* kinds 85..86 run one block per column over symbols in shared memory */
+#define PB_FEAT_IS_SYMBOLIC(k) ((k) == PB_FEAT_PERMUTATION_ENTROPY || (k) == PB_FEAT_LEMPEL_ZIV)
+#define PB_SYMBOLIC_WINDOW_MAX 8191
 
 /* ---- per-trajectory status written to status_out ---- */
 typedef enum {

@@ -659,6 +659,99 @@ static double window_feature(int feat, double param, double param2, const double
         if (feat == ORACLE_F_FFT_AGG_SKEW) return m3 / (pow(v, 1.5) + 1e-10);
         return m4 / (v * v + 1e-10);
     }
+    /* torch_features_entropy_complexity.py:97-110: entropy of the normalised power
+       spectrum (uncentred window), each share clamped at 1e-10 */
+    case ORACLE_F_FOURIER_ENTROPY: {
+        const int nb = n / 2 + 1;
+        double *psd = (double *)malloc(sizeof(double) * (size_t)nb);
+        if (!psd) return NAN;
+        power_spectrum(w, n, 0.0, psd);
+        double tot = 0.0, h = 0.0;
+        for (int k = 0; k < nb; ++k) tot += psd[k];
+        for (int k = 0; k < nb; ++k) {
+            double p = psd[k] / (tot + 1e-10);
+            if (p < 1e-10) p = 1e-10;
+            h -= p * log(p);
+        }
+        free(psd);
+        return h;
+    }
+    /* torch_features_entropy_complexity.py:13-54: each embedded vector
+       (w[i], w[i+tau], ..., w[i+(d-1)tau]) gets the id sum_p idx[p] * (d-1-p)!, idx
+       the indices that sort it (ties in index order); the Shannon entropy of the
+       ids' frequencies over log(d!).  The id is not one-to-one on permutations
+       (for d = 3 only three ids occur); the reference counts these ids. */
+    case ORACLE_F_PERMUTATION_ENTROPY: {
+        const int tau = (int)param, d = (int)param2;
+        const long np_ = (long)n - (long)(d - 1) * tau;
+        if (np_ <= 0 || d < 1 || d > 7) return 0.0;
+        int fact[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
+        double cnt[5040];
+        for (int k = 0; k < fact[d]; ++k) cnt[k] = 0.0;
+        for (long i = 0; i < np_; ++i) {
+            int id = 0;
+            for (int j = 0; j < d; ++j) {
+                const double vj = w[i + (long)j * tau];
+                int pos = 0;
+                for (int l = 0; l < d; ++l) {
+                    const double vl = w[i + (long)l * tau];
+                    pos += vl < vj || (vl == vj && l < j);
+                }
+                id += j * fact[d - 1 - pos];
+            }
+            cnt[id] += 1.0;
+        }
+        double h = 0.0;
+        for (int k = 0; k < fact[d]; ++k)
+            if (cnt[k] > 0.0) {
+                const double p = cnt[k] / np_;
+                h -= p * log(p);
+            }
+        return fact[d] > 1 ? h / log((double)fact[d]) : h;
+    }
+    /* torch_features_entropy_complexity.py:141-178: the window cut into `bins`
+       equal bins over [min, max + 1e-10), then parsed into phrases, each the
+       shortest substring from the current position not seen as a phrase before
+       (so every phrase extends an earlier one by one symbol: an LZ78 trie); the
+       phrase count over n / log n.  A final substring already seen adds nothing. */
+    case ORACLE_F_LEMPEL_ZIV: {
+        const int bins = (int)param;
+        const double range = (mx - mn) + 1e-10;
+        int *sym = (int *)malloc(sizeof(int) * (size_t)n);
+        int *child = (int *)malloc(sizeof(int) * (size_t)(n + 1) * (size_t)bins);
+        if (!sym || !child) {
+            free(sym);
+            free(child);
+            return NAN;
+        }
+        for (int i = 0; i < n; ++i) {
+            long b = (long)((w[i] - mn) / range * bins);
+            sym[i] = (int)(b < 0 ? 0 : (b > bins - 1 ? bins - 1 : b));
+        }
+        for (long q = 0; q < (long)(n + 1) * bins; ++q) child[q] = -1;
+        int nodes = 1, complexity = 0;
+        long i = 0;
+        while (i < n) {
+            int node = 0;
+            long len = 1;
+            while (i + len <= n) {
+                const int c = sym[i + len - 1];
+                const int nx = child[(long)node * bins + c];
+                if (nx < 0) {
+                    child[(long)node * bins + c] = nodes++;
+                    ++complexity;
+                    break;
+                }
+                node = nx;
+                ++len;
+            }
+            i += len;
+        }
+        free(sym);
+        free(child);
+        const double b_n = n > 1 ? n / (log((double)n) + 1e-10) : 1.0;
+        return complexity / b_n;
+    }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
     /* torch_features_count.py:42-45 */

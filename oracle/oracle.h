@@ -60,6 +60,9 @@ enum {
     /* spectral_frequency_ratio, fft_aggregated (centroid, variance, skew, kurtosis) */
     ORACLE_F_SPECTRAL_FREQ_RATIO = 79, ORACLE_F_FFT_AGG_CENTROID = 80, ORACLE_F_FFT_AGG_VARIANCE = 81,
     ORACLE_F_FFT_AGG_SKEW = 82, ORACLE_F_FFT_AGG_KURTOSIS = 83,
+    /* fourier_entropy (bins, unused by the reference), permutation_entropy (tau,
+       dimension), lempel_ziv_complexity (bins) */
+    ORACLE_F_FOURIER_ENTROPY = 84, ORACLE_F_PERMUTATION_ENTROPY = 85, ORACLE_F_LEMPEL_ZIV = 86,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

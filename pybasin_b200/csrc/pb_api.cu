@@ -32,6 +32,8 @@ struct MedianPlan {
     int sorted_m[PB_MAX_FEATURES];   // their window column indices m
     int n_spectral;                  // window columns of the spectral kinds (PB_FEAT_IS_SPECTRAL)
     int spectral_m[PB_MAX_FEATURES];
+    int n_symbolic;                  // window columns of the symbolic kinds (PB_FEAT_IS_SYMBOLIC)
+    int symbolic_m[PB_MAX_FEATURES];
 };
 
 __device__ __forceinline__ uint32_t float_key(float f)
@@ -104,8 +106,8 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
     const int64_t traj = row / plan.n_med;
     const int m = static_cast<int>(row - traj * plan.n_med);
     const int col = plan.col[m], kind = plan.kind[m];
-    if (PB_FEAT_IS_SORTED(kind) || PB_FEAT_IS_SPECTRAL(kind)) return;  // warp-uniform; written by
-                                                                       // k_window_sorted / k_window_spectrum
+    // warp-uniform; written by k_window_sorted / k_window_spectrum / k_window_symbolic
+    if (PB_FEAT_IS_SORTED(kind) || PB_FEAT_IS_SPECTRAL(kind) || PB_FEAT_IS_SYMBOLIC(kind)) return;
     const double param = plan.param[m];
     const double n = static_cast<double>(nwin);
     double result = CUDART_NAN;
@@ -879,7 +881,17 @@ __global__ void __launch_bounds__(256) k_window_spectrum(const float* __restrict
     }
     __syncthreads();
     double result;
-    if (kind == PB_FEAT_SPECTRAL_FREQ_RATIO) {
+    if (kind == PB_FEAT_FOURIER_ENTROPY) {  // shares clamped at 1e-10
+        double a = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) a += psd[k];
+        const double tot = block_sum_d(a, red) + 1e-10;
+        a = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+            const double p = fmax(psd[k] / tot, 1e-10);
+            a -= p * log(p);
+        }
+        result = block_sum_d(a, red);
+    } else if (kind == PB_FEAT_SPECTRAL_FREQ_RATIO) {
         if (threadIdx.x == 0) psd[0] = 0.0;
         __syncthreads();
         const int first = block_argmax(psd, nb, -1, red, redi);
@@ -909,6 +921,121 @@ __global__ void __launch_bounds__(256) k_window_spectrum(const float* __restrict
         else if (kind == PB_FEAT_FFT_AGG_VARIANCE) result = var;
         else if (kind == PB_FEAT_FFT_AGG_SKEW) result = m3 / (pow(var, 1.5) + 1e-10);
         else result = m4 / (var * var + 1e-10);
+    }
+    if (threadIdx.x == 0) out[traj * n_features + plan.col[m]] = result;
+}
+
+// Block-wide FP64 maximum over 256 threads (every thread gets it).
+__device__ double block_max_d(double v, double* red)
+{
+    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = -CUDART_INF;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t = fmax(t, red[w]);
+    __syncthreads();
+    return t;
+}
+
+__constant__ int kFactorial[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
+
+// Symbolic kinds (85, 86): one 256-thread block per (trajectory, column).
+// permutation_entropy: every embedded vector (x_i, x_(i+tau), ..) gets the id
+// sum_p idx[p] (d-1-p)!, idx the indices that sort it (ties in index order; the
+// reference's id, which is not one-to-one on permutations), counted in a shared
+// histogram of d! bins; the entropy of the id frequencies over log d!.
+// lempel_ziv_complexity: the window is cut into `bins` equal bins over [min, max +
+// 1e-10) and parsed into phrases, each the shortest substring from the current
+// position that is not an earlier phrase; every phrase extends an earlier one by a
+// symbol, so the phrases form a trie, held as an open-addressing table (node *
+// 256 + symbol -> child) in shared memory and walked by one thread; the phrase
+// count over n / log n.
+__global__ void __launch_bounds__(256) k_window_symbolic(const float* __restrict__ win, int nwin, int table_size,
+                                                         MedianPlan plan, double* __restrict__ out, int n_features)
+{
+    extern __shared__ __align__(16) unsigned sm[];
+    __shared__ double red[8];
+    const int64_t blk = blockIdx.x;
+    const int64_t traj = blk / plan.n_symbolic;
+    const int m = plan.symbolic_m[blk - traj * plan.n_symbolic];
+    const int kind = plan.kind[m];
+    const float* x = win + (traj * plan.n_med + m) * static_cast<int64_t>(nwin);
+    double result = 0.0;
+    if (kind == PB_FEAT_PERMUTATION_ENTROPY) {
+        const int tau = static_cast<int>(plan.param[m]), d = static_cast<int>(plan.param2[m]);
+        const int64_t npat = static_cast<int64_t>(nwin) - static_cast<int64_t>(d - 1) * tau;
+        if (npat > 0) {
+            const int nf = kFactorial[d];
+            for (int k = threadIdx.x; k < nf; k += blockDim.x) sm[k] = 0u;
+            __syncthreads();
+            for (int64_t i = threadIdx.x; i < npat; i += blockDim.x) {
+                float v[7];
+                for (int j = 0; j < d; ++j) v[j] = x[i + static_cast<int64_t>(j) * tau];
+                int id = 0;
+                for (int j = 0; j < d; ++j) {
+                    int pos = 0;
+                    for (int l = 0; l < d; ++l) pos += (v[l] < v[j] || (v[l] == v[j] && l < j)) ? 1 : 0;
+                    id += j * kFactorial[d - 1 - pos];
+                }
+                atomicAdd(&sm[id], 1u);
+            }
+            __syncthreads();
+            double h = 0.0;
+            for (int k = threadIdx.x; k < nf; k += blockDim.x)
+                if (sm[k] > 0u) {
+                    const double p = static_cast<double>(sm[k]) / static_cast<double>(npat);
+                    h -= p * log(p);
+                }
+            h = block_sum_d(h, red);
+            result = nf > 1 ? h / log(static_cast<double>(nf)) : h;
+        }
+    } else {
+        const int bins = static_cast<int>(plan.param[m]);
+        double lo = CUDART_INF, hi = -CUDART_INF;
+        for (int i = threadIdx.x; i < nwin; i += blockDim.x) {
+            lo = fmin(lo, static_cast<double>(x[i]));
+            hi = fmax(hi, static_cast<double>(x[i]));
+        }
+        lo = -block_max_d(-lo, red);
+        hi = block_max_d(hi, red);
+        const double range = (hi - lo) + 1e-10;
+        unsigned char* sym = reinterpret_cast<unsigned char*>(sm);
+        unsigned* keys = sm + (nwin + 15) / 16 * 4;
+        unsigned* vals = keys + table_size;
+        for (int i = threadIdx.x; i < nwin; i += blockDim.x) {
+            const long long b = static_cast<long long>((static_cast<double>(x[i]) - lo) / range * bins);
+            sym[i] = static_cast<unsigned char>(b < 0 ? 0 : (b > bins - 1 ? bins - 1 : b));
+        }
+        for (int q = threadIdx.x; q < table_size; q += blockDim.x) keys[q] = 0xffffffffu;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned mask = static_cast<unsigned>(table_size - 1);
+            int shift = 32;
+            for (int t = table_size; t > 1; t >>= 1) --shift;
+            unsigned nodes = 1u;
+            int complexity = 0;
+            int64_t i = 0;
+            while (i < nwin) {
+                unsigned node = 0u;
+                int64_t len = 1;
+                while (i + len <= nwin) {
+                    const unsigned key = node * 256u + sym[i + len - 1];
+                    unsigned h = (key * 2654435761u) >> shift;
+                    while (keys[h] != 0xffffffffu && keys[h] != key) h = (h + 1u) & mask;  // never full
+                    if (keys[h] == 0xffffffffu) {
+                        keys[h] = key;
+                        vals[h] = nodes++;
+                        ++complexity;
+                        break;
+                    }
+                    node = vals[h];
+                    ++len;
+                }
+                i += len;
+            }
+            const double nn = static_cast<double>(nwin);
+            result = nwin > 1 ? complexity / (nn / (log(nn) + 1e-10)) : static_cast<double>(complexity);
+        }
     }
     if (threadIdx.x == 0) out[traj * n_features + plan.col[m]] = result;
 }
@@ -1235,7 +1362,7 @@ static cudaError_t sort_by_probe(const pb_solve_args& a, const ScratchLayout& sl
 
 static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
 {
-    int m = 0, np = 0, ns = 0, nsp = 0;
+    int m = 0, np = 0, ns = 0, nsp = 0, nsy = 0;
     for (int c = 0; c < a.n_features; ++c)
         if (PB_FEAT_IS_WINDOW(a.feat_kind[c])) {
             if (plan) {
@@ -1250,11 +1377,14 @@ static int count_median_cols(const pb_solve_args& a, MedianPlan* plan)
             ns += PB_FEAT_IS_SORTED(a.feat_kind[c]) ? 1 : 0;
             if (plan && PB_FEAT_IS_SPECTRAL(a.feat_kind[c])) plan->spectral_m[nsp] = m;
             nsp += PB_FEAT_IS_SPECTRAL(a.feat_kind[c]) ? 1 : 0;
+            if (plan && PB_FEAT_IS_SYMBOLIC(a.feat_kind[c])) plan->symbolic_m[nsy] = m;
+            nsy += PB_FEAT_IS_SYMBOLIC(a.feat_kind[c]) ? 1 : 0;
             ++m;
         }
     if (plan) {
         plan->n_sorted = ns;
         plan->n_spectral = nsp;
+        plan->n_symbolic = nsy;
         plan->n_med = m;
         plan->n_peak_cols = np;
         plan->peak_cap = a.peak_cap;
@@ -1305,11 +1435,14 @@ int validate_args(const pb_solve_args* a, bool user_system)
             return PB_EINVAL;
         if (PB_FEAT_IS_SORTED(kind) && a->n_save - a->win_begin > PB_SORTED_WINDOW_MAX) return PB_EUNSUPPORTED;
         if (PB_FEAT_IS_SPECTRAL(kind) && a->n_save - a->win_begin > PB_SPECTRAL_WINDOW_MAX) return PB_EUNSUPPORTED;
+        if (kind == PB_FEAT_LEMPEL_ZIV && a->n_save - a->win_begin > PB_SYMBOLIC_WINDOW_MAX) return PB_EUNSUPPORTED;
         const double prm2 = a->feat_param2[c];
         const auto is_int = [](double v, double lo, double hi) {
             return v >= lo && v <= hi && v == static_cast<double>(static_cast<int>(v));
         };
         if (kind == PB_FEAT_PARTIAL_AUTOCORRELATION && !is_int(prm, 0.0, 63.0)) return PB_EINVAL;
+        if (kind == PB_FEAT_PERMUTATION_ENTROPY && !(is_int(prm, 1.0, 1e6) && is_int(prm2, 1.0, 7.0))) return PB_EINVAL;
+        if (kind == PB_FEAT_LEMPEL_ZIV && !is_int(prm, 1.0, 255.0)) return PB_EINVAL;
         if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))
             return PB_EINVAL;
         if (kind >= PB_FEAT_AGG_AUTOCORR_MEAN && kind <= PB_FEAT_AGG_AUTOCORR_VAR && !is_int(prm, 0.0, 128.0))
@@ -1474,6 +1607,27 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
             k_window_spectrum<<<static_cast<unsigned>(sblocks), 256, smem, st>>>(
                 reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), nwin,
                 plan, a.features_out, a.n_features);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return map_cuda(e);
+        }
+        if (plan.n_symbolic > 0) {
+            const int nwin = a.n_save - a.win_begin;
+            bool lz = false;
+            for (int q = 0; q < plan.n_symbolic; ++q) lz |= plan.kind[plan.symbolic_m[q]] == PB_FEAT_LEMPEL_ZIV;
+            // trie table: a power of two >= 2 (nwin + 1) entries (at most half full), keys and children
+            int table = 1;
+            while (table < 2 * (nwin + 1)) table <<= 1;
+            size_t smem = 5040 * sizeof(unsigned);  // the permutation histogram (d <= 7)
+            if (lz) smem = std::max(smem, static_cast<size_t>((nwin + 15) / 16 * 16) + 2 * sizeof(unsigned) * table);
+            const int64_t sblocks = a.n_traj * plan.n_symbolic;
+            if (sblocks > 0x7fffffffLL) return PB_EINVAL;
+            if (smem > 48 * 1024)
+                e = cudaFuncSetAttribute(k_window_symbolic, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+            if (e != cudaSuccess) return map_cuda(e);
+            k_window_symbolic<<<static_cast<unsigned>(sblocks), 256, smem, st>>>(
+                reinterpret_cast<const float*>(static_cast<const unsigned char*>(a.scratch) + sl.median_off), nwin,
+                table, plan, a.features_out, a.n_features);
             e = cudaGetLastError();
             if (e != cudaSuccess) return map_cuda(e);
         }

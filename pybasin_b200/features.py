@@ -80,6 +80,8 @@ FEATURE_KINDS: dict[str, int] = {
     "count_value": L.FEAT_COUNT_VALUE,
     "partial_autocorrelation": L.FEAT_PARTIAL_AUTOCORRELATION,
     "spectral_frequency_ratio": L.FEAT_SPECTRAL_FREQ_RATIO,
+    "fourier_entropy": L.FEAT_FOURIER_ENTROPY,
+    "lempel_ziv_complexity": L.FEAT_LEMPEL_ZIV,
 }
 
 #: Features with several parameters (FCParameters keys as in the reference's
@@ -92,6 +94,7 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "change_quantiles": None,
     "autocorrelation_periodicity": [{"output": "strength"}],
     "fft_aggregated": [{"aggtype": "centroid"}],
+    "permutation_entropy": [{"tau": 1, "dimension": 3}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -123,6 +126,9 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
         if agg not in kinds:
             raise ValueError(f"fft_aggregated: aggtype must be one of {sorted(kinds)}, got {agg!r}")
         return FeatureColumn(state, kinds[agg], 0.0, name)
+    if fname == "permutation_entropy":  # torch_features_entropy_complexity.py:13-54
+        return FeatureColumn(state, L.FEAT_PERMUTATION_ENTROPY, float(p.get("tau", 1)), name,
+                             float(p.get("dimension", 3)))
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140
@@ -161,6 +167,8 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_MEAN_N_ABS_MAX: ("number_of_maxima", 1.0),
     L.FEAT_COUNT_VALUE: ("value", 0.0),
     L.FEAT_PARTIAL_AUTOCORRELATION: ("lag", 1.0),
+    L.FEAT_FOURIER_ENTROPY: ("bins", 10.0),
+    L.FEAT_LEMPEL_ZIV: ("bins", 2.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).

@@ -213,6 +213,12 @@ def _features(ref: Path) -> None:
         **{f"{src}_fft_aggregated_{a}": fq.fft_aggregated(v, a).numpy()
            for src, v in (("x", x), ("periodic", per), ("even", even))
            for a in ("centroid", "variance", "skew", "kurtosis")},
+        # entropies and complexity
+        **{f"{src}_fourier_entropy": ec.fourier_entropy(v, 10).numpy() for src, v in (("x", x), ("periodic", per))},
+        **{f"{src}_permutation_entropy_{t}_{d}": ec.permutation_entropy(v, t, d).numpy()
+           for src, v in (("x", x), ("periodic", per)) for (t, d) in ((1, 3), (1, 4), (2, 5), (1, 7), (3, 3))},
+        **{f"{src}_lempel_ziv_complexity_{b}": ec.lempel_ziv_complexity(v, b).numpy()
+           for src, v in (("x", x), ("periodic", per)) for b in (2, 3, 5, 10, 100)},
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

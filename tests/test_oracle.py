@@ -230,12 +230,19 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
           for name, kind in (("spectral_frequency_ratio", 79), ("fft_aggregated_centroid", 80),
                              ("fft_aggregated_variance", 81), ("fft_aggregated_skew", 82),
                              ("fft_aggregated_kurtosis", 83))],
+        *[(f"{tag}_{name}", src, kind, p1, p2)
+          for tag, src in (("x", "x"), ("periodic", "x_periodic"))
+          for name, kind, p1, p2 in (("fourier_entropy", 84, 10.0, 0.0),
+                                     *[(f"permutation_entropy_{t}_{d}", 85, float(t), float(d))
+                                       for (t, d) in ((1, 3), (1, 4), (2, 5), (1, 7), (3, 3))],
+                                     *[(f"lempel_ziv_complexity_{b}", 86, float(b), 0.0) for b in (2, 3, 5, 10, 100)])],
     ],
 )
 def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name, src, kind, param, param2):
     """Partial and aggregated autocorrelation, autocorrelation periodicity (noisy
     sine waves of 16 periods, one constant column), spectral frequency ratio and
-    aggregated spectrum moments (odd and even lengths), energy ratio of a chunk,
+    aggregated spectrum moments (odd and even lengths), Fourier and permutation
+    entropy, Lempel-Ziv complexity (exact phrase counts), energy ratio of a chunk,
     count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
@@ -248,7 +255,7 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
                     for b in range(x.shape[1])])
     if 67 <= kind <= 70 or kind == 77:
         np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
-    elif 80 <= kind <= 83:  # torch's FFT against the oracle's direct sums
+    elif 80 <= kind <= 84:  # torch's FFT against the oracle's direct sums
         np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12)
     else:
         np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)
