@@ -159,10 +159,16 @@ typedef enum {
        torch_features_entropy_complexity.py:97-110), permutation_entropy (tau,
        feat_param2 = dimension <= 7; :13-54), lempel_ziv_complexity (bins <= 255, at
        most PB_SYMBOLIC_WINDOW_MAX window samples; :141-178) */
-    PB_FEAT_FOURIER_ENTROPY = 84, PB_FEAT_PERMUTATION_ENTROPY = 85, PB_FEAT_LEMPEL_ZIV = 86
+    PB_FEAT_FOURIER_ENTROPY = 84, PB_FEAT_PERMUTATION_ENTROPY = 85, PB_FEAT_LEMPEL_ZIV = 86,
+    /* agg_linear_trend (chunk_size, feat_param2 = attribute 0..4: slope, intercept,
+       rvalue, pvalue, stderr; f_agg mean / var / min / max in the kind;
+       torch_features_trend.py:60-83), ar_coefficient (k <= 10, feat_param2 = coeff;
+       Yule-Walker, torch_features_trend.py:86-131) */
+    PB_FEAT_AGG_TREND_MEAN = 87, PB_FEAT_AGG_TREND_VAR = 88, PB_FEAT_AGG_TREND_MIN = 89,
+    PB_FEAT_AGG_TREND_MAX = 90, PB_FEAT_AR_COEFFICIENT = 91
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_LEMPEL_ZIV
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..86): the
+#define PB_FEAT_LAST_KIND PB_FEAT_AR_COEFFICIENT
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..91): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window

@@ -163,6 +163,34 @@ static void power_spectrum(const double *w, int n, double shift, double *psd)
     }
 }
 
+/* torch_features_trend.py:11-51: least squares of a on t = 0..n-1, attribute 0..4
+   = slope, intercept, rvalue, the reference's pseudo p-value 1 / (1 + |t|), stderr */
+static double trend_attr(const double *a, int n, int attr)
+{
+    double am = 0.0;
+    for (int i = 0; i < n; ++i) am += a[i];
+    am /= n;
+    const double tm = 0.5 * (n - 1.0);
+    double ss_tt = 0.0, ss_tx = 0.0, ss_xx = 0.0;
+    for (int i = 0; i < n; ++i) {
+        ss_tt += (i - tm) * (i - tm);
+        ss_tx += (i - tm) * (a[i] - am);
+        ss_xx += (a[i] - am) * (a[i] - am);
+    }
+    const double slope = ss_tx / (ss_tt + 1e-10), intercept = am - slope * tm;
+    const double r = ss_tx / (sqrt(ss_tt * ss_xx) + 1e-10);
+    if (attr == 0) return slope;
+    if (attr == 1) return intercept;
+    if (attr == 2) return r;
+    if (attr == 3) return 1.0 / (1.0 + fabs(r * sqrt(n - 2.0) / (sqrt(1.0 - r * r) + 1e-10)));
+    double rss = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double e = a[i] - (slope * i + intercept);
+        rss += e * e;
+    }
+    return sqrt(rss / (n - 2.0) / (ss_tt + 1e-10));
+}
+
 static double window_feature(int feat, double param, double param2, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
@@ -751,6 +779,70 @@ static double window_feature(int feat, double param, double param2, const double
         free(child);
         const double b_n = n > 1 ? n / (log((double)n) + 1e-10) : 1.0;
         return complexity / b_n;
+    }
+    /* torch_features_trend.py:60-83: linear trend of the chunk aggregates (mean,
+       population variance, min or max of consecutive chunks of chunk_size samples;
+       a partial last chunk is dropped); 0 with fewer than two chunks */
+    case ORACLE_F_AGG_TREND_MEAN: case ORACLE_F_AGG_TREND_VAR: case ORACLE_F_AGG_TREND_MIN:
+    case ORACLE_F_AGG_TREND_MAX: {
+        const int cs = (int)param, nc = cs > 0 ? n / cs : 0;
+        if (nc < 2) return 0.0;
+        for (int c = 0; c < nc; ++c) {
+            const double *q = w + (long)c * cs;
+            double s1 = 0.0, lo = q[0], hi = q[0];
+            for (int i = 0; i < cs; ++i) {
+                s1 += q[i];
+                if (q[i] < lo) lo = q[i];
+                if (q[i] > hi) hi = q[i];
+            }
+            const double cm = s1 / cs;
+            double v = 0.0;
+            for (int i = 0; i < cs; ++i) v += (q[i] - cm) * (q[i] - cm);
+            scratch[c] = feat == ORACLE_F_AGG_TREND_MEAN ? cm
+                         : feat == ORACLE_F_AGG_TREND_VAR ? v / cs
+                         : feat == ORACLE_F_AGG_TREND_MIN ? lo : hi;
+        }
+        return trend_attr(scratch, nc, (int)param2);
+    }
+    /* torch_features_trend.py:86-131: Yule-Walker, R phi = r with R_ij =
+       acf[|i-j|] + 1e-6 delta_ij and r = acf[1..k], acf[k] = sum d_i d_(i+k) /
+       (sum d_i^2 + 1e-10); coefficient `coeff` of phi (0 when coeff >= k), solved by
+       Gaussian elimination with partial pivoting */
+    case ORACLE_F_AR_COEFFICIENT: {
+        const int k = (int)param, coeff = (int)param2;
+        if (coeff >= k || k < 1 || k > 10) return 0.0;
+        double acf[11], R[10][11];
+        for (int l = 0; l <= k; ++l) {
+            double r = 0.0;
+            for (int i = 0; i + l < n; ++i) r += (w[i] - mean) * (w[i + l] - mean);
+            acf[l] = r / (m2 + 1e-10);
+        }
+        for (int i = 0; i < k; ++i) {
+            for (int j = 0; j < k; ++j) R[i][j] = acf[abs(i - j)] + (i == j ? 1e-6 : 0.0);
+            R[i][k] = acf[i + 1];
+        }
+        for (int c = 0; c < k; ++c) {
+            int piv = c;
+            for (int i = c + 1; i < k; ++i)
+                if (fabs(R[i][c]) > fabs(R[piv][c])) piv = i;
+            if (piv != c)
+                for (int j = 0; j <= k; ++j) {
+                    const double t = R[c][j];
+                    R[c][j] = R[piv][j];
+                    R[piv][j] = t;
+                }
+            for (int i = c + 1; i < k; ++i) {
+                const double f = R[i][c] / R[c][c];
+                for (int j = c; j <= k; ++j) R[i][j] -= f * R[c][j];
+            }
+        }
+        double phi[10];
+        for (int i = k - 1; i >= 0; --i) {
+            double t = R[i][k];
+            for (int j = i + 1; j < k; ++j) t -= R[i][j] * phi[j];
+            phi[i] = t / R[i][i];
+        }
+        return phi[coeff];
     }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;

@@ -63,6 +63,10 @@ enum {
     /* fourier_entropy (bins, unused by the reference), permutation_entropy (tau,
        dimension), lempel_ziv_complexity (bins) */
     ORACLE_F_FOURIER_ENTROPY = 84, ORACLE_F_PERMUTATION_ENTROPY = 85, ORACLE_F_LEMPEL_ZIV = 86,
+    /* agg_linear_trend (chunk_size, attr index 0..4 = slope, intercept, rvalue,
+       pvalue, stderr; f_agg mean / var / min / max), ar_coefficient (k <= 10, coeff) */
+    ORACLE_F_AGG_TREND_MEAN = 87, ORACLE_F_AGG_TREND_VAR = 88, ORACLE_F_AGG_TREND_MIN = 89,
+    ORACLE_F_AGG_TREND_MAX = 90, ORACLE_F_AR_COEFFICIENT = 91,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

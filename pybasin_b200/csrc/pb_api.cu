@@ -90,6 +90,37 @@ __device__ __forceinline__ double warp_sum_d(double v)
     return v;
 }
 
+// Least squares of a series a(0..cnt-1) on t = 0..cnt-1 (torch_features_trend.py:11-51),
+// warp-collective: attr 0..4 = slope, intercept, rvalue, the reference's pseudo
+// p-value 1 / (1 + |t|), stderr.  `a` is evaluated on demand (two or three passes).
+template <class Series>
+__device__ double warp_trend(const Series& a, int cnt, int attr, int lane)
+{
+    double s = 0.0;
+    for (int i = lane; i < cnt; i += 32) s += a(i);
+    const double am = warp_sum_d(s) / cnt, tm = 0.5 * (cnt - 1.0);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int i = lane; i < cnt; i += 32) {
+        const double dt = static_cast<double>(i) - tm, dx = a(i) - am;
+        a0 += dt * dt;
+        a1 += dt * dx;
+        a2 += dx * dx;
+    }
+    const double ss_tt = warp_sum_d(a0), ss_tx = warp_sum_d(a1), ss_xx = warp_sum_d(a2);
+    const double slope = ss_tx / (ss_tt + 1e-10), intercept = am - slope * tm;
+    const double r = ss_tx / (sqrt(ss_tt * ss_xx) + 1e-10);
+    if (attr == 0) return slope;
+    if (attr == 1) return intercept;
+    if (attr == 2) return r;
+    if (attr == 3) return 1.0 / (1.0 + fabs(r * sqrt(cnt - 2.0) / (sqrt(1.0 - r * r) + 1e-10)));
+    double rss = 0.0;
+    for (int i = lane; i < cnt; i += 32) {
+        const double e = a(i) - (slope * static_cast<double>(i) + intercept);
+        rss += e * e;
+    }
+    return sqrt(warp_sum_d(rss) / (cnt - 2.0) / (ss_tt + 1e-10));
+}
+
 // Window pass: one warp per (trajectory, window column) computes the column's
 // feature from the stored window (torch semantics of the reference calculators:
 // median = lower middle value, quantile = linear interpolation, NaN in -> NaN out
@@ -769,6 +800,92 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 result = kind == PB_FEAT_ACF_PERIOD_STRENGTH ? out_v : out_lag;
                 break;
             }
+            case PB_FEAT_AGG_TREND_MEAN:
+            case PB_FEAT_AGG_TREND_VAR:
+            case PB_FEAT_AGG_TREND_MIN:
+            case PB_FEAT_AGG_TREND_MAX: {
+                // linear trend of chunk aggregates (a partial last chunk dropped), each
+                // chunk aggregated sequentially by the lane that needs it
+                const int cs = static_cast<int>(param), nc = nwin / cs;
+                if (nc < 2) {
+                    result = 0.0;
+                    break;
+                }
+                const auto agg = [&](int c) -> double {
+                    const float* q = x + static_cast<int64_t>(c) * cs;
+                    double s1 = 0.0, lo = q[0], hi = q[0];
+                    for (int i = 0; i < cs; ++i) {
+                        const double v = static_cast<double>(q[i]);
+                        s1 += v;
+                        lo = v < lo ? v : lo;
+                        hi = v > hi ? v : hi;
+                    }
+                    const double cm = s1 / cs;
+                    if (kind == PB_FEAT_AGG_TREND_MEAN) return cm;
+                    if (kind == PB_FEAT_AGG_TREND_MIN) return lo;
+                    if (kind == PB_FEAT_AGG_TREND_MAX) return hi;
+                    double v2 = 0.0;
+                    for (int i = 0; i < cs; ++i) v2 += (static_cast<double>(q[i]) - cm) * (static_cast<double>(q[i]) - cm);
+                    return v2 / cs;
+                };
+                result = warp_trend(agg, nc, static_cast<int>(plan.param2[m]), lane);
+                break;
+            }
+            case PB_FEAT_AR_COEFFICIENT: {
+                // Yule-Walker: R phi = r, R_ij = acf[|i-j|] + 1e-6 delta_ij, r = acf[1..k];
+                // acf by warp reductions into this warp's shared doubles (R at [0, 110),
+                // acf at [110, 121)), elimination with partial pivoting on lane 0
+                const int k = static_cast<int>(param), coeff = static_cast<int>(plan.param2[m]);
+                if (coeff >= k) {
+                    result = 0.0;
+                    break;
+                }
+                double* hd = reinterpret_cast<double*>(h);
+                double* acf = hd + 110;
+                for (int i = lane; i < nwin; i += 32) {
+                    const double d = static_cast<double>(x[i]) - mean;
+                    a0 += d * d;
+                }
+                const double m2 = warp_sum_d(a0);
+                for (int l = 1; l <= k; ++l) {
+                    double r = 0.0;
+                    for (int i = lane; i + l < nwin; i += 32)
+                        r += (static_cast<double>(x[i]) - mean) * (static_cast<double>(x[i + l]) - mean);
+                    r = warp_sum_d(r);
+                    if (lane == 0) acf[l] = r / (m2 + 1e-10);
+                }
+                if (lane == 0) {
+                    acf[0] = m2 / (m2 + 1e-10);
+                    double* R = hd;  // k rows of k + 1 (the last column: r, then phi)
+                    for (int i = 0; i < k; ++i) {
+                        for (int j = 0; j < k; ++j) R[i * 11 + j] = acf[abs(i - j)] + (i == j ? 1e-6 : 0.0);
+                        R[i * 11 + k] = acf[i + 1];
+                    }
+                    for (int c = 0; c < k; ++c) {
+                        int piv = c;
+                        for (int i = c + 1; i < k; ++i)
+                            if (fabs(R[i * 11 + c]) > fabs(R[piv * 11 + c])) piv = i;
+                        if (piv != c)
+                            for (int j = 0; j <= k; ++j) {
+                                const double t = R[c * 11 + j];
+                                R[c * 11 + j] = R[piv * 11 + j];
+                                R[piv * 11 + j] = t;
+                            }
+                        for (int i = c + 1; i < k; ++i) {
+                            const double f = R[i * 11 + c] / R[c * 11 + c];
+                            for (int j = c; j <= k; ++j) R[i * 11 + j] -= f * R[c * 11 + j];
+                        }
+                    }
+                    for (int i = k - 1; i >= 0; --i) {
+                        double t = R[i * 11 + k];
+                        for (int j = i + 1; j < k; ++j) t -= R[i * 11 + j] * R[j * 11 + k];
+                        R[i * 11 + k] = t / R[i * 11 + i];
+                    }
+                    result = R[coeff * 11 + k];
+                }
+                __syncwarp();
+                break;
+            }
             case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
                 const float v = static_cast<float>(param);
                 for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
@@ -1443,6 +1560,10 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_PARTIAL_AUTOCORRELATION && !is_int(prm, 0.0, 63.0)) return PB_EINVAL;
         if (kind == PB_FEAT_PERMUTATION_ENTROPY && !(is_int(prm, 1.0, 1e6) && is_int(prm2, 1.0, 7.0))) return PB_EINVAL;
         if (kind == PB_FEAT_LEMPEL_ZIV && !is_int(prm, 1.0, 255.0)) return PB_EINVAL;
+        if (kind >= PB_FEAT_AGG_TREND_MEAN && kind <= PB_FEAT_AGG_TREND_MAX &&
+            !(is_int(prm, 1.0, 1e9) && is_int(prm2, 0.0, 4.0)))
+            return PB_EINVAL;
+        if (kind == PB_FEAT_AR_COEFFICIENT && !(is_int(prm, 1.0, 10.0) && is_int(prm2, 0.0, 1e6))) return PB_EINVAL;
         if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))
             return PB_EINVAL;
         if (kind >= PB_FEAT_AGG_AUTOCORR_MEAN && kind <= PB_FEAT_AGG_AUTOCORR_VAR && !is_int(prm, 0.0, 128.0))

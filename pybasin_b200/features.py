@@ -95,6 +95,8 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "autocorrelation_periodicity": [{"output": "strength"}],
     "fft_aggregated": [{"aggtype": "centroid"}],
     "permutation_entropy": [{"tau": 1, "dimension": 3}],
+    "agg_linear_trend": [{"attr": "slope", "chunk_size": 10, "f_agg": "mean"}],
+    "ar_coefficient": [{"coeff": 0, "k": 1}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -129,6 +131,16 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
     if fname == "permutation_entropy":  # torch_features_entropy_complexity.py:13-54
         return FeatureColumn(state, L.FEAT_PERMUTATION_ENTROPY, float(p.get("tau", 1)), name,
                              float(p.get("dimension", 3)))
+    if fname == "agg_linear_trend":  # torch_features_trend.py:60-83
+        kinds = {"mean": L.FEAT_AGG_TREND_MEAN, "var": L.FEAT_AGG_TREND_VAR, "min": L.FEAT_AGG_TREND_MIN,
+                 "max": L.FEAT_AGG_TREND_MAX}
+        f_agg, attr = p.get("f_agg", "mean"), p.get("attr", "slope")
+        if f_agg not in kinds or attr not in _TREND_ATTRS:
+            raise ValueError(f"agg_linear_trend: f_agg in {sorted(kinds)}, attr in {_TREND_ATTRS}; got {f_agg!r}, {attr!r}")
+        return FeatureColumn(state, kinds[f_agg], float(p.get("chunk_size", 10)), name,
+                             float(_TREND_ATTRS.index(attr)))
+    if fname == "ar_coefficient":  # torch_features_trend.py:86-131
+        return FeatureColumn(state, L.FEAT_AR_COEFFICIENT, float(p.get("k", 1)), name, float(p.get("coeff", 0)))
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140
@@ -145,7 +157,12 @@ FEATURE_ATTR: dict[str, tuple[dict[str, int], str, str | None, float]] = {
     "linear_trend": ({"slope": L.FEAT_TREND_SLOPE, "intercept": L.FEAT_TREND_INTERCEPT,
                       "rvalue": L.FEAT_TREND_RVALUE, "pvalue": L.FEAT_TREND_PVALUE,
                       "stderr": L.FEAT_TREND_STDERR}, "slope", None, 0.0),
+    # the reference's linear_trend_timewise is linear_trend (torch_features_trend.py:54-56)
+    "linear_trend_timewise": ({"slope": L.FEAT_TREND_SLOPE, "intercept": L.FEAT_TREND_INTERCEPT,
+                               "rvalue": L.FEAT_TREND_RVALUE, "pvalue": L.FEAT_TREND_PVALUE,
+                               "stderr": L.FEAT_TREND_STDERR}, "slope", None, 0.0),
 }
+_TREND_ATTRS = ("slope", "intercept", "rvalue", "pvalue", "stderr")
 
 #: The parameter of each parameterised feature (its FCParameters key) and default.
 FEATURE_PARAM: dict[int, tuple[str, float]] = {

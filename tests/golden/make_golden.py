@@ -219,6 +219,16 @@ def _features(ref: Path) -> None:
            for src, v in (("x", x), ("periodic", per)) for (t, d) in ((1, 3), (1, 4), (2, 5), (1, 7), (3, 3))},
         **{f"{src}_lempel_ziv_complexity_{b}": ec.lempel_ziv_complexity(v, b).numpy()
            for src, v in (("x", x), ("periodic", per)) for b in (2, 3, 5, 10, 100)},
+        # trends of chunk aggregates, AR coefficients
+        **{f"{src}_agg_linear_trend_{a}_{c}_{f}": tr.agg_linear_trend(v, c, f, a).numpy()
+           for src, v in (("x", x), ("periodic", per))
+           for a in ("slope", "intercept", "rvalue", "pvalue", "stderr") for c in (5, 50, 200) for f in
+           ("mean", "var", "min", "max")},
+        **{f"{src}_linear_trend_timewise_{a}": tr.linear_trend_timewise(v, a).numpy()
+           for src, v in (("x", x),) for a in ("slope", "rvalue")},
+        **{f"{src}_ar_coefficient_{k}_{c}": tr.ar_coefficient(v, k, c).numpy()
+           for src, v in (("x", x), ("periodic", per)) for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0),
+                                                                       (4, 2))},
     }
     np.savez_compressed(OUT / "features_reference.npz", **res)
 

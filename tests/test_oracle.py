@@ -236,13 +236,22 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
                                      *[(f"permutation_entropy_{t}_{d}", 85, float(t), float(d))
                                        for (t, d) in ((1, 3), (1, 4), (2, 5), (1, 7), (3, 3))],
                                      *[(f"lempel_ziv_complexity_{b}", 86, float(b), 0.0) for b in (2, 3, 5, 10, 100)])],
+        *[(f"{tag}_agg_linear_trend_{a}_{c}_{f}", src, 87 + fi, float(c), float(ai))
+          for tag, src in (("x", "x"), ("periodic", "x_periodic"))
+          for ai, a in enumerate(("slope", "intercept", "rvalue", "pvalue", "stderr")) for c in (5, 50, 200)
+          for fi, f in enumerate(("mean", "var", "min", "max"))],
+        *[(f"x_linear_trend_timewise_{a}", "x", 36 + i, 0.0, 0.0) for i, a in ((0, "slope"), (2, "rvalue"))],
+        *[(f"{tag}_ar_coefficient_{k}_{c}", src, 91, float(k), float(c))
+          for tag, src in (("x", "x"), ("periodic", "x_periodic"))
+          for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0), (4, 2))],
     ],
 )
 def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name, src, kind, param, param2):
     """Partial and aggregated autocorrelation, autocorrelation periodicity (noisy
     sine waves of 16 periods, one constant column), spectral frequency ratio and
     aggregated spectrum moments (odd and even lengths), Fourier and permutation
-    entropy, Lempel-Ziv complexity (exact phrase counts), energy ratio of a chunk,
+    entropy, Lempel-Ziv complexity (exact phrase counts), trends of chunk
+    aggregates, AR coefficients (Yule-Walker), energy ratio of a chunk,
     count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
@@ -255,6 +264,8 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
                     for b in range(x.shape[1])])
     if 67 <= kind <= 70 or kind == 77:
         np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
+    elif kind == 91:  # Yule-Walker solved by torch's LU against the oracle's elimination
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12)
     elif 80 <= kind <= 84:  # torch's FFT against the oracle's direct sums
         np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12)
     else:
