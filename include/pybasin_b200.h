@@ -165,10 +165,15 @@ typedef enum {
        torch_features_trend.py:60-83), ar_coefficient (k <= 10, feat_param2 = coeff;
        Yule-Walker, torch_features_trend.py:86-131) */
     PB_FEAT_AGG_TREND_MEAN = 87, PB_FEAT_AGG_TREND_VAR = 88, PB_FEAT_AGG_TREND_MIN = 89,
-    PB_FEAT_AGG_TREND_MAX = 90, PB_FEAT_AR_COEFFICIENT = 91
+    PB_FEAT_AGG_TREND_MAX = 90, PB_FEAT_AR_COEFFICIENT = 91,
+    /* cwt_coefficients (w, feat_param2 = coeff, -1 when w is not one of the widths;
+       Ricker wavelet, torch_features_frequency.py:71-127), friedrich_coefficients
+       (m <= 6, feat_param2 = coeff) and max_langevin_fixed_point (m <= 6)
+       (torch_features_dynamical.py:87-174) */
+    PB_FEAT_CWT = 92, PB_FEAT_FRIEDRICH = 93, PB_FEAT_LANGEVIN = 94
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_AR_COEFFICIENT
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..91): the
+#define PB_FEAT_LAST_KIND PB_FEAT_LANGEVIN
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..94): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window

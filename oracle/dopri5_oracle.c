@@ -191,6 +191,55 @@ static double trend_attr(const double *a, int n, int attr)
     return sqrt(rss / (n - 2.0) / (ss_tt + 1e-10));
 }
 
+/* Least squares of velocity v_i = w[i+1] - w[i] on the powers p_i^m .. p_i^0 of
+   position p_i = w[i] (i < n-1) by the regularised normal equations (V'V + 1e-6 I)
+   c = V'v, solved with partial pivoting (torch_features_dynamical.py:87-127);
+   c[0] multiplies p^m.  Returns 0, or -1 when n < 2. */
+static int poly_velocity_fit(const double *w, int n, int m, double *c)
+{
+    if (n < 2) return -1;
+    double A[7][8], pw[13];
+    for (int i = 0; i <= m; ++i)
+        for (int j = 0; j <= m + 1; ++j) A[i][j] = 0.0;
+    double S[13], T[7];
+    for (int q = 0; q <= 2 * m; ++q) S[q] = 0.0;
+    for (int q = 0; q <= m; ++q) T[q] = 0.0;
+    for (int i = 0; i + 1 < n; ++i) {
+        const double p = w[i], v = w[i + 1] - w[i];
+        pw[0] = 1.0;
+        for (int q = 1; q <= 2 * m; ++q) pw[q] = pw[q - 1] * p;
+        for (int q = 0; q <= 2 * m; ++q) S[q] += pw[q];
+        for (int q = 0; q <= m; ++q) T[q] += pw[q] * v;
+    }
+    /* row a, column b of V'V: sum p^(m-a) p^(m-b) */
+    for (int a = 0; a <= m; ++a) {
+        for (int b = 0; b <= m; ++b) A[a][b] = S[2 * m - a - b] + (a == b ? 1e-6 : 0.0);
+        A[a][m + 1] = T[m - a];
+    }
+    const int k = m + 1;
+    for (int col = 0; col < k; ++col) {
+        int piv = col;
+        for (int i = col + 1; i < k; ++i)
+            if (fabs(A[i][col]) > fabs(A[piv][col])) piv = i;
+        if (piv != col)
+            for (int j = 0; j <= k; ++j) {
+                const double t = A[col][j];
+                A[col][j] = A[piv][j];
+                A[piv][j] = t;
+            }
+        for (int i = col + 1; i < k; ++i) {
+            const double f = A[i][col] / A[col][col];
+            for (int j = col; j <= k; ++j) A[i][j] -= f * A[col][j];
+        }
+    }
+    for (int i = k - 1; i >= 0; --i) {
+        double t = A[i][k];
+        for (int j = i + 1; j < k; ++j) t -= A[i][j] * c[j];
+        c[i] = t / A[i][i];
+    }
+    return 0;
+}
+
 static double window_feature(int feat, double param, double param2, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
@@ -843,6 +892,58 @@ static double window_feature(int feat, double param, double param2, const double
             phi[i] = t / R[i][i];
         }
         return phi[coeff];
+    }
+    /* torch_features_frequency.py:71-127: the Ricker wavelet of width w on t = -4w..4w,
+       (2 / (sqrt(3w) pi^0.25)) (1 - (t/w)^2) exp(-t^2 / (2 w^2)) -- the reference forms
+       the prefactor in FP32 (its sqrt of a default-dtype tensor), so it is rounded
+       the same way here -- correlated with the window padded by 4w samples
+       (reflected without repeating the edge, or replicated when n < 4w); the output
+       at index coeff (0 past the end or when w is not one of the widths) */
+    case ORACLE_F_CWT: {
+        const int wd = (int)param, coeff = (int)param2;
+        if (coeff < 0 || coeff >= n || wd < 1) return 0.0;
+        const float s32 = sqrtf((float)(3.0 * wd));
+        const double pi = 3.14159265358979323846;
+        const float pref32 = 2.0f / (s32 * (float)pow(pi, 0.25));
+        const double pref = (double)pref32, sig = (double)wd;
+        const int pad = 4 * wd;
+        double acc = 0.0;
+        for (int j = 0; j <= 8 * wd; ++j) {
+            const double t = (double)(j - pad);
+            const double psi = pref * (1.0 - (t / sig) * (t / sig)) * exp(-(t * t) / (2.0 * sig * sig));
+            long q = (long)coeff + j - pad;
+            if (n >= pad) {
+                if (q < 0) q = -q;
+                if (q >= n) q = 2L * (n - 1) - q;
+            } else {
+                q = q < 0 ? 0 : (q >= n ? n - 1 : q);
+            }
+            acc += w[q] * psi;
+        }
+        return acc;
+    }
+    /* torch_features_dynamical.py:87-127 (r unused, as in the reference) */
+    case ORACLE_F_FRIEDRICH: {
+        const int m = (int)param, coeff = (int)param2;
+        double c[7];
+        if (m < 0 || m > 6 || poly_velocity_fit(w, n, m, c) != 0) return 0.0;
+        return coeff <= m ? c[coeff] : 0.0;
+    }
+    /* torch_features_dynamical.py:131-174: the fitted velocity at each position in
+       time order; the largest position p_i (i < n-2) where the fit changes sign
+       strictly between i and i+1, 0 if none */
+    case ORACLE_F_LANGEVIN: {
+        const int m = (int)param;
+        double c[7];
+        if (m < 0 || m > 6 || poly_velocity_fit(w, n, m, c) != 0) return 0.0;
+        double best = -INFINITY, prev = 0.0;
+        for (int i = 0; i + 1 < n; ++i) {
+            double f = 0.0;
+            for (int q = 0; q <= m; ++q) f = f * w[i] + c[q];
+            if (i > 0 && prev * f < 0.0 && w[i - 1] > best) best = w[i - 1];
+            prev = f;
+        }
+        return best == -INFINITY ? 0.0 : best;
     }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;

@@ -67,6 +67,9 @@ enum {
        pvalue, stderr; f_agg mean / var / min / max), ar_coefficient (k <= 10, coeff) */
     ORACLE_F_AGG_TREND_MEAN = 87, ORACLE_F_AGG_TREND_VAR = 88, ORACLE_F_AGG_TREND_MIN = 89,
     ORACLE_F_AGG_TREND_MAX = 90, ORACLE_F_AR_COEFFICIENT = 91,
+    /* cwt_coefficients (w, coeff; coeff < 0: w not among the widths -> 0),
+       friedrich_coefficients (m <= 6, coeff), max_langevin_fixed_point (m <= 6) */
+    ORACLE_F_CWT = 92, ORACLE_F_FRIEDRICH = 93, ORACLE_F_LANGEVIN = 94,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

@@ -886,6 +886,112 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 __syncwarp();
                 break;
             }
+            case PB_FEAT_CWT: {
+                // Ricker wavelet of width w correlated with the window padded by 4w
+                // samples (reflected without the edge, or replicated when nwin < 4w), at
+                // output index coeff; the prefactor rounded in FP32 as the reference forms it
+                const int wd = static_cast<int>(param), coeff = static_cast<int>(plan.param2[m]);
+                if (coeff < 0 || coeff >= nwin) {
+                    result = 0.0;
+                    break;
+                }
+                const float pref32 = __fdiv_rn(2.0f, __fmul_rn(__fsqrt_rn(static_cast<float>(3.0 * wd)),
+                                                               static_cast<float>(1.3313353638003897)));
+                const double pref = static_cast<double>(pref32), sig = static_cast<double>(wd);
+                const int pad = 4 * wd;
+                for (int j = lane; j <= 8 * wd; j += 32) {
+                    const double t = static_cast<double>(j - pad);
+                    const double psi = pref * (1.0 - (t / sig) * (t / sig)) * exp(-(t * t) / (2.0 * sig * sig));
+                    int64_t q = static_cast<int64_t>(coeff) + j - pad;
+                    if (nwin >= pad) {
+                        if (q < 0) q = -q;
+                        if (q >= nwin) q = 2ll * (nwin - 1) - q;
+                    } else {
+                        q = q < 0 ? 0 : (q >= nwin ? nwin - 1 : q);
+                    }
+                    a0 += static_cast<double>(x[q]) * psi;
+                }
+                result = warp_sum_d(a0);
+                break;
+            }
+            case PB_FEAT_FRIEDRICH:
+            case PB_FEAT_LANGEVIN: {
+                // velocity v_i = x_(i+1) - x_i fitted by a degree-m polynomial of the
+                // position x_i: the regularised normal equations (V'V + 1e-6 I) c = V'v from
+                // warp sums of powers, solved on lane 0 (in this warp's shared doubles)
+                const int deg = static_cast<int>(param);
+                if (nwin < 2) {
+                    result = 0.0;
+                    break;
+                }
+                double S[13], T[7];
+#pragma unroll
+                for (int q = 0; q < 13; ++q) S[q] = 0.0;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) T[q] = 0.0;
+                for (int i = lane; i + 1 < nwin; i += 32) {
+                    const double p = static_cast<double>(x[i]), v = static_cast<double>(x[i + 1]) - p;
+                    double pw = 1.0;
+#pragma unroll
+                    for (int q = 0; q < 13; ++q) {
+                        if (q <= 2 * deg) S[q] += pw;
+                        if (q <= deg) T[q] += pw * v;
+                        pw *= p;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 13; ++q) S[q] = warp_sum_d(S[q]);
+#pragma unroll
+                for (int q = 0; q < 7; ++q) T[q] = warp_sum_d(T[q]);
+                double* A = reinterpret_cast<double*>(h);  // (deg + 1) rows of stride 8; column deg + 1: rhs, then c
+                const int k = deg + 1;
+                if (lane == 0) {
+                    for (int r = 0; r < k; ++r) {
+                        for (int c = 0; c < k; ++c) A[r * 8 + c] = S[2 * deg - r - c] + (r == c ? 1e-6 : 0.0);
+                        A[r * 8 + k] = T[deg - r];
+                    }
+                    for (int col = 0; col < k; ++col) {
+                        int piv = col;
+                        for (int i = col + 1; i < k; ++i)
+                            if (fabs(A[i * 8 + col]) > fabs(A[piv * 8 + col])) piv = i;
+                        if (piv != col)
+                            for (int j = 0; j <= k; ++j) {
+                                const double t = A[col * 8 + j];
+                                A[col * 8 + j] = A[piv * 8 + j];
+                                A[piv * 8 + j] = t;
+                            }
+                        for (int i = col + 1; i < k; ++i) {
+                            const double f = A[i * 8 + col] / A[col * 8 + col];
+                            for (int j = col; j <= k; ++j) A[i * 8 + j] -= f * A[col * 8 + j];
+                        }
+                    }
+                    for (int i = k - 1; i >= 0; --i) {
+                        double t = A[i * 8 + k];
+                        for (int j = i + 1; j < k; ++j) t -= A[i * 8 + j] * A[j * 8 + k];
+                        A[i * 8 + k] = t / A[i * 8 + i];
+                    }
+                }
+                __syncwarp();
+                if (kind == PB_FEAT_FRIEDRICH) {
+                    const int coeff = static_cast<int>(plan.param2[m]);
+                    result = coeff <= deg ? A[coeff * 8 + k] : 0.0;
+                } else {  // the largest position x_i (i < n-2) where the fit changes sign to i+1
+                    double best = -CUDART_INF;
+                    for (int i = lane; i + 2 < nwin; i += 32) {
+                        const double p0 = static_cast<double>(x[i]), p1 = static_cast<double>(x[i + 1]);
+                        double f0 = 0.0, f1 = 0.0;
+                        for (int q = 0; q <= deg; ++q) {
+                            f0 = f0 * p0 + A[q * 8 + k];
+                            f1 = f1 * p1 + A[q * 8 + k];
+                        }
+                        if (f0 * f1 < 0.0) best = fmax(best, p0);
+                    }
+                    for (int off = 16; off > 0; off >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, off));
+                    result = best == -CUDART_INF ? 0.0 : best;
+                }
+                __syncwarp();
+                break;
+            }
             case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
                 const float v = static_cast<float>(param);
                 for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
@@ -1564,6 +1670,9 @@ int validate_args(const pb_solve_args* a, bool user_system)
             !(is_int(prm, 1.0, 1e9) && is_int(prm2, 0.0, 4.0)))
             return PB_EINVAL;
         if (kind == PB_FEAT_AR_COEFFICIENT && !(is_int(prm, 1.0, 10.0) && is_int(prm2, 0.0, 1e6))) return PB_EINVAL;
+        if (kind == PB_FEAT_CWT && !(is_int(prm, 1.0, 1e4) && is_int(prm2, -1.0, 1e9))) return PB_EINVAL;
+        if ((kind == PB_FEAT_FRIEDRICH || kind == PB_FEAT_LANGEVIN) && !(is_int(prm, 0.0, 6.0) && is_int(prm2, 0.0, 1e6)))
+            return PB_EINVAL;
         if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))
             return PB_EINVAL;
         if (kind >= PB_FEAT_AGG_AUTOCORR_MEAN && kind <= PB_FEAT_AGG_AUTOCORR_VAR && !is_int(prm, 0.0, 128.0))

@@ -97,6 +97,9 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "permutation_entropy": [{"tau": 1, "dimension": 3}],
     "agg_linear_trend": [{"attr": "slope", "chunk_size": 10, "f_agg": "mean"}],
     "ar_coefficient": [{"coeff": 0, "k": 1}],
+    "cwt_coefficients": [{"widths": (2,), "coeff": 0, "w": 2}],
+    "friedrich_coefficients": [{"coeff": 0, "m": 3, "r": 30}],
+    "max_langevin_fixed_point": [{"m": 3, "r": 30}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -141,6 +144,17 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
                              float(_TREND_ATTRS.index(attr)))
     if fname == "ar_coefficient":  # torch_features_trend.py:86-131
         return FeatureColumn(state, L.FEAT_AR_COEFFICIENT, float(p.get("k", 1)), name, float(p.get("coeff", 0)))
+    if fname == "cwt_coefficients":  # torch_features_frequency.py:71-127
+        w = int(p.get("w", 2))
+        widths = tuple(int(v) for v in p.get("widths", (2,)))
+        return FeatureColumn(state, L.FEAT_CWT, float(w), name, float(p.get("coeff", 0)) if w in widths else -1.0)
+    if fname in ("friedrich_coefficients", "max_langevin_fixed_point"):  # torch_features_dynamical.py:87-174
+        m_deg = int(p.get("m", 3))
+        if not 0 <= m_deg <= 6:
+            raise ValueError(f"{fname}: the fused fit takes polynomial degrees m <= 6, got {m_deg}")
+        if fname == "friedrich_coefficients":
+            return FeatureColumn(state, L.FEAT_FRIEDRICH, float(m_deg), name, float(p.get("coeff", 0)))
+        return FeatureColumn(state, L.FEAT_LANGEVIN, float(m_deg), name)
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140

@@ -82,6 +82,7 @@ def _features(ref: Path) -> None:
     from pybasin.ts_torch.calculators import torch_features_statistical as st
     from pybasin.ts_torch.calculators import torch_features_advanced as ad
     from pybasin.ts_torch.calculators import torch_features_boolean as bo
+    from pybasin.ts_torch.calculators import torch_features_dynamical as dy
     from pybasin.ts_torch.calculators import torch_features_entropy_complexity as ec
     from pybasin.ts_torch.calculators import torch_features_frequency as fq
     from pybasin.ts_torch.calculators import torch_features_location as lo
@@ -226,6 +227,13 @@ def _features(ref: Path) -> None:
            ("mean", "var", "min", "max")},
         **{f"{src}_linear_trend_timewise_{a}": tr.linear_trend_timewise(v, a).numpy()
            for src, v in (("x", x),) for a in ("slope", "rvalue")},
+        **{f"{src}_cwt_coefficients_{w}_{c}": fq.cwt_coefficients(v, (w,), c, w).numpy()
+           for src, v in (("x", x), ("periodic", per)) for w in (2, 5, 10, 20) for c in (0, 3, 14, 128, 256)},
+        "x_cwt_coefficients_missing_width": fq.cwt_coefficients(x, (5,), 3, 2).numpy(),
+        **{f"{src}_friedrich_coefficients_{m}_{c}": dy.friedrich_coefficients(v, m, 30.0, c).numpy()
+           for src, v in (("x", x), ("periodic", per)) for m in (1, 3) for c in range(m + 2)},
+        **{f"{src}_max_langevin_fixed_point_{m}": dy.max_langevin_fixed_point(v, m=m, r=30.0).numpy()
+           for src, v in (("x", x), ("periodic", per)) for m in (1, 3)},
         **{f"{src}_ar_coefficient_{k}_{c}": tr.ar_coefficient(v, k, c).numpy()
            for src, v in (("x", x), ("periodic", per)) for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0),
                                                                        (4, 2))},

@@ -241,6 +241,13 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
           for ai, a in enumerate(("slope", "intercept", "rvalue", "pvalue", "stderr")) for c in (5, 50, 200)
           for fi, f in enumerate(("mean", "var", "min", "max"))],
         *[(f"x_linear_trend_timewise_{a}", "x", 36 + i, 0.0, 0.0) for i, a in ((0, "slope"), (2, "rvalue"))],
+        *[(f"{tag}_cwt_coefficients_{w}_{c}", src, 92, float(w), float(c))
+          for tag, src in (("x", "x"), ("periodic", "x_periodic")) for w in (2, 5, 10, 20) for c in (0, 3, 14, 128, 256)],
+        ("x_cwt_coefficients_missing_width", "x", 92, 2.0, -1.0),
+        *[(f"{tag}_friedrich_coefficients_{m}_{c}", src, 93, float(m), float(c))
+          for tag, src in (("x", "x"), ("periodic", "x_periodic")) for m in (1, 3) for c in range(m + 2)],
+        *[(f"{tag}_max_langevin_fixed_point_{m}", src, 94, float(m), 0.0)
+          for tag, src in (("x", "x"), ("periodic", "x_periodic")) for m in (1, 3)],
         *[(f"{tag}_ar_coefficient_{k}_{c}", src, 91, float(k), float(c))
           for tag, src in (("x", "x"), ("periodic", "x_periodic"))
           for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0), (4, 2))],
@@ -251,7 +258,9 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
     sine waves of 16 periods, one constant column), spectral frequency ratio and
     aggregated spectrum moments (odd and even lengths), Fourier and permutation
     entropy, Lempel-Ziv complexity (exact phrase counts), trends of chunk
-    aggregates, AR coefficients (Yule-Walker), energy ratio of a chunk,
+    aggregates, AR coefficients (Yule-Walker), Ricker-wavelet coefficients (the
+    reference's FP32 prefactor), Friedrich coefficients and the Langevin fixed
+    point, energy ratio of a chunk,
     count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the
@@ -264,7 +273,7 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
                     for b in range(x.shape[1])])
     if 67 <= kind <= 70 or kind == 77:
         np.testing.assert_allclose(got, want, rtol=0.0, atol=1e-10)
-    elif kind == 91:  # Yule-Walker solved by torch's LU against the oracle's elimination
+    elif kind in (91, 93):  # linear systems solved by torch's LU against the oracle's elimination
         np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12)
     elif 80 <= kind <= 84:  # torch's FFT against the oracle's direct sums
         np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12)

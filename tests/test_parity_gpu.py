@@ -598,19 +598,24 @@ ACF_PAIR_FEATS = [(0, L.FEAT_PARTIAL_AUTOCORRELATION, 1.0), (0, L.FEAT_PARTIAL_A
                   (1, L.FEAT_CHANGE_QUANTILES_VAR, 0.0, 0.4), (0, L.FEAT_CHANGE_QUANTILES_ABS_MEAN, 0.4, 1.0),
                   (1, L.FEAT_CHANGE_QUANTILES_ABS_VAR, 0.2, 0.8), (0, L.FEAT_CHANGE_QUANTILES_VAR, 0.5, 0.5),
                   (0, L.FEAT_ACF_PERIOD_STRENGTH, 2.0, 0.3), (0, L.FEAT_ACF_PERIOD_LAG, 2.0, 0.3),
-                  (1, L.FEAT_ACF_PERIOD_LAG, 50.0, 0.5), (1, L.FEAT_ACF_PERIOD_STRENGTH, 2.0, 0.99),
-                  (0, L.FEAT_AGG_TREND_MEAN, 50.0, 0.0), (1, L.FEAT_AGG_TREND_VAR, 5.0, 2.0),
+                  (1, L.FEAT_ACF_PERIOD_LAG, 50.0, 0.5), (1, L.FEAT_ACF_PERIOD_STRENGTH, 2.0, 0.99)]
+# second group (a solve takes at most 32 columns)
+DYN_FEATS = [(0, L.FEAT_AGG_TREND_MEAN, 50.0, 0.0), (1, L.FEAT_AGG_TREND_VAR, 5.0, 2.0),
                   (0, L.FEAT_AGG_TREND_MIN, 20.0, 4.0), (1, L.FEAT_AGG_TREND_MAX, 200.0, 3.0),
                   (0, L.FEAT_AGG_TREND_MEAN, 400.0, 1.0), (0, L.FEAT_AR_COEFFICIENT, 10.0, 0.0),
                   (1, L.FEAT_AR_COEFFICIENT, 10.0, 9.0), (0, L.FEAT_AR_COEFFICIENT, 4.0, 2.0),
-                  (1, L.FEAT_AR_COEFFICIENT, 3.0, 3.0)]
+                  (1, L.FEAT_AR_COEFFICIENT, 3.0, 3.0), (0, L.FEAT_CWT, 5.0, 100.0), (1, L.FEAT_CWT, 20.0, 0.0),
+                  (0, L.FEAT_CWT, 2.0, 3.0), (1, L.FEAT_CWT, 10.0, -1.0), (0, L.FEAT_CWT, 200.0, 700.0),
+                  (0, L.FEAT_FRIEDRICH, 3.0, 0.0), (1, L.FEAT_FRIEDRICH, 3.0, 3.0), (0, L.FEAT_FRIEDRICH, 1.0, 1.0),
+                  (0, L.FEAT_LANGEVIN, 3.0, 0.0), (1, L.FEAT_LANGEVIN, 1.0, 0.0)]
 
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
 def test_acf_and_two_parameter_features_on_identical_windows(precision):
     """Partial and aggregated autocorrelation, autocorrelation periodicity, chunk
-    energy ratio, count in range, change quantiles, trends of chunk aggregates
-    and AR coefficients from the window pass against the oracle evaluated on the
+    energy ratio, count in range, change quantiles, trends of chunk aggregates,
+    AR, Ricker-wavelet and Friedrich coefficients and the Langevin fixed point
+    from the window pass against the oracle evaluated on the
     kernel's own FP32 window (y_full holds the samples the window stores).  Counts
     and periods are exact; the rest differ by summation order only: the
     autocorrelations (at most 1 in size) to 1e-10 absolute, the others to 1e-9
@@ -619,25 +624,34 @@ def test_acf_and_two_parameter_features_on_identical_windows(precision):
     y0 = seeded_ics(DUFFING, 96, seed=21).double().numpy()
     save = np.linspace(0.0, 40.0, 2001)
     wb = int(np.nonzero(save >= 25.0)[0][0])
-    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 40.0), 1e-8, 1e-10,
-                    precision=precision, win_begin=wb, features=ACF_PAIR_FEATS, keep_full=True)
+    for feats in (ACF_PAIR_FEATS, DYN_FEATS):
+        g = _check_identical_windows(y0, save, wb, precision, feats)
+        if feats is ACF_PAIR_FEATS:
+            assert (g[:, 3] == 1.0).all()  # lag 0
+            assert np.ptp(g[:, 11]) > 0 and (g[:, 13] != 0).any()  # non-trivial counts and corridors
+            assert (g[:, 19] > 0).mean() > 0.5  # most windows of the forced oscillation show a period
+
+
+def _check_identical_windows(y0, save, wb, precision, feats):
+    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, float(save[-1])), 1e-8, 1e-10,
+                    precision=precision, win_begin=wb, features=feats, keep_full=True)
     assert (got["status"] == 0).all()
     win = got["y"][wb:].astype(np.float32).astype(np.float64)  # (n_win, n, 2)
     want = np.array([[O.window_feature(f[1], f[2], win[:, j, f[0]], f[3] if len(f) > 3 else 0.0)
-                      for f in ACF_PAIR_FEATS] for j in range(len(y0))])
+                      for f in feats] for j in range(len(y0))])
     g = got["features"]
-    for c, f in enumerate(ACF_PAIR_FEATS):
+    for c, f in enumerate(feats):
         if L.FEAT_PARTIAL_AUTOCORRELATION <= f[1] <= L.FEAT_AGG_AUTOCORR_VAR or f[1] == L.FEAT_ACF_PERIOD_STRENGTH:
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=0.0, atol=1e-10, err_msg=f"col {c} {f}")
-        elif f[1] == L.FEAT_AR_COEFFICIENT:  # Yule-Walker on near-1 autocorrelations: ill-conditioned
+        elif f[1] == L.FEAT_LANGEVIN:  # a window value chosen by the sign of a fit: equal or a near-zero flip
+            assert (g[:, c] == want[:, c]).mean() >= 0.95, (c, f)
+        elif f[1] in (L.FEAT_AR_COEFFICIENT, L.FEAT_FRIEDRICH):  # normal equations: ill-conditioned
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-6, atol=1e-9, err_msg=f"col {c} {f}")
         elif f[1] in (L.FEAT_COUNT_IN_RANGE, L.FEAT_ACF_PERIOD_LAG):
             np.testing.assert_array_equal(g[:, c], want[:, c], err_msg=f"col {c} {f}")
         else:
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-15, err_msg=f"col {c} {f}")
-    assert (g[:, 3] == 1.0).all()  # lag 0
-    assert np.ptp(g[:, 11]) > 0 and (g[:, 13] != 0).any()  # non-trivial counts and corridors
-    assert (g[:, 19] > 0).mean() > 0.5  # most windows of the forced oscillation show a period
+    return g
 
 
 def test_two_parameter_features_through_the_extractor_names():
@@ -653,17 +667,19 @@ def test_two_parameter_features_through_the_extractor_names():
            "autocorrelation_periodicity": [{"output": "strength"}, {"output": "period"}],
            "spectral_frequency_ratio": None, "fft_aggregated": [{"aggtype": "kurtosis"}],
            "agg_linear_trend": [{"attr": "rvalue", "chunk_size": 50, "f_agg": "max"}],
-           "ar_coefficient": [{"coeff": 1, "k": 10}], "linear_trend_timewise": [{"attr": "slope"}]}
+           "ar_coefficient": [{"coeff": 1, "k": 10}], "linear_trend_timewise": [{"attr": "slope"}],
+           "cwt_coefficients": [{"widths": (5,), "coeff": 3, "w": 5}], "friedrich_coefficients": None,
+           "max_langevin_fixed_point": None}
     fx = FusedFeatureExtractor(time_steady=900.0, features=None, features_per_state={0: cfg}, normalize=False)
     solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=2000, t_eval=(900, 1000), device="cuda:0",
                               precision="fp64", feature_extractor=fx)
     y0 = seeded_ics(DUFFING, 32, seed=3).double()
     t, y = solver.integrate(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0)
     f = fx.extract_features(type("S", (), {"y": y})())
-    assert f.shape == (32, 23) and torch.isfinite(f).all()
+    assert f.shape == (32, 26) and torch.isfinite(f).all()
     assert fx.feature_names[0] == "state_0__agg_autocorrelation__f_agg_mean__maxlag_40"
     assert fx.feature_names[19] == "state_0__fft_aggregated__aggtype_kurtosis"
-    assert fx.feature_names[-1] == "state_0__linear_trend_timewise__attr_slope"
+    assert fx.feature_names[22] == "state_0__linear_trend_timewise__attr_slope"
     # the ten chunk energy ratios partition the window's energy (200 samples per chunk)
     np.testing.assert_allclose(f[:, 6:16].sum(dim=1).cpu().numpy(), 1.0, rtol=1e-9)
 
