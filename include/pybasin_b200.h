@@ -170,10 +170,14 @@ typedef enum {
        Ricker wavelet, torch_features_frequency.py:71-127), friedrich_coefficients
        (m <= 6, feat_param2 = coeff) and max_langevin_fixed_point (m <= 6)
        (torch_features_dynamical.py:87-174) */
-    PB_FEAT_CWT = 92, PB_FEAT_FRIEDRICH = 93, PB_FEAT_LANGEVIN = 94
+    PB_FEAT_CWT = 92, PB_FEAT_FRIEDRICH = 93, PB_FEAT_LANGEVIN = 94,
+    /* augmented_dickey_fuller with attr teststat / pvalue / usedlag in the kind
+       (torch_features_trend.py:134-169), number_cwt_peaks (max_width <= 64;
+       torch_features_pattern.py:154-188) */
+    PB_FEAT_ADF_TESTSTAT = 95, PB_FEAT_ADF_PVALUE = 96, PB_FEAT_ADF_USEDLAG = 97, PB_FEAT_NUMBER_CWT_PEAKS = 98
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_LANGEVIN
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..94): the
+#define PB_FEAT_LAST_KIND PB_FEAT_NUMBER_CWT_PEAKS
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..98): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window

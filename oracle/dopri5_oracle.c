@@ -945,6 +945,58 @@ static double window_feature(int feat, double param, double param2, const double
         }
         return best == -INFINITY ? 0.0 : best;
     }
+    /* torch_features_trend.py:134-169: least squares of the first difference
+       d_i = w[i+1] - w[i] on the lagged value w[i] (i < n-1), t = beta / (se + 1e-10)
+       with se = sqrt(rss / (n - 3)) / (sqrt(ss_xx) + 1e-10); pvalue = 1 / (1 + |t|);
+       usedlag is 1 */
+    case ORACLE_F_ADF_TESTSTAT: case ORACLE_F_ADF_PVALUE: case ORACLE_F_ADF_USEDLAG: {
+        if (feat == ORACLE_F_ADF_USEDLAG) return 1.0;
+        const int nm = n - 1;
+        double xm = 0.0, ym = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            xm += w[i];
+            ym += w[i + 1] - w[i];
+        }
+        xm /= nm;
+        ym /= nm;
+        double sxx = 0.0, sxy = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            sxx += (w[i] - xm) * (w[i] - xm);
+            sxy += (w[i] - xm) * ((w[i + 1] - w[i]) - ym);
+        }
+        const double beta = sxy / (sxx + 1e-10);
+        double rss = 0.0;
+        for (int i = 0; i < nm; ++i) {
+            const double e = (w[i + 1] - w[i]) - (ym + beta * (w[i] - xm));
+            rss += e * e;
+        }
+        const double se = sqrt(rss / (n - 3.0)) / (sqrt(sxx) + 1e-10);
+        const double t = beta / (se + 1e-10);
+        return feat == ORACLE_F_ADF_TESTSTAT ? t : 1.0 / (1.0 + fabs(t));
+    }
+    /* torch_features_pattern.py:154-188: for each width 1..max_width with 2 width < n,
+       the samples i in [width, n - width) equal to the maximum of w[i-width..i+width]
+       (a NaN in that neighbourhood rules the sample out: max pooling propagates
+       NaN); the count averaged over those widths (0 if none) */
+    case ORACLE_F_NUMBER_CWT_PEAKS: {
+        const int mw = (int)param;
+        double tot = 0.0;
+        int nw = 0;
+        for (int wd = 1; wd <= mw; ++wd) {
+            if (!(2 * wd < n)) continue;
+            ++nw;
+            for (int i = wd; i < n - wd; ++i) {
+                double mxl = w[i - wd];
+                int nan_in = isnan(mxl) != 0;
+                for (int j = i - wd + 1; j <= i + wd; ++j) {
+                    nan_in |= isnan(w[j]) != 0;
+                    if (w[j] > mxl) mxl = w[j];
+                }
+                tot += !nan_in && w[i] == mxl;
+            }
+        }
+        return nw > 0 ? tot / nw : 0.0;
+    }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
     /* torch_features_count.py:42-45 */

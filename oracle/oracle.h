@@ -70,6 +70,8 @@ enum {
     /* cwt_coefficients (w, coeff; coeff < 0: w not among the widths -> 0),
        friedrich_coefficients (m <= 6, coeff), max_langevin_fixed_point (m <= 6) */
     ORACLE_F_CWT = 92, ORACLE_F_FRIEDRICH = 93, ORACLE_F_LANGEVIN = 94,
+    /* augmented_dickey_fuller (teststat, pvalue, usedlag), number_cwt_peaks (max_width) */
+    ORACLE_F_ADF_TESTSTAT = 95, ORACLE_F_ADF_PVALUE = 96, ORACLE_F_ADF_USEDLAG = 97, ORACLE_F_NUMBER_CWT_PEAKS = 98,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

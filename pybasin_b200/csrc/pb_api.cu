@@ -992,6 +992,62 @@ __global__ void __launch_bounds__(256) k_window(const float* __restrict__ win, i
                 __syncwarp();
                 break;
             }
+            case PB_FEAT_ADF_TESTSTAT:
+            case PB_FEAT_ADF_PVALUE:
+            case PB_FEAT_ADF_USEDLAG: {  // first difference regressed on the lagged value (usedlag: 1)
+                if (kind == PB_FEAT_ADF_USEDLAG) {
+                    result = 1.0;
+                    break;
+                }
+                const int nm = nwin - 1;
+                for (int i = lane; i < nm; i += 32) {
+                    const double p = static_cast<double>(x[i]);
+                    a0 += p;
+                    a1 += static_cast<double>(x[i + 1]) - p;
+                }
+                const double xm = warp_sum_d(a0) / nm, ym = warp_sum_d(a1) / nm;
+                a0 = 0.0;
+                a1 = 0.0;
+                for (int i = lane; i < nm; i += 32) {
+                    const double p = static_cast<double>(x[i]), d = static_cast<double>(x[i + 1]) - p;
+                    a0 += (p - xm) * (p - xm);
+                    a1 += (p - xm) * (d - ym);
+                }
+                const double sxx = warp_sum_d(a0), sxy = warp_sum_d(a1);
+                const double beta = sxy / (sxx + 1e-10);
+                for (int i = lane; i < nm; i += 32) {
+                    const double p = static_cast<double>(x[i]), d = static_cast<double>(x[i + 1]) - p;
+                    const double e = d - (ym + beta * (p - xm));
+                    a2 += e * e;
+                }
+                const double se = sqrt(warp_sum_d(a2) / (n - 3.0)) / (sqrt(sxx) + 1e-10);
+                const double t = beta / (se + 1e-10);
+                result = kind == PB_FEAT_ADF_TESTSTAT ? t : 1.0 / (1.0 + fabs(t));
+                break;
+            }
+            case PB_FEAT_NUMBER_CWT_PEAKS: {
+                // samples equal to the maximum of their +-width neighbourhood (a NaN in it
+                // rules the sample out, as max pooling propagates NaN), for each width
+                // 1..max_width with 2 width < n, averaged over those widths
+                const int mw = static_cast<int>(param);
+                int nw = 0;
+                for (int wd = 1; wd <= mw; ++wd) {
+                    if (!(2 * wd < nwin)) continue;
+                    ++nw;
+                    for (int i = wd + lane; i < nwin - wd; i += 32) {
+                        const float xi = x[i];
+                        bool nan_in = false, peak = true;
+                        for (int j = i - wd; j <= i + wd; ++j) {
+                            const float v = x[j];
+                            nan_in |= isnan(v);
+                            peak &= !(v > xi);
+                        }
+                        a0 += (peak && !nan_in) ? 1.0 : 0.0;
+                    }
+                }
+                result = nw > 0 ? warp_sum_d(a0) / nw : 0.0;
+                break;
+            }
             case PB_FEAT_COUNT_VALUE: {  // samples equal to the value, compared in the window's FP32
                 const float v = static_cast<float>(param);
                 for (int i = lane; i < nwin; i += 32) a0 += x[i] == v ? 1.0 : 0.0;
@@ -1671,6 +1727,7 @@ int validate_args(const pb_solve_args* a, bool user_system)
             return PB_EINVAL;
         if (kind == PB_FEAT_AR_COEFFICIENT && !(is_int(prm, 1.0, 10.0) && is_int(prm2, 0.0, 1e6))) return PB_EINVAL;
         if (kind == PB_FEAT_CWT && !(is_int(prm, 1.0, 1e4) && is_int(prm2, -1.0, 1e9))) return PB_EINVAL;
+        if (kind == PB_FEAT_NUMBER_CWT_PEAKS && !is_int(prm, 0.0, 64.0)) return PB_EINVAL;
         if ((kind == PB_FEAT_FRIEDRICH || kind == PB_FEAT_LANGEVIN) && !(is_int(prm, 0.0, 6.0) && is_int(prm2, 0.0, 1e6)))
             return PB_EINVAL;
         if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))

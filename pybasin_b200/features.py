@@ -82,6 +82,7 @@ FEATURE_KINDS: dict[str, int] = {
     "spectral_frequency_ratio": L.FEAT_SPECTRAL_FREQ_RATIO,
     "fourier_entropy": L.FEAT_FOURIER_ENTROPY,
     "lempel_ziv_complexity": L.FEAT_LEMPEL_ZIV,
+    "number_cwt_peaks": L.FEAT_NUMBER_CWT_PEAKS,
 }
 
 #: Features with several parameters (FCParameters keys as in the reference's
@@ -171,6 +172,8 @@ FEATURE_ATTR: dict[str, tuple[dict[str, int], str, str | None, float]] = {
     "linear_trend": ({"slope": L.FEAT_TREND_SLOPE, "intercept": L.FEAT_TREND_INTERCEPT,
                       "rvalue": L.FEAT_TREND_RVALUE, "pvalue": L.FEAT_TREND_PVALUE,
                       "stderr": L.FEAT_TREND_STDERR}, "slope", None, 0.0),
+    "augmented_dickey_fuller": ({"teststat": L.FEAT_ADF_TESTSTAT, "pvalue": L.FEAT_ADF_PVALUE,
+                                 "usedlag": L.FEAT_ADF_USEDLAG}, "teststat", None, 0.0),
     # the reference's linear_trend_timewise is linear_trend (torch_features_trend.py:54-56)
     "linear_trend_timewise": ({"slope": L.FEAT_TREND_SLOPE, "intercept": L.FEAT_TREND_INTERCEPT,
                                "rvalue": L.FEAT_TREND_RVALUE, "pvalue": L.FEAT_TREND_PVALUE,
@@ -200,6 +203,7 @@ FEATURE_PARAM: dict[int, tuple[str, float]] = {
     L.FEAT_PARTIAL_AUTOCORRELATION: ("lag", 1.0),
     L.FEAT_FOURIER_ENTROPY: ("bins", 10.0),
     L.FEAT_LEMPEL_ZIV: ("bins", 2.0),
+    L.FEAT_NUMBER_CWT_PEAKS: ("max_width", 5.0),
 }
 
 #: The reference's minimal set (src/pybasin/ts_torch/settings.py:376-395).

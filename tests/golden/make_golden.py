@@ -234,6 +234,10 @@ def _features(ref: Path) -> None:
            for src, v in (("x", x), ("periodic", per)) for m in (1, 3) for c in range(m + 2)},
         **{f"{src}_max_langevin_fixed_point_{m}": dy.max_langevin_fixed_point(v, m=m, r=30.0).numpy()
            for src, v in (("x", x), ("periodic", per)) for m in (1, 3)},
+        **{f"{src}_augmented_dickey_fuller_{a}": tr.augmented_dickey_fuller(v, a).numpy()
+           for src, v in (("x", x), ("periodic", per)) for a in ("teststat", "pvalue", "usedlag")},
+        **{f"{src}_number_cwt_peaks_{w}": pat.number_cwt_peaks(v, w).numpy()
+           for src, v in (("x", x), ("periodic", per), ("rep", rep)) for w in (1, 5, 200)},
         **{f"{src}_ar_coefficient_{k}_{c}": tr.ar_coefficient(v, k, c).numpy()
            for src, v in (("x", x), ("periodic", per)) for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0),
                                                                        (4, 2))},

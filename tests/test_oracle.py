@@ -248,6 +248,10 @@ _CQ_KIND = {(False, "mean"): 73, (False, "var"): 74, (True, "mean"): 75, (True, 
           for tag, src in (("x", "x"), ("periodic", "x_periodic")) for m in (1, 3) for c in range(m + 2)],
         *[(f"{tag}_max_langevin_fixed_point_{m}", src, 94, float(m), 0.0)
           for tag, src in (("x", "x"), ("periodic", "x_periodic")) for m in (1, 3)],
+        *[(f"{tag}_augmented_dickey_fuller_{a}", src, 95 + i, 0.0, 0.0)
+          for tag, src in (("x", "x"), ("periodic", "x_periodic")) for i, a in enumerate(("teststat", "pvalue", "usedlag"))],
+        *[(f"{tag}_number_cwt_peaks_{w}", src, 98, float(w), 0.0)
+          for tag, src in (("x", "x"), ("periodic", "x_periodic"), ("rep", "x_rep")) for w in (1, 5, 200)],
         *[(f"{tag}_ar_coefficient_{k}_{c}", src, 91, float(k), float(c))
           for tag, src in (("x", "x"), ("periodic", "x_periodic"))
           for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0), (4, 2))],
@@ -260,7 +264,8 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
     entropy, Lempel-Ziv complexity (exact phrase counts), trends of chunk
     aggregates, AR coefficients (Yule-Walker), Ricker-wavelet coefficients (the
     reference's FP32 prefactor), Friedrich coefficients and the Langevin fixed
-    point, energy ratio of a chunk,
+    point, augmented Dickey-Fuller, CWT-peak counts (ties and a NaN on the 0.5
+    grid), energy ratio of a chunk,
     count in a range and change quantiles.  The reference's autocorrelations come from a
     zero-padded FFT (another summation order than the oracle's direct lag sums):
     1e-10 absolute on values bounded by 1; count_in_range counts in FP32; the

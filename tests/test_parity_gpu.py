@@ -607,15 +607,18 @@ DYN_FEATS = [(0, L.FEAT_AGG_TREND_MEAN, 50.0, 0.0), (1, L.FEAT_AGG_TREND_VAR, 5.
                   (1, L.FEAT_AR_COEFFICIENT, 3.0, 3.0), (0, L.FEAT_CWT, 5.0, 100.0), (1, L.FEAT_CWT, 20.0, 0.0),
                   (0, L.FEAT_CWT, 2.0, 3.0), (1, L.FEAT_CWT, 10.0, -1.0), (0, L.FEAT_CWT, 200.0, 700.0),
                   (0, L.FEAT_FRIEDRICH, 3.0, 0.0), (1, L.FEAT_FRIEDRICH, 3.0, 3.0), (0, L.FEAT_FRIEDRICH, 1.0, 1.0),
-                  (0, L.FEAT_LANGEVIN, 3.0, 0.0), (1, L.FEAT_LANGEVIN, 1.0, 0.0)]
+                  (0, L.FEAT_LANGEVIN, 3.0, 0.0), (1, L.FEAT_LANGEVIN, 1.0, 0.0),
+                  (0, L.FEAT_ADF_TESTSTAT, 0.0, 0.0), (1, L.FEAT_ADF_PVALUE, 0.0, 0.0),
+                  (0, L.FEAT_ADF_USEDLAG, 0.0, 0.0), (0, L.FEAT_NUMBER_CWT_PEAKS, 1.0, 0.0),
+                  (1, L.FEAT_NUMBER_CWT_PEAKS, 5.0, 0.0), (0, L.FEAT_NUMBER_CWT_PEAKS, 64.0, 0.0)]
 
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
 def test_acf_and_two_parameter_features_on_identical_windows(precision):
     """Partial and aggregated autocorrelation, autocorrelation periodicity, chunk
     energy ratio, count in range, change quantiles, trends of chunk aggregates,
-    AR, Ricker-wavelet and Friedrich coefficients and the Langevin fixed point
-    from the window pass against the oracle evaluated on the
+    AR, Ricker-wavelet and Friedrich coefficients, the Langevin fixed point,
+    augmented Dickey-Fuller and CWT-peak counts from the window pass against the oracle evaluated on the
     kernel's own FP32 window (y_full holds the samples the window stores).  Counts
     and periods are exact; the rest differ by summation order only: the
     autocorrelations (at most 1 in size) to 1e-10 absolute, the others to 1e-9
@@ -647,7 +650,7 @@ def _check_identical_windows(y0, save, wb, precision, feats):
             assert (g[:, c] == want[:, c]).mean() >= 0.95, (c, f)
         elif f[1] in (L.FEAT_AR_COEFFICIENT, L.FEAT_FRIEDRICH):  # normal equations: ill-conditioned
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-6, atol=1e-9, err_msg=f"col {c} {f}")
-        elif f[1] in (L.FEAT_COUNT_IN_RANGE, L.FEAT_ACF_PERIOD_LAG):
+        elif f[1] in (L.FEAT_COUNT_IN_RANGE, L.FEAT_ACF_PERIOD_LAG, L.FEAT_NUMBER_CWT_PEAKS, L.FEAT_ADF_USEDLAG):
             np.testing.assert_array_equal(g[:, c], want[:, c], err_msg=f"col {c} {f}")
         else:
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-15, err_msg=f"col {c} {f}")
@@ -669,14 +672,15 @@ def test_two_parameter_features_through_the_extractor_names():
            "agg_linear_trend": [{"attr": "rvalue", "chunk_size": 50, "f_agg": "max"}],
            "ar_coefficient": [{"coeff": 1, "k": 10}], "linear_trend_timewise": [{"attr": "slope"}],
            "cwt_coefficients": [{"widths": (5,), "coeff": 3, "w": 5}], "friedrich_coefficients": None,
-           "max_langevin_fixed_point": None}
+           "max_langevin_fixed_point": None, "augmented_dickey_fuller": [{"attr": "pvalue"}],
+           "number_cwt_peaks": [{"max_width": 5}]}
     fx = FusedFeatureExtractor(time_steady=900.0, features=None, features_per_state={0: cfg}, normalize=False)
     solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=2000, t_eval=(900, 1000), device="cuda:0",
                               precision="fp64", feature_extractor=fx)
     y0 = seeded_ics(DUFFING, 32, seed=3).double()
     t, y = solver.integrate(DuffingODE(dict(zip(("delta", "k3", "A"), DUFFING.params))), y0)
     f = fx.extract_features(type("S", (), {"y": y})())
-    assert f.shape == (32, 26) and torch.isfinite(f).all()
+    assert f.shape == (32, 28) and torch.isfinite(f).all()
     assert fx.feature_names[0] == "state_0__agg_autocorrelation__f_agg_mean__maxlag_40"
     assert fx.feature_names[19] == "state_0__fft_aggregated__aggtype_kurtosis"
     assert fx.feature_names[22] == "state_0__linear_trend_timewise__attr_slope"
