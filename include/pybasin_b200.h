@@ -174,10 +174,14 @@ typedef enum {
     /* augmented_dickey_fuller with attr teststat / pvalue / usedlag in the kind
        (torch_features_trend.py:134-169), number_cwt_peaks (max_width <= 64;
        torch_features_pattern.py:154-188) */
-    PB_FEAT_ADF_TESTSTAT = 95, PB_FEAT_ADF_PVALUE = 96, PB_FEAT_ADF_USEDLAG = 97, PB_FEAT_NUMBER_CWT_PEAKS = 98
+    PB_FEAT_ADF_TESTSTAT = 95, PB_FEAT_ADF_PVALUE = 96, PB_FEAT_ADF_USEDLAG = 97, PB_FEAT_NUMBER_CWT_PEAKS = 98,
+    /* correlation_dimension (emb_dim <= 16, feat_param2 = lag * 1024 + n_rvals with
+       n_rvals <= 1023; Grassberger-Procaccia as src/pybasin/ts_torch/torch_corr_dim.py:17-110
+       states it; a symbolic kind, at most PB_SPECTRAL_WINDOW_MAX window samples) */
+    PB_FEAT_CORR_DIM = 99
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_NUMBER_CWT_PEAKS
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..98): the
+#define PB_FEAT_LAST_KIND PB_FEAT_CORR_DIM
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..99): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window
@@ -188,8 +192,8 @@ typedef enum {
    more window samples than this returns PB_EUNSUPPORTED */
 #define PB_FEAT_IS_SPECTRAL(k) ((k) >= PB_FEAT_SPECTRAL_FREQ_RATIO && (k) <= PB_FEAT_FOURIER_ENTROPY)
 #define PB_SPECTRAL_WINDOW_MAX 16384
-/* kinds 85..86 run one block per column over symbols in shared memory */
-#define PB_FEAT_IS_SYMBOLIC(k) ((k) == PB_FEAT_PERMUTATION_ENTROPY || (k) == PB_FEAT_LEMPEL_ZIV)
+/* kinds 85, 86 and 99 run one block per column with their data in shared memory */
+#define PB_FEAT_IS_SYMBOLIC(k) ((k) == PB_FEAT_PERMUTATION_ENTROPY || (k) == PB_FEAT_LEMPEL_ZIV || (k) == PB_FEAT_CORR_DIM)
 #define PB_SYMBOLIC_WINDOW_MAX 8191
 
 /* ---- per-trajectory status written to status_out ---- */

@@ -997,6 +997,77 @@ static double window_feature(int feat, double param, double param2, const double
         }
         return nw > 0 ? tot / nw : 0.0;
     }
+    /* ts_torch/torch_corr_dim.py:17-110 (Grassberger-Procaccia, as the reference
+       states it): delay vectors of emb_dim samples `lag` apart; n_rvals radii
+       exp(log(0.1 sd + 1e-10) + a_k (log(0.5 sd + 1e-10) - log(0.1 sd + 1e-10))), sd
+       the unbiased standard deviation, formed in FP32 as the reference's type
+       promotion does (a_k = torch.linspace(0, 1, n_rvals) in FP32: fma(step, k, 0)
+       for the first half, fma(-step, n_rvals - 1 - k, 1) for the rest); C(r_k) = the
+       share of ordered pairs of distinct vectors within r_k (Euclidean); the least-
+       squares slope of log C on log r over the radii with C > 0, NaN with fewer than
+       two or a degenerate fit */
+    case ORACLE_F_CORR_DIM: {
+        const int emb = (int)param, packed = (int)param2;
+        const int lag = packed / 1024, nr = packed % 1024;
+        const long M = (long)n - (long)(emb - 1) * lag;
+        if (M < 2 || nr < 1 || emb < 1 || lag < 1) return NAN;
+        const double sd = sqrt(m2 / (n - 1.0));
+        const double lmin = log(0.1 * sd + 1e-10), lmax = log(0.5 * sd + 1e-10);
+        const float ld = (float)(lmax - lmin), lmin32 = (float)lmin;
+        const float step = nr > 1 ? 1.0f / (float)(nr - 1) : 0.0f;
+        double *rv = (double *)malloc(sizeof(double) * (size_t)nr);
+        double *cnt = (double *)calloc((size_t)nr, sizeof(double));
+        if (!rv || !cnt) {
+            free(rv);
+            free(cnt);
+            return NAN;
+        }
+        for (int k = 0; k < nr; ++k) {
+            const float a = k < nr / 2 ? fmaf(step, (float)k, 0.0f) : fmaf(-step, (float)(nr - 1 - k), 1.0f);
+            const float prod = a * ld;
+            const float arg = lmin32 + prod;
+            rv[k] = (double)(float)exp((double)arg);
+        }
+        for (long i = 0; i < M; ++i)
+            for (long j = i + 1; j < M; ++j) {
+                double d2 = 0.0;
+                for (int e = 0; e < emb; ++e) {
+                    const double df = w[i + (long)e * lag] - w[j + (long)e * lag];
+                    d2 += df * df;
+                }
+                const double dist = sqrt(d2);
+                if (!(dist <= rv[nr - 1])) continue;
+                int lo = 0, hi = nr - 1; /* smallest k with dist <= rv[k] */
+                while (lo < hi) {
+                    const int mid = (lo + hi) / 2;
+                    if (dist <= rv[mid]) hi = mid;
+                    else lo = mid + 1;
+                }
+                cnt[lo] += 2.0;
+            }
+        /* the fit in centred form (n sum (r - mr)^2 equals the reference's
+           n sum r^2 - (sum r)^2, but is exactly 0 when all radii coincide) */
+        double acc = 0.0, nv = 0.0, sr = 0.0, sc = 0.0;
+        for (int k = 0; k < nr; ++k) {
+            acc += cnt[k];
+            cnt[k] = acc / ((double)M * (double)(M - 1)); /* C(r_k) */
+            if (!(cnt[k] > 0.0)) continue;
+            nv += 1.0;
+            sr += log(rv[k]);
+            sc += log(cnt[k] + 1e-30);
+        }
+        double srr = 0.0, src = 0.0;
+        for (int k = 0; k < nr; ++k) {
+            if (!(cnt[k] > 0.0)) continue;
+            const double dr = log(rv[k]) - sr / nv, dc = log(cnt[k] + 1e-30) - sc / nv;
+            srr += dr * dr;
+            src += dr * dc;
+        }
+        free(rv);
+        free(cnt);
+        const double den = nv * srr;
+        return (nv >= 2.0 && fabs(den) > 1e-10) ? (nv * src) / den : NAN;
+    }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;
     /* torch_features_count.py:42-45 */

@@ -72,6 +72,8 @@ enum {
     ORACLE_F_CWT = 92, ORACLE_F_FRIEDRICH = 93, ORACLE_F_LANGEVIN = 94,
     /* augmented_dickey_fuller (teststat, pvalue, usedlag), number_cwt_peaks (max_width) */
     ORACLE_F_ADF_TESTSTAT = 95, ORACLE_F_ADF_PVALUE = 96, ORACLE_F_ADF_USEDLAG = 97, ORACLE_F_NUMBER_CWT_PEAKS = 98,
+    /* correlation_dimension (emb_dim; param2 = lag * 1024 + n_rvals) */
+    ORACLE_F_CORR_DIM = 99,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

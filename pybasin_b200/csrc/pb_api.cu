@@ -1240,7 +1240,92 @@ __global__ void __launch_bounds__(256) k_window_symbolic(const float* __restrict
     const int kind = plan.kind[m];
     const float* x = win + (traj * plan.n_med + m) * static_cast<int64_t>(nwin);
     double result = 0.0;
-    if (kind == PB_FEAT_PERMUTATION_ENTROPY) {
+    if (kind == PB_FEAT_CORR_DIM) {
+        // correlation_dimension: delay vectors of emb samples `lag` apart from the
+        // window (kept as floats in shared memory); n_rvals radii between 0.1 and 0.5
+        // unbiased std on a log scale, formed in FP32 as the reference's type promotion
+        // does; every unordered pair of vectors adds 2 to the count of the smallest
+        // radius it lies within (binary search, a shared histogram per warp); then
+        // the least-squares slope of log C(r) on log r in centred form on thread 0
+        const int emb = static_cast<int>(plan.param[m]), packed = static_cast<int>(plan.param2[m]);
+        const int lag = packed / 1024, nr = packed % 1024;
+        const int64_t M = static_cast<int64_t>(nwin) - static_cast<int64_t>(emb - 1) * lag;
+        double sx = 0.0;
+        for (int i = threadIdx.x; i < nwin; i += blockDim.x) sx += static_cast<double>(x[i]);
+        const double mean = block_sum_d(sx, red) / nwin;
+        double sv = 0.0;
+        for (int i = threadIdx.x; i < nwin; i += blockDim.x) {
+            const double d = static_cast<double>(x[i]) - mean;
+            sv += d * d;
+        }
+        const double sd = sqrt(block_sum_d(sv, red) / (nwin - 1.0));
+        result = CUDART_NAN;
+        if (M >= 2) {
+            float* wx = reinterpret_cast<float*>(sm);
+            double* rv = reinterpret_cast<double*>(sm + (nwin + 3) / 4 * 4);
+            unsigned* hist = reinterpret_cast<unsigned*>(rv + nr);
+            const int nwarp = static_cast<int>(blockDim.x >> 5), warp = static_cast<int>(threadIdx.x >> 5);
+            for (int i = threadIdx.x; i < nwin; i += blockDim.x) wx[i] = x[i];
+            const double lmin = log(0.1 * sd + 1e-10), lmax = log(0.5 * sd + 1e-10);
+            const float ld = static_cast<float>(lmax - lmin), lmin32 = static_cast<float>(lmin);
+            const float step = nr > 1 ? __fdiv_rn(1.0f, static_cast<float>(nr - 1)) : 0.0f;
+            for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+                const float a = k < nr / 2 ? __fmaf_rn(step, static_cast<float>(k), 0.0f)
+                                           : __fmaf_rn(-step, static_cast<float>(nr - 1 - k), 1.0f);
+                const float arg = __fadd_rn(lmin32, __fmul_rn(a, ld));
+                rv[k] = static_cast<double>(static_cast<float>(exp(static_cast<double>(arg))));
+            }
+            for (int q = threadIdx.x; q < nwarp * nr; q += blockDim.x) hist[q] = 0u;
+            __syncthreads();
+            const double rmax = rv[nr - 1];
+            for (int64_t i = threadIdx.x; i < M; i += blockDim.x) {
+                float vi[16];
+                for (int e = 0; e < emb; ++e) vi[e] = wx[i + static_cast<int64_t>(e) * lag];
+                for (int64_t j = i + 1; j < M; ++j) {
+                    double d2 = 0.0;
+                    for (int e = 0; e < emb; ++e) {
+                        const double df =
+                            static_cast<double>(vi[e]) - static_cast<double>(wx[j + static_cast<int64_t>(e) * lag]);
+                        d2 += df * df;
+                    }
+                    const double dist = sqrt(d2);
+                    if (!(dist <= rmax)) continue;
+                    int lo = 0, hi = nr - 1;  // smallest k with dist <= rv[k]
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (dist <= rv[mid]) hi = mid;
+                        else lo = mid + 1;
+                    }
+                    atomicAdd(&hist[warp * nr + lo], 1u);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const double pairs = static_cast<double>(M) * static_cast<double>(M - 1);
+                double acc = 0.0, nv = 0.0, sr = 0.0, sc = 0.0;
+                for (int k = 0; k < nr; ++k) {
+                    for (int w = 0; w < nwarp; ++w) acc += 2.0 * hist[w * nr + k];
+                    const double c = acc / pairs;
+                    if (!(c > 0.0)) continue;
+                    nv += 1.0;
+                    sr += log(rv[k]);
+                    sc += log(c + 1e-30);
+                }
+                double srr = 0.0, src = 0.0;
+                acc = 0.0;
+                for (int k = 0; k < nr; ++k) {
+                    for (int w = 0; w < nwarp; ++w) acc += 2.0 * hist[w * nr + k];
+                    const double c = acc / pairs;
+                    if (!(c > 0.0)) continue;
+                    const double dr = log(rv[k]) - sr / nv, dc = log(c + 1e-30) - sc / nv;
+                    srr += dr * dr;
+                    src += dr * dc;
+                }
+                const double den = nv * srr;
+                result = (nv >= 2.0 && fabs(den) > 1e-10) ? (nv * src) / den : CUDART_NAN;
+            }
+        }
+    } else if (kind == PB_FEAT_PERMUTATION_ENTROPY) {
         const int tau = static_cast<int>(plan.param[m]), d = static_cast<int>(plan.param2[m]);
         const int64_t npat = static_cast<int64_t>(nwin) - static_cast<int64_t>(d - 1) * tau;
         if (npat > 0) {
@@ -1728,6 +1813,11 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_AR_COEFFICIENT && !(is_int(prm, 1.0, 10.0) && is_int(prm2, 0.0, 1e6))) return PB_EINVAL;
         if (kind == PB_FEAT_CWT && !(is_int(prm, 1.0, 1e4) && is_int(prm2, -1.0, 1e9))) return PB_EINVAL;
         if (kind == PB_FEAT_NUMBER_CWT_PEAKS && !is_int(prm, 0.0, 64.0)) return PB_EINVAL;
+        if (kind == PB_FEAT_CORR_DIM) {
+            if (!(is_int(prm, 1.0, 16.0) && is_int(prm2, 1024.0, 1024.0 * 100000.0 + 1023.0))) return PB_EINVAL;
+            if (static_cast<int>(prm2) % 1024 < 1) return PB_EINVAL;
+            if (a->n_save - a->win_begin > PB_SPECTRAL_WINDOW_MAX) return PB_EUNSUPPORTED;
+        }
         if ((kind == PB_FEAT_FRIEDRICH || kind == PB_FEAT_LANGEVIN) && !(is_int(prm, 0.0, 6.0) && is_int(prm2, 0.0, 1e6)))
             return PB_EINVAL;
         if ((kind == PB_FEAT_ACF_PERIOD_STRENGTH || kind == PB_FEAT_ACF_PERIOD_LAG) && !is_int(prm, 0.0, 1e9))
@@ -1900,12 +1990,22 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
         if (plan.n_symbolic > 0) {
             const int nwin = a.n_save - a.win_begin;
             bool lz = false;
-            for (int q = 0; q < plan.n_symbolic; ++q) lz |= plan.kind[plan.symbolic_m[q]] == PB_FEAT_LEMPEL_ZIV;
+            size_t cd = 0;  // correlation_dimension: window floats, radii (doubles), a histogram per warp
+            for (int q = 0; q < plan.n_symbolic; ++q) {
+                const int mq = plan.symbolic_m[q];
+                lz |= plan.kind[mq] == PB_FEAT_LEMPEL_ZIV;
+                if (plan.kind[mq] == PB_FEAT_CORR_DIM) {
+                    const size_t nr = static_cast<size_t>(static_cast<int>(plan.param2[mq]) % 1024);
+                    cd = std::max(cd, static_cast<size_t>((nwin + 3) / 4 * 16) + nr * sizeof(double) +
+                                          8 * nr * sizeof(unsigned));
+                }
+            }
             // trie table: a power of two >= 2 (nwin + 1) entries (at most half full), keys and children
             int table = 1;
             while (table < 2 * (nwin + 1)) table <<= 1;
             size_t smem = 5040 * sizeof(unsigned);  // the permutation histogram (d <= 7)
             if (lz) smem = std::max(smem, static_cast<size_t>((nwin + 15) / 16 * 16) + 2 * sizeof(unsigned) * table);
+            smem = std::max(smem, cd);
             const int64_t sblocks = a.n_traj * plan.n_symbolic;
             if (sblocks > 0x7fffffffLL) return PB_EINVAL;
             if (smem > 48 * 1024)

@@ -101,6 +101,7 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "cwt_coefficients": [{"widths": (2,), "coeff": 0, "w": 2}],
     "friedrich_coefficients": [{"coeff": 0, "m": 3, "r": 30}],
     "max_langevin_fixed_point": [{"m": 3, "r": 30}],
+    "correlation_dimension": [{"emb_dim": 4, "lag": 1, "n_rvals": 50}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -156,6 +157,11 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
         if fname == "friedrich_coefficients":
             return FeatureColumn(state, L.FEAT_FRIEDRICH, float(m_deg), name, float(p.get("coeff", 0)))
         return FeatureColumn(state, L.FEAT_LANGEVIN, float(m_deg), name)
+    if fname == "correlation_dimension":  # ts_torch/torch_corr_dim.py:17-110
+        emb, lag, nr = int(p.get("emb_dim", 4)), int(p.get("lag", 1)), int(p.get("n_rvals", 50))
+        if not (1 <= emb <= 16 and 1 <= lag <= 100000 and 1 <= nr <= 1023):
+            raise ValueError("correlation_dimension: emb_dim <= 16, lag <= 100000 and n_rvals <= 1023 are fused")
+        return FeatureColumn(state, L.FEAT_CORR_DIM, float(emb), name, float(lag * 1024 + nr))
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140

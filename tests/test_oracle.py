@@ -286,6 +286,26 @@ def test_oracle_two_parameter_and_acf_features_match_reference_calculators(name,
         np.testing.assert_allclose(got, want, rtol=2e-7 if want.dtype == np.float32 else 1e-12, atol=1e-12)
 
 
+@pytest.mark.parametrize("src", ["x", "x_periodic"])
+@pytest.mark.parametrize("emb, lag, n_rvals", [(4, 1, 50), (2, 3, 20), (6, 2, 50)])
+def test_oracle_correlation_dimension_matches_reference(src, emb, lag, n_rvals):
+    """Grassberger-Procaccia correlation dimension (ts_torch/torch_corr_dim.py).  The
+    reference fits the slope in FP32: 1e-4 relative, and where the exact slope is 0
+    (every radius holding the same pair count) its cancellation leaves up to 2e-3.
+    A constant window makes the fit degenerate; the reference then returns 0 or
+    NaN depending on its FP32 rounding, the oracle NaN, so those columns are skipped."""
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g[src]
+    tag = "x" if src == "x" else "periodic"
+    want = g[f"{tag}_correlation_dimension_{emb}_{lag}_{n_rvals}"].astype(np.float64)
+    got = np.array([[O.window_feature(99, float(emb), x[:, b, s], float(lag * 1024 + n_rvals)) for s in range(2)]
+                    for b in range(x.shape[1])])
+    live = x.std(axis=0) > 0
+    assert live.sum() >= 30
+    np.testing.assert_allclose(got[live], want[live], rtol=1e-4, atol=2e-3)
+    assert np.isnan(got[~live]).all()
+
+
 def test_oracle_quantile_even_length():
     g = np.load(GOLDEN / "features_reference.npz")
     x = g["x_even"]
