@@ -178,10 +178,14 @@ typedef enum {
     /* correlation_dimension (emb_dim <= 16, feat_param2 = lag * 1024 + n_rvals with
        n_rvals <= 1023; Grassberger-Procaccia as src/pybasin/ts_torch/torch_corr_dim.py:17-110
        states it; a symbolic kind, at most PB_SPECTRAL_WINDOW_MAX window samples) */
-    PB_FEAT_CORR_DIM = 99
+    PB_FEAT_CORR_DIM = 99,
+    /* lyapunov_r (feat_param = emb_dim * 1024 + trajectory_len, feat_param2 = lag, tau
+       = 1; Rosenstein as src/pybasin/ts_torch/torch_lyapunov_r.py states it; a
+       symbolic kind, at most PB_SPECTRAL_WINDOW_MAX window samples) */
+    PB_FEAT_LYAP_R = 100
 } pb_feature;
-#define PB_FEAT_LAST_KIND PB_FEAT_CORR_DIM
-/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..99): the
+#define PB_FEAT_LAST_KIND PB_FEAT_LYAP_R
+/* kinds computed from the stored feature window (PB_FEAT_MEDIAN and 18..100): the
    window costs n_traj x (n_save - win_begin) floats of scratch per such column */
 #define PB_FEAT_IS_WINDOW(k) ((k) == PB_FEAT_MEDIAN || ((k) >= PB_FEAT_QUANTILE && (k) <= PB_FEAT_LAST_KIND))
 /* kinds 59..64 sort the window in shared memory: a request with more window
@@ -192,8 +196,9 @@ typedef enum {
    more window samples than this returns PB_EUNSUPPORTED */
 #define PB_FEAT_IS_SPECTRAL(k) ((k) >= PB_FEAT_SPECTRAL_FREQ_RATIO && (k) <= PB_FEAT_FOURIER_ENTROPY)
 #define PB_SPECTRAL_WINDOW_MAX 16384
-/* kinds 85, 86 and 99 run one block per column with their data in shared memory */
-#define PB_FEAT_IS_SYMBOLIC(k) ((k) == PB_FEAT_PERMUTATION_ENTROPY || (k) == PB_FEAT_LEMPEL_ZIV || (k) == PB_FEAT_CORR_DIM)
+/* kinds 85, 86, 99 and 100 run one block per column with their data in shared memory */
+#define PB_FEAT_IS_SYMBOLIC(k) \
+    ((k) == PB_FEAT_PERMUTATION_ENTROPY || (k) == PB_FEAT_LEMPEL_ZIV || (k) == PB_FEAT_CORR_DIM || (k) == PB_FEAT_LYAP_R)
 #define PB_SYMBOLIC_WINDOW_MAX 8191
 
 /* ---- per-trajectory status written to status_out ---- */

@@ -240,6 +240,17 @@ static int poly_velocity_fit(const double *w, int n, int m, double *c)
     return 0;
 }
 
+/* Euclidean distance of the delay vectors starting at samples a and b */
+static double lyap_dist(const double *w, long a, long b, int emb, int lag)
+{
+    double d2 = 0.0;
+    for (int e = 0; e < emb; ++e) {
+        const double df = w[a + (long)e * lag] - w[b + (long)e * lag];
+        d2 += df * df;
+    }
+    return sqrt(d2);
+}
+
 static double window_feature(int feat, double param, double param2, const double *w, int n, double *scratch)
 {
     if (n <= 0) return NAN;
@@ -1067,6 +1078,80 @@ static double window_feature(int feat, double param, double param2, const double
         free(cnt);
         const double den = nv * srr;
         return (nv >= 2.0 && fabs(den) > 1e-10) ? (nv * src) / den : NAN;
+    }
+    /* ts_torch/torch_lyapunov_r.py (Rosenstein, as the reference states it):
+       min_tsep = ceil(1 / mean frequency) of the power spectrum of the window
+       zero-padded to 2n-1 (bins k >= 1, frequency k / (2n-1)), clamped to
+       [1, floor(n / 4)]; delay vectors of emb_dim samples `lag` apart; each of the
+       first ntraj = max(M - L + 1, 1) vectors takes as neighbour the first nearest
+       one among them more than min_tsep away (index 0 if none); div[k] = mean over
+       i of log d(i + k, nb(i) + k) over pairs inside the orbit with d > 0 (a pair
+       within min_tsep counts as +inf), stored in FP32 as the reference's buffer
+       is; the least-squares slope of div on k = 0..L-1 over its finite entries */
+    case ORACLE_F_LYAP_R: {
+        const int emb = (int)param / 1024, L = (int)param % 1024, lag = (int)param2;
+        const long M = (long)n - (long)(emb - 1) * lag;
+        if (M < 1 || emb < 1 || L < 1 || lag < 1) return NAN;
+        const long N2 = 2L * n - 1;
+        const double two_pi = 6.283185307179586476925286766559;
+        double sfp = 0.0, sp = 0.0;
+        for (long k = 1; k <= N2 / 2; ++k) {
+            double re = 0.0, im = 0.0;
+            long ph = 0;
+            for (int i = 0; i < n; ++i) {
+                const double ang = two_pi * (double)ph / N2;
+                re += w[i] * cos(ang);
+                im -= w[i] * sin(ang);
+                ph += k;
+                if (ph >= N2) ph -= N2;
+            }
+            const double p = re * re + im * im;
+            sfp += ((double)k / N2) * p;
+            sp += p;
+        }
+        const double mf = sfp / (sp + 1e-10);
+        long tsep = (long)ceil(1.0 / (mf + 1e-10));
+        const long maxt = (long)(0.25 * n);
+        if (tsep > maxt) tsep = maxt;
+        if (tsep < 1) tsep = 1;
+        const long ntraj = M - L + 1 > 1 ? M - L + 1 : 1;
+#define LYAP_DIST(a, b) (labs((a) - (b)) <= tsep ? INFINITY : lyap_dist(w, (a), (b), emb, lag))
+        long *nb = (long *)malloc(sizeof(long) * (size_t)ntraj);
+        if (!nb) return NAN;
+        for (long i = 0; i < ntraj; ++i) {
+            double best = INFINITY;
+            long bj = 0;
+            for (long j = 0; j < ntraj; ++j) {
+                const double d = LYAP_DIST(i, j);
+                if (d < best) {
+                    best = d;
+                    bj = j;
+                }
+            }
+            nb[i] = bj;
+        }
+        double nf = 0.0, sk = 0.0, sd = 0.0, skk = 0.0, skd = 0.0;
+        for (int k = 0; k < L; ++k) {
+            double acc = 0.0, cnt = 0.0;
+            for (long i = 0; i < ntraj; ++i) {
+                if (i + k >= M || nb[i] + k >= M) continue;
+                const double d = LYAP_DIST(i + k, nb[i] + k);
+                if (!(d > 0.0)) continue;
+                acc += log(d);
+                cnt += 1.0;
+            }
+            const double div = (double)(float)(cnt > 0.0 ? acc / cnt : NAN);
+            if (!isfinite(div)) continue;
+            nf += 1.0;
+            sk += k;
+            sd += div;
+            skk += (double)k * k;
+            skd += k * div;
+        }
+#undef LYAP_DIST
+        free(nb);
+        const double den = nf * skk - sk * sk;
+        return (nf >= 2.0 && fabs(den) > 1e-10) ? (nf * skd - sk * sd) / den : NAN;
     }
     /* torch_features_boolean.py:37-41 */
     case ORACLE_F_VAR_LARGER_THAN_STD: return sqrt(m2 / n) > 1.0 ? 1.0 : 0.0;

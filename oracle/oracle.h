@@ -74,6 +74,8 @@ enum {
     ORACLE_F_ADF_TESTSTAT = 95, ORACLE_F_ADF_PVALUE = 96, ORACLE_F_ADF_USEDLAG = 97, ORACLE_F_NUMBER_CWT_PEAKS = 98,
     /* correlation_dimension (emb_dim; param2 = lag * 1024 + n_rvals) */
     ORACLE_F_CORR_DIM = 99,
+    /* lyapunov_r (param = emb_dim * 1024 + trajectory_len, param2 = lag; tau = 1) */
+    ORACLE_F_LYAP_R = 100,
 };
 #define ORACLE_MAX_ACF_LAG 63 /* partial_autocorrelation lags held on the stack */
 

@@ -106,7 +106,7 @@ FEAT_AGG_TREND_MEAN, FEAT_AGG_TREND_VAR, FEAT_AGG_TREND_MIN, FEAT_AGG_TREND_MAX 
 FEAT_AR_COEFFICIENT = 91
 FEAT_CWT, FEAT_FRIEDRICH, FEAT_LANGEVIN = 92, 93, 94
 FEAT_ADF_TESTSTAT, FEAT_ADF_PVALUE, FEAT_ADF_USEDLAG, FEAT_NUMBER_CWT_PEAKS = 95, 96, 97, 98
-FEAT_CORR_DIM = 99
+FEAT_CORR_DIM, FEAT_LYAP_R = 99, 100
 SPECTRAL_WINDOW_MAX = 16384  # PB_SPECTRAL_WINDOW_MAX: window samples of the spectral kinds 79..84
 SYMBOLIC_WINDOW_MAX = 8191  # PB_SYMBOLIC_WINDOW_MAX: window samples of lempel_ziv_complexity
 SORTED_WINDOW_MAX = 32768  # PB_SORTED_WINDOW_MAX: window samples of the sorted kinds 59..64

@@ -1325,6 +1325,90 @@ __global__ void __launch_bounds__(256) k_window_symbolic(const float* __restrict
                 result = (nv >= 2.0 && fabs(den) > 1e-10) ? (nv * src) / den : CUDART_NAN;
             }
         }
+    } else if (kind == PB_FEAT_LYAP_R) {
+        // lyapunov_r (Rosenstein): min_tsep from the mean frequency of the window's
+        // spectrum zero-padded to 2n-1 (Goertzel per bin, bins over threads); each of
+        // the first ntraj delay vectors takes the first nearest one more than min_tsep
+        // away (threads over vectors, the window as floats in shared memory); the mean
+        // log divergence at each step k (block sums), rounded to FP32 as the reference
+        // stores it; the line fit on thread 0
+        const int emb = static_cast<int>(plan.param[m]) / 1024, L = static_cast<int>(plan.param[m]) % 1024;
+        const int lag = static_cast<int>(plan.param2[m]);
+        const int64_t M = static_cast<int64_t>(nwin) - static_cast<int64_t>(emb - 1) * lag;
+        result = CUDART_NAN;
+        if (M >= 1) {
+            float* wx = reinterpret_cast<float*>(sm);
+            int* nb = reinterpret_cast<int*>(sm + (nwin + 3) / 4 * 4);
+            for (int i = threadIdx.x; i < nwin; i += blockDim.x) wx[i] = x[i];
+            __syncthreads();
+            const int64_t N2 = 2ll * nwin - 1;
+            double afp = 0.0, ap = 0.0;
+            for (int64_t k = 1 + threadIdx.x; k <= N2 / 2; k += blockDim.x) {
+                double sn, cs;
+                sincospi(2.0 * static_cast<double>(k) / static_cast<double>(N2), &sn, &cs);
+                const double c = 2.0 * cs;
+                double s1 = 0.0, s2 = 0.0;
+                for (int i = 0; i < nwin; ++i) {
+                    const double t = fma(c, s1, static_cast<double>(wx[i]) - s2);
+                    s2 = s1;
+                    s1 = t;
+                }
+                const double re = s1 - cs * s2, im = sn * s2, p = re * re + im * im;
+                afp += (static_cast<double>(k) / static_cast<double>(N2)) * p;
+                ap += p;
+            }
+            const double sfp = block_sum_d(afp, red), sp = block_sum_d(ap, red);
+            int64_t tsep = static_cast<int64_t>(ceil(1.0 / (sfp / (sp + 1e-10) + 1e-10)));
+            const int64_t maxt = static_cast<int64_t>(0.25 * nwin);
+            tsep = tsep > maxt ? maxt : tsep;
+            tsep = tsep < 1 ? 1 : tsep;
+            const int64_t ntraj = M - L + 1 > 1 ? M - L + 1 : 1;
+            const auto dist = [&](int64_t a, int64_t b) -> double {
+                if ((a > b ? a - b : b - a) <= tsep) return CUDART_INF;
+                double d2 = 0.0;
+                for (int e = 0; e < emb; ++e) {
+                    const double df = static_cast<double>(wx[a + static_cast<int64_t>(e) * lag]) -
+                                      static_cast<double>(wx[b + static_cast<int64_t>(e) * lag]);
+                    d2 += df * df;
+                }
+                return sqrt(d2);
+            };
+            for (int64_t i = threadIdx.x; i < ntraj; i += blockDim.x) {
+                double best = CUDART_INF;
+                int bj = 0;
+                for (int64_t j = 0; j < ntraj; ++j) {
+                    const double d = dist(i, j);
+                    if (d < best) {
+                        best = d;
+                        bj = static_cast<int>(j);
+                    }
+                }
+                nb[i] = bj;
+            }
+            __syncthreads();
+            double nf = 0.0, sk = 0.0, sd = 0.0, skk = 0.0, skd = 0.0;
+            for (int k = 0; k < L; ++k) {
+                double acc = 0.0, cnt = 0.0;
+                for (int64_t i = threadIdx.x; i < ntraj; i += blockDim.x) {
+                    if (i + k >= M || nb[i] + k >= M) continue;
+                    const double d = dist(i + k, nb[i] + k);
+                    if (!(d > 0.0)) continue;
+                    acc += log(d);
+                    cnt += 1.0;
+                }
+                acc = block_sum_d(acc, red);
+                cnt = block_sum_d(cnt, red);
+                const double div = static_cast<double>(static_cast<float>(cnt > 0.0 ? acc / cnt : CUDART_NAN));
+                if (!isfinite(div)) continue;
+                nf += 1.0;
+                sk += k;
+                sd += div;
+                skk += static_cast<double>(k) * k;
+                skd += k * div;
+            }
+            const double den = nf * skk - sk * sk;
+            result = (nf >= 2.0 && fabs(den) > 1e-10) ? (nf * skd - sk * sd) / den : CUDART_NAN;
+        }
     } else if (kind == PB_FEAT_PERMUTATION_ENTROPY) {
         const int tau = static_cast<int>(plan.param[m]), d = static_cast<int>(plan.param2[m]);
         const int64_t npat = static_cast<int64_t>(nwin) - static_cast<int64_t>(d - 1) * tau;
@@ -1813,6 +1897,12 @@ int validate_args(const pb_solve_args* a, bool user_system)
         if (kind == PB_FEAT_AR_COEFFICIENT && !(is_int(prm, 1.0, 10.0) && is_int(prm2, 0.0, 1e6))) return PB_EINVAL;
         if (kind == PB_FEAT_CWT && !(is_int(prm, 1.0, 1e4) && is_int(prm2, -1.0, 1e9))) return PB_EINVAL;
         if (kind == PB_FEAT_NUMBER_CWT_PEAKS && !is_int(prm, 0.0, 64.0)) return PB_EINVAL;
+        if (kind == PB_FEAT_LYAP_R) {
+            const int e = static_cast<int>(prm) / 1024, tl = static_cast<int>(prm) % 1024;
+            if (!(is_int(prm, 1024.0, 64.0 * 1024.0 + 1023.0) && e >= 1 && tl >= 1 && is_int(prm2, 1.0, 100000.0)))
+                return PB_EINVAL;
+            if (a->n_save - a->win_begin > PB_SPECTRAL_WINDOW_MAX) return PB_EUNSUPPORTED;
+        }
         if (kind == PB_FEAT_CORR_DIM) {
             if (!(is_int(prm, 1.0, 16.0) && is_int(prm2, 1024.0, 1024.0 * 100000.0 + 1023.0))) return PB_EINVAL;
             if (static_cast<int>(prm2) % 1024 < 1) return PB_EINVAL;
@@ -1994,6 +2084,8 @@ int solve_with(const KernelSel& k, const pb_solve_args& a, cudaStream_t st)
             for (int q = 0; q < plan.n_symbolic; ++q) {
                 const int mq = plan.symbolic_m[q];
                 lz |= plan.kind[mq] == PB_FEAT_LEMPEL_ZIV;
+                if (plan.kind[mq] == PB_FEAT_LYAP_R)  // window floats and a neighbour index per vector
+                    cd = std::max(cd, static_cast<size_t>((nwin + 3) / 4 * 16) + sizeof(int) * nwin);
                 if (plan.kind[mq] == PB_FEAT_CORR_DIM) {
                     const size_t nr = static_cast<size_t>(static_cast<int>(plan.param2[mq]) % 1024);
                     cd = std::max(cd, static_cast<size_t>((nwin + 3) / 4 * 16) + nr * sizeof(double) +

@@ -102,6 +102,7 @@ FEATURE_MULTI: dict[str, list[dict[str, Any]] | None] = {
     "friedrich_coefficients": [{"coeff": 0, "m": 3, "r": 30}],
     "max_langevin_fixed_point": [{"m": 3, "r": 30}],
     "correlation_dimension": [{"emb_dim": 4, "lag": 1, "n_rvals": 50}],
+    "lyapunov_r": [{"emb_dim": 10, "lag": 1, "trajectory_len": 20, "tau": 1.0}],
 }
 _AGG_ACF_KIND = {"mean": L.FEAT_AGG_AUTOCORR_MEAN, "median": L.FEAT_AGG_AUTOCORR_MEDIAN,
                  "var": L.FEAT_AGG_AUTOCORR_VAR}
@@ -162,6 +163,11 @@ def _multi_column(fname: str, p: dict[str, Any], state: int) -> FeatureColumn:
         if not (1 <= emb <= 16 and 1 <= lag <= 100000 and 1 <= nr <= 1023):
             raise ValueError("correlation_dimension: emb_dim <= 16, lag <= 100000 and n_rvals <= 1023 are fused")
         return FeatureColumn(state, L.FEAT_CORR_DIM, float(emb), name, float(lag * 1024 + nr))
+    if fname == "lyapunov_r":  # ts_torch/torch_lyapunov_r.py (Rosenstein)
+        emb, lag, tl = int(p.get("emb_dim", 10)), int(p.get("lag", 1)), int(p.get("trajectory_len", 20))
+        if float(p.get("tau", 1.0)) != 1.0 or not (1 <= emb <= 64 and 1 <= lag <= 100000 and 1 <= tl <= 1023):
+            raise ValueError("lyapunov_r: the fused path takes tau = 1, emb_dim <= 64, trajectory_len <= 1023")
+        return FeatureColumn(state, L.FEAT_LYAP_R, float(emb * 1024 + tl), name, float(lag))
     if fname == "count_in_range":  # torch_features_count.py:37-39
         return FeatureColumn(state, L.FEAT_COUNT_IN_RANGE, float(p["min_val"]), name, float(p["max_val"]))
     # change_quantiles, torch_features_change.py:113-140

@@ -240,6 +240,8 @@ def _features(ref: Path) -> None:
            for src, v in (("x", x), ("periodic", per), ("rep", rep)) for w in (1, 5, 200)},
         **{f"{src}_correlation_dimension_{e}_{l}_{r}": dy.correlation_dimension(v, e, l, r).numpy()
            for src, v in (("x", x), ("periodic", per)) for (e, l, r) in ((4, 1, 50), (2, 3, 20), (6, 2, 50))},
+        **{f"{src}_lyapunov_r_{e}_{l}_{t}": dy.lyapunov_r(v, e, l, t, 1.0).numpy()
+           for src, v in (("x", x), ("periodic", per)) for (e, l, t) in ((10, 1, 20), (4, 2, 10), (3, 1, 40))},
         **{f"{src}_ar_coefficient_{k}_{c}": tr.ar_coefficient(v, k, c).numpy()
            for src, v in (("x", x), ("periodic", per)) for (k, c) in ((10, 0), (10, 3), (10, 9), (10, 10), (1, 0),
                                                                        (4, 2))},

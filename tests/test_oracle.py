@@ -306,6 +306,21 @@ def test_oracle_correlation_dimension_matches_reference(src, emb, lag, n_rvals):
     assert np.isnan(got[~live]).all()
 
 
+@pytest.mark.parametrize("src", ["x", "x_periodic"])
+@pytest.mark.parametrize("emb, lag, tlen", [(10, 1, 20), (4, 2, 10), (3, 1, 40)])
+def test_oracle_lyapunov_r_matches_reference(src, emb, lag, tlen):
+    """Largest Lyapunov exponent by Rosenstein's method (ts_torch/torch_lyapunov_r.py):
+    the reference keeps the divergence curve and its fit in FP32, so 1e-4 relative
+    (the differences seen are below 6e-6)."""
+    g = np.load(GOLDEN / "features_reference.npz")
+    x = g[src]
+    tag = "x" if src == "x" else "periodic"
+    want = g[f"{tag}_lyapunov_r_{emb}_{lag}_{tlen}"].astype(np.float64)
+    got = np.array([[O.window_feature(100, float(emb * 1024 + tlen), x[:, b, s], float(lag)) for s in range(2)]
+                    for b in range(x.shape[1])])
+    np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-6)
+
+
 def test_oracle_quantile_even_length():
     g = np.load(GOLDEN / "features_reference.npz")
     x = g["x_even"]

@@ -721,13 +721,15 @@ SYMBOLIC_FEATS = [(0, L.FEAT_PERMUTATION_ENTROPY, 1.0, 3.0), (1, L.FEAT_PERMUTAT
                   (0, L.FEAT_PERMUTATION_ENTROPY, 1.0, 7.0), (1, L.FEAT_PERMUTATION_ENTROPY, 40.0, 4.0),
                   (0, L.FEAT_LEMPEL_ZIV, 2.0), (1, L.FEAT_LEMPEL_ZIV, 10.0), (0, L.FEAT_LEMPEL_ZIV, 100.0),
                   (1, L.FEAT_LEMPEL_ZIV, 255.0), (0, L.FEAT_CORR_DIM, 4.0, 1 * 1024 + 50.0),
-                  (1, L.FEAT_CORR_DIM, 2.0, 3 * 1024 + 20.0), (0, L.FEAT_FOURIER_ENTROPY, 10.0)]
+                  (1, L.FEAT_CORR_DIM, 2.0, 3 * 1024 + 20.0), (0, L.FEAT_LYAP_R, 10 * 1024 + 20.0, 1.0),
+                  (1, L.FEAT_LYAP_R, 4 * 1024 + 10.0, 2.0), (0, L.FEAT_FOURIER_ENTROPY, 10.0)]
 
 
 @pytest.mark.parametrize("n_save", [1001, 8191 + 250])
 def test_entropy_and_complexity_features_on_identical_windows(n_save):
-    """Permutation entropy, Lempel-Ziv complexity, correlation dimension and
-    Fourier entropy from the symbolic and spectrum passes against the oracle on the kernel's own FP32
+    """Permutation entropy, Lempel-Ziv complexity, correlation dimension, the
+    largest Lyapunov exponent and Fourier entropy from the symbolic and spectrum
+    passes against the oracle on the kernel's own FP32
     window: the phrase counts exactly, the permutation entropy to summation order,
     the Fourier entropy to 1e-8 (the spectrum pass's rounding).  The
     long case fills the largest Lempel-Ziv window (8,191 samples; a 128 KB trie
@@ -737,7 +739,8 @@ def test_entropy_and_complexity_features_on_identical_windows(n_save):
     wb = 250 if n_save > 8191 else int(np.nonzero(save >= 20.0)[0][0])
     # the oracle's direct DFT and pair counts are O(n^2): the long case keeps the linear kinds
     feats = SYMBOLIC_FEATS if n_save < 8191 else [f for f in SYMBOLIC_FEATS
-                                                  if f[1] not in (L.FEAT_FOURIER_ENTROPY, L.FEAT_CORR_DIM)]
+                                                  if f[1] not in (L.FEAT_FOURIER_ENTROPY, L.FEAT_CORR_DIM,
+                                                                  L.FEAT_LYAP_R)]
     got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 60.0), 1e-8, 1e-10,
                     win_begin=wb, features=feats, keep_full=True)
     assert (got["status"] == 0).all()
@@ -748,6 +751,8 @@ def test_entropy_and_complexity_features_on_identical_windows(n_save):
     for c, f in enumerate(feats):
         if f[1] == L.FEAT_LEMPEL_ZIV:
             np.testing.assert_array_equal(g[:, c], want[:, c], err_msg=f"col {c} {f}")
+        elif f[1] == L.FEAT_LYAP_R:  # same neighbours; divergences rounded to FP32 as the reference stores them
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-5, atol=1e-7, err_msg=f"col {c} {f}")
         elif f[1] == L.FEAT_CORR_DIM:  # exact pair counts; the log-log fit to summation order
             np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-12, err_msg=f"col {c} {f}")
         elif f[1] == L.FEAT_FOURIER_ENTROPY:  # spectrum by Goertzel: rounding grows as n eps / sin(w)
