@@ -570,8 +570,8 @@ def run_b200_arm(args) -> None:
                 "frac": achieved / peak32,
                 "traffic": 1.6934e9 * (n + len(DUFFING["templates"])) / 50005,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel "
-                                  "(main phase of the probed integrator) at N=50,000, scaled by trajectories "
-                                  "(profiles/k_solve_queue_probed_duffing50k.md): the window's step records, "
+                                  "(main phase of the probed integrator) at N=50,000, scaled by trajectories: "
+                                  "the window's step records, "
                                   "written by the integrating lanes and read back by the warps that drain "
                                   "the sampling into the same launch",
                 "note": "achieved counts the integration FLOPs only; the dominant kernel's time also holds "

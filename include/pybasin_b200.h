@@ -382,7 +382,8 @@ int pb_probe_fma(int32_t precision, int32_t blocks, int32_t iters, float* sink, 
  * loaded on (held until the process exits).  A request whose scratch
  * (pb_solve_scratch_bytes + 256) exceeds that size returns PB_ESCRATCH_LIMIT and
  * launches nothing.  The first call on a device looks up the array's device
- * address (once per device); make that first call before any stream capture.
+ * address (once per device and context: after cudaDeviceReset the next call
+ * looks it up again); make that first call before any stream capture.
  * All calls on a device share the one array: calls whose kernels may overlap on
  * the GPU (different streams, or several host threads) race and must be
  * serialised by the caller.  The call itself allocates nothing. */

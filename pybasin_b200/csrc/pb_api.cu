@@ -2141,6 +2141,8 @@ const char* pb_error_string(int32_t s)
 int64_t pb_solve_scratch_bytes(const pb_solve_args* a)
 {
     if (!a || a->n_traj < 0 || a->n_save < 1 || a->win_begin < 0 || a->win_begin >= a->n_save) return -1;
+    // the layout walks feat_kind / feat_state up to n_features: bound it to the arrays first
+    if (a->n_features < 0 || a->n_features > PB_MAX_FEATURES) return -1;
     const ScratchLayout sl = scratch_layout(*a);
     if (!sl.probed) return sl.total;
     if (a->n_traj > 0x7fffffffLL) return -1;

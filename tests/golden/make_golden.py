@@ -4,6 +4,8 @@ Run once in a container where the reference tree is present:
 
     python tests/golden/make_golden.py /root/reference
 
+(the reference tree is a required argument, or the PYBASIN_REFERENCE
+environment variable).
 It imports the reference (with empty stand-in modules for the two imports that
 are not installed, ``torchdiffeq`` and ``matplotlib``; neither is on the paths
 used here) and writes:
@@ -30,6 +32,7 @@ used here) and writes:
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tempfile
 import types
@@ -303,7 +306,10 @@ def _rossler(ref: Path) -> None:
 
 
 def main() -> None:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYBASIN_REFERENCE")
+    if not src:
+        sys.exit("usage: make_golden.py <reference tree> (or set PYBASIN_REFERENCE)")
+    ref = Path(src)
     _install_stubs()
     sys.path.insert(0, str(ref / "src"))
     it = ref / "tests" / "integration"

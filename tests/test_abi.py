@@ -87,3 +87,20 @@ def test_occupancy_query_needs_a_device_or_reports_error():
     rc = lib.pb_query_occupancy(L.SYS_DUFFING, 2, L.PREC_MIXED, L.SCHED_QUEUE, 128, ctypes.byref(bps), ctypes.byref(sms))
     assert rc in (L.PB_SUCCESS, L.PB_ECUDA)
     assert lib.pb_query_occupancy(99, 2, 0, 0, 128, None, None) == L.PB_EINVALID_ODE
+
+
+def test_scratch_size_and_noalloc_bound_the_feature_count_first():
+    """A feature count beyond the fixed arrays of pb_solve_args is refused before the
+    scratch layout walks those arrays (no GPU involved)."""
+    lib = L.load()
+    a = L.SolveArgs()
+    a.dim = 2
+    a.n_traj = 4
+    a.n_ic = 4
+    a.n_save = 8
+    a.n_features = L.MAX_FEATURES + 1
+    assert lib.pb_solve_scratch_bytes(ctypes.byref(a)) == -1
+    assert lib.pb_solve_batch_noalloc(ctypes.byref(a), None) == L.PB_EINVAL
+    a.n_features = -1
+    assert lib.pb_solve_scratch_bytes(ctypes.byref(a)) == -1
+    assert lib.pb_solve_batch_noalloc(ctypes.byref(a), None) == L.PB_EINVAL

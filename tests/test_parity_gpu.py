@@ -762,6 +762,45 @@ def test_entropy_and_complexity_features_on_identical_windows(n_save):
     assert (g[:, 4] > 0).all() and (g[:, 0] > 0).all()
 
 
+@pytest.mark.parametrize("n_save", [3001, 4800])
+def test_pair_count_features_on_long_windows(n_save):
+    """correlation_dimension and lyapunov_r are O(n^2) per column (all pairs of
+    delay vectors; every vector's nearest neighbour): on windows of a few thousand
+    samples, a handful of trajectories, against the oracle on the kernel's own FP32
+    window, with the symbolic pass's time per (trajectory, column) printed."""
+    y0 = seeded_ics(DUFFING, 6, seed=31).double().numpy()
+    save = np.linspace(0.0, 160.0, n_save)
+    wb = n_save // 10
+    feats = [(0, L.FEAT_CORR_DIM, 4.0, 2 * 1024 + 50.0), (1, L.FEAT_CORR_DIM, 2.0, 1 * 1024 + 20.0),
+             (0, L.FEAT_LYAP_R, 10 * 1024 + 20.0, 1.0), (1, L.FEAT_LYAP_R, 4 * 1024 + 10.0, 2.0)]
+    got = gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 160.0), 1e-8, 1e-10,
+                    win_begin=wb, features=feats, keep_full=True)
+    assert (got["status"] == 0).all()
+    win = got["y"][wb:].astype(np.float32).astype(np.float64)
+    want = np.array([[O.window_feature(f[1], f[2], win[:, j, f[0]], f[3]) for f in feats] for j in range(len(y0))])
+    g = got["features"]
+    for c, f in enumerate(feats):
+        if f[1] == L.FEAT_LYAP_R:
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-5, atol=1e-7, err_msg=f"col {c} {f}")
+        else:
+            np.testing.assert_allclose(g[:, c], want[:, c], rtol=1e-9, atol=1e-12, err_msg=f"col {c} {f}")
+    # cost of the pass: the same solve with and without the pair-count columns
+    def timed(columns):
+        ts = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            gpu_solve(O.SYS_DUFFING, y0, np.array([DUFFING.params]), save, (0.0, 160.0), 1e-8, 1e-10,
+                      win_begin=wb, features=columns)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
+    extra = timed(feats) - timed([(0, L.FEAT_MEDIAN, 0.0)])
+    print(f"pair-count pass, window {n_save - wb}: {extra / (len(y0) * len(feats)):.3f} ms per (trajectory, column)")
+
+
 def test_spectral_features_reject_oversized_windows():
     """The spectrum sits in shared memory: more than 16,384 window samples is refused."""
     save = np.linspace(0.0, 1.0, L.SPECTRAL_WINDOW_MAX + 1)

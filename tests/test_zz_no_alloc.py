@@ -24,7 +24,7 @@ from pybasin_b200.engine import FeatureColumn, SolveRequest, SolveResult, alloc_
 pytestmark = pytest.mark.gpu
 
 
-def _request(dev: torch.device, n: int) -> SolveRequest:
+def _request(dev: torch.device, n: int, schedule: int = L.SCHED_QUEUE) -> SolveRequest:
     torch.manual_seed(5)
     y0 = (torch.rand(n, 2) * torch.tensor([2.0, 1.5]) + torch.tensor([-1.0, -0.5])).to(dev)
     save = torch.linspace(900.0, 1000.0, 5000, dtype=torch.float32).double().to(dev)
@@ -47,7 +47,7 @@ def _request(dev: torch.device, n: int) -> SolveRequest:
         n_traj=n,
         columns=cols,
         precision=L.PREC_MIXED,
-        schedule=L.SCHED_QUEUE,
+        schedule=schedule,
         dense_mode=L.DENSE_DEFERRED,
         keep_steps=True,
     )
@@ -64,10 +64,14 @@ def _outputs(req: SolveRequest, dev: torch.device) -> SolveResult:
     )
 
 
-def test_noalloc_matches_allocating_entry_point_on_two_calls():
+# the queue schedule, and the probed one (probe phase, longest-first radix sort
+# whose temporary storage also lives in the fixed array, main phase with the
+# sampling drained into it)
+@pytest.mark.parametrize("schedule", [L.SCHED_QUEUE, L.SCHED_PROBED], ids=["queue", "probed"])
+def test_noalloc_matches_allocating_entry_point_on_two_calls(schedule):
     dev = torch.device("cuda:0")
     lib = L.load()
-    req = _request(dev, 256)
+    req = _request(dev, 256, schedule)
     stream = torch.cuda.current_stream(dev)
     s = ctypes.c_void_p(stream.cuda_stream)
 
