@@ -502,6 +502,62 @@ int pb_gate_summary(const int32_t* label, int64_t n, int32_t C, const int32_t* r
                     const int32_t* surrogate_label_of_routed, const int32_t* integrated, int64_t* counts,
                     int32_t* stats, void* stream);
 
+/* ---- surrogate training on the tensor cores (tcgen05) ----------------------
+ * No counterpart in the reference.  One minibatch step of the surrogate is
+ * forward GEMMs (PB_TRAIN_FWD_GELU, PB_TRAIN_FWD_LINEAR for the logits),
+ * pb_train_xent, input-gradient GEMMs (PB_TRAIN_DX) and weight-gradient GEMMs
+ * (PB_TRAIN_DW), then pb_train_adamw; nothing allocates, so a whole training
+ * run can be captured as one CUDA graph. */
+enum pb_train_mode {
+    PB_TRAIN_FWD_GELU = 0,   /* out_bf16 = GELU(A B^T + bias) (BF16), z_pre = A B^T + bias (FP32, optional) */
+    PB_TRAIN_FWD_LINEAR = 1, /* out_f32 = A B^T + bias (bias optional) */
+    PB_TRAIN_DX = 2,         /* out_bf16 = (A B^T) * GELU'(z_in); col_part (optional) per-warp column sums */
+    PB_TRAIN_DW = 3          /* out_f32 + z * M * ldc = A B^T over K chunk z (split-K partials); with
+                                col_part, col_part[z * ldp + m] = sum over the chunk of A(m, k) (the bias
+                                gradient partial: B gets a virtual row N of ones) */
+};
+/* C (M x N) = A (M x K) B^T with B given as (N x K): A(m,k) = A[m*sam + k*sak],
+ * B(n,k) = B[n*sbn + k*sbk] (BF16, device); each operand is contiguous along K
+ * (sak = 1 / sbk = 1) or along its rows (sam = 1 / sbn = 1; slower: staged by
+ * scattered shared-memory stores).  out_t (optional, BF16 modes) receives the BF16
+ * output transposed, out_t[n * ldt + m], so that a following weight-gradient GEMM
+ * reads it contiguous along K.  A CTA computes 128
+ * rows x bn columns over a K chunk of kc (bn, kc multiples of 16, <= 256) with
+ * tcgen05.mma, FP32 accumulators in tensor memory; the forward and input-gradient
+ * modes need kc >= K.  Outputs have row stride ldc; col_part has row stride ldp
+ * and ceil(M / 128) * 4 rows for PB_TRAIN_DX, ceil(K / kc) rows for PB_TRAIN_DW.
+ * error_flag (device int32, optional) is set to 1 when a CTA gave up waiting
+ * for its MMAs. */
+int pb_train_gemm(const void* A, int64_t sam, int64_t sak, const void* B, int64_t sbn, int64_t sbk, int32_t M,
+                  int32_t N, int32_t K, int32_t mode, int32_t kc, int32_t bn, const float* bias, const float* z_in,
+                  int64_t ldz, float* out_f32, void* out_bf16, void* out_t, float* z_pre, float* col_part,
+                  int64_t ldc, int64_t ldt, int64_t ldp, int32_t* error_flag, void* stream);
+/* Softmax cross-entropy of logits (M x C, row stride ldl; C <= 32) against
+ * labels: dz = (softmax - onehot) * scale (BF16, row stride ldd; dz_t, optional,
+ * the same transposed: dz_t[c * ldt + m]); bias_part
+ * (optional) receives pb_train_xent_parts(M) rows of C column sums of dz;
+ * loss_sum and correct (optional) accumulate -log p[label] and argmax hits. */
+int pb_train_xent(const float* logits, int64_t ldl, const int32_t* labels, int32_t M, int32_t C, float scale,
+                  void* dz_bf16, int64_t ldd, void* dz_t, int64_t ldt, float* bias_part, float* loss_sum,
+                  int32_t* correct, void* stream);
+int pb_train_xent_parts(int32_t M);
+/* AdamW step `step` (>= 1) over n_tensors (<= 16) parameter tensors in one
+ * launch.  Tensor s: FP32 weights w[s] (n[s] = rows x cols[s], row-major),
+ * optional BF16 copy w_bf16[s] and transposed BF16 copy w_bf16_t[s] (cols x
+ * rows; w_bf16, w_bf16_t and cols may be NULL), moments m1[s], m2[s], and its
+ * gradient as n_parts[s] partials summed in order, partial p of element i at
+ * grad_parts[s][p * part_stride[s] + i]; weight_decay[s] per tensor.  The
+ * pointer arrays are host arrays. */
+int pb_train_adamw(int32_t n_tensors, float* const* w, void* const* w_bf16, void* const* w_bf16_t,
+                   const int64_t* cols, float* const* m1, float* const* m2, const float* const* grad_parts,
+                   const int64_t* n, const int64_t* part_stride, const int32_t* n_parts, const float* weight_decay,
+                   float lr, float beta1, float beta2, float eps, int32_t step, void* stream);
+/* out[k, :] = x[idx[k], :] (BF16 rows of `width`), out_t[c * n + k] = the same
+ * transposed (optional), labels_out[k] = labels[idx[k]] (optional), k < n: the
+ * shuffled copy of a training set for one epoch. */
+int pb_train_gather(const void* x_bf16, int32_t width, const int32_t* labels, const int32_t* idx, int64_t n,
+                    void* out_bf16, void* out_t, int32_t* labels_out, void* stream);
+
 /* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
 const char* pb_error_string(int32_t status);
 

@@ -140,10 +140,16 @@ class MLPSurrogate:
     ``d_in = d_raw + 2 n_freq``."""
 
     def __init__(self, d_raw: int, n_classes: int, hidden: int = 256, depth: int = 4, seed: int = 0,
-                 device: torch.device | str = "cuda", n_freq: int = 0, freq_scale: float = 0.3):
+                 device: torch.device | str = "cuda", n_freq: int = 0, freq_scale: float = 0.3,
+                 pad_inputs: bool = False):
         self.dev = torch.device(device)
         self.d_raw, self.n_freq = d_raw, n_freq
         d_in = d_raw + 2 * n_freq
+        # with pad_inputs, input rows are zero padded to a multiple of 8 columns (16-byte
+        # rows for the tensor-core training kernels); the padded columns' weights are 0
+        self.d_used = d_in
+        if pad_inputs:
+            d_in = -(-d_in // 8) * 8
         self.d_in, self.n_classes, self.hidden, self.depth = d_in, n_classes, hidden, depth
         rng = np.random.default_rng(seed)
         self.freq = torch.tensor(rng.normal(0.0, freq_scale, (max(n_freq, 1), d_raw)), dtype=torch.float32,
@@ -152,9 +158,12 @@ class MLPSurrogate:
         self.W: list[torch.Tensor] = []
         self.b: list[torch.Tensor] = []
         for fan_in, fan_out in zip(dims[:-1], dims[1:]):
-            bound = 1.0 / np.sqrt(fan_in)  # torch.nn.Linear's default uniform bound
-            self.W.append(torch.tensor(rng.uniform(-bound, bound, (fan_out, fan_in)), dtype=torch.float32,
-                                       device=self.dev))
+            # torch.nn.Linear's default uniform bound (over the unpadded inputs)
+            bound = 1.0 / np.sqrt(self.d_used if not self.W else fan_in)
+            w = rng.uniform(-bound, bound, (fan_out, fan_in))
+            if len(self.W) == 0:
+                w[:, self.d_used:] = 0.0  # weights of the zero padding columns
+            self.W.append(torch.tensor(w, dtype=torch.float32, device=self.dev))
             self.b.append(torch.tensor(rng.uniform(-bound, bound, fan_out), dtype=torch.float32, device=self.dev))
         self.Wb = [w.to(torch.bfloat16) for w in self.W]
         self.shift = torch.zeros(d_raw, dtype=torch.float32, device=self.dev)
@@ -353,8 +362,9 @@ class MLPSurrogate:
 
     def fold_temperature(self, T: float) -> None:
         """Divide the logits by T (folded into the last layer's weights and bias)."""
-        self.W[-1] = (self.W[-1] / T).contiguous()
-        self.b[-1] = (self.b[-1] / T).contiguous()
-        self.Wb[-1] = self.W[-1].to(torch.bfloat16)
+        # in place: a captured training graph keeps pointing at these tensors
+        self.W[-1].div_(T)
+        self.b[-1].div_(T)
+        self.Wb[-1].copy_(self.W[-1])
         self._adam = None  # the optimiser state no longer matches the weights
         self._step += 1  # repack the tensor-core weights

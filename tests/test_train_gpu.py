@@ -1,0 +1,147 @@
+"""Surrogate training on the tensor cores (pb_train_*) against the FP64 oracle.
+
+Tolerances: BF16 operands carry 8 mantissa bits, so each GEMM is compared with
+the FP64 product of the *same* BF16-rounded operands at 1e-4 of the output's
+scale (FP32 accumulation only); end-to-end gradients (which also round dZ and
+the activations to BF16) at 3e-2 of the largest gradient entry, as for the
+mma.sync training kernels.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_oracle as MO
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def _bf16(a: np.ndarray) -> np.ndarray:
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(torch.float64).numpy()
+
+
+def _dev_bf16(a: np.ndarray) -> torch.Tensor:
+    return torch.tensor(a, dtype=torch.float32, device=DEV).to(torch.bfloat16).contiguous()
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 16, 16), (130, 6, 136), (256, 256, 256), (4096, 64, 200), (300, 136, 48)])
+def test_forward_modes_match_fp64(M, N, K):
+    from pybasin_b200.train import TRAIN_FWD_GELU, TRAIN_FWD_LINEAR, gemm_tc
+
+    rng = np.random.default_rng(M + 7 * N + K)
+    a, w = _bf16(rng.normal(size=(M, K))), _bf16(rng.normal(size=(N, K)))
+    bias = rng.normal(size=N).astype(np.float32)
+    A, W, b = _dev_bf16(a), _dev_bf16(w), torch.tensor(bias, device=DEV)
+    out = torch.full((M, N), float("nan"), dtype=torch.bfloat16, device=DEV)
+    zpre = torch.full((M, N), float("nan"), dtype=torch.float32, device=DEV)
+    lin = torch.full((M, N), float("nan"), dtype=torch.float32, device=DEV)
+    err = torch.zeros((1,), dtype=torch.int32, device=DEV)
+    gemm_tc(A, K, 1, W, K, 1, M, N, K, TRAIN_FWD_GELU, bias=b, out_bf16=out, z_pre=zpre, error=err)
+    gemm_tc(A, K, 1, W, K, 1, M, N, K, TRAIN_FWD_LINEAR, bias=b, out_f32=lin, error=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    z = a @ w.T + bias
+    scale = np.abs(z).max()
+    np.testing.assert_allclose(zpre.cpu().numpy(), z, rtol=0, atol=1e-4 * scale)
+    np.testing.assert_allclose(lin.cpu().numpy(), z, rtol=0, atol=1e-4 * scale)
+    g = MO.gelu(z)
+    np.testing.assert_allclose(out.float().cpu().numpy(), g, rtol=1e-2, atol=1e-4 * scale)
+
+
+@pytest.mark.parametrize("M,N,K", [(200, 136, 256), (4096, 256, 256), (64, 256, 6)])
+def test_input_gradient_mode_matches_fp64(M, N, K):
+    """dZ_below = (dZ W) * GELU'(Z_below) with W read transposed (contiguous along N),
+    and the per-warp column sums of dZ_below."""
+    from pybasin_b200.train import TRAIN_DX, gemm_tc
+
+    rng = np.random.default_rng(M + N + 3 * K)
+    dz, w = _bf16(rng.normal(size=(M, K))), _bf16(rng.normal(size=(K, N)))  # W is (K x N): dZ (M x K) @ W
+    z_below = rng.normal(size=(M, N)).astype(np.float32)
+    out = torch.full((M, N), float("nan"), dtype=torch.bfloat16, device=DEV)
+    parts = torch.full((-(-M // 128) * 4, N), float("nan"), dtype=torch.float32, device=DEV)
+    # B(n, k) = W[k, n]: sbn = 1, sbk = N
+    gemm_tc(_dev_bf16(dz), K, 1, _dev_bf16(w), 1, N, M, N, K, TRAIN_DX, z_in=torch.tensor(z_below, device=DEV),
+            ldz=N, out_bf16=out, col_part=parts, ldc=N, ldp=N)
+    torch.cuda.synchronize()
+    want = (dz @ w) * MO.gelu_grad(z_below.astype(np.float64))
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(out.float().cpu().numpy(), want, rtol=1e-2, atol=2e-4 * scale)
+    np.testing.assert_allclose(parts.sum(0).cpu().numpy(), want.sum(0), rtol=0, atol=1e-4 * np.abs(want).sum(0).max())
+
+
+@pytest.mark.parametrize("M,N,K", [(256, 136, 4096), (6, 256, 1000), (256, 256, 300)])
+def test_weight_gradient_split_k_matches_fp64(M, N, K):
+    """dW = dZ^T X over the batch (K rows), both operands read along their rows, in
+    chunks of 256 rows whose partials sum to the product."""
+    from pybasin_b200.train import TRAIN_DW, gemm_tc
+
+    rng = np.random.default_rng(M * N + K)
+    dz, x = _bf16(rng.normal(size=(K, M))), _bf16(rng.normal(size=(K, N)))
+    splits = -(-K // 256)
+    part = torch.full((splits, M, N), float("nan"), dtype=torch.float32, device=DEV)
+    gemm_tc(_dev_bf16(dz), 1, M, _dev_bf16(x), 1, N, M, N, K, TRAIN_DW, out_f32=part, ldc=N)
+    # the same with the bias partials from the column of ones
+    part2 = torch.full((splits, M, N), float("nan"), dtype=torch.float32, device=DEV)
+    bpart = torch.full((splits, M), float("nan"), dtype=torch.float32, device=DEV)
+    gemm_tc(_dev_bf16(dz), 1, M, _dev_bf16(x), 1, N, M, N, K, TRAIN_DW, out_f32=part2, ldc=N, col_part=bpart, ldp=M)
+    torch.cuda.synchronize()
+    want = dz.T @ x
+    np.testing.assert_allclose(part.sum(0).cpu().numpy(), want, rtol=0, atol=1e-4 * np.abs(want).max())
+    assert torch.equal(part, part2)
+    np.testing.assert_allclose(bpart.sum(0).cpu().numpy(), dz.sum(0), rtol=0, atol=1e-4 * np.abs(dz).sum(0).max())
+
+
+def test_trainer_gradients_match_oracle():
+    from pybasin_b200.surrogate import MLPSurrogate
+    from pybasin_b200.train import GraphTrainer
+
+    net = MLPSurrogate(3, 6, hidden=64, depth=3, seed=1, device=DEV, n_freq=7, pad_inputs=True)
+    assert net.d_in == 24 and net.d_used == 17
+    rng = np.random.default_rng(2)
+    n = 700
+    x = np.zeros((n, net.d_in))
+    x[:, : net.d_used] = _bf16(rng.normal(size=(n, net.d_used)))
+    y = rng.integers(0, 6, n)
+    tr = GraphTrainer(net, n_rows=n, epochs=1, batch=n)
+    gW, gb = tr.gradients(_dev_bf16(x), torch.tensor(y, dtype=torch.int32))
+    torch.cuda.synchronize()
+    Ws = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
+    bs = [b.double().cpu().numpy() for b in net.b]
+    z, acts, pres = MO.forward(x, Ws, bs)
+    _, d = MO.loss_and_grad(z, y)
+    oW, ob = MO.backward(d, acts, pres, Ws)  # d is already the batch mean
+    for li in range(len(Ws)):
+        np.testing.assert_allclose(gW[li].cpu().numpy(), oW[li], rtol=0, atol=3e-2 * np.abs(oW[li]).max())
+        np.testing.assert_allclose(gb[li].cpu().numpy(), ob[li], rtol=0, atol=3e-2 * np.abs(ob[li]).max())
+    # the padding columns' weights get no gradient
+    assert float(gW[0][:, net.d_used :].abs().max()) == 0.0
+
+
+def test_graph_replay_equals_eager_run_and_learns():
+    """A captured run replays to bit-identical weights of an eager run (deterministic
+    partial sums), twice in a row from the reset weights, and it learns."""
+    from pybasin_b200.surrogate import MLPSurrogate
+    from pybasin_b200.train import GraphTrainer
+
+    g = torch.Generator().manual_seed(0)
+    pts = torch.rand(6000, 2, generator=g) * 2 - 1
+    y = ((pts[:, 0] > 0).int() + 2 * (pts[:, 0] ** 2 + pts[:, 1] ** 2 < 0.3).int()).to(torch.int32)
+    net = MLPSurrogate(2, 4, hidden=128, depth=3, seed=0, device=DEV, n_freq=16, pad_inputs=True)
+    net.fit_normalisation(pts.to(DEV))
+    xi = net.inputs(pts.to(DEV), None)
+    tr = GraphTrainer(net, n_rows=6000, epochs=12, batch=1024, lr=4e-3)
+    tr.train(xi, y.to(DEV), use_graph=False)
+    torch.cuda.synchronize()
+    eager = [w.clone() for w in net.W]
+    st = tr.stats()
+    assert st["error"] == 0 and st["accuracy"] > 0.85
+    for _ in range(2):
+        tr.train(use_graph=True)
+        torch.cuda.synchronize()
+        for a, b in zip(eager, net.W):
+            assert torch.equal(a, b)
+    acc = float((net.logits(xi).argmax(1).cpu() == y).float().mean())
+    assert acc > 0.97
