@@ -19,6 +19,7 @@ import torch
 from pybasin_b200 import _lib as L
 from pybasin_b200.pipeline import BasinStabilityPipeline, to_host_pinned
 from pybasin_b200.surrogate import MLPSurrogate, TrainHistory, _bind, _p
+from pybasin_b200.train import GraphTrainer
 
 
 class GateStats:
@@ -57,13 +58,17 @@ class GateStats:
     def audit_error(self) -> float:
         return self.audit_disagree / max(self.audit_confident, 1)
 
-    @property
-    def routed_fraction(self) -> float:
-        return self.n_routed / max(self.n, 1)
 
-    @property
-    def audit_error(self) -> float:
-        return self.audit_disagree / max(self.audit_confident, 1)
+def calibrate_temperature_device(logits: torch.Tensor, labels: torch.Tensor, lo: float = 0.5, hi: float = 4.0,
+                                 steps: int = 71) -> torch.Tensor:
+    """The temperature of :func:`calibrate_temperature`, computed on the device
+    (a 0-d tensor; nothing waits for it): the grid point over [lo, hi] minimising the
+    mean negative log-likelihood of ``labels`` under ``logits / T``."""
+    grid = torch.linspace(lo, hi, steps, device=logits.device, dtype=torch.float64)
+    z = logits.to(torch.float64)[None] / grid[:, None, None]
+    lab = labels.to(torch.int64)
+    nll = torch.logsumexp(z, dim=2) - z.gather(2, lab[None, :, None].expand(steps, -1, 1))[..., 0]
+    return grid[torch.argmin(nll.mean(dim=1))].to(torch.float32)
 
 
 def calibrate_temperature(logits: np.ndarray, labels: np.ndarray, grid: np.ndarray | None = None) -> float:
@@ -81,6 +86,30 @@ def calibrate_temperature(logits: np.ndarray, labels: np.ndarray, grid: np.ndarr
     return best_t
 
 
+class FitInfo:
+    """What one :meth:`SurrogateGatedPipeline.fit` did; reading it waits for the device."""
+
+    def __init__(self, trainers: list, n_train: int, n_calibration: int, owner: "SurrogateGatedPipeline"):
+        self.trainers = trainers
+        self.n_train = n_train
+        self.n_calibration = n_calibration
+        self._owner = owner
+
+    @property
+    def temperature(self) -> float:
+        T = getattr(self._owner, "_temperature_dev", None)
+        return 1.0 if T is None else float(T.item())
+
+    def summary(self) -> dict:
+        st = [t.stats() for t in self.trainers]
+        return {"n_train": self.n_train, "n_calibration": self.n_calibration, "temperature": self.temperature,
+                "train_accuracy": st[-1]["accuracy"], "train_error_flag": max(x["error"] for x in st),
+                "train_steps": sum(t.steps for t in self.trainers),
+                "train_launches": sum(t.launches for t in self.trainers),
+                "train_flop": sum(t.flops() for t in self.trainers),
+                "graph_capture_s": sum(t.capture_s for t in self.trainers)}
+
+
 class SurrogateGatedPipeline:
     """Surrogate in front of a ``BasinStabilityPipeline`` for one ODE system and parameter row."""
 
@@ -96,14 +125,17 @@ class SurrogateGatedPipeline:
         n_freq: int = 64,
         freq_scale: float = 0.3,
         calib_fraction: float = 0.1,
+        max_chunk: int = 1 << 20,
     ):
         self.pipe = pipeline
+        self.max_chunk = max_chunk
         self.dev = pipeline.dev
         self.params = pipeline.params[0].to(torch.float64)  # the main parameter row
         self.S = pipeline.dim
         self.C = pipeline.n_classes + 1  # + unbounded
         self.net = MLPSurrogate(self.S + self.params.numel(), self.C, hidden=hidden, depth=depth, seed=seed,
-                                device=self.dev, n_freq=n_freq, freq_scale=freq_scale)
+                                device=self.dev, n_freq=n_freq, freq_scale=freq_scale, pad_inputs=True)
+        self._trainers: dict[tuple, GraphTrainer] = {}
         self.calib_fraction = calib_fraction
         self.temperature = 1.0
         self.threshold = threshold
@@ -144,6 +176,71 @@ class SurrogateGatedPipeline:
         return hist, {"label_s": t1 - t0, "train_s": t2 - t1, "n_train": int(n - n_cal), "n_calibration": n_cal,
                       "temperature": self.temperature}
 
+    def _trainer(self, n_rows: int, epochs: int, batch: int, lr: float, resume: bool, seed: int) -> GraphTrainer:
+        key = (n_rows, epochs, batch, lr, resume, seed)
+        tr = self._trainers.get(key)
+        if tr is None:
+            tr = GraphTrainer(self.net, n_rows=n_rows, epochs=epochs, batch=batch, lr=lr, seed=seed, resume=resume)
+            self._trainers[key] = tr
+        return tr
+
+    def fit(self, y0_random: torch.Tensor, y0_pool: torch.Tensor | None = None, n_active: int = 0,
+            epochs: int = 40, batch: int = 4096, lr: float = 5e-3, seed: int = 0) -> "FitInfo":
+        """Train the surrogate on labels of the integrator, on the tensor cores
+        (``GraphTrainer``: one captured CUDA graph per training run), without a host
+        round trip: every step is queued on the current stream.
+
+        The first ``calib_fraction`` of ``y0_random`` (device ICs) is held out for
+        calibration, the rest is labelled by the integrator and trained on.  With
+        ``n_active`` > 0 that first run takes ``epochs // 2`` epochs; then the
+        ``n_active`` ICs of ``y0_pool`` the network is least confident about
+        (labels where the basins interleave) are labelled too, and training resumes
+        on both sets for ``epochs`` epochs.  Last, the softmax temperature minimising
+        the held-out negative log-likelihood is folded into the last layer, so the
+        gate's threshold reads as a probability of the label being right."""
+        lib = L.load()
+        _bind(lib)
+        s = torch.cuda.current_stream(self.dev).cuda_stream
+        net = self.net
+        n = y0_random.shape[0]
+        n_cal = int(n * self.calib_fraction) if n >= 100 else 0
+        labels, _ = self.pipe.run_device(y0_random)
+        lab = labels.clone()
+        fit_ic, fit_lab = y0_random[n_cal:], lab[n_cal:]
+        net.fit_normalisation(self._raw_inputs(fit_ic))
+        x_r = net.inputs(fit_ic, self.params)
+        active = n_active > 0 and y0_pool is not None
+        tr1 = self._trainer(n - n_cal, max(epochs // 2, 1) if active else epochs, batch, lr, False, seed)
+        tr1.train(x_r, fit_lab)
+        trainers = [tr1]
+        if active:
+            m = y0_pool.shape[0]
+            logits = net.logits(net.inputs(y0_pool, self.params))
+            label = torch.empty((m,), dtype=torch.int32, device=self.dev)
+            conf = torch.empty((m,), dtype=torch.float32, device=self.dev)
+            route = torch.empty((m,), dtype=torch.int32, device=self.dev)
+            n_route = torch.empty((1,), dtype=torch.int32, device=self.dev)
+            # threshold 0: nothing routed, only the confidences wanted
+            L.check(lib.pb_surrogate_gate(_p(logits), m, self.C, 0.0, None, _p(label), _p(conf), _p(route),
+                                          _p(n_route), s), "pb_surrogate_gate")
+            pick = torch.topk(conf, min(n_active, m), largest=False).indices
+            y0_act = y0_pool.index_select(0, pick).contiguous()
+            lab_a, _ = self.pipe.run_device(y0_act)
+            x_all = torch.cat([x_r, net.inputs(y0_act, self.params)])
+            lab_all = torch.cat([fit_lab, lab_a])
+            tr2 = self._trainer(x_all.shape[0], epochs, batch, lr, True, seed + 1)
+            tr2.train(x_all, lab_all)
+            trainers.append(tr2)
+        if n_cal > 0:
+            z = net.logits(net.inputs(y0_random[:n_cal], self.params))
+            T = calibrate_temperature_device(z, lab[:n_cal])
+            net.W[-1].div_(T)
+            net.b[-1].div_(T)
+            net.Wb[-1].copy_(net.W[-1])
+            net._step += 1  # repack the inference weights
+            self._temperature_dev = T
+        return FitInfo(trainers, n - n_cal + (n_active if active else 0), n_cal, self)
+
     # -- inference -------------------------------------------------------------------
     def audit_mask(self, n: int) -> torch.Tensor:
         m = self._audit.get(n)
@@ -173,7 +270,17 @@ class SurrogateGatedPipeline:
             routed = torch.empty((k, self.S), dtype=torch.float32, device=self.dev)
             L.check(lib.pb_gather_rows(_p(y0.contiguous()), self.S, _p(route), _p(n_route), k, _p(routed), s),
                     "pb_gather_rows")
-            integ, _ = self.pipe.run_device(routed)
+            # integrated in chunks of at most max_chunk ICs: the deferred dense output's
+            # step records are sized per trajectory (1024 records of 48 B for one FP32
+            # state), so a chunk bounds the scratch (1M ICs: 48 GiB)
+            if k <= self.max_chunk:
+                integ, _ = self.pipe.run_device(routed)
+            else:
+                integ = torch.empty((k,), dtype=torch.int32, device=self.dev)
+                for c0 in range(0, k, self.max_chunk):
+                    c1 = min(k, c0 + self.max_chunk)
+                    lab_c, _ = self.pipe.run_device(routed[c0:c1])
+                    integ[c0:c1].copy_(lab_c)
             sur_of_routed = torch.empty((k,), dtype=torch.int32, device=self.dev)
             L.check(lib.pb_merge_labels(_p(integ), _p(route), _p(n_route), k, _p(label), _p(sur_of_routed), s),
                     "pb_merge_labels")

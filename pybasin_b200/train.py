@@ -92,10 +92,13 @@ class GraphTrainer:
 
     def __init__(self, net: MLPSurrogate, n_rows: int, epochs: int, batch: int = 4096, lr: float = 4e-3,
                  weight_decay: float = 1e-4, seed: int = 0, betas: tuple[float, float] = (0.9, 0.999),
-                 eps: float = 1e-8):
+                 eps: float = 1e-8, resume: bool = False):
+        """With ``resume``, a run starts from the net's current weights (fresh AdamW
+        moments) instead of the weights it had when the trainer was built."""
         if net.d_in % 8:
             raise ValueError("GraphTrainer needs input rows of a multiple of 8 columns (MLPSurrogate(pad_inputs=True))")
         self.net = net
+        self.resume = resume
         self.dev = net.dev
         self.n, self.epochs, self.batch = n_rows, epochs, min(batch, n_rows)
         self.lr, self.wd, self.betas, self.eps = lr, weight_decay, betas, eps
@@ -120,7 +123,12 @@ class GraphTrainer:
         self.actT = [None] + [torch.zeros((self.dims[l + 1], B), dtype=torch.bfloat16, device=dev)
                               for l in range(L_ - 1)]
         self.dzT = [torch.zeros((self.dims[l + 1], B), dtype=torch.bfloat16, device=dev) for l in range(L_)]
-        self.WbT = [w.t().contiguous() for w in net.Wb]
+        # the transposed BF16 weights live on the net, shared by its trainers (a resumed
+        # run reads the ones the previous run's optimiser wrote)
+        if getattr(net, "WbT", None) is None or [tuple(w.shape) for w in net.WbT] != \
+                [tuple(w.shape[::-1]) for w in net.Wb]:
+            net.WbT = [w.t().contiguous() for w in net.Wb]
+        self.WbT = net.WbT
         splits = -(-B // KC)
         self.gw_part = [torch.zeros((splits,) + tuple(w.shape), dtype=torch.float32, device=dev) for w in net.W]
         # bias gradients come out of the weight-gradient GEMMs (a column of ones), one
@@ -142,12 +150,13 @@ class GraphTrainer:
 
     # -- one run, as launched (captured once) ------------------------------------------
     def _reset(self) -> None:
-        for p, p0 in zip(self.params, self.init):
-            p.copy_(p0)
-        for w, w0 in zip(self.net.Wb, self.init_bf16):
-            w.copy_(w0)
-        for w, w0 in zip(self.WbT, self.init_bf16_t):
-            w.copy_(w0)
+        if not self.resume:
+            for p, p0 in zip(self.params, self.init):
+                p.copy_(p0)
+            for w, w0 in zip(self.net.Wb, self.init_bf16):
+                w.copy_(w0)
+            for w, w0 in zip(self.WbT, self.init_bf16_t):
+                w.copy_(w0)
         for m in self.m1 + self.m2:
             m.zero_()
         self.loss.zero_()

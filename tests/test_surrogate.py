@@ -301,3 +301,62 @@ def test_gate_summary_counts_without_routed_rows():
                                _p(tally), s) != 0
     assert lib.pb_gate_summary(_p(label), 10, 6, _p(label), None, 10, None, None, 0.95, None, None, _p(counts),
                                _p(tally), s) != 0
+
+
+def test_device_temperature_calibration_equals_the_host_one():
+    """The on-device grid search (torch tensors, here on the CPU) picks the same
+    temperature as the NumPy one."""
+    from pybasin_b200.gated import calibrate_temperature, calibrate_temperature_device
+
+    rng = np.random.default_rng(6)
+    z = rng.normal(0.0, 3.0, (5000, 6))
+    p = np.exp(z / 1.5 - (z / 1.5).max(axis=1, keepdims=True))
+    p /= p.sum(axis=1, keepdims=True)
+    labels = np.array([rng.choice(6, p=row) for row in p])
+    want = calibrate_temperature(z, labels)
+    got = float(calibrate_temperature_device(torch.tensor(z, dtype=torch.float32), torch.tensor(labels)))
+    assert abs(got - want) < 1e-6
+
+
+@pytest.mark.gpu
+def test_active_fit_on_the_tensor_cores_gates_duffing_within_delta_bs():
+    """fit(): integrator labels of random ICs, a first training run on the tensor
+    cores, the least confident ICs of a pool labelled and trained on too, the
+    temperature folded in, all queued without a host round trip; then the gated
+    pass against the integrator on fresh ICs.  Two fits in a row end in the same
+    weights (captured runs replay deterministically)."""
+    from pybasin_b200 import B200Dopri5Solver, DuffingODE, FusedFeatureExtractor
+    from pybasin_b200.gated import SurrogateGatedPipeline
+    from pybasin_b200.pipeline import BasinStabilityPipeline
+
+    dev = torch.device("cuda:0")
+    fx = FusedFeatureExtractor(time_steady=900.0, features=None,
+                               features_per_state={0: {"maximum": None, "standard_deviation": None}}, normalize=False)
+    solver = B200Dopri5Solver(t_span=(0, 1000), t_steps=5000, t_eval=(900, 1000), device="cuda:0", precision="mixed",
+                              feature_extractor=fx)
+    tpl = [[-0.21, 0.02], [1.05, 0.77], [-0.67, 0.02], [-0.46, 0.30], [-0.43, 0.12]]
+    pipe = BasinStabilityPipeline(DuffingODE({"delta": 0.08, "k3": 1.0, "A": 0.2}), solver, tpl,
+                                  ["y1", "y2", "y3", "y4", "y5"], device=dev)
+    gated = SurrogateGatedPipeline(pipe, hidden=128, depth=3, threshold=0.95, freq_scale=0.6)
+
+    def ics(n, seed):
+        torch.manual_seed(seed)
+        return (torch.rand(n, 2) * torch.tensor([2.0, 1.5]) + torch.tensor([-1.0, -0.5])).to(dev)
+
+    weights = []
+    for _ in range(2):
+        info = gated.fit(ics(12000, 1), ics(60000, 3), n_active=6000, epochs=16, batch=2048)
+        torch.cuda.synchronize()
+        weights.append([w.clone() for w in gated.net.W])
+    s = info.summary()
+    assert s["train_error_flag"] == 0 and s["n_train"] == 10800 + 6000 and s["n_calibration"] == 1200
+    assert 0.5 <= s["temperature"] <= 4.0
+    assert all(torch.equal(a, b) for a, b in zip(*weights))
+    y0 = ics(20000, 2)
+    ref = pipe.run_device(y0)[0].clone()
+    label, counts, stats = gated.run_device(y0)
+    torch.cuda.synchronize()
+    assert stats.n_routed < 0.6 * stats.n
+    dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
+    assert float(dbs) <= 0.005
+    assert float((label == ref).double().mean()) >= 0.99
