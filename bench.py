@@ -191,12 +191,16 @@ def cpu_sample_size(threads: int, target_s: float) -> tuple[int, float]:
 
 
 def run_reference_arm(args) -> None:
+    """The CPU path on the host cores: the FP64 oracle port of the reference's native
+    Dopri5 (OpenMP over the ICs) + the reference's 1-NN, on a bounded sample of the
+    same seeded ICs the B200 arm labels (the first of them, up to 10^5 per step)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    n, _ = cpu_sample_size(threads, 3.0)
-    y0 = seeded_ics(n, 42).double().numpy()
+    n, _ = cpu_sample_size(threads, 4.0)
+    surrogate = args.c5_n > 0 and not args.no_surrogate
+    y0 = (seeded_ics(args.c5_n, 7)[:n] if surrogate else seeded_ics(args.n, 42)[:n]).double().numpy()
     for _ in range(args.warmup):
         cpu_reference_pass(y0[: max(n // 16, 64)], threads)
     times = []
@@ -205,8 +209,9 @@ def run_reference_arm(args) -> None:
         times.append(dt)
     ms = 1000.0 * statistics.mean(times)
     value = n / (ms / 1000.0)
+    total = args.c5_n if surrogate else args.n
     line = {
-        "metric": "labelled ICs/sec (Duffing, |dBS|<=0.005 vs FP64)",
+        "metric": "labelled ICs/sec at |dBS|<=0.005 vs FP64 (fused FP32 + surrogate vs plain Dopri5)",
         "value": value,
         "unit": "ICs/s",
         "n_gpus": args.gpus,
@@ -219,15 +224,16 @@ def run_reference_arm(args) -> None:
         "dtype": "f64",
         "data": "synthetic (seeded uniform ICs, reference sampler)",
         "impl": "reference",
-        "config": {"workload": f"duffing forced, N={n} per pass (bounded sample of N=100000), t=[0,1000], "
-                               "window [900,1000] x 5000 saves, rtol 1e-8 atol 1e-6, 1-NN on 5 templates",
-                   "n_ic": n},
+        "config": {"workload": f"duffing forced, the first {n} of the {total} seeded ICs of the B200 arm per "
+                               "step (a bounded sample), t=[0,1000], window [900,1000] x 5000 saves, rtol 1e-8 "
+                               "atol 1e-6, 1-NN on 5 templates",
+                   "n_ic": n, "same_ics": True},
         "cpu_baseline": {
             "value": value,
             "unit": "ICs/s",
             "cores": threads,
             "kind": "port",
-            "sample": f"{n} seeded Duffing ICs per pass; FP64 oracle (restatement of the reference's native "
+            "sample": f"{n} seeded Duffing ICs per step; FP64 oracle (restatement of the reference's native "
                       "Dopri5, src/zigode/src/solver/dopri5_generic.zig) on OpenMP threads + sklearn 1-NN",
         },
         "e2e": {"value": value, "unit": "ICs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -372,6 +378,187 @@ def global_counts(counts: torch.Tensor, dist_on: bool) -> torch.Tensor:
     return reduce_counts(counts[0]) if dist_on else counts[0].clone()
 
 
+# The learned-surrogate workload: 10^7 seeded Duffing ICs, the surrogate trained
+# inside every timed step on 50,000 integrator labels (25,000 random + 25,000 chosen
+# as the least confident of a 500,000-IC pool; 10 % of the random ones held out for
+# calibration), gate 0.95, 1 % audit (default_rng(123)).
+C5_N = 10_000_000
+C5_RANDOM = 27_778
+C5_ACTIVE = 25_000
+C5_POOL = 500_000
+C5_EPOCHS = 40
+C5_BATCH = 4096
+C5_LR = 5e-3
+C5_FREQ_SCALE = 0.6
+FP64_CHUNK = 500_000  # plain FP64 kernel over 10^7 ICs: chunks bound its step-record scratch
+
+
+def chunked_labels(pipe, y0: torch.Tensor, chunk: int) -> tuple[torch.Tensor, torch.Tensor, int]:
+    """Labels and per-class counts of ``pipe`` over ``y0`` in chunks (the pipeline's
+    scratch scales with the chunk); returns the launches of this library too."""
+    n = y0.shape[0]
+    labels = torch.empty((n,), dtype=torch.int32, device=y0.device)
+    counts = torch.zeros((pipe.n_classes + 1,), dtype=torch.int64, device=y0.device)
+    launches = 0
+    for c0 in range(0, n, chunk):
+        lab, cnt = pipe.run_device(y0[c0 : c0 + chunk])
+        labels[c0 : c0 + lab.shape[0]].copy_(lab)
+        counts += cnt[0]
+        launches += pipe.kernel_launches_per_pass()
+    return labels, counts, launches
+
+
+def event_ms(fn, steps: int, flush: torch.Tensor | None = None, clk=None) -> list[float]:
+    """CUDA-event time of ``fn`` per step (L2 flushed before each step)."""
+    out = []
+    window = clk.timed() if clk is not None else contextlib.nullcontext()
+    with window:
+        for i in range(steps):
+            if flush is not None:
+                flush.fill_(i)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+    return out
+
+
+def run_surrogate_workload(args, dev, rank: int, world: int, dist_on: bool, flush: torch.Tensor, clk,
+                           pipe) -> dict:
+    """The surrogate workload at 10^7 ICs with training counted in every step."""
+    from pybasin_b200.gated import SurrogateGatedPipeline
+
+    n = args.c5_n
+    y0_host = seeded_ics(n, 7 + rank)
+    yr_host = seeded_ics(C5_RANDOM, 1042 + rank)
+    pool_host = seeded_ics(C5_POOL, 2042 + rank)
+    y0, yr, pool = y0_host.to(dev), yr_host.to(dev), pool_host.to(dev)
+    gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01,
+                                   freq_scale=C5_FREQ_SCALE)
+    state = {}
+
+    def step_device():
+        state["info"] = gated.fit(yr, pool, n_active=C5_ACTIVE, epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR)
+        state["label"], state["counts"], state["stats"] = gated.run_device(y0)
+
+    t0 = time.perf_counter()
+    for _ in range(max(args.warmup, 1)):
+        step_device()  # the first one captures the two training graphs
+    torch.cuda.synchronize()
+    warm_s = time.perf_counter() - t0
+    if dist_on:
+        torch.distributed.barrier()
+    times = event_ms(step_device, args.steps, flush, clk)
+    (ms,) = max_over_ranks([statistics.mean(times)], dev, dist_on)
+    st, info = state["stats"], state["info"]
+    counts = global_counts(state["counts"].view(1, -1), dist_on)
+    label = state["label"]
+    fit_summary = info.summary()
+
+    # phases of one step: training run times from the trainers' events, fit and run
+    for t in info.trainers:
+        t.timing = True
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    info2 = gated.fit(yr, pool, n_active=C5_ACTIVE, epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR)
+    e[1].record()
+    gated.run_device(y0)
+    e[2].record()
+    torch.cuda.synchronize()
+    train_ms = [t.run_ms() for t in info2.trainers]
+    for t in info.trainers:
+        t.timing = False
+    peak, peak_src = bf16_peak()
+    train_flop = fit_summary["train_flop"]
+    train_tflops = train_flop / (sum(train_ms) / 1000.0) / 1e12
+
+    # the plain FP64 kernel (the reference algorithm at the reference's tolerance) on
+    # all n ICs: the |dBS| reference and the denominator of the speed-up
+    pipe64 = make_pipeline(dev, "fp64", "plain")
+    chunked_labels(pipe64, y0[:FP64_CHUNK], FP64_CHUNK)
+    torch.cuda.synchronize()
+    res64 = {}
+
+    def fp64_pass():
+        res64["labels"], res64["counts"], _ = chunked_labels(pipe64, y0, FP64_CHUNK)
+
+    (ms64,) = max_over_ranks([statistics.mean(event_ms(fp64_pass, 1))], dev, dist_on)
+    counts64 = global_counts(res64["counts"].view(1, -1), dist_on)
+    n_all = n * world
+    dbs = (counts[:5].double() - counts64[:5].double()).abs().max().item() / n_all
+    agree = float((label == res64["labels"]).float().mean())
+    del pipe64
+    torch.cuda.empty_cache()
+
+    # the fused FP32 integrator alone on all n ICs (chunks of the gated pass's size)
+    res32 = {}
+
+    def fused_pass():
+        res32["labels"], res32["counts"], res32["launches"] = chunked_labels(pipe, y0, gated.max_chunk)
+
+    fused_pass()
+    torch.cuda.synchronize()
+    (ms32,) = max_over_ranks([statistics.mean(event_ms(fused_pass, 2, flush))], dev, dist_on)
+    counts32 = global_counts(res32["counts"].view(1, -1), dist_on)
+    dbs32 = (counts32[:5].double() - counts64[:5].double()).abs().max().item() / n_all
+
+    # end to end through the public API: host ICs in (the training sets too), labels out
+    y0_pinned, yr_pinned, pool_pinned = y0_host.pin_memory(), yr_host.pin_memory(), pool_host.pin_memory()
+
+    def step_e2e():
+        gated.fit(yr_pinned.to(dev, non_blocking=True), pool_pinned.to(dev, non_blocking=True), n_active=C5_ACTIVE,
+                  epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR)
+        gated.run(y0_pinned, names=False)
+
+    step_e2e()
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    (e2e_ms,) = max_over_ranks([statistics.mean(event_ms(step_e2e, args.steps, flush, clk))], dev, dist_on)
+
+    mlp_roof = mlp_roofline(gated, y0)
+    n_chunks = -(-st.n_routed // gated.max_chunk)
+    launches_step = (pipe.kernel_launches_per_pass() * (2 + n_chunks) + fit_summary["train_launches"] + 3 + 2
+                     + 3 + 3)
+    return {
+        "n_ic_per_gpu": n,
+        "value": n_all / (ms / 1000.0),
+        "ms_per_step": ms,
+        "fit_ms": e[0].elapsed_time(e[1]),
+        "gated_pass_ms": e[1].elapsed_time(e[2]),
+        "delta_bs_vs_fp64": dbs,
+        "label_agreement_vs_fp64": agree,
+        "routed_fraction": st.routed_fraction,
+        "audited": st.n_audited,
+        "audit_error_of_confident_labels": st.audit_error,
+        "threshold": 0.95,
+        "labels_for_training": {"random": C5_RANDOM - fit_summary["n_calibration"], "active": C5_ACTIVE,
+                                "calibration": fit_summary["n_calibration"], "pool": C5_POOL},
+        "train": {"epochs": C5_EPOCHS, "batch": C5_BATCH, "steps": fit_summary["train_steps"],
+                  "launches": fit_summary["train_launches"], "run_ms": train_ms,
+                  "accuracy": fit_summary["train_accuracy"], "temperature": fit_summary["temperature"],
+                  "error_flag": fit_summary["train_error_flag"],
+                  "roofline": {"bound": "tensor", "achieved": train_tflops, "peak": peak / 1e12, "unit": "TFLOP/s",
+                               "frac": train_tflops * 1e12 / peak, "flop": train_flop, "peak_source": peak_src},
+                  "graph_capture_s": fit_summary["graph_capture_s"], "warmup_s": warm_s},
+        "mlp_roofline": mlp_roof,
+        "plain_fp64": {"value": n_all / (ms64 / 1000.0), "ms_per_pass": ms64, "chunk": FP64_CHUNK,
+                       "rtol_atol": [DUFFING["rtol"], DUFFING["atol"]]},
+        "fused_fp32": {"value": n_all / (ms32 / 1000.0), "ms_per_pass": ms32, "delta_bs_vs_fp64": dbs32,
+                       "chunk": gated.max_chunk},
+        "speedup_vs_plain_fp64": {"with_training": ms64 / ms, "without_training": ms64 / e[1].elapsed_time(e[2]),
+                                  "fused_fp32_alone": ms64 / ms32},
+        "e2e": {"value": n_all / (e2e_ms / 1000.0), "unit": "ICs/s",
+                "h2d_bytes_per_step": int((n + C5_RANDOM + C5_POOL) * 2 * 4),
+                "d2h_bytes_per_step": int(n * 4 + (pipe.n_classes + 1) * 8),
+                "labels": "int32 class indices per IC and the per-class counts, in host memory; training ICs "
+                          "copied in from host memory as well"},
+        "gpu_launches_per_step": launches_step,
+    }
+
+
 def run_b200_arm(args) -> None:
     from pybasin_b200 import _lib as L
 
@@ -391,6 +578,7 @@ def run_b200_arm(args) -> None:
     y0_dev = y0_host.to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    # ---- the Duffing workload of the reference (10^5 ICs): fused integrator -------
     pipe = make_pipeline(dev, "mixed", "probed")
     pipe.run_device(y0_dev)
     torch.cuda.synchronize()
@@ -406,6 +594,16 @@ def run_b200_arm(args) -> None:
     steps_mixed = pipe.out.steps[:n].clone()
     value_fused = n * world / (ms / 1000.0)
 
+    # the same pass through the public API: pinned host ICs in, labels out
+    y0_pinned = y0_host.pin_memory()
+    run_fused = lambda: pipe.run(y0_pinned, use_graph=True, names=False)  # noqa: E731
+    for _ in range(2):
+        run_fused()
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    (e2e_fused_ms,) = max_over_ranks([statistics.mean(event_ms(run_fused, args.steps, flush, clk))], dev, dist_on)
+
     # plain FP64 kernel (the reference algorithm, one thread per trajectory) on the same ICs
     pipe64 = make_pipeline(dev, "fp64", "plain")
     pipe64.run_device(y0_dev)
@@ -417,66 +615,44 @@ def run_b200_arm(args) -> None:
     n_all = n * world
     agree = float((labels64 == labels_mixed).float().mean())
     dbs = (counts_mixed[:5].double() - counts64[:5].double()).abs().max().item() / n_all
+    del pipe64
+    torch.cuda.empty_cache()
 
-    # surrogate in front of the fused integrator: trained (untimed, reported) on
-    # 50,000 integrator labels of separately seeded ICs, then gated passes
+    # the surrogate at this size, trained inside every step too (informational: at
+    # 10^5 ICs the 50,000 training labels are half the work)
     from pybasin_b200.gated import SurrogateGatedPipeline
 
-    gated = None
+    small = None
     if not args.no_surrogate:
-        gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01)
-        hist, tinfo = gated.train(seeded_ics(50_000, 1042 + rank).to(dev), epochs=80, batch=512, lr=2e-3)
-        for _ in range(args.warmup):
-            gated.run_device(y0_dev)
+        gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01,
+                                       freq_scale=C5_FREQ_SCALE)
+        yr, pool = seeded_ics(C5_RANDOM, 1042 + rank).to(dev), seeded_ics(C5_POOL, 2042 + rank).to(dev)
+        box = {}
+
+        def fit_only():
+            box["info"] = gated.fit(yr, pool, n_active=C5_ACTIVE, epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR)
+
+        def gated_only():
+            box["out"] = gated.run_device(y0_dev)
+
+        for _ in range(2):
+            fit_only()
+            gated_only()
         torch.cuda.synchronize()
-        if dist_on:
-            torch.distributed.barrier()
-        g_times, g_stats = [], []
-        with clk.timed():
-            for i in range(args.steps):
-                flush.fill_(i)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                lab_g, cnt_g, st_g = gated.run_device(y0_dev)
-                e1.record()
-                torch.cuda.synchronize()
-                g_times.append(e0.elapsed_time(e1))
-                g_stats.append(st_g)
-        (ms_g,) = max_over_ranks([statistics.mean(g_times)], dev, dist_on)
+        (fit_ms,) = max_over_ranks([statistics.mean(event_ms(fit_only, max(1, min(args.steps, 3)), flush))], dev,
+                                   dist_on)
+        (gate_ms,) = max_over_ranks([statistics.mean(event_ms(gated_only, args.steps, flush))], dev, dist_on)
+        lab_g, cnt_g, st_g = box["out"]
         counts_g = global_counts(cnt_g.view(1, -1), dist_on)
-        dbs_g = (counts_g[:5].double() - counts64[:5].double()).abs().max().item() / n_all
-        agree_g = float((lab_g == labels64).float().mean())
-        value_gated = n_all / (ms_g / 1000.0)
-        mlp_roof = mlp_roofline(gated, y0_dev)
-
-    use_gate = gated is not None and dbs_g <= 0.005 and value_gated > value_fused
-    value = value_gated if use_gate else value_fused
-    ms_pass = ms_g if use_gate else ms
-
-    # end to end through the public API: pinned host ICs in, labels out
-    y0_pinned = y0_host.pin_memory()
-    # labels out as class indices (the class list alongside), the form a high-rate
-    # caller takes; run(..., names=True) adds one string object per IC on the host
-    run_e2e = ((lambda: gated.run(y0_pinned, names=False)) if use_gate
-               else (lambda: pipe.run(y0_pinned, use_graph=True, names=False)))
-    for _ in range(2):
-        run_e2e()
-    torch.cuda.synchronize()
-    if dist_on:
-        torch.distributed.barrier()
-    e2e_times = []
-    with clk.timed():
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            run_e2e()
-            e1.record()
-            torch.cuda.synchronize()
-            e2e_times.append(e0.elapsed_time(e1))
-    clk.__exit__(None, None, None)
-    (e2e_ms,) = max_over_ranks([statistics.mean(e2e_times)], dev, dist_on)
+        small = {
+            "inference_only": {"value": n_all / (gate_ms / 1000.0), "ms_per_step": gate_ms,
+                               "delta_bs_vs_fp64": (counts_g[:5].double() - counts64[:5].double()).abs().max().item()
+                               / n_all,
+                               "label_agreement_vs_fp64": float((lab_g == labels64).float().mean()),
+                               "routed_fraction": st_g.routed_fraction},
+            "with_training": {"value": n_all / ((gate_ms + fit_ms) / 1000.0), "ms_per_step": gate_ms + fit_ms,
+                              "fit_ms": fit_ms},
+        }
 
     # roofline of the integrator kernel: algorithmic FLOPs per launch / kernel time
     mean_steps = float(steps_mixed.double().mean())
@@ -485,6 +661,31 @@ def run_b200_arm(args) -> None:
     achieved = (n + len(DUFFING["templates"])) * flop_per_ic / (kms / 1000.0)
     peak32 = fma_peak(dev, L.PREC_MIXED)
     peak64 = fma_peak(dev, L.PREC_FP64)
+    roofline = {
+        "bound": "fp32-fma",
+        "achieved": achieved / 1e12,
+        "peak": peak32 / 1e12,
+        "unit": "TFLOP/s",
+        "frac": achieved / peak32,
+        "traffic": 1.6934e9 * (n + len(DUFFING["templates"])) / 50005,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel "
+                          "(main phase of the probed integrator) at N=50,000, scaled by trajectories: "
+                          "the window's step records, written by the integrating lanes and read back by the "
+                          "warps that drain the sampling into the same launch",
+        "note": "the fused integrator pass on 10^5 Duffing ICs; achieved counts the integration FLOPs only",
+        "peak_source": "FP32 FMA probe kernel measured in this run (the measured-peaks file holds only "
+                       "HBM-copy and bf16-GEMM peaks, neither of which bounds this kernel)",
+        "fp64_fma_peak": peak64 / 1e12,
+        "kernel_ms": kms,
+        "mean_steps_per_ic": mean_steps,
+        "flop_per_ic": flop_per_ic,
+    }
+
+    # ---- the learned-surrogate workload (10^7 ICs, training in every step) ----------
+    big = None
+    if not args.no_surrogate and args.c5_n > 0:
+        big = run_surrogate_workload(args, dev, rank, world, dist_on, flush, clk, pipe)
+    clk.__exit__(None, None, None)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -496,14 +697,45 @@ def run_b200_arm(args) -> None:
             "unit": "ICs/s",
             "cores": threads,
             "kind": "port",
-            "sample": f"{n_cpu} of the {n} seeded Duffing ICs; FP64 oracle (restatement of the reference's "
-                      "native Dopri5) at rtol 1e-8 atol 1e-6 on OpenMP threads + sklearn 1-NN",
+            "sample": f"{n_cpu} seeded Duffing ICs; FP64 oracle (restatement of the reference's native Dopri5) at "
+                      "rtol 1e-8 atol 1e-6 on OpenMP threads + sklearn 1-NN",
         }
     if dist_on:
         torch.distributed.barrier()
     if rank == 0:
+        duffing = {
+            "workload": f"duffing forced (delta 0.08, k3 1, A 0.2), N={n} ICs per GPU, t=[0,1000], window "
+                        "[900,1000] x 5000 saves, features max+std of x, 1-NN on 5 templates",
+            "fused_fp32": {"value": value_fused, "ms_per_step": ms, "delta_bs_vs_fp64": dbs,
+                           "label_agreement_vs_fp64": agree,
+                           "e2e": {"value": n_all / (e2e_fused_ms / 1000.0), "unit": "ICs/s",
+                                   "h2d_bytes_per_step": int(y0_host.numel() * 4),
+                                   "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8)}},
+            "plain_fp64": {"value": n_all / (ms64 / 1000.0), "ms_per_step": ms64,
+                           "kernel_ms": statistics.mean(kern64), "rtol_atol": [DUFFING["rtol"], DUFFING["atol"]]},
+            "speedup_fused_vs_plain_fp64": ms64 / ms,
+            "surrogate": small,
+        }
+        use_big = big is not None and big["delta_bs_vs_fp64"] <= 0.005
+        if use_big:
+            value, ms_pass, e2e = big["value"], big["ms_per_step"], big["e2e"]
+            workload = (f"learned surrogate: duffing forced, N={args.c5_n} seeded ICs per GPU, surrogate trained "
+                        f"in every step on {C5_RANDOM + C5_ACTIVE} integrator labels ({C5_ACTIVE} chosen "
+                        f"actively from a {C5_POOL}-IC pool), MLP 4 x 256 GELU bf16 on tcgen05, gate 0.95, "
+                        "1% audit; routed ICs on the fused FP32 integrator, t=[0,1000], window [900,1000] x "
+                        "5000 saves, 1-NN on 5 templates")
+            path = "surrogate (trained in the step) + fused FP32 integrator"
+            dbs_line, agree_line = big["delta_bs_vs_fp64"], big["label_agreement_vs_fp64"]
+            launches = big["gpu_launches_per_step"] * args.steps
+        else:
+            value, ms_pass = value_fused, ms
+            e2e = duffing["fused_fp32"]["e2e"]
+            workload = duffing["workload"]
+            path = "fused FP32 integrator"
+            dbs_line, agree_line = dbs, agree
+            launches = pipe.kernel_launches_per_pass() * args.steps
         line = {
-            "metric": "labelled ICs/sec (Duffing, |dBS|<=0.005 vs FP64)",
+            "metric": "labelled ICs/sec at |dBS|<=0.005 vs FP64 (fused FP32 + surrogate vs plain Dopri5)",
             "value": value,
             "unit": "ICs/s",
             "n_gpus": world,
@@ -516,74 +748,21 @@ def run_b200_arm(args) -> None:
             "dtype": "f32 stages / f64 time+error+control (surrogate: bf16 operands, f32 accumulate)",
             "data": "synthetic (seeded uniform ICs, reference sampler)",
             "config": {
-                "workload": "duffing forced (delta 0.08, k3 1, A 0.2), N=100000 ICs per GPU, t=[0,1000], "
-                            "window [900,1000] x 5000 saves, features max+std of x, 1-NN on 5 templates",
-                "n_ic_per_gpu": n,
+                "workload": workload,
+                "n_ic_per_gpu": args.c5_n if use_big else n,
                 "rtol_atol": list(pipe.solver.effective_tolerances()),
                 "schedule": "probed",
-                "l2": "flushed between timed steps (256 MB write)",
+                "l2": "flushed between timed steps (256 MB write); the inputs exceed the L2",
                 "parallelism": f"ic-shard x{world}",
             },
-            "path": "fused FP32 + surrogate gate" if use_gate else "fused FP32 integrator",
-            "delta_bs_vs_fp64": dbs_g if use_gate else dbs,
-            "label_agreement_vs_fp64": agree_g if use_gate else agree,
-            "fused_fp32": {"value": value_fused, "ms_per_step": ms, "delta_bs_vs_fp64": dbs,
-                           "label_agreement_vs_fp64": agree},
-            "surrogate": None if gated is None else {
-                "value": value_gated,
-                "ms_per_step": ms_g,
-                "delta_bs_vs_fp64": dbs_g,
-                "label_agreement_vs_fp64": agree_g,
-                "routed_fraction": g_stats[-1].routed_fraction,
-                "audited": g_stats[-1].n_audited,
-                "audit_error_of_confident_labels": g_stats[-1].audit_error,
-                "threshold": 0.95,
-                "mlp_roofline": mlp_roof,
-                "net": ("MLP (z-scored IC and params, sin/cos of 64 random Fourier projections) -> 4 x 256 GELU "
-                        "-> 6 logits; inference on tcgen05 (TMEM accumulators), training on BF16 mma.sync, "
-                        "FP32 accumulate; softmax temperature fitted on held-out labels"),
-                "train_labels": tinfo["n_train"],
-                "calibration_labels": tinfo["n_calibration"],
-                "temperature": tinfo["temperature"],
-                "train_label_s": tinfo["label_s"],
-                "train_s": tinfo["train_s"],
-                "train_accuracy": hist.accuracy[-1],
-                "timed": "inference, gate, integration of the routed ICs, merge (training excluded)",
-            },
-            "plain_fp64": {"value": n_all / (ms64 / 1000.0), "ms_per_step": ms64,
-                           "kernel_ms": statistics.mean(kern64), "rtol_atol": [DUFFING["rtol"], DUFFING["atol"]]},
-            "speedup_vs_plain_fp64": ms64 / ms_pass,
-            "e2e": {
-                "value": n * world / (e2e_ms / 1000.0),
-                "unit": "ICs/s",
-                "h2d_bytes_per_step": int(y0_host.numel() * 4),
-                "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8),
-                "labels": "int32 class indices per IC and the per-class counts, in host memory",
-            },
-            # gated: input features, tensor-core MLP, gate, gather, merge, summary
-            "gpu_launches": (pipe.kernel_launches_per_pass() + (6 if use_gate else 0)) * args.steps,
-            "roofline": {
-                "bound": "fp32-fma",
-                "achieved": achieved / 1e12,
-                "peak": peak32 / 1e12,
-                "unit": "TFLOP/s",
-                "frac": achieved / peak32,
-                "traffic": 1.6934e9 * (n + len(DUFFING["templates"])) / 50005,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel "
-                                  "(main phase of the probed integrator) at N=50,000, scaled by trajectories: "
-                                  "the window's step records, "
-                                  "written by the integrating lanes and read back by the warps that drain "
-                                  "the sampling into the same launch",
-                "note": "achieved counts the integration FLOPs only; the dominant kernel's time also holds "
-                        "the window sampling drained into it",
-                "peak_source": "FP32 FMA probe kernel measured in this run (the measured-peaks file, when "
-                               "present, holds only HBM-copy and bf16-GEMM peaks, neither of which bounds "
-                               "this kernel)",
-                "fp64_fma_peak": peak64 / 1e12,
-                "kernel_ms": kms,
-                "mean_steps_per_ic": mean_steps,
-                "flop_per_ic": flop_per_ic,
-            },
+            "path": path,
+            "delta_bs_vs_fp64": dbs_line,
+            "label_agreement_vs_fp64": agree_line,
+            "surrogate_1e7": big,
+            "duffing_1e5": duffing,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "roofline": roofline,
             "clocks": clk.summary(),
         }
         if cpu is not None:
@@ -602,6 +781,7 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="time the fused integrator path alone")
+    ap.add_argument("--c5-n", type=int, default=C5_N, help="ICs of the surrogate workload (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

@@ -147,6 +147,7 @@ class GraphTrainer:
         self.steps = sum(-(-n_rows // B) for _ in range(epochs))
         self.capture_s = 0.0
         self.launches = 0
+        self.timing = False
 
     # -- one run, as launched (captured once) ------------------------------------------
     def _reset(self) -> None:
@@ -291,14 +292,28 @@ class GraphTrainer:
         asynchronous on the current stream.  The net's weights hold the result."""
         if x is not None:
             self.load(x, labels)
+        if use_graph and self.graph is None:
+            self.capture()
+        ev = None
+        if self.timing:  # CUDA events around the run (read by run_ms)
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         if use_graph:
-            if self.graph is None:
-                self.capture()
             self.graph.replay()
         else:
             self._run()
+        if ev is not None:
+            ev[1].record()
+        self._events = ev
         self.net._step += 1  # repack the inference weights
         self.net._adam = None
+
+    def run_ms(self) -> float | None:
+        """Device time of the last run when ``timing`` was set (waits for it)."""
+        if getattr(self, "_events", None) is None:
+            return None
+        self._events[1].synchronize()
+        return self._events[0].elapsed_time(self._events[1])
 
     def stats(self) -> dict[str, float]:
         """Mean training loss and accuracy over all epochs of the last run, and the error flag."""
