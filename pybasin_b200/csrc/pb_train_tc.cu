@@ -14,9 +14,13 @@
 // Every operand is read from global memory through element strides and staged
 // into shared memory in the K-major core-matrix layout of tcgen05.mma (8 rows x
 // 16 bytes per core matrix, core (row/8, k/8) at ((row/8) * (KC/8) + k/8) * 128
-// bytes).  An operand contiguous along K is copied with cp.async, 16 bytes (8 k)
-// at a time, all copies in flight before one wait; one contiguous along its rows
-// is read 16 bytes (8 rows) at a time and scattered to the 8 core rows.  The
+// bytes).  An operand contiguous along K, with rows and K multiples of 8 and
+// 16-byte aligned rows, is brought in by one TMA copy: a 4-D tensor map over
+// (k mod 8, row mod 8, k / 8, row / 8) with strides (2 B, row pitch, 16 B, 8 row
+// pitches), whose box lands in shared memory in exactly the core-matrix order.
+// Other K-contiguous operands are copied with cp.async, 16 bytes (8 k) at a time;
+// one contiguous along its rows is read 16 bytes (8 rows) at a time and
+// scattered to the 8 core rows.  The
 // training step keeps every operand K-contiguous: the producers of the
 // activations and of dZ also write transposed copies (one row of the copy per
 // column, consecutive threads writing consecutive elements), the optimiser
@@ -37,12 +41,15 @@
 // Every mbarrier wait is bounded: on a timeout the CTA sets the error flag,
 // frees its tensor memory and returns.  There is no counterpart in the
 // reference (its surrogate-free pipeline has no learned part).
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
 
 #include <atomic>
+#include <cstdlib>
+#include <mutex>
 
 #include "pb_gelu.cuh"
 #include "pybasin_b200.h"
@@ -76,7 +83,8 @@ struct GemmTcArgs {
     int64_t ldc, ldt, ldp;
     int* error;
     int zin_off;  // input gradient: the z_in tile, loaded while the MMAs run
-    int bar_off;  // the mbarrier and the tensor-memory slot
+    int bar_off;  // the mbarriers and the tensor-memory slot
+    int tma_a, tma_b;  // operand brought in by its tensor map (else cp.async / scatter)
 };
 
 // Shared memory of one CTA: the operand tiles (A 128 x kc, B bn x kc), then for
@@ -142,6 +150,35 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     for (long long i = 0; i < kWaitPolls; ++i)
         if (mbar_try(bar, parity)) return true;
     return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// One tile of an operand by its 4-D tensor map: coordinates (k mod 8 = 0, row mod 8
+// = 0, k0 / 8, row0 / 8); completes on the mbarrier with the box's byte count.
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, int k0, int row0, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(k0 >> 3), "r"(row0 >> 3), "r"(bar)
+        : "memory");
+}
+
+// The virtual row of ones (the bias column) of a TMA-staged B tile: the copy left
+// it zero (it lies past the tensor map's rows), so it is written after the copy.
+__device__ __forceinline__ void ones_row(uint8_t* s, int r, int KC, int k0, int kend)
+{
+    const __nv_bfloat16 zero = __float2bfloat16(0.f), one = __float2bfloat16(1.f);
+    for (int kg = threadIdx.x; kg < (KC >> 3); kg += kThreads) {
+        __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) h[j] = k0 + kg * 8 + j < kend ? one : zero;
+        *reinterpret_cast<uint4*>(s + core_offset(r, kg * 8, KC)) = *reinterpret_cast<const uint4*>(h);
+    }
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
@@ -319,14 +356,15 @@ __device__ __forceinline__ void tile_out(const uint8_t* t, int tp, uint8_t* dst,
 
 // MODE: the epilogue (PB_TRAIN_*); AK / BK: A / B contiguous along K (else along its rows)
 template <int MODE, bool AK, bool BK>
-__global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(const GemmTcArgs p)
+__global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(const GemmTcArgs p, const __grid_constant__ CUtensorMap map_a,
+                                                          const __grid_constant__ CUtensorMap map_b)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int KC = p.kc, BN = p.bn;
     uint8_t* As = smem;
     uint8_t* Bs = smem + kRows * KC * 2;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + p.bar_off);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + p.bar_off);  // [0] MMAs done, [1] TMA copies done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kRows, n0 = blockIdx.y * BN, k0 = blockIdx.z * KC;
     const int kend = min(p.K, k0 + KC);
@@ -336,6 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(const GemmTcArgs p)
 
     if (tid == 0) {
         mbar_init(smem_u32(bar), 1);
+        mbar_init(smem_u32(bar + 1), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -347,22 +386,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(const GemmTcArgs p)
     // weight gradient with bias partials: B gets a virtual row N of ones, so column N
     // of the product holds the column sums of A^T (the bias gradient)
     const bool with_bias = MODE == PB_TRAIN_DW && p.col_part != nullptr;
-    if constexpr (AK)
-        stage_kcontig(As, p.A, p.sam, m0, kRows, p.M, k0, KC, kend, -1);
-    else
-        stage_rowcontig(As, p.A, p.sam, p.sak, m0, kRows, p.M, k0, KC, kend, -1);
-    if constexpr (BK)
-        stage_kcontig(Bs, p.B, p.sbn, n0, BN, p.N, k0, KC, kend, with_bias ? p.N : -1);
-    else
-        stage_rowcontig(Bs, p.B, p.sbn, p.sbk, n0, BN, p.N, k0, KC, kend, with_bias ? p.N : -1);
+    const bool tma = p.tma_a || p.tma_b;
+    if (tma) {
+        __syncthreads();  // the barrier's initialisation is visible before the copies arrive on it
+        if (tid == 0) {
+            mbar_expect_tx(smem_u32(bar + 1),
+                           (p.tma_a ? kRows * KC * 2u : 0u) + (p.tma_b ? static_cast<uint32_t>(BN) * KC * 2u : 0u));
+            if (p.tma_a) tma_load_tile(smem_u32(As), &map_a, k0, m0, smem_u32(bar + 1));
+            if (p.tma_b) tma_load_tile(smem_u32(Bs), &map_b, k0, n0, smem_u32(bar + 1));
+        }
+    }
+    if (!p.tma_a) {
+        if constexpr (AK)
+            stage_kcontig(As, p.A, p.sam, m0, kRows, p.M, k0, KC, kend, -1);
+        else
+            stage_rowcontig(As, p.A, p.sam, p.sak, m0, kRows, p.M, k0, KC, kend, -1);
+    }
+    if (!p.tma_b) {
+        if constexpr (BK)
+            stage_kcontig(Bs, p.B, p.sbn, n0, BN, p.N, k0, KC, kend, with_bias ? p.N : -1);
+        else
+            stage_rowcontig(Bs, p.B, p.sbn, p.sbk, n0, BN, p.N, k0, KC, kend, with_bias ? p.N : -1);
+    }
     cp_async_wait_all();
+    bool staged = true;
+    if (tma) {
+        staged = !__syncthreads_or(!mbar_wait(smem_u32(bar + 1), 0));
+        if (p.tma_b && with_bias && p.N - n0 >= 0 && p.N - n0 < BN) ones_row(Bs, p.N - n0, KC, k0, kend);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (tid == 0) {
+    if (tid == 0 && staged) {
         const uint32_t sbo_a = static_cast<uint32_t>(KC >> 3) << 7;
         const uint32_t idesc = instr_desc(kRows, BN);
         for (int kk = 0; kk < (KC >> 4); ++kk)
@@ -387,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tc(const GemmTcArgs p)
         }
         cp_async_wait_all();
     }
-    const bool ok = !__syncthreads_or(!mbar_wait(smem_u32(bar), 0));
+    const bool ok = staged && !__syncthreads_or(!mbar_wait(smem_u32(bar), 0));
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
         const int quarter = warp & 3, half = warp >> 2;
@@ -679,7 +737,7 @@ __global__ void k_gather_train(const __nv_bfloat16* __restrict__ x, int width, c
     }
 }
 
-using GemmFn = void (*)(GemmTcArgs);
+using GemmFn = void (*)(GemmTcArgs, CUtensorMap, CUtensorMap);
 
 template <int MODE>
 constexpr GemmFn gemm_of(bool ak, bool bk)
@@ -714,6 +772,54 @@ cudaError_t ensure_gemm_smem()
                                      kMaxSmem);
     if (e == cudaSuccess && dev >= 0 && dev < kDevs) done[dev].store(1, std::memory_order_release);
     return e;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry points (the library
+// does not link libcuda); nullptr if unavailable (the copies then use cp.async)
+using FnEncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+// PB_TRAIN_NO_TMA=1 in the environment keeps every copy on cp.async (a comparison switch)
+bool no_tma()
+{
+    static const bool off = [] {
+        const char* v = getenv("PB_TRAIN_NO_TMA");
+        return v && v[0] == '1';
+    }();
+    return off;
+}
+
+FnEncodeTiled encode_tiled()
+{
+    static FnEncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* q = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<FnEncodeTiled>(q);
+    });
+    return fn;
+}
+
+// The 4-D tensor map of a K-contiguous operand X (rows x K, row pitch sr
+// elements) whose (8 k x 8 rows x kc/8 x rows_box/8) box is a run of core
+// matrices; false (no map) unless rows and K are multiples of 8 and the rows
+// 16-byte aligned.
+bool operand_map(CUtensorMap* map, const void* X, int64_t sr, int rows, int K, int kc, int rows_box)
+{
+    const FnEncodeTiled enc = encode_tiled();
+    if (!enc || rows % 8 || K % 8 || (sr * 2) % 16 || reinterpret_cast<uintptr_t>(X) % 16 || rows_box % 8 ||
+        rows_box > 256 * 8 || kc > 256 * 8)
+        return false;
+    const cuuint64_t dims[4] = {8, 8, static_cast<cuuint64_t>(K / 8), static_cast<cuuint64_t>(rows / 8)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(sr * 2), 16, static_cast<cuuint64_t>(sr * 2 * 8)};
+    const cuuint32_t box[4] = {8, 8, static_cast<cuuint32_t>(kc / 8), static_cast<cuuint32_t>(rows_box / 8)};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(X), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 int grid_cap(int64_t work, int block)
@@ -785,7 +891,13 @@ int pb_train_gemm(const void* A, int64_t sam, int64_t sak, const void* B, int64_
     smem_plan(mode, kc, bn, &p.zin_off, &p.bar_off, &smem);
     if (smem > kMaxSmem) return PB_EINVAL;  // e.g. the input gradient with bn > 128
     if (ensure_gemm_smem() != cudaSuccess) return PB_ECUDA;
-    gemm_kernel(mode, sak == 1, sbk == 1)<<<grid, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+    CUtensorMap map_a{}, map_b{};
+    if (!no_tma()) {
+        p.tma_a = sak == 1 && operand_map(&map_a, A, sam, M, K, kc, kRows) ? 1 : 0;
+        p.tma_b = sbk == 1 && operand_map(&map_b, B, sbn, N, K, kc, bn) ? 1 : 0;
+    }
+    gemm_kernel(mode, sak == 1, sbk == 1)<<<grid, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(p, map_a,
+                                                                                                      map_b);
     return cudaGetLastError() == cudaSuccess ? PB_SUCCESS : PB_ECUDA;
 }
 
