@@ -292,7 +292,10 @@ typedef struct pb_solve_args {
        itself holds the full count.  NULL = not written. */
     double* peaks_out;
     int32_t peak_cap;
-    int32_t _pad3;
+    /* QUEUE / PROBED schedules (ABI >= 102): a warp fetches new queue positions for
+       its idle lanes once refill_lanes of its 32 lanes are idle, so lanes whose
+       trajectories finished early take new work (0 or 32: when all 32 are idle). */
+    int32_t refill_lanes;
     /* second parameter of the two-parameter window kinds (segment_focus, max_val, qh) */
     double feat_param2[PB_MAX_FEATURES];
 } pb_solve_args;

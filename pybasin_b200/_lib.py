@@ -179,7 +179,7 @@ class SolveArgs(ctypes.Structure):
         ("window_record_cap", _c_i32),
         ("peaks_out", _c_vp),
         ("peak_cap", _c_i32),
-        ("_pad3", _c_i32),
+        ("refill_lanes", _c_i32),
         ("feat_param2", _c_dbl * MAX_FEATURES),
     ]
 

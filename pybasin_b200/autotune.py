@@ -12,7 +12,17 @@ one full pass on the caller's own ICs and keeps the fastest:
   fewer warps in flight;
 * ``dense_mode`` — deferred (step records + sampling pass) or inline;
 * ``schedule`` — the queue in processing order, or probed (a probe over the
-  first 5 % of the span orders the trajectories longest first).
+  first 5 % of the span orders the trajectories longest first);
+* ``refill_lanes`` — the queue depth of a warp: it fetches new queue positions
+  for its idle lanes once this many of its 32 lanes are idle (32: only a fully
+  idle warp refills; fewer: lanes whose trajectories finished early or stopped
+  take new work while the rest of the warp integrates).
+
+Lanes per trajectory are not a knob for the built-in systems: a trajectory of
+two or three states is one serial chain of stages (splitting it over lanes
+adds shuffles to every stage and leaves lanes idle), and the network systems
+take one warp per trajectory with their nodes spread over its lanes, the
+register budget bounding the nodes per lane.
 
 Tuning time is reported, never part of a timed pass.  Results are cached in
 memory and, with ``path``, in a JSON file.
@@ -37,6 +47,7 @@ class LaunchShape:
     grid_blocks: int  # 0 = one block per block_size trajectories (every warp one task)
     dense_mode: str  # "deferred" | "inline"
     schedule: str = "queue"  # "queue" | "probed"
+    refill_lanes: int = 32  # idle lanes of a warp that trigger a refill from the queue
 
 
 @dataclass
@@ -57,14 +68,18 @@ def candidate_shapes(
     sms: int,
     dense_modes: tuple[str, ...] = ("deferred",),
     schedules: tuple[str, ...] = ("queue", "probed"),
+    refills: tuple[int, ...] = (32, 16, 8),
+    block_sizes: tuple[int, ...] = (64, 128, 256),
 ) -> list[LaunchShape]:
-    """Block sizes 64/128/256 x grids from one task per warp down to ~1.5 SM-waves."""
+    """Block sizes x grids from one task per warp down to ~1.5 SM-waves x refill
+    thresholds (the refill only matters where warps come back to the queue, so the
+    smaller thresholds are paired with the full grid of each block size)."""
     out: list[LaunchShape] = []
     for sched in schedules:
         for mode in dense_modes:
             if sched == "probed" and mode != "deferred":
                 continue  # the probed schedule applies to deferred dense output
-            for bs in (64, 128, 256):
+            for bs in block_sizes:
                 need = math.ceil(n_traj / bs)
                 grids = {0}
                 for frac in (0.75, 0.5, 0.33, 0.25):
@@ -72,7 +87,10 @@ def candidate_shapes(
                     if g >= sms:
                         grids.add(g)
                 for g in sorted(grids, reverse=True):
-                    out.append(LaunchShape(bs, g, mode, sched))
+                    out.append(LaunchShape(bs, g, mode, sched, 32))
+                for r in refills:
+                    if r != 32:
+                        out.append(LaunchShape(bs, 0, mode, sched, r))
     return out
 
 
@@ -102,8 +120,10 @@ def _apply(pipe: Any, shape: LaunchShape) -> None:
         pipe.solver.dense_mode = shape.dense_mode
         pipe.solver.schedule = shape.schedule
         pipe._allocate(pipe.capacity)  # the scratch layout depends on both
+    pipe.solver.refill_lanes = shape.refill_lanes
     pipe.args.block_size = shape.block_size
     pipe.args.grid_blocks = shape.grid_blocks
+    pipe.args.refill_lanes = shape.refill_lanes
     pipe._graph = None
 
 
@@ -138,7 +158,7 @@ def tune_pipeline(
     cache = {**_load(p), **_MEMO}
     if not force and key in cache:
         ent = cache[key]
-        best = LaunchShape(**ent["best"])
+        best = LaunchShape(**{k: v for k, v in ent["best"].items() if k in LaunchShape.__dataclass_fields__})
         _apply(pipe, best)
         return TuneResult(best, ent["best_ms"], [], 0.0, key)
     if pipe.solver.schedule not in ("queue", "probed"):

@@ -1945,6 +1945,7 @@ int validate_args(const pb_solve_args* a, bool user_system)
     if ((a->schedule == PB_SCHED_QUEUE || a->schedule == PB_SCHED_PROBED) && !a->queue_counter) return PB_EINVAL;
     if (a->schedule == PB_SCHED_PROBED && a->n_traj > 0x7fffffffLL) return PB_EINVAL;  // 32-bit sort values
     if (a->block_size < 0 || (a->block_size % 32) != 0 || a->block_size > 256) return PB_EINVAL;
+    if (a->refill_lanes < 0 || a->refill_lanes > 32) return PB_EINVAL;
     return PB_SUCCESS;
 }
 
@@ -2120,7 +2121,8 @@ using namespace pb;
 
 extern "C" {
 
-int32_t pb_abi_version(void) { return 101; }  // 101: pb_solve_args gained feat_param2
+// 101: pb_solve_args gained feat_param2; 102: refill_lanes (in place of a padding word)
+int32_t pb_abi_version(void) { return 102; }
 
 const char* pb_error_string(int32_t s)
 {

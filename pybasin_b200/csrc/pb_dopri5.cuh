@@ -876,6 +876,53 @@ __global__ void __launch_bounds__(256) k_solve_queue(const pb_solve_args a, int 
     const int lane = threadIdx.x & 31;
     auto st = stats_slot<Sys>(smem, !DEFER);
     const double t_probe = a.t0 + kProbeFraction * (a.t1 - a.t0);
+    // Refill threshold (work-queue compaction): with refill_lanes r in [1, 32), a warp
+    // fetches new queue positions for its idle lanes as soon as r of them are idle,
+    // so lanes whose trajectories finished early or stopped (diverged, unbounded)
+    // take new work while their neighbours keep integrating.  The lanes fetched
+    // together take consecutive positions of the processing order.  r = 32 (or 0) is
+    // the whole-warp schedule below; the probe phase always uses it.
+    const int refill = (a.refill_lanes > 0 && a.refill_lanes < 32) ? a.refill_lanes : 32;
+    if (PHASE != 1 && refill < 32) {
+        typename I::L_t L;
+        int64_t traj = -1;
+        bool active = false, exhausted = false;
+        while (true) {
+            const unsigned idle = __ballot_sync(0xffffffffu, !active);
+            if (!exhausted && __popc(idle) >= refill) {
+                const int leader = __ffs(idle) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(a.queue_counter, static_cast<unsigned long long>(__popc(idle)));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (static_cast<int64_t>(base) >= a.n_traj) exhausted = true;
+                const int64_t q = static_cast<int64_t>(base) + __popc(idle & ((1u << lane) - 1u));
+                if (!active && q < a.n_traj) {
+                    traj = PHASE == 2 ? static_cast<int64_t>(sort_vec(a, pl.sl.val_out_off)[q]) : traj_at(a, q);
+                    const bool in_range = traj >= 0 && traj < a.n_traj;  // an order entry out of range is ignored
+                    const bool skip = !in_range ||
+                                      (redo_only && reinterpret_cast<const int*>(tail_ptr(a, pl.sl, traj))[0] >= 0);
+                    if (!skip) {
+                        if (PHASE == 2) {
+                            active = I::resume(L, pl, traj, a);
+                        } else {
+                            I::begin(L, st, traj, a);
+                            active = true;
+                        }
+                    }
+                    if constexpr (PHASE == 2 && Drain::kOn)
+                        if (!active) Drain::publish(a, pl, skip ? -1 : traj);  // skipped, or done in the probe
+                }
+            }
+            if (exhausted && __ballot_sync(0xffffffffu, active) == 0u) break;
+            if (active && I::template step<DEFER>(L, st, pl, traj, a)) {
+                I::template finish<DEFER>(L, st, pl, traj, a);
+                if constexpr (PHASE == 2 && Drain::kOn) Drain::publish(a, pl, traj);
+                active = false;
+            }
+        }
+        if constexpr (Drain::kOn) Drain::drain(a, pl, lane);
+        return;
+    }
     while (true) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.queue_counter, 32ull);

@@ -53,6 +53,7 @@ class SolveRequest:
     keep_steps: bool = False
     block_size: int = 0
     grid_blocks: int = 0
+    refill_lanes: int = 0  # QUEUE / PROBED: refill a warp's idle lanes once this many are idle (0: all 32)
     order: torch.Tensor | None = None  # (n_traj,) int32 processing order
     dense_mode: int = L.DENSE_DEFERRED
     window_record_cap: int = 0
@@ -98,6 +99,7 @@ def build_args(
     a.n_params = req.params.shape[1]
     a.block_size = req.block_size
     a.grid_blocks = req.grid_blocks
+    a.refill_lanes = req.refill_lanes
     a.n_ic = req.y0.shape[0]
     a.n_param_rows = req.params.shape[0]
     a.n_traj = n_traj

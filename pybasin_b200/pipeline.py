@@ -149,6 +149,7 @@ class BasinStabilityPipeline:
             keep_final=False,
             block_size=self.solver.block_size,
             grid_blocks=self.solver.grid_blocks,
+            refill_lanes=getattr(self.solver, "refill_lanes", 0),
             order=self.order if self.solver.order == "morton" else None,
             dense_mode=L.DENSE_DEFERRED if self.solver.dense_mode == "deferred" else L.DENSE_INLINE,
         )
@@ -180,6 +181,16 @@ class BasinStabilityPipeline:
         if self._n != n:
             self._graph = None
         self._n = n
+
+    def autotune(self, y0: torch.Tensor, path: str | None = None, force: bool = False, **kw):
+        """Pick the integrator's launch shape (block size, grid, dense mode, schedule,
+        refill threshold) by timing candidate passes over device ICs ``y0``; the
+        result is cached per workload signature (in memory, and in ``path`` when
+        given) and left configured on this pipeline.  Returns the ``TuneResult``
+        (its ``tune_s`` is the tuning time, kept out of any timed pass)."""
+        from pybasin_b200.autotune import tune_pipeline
+
+        return tune_pipeline(self, y0, path=path, force=force, **kw)
 
     # -- one pass ----------------------------------------------------------------
     def _launch(self) -> None:

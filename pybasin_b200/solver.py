@@ -173,6 +173,7 @@ class B200Dopri5Solver:
         grid_blocks: int = 0,
         order: str = "morton",
         dense_mode: str = "deferred",
+        refill_lanes: int = 0,
     ):
         if t_eval is not None and (t_eval[0] < t_span[0] or t_eval[1] > t_span[1]):
             raise ValueError(f"t_eval {t_eval} must be within t_span {t_span}.")
@@ -190,6 +191,9 @@ class B200Dopri5Solver:
             raise ValueError("order must be 'morton' or 'none'")
         if dense_mode not in ("deferred", "inline"):
             raise ValueError("dense_mode must be 'deferred' or 'inline'")
+        if not 0 <= refill_lanes <= 32:
+            raise ValueError("refill_lanes must be in [0, 32] (0 or 32: refill only a fully idle warp)")
+        self.refill_lanes = int(refill_lanes)
         self.order = order
         self.dense_mode = dense_mode
         self.t_span = t_span
@@ -253,6 +257,7 @@ class B200Dopri5Solver:
             grid_blocks=self.grid_blocks,
             order=self.order,
             dense_mode=self.dense_mode,
+            refill_lanes=self.refill_lanes,
         )
 
     def compute_device(self) -> torch.device:
@@ -391,6 +396,7 @@ class B200Dopri5Solver:
                 out_dtype=y0.dtype,
                 block_size=self.block_size,
                 grid_blocks=self.grid_blocks,
+                refill_lanes=self.refill_lanes,
                 order=order,
                 dense_mode=L.DENSE_DEFERRED if self.dense_mode == "deferred" else L.DENSE_INLINE,
                 csr_row=csr_row,

@@ -25,7 +25,7 @@ def test_library_builds_and_loads():
     path = B.build()
     assert path.exists()
     lib = L.load()
-    assert lib.pb_abi_version() == 101
+    assert lib.pb_abi_version() == 102
 
 
 def test_every_declared_symbol_is_exported():

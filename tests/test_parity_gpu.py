@@ -57,6 +57,7 @@ def gpu_solve(
     grid_blocks: int = 0,
     dense_mode: int = L.DENSE_DEFERRED,
     window_record_cap: int = 0,
+    refill_lanes: int = 0,
 ):
     y0_t = torch.as_tensor(np.ascontiguousarray(y0), dtype=y0_dtype, device=DEV)
     p_t = torch.as_tensor(np.ascontiguousarray(np.atleast_2d(params)), dtype=torch.float64, device=DEV)
@@ -87,6 +88,7 @@ def gpu_solve(
         grid_blocks=grid_blocks,
         dense_mode=dense_mode,
         window_record_cap=window_record_cap,
+        refill_lanes=refill_lanes,
     )
     r = solve(req)
     torch.cuda.synchronize()
@@ -885,3 +887,29 @@ def test_features_are_bit_identical_across_schedules(feats, precision):
                         schedule=sched, **kw)
         np.testing.assert_array_equal(got["features"], ref["features"])
         np.testing.assert_array_equal(got["status"], ref["status"])
+
+
+@pytest.mark.parametrize("schedule,dense", [(L.SCHED_QUEUE, L.DENSE_DEFERRED), (L.SCHED_QUEUE, L.DENSE_INLINE),
+                                            (L.SCHED_PROBED, L.DENSE_DEFERRED)])
+@pytest.mark.parametrize("refill", [1, 8])
+def test_lane_refill_is_bit_identical_to_whole_warp_refill(schedule, dense, refill):
+    """Refilling idle lanes from the queue (a warp takes new positions once `refill`
+    of its lanes are idle) changes which lane integrates which trajectory, never a
+    trajectory's steps: statuses, step counts, features and final states equal those
+    of the whole-warp schedule, with trajectories that stop early (unbounded runaways
+    of the broken-butterfly Lorenz system, a NaN IC, a step budget) among them."""
+    rng = np.random.default_rng(17)
+    y0 = rng.uniform(-20.0, 20.0, (3000, 3))
+    y0[5] = np.nan
+    params = np.array([[0.12, 0.0, -0.6]])  # sigma, r, b: runaway trajectories
+    save = np.linspace(0.0, 30.0, 301)
+    feats = [(0, L.FEAT_MEAN, 0.0), (2, L.FEAT_MAX, 0.0), (1, L.FEAT_STD, 0.0)]
+    kw = dict(precision=L.PREC_MIXED, schedule=schedule, dense_mode=dense, win_begin=100, features=feats,
+              unbounded_thr=200.0, max_steps=3000)
+    ref = gpu_solve(O.SYS_LORENZ, y0, params, save, (0.0, 30.0), 1e-6, 1e-6, **kw)
+    got = gpu_solve(O.SYS_LORENZ, y0, params, save, (0.0, 30.0), 1e-6, 1e-6, refill_lanes=refill, **kw)
+    assert len(set(ref["status"].tolist())) >= 2  # early stops are among them
+    np.testing.assert_array_equal(got["status"], ref["status"])
+    np.testing.assert_array_equal(got["steps"], ref["steps"])
+    np.testing.assert_array_equal(got["features"], ref["features"])
+    np.testing.assert_array_equal(got["y_final"], ref["y_final"])
