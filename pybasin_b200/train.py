@@ -92,13 +92,19 @@ class GraphTrainer:
 
     def __init__(self, net: MLPSurrogate, n_rows: int, epochs: int, batch: int = 4096, lr: float = 4e-3,
                  weight_decay: float = 1e-4, seed: int = 0, betas: tuple[float, float] = (0.9, 0.999),
-                 eps: float = 1e-8, resume: bool = False):
+                 eps: float = 1e-8, resume: bool = False, data_parallel: bool = False, group=None):
         """With ``resume``, a run starts from the net's current weights (fresh AdamW
-        moments) instead of the weights it had when the trainer was built."""
+        moments) instead of the weights it had when the trainer was built.  With
+        ``data_parallel`` every rank of the process group trains on its own rows
+        (the same row count, batch and epochs on every rank): after each backward
+        pass the gradients are summed over the rank's chunks and averaged over the
+        ranks in one collective, so every rank takes the same AdamW step."""
         if net.d_in % 8:
             raise ValueError("GraphTrainer needs input rows of a multiple of 8 columns (MLPSurrogate(pad_inputs=True))")
         self.net = net
         self.resume = resume
+        self.data_parallel = data_parallel
+        self.group = group
         self.dev = net.dev
         self.n, self.epochs, self.batch = n_rows, epochs, min(batch, n_rows)
         self.lr, self.wd, self.betas, self.eps = lr, weight_decay, betas, eps
@@ -177,7 +183,7 @@ class GraphTrainer:
         parts = (vp * nt)(*([g.data_ptr() for g in self.gw_part] + [g.data_ptr() for g in self.gb_part]))
         n = (ctypes.c_int64 * nt)(*[p.numel() for p in self.params])
         stride = (ctypes.c_int64 * nt)(*([w_.numel() for w_ in net.W] + [b.numel() for b in net.b]))
-        splits = -(-M // KC)
+        splits = 1 if self.data_parallel else -(-M // KC)  # data parallel: reduced into partial 0
         nparts = (ctypes.c_int32 * nt)(*([splits] * (2 * L_)))
         wd = (ctypes.c_float * nt)(*([self.wd] * L_ + [0.0] * L_))
         L.check(lib.pb_train_adamw(nt, w, wb, wbt, cols, m1, m2, parts, n, stride, nparts, wd, lr, self.betas[0],
@@ -221,6 +227,19 @@ class GraphTrainer:
                 launches += 1
         return launches
 
+    def _exchange(self, M: int) -> None:
+        """Data parallel: each gradient's chunk partials summed into partial 0, then
+        averaged over the ranks (one flat all-reduce)."""
+        from pybasin_b200.sharding import allreduce_gradients
+
+        splits = -(-M // KC)
+        firsts = []
+        for parts in self.gw_part + self.gb_part:
+            if splits > 1:
+                parts[0].copy_(parts[:splits].sum(0))
+            firsts.append(parts[0])
+        allreduce_gradients(firsts, group=self.group)
+
     def gradients(self, x: torch.Tensor, labels: torch.Tensor) -> tuple[list[torch.Tensor], list[torch.Tensor]]:
         """Gradients of the mean loss over one minibatch (at most ``batch`` rows) at the
         current weights, summed from their partials (for checking; no update)."""
@@ -252,6 +271,8 @@ class GraphTrainer:
                 M = min(self.batch, self.n - b0)
                 launches += self._grads(lib, s, self.Xs[b0 : b0 + M], self.XsT[:, b0:], self.n, self.Ys[b0 : b0 + M],
                                         M)
+                if self.data_parallel:
+                    self._exchange(M)
                 step += 1
                 self._adamw(lib, s, M, lr, step)
                 launches += 1
@@ -292,6 +313,11 @@ class GraphTrainer:
         asynchronous on the current stream.  The net's weights hold the result."""
         if x is not None:
             self.load(x, labels)
+        if use_graph and self.data_parallel:
+            import torch.distributed as dist
+
+            # a collective inside the captured run needs NCCL (gloo is host-driven)
+            use_graph = dist.is_initialized() and dist.get_backend(self.group) == "nccl"
         if use_graph and self.graph is None:
             self.capture()
         ev = None

@@ -145,3 +145,40 @@ def test_graph_replay_equals_eager_run_and_learns():
             assert torch.equal(a, b)
     acc = float((net.logits(xi).argmax(1).cpu() == y).float().mean())
     assert acc > 0.97
+
+
+def test_data_parallel_trainer_under_a_one_rank_group():
+    """The data-parallel path (chunk partials summed, the one all-reduce, AdamW on a
+    single partial) under a one-rank NCCL group gives the single-process step: one
+    full-batch step from the same weights, equal to summation-order rounding."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from pybasin_b200.surrogate import MLPSurrogate
+    from pybasin_b200.train import GraphTrainer
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=DEV)
+    try:
+        g = torch.Generator().manual_seed(3)
+        pts = torch.rand(3000, 2, generator=g) * 2 - 1
+        y = (pts[:, 0] > 0).to(torch.int32)
+        out = []
+        for dp in (False, True):
+            net = MLPSurrogate(2, 4, hidden=64, depth=2, seed=5, device=DEV, n_freq=8, pad_inputs=True)
+            net.fit_normalisation(pts.to(DEV))
+            xi = net.inputs(pts.to(DEV), None)
+            tr = GraphTrainer(net, n_rows=3000, epochs=1, batch=3000, lr=4e-3, data_parallel=dp)
+            tr.train(xi, y.to(DEV), use_graph=False)
+            torch.cuda.synchronize()
+            out.append([w.clone() for w in net.W])
+        for a, b in zip(*out):
+            assert (a - b).abs().max().item() <= 1e-6
+    finally:
+        dist.destroy_process_group()
