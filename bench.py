@@ -598,6 +598,7 @@ def run_surrogate_workload(args, dev, rank: int, world: int, dist_on: bool, flus
         "delta_bs_vs_fp64": dbs,
         "label_agreement_vs_fp64": agree,
         "routed_fraction": st.routed_fraction,
+        "integrated_fraction": st.integrated_fraction,
         "audited": st.n_audited,
         "audit_error_of_confident_labels": st.audit_error,
         "threshold": 0.95,
@@ -625,6 +626,95 @@ def run_surrogate_workload(args, dev, rank: int, world: int, dist_on: bool, flus
         "gpu_launches_per_step": launches_step,
         "autotune": {"best": vars(tune.best), "best_ms": tune.best_ms, "tune_s": tune.tune_s,
                      "candidates": len(tune.table), "n_ic": gated.max_chunk},
+    }
+
+
+SWEEP_POINTS = 64
+
+
+def run_sweep_surrogate(args, dev, rank: int, world: int, dist_on: bool, flush, clk) -> dict:
+    """The surrogate of the pendulum torque sweep (the torque is a network input):
+    10^7 seeded ICs spread uniformly over the 64 torque points of the study, the
+    surrogate trained inside every step on 25,000 random + 25,000 active integrator
+    labels across the points; per-point basin stability against the plain FP64
+    kernel on all ICs."""
+    from pybasin_b200 import studies as S
+    from pybasin_b200.gated import SurrogateGatedPipeline
+
+    n = args.c5_n
+    rows = np.array([[0.1, t, 1.0] for t in np.linspace(0.1, 1.0, SWEEP_POINTS)])
+
+    def sample(m, seed):
+        y0 = S.uniform_ics(*S.PENDULUM_BOX, m, seed)
+        grp = torch.from_numpy(np.random.default_rng(seed).integers(0, SWEEP_POINTS, m).astype(np.int32))
+        return y0.to(dev), grp.to(dev)
+
+    y0, grp = sample(n, 7 + rank)
+    yr, gr = sample(C5_RANDOM, 1042 + rank)
+    yp, gp = sample(C5_POOL, 2042 + rank)
+    pipe = S.pendulum_pipeline("mixed", rows, dev)
+    gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01)
+    state = {}
+
+    def step_device():
+        state["info"] = gated.fit(yr, yp, n_active=C5_ACTIVE, epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR,
+                                  group_random=gr, group_pool=gp)
+        state["label"], state["counts"], state["stats"] = gated.run_device(y0, grp)
+
+    for _ in range(max(args.warmup, 1)):
+        step_device()
+    torch.cuda.synchronize()
+    if dist_on:
+        torch.distributed.barrier()
+    (ms,) = max_over_ranks([statistics.mean(event_ms(step_device, args.steps, flush, clk))], dev, dist_on)
+    counts = state["counts"].clone()
+    st = state["stats"]
+    fit_summary = state["info"].summary()
+
+    def chunked(p, chunk):
+        lab = torch.empty((n,), dtype=torch.int32, device=dev)
+        cnt = torch.zeros((SWEEP_POINTS, 3), dtype=torch.int64, device=dev)
+        for c0 in range(0, n, chunk):
+            l, c = p.run_device(y0[c0 : c0 + chunk], group=grp[c0 : c0 + chunk])
+            lab[c0 : c0 + l.shape[0]].copy_(l)
+            cnt += c
+        return lab, cnt
+
+    fb = getattr(gated, "last_fallback_points", None)
+    gated_bad = None if fb is None else int(fb.sum())
+    res = {}
+    fused = lambda: res.__setitem__("m", chunked(pipe, gated.max_chunk))  # noqa: E731
+    fused()
+    torch.cuda.synchronize()
+    (ms32,) = max_over_ranks([statistics.mean(event_ms(fused, 1, flush))], dev, dist_on)
+    del gated
+    pipe.release()
+    torch.cuda.empty_cache()
+    p64 = S.pendulum_pipeline("fp64", rows, dev)
+    (ms64,) = max_over_ranks([statistics.mean(event_ms(lambda: res.__setitem__("d", chunked(p64, FP64_CHUNK)),
+                                                       1, flush))], dev, dist_on)
+    lab64, cnt64 = res["d"]
+    p64.release()
+    torch.cuda.empty_cache()
+    n_p = cnt64.sum(dim=1).double().clamp_min(1)
+    dbs = ((counts[:, :2] - cnt64[:, :2]).abs().max(dim=1).values.double() / n_p).max().item()
+    dbs32 = ((res["m"][1][:, :2] - cnt64[:, :2]).abs().max(dim=1).values.double() / n_p).max().item()
+    agree = float((state["label"] == lab64).float().mean())
+    n_all = n * world
+    return {
+        "workload": f"pendulum torque sweep, {SWEEP_POINTS} points T in [0.1, 1.0], N={n} seeded ICs per GPU "
+                    "spread uniformly over the points, surrogate inputs (IC, T), trained in every step on "
+                    f"{C5_RANDOM + C5_ACTIVE} integrator labels ({C5_ACTIVE} active from a {C5_POOL}-IC pool)",
+        "value": n_all / (ms / 1000.0), "unit": "ICs/s", "ms_per_step": ms,
+        "max_point_delta_bs_vs_fp64": dbs, "label_agreement_vs_fp64": agree,
+        "routed_fraction": st.routed_fraction, "audited": st.n_audited,
+        "audit_error_of_confident_labels": st.audit_error, "temperature": fit_summary["temperature"],
+        "points_fallen_back_to_the_integrator": int(gated_bad) if gated_bad is not None else 0,
+        "integrated_fraction": st.integrated_fraction,
+        "train_steps": fit_summary["train_steps"],
+        "plain_fp64": {"value": n_all / (ms64 / 1000.0), "ms_per_pass": ms64},
+        "fused_fp32": {"value": n_all / (ms32 / 1000.0), "ms_per_pass": ms32, "max_point_delta_bs_vs_fp64": dbs32},
+        "speedup_vs_plain_fp64": {"with_training": ms64 / ms, "fused_fp32_alone": ms64 / ms32},
     }
 
 
@@ -761,9 +851,16 @@ def run_b200_arm(args) -> None:
         studies = run_studies(args, dev, flush, clk)
 
     # ---- the learned-surrogate workload (10^7 ICs, training in every step) ----------
-    big = None
+    big = sweep = None
+    launches_c2 = pipe.kernel_launches_per_pass()
+    tolerances = list(pipe.solver.effective_tolerances())
+    n_count_words = pipe.counts.numel()
     if not args.no_surrogate and args.c5_n > 0:
         big = run_surrogate_workload(args, dev, rank, world, dist_on, flush, clk, pipe)
+        pipe.release()
+        torch.cuda.empty_cache()
+        if not args.no_studies:
+            sweep = run_sweep_surrogate(args, dev, rank, world, dist_on, flush, clk)
     clk.__exit__(None, None, None)
 
     cpu = None
@@ -789,7 +886,7 @@ def run_b200_arm(args) -> None:
                            "label_agreement_vs_fp64": agree,
                            "e2e": {"value": n_all / (e2e_fused_ms / 1000.0), "unit": "ICs/s",
                                    "h2d_bytes_per_step": int(y0_host.numel() * 4),
-                                   "d2h_bytes_per_step": int(n * 4 + pipe.counts.numel() * 8)}},
+                                   "d2h_bytes_per_step": int(n * 4 + n_count_words * 8)}},
             "plain_fp64": {"value": n_all / (ms64 / 1000.0), "ms_per_step": ms64,
                            "kernel_ms": statistics.mean(kern64), "rtol_atol": [DUFFING["rtol"], DUFFING["atol"]]},
             "speedup_fused_vs_plain_fp64": ms64 / ms,
@@ -815,7 +912,7 @@ def run_b200_arm(args) -> None:
             workload = duffing["workload"]
             path = "fused FP32 integrator"
             dbs_line, agree_line = dbs, agree
-            launches = pipe.kernel_launches_per_pass() * args.steps
+            launches = launches_c2 * args.steps
         line = {
             "metric": "labelled ICs/sec at |dBS|<=0.005 vs FP64 (fused FP32 + surrogate vs plain Dopri5)",
             "value": value,
@@ -832,7 +929,7 @@ def run_b200_arm(args) -> None:
             "config": {
                 "workload": workload,
                 "n_ic_per_gpu": args.c5_n if use_big else n,
-                "rtol_atol": list(pipe.solver.effective_tolerances()),
+                "rtol_atol": tolerances,
                 "launch_shape": {k: getattr(pipe.solver, k) for k in ("block_size", "grid_blocks", "schedule",
                                                                       "dense_mode", "refill_lanes")},
                 "l2": "flushed between timed steps (256 MB write); the inputs exceed the L2",
@@ -842,6 +939,7 @@ def run_b200_arm(args) -> None:
             "delta_bs_vs_fp64": dbs_line,
             "label_agreement_vs_fp64": agree_line,
             "surrogate_1e7": big,
+            "surrogate_pendulum_sweep_1e7": sweep,
             "duffing_1e5": duffing,
             "studies": studies,
             "e2e": e2e,

@@ -481,9 +481,17 @@ int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream);
 int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
                         const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
                         void* out_bf16, void* stream);
+/* The same with a parameter row per IC (parameter studies): params is an
+ * (n_param_rows x n_params) FP64 table and row r of the inputs takes row
+ * param_index[r] (NULL: row 0); an index outside the table gives NaN inputs,
+ * which the gate routes to the integrator. */
+int pb_surrogate_inputs_rows(const float* ic, int32_t S, const double* params, int64_t n_param_rows,
+                             int32_t n_params, const int32_t* param_index, const float* shift, const float* scale,
+                             const float* freq, int32_t n_freq, int64_t n, int32_t d_pad, void* out_bf16,
+                             void* stream);
 /* Confidence gate: label = argmax, conf = max softmax probability; rows with
- * conf < threshold or audit[i] != 0 are appended to route (n_route counts them,
- * reset by the call). */
+ * conf < threshold (or not finite) or audit[i] != 0 are appended to route
+ * (n_route counts them, reset by the call). */
 int pb_surrogate_gate(const float* logits, int64_t n, int32_t C, float threshold, const uint8_t* audit,
                       int32_t* label, float* conf, int32_t* route, int32_t* n_route, void* stream);
 /* y[k, :] = x[idx[k], :] for k < min(*n_idx, max_rows). */

@@ -209,6 +209,7 @@ constexpr int kMaxRawInputs = 16;
 // Dynamic shared memory: (n_freq + R) * d floats.
 __global__ void __launch_bounds__(256) k_features_in(const float* __restrict__ ic, int S,
                                                      const double* __restrict__ prm, int np,
+                                                     const int32_t* __restrict__ prow, int64_t n_rows,
                                                      const float* __restrict__ shift,
                                                      const float* __restrict__ scale,
                                                      const float* __restrict__ freq, int n_freq, int64_t n,
@@ -229,7 +230,16 @@ __global__ void __launch_bounds__(256) k_features_in(const float* __restrict__ i
             const int rr = i / d, c = i - rr * d;
             const int64_t r = r0 + rr;
             float v = 0.f;
-            if (r < n) v = c < S ? ic[r * S + c] : static_cast<float>(prm[c - S]);
+            if (r < n) {
+                if (c < S) {
+                    v = ic[r * S + c];
+                } else {
+                    // the IC's own parameter row (prow), else row 0; a row index out of
+                    // range gives NaN inputs, whose logits the gate routes to the integrator
+                    const int64_t q = prow ? static_cast<int64_t>(prow[r]) : 0;
+                    v = (q >= 0 && q < n_rows) ? static_cast<float>(prm[q * np + (c - S)]) : CUDART_NAN_F;
+                }
+            }
             z_s[i] = (v - shift[c]) * scale[c];
         }
         __syncthreads();
@@ -273,7 +283,7 @@ __global__ void k_gate(const float* __restrict__ logits, int64_t n, int C, float
     label[i] = arg;
     if (conf) conf[i] = p;
     const bool aud = audit && audit[i];
-    if (p < threshold || aud) {
+    if (!(p >= threshold) || aud) {  // a non-finite confidence is routed too
         const int pos = atomicAdd(n_route, 1);
         route[pos] = static_cast<int32_t>(i);
     }
@@ -426,21 +436,31 @@ int pb_mlp_cast_bf16(const float* x, void* y, int64_t n, void* stream)
     return map_err(cudaGetLastError());
 }
 
-int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
-                        const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
-                        void* out_bf16, void* stream)
+int pb_surrogate_inputs_rows(const float* ic, int32_t S, const double* params, int64_t n_param_rows,
+                             int32_t n_params, const int32_t* param_index, const float* shift, const float* scale,
+                             const float* freq, int32_t n_freq, int64_t n, int32_t d_pad, void* out_bf16,
+                             void* stream)
 {
     if (!ic || !shift || !scale || !out_bf16 || S <= 0 || n_params < 0 || n_freq < 0 ||
-        S + n_params > kMaxRawInputs || S + n_params + 2 * n_freq > d_pad || n < 0)
+        S + n_params > kMaxRawInputs || S + n_params + 2 * n_freq > d_pad || n < 0 || n_param_rows < 0)
         return PB_EINVAL;
-    if ((n_params > 0 && !params) || (n_freq > 0 && !freq)) return PB_EINVAL;
+    if ((n_params > 0 && (!params || n_param_rows < 1)) || (n_freq > 0 && !freq)) return PB_EINVAL;
     if (n == 0) return PB_SUCCESS;
     if (n_freq > 128) return PB_EINVAL;  // at least two rows per 256-thread block
     const int U = n_freq > 0 ? n_freq : 1, R = 256 / U;
     const size_t fsmem = static_cast<size_t>(n_freq + R) * (S + n_params) * sizeof(float);
     k_features_in<<<grid_for((n + R - 1) / R, 1), 256, fsmem, static_cast<cudaStream_t>(stream)>>>(
-        ic, S, params, n_params, shift, scale, freq, n_freq, n, d_pad, static_cast<__nv_bfloat16*>(out_bf16));
+        ic, S, params, n_params, param_index, n_param_rows, shift, scale, freq, n_freq, n, d_pad,
+        static_cast<__nv_bfloat16*>(out_bf16));
     return map_err(cudaGetLastError());
+}
+
+int pb_surrogate_inputs(const float* ic, int32_t S, const double* params, int32_t n_params, const float* shift,
+                        const float* scale, const float* freq, int32_t n_freq, int64_t n, int32_t d_pad,
+                        void* out_bf16, void* stream)
+{
+    return pb_surrogate_inputs_rows(ic, S, params, 1, n_params, nullptr, shift, scale, freq, n_freq, n, d_pad,
+                                    out_bf16, stream);
 }
 
 int pb_surrogate_gate(const float* logits, int64_t n, int32_t C, float threshold, const uint8_t* audit,

@@ -5,7 +5,8 @@ the routed ICs (low confidence or audited) are integrated with the fused Dopri5
 pipeline together with the templates -> labels merged back -> counts.  Every
 label is either an integrator label or a confident surrogate label, and the
 audit slice measures how often a confident surrogate label disagrees with the
-integrator.
+integrator; where that happens too often at a parameter point (or over the whole
+pass), the point's surrogate labels are replaced by integrated ones.
 """
 
 from __future__ import annotations
@@ -28,6 +29,7 @@ class GateStats:
     def __init__(self, n: int, n_routed: int, tally: torch.Tensor | None):
         self.n = n
         self.n_routed = n_routed
+        self.n_fallback = 0  # ICs of points whose audit failed, integrated as well
         self._tally = tally  # int32 (3,): audited, audited-and-confident, ... of which relabelled
         self._host: list[int] | None = None
 
@@ -57,6 +59,11 @@ class GateStats:
     @property
     def audit_error(self) -> float:
         return self.audit_disagree / max(self.audit_confident, 1)
+
+    @property
+    def integrated_fraction(self) -> float:
+        """Routed by the gate or by a failed audit: labelled by the integrator."""
+        return (self.n_routed + self.n_fallback) / max(self.n, 1)
 
 
 def calibrate_temperature_device(logits: torch.Tensor, labels: torch.Tensor, lo: float = 0.5, hi: float = 4.0,
@@ -126,11 +133,18 @@ class SurrogateGatedPipeline:
         freq_scale: float = 0.3,
         calib_fraction: float = 0.1,
         max_chunk: int = 1 << 20,
+        audit_tolerance: float | None = 0.002,
+        audit_min_disagree: int = 3,
     ):
         self.pipe = pipeline
         self.max_chunk = max_chunk
+        self.audit_tolerance = audit_tolerance
+        self.audit_min_disagree = audit_min_disagree
         self.dev = pipeline.dev
-        self.params = pipeline.params[0].to(torch.float64)  # the main parameter row
+        # the parameter points (a study's rows; the pipeline's last row is the templates')
+        self.n_groups = pipeline.n_groups
+        self.param_table = pipeline.params[: self.n_groups].to(torch.float64).contiguous()
+        self.params = self.param_table[0]  # the main parameter row
         self.S = pipeline.dim
         self.C = pipeline.n_classes + 1  # + unbounded
         self.net = MLPSurrogate(self.S + self.params.numel(), self.C, hidden=hidden, depth=depth, seed=seed,
@@ -144,9 +158,18 @@ class SurrogateGatedPipeline:
         self._audit: dict[int, torch.Tensor] = {}
 
     # -- training ------------------------------------------------------------------
-    def _raw_inputs(self, y0: torch.Tensor) -> torch.Tensor:
-        p = self.params.to(torch.float32).expand(y0.shape[0], -1)
+    def _raw_inputs(self, y0: torch.Tensor, group: torch.Tensor | None = None) -> torch.Tensor:
+        if group is None:
+            p = self.params.to(torch.float32).expand(y0.shape[0], -1)
+        else:
+            p = self.param_table.to(torch.float32).index_select(0, group.to(self.dev, torch.int64))
         return torch.cat([y0.to(torch.float32), p], dim=1)
+
+    def _x(self, y0: torch.Tensor, group: torch.Tensor | None = None) -> torch.Tensor:
+        """Network inputs of ICs (with the parameter point of each for a study)."""
+        if group is None:
+            return self.net.inputs(y0, self.params)
+        return self.net.inputs(y0, self.param_table, group)
 
     def train(self, y0_train: torch.Tensor, epochs: int = 30, batch: int = 1024, lr: float = 2e-3,
               seed: int = 0) -> tuple[TrainHistory, dict[str, float]]:
@@ -185,7 +208,8 @@ class SurrogateGatedPipeline:
         return tr
 
     def fit(self, y0_random: torch.Tensor, y0_pool: torch.Tensor | None = None, n_active: int = 0,
-            epochs: int = 40, batch: int = 4096, lr: float = 5e-3, seed: int = 0) -> "FitInfo":
+            epochs: int = 40, batch: int = 4096, lr: float = 5e-3, seed: int = 0,
+            group_random: torch.Tensor | None = None, group_pool: torch.Tensor | None = None) -> "FitInfo":
         """Train the surrogate on labels of the integrator, on the tensor cores
         (``GraphTrainer``: one captured CUDA graph per training run), without a host
         round trip: every step is queued on the current stream.
@@ -197,25 +221,30 @@ class SurrogateGatedPipeline:
         (labels where the basins interleave) are labelled too, and training resumes
         on both sets for ``epochs`` epochs.  Last, the softmax temperature minimising
         the held-out negative log-likelihood is folded into the last layer, so the
-        gate's threshold reads as a probability of the label being right."""
+        gate's threshold reads as a probability of the label being right.  For a
+        parameter study, ``group_random`` / ``group_pool`` give each IC's point: the
+        network then sees the point's parameters next to the IC."""
         lib = L.load()
         _bind(lib)
         s = torch.cuda.current_stream(self.dev).cuda_stream
         net = self.net
         n = y0_random.shape[0]
         n_cal = int(n * self.calib_fraction) if n >= 100 else 0
-        labels, _ = self.pipe.run_device(y0_random)
+        g_r = None if group_random is None else group_random.to(self.dev, torch.int32)
+        labels, _ = self.pipe.run_device(y0_random, group=g_r)
         lab = labels.clone()
         fit_ic, fit_lab = y0_random[n_cal:], lab[n_cal:]
-        net.fit_normalisation(self._raw_inputs(fit_ic))
-        x_r = net.inputs(fit_ic, self.params)
+        g_fit = None if g_r is None else g_r[n_cal:]
+        net.fit_normalisation(self._raw_inputs(fit_ic, g_fit))
+        x_r = self._x(fit_ic, g_fit)
         active = n_active > 0 and y0_pool is not None
         tr1 = self._trainer(n - n_cal, max(epochs // 2, 1) if active else epochs, batch, lr, False, seed)
         tr1.train(x_r, fit_lab)
         trainers = [tr1]
         if active:
             m = y0_pool.shape[0]
-            logits = net.logits(net.inputs(y0_pool, self.params))
+            g_p = None if group_pool is None else group_pool.to(self.dev, torch.int32)
+            logits = net.logits(self._x(y0_pool, g_p))
             label = torch.empty((m,), dtype=torch.int32, device=self.dev)
             conf = torch.empty((m,), dtype=torch.float32, device=self.dev)
             route = torch.empty((m,), dtype=torch.int32, device=self.dev)
@@ -225,14 +254,15 @@ class SurrogateGatedPipeline:
                                           _p(n_route), s), "pb_surrogate_gate")
             pick = torch.topk(conf, min(n_active, m), largest=False).indices
             y0_act = y0_pool.index_select(0, pick).contiguous()
-            lab_a, _ = self.pipe.run_device(y0_act)
-            x_all = torch.cat([x_r, net.inputs(y0_act, self.params)])
+            g_a = None if g_p is None else g_p.index_select(0, pick).contiguous()
+            lab_a, _ = self.pipe.run_device(y0_act, group=g_a)
+            x_all = torch.cat([x_r, self._x(y0_act, g_a)])
             lab_all = torch.cat([fit_lab, lab_a])
             tr2 = self._trainer(x_all.shape[0], epochs, batch, lr, True, seed + 1)
             tr2.train(x_all, lab_all)
             trainers.append(tr2)
         if n_cal > 0:
-            z = net.logits(net.inputs(y0_random[:n_cal], self.params))
+            z = net.logits(self._x(y0_random[:n_cal], None if g_r is None else g_r[:n_cal]))
             T = calibrate_temperature_device(z, lab[:n_cal])
             net.W[-1].div_(T)
             net.b[-1].div_(T)
@@ -250,13 +280,17 @@ class SurrogateGatedPipeline:
             self._audit[n] = m
         return m
 
-    def run_device(self, y0: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor, GateStats]:
-        """Labels (int32, class n_classes = unbounded) and per-class counts for device ICs."""
+    def run_device(self, y0: torch.Tensor, group: torch.Tensor | None = None
+                   ) -> tuple[torch.Tensor, torch.Tensor, GateStats]:
+        """Labels (int32, class n_classes = unbounded) and per-class counts for device
+        ICs; for a parameter study ``group`` gives each IC's point and the counts are
+        per point, (points, classes)."""
         lib = L.load()
         _bind(lib)
         s = torch.cuda.current_stream(self.dev).cuda_stream
         n = y0.shape[0]
-        x = self.net.inputs(y0, self.params)
+        grp = None if group is None else group.to(self.dev, torch.int32).contiguous()
+        x = self._x(y0, grp)
         logits = self.net.logits(x)
         audit = self.audit_mask(n)
         label = torch.empty((n,), dtype=torch.int32, device=self.dev)
@@ -273,13 +307,18 @@ class SurrogateGatedPipeline:
             # integrated in chunks of at most max_chunk ICs: the deferred dense output's
             # step records are sized per trajectory (1024 records of 48 B for one FP32
             # state), so a chunk bounds the scratch (1M ICs: 48 GiB)
+            routed_g = None
+            if grp is not None:  # the routed ICs' points (int32 moved as 4-byte words)
+                routed_g = torch.empty((k,), dtype=torch.int32, device=self.dev)
+                L.check(lib.pb_gather_rows(_p(grp), 1, _p(route), _p(n_route), k, _p(routed_g), s),
+                        "pb_gather_rows")
             if k <= self.max_chunk:
-                integ, _ = self.pipe.run_device(routed)
+                integ, _ = self.pipe.run_device(routed, group=routed_g)
             else:
                 integ = torch.empty((k,), dtype=torch.int32, device=self.dev)
                 for c0 in range(0, k, self.max_chunk):
                     c1 = min(k, c0 + self.max_chunk)
-                    lab_c, _ = self.pipe.run_device(routed[c0:c1])
+                    lab_c, _ = self.pipe.run_device(routed[c0:c1], group=None if routed_g is None else routed_g[c0:c1])
                     integ[c0:c1].copy_(lab_c)
             sur_of_routed = torch.empty((k,), dtype=torch.int32, device=self.dev)
             L.check(lib.pb_merge_labels(_p(integ), _p(route), _p(n_route), k, _p(label), _p(sur_of_routed), s),
@@ -291,17 +330,67 @@ class SurrogateGatedPipeline:
         L.check(lib.pb_gate_summary(_p(label), n, self.C, _p(route) if k > 0 else None, _p(n_route), k, _p(audit),
                                     _p(conf), self.threshold, _p(sur_of_routed), _p(integ), _p(counts), _p(tally), s),
                 "pb_gate_summary")
-        return label, counts, GateStats(n, k, tally)
+        n_fallback = 0
+        if k > 0 and self.audit_tolerance is not None:
+            n_fallback = self._audit_fallback(y0, grp, label, route[:k], sur_of_routed, integ, conf, audit)
+            if n_fallback > 0 and grp is None:
+                counts.copy_(torch.bincount(label.to(torch.int64), minlength=self.C))
+        if grp is not None:  # per point: (points, classes)
+            idx = grp.to(torch.int64) * self.C + label.to(torch.int64)
+            counts = torch.bincount(idx, minlength=self.n_groups * self.C).view(self.n_groups, self.C)
+        st = GateStats(n, k, tally)
+        st.n_fallback = n_fallback
+        return label, counts, st
 
-    def run(self, y0_host: torch.Tensor, names: bool = True) -> tuple[np.ndarray, dict[str, float], GateStats]:
+    def _audit_fallback(self, y0, grp, label, route, sur_of_routed, integ, conf, audit) -> int:
+        """The audit judges the surrogate point by point: where the audited confident
+        labels of a parameter point (of the whole pass without a study) disagree with
+        the integrator's in more than ``audit_tolerance`` of them (and at least
+        ``audit_min_disagree`` times), every IC of that point the surrogate labelled
+        is integrated too and takes the integrator's label.  Returns how many."""
+        P = self.n_groups if grp is not None else 1
+        n = y0.shape[0]
+        r = route.to(torch.int64)
+        g_all = grp.to(torch.int64) if grp is not None else torch.zeros((n,), dtype=torch.int64, device=self.dev)
+        g_r = g_all.index_select(0, r)
+        aud = audit.index_select(0, r).bool() & (conf.index_select(0, r) >= self.threshold)
+        dis = aud & (sur_of_routed != integ)
+        n_aud = torch.bincount(g_r[aud], minlength=P).double()
+        n_dis = torch.bincount(g_r[dis], minlength=P).double()
+        bad = (n_dis >= self.audit_min_disagree) & (n_dis > self.audit_tolerance * n_aud)
+        self.last_fallback_points = bad
+        if not bool(bad.any()):  # one host read
+            return 0
+        routed = torch.zeros((n,), dtype=torch.bool, device=self.dev)
+        routed[r] = True
+        extra = torch.nonzero(bad.index_select(0, g_all) & ~routed).flatten()
+        m = extra.numel()
+        if m == 0:
+            return 0
+        ye = y0.index_select(0, extra).contiguous()
+        ge = None if grp is None else grp.index_select(0, extra).contiguous()
+        for c0 in range(0, m, self.max_chunk):
+            c1 = min(m, c0 + self.max_chunk)
+            lab_c, _ = self.pipe.run_device(ye[c0:c1], group=None if ge is None else ge[c0:c1])
+            label[extra[c0:c1]] = lab_c
+        return m
+
+    def run(self, y0_host: torch.Tensor, names: bool = True, group: torch.Tensor | None = None):
         """Host ICs -> (labels, basin stability per class, gate statistics); labels as
         class names, or with ``names=False`` as int32 indices into
-        ``pipe.classes + ["unbounded"]`` (no per-IC string objects to build)."""
+        ``pipe.classes + ["unbounded"]`` (no per-IC string objects to build).  For a
+        parameter study (``group``: each IC's point) the basin stability is a list
+        with one dict per point."""
         with torch.cuda.device(self.dev):
             y0 = y0_host.to(self.dev, dtype=torch.float32, non_blocking=True)
-            label, counts, stats = self.run_device(y0)
+            g = None if group is None else group.to(self.dev, dtype=torch.int32, non_blocking=True)
+            label, counts, stats = self.run_device(y0, g)
             lab, cnt = to_host_pinned(self, label, counts)
         classes = np.array(self.pipe.classes + ["unbounded"], dtype=object)
-        n = max(int(cnt.sum()), 1)
-        bs = {classes[i]: float(cnt[i]) / n for i in range(len(classes)) if cnt[i] > 0}
+
+        def fractions(c):
+            n = max(int(c.sum()), 1)
+            return {classes[i]: float(c[i]) / n for i in range(len(classes)) if c[i] > 0}
+
+        bs = fractions(cnt) if group is None else [fractions(row) for row in cnt.reshape(self.n_groups, self.C)]
         return (classes[lab] if names else lab.copy()), bs, stats

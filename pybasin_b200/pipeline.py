@@ -162,6 +162,16 @@ class BasinStabilityPipeline:
         self._n = None
         self._graph = None
 
+    def release(self) -> None:
+        """Drop the buffers sized for the largest batch so far (the next pass
+        allocates again): the step-record scratch of 10^6 ICs is tens of GB."""
+        for name in ("y0_buf", "pidx", "out", "queue", "order", "labels", "scratch", "args", "program"):
+            if hasattr(self, name):
+                delattr(self, name)
+        self.capacity = -1
+        self._n = None
+        self._graph = None
+
     def _prepare(self, n: int, group: torch.Tensor | None = None) -> None:
         """Place the templates after the first n rows and size the launch to n + templates."""
         T = self.n_tpl

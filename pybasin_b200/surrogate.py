@@ -37,6 +37,7 @@ def _bind(lib: ctypes.CDLL) -> None:
     lib.pb_mlp_adamw.argtypes = [vp, vp, vp, vp, vp, i64, f32, f32, f32, f32, f32, i32, vp]
     lib.pb_mlp_cast_bf16.argtypes = [vp, vp, i64, vp]
     lib.pb_surrogate_inputs.argtypes = [vp, i32, vp, i32, vp, vp, vp, i32, i64, i32, vp, vp]
+    lib.pb_surrogate_inputs_rows.argtypes = [vp, i32, vp, i64, i32, vp, vp, vp, vp, i32, i64, i32, vp, vp]
     lib.pb_surrogate_gate.argtypes = [vp, i64, i32, f32, vp, vp, vp, vp, vp, vp]
     lib.pb_gather_rows.argtypes = [vp, i32, vp, vp, i64, vp, vp]
     lib.pb_merge_labels.argtypes = [vp, vp, vp, i64, vp, vp, vp]
@@ -52,6 +53,7 @@ def _bind(lib: ctypes.CDLL) -> None:
         "pb_mlp_adamw",
         "pb_mlp_cast_bf16",
         "pb_surrogate_inputs",
+        "pb_surrogate_inputs_rows",
         "pb_surrogate_gate",
         "pb_gather_rows",
         "pb_merge_labels",
@@ -183,21 +185,31 @@ class MLPSurrogate:
         self.shift = mean.to(torch.float32).contiguous()
         self.scale = torch.where(std > 0, 1.0 / std, torch.zeros_like(std)).to(torch.float32).contiguous()
 
-    def inputs(self, ic: torch.Tensor, params: torch.Tensor | None) -> torch.Tensor:
-        """BF16 network inputs from FP32 ICs (n, S) and one FP64 parameter row."""
+    def inputs(self, ic: torch.Tensor, params: torch.Tensor | None,
+               param_index: torch.Tensor | None = None) -> torch.Tensor:
+        """BF16 network inputs from FP32 ICs (n, S) and FP64 parameters: one row for
+        every IC, or with ``param_index`` (n,) int32 a table ``params`` (P, n_params)
+        whose row param_index[r] goes with IC r (a parameter study)."""
         lib = L.load()
         _bind(lib)
         n, S = ic.shape
-        npar = 0 if params is None else int(params.numel())
+        prm = None if params is None else params.to(self.dev, torch.float64)
+        if prm is not None and prm.dim() == 1:
+            prm = prm[None]
+        rows, npar = (0, 0) if prm is None else (int(prm.shape[0]), int(prm.shape[1]))
         if S + npar != self.d_raw:
             raise ValueError(f"surrogate expects {self.d_raw} inputs, got {S}+{npar}")
+        if param_index is None and rows > 1:
+            raise ValueError("a parameter table needs the row of every IC (param_index)")
         out = torch.empty((n, self.d_in), dtype=torch.bfloat16, device=self.dev)
         s = torch.cuda.current_stream(self.dev).cuda_stream
         icc = ic.to(self.dev, torch.float32).contiguous()
-        prm = None if params is None else params.to(self.dev, torch.float64).contiguous()
+        prm = None if prm is None else prm.contiguous()
+        pidx = None if param_index is None else param_index.to(self.dev, torch.int32).contiguous()
         freq = self.freq if self.n_freq > 0 else None
-        L.check(lib.pb_surrogate_inputs(_p(icc), S, _p(prm), npar, _p(self.shift), _p(self.scale), _p(freq),
-                                        self.n_freq, n, self.d_in, _p(out), s), "pb_surrogate_inputs")
+        L.check(lib.pb_surrogate_inputs_rows(_p(icc), S, _p(prm), rows, npar, _p(pidx), _p(self.shift),
+                                             _p(self.scale), _p(freq), self.n_freq, n, self.d_in, _p(out), s),
+                "pb_surrogate_inputs_rows")
         return out
 
     # -- forward / backward ----------------------------------------------------

@@ -360,3 +360,71 @@ def test_active_fit_on_the_tensor_cores_gates_duffing_within_delta_bs():
     dbs = (torch.bincount(label.long(), minlength=6) - torch.bincount(ref.long(), minlength=6)).abs().max() / 20000
     assert float(dbs) <= 0.005
     assert float((label == ref).double().mean()) >= 0.99
+
+
+@pytest.mark.gpu
+def test_row_indexed_inputs_and_an_index_out_of_range():
+    """pb_surrogate_inputs_rows: each IC takes its own parameter row; a row index
+    outside the table gives NaN inputs, and the gate routes such rows."""
+    from pybasin_b200.surrogate import MLPSurrogate
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(5, 3, hidden=32, depth=2, seed=1, device=dev, n_freq=4, freq_scale=0.5, pad_inputs=True)
+    g = torch.Generator().manual_seed(2)
+    ic = (torch.rand(500, 2, generator=g) * 2 - 1).to(dev)
+    table = torch.tensor([[0.1, t, 1.0] for t in np.linspace(0.1, 1.0, 7)], dtype=torch.float64, device=dev)
+    grp = torch.randint(0, 7, (500,), generator=g, dtype=torch.int32).to(dev)
+    raw = torch.cat([ic, table.float()[grp.long()]], dim=1)
+    net.fit_normalisation(raw)
+    x = net.inputs(ic, table, grp).float()
+    z = (raw - net.shift) * net.scale
+    ph = 2 * np.pi * (z.double() @ net.freq.double().T)
+    ref = torch.cat([z.double(), torch.sin(ph), torch.cos(ph)], dim=1).float().to(torch.bfloat16).float()
+    assert (x[:, : net.d_used] - ref).abs().max().item() <= 2.0 ** -7 + 1e-6
+    bad = grp.clone()
+    bad[3] = 7
+    xb = net.inputs(ic, table, bad).float()
+    assert torch.isnan(xb[3, 2:5]).all() and torch.isfinite(xb[4]).all()
+
+
+@pytest.mark.gpu
+def test_gated_pendulum_torque_sweep_matches_the_integrator_per_point():
+    """The surrogate of a parameter study sees each IC's torque: fit on random and
+    actively chosen ICs across 16 torque points, then the gated labels of fresh
+    ICs against the integrator's, per point.  A 25 % audit (about 1,000 confident
+    audited labels per point) lets points whose confident labels disagree with the
+    integrator too often fall back to it: at 5,000 ICs per point a basin-stability
+    difference of 0.005 is 25 labels, which a smaller audit slice does not resolve."""
+    from pybasin_b200 import studies as S
+    from pybasin_b200.gated import SurrogateGatedPipeline
+
+    dev = torch.device("cuda:0")
+    rows = np.array([[0.1, t, 1.0] for t in np.linspace(0.1, 1.0, 16)])
+    pipe = S.pendulum_pipeline("mixed", rows, dev)
+    gated = SurrogateGatedPipeline(pipe, hidden=128, depth=3, threshold=0.95, audit_fraction=0.25)
+
+    def sample(n, seed):
+        y0 = S.uniform_ics(*S.PENDULUM_BOX, n, seed).to(dev)
+        grp = torch.from_numpy(np.random.default_rng(seed).integers(0, 16, n).astype(np.int32)).to(dev)
+        return y0, grp
+
+    yr, gr = sample(12000, 1)
+    yp, gp = sample(60000, 3)
+    info = gated.fit(yr, yp, n_active=6000, epochs=16, batch=2048, group_random=gr, group_pool=gp)
+    y0, grp = sample(80000, 2)
+    ref_lab, ref_cnt = pipe.run_device(y0, group=grp)
+    ref_lab, ref_cnt = ref_lab.clone(), ref_cnt.clone()
+    label, counts, stats = gated.run_device(y0, grp)
+    torch.cuda.synchronize()
+    assert info.summary()["train_error_flag"] == 0
+    assert counts.shape == (16, 3) and int(counts.sum()) == 80000
+    assert stats.integrated_fraction < 0.9
+    n_p = ref_cnt.sum(dim=1).double()
+    dbs = ((counts[:, :2] - ref_cnt[:, :2]).abs().max(dim=1).values.double() / n_p).max().item()
+    assert dbs <= 0.005
+    assert float((label == ref_lab).double().mean()) >= 0.995
+    # a fallen-back point carries the integrator's labels exactly
+    bad = gated.last_fallback_points.cpu().numpy()
+    for q in np.nonzero(bad)[0]:
+        sel = (grp == int(q))
+        assert torch.equal(label[sel], ref_lab[sel])
