@@ -718,6 +718,42 @@ def run_sweep_surrogate(args, dev, rank: int, world: int, dist_on: bool, flush, 
     }
 
 
+def profile_surrogate(args) -> None:
+    """``--only surrogate``: the surrogate workload's steps alone (warm-up, then
+    ``steps`` steps each in an NVTX range "surrogate_step"), for a profiler; prints
+    the mean step time, no comparisons."""
+    from pybasin_b200.gated import SurrogateGatedPipeline
+
+    dev = torch.device(f"cuda:{int(os.environ.get('LOCAL_RANK', '0'))}")
+    torch.cuda.set_device(dev)
+    n = args.c5_n
+    y0 = seeded_ics(n, 7).to(dev)
+    yr, pool = seeded_ics(C5_RANDOM, 1042).to(dev), seeded_ics(C5_POOL, 2042).to(dev)
+    pipe = make_pipeline(dev, "mixed", "probed")
+    gated = SurrogateGatedPipeline(pipe, hidden=256, depth=4, threshold=0.95, audit_fraction=0.01,
+                                   freq_scale=C5_FREQ_SCALE)
+
+    def step():
+        gated.fit(yr, pool, n_active=C5_ACTIVE, epochs=C5_EPOCHS, batch=C5_BATCH, lr=C5_LR)
+        return gated.run_device(y0)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("surrogate_step")
+        e0.record()
+        _, _, st = step()
+        e1.record()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        ts.append(e0.elapsed_time(e1))
+    print(json.dumps({"only": "surrogate", "n_ic": n, "ms_per_step": statistics.mean(ts),
+                      "routed_fraction": st.routed_fraction}), flush=True)
+
+
 def run_b200_arm(args) -> None:
     from pybasin_b200 import _lib as L
 
@@ -965,9 +1001,13 @@ def main() -> None:
     ap.add_argument("--no-surrogate", action="store_true", help="time the fused integrator path alone")
     ap.add_argument("--c5-n", type=int, default=C5_N, help="ICs of the surrogate workload (0: skip it)")
     ap.add_argument("--no-studies", action="store_true", help="skip the parameter studies at full size")
+    ap.add_argument("--only", default="all", choices=["all", "surrogate"],
+                    help="surrogate: that workload's steps alone, NVTX-marked, for a profiler")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.only == "surrogate":
+        profile_surrogate(args)
     else:
         run_b200_arm(args)
 
