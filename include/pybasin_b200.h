@@ -569,6 +569,47 @@ int pb_train_adamw(int32_t n_tensors, float* const* w, void* const* w_bf16, void
 int pb_train_gather(const void* x_bf16, int32_t width, const int32_t* labels, const int32_t* idx, int64_t n,
                     void* out_bf16, void* out_t, int32_t* labels_out, void* stream);
 
+/* ---- fused training step (tcgen05) ------------------------------------------
+ * No counterpart in the reference.  One minibatch step of an MLP with layer
+ * widths dims[0..n_layers] (GELU between layers, softmax cross-entropy on the
+ * dims[n_layers] logits, AdamW) as two launches: one CTA per 128 rows runs the
+ * forward pass, the loss and the input gradients of its rows; one cluster per
+ * weight tile sums the weight gradient over the minibatch and applies AdamW.
+ * Limits: 1 <= n_layers <= PB_TRAIN_MAX_LAYERS, dims[0] a multiple of 8 in
+ * [8, 256], hidden widths multiples of 16 in [16, 256], 2 <= dims[n_layers] <= 32.
+ *
+ * Parameters live augmented: layer l is an FP32 (npad_l x kaug_l) row-major
+ * matrix [W_l | b_l | 0] (npad_l = dims[l+1] rounded up to 16 with zero rows,
+ * kaug_l = dims[l] + 1 rounded up to 16; the bias in column dims[l]), all layers
+ * concatenated at element offsets aug_off_l; AdamW moments m1, m2 have the same
+ * shape; w_img holds the BF16 weight images the kernels read (img_bytes). */
+#define PB_TRAIN_MAX_LAYERS 8
+/* Sizes for a network and minibatch size `batch`: out[0] = img_bytes, out[1] =
+ * scratch bytes, out[2] = augmented elements; then per layer l: out[3+4l] =
+ * kaug_l, out[4+4l] = npad_l, out[5+4l] = aug_off_l, out[6+4l] = byte offset
+ * of the layer's image.  out_len >= 3 + 4 n_layers. */
+int pb_train_fused_geometry(int32_t n_layers, const int32_t* dims, int32_t batch, int64_t* out, int32_t out_len);
+/* w_img = the BF16 images of the augmented weights w_aug (device). */
+int pb_train_fused_pack(int32_t n_layers, const int32_t* dims, const float* w_aug, void* w_img, void* stream);
+/* One minibatch step over rows[0..M) (M <= batch) of the training set x (BF16,
+ * n_rows x dims[0], 16-byte aligned) with int32 labels; a row index outside
+ * [0, n_rows) is not read (the row counts as zero and error_flag is set).  grad NULL: AdamW step `step`
+ * (>= 1; weight decay on the weights, not the bias) on w_aug, m1, m2, w_img.
+ * grad non-NULL: the minibatch-mean gradient (augmented layout) is written to
+ * grad and nothing is updated.  loss_sum / correct (optional) accumulate the
+ * summed loss and argmax hits; error_flag (optional) is set to 1 when a wait gave
+ * up.  scratch: the geometry's scratch bytes for `batch`, 16-byte aligned. */
+int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf16, const int32_t* labels,
+                        int32_t n_rows, const int32_t* rows, int32_t M, int32_t batch, float* w_aug, float* m1, float* m2,
+                        void* w_img, void* scratch, float* grad, float lr, float beta1, float beta2, float eps,
+                        float weight_decay, int32_t step, float* loss_sum, int32_t* correct, int32_t* error_flag,
+                        void* stream);
+/* AdamW step from a gradient in the augmented layout (e.g. after a data-parallel
+ * all-reduce of pb_train_fused_step's grad output), refreshing w_img. */
+int pb_train_fused_adamw(int32_t n_layers, const int32_t* dims, float* w_aug, float* m1, float* m2, const float* grad,
+                         void* w_img, float lr, float beta1, float beta2, float eps, float weight_decay, int32_t step,
+                         void* stream);
+
 /* Human-readable text of a pb_status (src/zigode/zig_solver.py:333-341). */
 const char* pb_error_string(int32_t status);
 

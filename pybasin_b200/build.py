@@ -17,7 +17,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB_NAME = "libpybasin_b200.so"
-SOURCES = ["pb_api.cu", "pb_noalloc.cu", "pb_mlp.cu", "pb_order.cu", "pb_rtc.cu", "pb_mlp_tc.cu", "pb_train_tc.cu"]
+SOURCES = ["pb_api.cu", "pb_noalloc.cu", "pb_mlp.cu", "pb_order.cu", "pb_rtc.cu", "pb_mlp_tc.cu", "pb_train_tc.cu",
+           "pb_train_fused.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

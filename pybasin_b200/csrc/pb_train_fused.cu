@@ -1,0 +1,1161 @@
+// Fused surrogate training step on the 5th-generation tensor cores.
+//
+// One minibatch step of the MLP (layers dims[0] -> ... -> dims[L], GELU between,
+// softmax cross-entropy on the logits, AdamW) is two launches:
+//
+//   k_train_fb   one CTA per 128-row tile of the minibatch runs the whole layer
+//                chain of its rows: it gathers its input rows, runs every layer's
+//                forward GEMM, the cross entropy, and every layer's input-gradient
+//                GEMM, keeping activations and gradients in shared memory.  For
+//                the weight gradients it leaves each layer's input X_l and output
+//                gradient dZ_l of its rows in global scratch (as images of the
+//                shared-memory operand layout), and GELU'(Z_l) for its own
+//                backward pass.
+//   k_train_dw   one thread-block cluster per tile of a weight matrix: the CTAs of
+//                the cluster split the minibatch's row tiles, each accumulates
+//                dW = dZ^T X over its rows in tensor memory, the partials are
+//                summed over the cluster through distributed shared memory in a
+//                fixed order (so a step is deterministic), and each CTA applies
+//                AdamW to its share of the tile and refreshes the BF16 image.
+//
+// The bias rides in the GEMMs: every layer input carries a column of ones after
+// its features (X_aug = [X | 1 | 0 ...], K padded to 16), and the weights are kept
+// augmented, W_aug = [W | b | 0 ...] (rows padded to 16), so the forward product
+// already holds the bias and the weight gradient's ones column is the bias
+// gradient.
+//
+// Operand layout: K-major core matrices (8 rows x 16 bytes; core (row/8, k/8) of
+// a block at ((row/8) * (width/8) + k/8) * 128 bytes), in column blocks:
+//   * an activation image (128 rows x K_aug) is split into chunks of 64 columns,
+//     the ones-and-padding tail joined to the last chunk (widths 16..80);
+//   * a gradient image (128 rows x N_pad) into pieces of 64 columns;
+//   * a weight image into tiles (64-row piece of N_pad) x (chunk of K_aug).
+// The same bytes serve both orientations: a weight tile is the K-major B operand
+// of the forward GEMM (n = output, k = input) and, read with an MN-major
+// descriptor, the B operand of the input-gradient GEMM (n = input, k = output);
+// the images of X and dZ are the K-major A operands of the layer chain and, read
+// MN-major, the operands of the weight-gradient GEMM (k = rows).  No transposed
+// copy is ever written.  For the MN-major (no swizzle) descriptor the stride byte
+// offset is the core stride along M/N and the leading byte offset the stride
+// between groups of 8 along K.
+//
+// Every mbarrier wait is bounded (on a timeout the thread records an error and
+// skips the work that depended on it, but still passes every barrier); there is
+// no counterpart in the reference (its pipeline has no learned part).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include <cmath>
+
+#include "pb_gelu.cuh"
+#include "pybasin_b200.h"
+
+namespace {
+
+constexpr int kRows = 128;                 // rows of a tile = MMA M = TMEM lanes
+constexpr int kMaxLayers = PB_TRAIN_MAX_LAYERS;
+constexpr int kMaxWidth = 256;             // largest layer width
+constexpr int kMaxChunks = 5;              // chunks of an activation image (K_aug <= 272)
+constexpr int kMaxPieces = 4;              // 64-column pieces of a layer output (N_pad <= 256)
+constexpr int kMaxKaug = 272;
+constexpr int kMaxClasses = 32;            // the cross entropy reads one 32-column TMEM load
+constexpr long long kWaitPolls = 1ll << 22;
+
+// k_train_fb: 16 epilogue warps (TMEM lane quarter w % 4, output piece w / 4),
+// one MMA-issuing warp, one warp streaming the weight tiles
+constexpr int kEpiWarps = 16;
+constexpr int kMmaWarp = kEpiWarps;
+constexpr int kLoadWarp = kEpiWarps + 1;
+constexpr int kFbThreads = (kEpiWarps + 2) * 32;
+constexpr int kLayerBarThreads = (kEpiWarps + 1) * 32;  // epilogue warps + the MMA warp
+constexpr int kRing = 8;                                 // weight-tile slots
+constexpr int kTileBytes = 64 * 80 * 2;                  // largest weight tile
+constexpr int kImgBytes = kRows * kMaxKaug * 2;          // largest activation / gradient image
+constexpr int kFbTail = 1024;                           // barriers, flags, the tile's labels
+// the whole 227 KB: the operand reads of the last ring slots stay inside the
+// allocation whatever stride a descriptor field is read as
+constexpr int kFbSmem = 227 * 1024;
+
+// k_train_dw
+constexpr int kDwThreads = 256;
+constexpr int kDwStages = 3;
+constexpr int kDwABytes = kRows * kRows * 2;  // 128 outputs x 128 rows
+constexpr int kDwBBytes = kRows * 80 * 2;     // 128 rows x a chunk of <= 80 inputs
+constexpr int kDwStageBytes = kDwABytes + kDwBBytes;
+constexpr int kDwTail = 256;
+constexpr int kDwSmem = 227 * 1024;  // as kFbSmem
+constexpr int kMaxCluster = 8;
+constexpr int kMaxDwTiles = kMaxLayers * 2 * kMaxChunks;
+
+// ---- geometry ----------------------------------------------------------------
+
+struct LayerGeo {
+    int din, dout;        // real widths
+    int kaug;             // K of the forward GEMM: din + 1 (ones) rounded up to 16
+    int npad;             // output rows padded to 16
+    int n_chunks;         // chunks of the input image
+    int c0[kMaxChunks], cw[kMaxChunks];
+    int n_pieces;         // 64-row pieces of npad
+    int p0[kMaxPieces], ph[kMaxPieces];
+    int64_t w_off;        // byte offset of this layer's weight image in the image buffer
+    int64_t aug_off;      // element offset of this layer in the concatenated augmented (npad x kaug) arrays
+    int64_t x_off, z_off, g_off;  // byte offsets in the scratch of the layer's X / dZ / GELU' images (tile 0)
+    int64_t x_tile, z_tile, g_tile;  // bytes per row tile
+};
+
+struct Geo {
+    int n_layers, tiles;
+    LayerGeo l[kMaxLayers];
+    int64_t img_bytes, scratch_bytes, aug_elems;
+};
+
+// Chunks of an image of `real` columns followed by the ones column and padding
+// to `aug` (a multiple of 16): 64-column pieces of the real part, the tail on the
+// last piece, and a last chunk of 16 or less joined to the one before it.
+__host__ __device__ inline int split_chunks(int real, int aug, int* c0, int* cw)
+{
+    int n = 0;
+    for (int c = 0; c < real; c += 64) {
+        c0[n] = c;
+        cw[n] = (real - c < 64) ? real - c : 64;
+        ++n;
+    }
+    if (n == 0) {
+        c0[0] = 0;
+        cw[0] = 0;
+        n = 1;
+    }
+    cw[n - 1] = aug - c0[n - 1];  // the tail joins the last piece
+    if (n > 1 && cw[n - 1] <= 16) {
+        cw[n - 2] += cw[n - 1];
+        --n;
+    }
+    return n;
+}
+
+inline int geo_build(int n_layers, const int32_t* dims, int batch, Geo* g)
+{
+    if (n_layers < 1 || n_layers > kMaxLayers || batch < 1 || !dims) return PB_EINVAL;
+    if (dims[0] < 8 || dims[0] > kMaxWidth || dims[0] % 8) return PB_EINVAL;
+    for (int l = 1; l < n_layers; ++l)
+        if (dims[l] < 16 || dims[l] > kMaxWidth || dims[l] % 16) return PB_EINVAL;
+    if (dims[n_layers] < 2 || dims[n_layers] > kMaxClasses) return PB_EINVAL;
+    g->n_layers = n_layers;
+    g->tiles = (batch + kRows - 1) / kRows;
+    int64_t img = 0, aug = 0, scr = 0;
+    for (int l = 0; l < n_layers; ++l) {
+        LayerGeo& L = g->l[l];
+        L.din = dims[l];
+        L.dout = dims[l + 1];
+        L.kaug = (L.din + 1 + 15) / 16 * 16;
+        L.npad = (L.dout + 15) / 16 * 16;
+        L.n_chunks = split_chunks(L.din, L.kaug, L.c0, L.cw);
+        L.n_pieces = 0;
+        for (int o = 0; o < L.npad; o += 64) {
+            L.p0[L.n_pieces] = o;
+            L.ph[L.n_pieces] = L.npad - o < 64 ? L.npad - o : 64;
+            ++L.n_pieces;
+        }
+        L.w_off = img;
+        img += static_cast<int64_t>(L.npad) * L.kaug * 2;
+        L.aug_off = aug;
+        aug += static_cast<int64_t>(L.npad) * L.kaug;
+        L.x_tile = static_cast<int64_t>(kRows) * L.kaug * 2;
+        L.z_tile = static_cast<int64_t>(kRows) * L.npad * 2;
+        L.g_tile = l + 1 < n_layers ? static_cast<int64_t>(kRows) * L.dout * 2 : 0;
+    }
+    for (int l = 0; l < n_layers; ++l) {
+        LayerGeo& L = g->l[l];
+        L.x_off = scr;
+        scr += L.x_tile * g->tiles;
+        L.z_off = scr;
+        scr += L.z_tile * g->tiles;
+        L.g_off = scr;
+        scr += L.g_tile * g->tiles;
+    }
+    g->img_bytes = img;
+    g->aug_elems = aug;
+    g->scratch_bytes = scr;
+    return PB_SUCCESS;
+}
+
+// byte offset of weight-image element (o, i) of a layer, relative to the layer's image
+__host__ __device__ inline int64_t w_elem(const LayerGeo& L, int o, int i)
+{
+    int p = o >> 6, c = 0;
+    while (c + 1 < L.n_chunks && i >= L.c0[c + 1]) ++c;
+    const int h = L.ph[p], w = L.cw[c];
+    const int64_t tile = static_cast<int64_t>(L.p0[p]) * L.kaug * 2 + static_cast<int64_t>(h) * L.c0[c] * 2;
+    const int ol = o - L.p0[p], il = i - L.c0[c];
+    return tile + (((ol >> 3) * (w >> 3) + (il >> 3)) << 7) + ((ol & 7) << 4) + ((il & 7) << 1);
+}
+
+// byte offset of the weight tile (piece p, chunk c) of a layer
+__host__ __device__ inline int64_t w_tile(const LayerGeo& L, int p, int c)
+{
+    return static_cast<int64_t>(L.p0[p]) * L.kaug * 2 + static_cast<int64_t>(L.ph[p]) * L.c0[c] * 2;
+}
+
+// byte offset of element (r, k) in an image whose columns are split into blocks
+// (start b0[j], width bw[j]); blocks are stored one after the other
+__device__ __forceinline__ uint32_t img_off(const int* b0, const int* bw, int j, int r, int k)
+{
+    const int kl = k - b0[j];
+    return static_cast<uint32_t>(b0[j]) * (kRows * 2) + (((r >> 3) * (bw[j] >> 3) + (kl >> 3)) << 7) +
+           ((r & 7) << 4) + ((kl & 7) << 1);
+}
+
+// ---- device helpers ----------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: start, leading / stride byte offsets (16-byte
+// units), version 1, base offset 0, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B; a_mn / b_mn
+// select the MN-major (transposed) operand layouts
+__device__ __forceinline__ uint32_t instr_desc(int M, int N, bool a_mn, bool b_mn)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn ? 1u << 15 : 0u) | (b_mn ? 1u << 16 : 0u) |
+           (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// waits for the phase of the given parity; gives up (false) after kWaitPolls polls
+// or at once when *abort is set
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort)
+{
+    for (long long i = 0; i < kWaitPolls; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 1023) == 1023 && *abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ uint32_t pack_f16(float a, float b)
+{
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ float2 unpack_f16(uint32_t u)
+{
+    return __half22float2(*reinterpret_cast<const __half2*>(&u));
+}
+
+using pb::gelu;
+using pb::gelu_grad;
+
+}  // namespace
+
+namespace {
+
+// GELU and its derivative sharing one tanh (the forms of pb_gelu.cuh)
+__device__ __forceinline__ void gelu_both(float x, float& g, float& d)
+{
+    const float x2 = x * x;
+    const float t = pb::tanh_approx(x * fmaf(pb::kGeluB, x2, pb::kGeluA));
+    const float hx = 0.5f * x;
+    g = fmaf(hx, t, hx);
+    const float du = fmaf(pb::kGeluB3, x2, pb::kGeluA);
+    d = fmaf(hx * du, fmaf(-t, t, 1.f), 0.5f * (1.f + t));
+}
+
+struct FbArgs {
+    Geo geo;
+    const __nv_bfloat16* x;  // training inputs (n_rows x dims[0]) BF16
+    const int32_t* labels;   // (n_rows)
+    const int32_t* rows;     // the minibatch's rows of x (M)
+    int n_rows;              // rows of x (and labels)
+    int M;
+    float scale;             // 1 / M: the loss is the minibatch mean
+    const uint8_t* w_img;    // BF16 weight images, all layers
+    uint8_t* scratch;        // X / dZ / GELU' images of the minibatch's row tiles
+    float* loss_sum;
+    int32_t* correct;
+    int32_t* error;
+};
+
+// Shared memory of k_train_fb: two image buffers (the layer chain alternates
+// between them), the weight-tile ring, then barriers and flags.
+struct FbSmem {
+    uint64_t full[kRing], empty[kRing], mdone[kMaxPieces];
+    uint32_t tmem;
+    int abort;
+    int y[kRows];
+};
+static_assert(sizeof(FbSmem) <= kFbTail, "k_train_fb: barrier block");
+static_assert(2 * kImgBytes + kRing * kTileBytes + kFbTail <= kFbSmem, "k_train_fb: shared memory");
+
+// Epilogue of one forward piece of a hidden layer: z (TMEM columns p0 .. p0 + h)
+// -> GELU(z) into the next layer's input image, GELU'(z) (FP16) to global.
+__device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* xo,
+                                                const LayerGeo& Ln, int chunk, uint8_t* gimg)
+{
+    for (int cc = 0; cc < ncols; cc += 32) {
+        float z[32];
+        if (ncols - cc >= 32) {
+            uint32_t v[32];
+            tmem_ld32(tm + static_cast<uint32_t>(cc), v);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) z[j] = __uint_as_float(v[j]);
+        } else {
+            uint32_t v[16];
+            tmem_ld16(tm + static_cast<uint32_t>(cc), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) z[j] = __uint_as_float(v[j]);
+#pragma unroll
+            for (int j = 16; j < 32; ++j) z[j] = 0.f;
+        }
+        const int groups = (ncols - cc >= 32 ? 32 : 16) >> 3;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q >= groups) break;
+            uint32_t hx[4], hd[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float g0, d0, g1, d1;
+                gelu_both(z[q * 8 + 2 * k], g0, d0);
+                gelu_both(z[q * 8 + 2 * k + 1], g1, d1);
+                hx[k] = pack_bf16(g0, g1);
+                hd[k] = pack_f16(d0, d1);
+            }
+            const int col = col0 + cc + q * 8;
+            *reinterpret_cast<uint4*>(xo + img_off(Ln.c0, Ln.cw, chunk, r, col)) = make_uint4(hx[0], hx[1], hx[2], hx[3]);
+            *reinterpret_cast<uint4*>(gimg + ((static_cast<int64_t>(col >> 3) * kRows + r) << 4)) =
+                make_uint4(hd[0], hd[1], hd[2], hd[3]);
+        }
+    }
+}
+
+// Epilogue of one input-gradient piece: dZ_below = acc * GELU'(Z_below) (TMEM
+// columns c0 .. c0 + n) into the gradient image of the layer below.
+__device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* zo, const LayerGeo& Lb,
+                                        int piece, const uint8_t* gimg)
+{
+    for (int cc = 0; cc < ncols; cc += 32) {
+        const int n = ncols - cc >= 32 ? 32 : 16;
+        uint4 gd[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (q * 8 < n)
+                gd[q] = __ldg(reinterpret_cast<const uint4*>(gimg + ((static_cast<int64_t>((col0 + cc) / 8 + q) * kRows + r) << 4)));
+        float a[32];
+        if (n == 32) {
+            uint32_t v[32];
+            tmem_ld32(tm + static_cast<uint32_t>(cc), v);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) a[j] = __uint_as_float(v[j]);
+        } else {
+            uint32_t v[16];
+            tmem_ld16(tm + static_cast<uint32_t>(cc), v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) a[j] = __uint_as_float(v[j]);
+#pragma unroll
+            for (int j = 16; j < 32; ++j) a[j] = 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q * 8 >= n) break;
+            const uint32_t gw[4] = {gd[q].x, gd[q].y, gd[q].z, gd[q].w};
+            uint32_t h[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float2 d = unpack_f16(gw[k]);
+                h[k] = pack_bf16(a[q * 8 + 2 * k] * d.x, a[q * 8 + 2 * k + 1] * d.y);
+            }
+            *reinterpret_cast<uint4*>(zo + img_off(Lb.p0, Lb.ph, piece, r, col0 + cc + q * 8)) =
+                make_uint4(h[0], h[1], h[2], h[3]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constant__ FbArgs p)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    // image buffer b at smem + b * kImgBytes
+    uint8_t* ring = smem + 2 * kImgBytes;
+    FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kTileBytes);
+    volatile int* abort = &sh->abort;
+    const Geo& G = p.geo;
+    const int NL = G.n_layers;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile = blockIdx.x;
+    const int m0 = tile * kRows;
+    const int mt = min(kRows, p.M - m0);  // valid rows of this tile
+
+    if (tid == 0) {
+        for (int s = 0; s < kRing; ++s) {
+            mbar_init(smem_u32(&sh->full[s]), 1);
+            mbar_init(smem_u32(&sh->empty[s]), 1);
+        }
+        for (int j = 0; j < kMaxPieces; ++j) mbar_init(smem_u32(&sh->mdone[j]), 1);
+        sh->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
+                     "r"(256)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = sh->tmem;
+
+    if (warp == kLoadWarp) {
+        // ---- weight tiles into the ring, in the order the MMA warp consumes them
+        if (lane == 0) {
+            uint32_t u = 0;
+            auto put = [&](const LayerGeo& L, int pc, int cc) {
+                const uint32_t s = u % kRing, round = u / kRing;
+                ++u;
+                if (round > 0 && !mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1u, abort)) return;
+                const uint32_t bytes = static_cast<uint32_t>(L.ph[pc]) * L.cw[cc] * 2u;
+                mbar_expect_tx(smem_u32(&sh->full[s]), bytes);
+                bulk_load(smem_u32(ring + s * kTileBytes), p.w_img + L.w_off + w_tile(L, pc, cc), bytes,
+                          smem_u32(&sh->full[s]));
+            };
+            for (int l = 0; l < NL && !*abort; ++l) {
+                const LayerGeo& L = G.l[l];
+                for (int pc = 0; pc < L.n_pieces; ++pc)
+                    for (int cc = 0; cc < L.n_chunks; ++cc) put(L, pc, cc);
+            }
+            for (int l = NL - 1; l >= 1 && !*abort; --l) {
+                const LayerGeo& L = G.l[l];
+                for (int cc = 0; cc < L.n_chunks; ++cc)
+                    for (int pc = 0; pc < L.n_pieces; ++pc) put(L, pc, cc);
+            }
+        }
+        __syncwarp();
+        __syncthreads();
+        if (tid == kLoadWarp * 32 && *abort && p.error) atomicExch(p.error, 1);
+        return;
+    }
+
+    // ---- the row tile's inputs: rows of x by the minibatch's indices, the ones
+    // column after them, zero rows past the minibatch
+    if (warp < kEpiWarps) {
+        const LayerGeo& L0 = G.l[0];
+        const int pieces = L0.kaug >> 3;
+        for (int idx = tid; idx < kRows * pieces; idx += kEpiWarps * 32) {
+            const int r = idx & (kRows - 1), col = (idx >> 7) << 3;
+            int c = 0;
+            while (c + 1 < L0.n_chunks && col >= L0.c0[c + 1]) ++c;
+            uint8_t* dst = smem + img_off(L0.c0, L0.cw, c, r, col);
+            const int row = r < mt ? __ldg(p.rows + m0 + r) : -1;
+            const bool in_range = row >= 0 && row < p.n_rows;
+            if (r < mt && !in_range && col == 0) sh->abort = 1;  // a row index outside x: reported, not read
+            if (in_range && col < L0.din) {
+                const int64_t src = static_cast<int64_t>(row) * L0.din + col;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(p.x + src) : "memory");
+            } else {
+                const uint32_t one = (r < mt && col == L0.din) ? 0x3F80u : 0u;  // BF16 1.0 in the first slot
+                *reinterpret_cast<uint4*>(dst) = make_uint4(one, 0u, 0u, 0u);
+            }
+        }
+        for (int r = tid; r < kRows; r += kEpiWarps * 32) {
+            const int row = r < mt ? __ldg(p.rows + m0 + r) : -1;
+            sh->y[r] = (row >= 0 && row < p.n_rows) ? __ldg(p.labels + row) : -1;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        proxy_fence();
+    }
+    named_sync(1, kLayerBarThreads);
+    if (tid == 0) {
+        bulk_store(p.scratch + G.l[0].x_off + tile * G.l[0].x_tile, smem_u32(smem),
+                   static_cast<uint32_t>(G.l[0].x_tile));
+        bulk_commit();
+    }
+
+    const int quarter = warp & 3, grp = warp >> 2;
+    const int r = quarter * 32 + lane;  // this thread's row (TMEM lane)
+    const uint32_t tm_row = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+    const bool leader = (tid & 127) == 0 && warp < kEpiWarps;
+    uint32_t u = 0;                      // weight tiles consumed (MMA warp)
+    uint32_t uses = 0;                   // waits on mdone[grp] so far (epilogue warps)
+    int cur = 0;
+    float loss = 0.f;
+    int hits = 0;
+
+    // ---- forward
+    for (int l = 0; l < NL; ++l) {
+        const LayerGeo& L = G.l[l];
+        const bool last = l + 1 == NL;
+        if (warp == kMmaWarp) {
+            if (lane == 0) {
+                tc_after();
+                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
+                for (int pc = 0; pc < L.n_pieces; ++pc) {
+                    const uint32_t idesc = instr_desc(kRows, L.ph[pc], false, false);
+                    for (int cc = 0; cc < L.n_chunks; ++cc) {
+                        const uint32_t s = u % kRing, round = u / kRing;
+                        ++u;
+                        const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
+                        tc_after();
+                        const uint32_t sbo = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;
+                        const uint32_t wa = smem_u32(ring + s * kTileBytes);
+                        for (int ks = 0; ok && ks < (L.cw[cc] >> 4); ++ks)
+                            mma_bf16(tmem + static_cast<uint32_t>(L.p0[pc]),
+                                     smem_desc(a0 + L.c0[cc] * (kRows * 2) + ks * 256u, 128u, sbo),
+                                     smem_desc(wa + ks * 256u, 128u, sbo), idesc, (cc > 0 || ks > 0) ? 1u : 0u);
+                        mma_commit(smem_u32(&sh->empty[s]));
+                    }
+                    mma_commit(smem_u32(&sh->mdone[pc]));
+                }
+            }
+            __syncwarp();
+        } else if (grp < L.n_pieces) {
+            const int pc = grp;
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone[pc]), uses & 1u, abort));
+            tc_after();
+            uint8_t* out = smem + (cur ^ 1) * kImgBytes;
+            if (!last) {
+                const LayerGeo& Ln = G.l[l + 1];
+                uint8_t* gimg = p.scratch + L.g_off + tile * L.g_tile;
+                if (ok) fwd_hidden_cols(tm_row + static_cast<uint32_t>(L.p0[pc]), L.ph[pc], L.p0[pc], r, out, Ln, pc, gimg);
+                if (pc == L.n_pieces - 1) {
+                    // the ones column of the next layer's input, then zeros to its K
+                    for (int col = L.dout; col < Ln.kaug; col += 8) {
+                        const uint32_t one = (r < mt && col == L.dout) ? 0x3F80u : 0u;
+                        *reinterpret_cast<uint4*>(out + img_off(Ln.c0, Ln.cw, pc, r, col)) = make_uint4(one, 0u, 0u, 0u);
+                    }
+                }
+            } else {
+                // softmax cross entropy of the logits (TMEM columns 0 .. npad)
+                uint32_t v[32];
+                if (ok) tmem_ld32(tm_row, v);
+                const int C = L.dout;
+                const int y = sh->y[r];
+                float z[32];
+                float mx = -CUDART_INF_F, zy = 0.f;
+                int arg = 0;
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    z[c] = __uint_as_float(v[c]);
+                    if (c < C && z[c] > mx) {
+                        mx = z[c];
+                        arg = c;
+                    }
+                    if (c == y) zy = z[c];
+                }
+                float se = 0.f;
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    z[c] = c < C ? __expf(z[c] - mx) : 0.f;
+                    se += z[c];
+                }
+                const float inv = 1.f / se;
+                const bool valid = r < mt && ok;
+#pragma unroll
+                for (int c8 = 0; c8 < 32; c8 += 8) {
+                    if (c8 >= L.npad) break;
+                    uint32_t h[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int c = c8 + 2 * k;
+                        const float d0 = valid ? (z[c] * inv - (c == y ? 1.f : 0.f)) * p.scale : 0.f;
+                        const float d1 = valid ? (z[c + 1] * inv - (c + 1 == y ? 1.f : 0.f)) * p.scale : 0.f;
+                        h[k] = pack_bf16(d0, d1);
+                    }
+                    *reinterpret_cast<uint4*>(out + img_off(L.p0, L.ph, 0, r, c8)) = make_uint4(h[0], h[1], h[2], h[3]);
+                }
+                if (valid && y >= 0 && y < C) {
+                    loss = -(zy - mx - __logf(se));
+                    hits = arg == y ? 1 : 0;
+                }
+            }
+            proxy_fence();
+            tc_before();
+            named_sync(2 + pc, 128);
+            if (leader) {
+                if (!last) {
+                    const LayerGeo& Ln = G.l[l + 1];
+                    const uint32_t off = static_cast<uint32_t>(Ln.c0[pc]) * (kRows * 2);
+                    bulk_store(p.scratch + Ln.x_off + tile * Ln.x_tile + off, smem_u32(out) + off,
+                               static_cast<uint32_t>(Ln.cw[pc]) * (kRows * 2));
+                } else {
+                    bulk_store(p.scratch + L.z_off + tile * L.z_tile, smem_u32(out), static_cast<uint32_t>(L.z_tile));
+                }
+                bulk_commit();
+                bulk_wait_read();
+            }
+        }
+        if (warp < kEpiWarps && grp < L.n_pieces) ++uses;
+        named_sync(1, kLayerBarThreads);
+        cur ^= 1;
+    }
+
+    // ---- input gradients, last layer first: dZ_l-1 = (dZ_l W_l) * GELU'(Z_l-1);
+    // output piece j is input chunk j of layer l (its real columns)
+    for (int l = NL - 1; l >= 1; --l) {
+        const LayerGeo& L = G.l[l];
+        const LayerGeo& Lb = G.l[l - 1];
+        if (warp == kMmaWarp) {
+            if (lane == 0) {
+                tc_after();
+                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);  // dZ_l
+                for (int cc = 0; cc < L.n_chunks; ++cc) {
+                    const int N = min(L.cw[cc], L.din - L.c0[cc]);
+                    const uint32_t idesc = instr_desc(kRows, N, false, true);
+                    const uint32_t kstride = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;  // 8 outputs of the tile
+                    for (int pc = 0; pc < L.n_pieces; ++pc) {
+                        const uint32_t s = u % kRing, round = u / kRing;
+                        ++u;
+                        const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
+                        tc_after();
+                        const uint32_t sbo_a = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
+                        const uint32_t wa = smem_u32(ring + s * kTileBytes);
+                        for (int ks = 0; ok && ks < (L.ph[pc] >> 4); ++ks)
+                            mma_bf16(tmem + static_cast<uint32_t>(L.c0[cc]),
+                                     smem_desc(a0 + L.p0[pc] * (kRows * 2) + ks * 256u, 128u, sbo_a),
+                                     smem_desc(wa + ks * 2u * kstride, kstride, 128u), idesc,
+                                     (pc > 0 || ks > 0) ? 1u : 0u);
+                        mma_commit(smem_u32(&sh->empty[s]));
+                    }
+                    mma_commit(smem_u32(&sh->mdone[cc]));
+                }
+            }
+            __syncwarp();
+        } else if (grp < L.n_chunks) {
+            const int cc = grp;
+            const int N = min(L.cw[cc], L.din - L.c0[cc]);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone[cc]), uses & 1u, abort));
+            tc_after();
+            uint8_t* out = smem + (cur ^ 1) * kImgBytes;
+            const uint8_t* gimg = p.scratch + Lb.g_off + tile * Lb.g_tile;
+            if (ok) dx_cols(tm_row + static_cast<uint32_t>(L.c0[cc]), N, L.c0[cc], r, out, Lb, cc, gimg);
+            proxy_fence();
+            tc_before();
+            named_sync(2 + cc, 128);
+            if (leader) {
+                const uint32_t off = static_cast<uint32_t>(Lb.p0[cc]) * (kRows * 2);
+                bulk_store(p.scratch + Lb.z_off + tile * Lb.z_tile + off, smem_u32(out) + off,
+                           static_cast<uint32_t>(Lb.ph[cc]) * (kRows * 2));
+                bulk_commit();
+                bulk_wait_read();
+            }
+        }
+        if (warp < kEpiWarps && grp < L.n_chunks) ++uses;
+        named_sync(1, kLayerBarThreads);
+        cur ^= 1;
+    }
+
+    if (leader) bulk_wait_all();
+    if (warp < kEpiWarps) {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            loss += __shfl_xor_sync(0xffffffffu, loss, o);
+            hits += __shfl_xor_sync(0xffffffffu, hits, o);
+        }
+        if (lane == 0 && grp == 0) {
+            if (p.loss_sum && loss != 0.f) atomicAdd(p.loss_sum, loss);
+            if (p.correct && hits) atomicAdd(p.correct, hits);
+        }
+    }
+    tc_before();
+    __syncthreads();
+    if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+}
+
+// ---- weight gradients and AdamW ---------------------------------------------
+
+struct DwTile {
+    int layer, o0, oh, chunk;  // outputs [o0, o0 + oh) x input chunk
+};
+
+struct DwArgs {
+    Geo geo;
+    DwTile t[kMaxDwTiles];
+    int n_tiles;
+    int M;
+    const uint8_t* scratch;
+    uint8_t* w_img;
+    float* w_aug;
+    float* m1;
+    float* m2;
+    float* grad;  // non-null: write the summed gradient here, no AdamW
+    float lr, b1, b2, eps, wd, bc1, bc2;
+    int32_t* error;
+};
+
+struct DwSmem {
+    uint64_t full[kDwStages], empty[kDwStages], done;
+    uint32_t tmem;
+    int abort;
+};
+static_assert(sizeof(DwSmem) <= kDwTail, "k_train_dw: barrier block");
+static_assert(kDwStages * kDwStageBytes + kDwTail <= kDwSmem, "k_train_dw: shared memory");
+static_assert(kRows * (80 + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
+
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float ld_cluster_f32(uint32_t local, uint32_t rank)
+{
+    uint32_t remote;
+    float v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(remote) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void adamw_elem(float g, float* w, float* m1, float* m2, float wd, float lr, float b1,
+                                           float b2, float eps, float bc1, float bc2, __nv_bfloat16* img)
+{
+    const float a = b1 * *m1 + (1.f - b1) * g;
+    const float b = b2 * *m2 + (1.f - b2) * g * g;
+    *m1 = a;
+    *m2 = b;
+    float x = *w * (1.f - lr * wd);
+    x -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
+    *w = x;
+    *img = __float2bfloat16(x);
+}
+
+__global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constant__ DwArgs p)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    DwSmem* sh = reinterpret_cast<DwSmem*>(smem + kDwStages * kDwStageBytes);
+    volatile int* abort = &sh->abort;
+    uint32_t rank, nrank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(nrank));
+    const DwTile T = p.t[blockIdx.x / nrank];
+    const LayerGeo& L = p.geo.l[T.layer];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles = (p.M + kRows - 1) / kRows;
+    const int t0 = static_cast<int>(rank) * tiles / static_cast<int>(nrank);
+    const int t1 = (static_cast<int>(rank) + 1) * tiles / static_cast<int>(nrank);
+    const int nk = t1 - t0;
+    const int cw = L.cw[T.chunk], c0 = L.c0[T.chunk];
+    const uint32_t ncol_b = static_cast<uint32_t>(cw >> 3) << 7;  // bytes of one row group of the X chunk
+
+    if (tid == 0) {
+        for (int s = 0; s < kDwStages; ++s) {
+            mbar_init(smem_u32(&sh->full[s]), 1);
+            mbar_init(smem_u32(&sh->empty[s]), 1);
+        }
+        mbar_init(smem_u32(&sh->done), 1);
+        sh->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
+                     "r"(128)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (T.oh < kRows) {  // outputs past the tile read zeros (the copies fill only oh / 8 cores per row group)
+        for (int s = 0; s < kDwStages; ++s)
+            for (int i = tid; i < kDwABytes / 16; i += kDwThreads)
+                reinterpret_cast<uint4*>(smem + s * kDwStageBytes)[i] = make_uint4(0u, 0u, 0u, 0u);
+        proxy_fence();
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = sh->tmem;
+
+    if (warp == 1) {
+        // ---- producer: per row tile, dZ of the outputs (row group by row group, the
+        // 64-output pieces side by side) and the X chunk (one contiguous block)
+        int pa = 0;
+        while (pa + 1 < L.n_pieces && L.p0[pa + 1] <= T.o0) ++pa;
+        for (int k = 0; k < nk; ++k) {
+            const int s = k % kDwStages, round = k / kDwStages;
+            bool ok = true;
+            if (lane == 0 && round > 0) ok = mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1, abort);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            const uint32_t full = smem_u32(&sh->full[s]);
+            if (lane == 0) mbar_expect_tx(full, static_cast<uint32_t>(T.oh) * (kRows * 2) + static_cast<uint32_t>(cw) * (kRows * 2));
+            __syncwarp();
+            const int t = t0 + k;
+            const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
+            const int pc = pa + (lane >> 4), g = lane & 15;
+            if (pc < L.n_pieces && L.p0[pc] < T.o0 + T.oh) {
+                const uint32_t bytes = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
+                bulk_load(a_s + g * 2048u + (static_cast<uint32_t>(L.p0[pc] - T.o0) >> 3) * 128u,
+                          p.scratch + L.z_off + static_cast<int64_t>(t) * L.z_tile +
+                              static_cast<int64_t>(L.p0[pc]) * (kRows * 2) + g * bytes,
+                          bytes, full);
+            }
+            if (lane == 0)
+                bulk_load(b_s, p.scratch + L.x_off + static_cast<int64_t>(t) * L.x_tile + static_cast<int64_t>(c0) * (kRows * 2),
+                          static_cast<uint32_t>(cw) * (kRows * 2), full);
+        }
+    } else if (warp == 0 && lane == 0) {
+        // ---- MMAs: dW (outputs x inputs) += dZ^T X over the row tile, both operands MN-major
+        const uint32_t idesc = instr_desc(kRows, cw, true, true);
+        for (int k = 0; k < nk; ++k) {
+            const int s = k % kDwStages, round = k / kDwStages;
+            const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1, abort);
+            tc_after();
+            const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
+            for (int ks = 0; ok && ks < kRows / 16; ++ks)
+                mma_bf16(tmem, smem_desc(a_s + ks * 4096u, 2048u, 128u), smem_desc(b_s + ks * 2u * ncol_b, ncol_b, 128u),
+                         idesc, (k > 0 || ks > 0) ? 1u : 0u);
+            mma_commit(smem_u32(&sh->empty[s]));
+        }
+        if (nk > 0) mma_commit(smem_u32(&sh->done));
+    }
+    __syncwarp();
+
+    // ---- this CTA's partial into its shared memory (FP32, rows of cw + 4)
+    float* P = reinterpret_cast<float*>(smem);
+    const int pitch = cw + 4;
+    {
+        const bool ok = __all_sync(0xffffffffu, nk > 0 && mbar_wait(smem_u32(&sh->done), 0, abort));
+        tc_after();
+        const int q = warp & 3, hh = warp >> 2;
+        const int r = q * 32 + lane;
+        for (int u = hh; u < (cw >> 4); u += kDwThreads / 128) {
+            uint32_t v[16];
+            if (ok) tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(u * 16), v);
+            float4* d = reinterpret_cast<float4*>(P + r * pitch + u * 16);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                d[j] = ok ? make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                        __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    tc_before();
+    cluster_sync();
+
+    // ---- this CTA's share of the tile's rows: the partials of the cluster summed in
+    // rank order, then the gradient out or the AdamW step
+    {
+        const int per = (T.oh + static_cast<int>(nrank) - 1) / static_cast<int>(nrank);
+        const int rb = static_cast<int>(rank) * per, re = min(T.oh, rb + per);
+        const uint32_t pbase = smem_u32(P);
+        for (int idx = tid; idx < (re - rb) * cw; idx += kDwThreads) {
+            const int ol = rb + idx / cw, i = idx % cw;
+            const int o = T.o0 + ol, ia = c0 + i;
+            if (o >= L.dout || ia > L.din) continue;
+            const uint32_t la = pbase + static_cast<uint32_t>(ol * pitch + i) * 4u;
+            float g = 0.f;
+            for (uint32_t q = 0; q < nrank; ++q) g += ld_cluster_f32(la, q);
+            const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
+            if (p.grad) {
+                p.grad[e] = g;
+            } else {
+                adamw_elem(g, p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr, p.b1, p.b2, p.eps, p.bc1,
+                           p.bc2, reinterpret_cast<__nv_bfloat16*>(p.w_img + L.w_off + w_elem(L, o, ia)));
+            }
+        }
+    }
+    cluster_sync();
+    if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
+}
+
+// ---- packing and the stand-alone AdamW (data parallel) ------------------------
+
+struct GeoArgs {
+    Geo geo;
+};
+
+__device__ __forceinline__ int layer_of(const Geo& G, int64_t e)
+{
+    int l = 0;
+    while (l + 1 < G.n_layers && e >= G.l[l + 1].aug_off) ++l;
+    return l;
+}
+
+__global__ void k_fused_pack(const __grid_constant__ GeoArgs a, const float* __restrict__ w_aug, uint8_t* w_img)
+{
+    const Geo& G = a.geo;
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < G.aug_elems;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const LayerGeo& L = G.l[layer_of(G, e)];
+        const int64_t el = e - L.aug_off;
+        const int o = static_cast<int>(el / L.kaug), i = static_cast<int>(el - static_cast<int64_t>(o) * L.kaug);
+        *reinterpret_cast<__nv_bfloat16*>(w_img + L.w_off + w_elem(L, o, i)) = __float2bfloat16(w_aug[e]);
+    }
+}
+
+struct AdamScalars {
+    float lr, b1, b2, eps, wd, bc1, bc2;
+};
+
+__global__ void k_fused_adamw(const __grid_constant__ GeoArgs a, const AdamScalars h, float* w_aug, float* m1,
+                              float* m2, const float* __restrict__ grad, uint8_t* w_img)
+{
+    const Geo& G = a.geo;
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < G.aug_elems;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const LayerGeo& L = G.l[layer_of(G, e)];
+        const int64_t el = e - L.aug_off;
+        const int o = static_cast<int>(el / L.kaug), i = static_cast<int>(el - static_cast<int64_t>(o) * L.kaug);
+        if (o >= L.dout || i > L.din) continue;
+        adamw_elem(grad[e], w_aug + e, m1 + e, m2 + e, i < L.din ? h.wd : 0.f, h.lr, h.b1, h.b2, h.eps, h.bc1, h.bc2,
+                   reinterpret_cast<__nv_bfloat16*>(w_img + L.w_off + w_elem(L, o, i)));
+    }
+}
+
+cudaError_t ensure_fused_smem()
+{
+    constexpr int kDevs = 64;
+    static int done[kDevs];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < kDevs && __atomic_load_n(&done[dev], __ATOMIC_ACQUIRE)) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kFbSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_train_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, kDwSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_train_dw, cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+    if (e == cudaSuccess && dev >= 0 && dev < kDevs) __atomic_store_n(&done[dev], 1, __ATOMIC_RELEASE);
+    return e;
+}
+
+bool aligned16h(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; }
+
+int grid_for(int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 8) g = 148 * 8;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pb_train_fused_geometry(int32_t n_layers, const int32_t* dims, int32_t batch, int64_t* out, int32_t out_len)
+{
+    Geo g;
+    const int rc = geo_build(n_layers, dims, batch, &g);
+    if (rc != PB_SUCCESS) return rc;
+    if (!out || out_len < 3 + 4 * n_layers) return PB_EINVAL;
+    out[0] = g.img_bytes;
+    out[1] = g.scratch_bytes;
+    out[2] = g.aug_elems;
+    for (int l = 0; l < n_layers; ++l) {
+        out[3 + 4 * l + 0] = g.l[l].kaug;
+        out[3 + 4 * l + 1] = g.l[l].npad;
+        out[3 + 4 * l + 2] = g.l[l].aug_off;
+        out[3 + 4 * l + 3] = g.l[l].w_off;
+    }
+    return PB_SUCCESS;
+}
+
+int pb_train_fused_pack(int32_t n_layers, const int32_t* dims, const float* w_aug, void* w_img, void* stream)
+{
+    GeoArgs a;
+    const int rc = geo_build(n_layers, dims, 1, &a.geo);
+    if (rc != PB_SUCCESS) return rc;
+    if (!w_aug || !w_img || !aligned16h(w_img)) return PB_EINVAL;
+    k_fused_pack<<<grid_for(a.geo.aug_elems), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        a, w_aug, static_cast<uint8_t*>(w_img));
+    return cudaGetLastError() == cudaSuccess ? PB_SUCCESS : PB_ECUDA;
+}
+
+int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf16, const int32_t* labels,
+                        int32_t n_rows, const int32_t* rows, int32_t M, int32_t batch, float* w_aug, float* m1, float* m2,
+                        void* w_img, void* scratch, float* grad, float lr, float beta1, float beta2, float eps,
+                        float weight_decay, int32_t step, float* loss_sum, int32_t* correct, int32_t* error_flag,
+                        void* stream)
+{
+    FbArgs* fb = new FbArgs();
+    DwArgs* dw = new DwArgs();
+    auto finish = [&](int rc) {
+        delete fb;
+        delete dw;
+        return rc;
+    };
+    int rc = geo_build(n_layers, dims, batch, &fb->geo);
+    if (rc != PB_SUCCESS) return finish(rc);
+    if (M < 1 || M > batch || step < 1 || n_rows < 1) return finish(PB_EINVAL);
+    if (!x_bf16 || !labels || !rows || !w_img || !scratch || !aligned16h(x_bf16) || !aligned16h(w_img) ||
+        !aligned16h(scratch))
+        return finish(PB_EINVAL);
+    if (!grad && (!w_aug || !m1 || !m2)) return finish(PB_EINVAL);
+    if (ensure_fused_smem() != cudaSuccess) return finish(PB_ECUDA);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    fb->x = static_cast<const __nv_bfloat16*>(x_bf16);
+    fb->labels = labels;
+    fb->rows = rows;
+    fb->n_rows = n_rows;
+    fb->M = M;
+    fb->scale = 1.f / static_cast<float>(M);
+    fb->w_img = static_cast<const uint8_t*>(w_img);
+    fb->scratch = static_cast<uint8_t*>(scratch);
+    fb->loss_sum = loss_sum;
+    fb->correct = correct;
+    fb->error = error_flag;
+    const int row_tiles = (M + kRows - 1) / kRows;
+    k_train_fb<<<row_tiles, kFbThreads, kFbSmem, s>>>(*fb);
+    if (cudaGetLastError() != cudaSuccess) return finish(PB_ECUDA);
+
+    dw->geo = fb->geo;
+    int nt = 0;
+    for (int l = 0; l < n_layers; ++l) {
+        const LayerGeo& L = dw->geo.l[l];
+        for (int o0 = 0; o0 < L.npad; o0 += kRows)
+            for (int c = 0; c < L.n_chunks; ++c) dw->t[nt++] = DwTile{l, o0, min(kRows, L.npad - o0), c};
+    }
+    dw->n_tiles = nt;
+    dw->M = M;
+    dw->scratch = static_cast<const uint8_t*>(scratch);
+    dw->w_img = static_cast<uint8_t*>(w_img);
+    dw->w_aug = w_aug;
+    dw->m1 = m1;
+    dw->m2 = m2;
+    dw->grad = grad;
+    dw->lr = lr;
+    dw->b1 = beta1;
+    dw->b2 = beta2;
+    dw->eps = eps;
+    dw->wd = weight_decay;
+    dw->bc1 = static_cast<float>(1.0 - std::pow(static_cast<double>(beta1), step));
+    dw->bc2 = static_cast<float>(1.0 - std::pow(static_cast<double>(beta2), step));
+    dw->error = error_flag;
+    // the CTAs of a cluster split the row tiles: as many as fill the GPU once
+    int cs = 148 / nt;
+    cs = cs < 1 ? 1 : (cs > kMaxCluster ? kMaxCluster : cs);
+    if (cs > row_tiles) cs = row_tiles;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(nt * cs), 1, 1);
+    cfg.blockDim = dim3(kDwThreads, 1, 1);
+    cfg.dynamicSmemBytes = kDwSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(cs);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_train_dw, *dw) != cudaSuccess) return finish(PB_ECUDA);
+    return finish(PB_SUCCESS);
+}
+
+int pb_train_fused_adamw(int32_t n_layers, const int32_t* dims, float* w_aug, float* m1, float* m2, const float* grad,
+                         void* w_img, float lr, float beta1, float beta2, float eps, float weight_decay, int32_t step,
+                         void* stream)
+{
+    GeoArgs a;
+    const int rc = geo_build(n_layers, dims, 1, &a.geo);
+    if (rc != PB_SUCCESS) return rc;
+    if (!w_aug || !m1 || !m2 || !grad || !w_img || !aligned16h(w_img) || step < 1) return PB_EINVAL;
+    AdamScalars h{lr, beta1, beta2, eps, weight_decay,
+                  static_cast<float>(1.0 - std::pow(static_cast<double>(beta1), step)),
+                  static_cast<float>(1.0 - std::pow(static_cast<double>(beta2), step))};
+    k_fused_adamw<<<grid_for(a.geo.aug_elems), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        a, h, w_aug, m1, m2, grad, static_cast<uint8_t*>(w_img));
+    return cudaGetLastError() == cudaSuccess ? PB_SUCCESS : PB_ECUDA;
+}
+
+}  // extern "C"

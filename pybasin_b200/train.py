@@ -49,7 +49,14 @@ def bind(lib: ctypes.CDLL) -> None:
     lib.pb_train_adamw.argtypes = [i32, PV, PV, PV, PI64, PV, PV, PV, PI64, PI64, ctypes.POINTER(i32),
                                    ctypes.POINTER(f32), f32, f32, f32, f32, i32, vp]
     lib.pb_train_gather.argtypes = [vp, i32, vp, vp, i64, vp, vp, vp, vp]
-    for name in ("pb_train_gemm", "pb_train_xent", "pb_train_xent_parts", "pb_train_adamw", "pb_train_gather"):
+    PI32 = ctypes.POINTER(i32)
+    lib.pb_train_fused_geometry.argtypes = [i32, PI32, i32, PI64, i32]
+    lib.pb_train_fused_pack.argtypes = [i32, PI32, vp, vp, vp]
+    lib.pb_train_fused_step.argtypes = [i32, PI32, vp, vp, i32, vp, i32, i32, vp, vp, vp, vp, vp, vp, f32, f32, f32,
+                                        f32, f32, i32, vp, vp, vp, vp]
+    lib.pb_train_fused_adamw.argtypes = [i32, PI32, vp, vp, vp, vp, vp, f32, f32, f32, f32, f32, i32, vp]
+    for name in ("pb_train_gemm", "pb_train_xent", "pb_train_xent_parts", "pb_train_adamw", "pb_train_gather",
+                 "pb_train_fused_geometry", "pb_train_fused_pack", "pb_train_fused_step", "pb_train_fused_adamw"):
         getattr(lib, name).restype = ctypes.c_int
     lib._pb_train_bound = True
 
@@ -79,6 +86,15 @@ def gemm_tc(A: torch.Tensor, sam: int, sak: int, B: torch.Tensor, sbn: int, sbk:
     L.check(rc, "pb_train_gemm")
 
 
+def fused_supported(dims: list[int]) -> bool:
+    """Whether the fused step (``pb_train_fused_step``) takes a network of these layer
+    widths: at most 8 layers, inputs a multiple of 8 up to 256, hidden widths
+    multiples of 16 up to 256, 2 to 32 classes."""
+    n = len(dims) - 1
+    return (1 <= n <= 8 and dims[0] % 8 == 0 and 8 <= dims[0] <= 256
+            and all(d % 16 == 0 and 16 <= d <= 256 for d in dims[1:-1]) and 2 <= dims[-1] <= 32)
+
+
 def dw_tile(n: int) -> int:
     """Columns per CTA of a weight-gradient GEMM with n weight columns plus the bias's
     column of ones: as many tiles as n alone needs at 64 columns, widened to fit."""
@@ -88,16 +104,23 @@ def dw_tile(n: int) -> int:
 
 class GraphTrainer:
     """A captured training run of ``net`` on ``n_rows`` rows (BF16 inputs of width
-    ``net.d_in``, int32 labels): ``epochs`` epochs of minibatches of ``batch`` rows."""
+    ``net.d_in``, int32 labels): ``epochs`` epochs of minibatches of ``batch`` rows.
+
+    With ``fused`` (the default where :func:`fused_supported` holds) a minibatch step
+    is two launches of ``pb_train_fused_step`` (the layer chain of each 128-row tile
+    in one kernel, the weight gradients with AdamW in another), on augmented
+    parameters ``[W | b]``; otherwise it is the per-GEMM sequence of ``pb_train_gemm``
+    launches."""
 
     def __init__(self, net: MLPSurrogate, n_rows: int, epochs: int, batch: int = 4096, lr: float = 4e-3,
                  weight_decay: float = 1e-4, seed: int = 0, betas: tuple[float, float] = (0.9, 0.999),
-                 eps: float = 1e-8, resume: bool = False, data_parallel: bool = False, group=None):
+                 eps: float = 1e-8, resume: bool = False, data_parallel: bool = False, group=None,
+                 fused: bool | None = None):
         """With ``resume``, a run starts from the net's current weights (fresh AdamW
         moments) instead of the weights it had when the trainer was built.  With
         ``data_parallel`` every rank of the process group trains on its own rows
         (the same row count, batch and epochs on every rank): after each backward
-        pass the gradients are summed over the rank's chunks and averaged over the
+        pass the gradients are summed over the rank's rows and averaged over the
         ranks in one collective, so every rank takes the same AdamW step."""
         if net.d_in % 8:
             raise ValueError("GraphTrainer needs input rows of a multiple of 8 columns (MLPSurrogate(pad_inputs=True))")
@@ -109,17 +132,58 @@ class GraphTrainer:
         self.n, self.epochs, self.batch = n_rows, epochs, min(batch, n_rows)
         self.lr, self.wd, self.betas, self.eps = lr, weight_decay, betas, eps
         dev = self.dev
-        L_ = net.n_layers
         self.dims = [net.d_in] + [int(w.shape[0]) for w in net.W]
-        B = self.batch
+        self.fused = fused_supported(self.dims) if fused is None else fused
+        if self.fused and not fused_supported(self.dims):
+            raise ValueError(f"layer widths {self.dims} are outside the fused training step's limits")
         self.X = torch.zeros((n_rows, net.d_in), dtype=torch.bfloat16, device=dev)
         self.Y = torch.zeros((n_rows,), dtype=torch.int32, device=dev)
-        self.Xs = torch.zeros_like(self.X)
-        self.XsT = torch.zeros((net.d_in, n_rows), dtype=torch.bfloat16, device=dev)  # the shuffled inputs transposed
-        self.Ys = torch.zeros_like(self.Y)
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.perm = torch.stack([torch.randperm(n_rows, generator=g) for _ in range(epochs)]).to(
             dev, torch.int32).contiguous()
+        self.loss = torch.zeros((1,), dtype=torch.float32, device=dev)
+        self.correct = torch.zeros((1,), dtype=torch.int32, device=dev)
+        self.error = torch.zeros((1,), dtype=torch.int32, device=dev)
+        self.graph: torch.cuda.CUDAGraph | None = None
+        self.steps = sum(-(-n_rows // self.batch) for _ in range(epochs))
+        self.capture_s = 0.0
+        self.launches = 0
+        self.timing = False
+        if self.fused:
+            self._init_fused()
+        else:
+            self._init_gemm()
+
+    def _init_fused(self) -> None:
+        lib = _lib()
+        net, dev = self.net, self.dev
+        L_ = net.n_layers
+        self._dims_c = (ctypes.c_int32 * len(self.dims))(*self.dims)
+        geo = (ctypes.c_int64 * (3 + 4 * L_))()
+        L.check(lib.pb_train_fused_geometry(L_, self._dims_c, self.batch, geo, len(geo)), "pb_train_fused_geometry")
+        img_bytes, scratch_bytes, n_aug = int(geo[0]), int(geo[1]), int(geo[2])
+        self.kaug = [int(geo[3 + 4 * l]) for l in range(L_)]
+        self.npad = [int(geo[4 + 4 * l]) for l in range(L_)]
+        self.aug_off = [int(geo[5 + 4 * l]) for l in range(L_)]
+        self.w_aug = torch.zeros((n_aug,), dtype=torch.float32, device=dev)
+        self.m1 = torch.zeros_like(self.w_aug)
+        self.m2 = torch.zeros_like(self.w_aug)
+        self.grad = torch.zeros_like(self.w_aug)
+        self.w_img = torch.zeros((img_bytes,), dtype=torch.uint8, device=dev)
+        self.scratch = torch.zeros((scratch_bytes,), dtype=torch.uint8, device=dev)
+        self._views = [self.w_aug[o : o + n * k].view(n, k) for o, n, k in zip(self.aug_off, self.npad, self.kaug)]
+        self._gviews = [self.grad[o : o + n * k].view(n, k) for o, n, k in zip(self.aug_off, self.npad, self.kaug)]
+        self._aug_from_net()
+        self.init_aug = self.w_aug.clone()
+
+    def _init_gemm(self) -> None:
+        net, dev = self.net, self.dev
+        L_ = net.n_layers
+        B = self.batch
+        n_rows = self.n
+        self.Xs = torch.zeros_like(self.X)
+        self.XsT = torch.zeros((net.d_in, n_rows), dtype=torch.bfloat16, device=dev)  # the shuffled inputs transposed
+        self.Ys = torch.zeros_like(self.Y)
         self.act = [None] + [torch.zeros((B, self.dims[l + 1]), dtype=torch.bfloat16, device=dev)
                              for l in range(L_ - 1)]
         self.z = [torch.zeros((B, self.dims[l + 1]), dtype=torch.float32, device=dev) for l in range(L_ - 1)]
@@ -146,14 +210,72 @@ class GraphTrainer:
         self.init = [p.clone() for p in self.params]
         self.init_bf16 = [w.clone() for w in net.Wb]
         self.init_bf16_t = [w.clone() for w in self.WbT]
-        self.loss = torch.zeros((1,), dtype=torch.float32, device=dev)
-        self.correct = torch.zeros((1,), dtype=torch.int32, device=dev)
-        self.error = torch.zeros((1,), dtype=torch.int32, device=dev)
-        self.graph: torch.cuda.CUDAGraph | None = None
-        self.steps = sum(-(-n_rows // B) for _ in range(epochs))
-        self.capture_s = 0.0
-        self.launches = 0
-        self.timing = False
+
+    # -- the fused step's augmented parameters -------------------------------------
+    def _aug_from_net(self) -> None:
+        """[W | b | 0] of every layer from the net's FP32 weights."""
+        self.w_aug.zero_()
+        for l, A in enumerate(self._views):
+            dout, din = self.dims[l + 1], self.dims[l]
+            A[:dout, :din].copy_(self.net.W[l])
+            A[:dout, din].copy_(self.net.b[l])
+
+    def _net_from_aug(self) -> None:
+        """The net's FP32 weights, biases and BF16 copies from the augmented parameters."""
+        net = self.net
+        for l, A in enumerate(self._views):
+            dout, din = self.dims[l + 1], self.dims[l]
+            net.W[l].copy_(A[:dout, :din])
+            net.b[l].copy_(A[:dout, din])
+            net.Wb[l].copy_(net.W[l])
+            if getattr(net, "WbT", None) is not None and tuple(net.WbT[l].shape) == (din, dout):
+                net.WbT[l].copy_(net.W[l].t())
+
+    def _pack(self, lib, s: int) -> None:
+        L.check(lib.pb_train_fused_pack(self.net.n_layers, self._dims_c, _p(self.w_aug), _p(self.w_img), s),
+                "pb_train_fused_pack")
+
+    def _fused_step(self, lib, s: int, x: torch.Tensor, y: torch.Tensor, rows: torch.Tensor, M: int, lr: float,
+                    step: int, grad: bool) -> None:
+        b1, b2 = self.betas
+        L.check(lib.pb_train_fused_step(self.net.n_layers, self._dims_c, _p(x), _p(y), x.shape[0], _p(rows), M,
+                                        self.batch,
+                                        _p(self.w_aug), _p(self.m1), _p(self.m2), _p(self.w_img), _p(self.scratch),
+                                        _p(self.grad) if grad else None, lr, b1, b2, self.eps, self.wd, step,
+                                        _p(self.loss), _p(self.correct), _p(self.error), s), "pb_train_fused_step")
+
+    def _run_fused(self) -> None:
+        lib = _lib()
+        s = torch.cuda.current_stream(self.dev).cuda_stream
+        if self.resume:
+            self._aug_from_net()
+        else:
+            self.w_aug.copy_(self.init_aug)
+        self._pack(lib, s)
+        self.m1.zero_()
+        self.m2.zero_()
+        self.loss.zero_()
+        self.correct.zero_()
+        b1, b2 = self.betas
+        step, launches = 0, 1
+        for ep in range(self.epochs):
+            lr = self.lr * 0.5 * (1.0 + math.cos(math.pi * ep / max(self.epochs, 1)))
+            for b0 in range(0, self.n, self.batch):
+                M = min(self.batch, self.n - b0)
+                step += 1
+                self._fused_step(lib, s, self.X, self.Y, self.perm[ep, b0 : b0 + M], M, lr, step,
+                                 grad=self.data_parallel)
+                launches += 2
+                if self.data_parallel:
+                    from pybasin_b200.sharding import allreduce_gradients
+
+                    allreduce_gradients([self.grad], group=self.group)
+                    L.check(lib.pb_train_fused_adamw(self.net.n_layers, self._dims_c, _p(self.w_aug), _p(self.m1),
+                                                     _p(self.m2), _p(self.grad), _p(self.w_img), lr, b1, b2,
+                                                     self.eps, self.wd, step, s), "pb_train_fused_adamw")
+                    launches += 1
+        self._net_from_aug()
+        self.launches = launches
 
     # -- one run, as launched (captured once) ------------------------------------------
     def _reset(self) -> None:
@@ -249,6 +371,15 @@ class GraphTrainer:
             raise ValueError("at most one minibatch")
         y = labels.to(self.dev, torch.int32).contiguous()
         x = x.contiguous()
+        if self.fused:
+            s = torch.cuda.current_stream(self.dev).cuda_stream
+            self._aug_from_net()
+            self._pack(lib, s)
+            rows = torch.arange(M, dtype=torch.int32, device=self.dev)
+            self._fused_step(lib, s, x, y, rows, M, 0.0, 1, grad=True)
+            gW = [G[: self.dims[l + 1], : self.dims[l]].clone() for l, G in enumerate(self._gviews)]
+            gb = [G[: self.dims[l + 1], self.dims[l]].clone() for l, G in enumerate(self._gviews)]
+            return gW, gb
         self._grads(lib, torch.cuda.current_stream(self.dev).cuda_stream, x, x.t().contiguous(), M, y, M)
         splits = -(-M // KC)
         gW = [g[:splits].sum(0) for g in self.gw_part]
@@ -256,6 +387,9 @@ class GraphTrainer:
         return gW, gb
 
     def _run(self) -> None:
+        if self.fused:
+            self._run_fused()
+            return
         lib = _lib()
         s = torch.cuda.current_stream(self.dev).cuda_stream
         d = self.net.d_in
@@ -284,11 +418,17 @@ class GraphTrainer:
         if self.graph is not None:
             return 0.0
         t0 = time.perf_counter()
-        # one eager launch first: the GEMM's shared-memory limit is raised outside the capture
-        gemm_tc(self.X, self.net.d_in, 1, self.net.Wb[0], self.net.d_in, 1, 1, 16, self.net.d_in, TRAIN_FWD_LINEAR,
-                out_f32=self.logits, ldc=self.logits.shape[1], bn=16) if self.logits.shape[1] >= 16 else \
-            gemm_tc(self.X, self.net.d_in, 1, self.net.Wb[0], self.net.d_in, 1, 1, self.logits.shape[1],
-                    self.net.d_in, TRAIN_FWD_LINEAR, out_f32=self.logits, ldc=self.logits.shape[1])
+        # one eager launch first: the kernels' shared-memory limits are raised outside the capture
+        if self.fused:
+            lib = _lib()
+            s = torch.cuda.current_stream(self.dev).cuda_stream
+            M = min(self.batch, self.n)
+            self._fused_step(lib, s, self.X, self.Y, self.perm[0, :M], M, 0.0, 1, grad=True)
+        else:
+            gemm_tc(self.X, self.net.d_in, 1, self.net.Wb[0], self.net.d_in, 1, 1, 16, self.net.d_in, TRAIN_FWD_LINEAR,
+                    out_f32=self.logits, ldc=self.logits.shape[1], bn=16) if self.logits.shape[1] >= 16 else \
+                gemm_tc(self.X, self.net.d_in, 1, self.net.Wb[0], self.net.d_in, 1, 1, self.logits.shape[1],
+                        self.net.d_in, TRAIN_FWD_LINEAR, out_f32=self.logits, ldc=self.logits.shape[1])
         torch.cuda.synchronize(self.dev)
         side = torch.cuda.Stream(device=self.dev)
         side.wait_stream(torch.cuda.current_stream(self.dev))

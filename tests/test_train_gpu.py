@@ -94,7 +94,8 @@ def test_weight_gradient_split_k_matches_fp64(M, N, K):
     np.testing.assert_allclose(bpart.sum(0).cpu().numpy(), dz.sum(0), rtol=0, atol=1e-4 * np.abs(dz).sum(0).max())
 
 
-def test_trainer_gradients_match_oracle():
+@pytest.mark.parametrize("fused", [True, False])
+def test_trainer_gradients_match_oracle(fused):
     from pybasin_b200.surrogate import MLPSurrogate
     from pybasin_b200.train import GraphTrainer
 
@@ -105,7 +106,7 @@ def test_trainer_gradients_match_oracle():
     x = np.zeros((n, net.d_in))
     x[:, : net.d_used] = _bf16(rng.normal(size=(n, net.d_used)))
     y = rng.integers(0, 6, n)
-    tr = GraphTrainer(net, n_rows=n, epochs=1, batch=n)
+    tr = GraphTrainer(net, n_rows=n, epochs=1, batch=n, fused=fused)
     gW, gb = tr.gradients(_dev_bf16(x), torch.tensor(y, dtype=torch.int32))
     torch.cuda.synchronize()
     Ws = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
@@ -120,7 +121,8 @@ def test_trainer_gradients_match_oracle():
     assert float(gW[0][:, net.d_used :].abs().max()) == 0.0
 
 
-def test_graph_replay_equals_eager_run_and_learns():
+@pytest.mark.parametrize("fused", [True, False])
+def test_graph_replay_equals_eager_run_and_learns(fused):
     """A captured run replays to bit-identical weights of an eager run (deterministic
     partial sums), twice in a row from the reset weights, and it learns."""
     from pybasin_b200.surrogate import MLPSurrogate
@@ -132,7 +134,7 @@ def test_graph_replay_equals_eager_run_and_learns():
     net = MLPSurrogate(2, 4, hidden=128, depth=3, seed=0, device=DEV, n_freq=16, pad_inputs=True)
     net.fit_normalisation(pts.to(DEV))
     xi = net.inputs(pts.to(DEV), None)
-    tr = GraphTrainer(net, n_rows=6000, epochs=12, batch=1024, lr=4e-3)
+    tr = GraphTrainer(net, n_rows=6000, epochs=12, batch=1024, lr=4e-3, fused=fused)
     tr.train(xi, y.to(DEV), use_graph=False)
     torch.cuda.synchronize()
     eager = [w.clone() for w in net.W]
@@ -147,7 +149,8 @@ def test_graph_replay_equals_eager_run_and_learns():
     assert acc > 0.97
 
 
-def test_data_parallel_trainer_under_a_one_rank_group():
+@pytest.mark.parametrize("fused", [True, False])
+def test_data_parallel_trainer_under_a_one_rank_group(fused):
     """The data-parallel path (chunk partials summed, the one all-reduce, AdamW on a
     single partial) under a one-rank NCCL group gives the single-process step: one
     full-batch step from the same weights, equal to summation-order rounding."""
@@ -174,7 +177,7 @@ def test_data_parallel_trainer_under_a_one_rank_group():
             net = MLPSurrogate(2, 4, hidden=64, depth=2, seed=5, device=DEV, n_freq=8, pad_inputs=True)
             net.fit_normalisation(pts.to(DEV))
             xi = net.inputs(pts.to(DEV), None)
-            tr = GraphTrainer(net, n_rows=3000, epochs=1, batch=3000, lr=4e-3, data_parallel=dp)
+            tr = GraphTrainer(net, n_rows=3000, epochs=1, batch=3000, lr=4e-3, data_parallel=dp, fused=fused)
             tr.train(xi, y.to(DEV), use_graph=False)
             torch.cuda.synchronize()
             out.append([w.clone() for w in net.W])
@@ -182,3 +185,54 @@ def test_data_parallel_trainer_under_a_one_rank_group():
             assert (a - b).abs().max().item() <= 1e-6
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n", [300, 4096])
+def test_fused_step_gradients_of_the_surrogate_shape(n):
+    """The surrogate's own shape (136 inputs, 4 x 256 GELU, 6 classes) through the
+    fused step: several row tiles (the last one ragged for n = 300), every layer's
+    chunks and pieces, the weight gradients summed over a cluster.  Gradients of
+    the mean loss against the FP64 oracle on the same BF16 inputs and weights."""
+    from pybasin_b200.surrogate import MLPSurrogate
+    from pybasin_b200.train import GraphTrainer
+
+    net = MLPSurrogate(2, 6, hidden=256, depth=4, seed=3, device=DEV, n_freq=64, pad_inputs=True)
+    assert net.d_in == 136
+    rng = np.random.default_rng(n)
+    x = np.zeros((n, net.d_in))
+    x[:, : net.d_used] = _bf16(rng.normal(size=(n, net.d_used)))
+    y = rng.integers(0, 6, n)
+    tr = GraphTrainer(net, n_rows=n, epochs=1, batch=n, fused=True)
+    gW, gb = tr.gradients(_dev_bf16(x), torch.tensor(y, dtype=torch.int32))
+    torch.cuda.synchronize()
+    assert int(tr.error.item()) == 0
+    Ws = [w.to(torch.bfloat16).double().cpu().numpy() for w in net.W]
+    bs = [b.double().cpu().numpy() for b in net.b]
+    z, acts, pres = MO.forward(x, Ws, bs)
+    _, d = MO.loss_and_grad(z, y)
+    oW, ob = MO.backward(d, acts, pres, Ws)
+    for li in range(len(Ws)):
+        np.testing.assert_allclose(gW[li].cpu().numpy(), oW[li], rtol=0, atol=3e-2 * np.abs(oW[li]).max())
+        np.testing.assert_allclose(gb[li].cpu().numpy(), ob[li], rtol=0, atol=3e-2 * np.abs(ob[li]).max())
+
+
+def test_fused_and_per_gemm_training_agree():
+    """The same run (shuffles, learning rates, steps) on the two paths: accuracy of the
+    trained networks within a point, weights within BF16 training noise."""
+    from pybasin_b200.surrogate import MLPSurrogate
+    from pybasin_b200.train import GraphTrainer
+
+    g = torch.Generator().manual_seed(5)
+    pts = torch.rand(8000, 2, generator=g) * 2 - 1
+    y = ((pts[:, 0] > 0).int() + 2 * (pts[:, 0] ** 2 + pts[:, 1] ** 2 < 0.3).int()).to(torch.int32)
+    accs = []
+    for fused in (True, False):
+        net = MLPSurrogate(2, 4, hidden=256, depth=4, seed=0, device=DEV, n_freq=32, pad_inputs=True)
+        net.fit_normalisation(pts.to(DEV))
+        xi = net.inputs(pts.to(DEV), None)
+        tr = GraphTrainer(net, n_rows=8000, epochs=10, batch=2048, lr=4e-3, fused=fused)
+        tr.train(xi, y.to(DEV))
+        torch.cuda.synchronize()
+        assert tr.stats()["error"] == 0
+        accs.append(float((net.logits(xi).argmax(1).cpu() == y).float().mean()))
+    assert accs[0] > 0.97 and abs(accs[0] - accs[1]) < 0.01
