@@ -70,7 +70,6 @@ constexpr int kEpiWarps = 16;
 constexpr int kMmaWarp = kEpiWarps;
 constexpr int kLoadWarp = kEpiWarps + 1;
 constexpr int kFbThreads = (kEpiWarps + 2) * 32;
-constexpr int kLayerBarThreads = (kEpiWarps + 1) * 32;  // epilogue warps + the MMA warp
 constexpr int kRing = 8;                                 // weight-tile slots
 constexpr int kTileBytes = 64 * 80 * 2;                  // largest weight tile
 constexpr int kImgBytes = kRows * kMaxKaug * 2;          // largest activation / gradient image
@@ -88,6 +87,7 @@ constexpr int kDwStageBytes = kDwABytes + kDwBBytes;
 constexpr int kDwTail = 256;
 constexpr int kDwSmem = 227 * 1024;  // as kFbSmem
 constexpr int kMaxCluster = 8;
+constexpr int kDwAcc = 4;  // accumulators a weight-gradient CTA rotates its K steps over (128 TMEM columns each)
 constexpr int kMaxDwTiles = kMaxLayers * 2 * kMaxChunks;
 
 // ---- geometry ----------------------------------------------------------------
@@ -323,9 +323,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ void named_sync(int id, int threads)
+// All threads of the CTA, in the non-aligned form (warps may arrive diverged:
+// one lane issued the MMAs or the copies)
+__device__ __forceinline__ void cta_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
 {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -384,8 +388,11 @@ struct FbArgs {
 
 // Shared memory of k_train_fb: two image buffers (the layer chain alternates
 // between them), the weight-tile ring, then barriers and flags.
+// full / empty: the weight-tile ring; mdone[j]: the MMAs of output piece j are
+// done; grp_done[j]: the 4 warps of epilogue group j wrote their piece; epi_done:
+// every epilogue warp finished the phase (the MMA warp starts the next layer)
 struct FbSmem {
-    uint64_t full[kRing], empty[kRing], mdone[kMaxPieces];
+    uint64_t full[kRing], empty[kRing], mdone[kMaxPieces], grp_done[kMaxPieces], epi_done;
     uint32_t tmem;
     int abort;
     int y[kRows];
@@ -495,7 +502,11 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             mbar_init(smem_u32(&sh->full[s]), 1);
             mbar_init(smem_u32(&sh->empty[s]), 1);
         }
-        for (int j = 0; j < kMaxPieces; ++j) mbar_init(smem_u32(&sh->mdone[j]), 1);
+        for (int j = 0; j < kMaxPieces; ++j) {
+            mbar_init(smem_u32(&sh->mdone[j]), 1);
+            mbar_init(smem_u32(&sh->grp_done[j]), 4);
+        }
+        mbar_init(smem_u32(&sh->epi_done), kEpiWarps);
         sh->abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -506,7 +517,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     tc_before();
-    __syncthreads();
+    cta_sync();
     tc_after();
     const uint32_t tmem = sh->tmem;
 
@@ -523,19 +534,21 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 bulk_load(smem_u32(ring + s * kTileBytes), p.w_img + L.w_off + w_tile(L, pc, cc), bytes,
                           smem_u32(&sh->full[s]));
             };
+            // forward: chunk by chunk, every output piece of a chunk; input
+            // gradients: piece by piece, every input chunk of a piece (the order in
+            // which the MMA warp interleaves its accumulators)
             for (int l = 0; l < NL && !*abort; ++l) {
-                const LayerGeo& L = G.l[l];
-                for (int pc = 0; pc < L.n_pieces; ++pc)
-                    for (int cc = 0; cc < L.n_chunks; ++cc) put(L, pc, cc);
-            }
-            for (int l = NL - 1; l >= 1 && !*abort; --l) {
                 const LayerGeo& L = G.l[l];
                 for (int cc = 0; cc < L.n_chunks; ++cc)
                     for (int pc = 0; pc < L.n_pieces; ++pc) put(L, pc, cc);
             }
+            for (int l = NL - 1; l >= 1 && !*abort; --l) {
+                const LayerGeo& L = G.l[l];
+                for (int pc = 0; pc < L.n_pieces; ++pc)
+                    for (int cc = 0; cc < L.n_chunks; ++cc) put(L, pc, cc);
+            }
         }
-        __syncwarp();
-        __syncthreads();
+        cta_sync();
         if (tid == kLoadWarp * 32 && *abort && p.error) atomicExch(p.error, 1);
         return;
     }
@@ -567,9 +580,11 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
         proxy_fence();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
     }
-    named_sync(1, kLayerBarThreads);
     if (tid == 0) {
+        mbar_wait(smem_u32(&sh->epi_done), 0, abort);
         bulk_store(p.scratch + G.l[0].x_off + tile * G.l[0].x_tile, smem_u32(smem),
                    static_cast<uint32_t>(G.l[0].x_tile));
         bulk_commit();
@@ -581,6 +596,8 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     const bool leader = (tid & 127) == 0 && warp < kEpiWarps;
     uint32_t u = 0;                      // weight tiles consumed (MMA warp)
     uint32_t uses = 0;                   // waits on mdone[grp] so far (epilogue warps)
+    uint32_t epi_phase = 0;              // phases of epi_done waited for (MMA warp)
+    uint32_t ph = 1;                     // this phase of epi_done (the gather was phase 0)
     int cur = 0;
     float loss = 0.f;
     int hits = 0;
@@ -591,25 +608,31 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         const bool last = l + 1 == NL;
         if (warp == kMmaWarp) {
             if (lane == 0) {
+                mbar_wait(smem_u32(&sh->epi_done), epi_phase++ & 1u, abort);  // the inputs are written
                 tc_after();
                 const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
-                for (int pc = 0; pc < L.n_pieces; ++pc) {
-                    const uint32_t idesc = instr_desc(kRows, L.ph[pc], false, false);
-                    for (int cc = 0; cc < L.n_chunks; ++cc) {
-                        const uint32_t s = u % kRing, round = u / kRing;
-                        ++u;
-                        const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
-                        tc_after();
-                        const uint32_t sbo = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;
-                        const uint32_t wa = smem_u32(ring + s * kTileBytes);
-                        for (int ks = 0; ok && ks < (L.cw[cc] >> 4); ++ks)
+                // chunk by chunk; within a chunk the output pieces take turns per K
+                // step, so consecutive MMAs feed independent accumulators
+                for (int cc = 0; cc < L.n_chunks; ++cc) {
+                    bool ok = true;
+                    uint32_t wa[kMaxPieces];
+                    for (int pc = 0; pc < L.n_pieces; ++pc) {
+                        const uint32_t s = (u + pc) % kRing, round = (u + pc) / kRing;
+                        ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort) && ok;
+                        wa[pc] = smem_u32(ring + s * kTileBytes);
+                    }
+                    tc_after();
+                    const uint32_t sbo = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;
+                    for (int ks = 0; ok && ks < (L.cw[cc] >> 4); ++ks)
+                        for (int pc = 0; pc < L.n_pieces; ++pc)
                             mma_bf16(tmem + static_cast<uint32_t>(L.p0[pc]),
                                      smem_desc(a0 + L.c0[cc] * (kRows * 2) + ks * 256u, 128u, sbo),
-                                     smem_desc(wa + ks * 256u, 128u, sbo), idesc, (cc > 0 || ks > 0) ? 1u : 0u);
-                        mma_commit(smem_u32(&sh->empty[s]));
-                    }
-                    mma_commit(smem_u32(&sh->mdone[pc]));
+                                     smem_desc(wa[pc] + ks * 256u, 128u, sbo), instr_desc(kRows, L.ph[pc], false, false),
+                                     (cc > 0 || ks > 0) ? 1u : 0u);
+                    for (int pc = 0; pc < L.n_pieces; ++pc) mma_commit(smem_u32(&sh->empty[(u + pc) % kRing]));
+                    u += L.n_pieces;
                 }
+                for (int pc = 0; pc < L.n_pieces; ++pc) mma_commit(smem_u32(&sh->mdone[pc]));
             }
             __syncwarp();
         } else if (grp < L.n_pieces) {
@@ -674,8 +697,10 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             }
             proxy_fence();
             tc_before();
-            named_sync(2 + pc, 128);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->grp_done[pc]));
             if (leader) {
+                mbar_wait(smem_u32(&sh->grp_done[pc]), uses & 1u, abort);  // the group's piece is written
                 if (!last) {
                     const LayerGeo& Ln = G.l[l + 1];
                     const uint32_t off = static_cast<uint32_t>(Ln.c0[pc]) * (kRows * 2);
@@ -688,8 +713,17 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 bulk_wait_read();
             }
         }
-        if (warp < kEpiWarps && grp < L.n_pieces) ++uses;
-        named_sync(1, kLayerBarThreads);
+        if (warp < kEpiWarps) {
+            // a warp without a piece waits for the previous phase first, so that its
+            // arrival counts for this one
+            if (grp < L.n_pieces)
+                ++uses;
+            else if (lane == 0)
+                mbar_wait(smem_u32(&sh->epi_done), (ph - 1) & 1u, abort);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
+        }
+        ++ph;
         cur ^= 1;
     }
 
@@ -700,28 +734,34 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         const LayerGeo& Lb = G.l[l - 1];
         if (warp == kMmaWarp) {
             if (lane == 0) {
+                mbar_wait(smem_u32(&sh->epi_done), epi_phase++ & 1u, abort);
                 tc_after();
                 const uint32_t a0 = smem_u32(smem + cur * kImgBytes);  // dZ_l
-                for (int cc = 0; cc < L.n_chunks; ++cc) {
-                    const int N = min(L.cw[cc], L.din - L.c0[cc]);
-                    const uint32_t idesc = instr_desc(kRows, N, false, true);
-                    const uint32_t kstride = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;  // 8 outputs of the tile
-                    for (int pc = 0; pc < L.n_pieces; ++pc) {
-                        const uint32_t s = u % kRing, round = u / kRing;
-                        ++u;
-                        const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
-                        tc_after();
-                        const uint32_t sbo_a = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
-                        const uint32_t wa = smem_u32(ring + s * kTileBytes);
-                        for (int ks = 0; ok && ks < (L.ph[pc] >> 4); ++ks)
+                // piece by piece (the K of this GEMM); within a piece the input
+                // chunks (the outputs) take turns per K step
+                for (int pc = 0; pc < L.n_pieces; ++pc) {
+                    bool ok = true;
+                    uint32_t wa[kMaxChunks];
+                    for (int cc = 0; cc < L.n_chunks; ++cc) {
+                        const uint32_t s = (u + cc) % kRing, round = (u + cc) / kRing;
+                        ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort) && ok;
+                        wa[cc] = smem_u32(ring + s * kTileBytes);
+                    }
+                    tc_after();
+                    const uint32_t sbo_a = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
+                    for (int ks = 0; ok && ks < (L.ph[pc] >> 4); ++ks)
+                        for (int cc = 0; cc < L.n_chunks; ++cc) {
+                            const uint32_t kstride = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;  // 8 outputs of the tile
                             mma_bf16(tmem + static_cast<uint32_t>(L.c0[cc]),
                                      smem_desc(a0 + L.p0[pc] * (kRows * 2) + ks * 256u, 128u, sbo_a),
-                                     smem_desc(wa + ks * 2u * kstride, kstride, 128u), idesc,
+                                     smem_desc(wa[cc] + ks * 2u * kstride, kstride, 128u),
+                                     instr_desc(kRows, min(L.cw[cc], L.din - L.c0[cc]), false, true),
                                      (pc > 0 || ks > 0) ? 1u : 0u);
-                        mma_commit(smem_u32(&sh->empty[s]));
-                    }
-                    mma_commit(smem_u32(&sh->mdone[cc]));
+                        }
+                    for (int cc = 0; cc < L.n_chunks; ++cc) mma_commit(smem_u32(&sh->empty[(u + cc) % kRing]));
+                    u += L.n_chunks;
                 }
+                for (int cc = 0; cc < L.n_chunks; ++cc) mma_commit(smem_u32(&sh->mdone[cc]));
             }
             __syncwarp();
         } else if (grp < L.n_chunks) {
@@ -734,8 +774,10 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             if (ok) dx_cols(tm_row + static_cast<uint32_t>(L.c0[cc]), N, L.c0[cc], r, out, Lb, cc, gimg);
             proxy_fence();
             tc_before();
-            named_sync(2 + cc, 128);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->grp_done[cc]));
             if (leader) {
+                mbar_wait(smem_u32(&sh->grp_done[cc]), uses & 1u, abort);
                 const uint32_t off = static_cast<uint32_t>(Lb.p0[cc]) * (kRows * 2);
                 bulk_store(p.scratch + Lb.z_off + tile * Lb.z_tile + off, smem_u32(out) + off,
                            static_cast<uint32_t>(Lb.ph[cc]) * (kRows * 2));
@@ -743,8 +785,15 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 bulk_wait_read();
             }
         }
-        if (warp < kEpiWarps && grp < L.n_chunks) ++uses;
-        named_sync(1, kLayerBarThreads);
+        if (warp < kEpiWarps) {
+            if (grp < L.n_chunks)
+                ++uses;
+            else if (lane == 0)
+                mbar_wait(smem_u32(&sh->epi_done), (ph - 1) & 1u, abort);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
+        }
+        ++ph;
         cur ^= 1;
     }
 
@@ -761,7 +810,8 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         }
     }
     tc_before();
-    __syncthreads();
+    cta_sync();
+    __syncwarp();
     if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
 }
@@ -796,17 +846,22 @@ static_assert(sizeof(DwSmem) <= kDwTail, "k_train_dw: barrier block");
 static_assert(kDwStages * kDwStageBytes + kDwTail <= kDwSmem, "k_train_dw: shared memory");
 static_assert(kRows * (80 + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
 
+// every thread of the cluster (non-aligned: warps may arrive diverged)
 __device__ __forceinline__ void cluster_sync()
 {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
 
-__device__ __forceinline__ float ld_cluster_f32(uint32_t local, uint32_t rank)
+// four floats of CTA `rank`'s shared memory at the local address's offset
+__device__ __forceinline__ float4 ld_cluster_v4(uint32_t local, uint32_t rank)
 {
     uint32_t remote;
-    float v;
+    float4 v;
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
-    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(remote) : "memory");
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(remote)
+                 : "memory");
     return v;
 }
 
@@ -852,7 +907,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
-                     "r"(128)
+                     "r"(kDwAcc * 128)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -863,7 +918,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
         proxy_fence();
     }
     tc_before();
-    __syncthreads();
+    cta_sync();
     tc_after();
     const uint32_t tmem = sh->tmem;
 
@@ -896,7 +951,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
                           static_cast<uint32_t>(cw) * (kRows * 2), full);
         }
     } else if (warp == 0 && lane == 0) {
-        // ---- MMAs: dW (outputs x inputs) += dZ^T X over the row tile, both operands MN-major
+        // ---- MMAs: dW (outputs x inputs) += dZ^T X over the row tile, both operands
+        // MN-major; K step ks accumulates into accumulator ks % kDwAcc, so that
+        // consecutive MMAs are independent (the epilogue adds the accumulators)
         const uint32_t idesc = instr_desc(kRows, cw, true, true);
         for (int k = 0; k < nk; ++k) {
             const int s = k % kDwStages, round = k / kDwStages;
@@ -904,8 +961,8 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
             tc_after();
             const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
             for (int ks = 0; ok && ks < kRows / 16; ++ks)
-                mma_bf16(tmem, smem_desc(a_s + ks * 4096u, 2048u, 128u), smem_desc(b_s + ks * 2u * ncol_b, ncol_b, 128u),
-                         idesc, (k > 0 || ks > 0) ? 1u : 0u);
+                mma_bf16(tmem + static_cast<uint32_t>((ks % kDwAcc) * 128), smem_desc(a_s + ks * 4096u, 2048u, 128u),
+                         smem_desc(b_s + ks * 2u * ncol_b, ncol_b, 128u), idesc, (k > 0 || ks >= kDwAcc) ? 1u : 0u);
             mma_commit(smem_u32(&sh->empty[s]));
         }
         if (nk > 0) mma_commit(smem_u32(&sh->done));
@@ -921,14 +978,21 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
         const int q = warp & 3, hh = warp >> 2;
         const int r = q * 32 + lane;
         for (int u = hh; u < (cw >> 4); u += kDwThreads / 128) {
-            uint32_t v[16];
-            if (ok) tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(u * 16), v);
+            float a[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) a[j] = 0.f;
+            if (ok) {
+#pragma unroll
+                for (int acc = 0; acc < kDwAcc; ++acc) {  // the accumulators in order
+                    uint32_t v[16];
+                    tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * 128 + u * 16), v);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) a[j] += __uint_as_float(v[j]);
+                }
+            }
             float4* d = reinterpret_cast<float4*>(P + r * pitch + u * 16);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                d[j] = ok ? make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
-                                        __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int j = 0; j < 4; ++j) d[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
         }
     }
     tc_before();
@@ -940,25 +1004,44 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
         const int per = (T.oh + static_cast<int>(nrank) - 1) / static_cast<int>(nrank);
         const int rb = static_cast<int>(rank) * per, re = min(T.oh, rb + per);
         const uint32_t pbase = smem_u32(P);
-        for (int idx = tid; idx < (re - rb) * cw; idx += kDwThreads) {
-            const int ol = rb + idx / cw, i = idx % cw;
-            const int o = T.o0 + ol, ia = c0 + i;
-            if (o >= L.dout || ia > L.din) continue;
+        const int q4 = cw >> 2;  // groups of 4 columns
+        for (int idx = tid; idx < (re - rb) * q4; idx += kDwThreads) {
+            const int ol = rb + idx / q4, i = (idx % q4) * 4;
+            const int o = T.o0 + ol;
+            if (o >= L.dout || c0 + i > L.din) continue;
             const uint32_t la = pbase + static_cast<uint32_t>(ol * pitch + i) * 4u;
-            float g = 0.f;
-            for (uint32_t q = 0; q < nrank; ++q) g += ld_cluster_f32(la, q);
-            const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
-            if (p.grad) {
-                p.grad[e] = g;
-            } else {
-                adamw_elem(g, p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr, p.b1, p.b2, p.eps, p.bc1,
-                           p.bc2, reinterpret_cast<__nv_bfloat16*>(p.w_img + L.w_off + w_elem(L, o, ia)));
+            float4 part[kMaxCluster];
+#pragma unroll
+            for (int q = 0; q < kMaxCluster; ++q)
+                if (q < static_cast<int>(nrank)) part[q] = ld_cluster_v4(la, static_cast<uint32_t>(q));
+            float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < kMaxCluster; ++q)  // in rank order
+                if (q < static_cast<int>(nrank)) {
+                    g.x += part[q].x;
+                    g.y += part[q].y;
+                    g.z += part[q].z;
+                    g.w += part[q].w;
+                }
+            const float gv[4] = {g.x, g.y, g.z, g.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int ia = c0 + i + j;
+                if (ia > L.din) break;
+                const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
+                if (p.grad) {
+                    p.grad[e] = gv[j];
+                } else {
+                    adamw_elem(gv[j], p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr, p.b1, p.b2, p.eps,
+                               p.bc1, p.bc2, reinterpret_cast<__nv_bfloat16*>(p.w_img + L.w_off + w_elem(L, o, ia)));
+                }
             }
         }
     }
     cluster_sync();
     if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDwAcc * 128) : "memory");
 }
 
 // ---- packing and the stand-alone AdamW (data parallel) ------------------------
