@@ -16,7 +16,7 @@
 //                dW = dZ^T X over its rows in tensor memory, the partials are
 //                summed over the cluster through distributed shared memory in a
 //                fixed order (so a step is deterministic), and each CTA applies
-//                AdamW to its share of the tile and refreshes the BF16 image.
+//                AdamW to its share of the tile and refreshes the BF16 images.
 //
 // The bias rides in the GEMMs: every layer input carries a column of ones after
 // its features (X_aug = [X | 1 | 0 ...], K padded to 16), and the weights are kept
@@ -24,24 +24,26 @@
 // already holds the bias and the weight gradient's ones column is the bias
 // gradient.
 //
-// Operand layout: K-major core matrices (8 rows x 16 bytes; core (row/8, k/8) of
-// a block at ((row/8) * (width/8) + k/8) * 128 bytes), in column blocks:
-//   * an activation image (128 rows x K_aug) is split into chunks of 64 columns,
-//     the ones-and-padding tail joined to the last chunk (widths 16..80);
-//   * a gradient image (128 rows x N_pad) into pieces of 64 columns;
-//   * a weight image into tiles (64-row piece of N_pad) x (chunk of K_aug).
-// The same bytes serve both orientations: a weight tile is the K-major B operand
-// of the forward GEMM (n = output, k = input) and, read with an MN-major
-// descriptor, the B operand of the input-gradient GEMM (n = input, k = output);
-// the images of X and dZ are the K-major A operands of the layer chain and, read
-// MN-major, the operands of the weight-gradient GEMM (k = rows).  No transposed
-// copy is ever written.  For the MN-major (no swizzle) descriptor the stride byte
-// offset is the core stride along M/N and the leading byte offset the stride
-// between groups of 8 along K.
+// A tcgen05.mma of M = 128 occupies the tensor pipe for about as long at N = 64 as
+// at N = 256 (measured: ~130 cycles either way), so every GEMM here runs the full
+// layer width per instruction.  Operand layout: K-major core matrices (8 rows x
+// 16 bytes; core (row/8, k/8) of a block of width w at ((row/8) * (w/8) + k/8) *
+// 128 bytes):
+//   * an activation image X (128 rows x K_aug) and a gradient image dZ (128 rows
+//     x N_pad) are one block each;
+//   * the forward weights W_aug (N_pad x K_aug) are slabs of 32 input columns
+//     with all output rows (one bulk copy, the B operand of N_pad-wide MMAs);
+//   * the input-gradient GEMM reads W^T (d_in x N_pad), kept as slabs of 32
+//     outputs with all d_in rows, so it too runs d_in-wide MMAs.
+// The weight-gradient GEMM reads the X and dZ images of the row tiles through
+// MN-major descriptors (k = rows; the stride byte offset is the core stride along
+// M/N, the leading byte offset the stride between groups of 8 along K), so no
+// transposed activation is ever written.
 //
 // Every mbarrier wait is bounded (on a timeout the thread records an error and
-// skips the work that depended on it, but still passes every barrier); there is
-// no counterpart in the reference (its pipeline has no learned part).
+// skips the work that depended on it, but still arrives everywhere it is
+// expected); there is no counterpart in the reference (its pipeline has no
+// learned part).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -58,37 +60,34 @@ namespace {
 constexpr int kRows = 128;                 // rows of a tile = MMA M = TMEM lanes
 constexpr int kMaxLayers = PB_TRAIN_MAX_LAYERS;
 constexpr int kMaxWidth = 256;             // largest layer width
-constexpr int kMaxChunks = 5;              // chunks of an activation image (K_aug <= 272)
-constexpr int kMaxPieces = 4;              // 64-column pieces of a layer output (N_pad <= 256)
+constexpr int kMaxPieces = 4;              // 64-column pieces of a layer output (<= 256)
 constexpr int kMaxKaug = 272;
 constexpr int kMaxClasses = 32;            // the cross entropy reads one 32-column TMEM load
+constexpr int kSlab = 32;                  // columns (rows of W^T) of a weight slab
 constexpr long long kWaitPolls = 1ll << 22;
 
 // k_train_fb: 16 epilogue warps (TMEM lane quarter w % 4, output piece w / 4),
-// one MMA-issuing warp, one warp streaming the weight tiles
+// one MMA-issuing warp, one warp streaming the weight slabs
 constexpr int kEpiWarps = 16;
 constexpr int kMmaWarp = kEpiWarps;
 constexpr int kLoadWarp = kEpiWarps + 1;
 constexpr int kFbThreads = (kEpiWarps + 2) * 32;
-constexpr int kRing = 8;                                 // weight-tile slots
-constexpr int kTileBytes = 64 * 80 * 2;                  // largest weight tile
+constexpr int kRing = 5;                                 // weight-slab slots
+constexpr int kSlabBytes = kMaxWidth * kSlab * 2;        // 16 KB
 constexpr int kImgBytes = kRows * kMaxKaug * 2;          // largest activation / gradient image
-constexpr int kFbTail = 1024;                           // barriers, flags, the tile's labels
-// the whole 227 KB: the operand reads of the last ring slots stay inside the
-// allocation whatever stride a descriptor field is read as
-constexpr int kFbSmem = 227 * 1024;
+constexpr int kFbTail = 1024;                            // barriers, flags, the tile's labels
+constexpr int kFbSmem = 2 * kImgBytes + kRing * kSlabBytes + kFbTail;
 
 // k_train_dw
 constexpr int kDwThreads = 256;
-constexpr int kDwStages = 3;
-constexpr int kDwABytes = kRows * kRows * 2;  // 128 outputs x 128 rows
-constexpr int kDwBBytes = kRows * 80 * 2;     // 128 rows x a chunk of <= 80 inputs
+constexpr int kDwStages = 2;
+constexpr int kDwABytes = kRows * kRows * 2;        // 128 outputs x 128 rows
+constexpr int kDwBBytes = kRows * kMaxWidth * 2;    // 128 rows x <= 256 inputs
 constexpr int kDwStageBytes = kDwABytes + kDwBBytes;
 constexpr int kDwTail = 256;
-constexpr int kDwSmem = 227 * 1024;  // as kFbSmem
+constexpr int kDwSmem = kDwStages * kDwStageBytes + kDwTail;
 constexpr int kMaxCluster = 8;
-constexpr int kDwAcc = 4;  // accumulators a weight-gradient CTA rotates its K steps over (128 TMEM columns each)
-constexpr int kMaxDwTiles = kMaxLayers * 2 * kMaxChunks;
+constexpr int kMaxDwTiles = kMaxLayers * 2 * 2;
 
 // ---- geometry ----------------------------------------------------------------
 
@@ -96,13 +95,14 @@ struct LayerGeo {
     int din, dout;        // real widths
     int kaug;             // K of the forward GEMM: din + 1 (ones) rounded up to 16
     int npad;             // output rows padded to 16
-    int n_chunks;         // chunks of the input image
-    int c0[kMaxChunks], cw[kMaxChunks];
-    int n_pieces;         // 64-row pieces of npad
+    int n_pieces;         // 64-column pieces of npad (forward outputs)
     int p0[kMaxPieces], ph[kMaxPieces];
-    int64_t w_off;        // byte offset of this layer's weight image in the image buffer
+    int n_dx;             // 64-column pieces of din (input-gradient outputs, layers >= 1)
+    int d0[kMaxPieces], dw[kMaxPieces];
+    int64_t w_off;        // byte offset of this layer's W slabs in the image buffer
+    int64_t wt_off;       // byte offset of its W^T slabs (layers >= 1)
     int64_t aug_off;      // element offset of this layer in the concatenated augmented (npad x kaug) arrays
-    int64_t x_off, z_off, g_off;  // byte offsets in the scratch of the layer's X / dZ / GELU' images (tile 0)
+    int64_t x_off, z_off, g_off;     // byte offsets in the scratch of the layer's X / dZ / GELU' images (tile 0)
     int64_t x_tile, z_tile, g_tile;  // bytes per row tile
 };
 
@@ -112,28 +112,15 @@ struct Geo {
     int64_t img_bytes, scratch_bytes, aug_elems;
 };
 
-// Chunks of an image of `real` columns followed by the ones column and padding
-// to `aug` (a multiple of 16): 64-column pieces of the real part, the tail on the
-// last piece, and a last chunk of 16 or less joined to the one before it.
-__host__ __device__ inline int split_chunks(int real, int aug, int* c0, int* cw)
+__host__ __device__ inline int split64(int n, int* o0, int* w)
 {
-    int n = 0;
-    for (int c = 0; c < real; c += 64) {
-        c0[n] = c;
-        cw[n] = (real - c < 64) ? real - c : 64;
-        ++n;
+    int k = 0;
+    for (int o = 0; o < n; o += 64) {
+        o0[k] = o;
+        w[k] = n - o < 64 ? n - o : 64;
+        ++k;
     }
-    if (n == 0) {
-        c0[0] = 0;
-        cw[0] = 0;
-        n = 1;
-    }
-    cw[n - 1] = aug - c0[n - 1];  // the tail joins the last piece
-    if (n > 1 && cw[n - 1] <= 16) {
-        cw[n - 2] += cw[n - 1];
-        --n;
-    }
-    return n;
+    return k;
 }
 
 inline int geo_build(int n_layers, const int32_t* dims, int batch, Geo* g)
@@ -152,15 +139,12 @@ inline int geo_build(int n_layers, const int32_t* dims, int batch, Geo* g)
         L.dout = dims[l + 1];
         L.kaug = (L.din + 1 + 15) / 16 * 16;
         L.npad = (L.dout + 15) / 16 * 16;
-        L.n_chunks = split_chunks(L.din, L.kaug, L.c0, L.cw);
-        L.n_pieces = 0;
-        for (int o = 0; o < L.npad; o += 64) {
-            L.p0[L.n_pieces] = o;
-            L.ph[L.n_pieces] = L.npad - o < 64 ? L.npad - o : 64;
-            ++L.n_pieces;
-        }
+        L.n_pieces = split64(L.npad, L.p0, L.ph);
+        L.n_dx = l > 0 ? split64(L.din, L.d0, L.dw) : 0;
         L.w_off = img;
         img += static_cast<int64_t>(L.npad) * L.kaug * 2;
+        L.wt_off = img;
+        if (l > 0) img += static_cast<int64_t>(L.din) * L.npad * 2;
         L.aug_off = aug;
         aug += static_cast<int64_t>(L.npad) * L.kaug;
         L.x_tile = static_cast<int64_t>(kRows) * L.kaug * 2;
@@ -182,30 +166,26 @@ inline int geo_build(int n_layers, const int32_t* dims, int batch, Geo* g)
     return PB_SUCCESS;
 }
 
-// byte offset of weight-image element (o, i) of a layer, relative to the layer's image
+// byte offset of element (r, k) in a single-block image of width w
+__host__ __device__ __forceinline__ uint32_t img_off(int w, int r, int k)
+{
+    return static_cast<uint32_t>((((r >> 3) * (w >> 3) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// byte offset (relative to the layer's W slabs) of weight element (o, i): slab
+// i / 32 holds all npad rows of 32 (or the last 16) columns
 __host__ __device__ inline int64_t w_elem(const LayerGeo& L, int o, int i)
 {
-    int p = o >> 6, c = 0;
-    while (c + 1 < L.n_chunks && i >= L.c0[c + 1]) ++c;
-    const int h = L.ph[p], w = L.cw[c];
-    const int64_t tile = static_cast<int64_t>(L.p0[p]) * L.kaug * 2 + static_cast<int64_t>(h) * L.c0[c] * 2;
-    const int ol = o - L.p0[p], il = i - L.c0[c];
-    return tile + (((ol >> 3) * (w >> 3) + (il >> 3)) << 7) + ((ol & 7) << 4) + ((il & 7) << 1);
+    const int k0 = i / kSlab * kSlab, kw = min(kSlab, L.kaug - k0);
+    return static_cast<int64_t>(L.npad) * k0 * 2 + img_off(kw, o, i - k0);
 }
 
-// byte offset of the weight tile (piece p, chunk c) of a layer
-__host__ __device__ inline int64_t w_tile(const LayerGeo& L, int p, int c)
+// byte offset (relative to the layer's W^T slabs) of weight element (o, i), i < din:
+// slab o / 32 holds all din rows of W^T for 32 (or the last 16) outputs
+__host__ __device__ inline int64_t wt_elem(const LayerGeo& L, int o, int i)
 {
-    return static_cast<int64_t>(L.p0[p]) * L.kaug * 2 + static_cast<int64_t>(L.ph[p]) * L.c0[c] * 2;
-}
-
-// byte offset of element (r, k) in an image whose columns are split into blocks
-// (start b0[j], width bw[j]); blocks are stored one after the other
-__device__ __forceinline__ uint32_t img_off(const int* b0, const int* bw, int j, int r, int k)
-{
-    const int kl = k - b0[j];
-    return static_cast<uint32_t>(b0[j]) * (kRows * 2) + (((r >> 3) * (bw[j] >> 3) + (kl >> 3)) << 7) +
-           ((r & 7) << 4) + ((kl & 7) << 1);
+    const int o0 = o / kSlab * kSlab, ow = min(kSlab, L.npad - o0);
+    return static_cast<int64_t>(L.din) * o0 * 2 + img_off(ow, i, o - o0);
 }
 
 // ---- device helpers ----------------------------------------------------------
@@ -280,7 +260,11 @@ __device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t byt
 }
 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
@@ -379,35 +363,34 @@ struct FbArgs {
     int n_rows;              // rows of x (and labels)
     int M;
     float scale;             // 1 / M: the loss is the minibatch mean
-    const uint8_t* w_img;    // BF16 weight images, all layers
+    const uint8_t* w_img;    // BF16 weight slabs, all layers
     uint8_t* scratch;        // X / dZ / GELU' images of the minibatch's row tiles
     float* loss_sum;
     int32_t* correct;
     int32_t* error;
 };
 
-// Shared memory of k_train_fb: two image buffers (the layer chain alternates
-// between them), the weight-tile ring, then barriers and flags.
-// full / empty: the weight-tile ring; mdone[j]: the MMAs of output piece j are
-// done; grp_done[j]: the 4 warps of epilogue group j wrote their piece; epi_done:
-// every epilogue warp finished the phase (the MMA warp starts the next layer)
+// full / empty: the weight-slab ring; mdone: the MMAs of a phase are done;
+// epi_done: every epilogue warp finished the phase (the MMA warp starts the next)
 struct FbSmem {
-    uint64_t full[kRing], empty[kRing], mdone[kMaxPieces], grp_done[kMaxPieces], epi_done;
+    uint64_t full[kRing], empty[kRing], mdone, epi_done;
     uint32_t tmem;
     int abort;
     int y[kRows];
 };
 static_assert(sizeof(FbSmem) <= kFbTail, "k_train_fb: barrier block");
-static_assert(2 * kImgBytes + kRing * kTileBytes + kFbTail <= kFbSmem, "k_train_fb: shared memory");
+static_assert(kFbSmem <= 227 * 1024, "k_train_fb: shared memory");
 
-// Epilogue of one forward piece of a hidden layer: z (TMEM columns p0 .. p0 + h)
-// -> GELU(z) into the next layer's input image, GELU'(z) (FP16) to global.
-__device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* xo,
-                                                const LayerGeo& Ln, int chunk, uint8_t* gimg)
+// Epilogue of one forward piece of a hidden layer: z (TMEM columns col0 .. col0 +
+// ncols) -> GELU(z) into the next layer's input image (width wn), GELU'(z) (FP16)
+// to global.
+__device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* xo, int wn,
+                                                uint8_t* gimg)
 {
     for (int cc = 0; cc < ncols; cc += 32) {
+        const int n = ncols - cc >= 32 ? 32 : 16;
         float z[32];
-        if (ncols - cc >= 32) {
+        if (n == 32) {
             uint32_t v[32];
             tmem_ld32(tm + static_cast<uint32_t>(cc), v);
 #pragma unroll
@@ -420,10 +403,9 @@ __device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0
 #pragma unroll
             for (int j = 16; j < 32; ++j) z[j] = 0.f;
         }
-        const int groups = (ncols - cc >= 32 ? 32 : 16) >> 3;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            if (q >= groups) break;
+            if (q * 8 >= n) break;
             uint32_t hx[4], hd[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -434,7 +416,7 @@ __device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0
                 hd[k] = pack_f16(d0, d1);
             }
             const int col = col0 + cc + q * 8;
-            *reinterpret_cast<uint4*>(xo + img_off(Ln.c0, Ln.cw, chunk, r, col)) = make_uint4(hx[0], hx[1], hx[2], hx[3]);
+            *reinterpret_cast<uint4*>(xo + img_off(wn, r, col)) = make_uint4(hx[0], hx[1], hx[2], hx[3]);
             *reinterpret_cast<uint4*>(gimg + ((static_cast<int64_t>(col >> 3) * kRows + r) << 4)) =
                 make_uint4(hd[0], hd[1], hd[2], hd[3]);
         }
@@ -442,9 +424,9 @@ __device__ __forceinline__ void fwd_hidden_cols(uint32_t tm, int ncols, int col0
 }
 
 // Epilogue of one input-gradient piece: dZ_below = acc * GELU'(Z_below) (TMEM
-// columns c0 .. c0 + n) into the gradient image of the layer below.
-__device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* zo, const LayerGeo& Lb,
-                                        int piece, const uint8_t* gimg)
+// columns col0 .. col0 + ncols) into the gradient image (width wb) of the layer below.
+__device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r, uint8_t* zo, int wb,
+                                        const uint8_t* gimg)
 {
     for (int cc = 0; cc < ncols; cc += 32) {
         const int n = ncols - cc >= 32 ? 32 : 16;
@@ -452,7 +434,8 @@ __device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r,
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (q * 8 < n)
-                gd[q] = __ldg(reinterpret_cast<const uint4*>(gimg + ((static_cast<int64_t>((col0 + cc) / 8 + q) * kRows + r) << 4)));
+                gd[q] = __ldg(reinterpret_cast<const uint4*>(
+                    gimg + ((static_cast<int64_t>((col0 + cc) / 8 + q) * kRows + r) << 4)));
         float a[32];
         if (n == 32) {
             uint32_t v[32];
@@ -477,8 +460,7 @@ __device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r,
                 const float2 d = unpack_f16(gw[k]);
                 h[k] = pack_bf16(a[q * 8 + 2 * k] * d.x, a[q * 8 + 2 * k + 1] * d.y);
             }
-            *reinterpret_cast<uint4*>(zo + img_off(Lb.p0, Lb.ph, piece, r, col0 + cc + q * 8)) =
-                make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4*>(zo + img_off(wb, r, col0 + cc + q * 8)) = make_uint4(h[0], h[1], h[2], h[3]);
         }
     }
 }
@@ -486,9 +468,9 @@ __device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r,
 __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constant__ FbArgs p)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
-    // image buffer b at smem + b * kImgBytes
+    // image buffer b at smem + b * kImgBytes, then the slab ring, then FbSmem
     uint8_t* ring = smem + 2 * kImgBytes;
-    FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kTileBytes);
+    FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kSlabBytes);
     volatile int* abort = &sh->abort;
     const Geo& G = p.geo;
     const int NL = G.n_layers;
@@ -502,10 +484,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             mbar_init(smem_u32(&sh->full[s]), 1);
             mbar_init(smem_u32(&sh->empty[s]), 1);
         }
-        for (int j = 0; j < kMaxPieces; ++j) {
-            mbar_init(smem_u32(&sh->mdone[j]), 1);
-            mbar_init(smem_u32(&sh->grp_done[j]), 4);
-        }
+        mbar_init(smem_u32(&sh->mdone), 1);
         mbar_init(smem_u32(&sh->epi_done), kEpiWarps);
         sh->abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -522,47 +501,112 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     const uint32_t tmem = sh->tmem;
 
     if (warp == kLoadWarp) {
-        // ---- weight tiles into the ring, in the order the MMA warp consumes them
+        // ---- weight slabs into the ring, in the order the MMA warp consumes them:
+        // forward W slabs of every layer, then the W^T slabs from the last layer down
         if (lane == 0) {
             uint32_t u = 0;
-            auto put = [&](const LayerGeo& L, int pc, int cc) {
+            auto put = [&](int64_t off, uint32_t bytes) {
                 const uint32_t s = u % kRing, round = u / kRing;
                 ++u;
                 if (round > 0 && !mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1u, abort)) return;
-                const uint32_t bytes = static_cast<uint32_t>(L.ph[pc]) * L.cw[cc] * 2u;
                 mbar_expect_tx(smem_u32(&sh->full[s]), bytes);
-                bulk_load(smem_u32(ring + s * kTileBytes), p.w_img + L.w_off + w_tile(L, pc, cc), bytes,
-                          smem_u32(&sh->full[s]));
+                bulk_load(smem_u32(ring + s * kSlabBytes), p.w_img + off, bytes, smem_u32(&sh->full[s]));
             };
-            // forward: chunk by chunk, every output piece of a chunk; input
-            // gradients: piece by piece, every input chunk of a piece (the order in
-            // which the MMA warp interleaves its accumulators)
             for (int l = 0; l < NL && !*abort; ++l) {
                 const LayerGeo& L = G.l[l];
-                for (int cc = 0; cc < L.n_chunks; ++cc)
-                    for (int pc = 0; pc < L.n_pieces; ++pc) put(L, pc, cc);
+                for (int k0 = 0; k0 < L.kaug; k0 += kSlab)
+                    put(L.w_off + static_cast<int64_t>(L.npad) * k0 * 2,
+                        static_cast<uint32_t>(L.npad) * min(kSlab, L.kaug - k0) * 2u);
             }
             for (int l = NL - 1; l >= 1 && !*abort; --l) {
                 const LayerGeo& L = G.l[l];
-                for (int pc = 0; pc < L.n_pieces; ++pc)
-                    for (int cc = 0; cc < L.n_chunks; ++cc) put(L, pc, cc);
+                for (int o0 = 0; o0 < L.npad; o0 += kSlab)
+                    put(L.wt_off + static_cast<int64_t>(L.din) * o0 * 2,
+                        static_cast<uint32_t>(L.din) * min(kSlab, L.npad - o0) * 2u);
             }
         }
+        __syncwarp();
         cta_sync();
         if (tid == kLoadWarp * 32 && *abort && p.error) atomicExch(p.error, 1);
         return;
     }
 
-    // ---- the row tile's inputs: rows of x by the minibatch's indices, the ones
-    // column after them, zero rows past the minibatch
-    if (warp < kEpiWarps) {
+    if (warp == kMmaWarp) {
+        // ---- MMAs, one phase per layer: the previous phase's epilogues are done,
+        // the image they consumed and the one they wrote are final; the MMAs read the
+        // latter, and its copy to global scratch (for the weight gradients) starts
+        if (lane == 0) {
+            uint32_t u = 0, ep = 0;
+            int cur = 0;
+            auto begin_phase = [&](uint8_t* dst, uint32_t bytes) {
+                mbar_wait(smem_u32(&sh->epi_done), ep++ & 1u, abort);
+                tc_after();
+                bulk_store(dst, smem_u32(smem + cur * kImgBytes), bytes);
+                bulk_commit();
+                bulk_wait_read<1>();  // the copy of two phases ago has read its buffer
+            };
+            auto slab = [&](uint32_t& s) {
+                s = u % kRing;
+                const uint32_t round = u / kRing;
+                ++u;
+                const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
+                tc_after();
+                return ok;
+            };
+            for (int l = 0; l < NL; ++l) {  // forward: Z_l (128 x npad) = X_l W_l^T, K = kaug
+                const LayerGeo& L = G.l[l];
+                begin_phase(p.scratch + L.x_off + tile * L.x_tile, static_cast<uint32_t>(L.x_tile));
+                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
+                const uint32_t sbo_a = static_cast<uint32_t>(L.kaug >> 3) << 7;
+                const uint32_t idesc = instr_desc(kRows, L.npad, false, false);
+                for (int k0 = 0; k0 < L.kaug; k0 += kSlab) {
+                    uint32_t s;
+                    const bool ok = slab(s);
+                    const int kw = min(kSlab, L.kaug - k0);
+                    const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
+                    for (int ks = 0; ok && ks < (kw >> 4); ++ks)
+                        mma_bf16(tmem, smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                 smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                    mma_commit(smem_u32(&sh->empty[s]));
+                }
+                mma_commit(smem_u32(&sh->mdone));
+                cur ^= 1;
+            }
+            for (int l = NL - 1; l >= 1; --l) {  // input gradients: (128 x din) = dZ_l W_l, K = npad
+                const LayerGeo& L = G.l[l];
+                begin_phase(p.scratch + L.z_off + tile * L.z_tile, static_cast<uint32_t>(L.z_tile));
+                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
+                const uint32_t sbo_a = static_cast<uint32_t>(L.npad >> 3) << 7;
+                const uint32_t idesc = instr_desc(kRows, L.din, false, false);
+                for (int o0 = 0; o0 < L.npad; o0 += kSlab) {
+                    uint32_t s;
+                    const bool ok = slab(s);
+                    const int ow = min(kSlab, L.npad - o0);
+                    const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(ow >> 3) << 7;
+                    for (int ks = 0; ok && ks < (ow >> 4); ++ks)
+                        mma_bf16(tmem, smem_desc(a0 + ((o0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                 smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (o0 > 0 || ks > 0) ? 1u : 0u);
+                    mma_commit(smem_u32(&sh->empty[s]));
+                }
+                mma_commit(smem_u32(&sh->mdone));
+                cur ^= 1;
+            }
+            // the last image written (dZ_0) to scratch once its phase is done
+            mbar_wait(smem_u32(&sh->epi_done), ep++ & 1u, abort);
+            bulk_store(p.scratch + G.l[0].z_off + tile * G.l[0].z_tile, smem_u32(smem + cur * kImgBytes),
+                       static_cast<uint32_t>(G.l[0].z_tile));
+            bulk_commit();
+            bulk_wait_all();
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue warps: the inputs of the row tile first (rows of x by the
+        // minibatch's indices, the ones column after them, zero rows past the minibatch)
         const LayerGeo& L0 = G.l[0];
         const int pieces = L0.kaug >> 3;
         for (int idx = tid; idx < kRows * pieces; idx += kEpiWarps * 32) {
             const int r = idx & (kRows - 1), col = (idx >> 7) << 3;
-            int c = 0;
-            while (c + 1 < L0.n_chunks && col >= L0.c0[c + 1]) ++c;
-            uint8_t* dst = smem + img_off(L0.c0, L0.cw, c, r, col);
+            uint8_t* dst = smem + img_off(L0.kaug, r, col);
             const int row = r < mt ? __ldg(p.rows + m0 + r) : -1;
             const bool in_range = row >= 0 && row < p.n_rows;
             if (r < mt && !in_range && col == 0) sh->abort = 1;  // a row index outside x: reported, not read
@@ -582,223 +626,111 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         proxy_fence();
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
-    }
-    if (tid == 0) {
-        mbar_wait(smem_u32(&sh->epi_done), 0, abort);
-        bulk_store(p.scratch + G.l[0].x_off + tile * G.l[0].x_tile, smem_u32(smem),
-                   static_cast<uint32_t>(G.l[0].x_tile));
-        bulk_commit();
-    }
 
-    const int quarter = warp & 3, grp = warp >> 2;
-    const int r = quarter * 32 + lane;  // this thread's row (TMEM lane)
-    const uint32_t tm_row = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
-    const bool leader = (tid & 127) == 0 && warp < kEpiWarps;
-    uint32_t u = 0;                      // weight tiles consumed (MMA warp)
-    uint32_t uses = 0;                   // waits on mdone[grp] so far (epilogue warps)
-    uint32_t epi_phase = 0;              // phases of epi_done waited for (MMA warp)
-    uint32_t ph = 1;                     // this phase of epi_done (the gather was phase 0)
-    int cur = 0;
-    float loss = 0.f;
-    int hits = 0;
-
-    // ---- forward
-    for (int l = 0; l < NL; ++l) {
-        const LayerGeo& L = G.l[l];
-        const bool last = l + 1 == NL;
-        if (warp == kMmaWarp) {
-            if (lane == 0) {
-                mbar_wait(smem_u32(&sh->epi_done), epi_phase++ & 1u, abort);  // the inputs are written
+        const int quarter = warp & 3, grp = warp >> 2;
+        const int r = quarter * 32 + lane;  // this thread's row (TMEM lane)
+        const uint32_t tm_row = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+        uint32_t ph = 1;                    // this phase (the gather was phase 0)
+        int cur = 0;
+        float loss = 0.f;
+        int hits = 0;
+        // one phase of the epilogue.  Every warp waits for the phase's MMAs (mdone
+        // completes once per phase, and a wait by parity cannot tell phases two
+        // apart, so no warp may skip one), works on its piece if it has one, and
+        // arrives on epi_done.
+        auto end_phase = [&](bool worked) {
+            if (worked) {
+                proxy_fence();
+                tc_before();
+            } else if (lane == 0) {
+                mbar_wait(smem_u32(&sh->mdone), (ph - 1) & 1u, abort);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
+            ++ph;
+            cur ^= 1;
+        };
+        for (int l = 0; l < NL; ++l) {
+            const LayerGeo& L = G.l[l];
+            const bool last = l + 1 == NL;
+            const bool mine = last ? grp == 0 : grp < L.n_pieces;
+            if (mine) {
+                const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone), (ph - 1) & 1u, abort));
                 tc_after();
-                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
-                // chunk by chunk; within a chunk the output pieces take turns per K
-                // step, so consecutive MMAs feed independent accumulators
-                for (int cc = 0; cc < L.n_chunks; ++cc) {
-                    bool ok = true;
-                    uint32_t wa[kMaxPieces];
-                    for (int pc = 0; pc < L.n_pieces; ++pc) {
-                        const uint32_t s = (u + pc) % kRing, round = (u + pc) / kRing;
-                        ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort) && ok;
-                        wa[pc] = smem_u32(ring + s * kTileBytes);
-                    }
-                    tc_after();
-                    const uint32_t sbo = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;
-                    for (int ks = 0; ok && ks < (L.cw[cc] >> 4); ++ks)
-                        for (int pc = 0; pc < L.n_pieces; ++pc)
-                            mma_bf16(tmem + static_cast<uint32_t>(L.p0[pc]),
-                                     smem_desc(a0 + L.c0[cc] * (kRows * 2) + ks * 256u, 128u, sbo),
-                                     smem_desc(wa[pc] + ks * 256u, 128u, sbo), instr_desc(kRows, L.ph[pc], false, false),
-                                     (cc > 0 || ks > 0) ? 1u : 0u);
-                    for (int pc = 0; pc < L.n_pieces; ++pc) mma_commit(smem_u32(&sh->empty[(u + pc) % kRing]));
-                    u += L.n_pieces;
-                }
-                for (int pc = 0; pc < L.n_pieces; ++pc) mma_commit(smem_u32(&sh->mdone[pc]));
-            }
-            __syncwarp();
-        } else if (grp < L.n_pieces) {
-            const int pc = grp;
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone[pc]), uses & 1u, abort));
-            tc_after();
-            uint8_t* out = smem + (cur ^ 1) * kImgBytes;
-            if (!last) {
-                const LayerGeo& Ln = G.l[l + 1];
-                uint8_t* gimg = p.scratch + L.g_off + tile * L.g_tile;
-                if (ok) fwd_hidden_cols(tm_row + static_cast<uint32_t>(L.p0[pc]), L.ph[pc], L.p0[pc], r, out, Ln, pc, gimg);
-                if (pc == L.n_pieces - 1) {
-                    // the ones column of the next layer's input, then zeros to its K
-                    for (int col = L.dout; col < Ln.kaug; col += 8) {
-                        const uint32_t one = (r < mt && col == L.dout) ? 0x3F80u : 0u;
-                        *reinterpret_cast<uint4*>(out + img_off(Ln.c0, Ln.cw, pc, r, col)) = make_uint4(one, 0u, 0u, 0u);
-                    }
-                }
-            } else {
-                // softmax cross entropy of the logits (TMEM columns 0 .. npad)
-                uint32_t v[32];
-                if (ok) tmem_ld32(tm_row, v);
-                const int C = L.dout;
-                const int y = sh->y[r];
-                float z[32];
-                float mx = -CUDART_INF_F, zy = 0.f;
-                int arg = 0;
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    z[c] = __uint_as_float(v[c]);
-                    if (c < C && z[c] > mx) {
-                        mx = z[c];
-                        arg = c;
-                    }
-                    if (c == y) zy = z[c];
-                }
-                float se = 0.f;
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    z[c] = c < C ? __expf(z[c] - mx) : 0.f;
-                    se += z[c];
-                }
-                const float inv = 1.f / se;
-                const bool valid = r < mt && ok;
-#pragma unroll
-                for (int c8 = 0; c8 < 32; c8 += 8) {
-                    if (c8 >= L.npad) break;
-                    uint32_t h[4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int c = c8 + 2 * k;
-                        const float d0 = valid ? (z[c] * inv - (c == y ? 1.f : 0.f)) * p.scale : 0.f;
-                        const float d1 = valid ? (z[c + 1] * inv - (c + 1 == y ? 1.f : 0.f)) * p.scale : 0.f;
-                        h[k] = pack_bf16(d0, d1);
-                    }
-                    *reinterpret_cast<uint4*>(out + img_off(L.p0, L.ph, 0, r, c8)) = make_uint4(h[0], h[1], h[2], h[3]);
-                }
-                if (valid && y >= 0 && y < C) {
-                    loss = -(zy - mx - __logf(se));
-                    hits = arg == y ? 1 : 0;
-                }
-            }
-            proxy_fence();
-            tc_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh->grp_done[pc]));
-            if (leader) {
-                mbar_wait(smem_u32(&sh->grp_done[pc]), uses & 1u, abort);  // the group's piece is written
+                uint8_t* out = smem + (cur ^ 1) * kImgBytes;
                 if (!last) {
                     const LayerGeo& Ln = G.l[l + 1];
-                    const uint32_t off = static_cast<uint32_t>(Ln.c0[pc]) * (kRows * 2);
-                    bulk_store(p.scratch + Ln.x_off + tile * Ln.x_tile + off, smem_u32(out) + off,
-                               static_cast<uint32_t>(Ln.cw[pc]) * (kRows * 2));
-                } else {
-                    bulk_store(p.scratch + L.z_off + tile * L.z_tile, smem_u32(out), static_cast<uint32_t>(L.z_tile));
-                }
-                bulk_commit();
-                bulk_wait_read();
-            }
-        }
-        if (warp < kEpiWarps) {
-            // a warp without a piece waits for the previous phase first, so that its
-            // arrival counts for this one
-            if (grp < L.n_pieces)
-                ++uses;
-            else if (lane == 0)
-                mbar_wait(smem_u32(&sh->epi_done), (ph - 1) & 1u, abort);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
-        }
-        ++ph;
-        cur ^= 1;
-    }
-
-    // ---- input gradients, last layer first: dZ_l-1 = (dZ_l W_l) * GELU'(Z_l-1);
-    // output piece j is input chunk j of layer l (its real columns)
-    for (int l = NL - 1; l >= 1; --l) {
-        const LayerGeo& L = G.l[l];
-        const LayerGeo& Lb = G.l[l - 1];
-        if (warp == kMmaWarp) {
-            if (lane == 0) {
-                mbar_wait(smem_u32(&sh->epi_done), epi_phase++ & 1u, abort);
-                tc_after();
-                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);  // dZ_l
-                // piece by piece (the K of this GEMM); within a piece the input
-                // chunks (the outputs) take turns per K step
-                for (int pc = 0; pc < L.n_pieces; ++pc) {
-                    bool ok = true;
-                    uint32_t wa[kMaxChunks];
-                    for (int cc = 0; cc < L.n_chunks; ++cc) {
-                        const uint32_t s = (u + cc) % kRing, round = (u + cc) / kRing;
-                        ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort) && ok;
-                        wa[cc] = smem_u32(ring + s * kTileBytes);
-                    }
-                    tc_after();
-                    const uint32_t sbo_a = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
-                    for (int ks = 0; ok && ks < (L.ph[pc] >> 4); ++ks)
-                        for (int cc = 0; cc < L.n_chunks; ++cc) {
-                            const uint32_t kstride = static_cast<uint32_t>(L.cw[cc] >> 3) << 7;  // 8 outputs of the tile
-                            mma_bf16(tmem + static_cast<uint32_t>(L.c0[cc]),
-                                     smem_desc(a0 + L.p0[pc] * (kRows * 2) + ks * 256u, 128u, sbo_a),
-                                     smem_desc(wa[cc] + ks * 2u * kstride, kstride, 128u),
-                                     instr_desc(kRows, min(L.cw[cc], L.din - L.c0[cc]), false, true),
-                                     (pc > 0 || ks > 0) ? 1u : 0u);
+                    const int pc = grp;
+                    if (ok)
+                        fwd_hidden_cols(tm_row + static_cast<uint32_t>(L.p0[pc]), L.ph[pc], L.p0[pc], r, out, Ln.kaug,
+                                        p.scratch + L.g_off + tile * L.g_tile);
+                    if (pc == L.n_pieces - 1) {
+                        // the ones column of the next layer's input, then zeros to its K
+                        for (int col = L.dout; col < Ln.kaug; col += 8) {
+                            const uint32_t one = (r < mt && col == L.dout) ? 0x3F80u : 0u;
+                            *reinterpret_cast<uint4*>(out + img_off(Ln.kaug, r, col)) = make_uint4(one, 0u, 0u, 0u);
                         }
-                    for (int cc = 0; cc < L.n_chunks; ++cc) mma_commit(smem_u32(&sh->empty[(u + cc) % kRing]));
-                    u += L.n_chunks;
+                    }
+                } else {
+                    // softmax cross entropy of the logits (TMEM columns 0 .. npad)
+                    uint32_t v[32];
+                    if (ok) tmem_ld32(tm_row, v);
+                    const int C = L.dout;
+                    const int y = sh->y[r];
+                    float z[32];
+                    float mx = -CUDART_INF_F, zy = 0.f;
+                    int arg = 0;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        z[c] = __uint_as_float(v[c]);
+                        if (c < C && z[c] > mx) {
+                            mx = z[c];
+                            arg = c;
+                        }
+                        if (c == y) zy = z[c];
+                    }
+                    float se = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        z[c] = c < C ? __expf(z[c] - mx) : 0.f;
+                        se += z[c];
+                    }
+                    const float inv = 1.f / se;
+                    const bool valid = r < mt && ok;
+#pragma unroll
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        if (c8 >= L.npad) break;
+                        uint32_t h[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int c = c8 + 2 * k;
+                            const float d0 = valid ? (z[c] * inv - (c == y ? 1.f : 0.f)) * p.scale : 0.f;
+                            const float d1 = valid ? (z[c + 1] * inv - (c + 1 == y ? 1.f : 0.f)) * p.scale : 0.f;
+                            h[k] = pack_bf16(d0, d1);
+                        }
+                        *reinterpret_cast<uint4*>(out + img_off(L.npad, r, c8)) = make_uint4(h[0], h[1], h[2], h[3]);
+                    }
+                    if (valid && y >= 0 && y < C) {
+                        loss = -(zy - mx - __logf(se));
+                        hits = arg == y ? 1 : 0;
+                    }
                 }
-                for (int cc = 0; cc < L.n_chunks; ++cc) mma_commit(smem_u32(&sh->mdone[cc]));
             }
-            __syncwarp();
-        } else if (grp < L.n_chunks) {
-            const int cc = grp;
-            const int N = min(L.cw[cc], L.din - L.c0[cc]);
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone[cc]), uses & 1u, abort));
-            tc_after();
-            uint8_t* out = smem + (cur ^ 1) * kImgBytes;
-            const uint8_t* gimg = p.scratch + Lb.g_off + tile * Lb.g_tile;
-            if (ok) dx_cols(tm_row + static_cast<uint32_t>(L.c0[cc]), N, L.c0[cc], r, out, Lb, cc, gimg);
-            proxy_fence();
-            tc_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh->grp_done[cc]));
-            if (leader) {
-                mbar_wait(smem_u32(&sh->grp_done[cc]), uses & 1u, abort);
-                const uint32_t off = static_cast<uint32_t>(Lb.p0[cc]) * (kRows * 2);
-                bulk_store(p.scratch + Lb.z_off + tile * Lb.z_tile + off, smem_u32(out) + off,
-                           static_cast<uint32_t>(Lb.ph[cc]) * (kRows * 2));
-                bulk_commit();
-                bulk_wait_read();
+            end_phase(mine);
+        }
+        for (int l = NL - 1; l >= 1; --l) {
+            const LayerGeo& L = G.l[l];
+            const LayerGeo& Lb = G.l[l - 1];
+            const bool mine = grp < L.n_dx;
+            if (mine) {
+                const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone), (ph - 1) & 1u, abort));
+                tc_after();
+                if (ok)
+                    dx_cols(tm_row + static_cast<uint32_t>(L.d0[grp]), L.dw[grp], L.d0[grp], r,
+                            smem + (cur ^ 1) * kImgBytes, Lb.npad, p.scratch + Lb.g_off + tile * Lb.g_tile);
             }
+            end_phase(mine);
         }
-        if (warp < kEpiWarps) {
-            if (grp < L.n_chunks)
-                ++uses;
-            else if (lane == 0)
-                mbar_wait(smem_u32(&sh->epi_done), (ph - 1) & 1u, abort);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
-        }
-        ++ph;
-        cur ^= 1;
-    }
-
-    if (leader) bulk_wait_all();
-    if (warp < kEpiWarps) {
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
             loss += __shfl_xor_sync(0xffffffffu, loss, o);
@@ -819,7 +751,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
 // ---- weight gradients and AdamW ---------------------------------------------
 
 struct DwTile {
-    int layer, o0, oh, chunk;  // outputs [o0, o0 + oh) x input chunk
+    int layer, o0, oh, i0, iw;  // outputs [o0, o0 + oh) x inputs [i0, i0 + iw)
 };
 
 struct DwArgs {
@@ -843,8 +775,8 @@ struct DwSmem {
     int abort;
 };
 static_assert(sizeof(DwSmem) <= kDwTail, "k_train_dw: barrier block");
-static_assert(kDwStages * kDwStageBytes + kDwTail <= kDwSmem, "k_train_dw: shared memory");
-static_assert(kRows * (80 + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
+static_assert(kDwSmem <= 227 * 1024, "k_train_dw: shared memory");
+static_assert(kRows * (kMaxWidth + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
 
 // every thread of the cluster (non-aligned: warps may arrive diverged)
 __device__ __forceinline__ void cluster_sync()
@@ -865,8 +797,8 @@ __device__ __forceinline__ float4 ld_cluster_v4(uint32_t local, uint32_t rank)
     return v;
 }
 
-__device__ __forceinline__ void adamw_elem(float g, float* w, float* m1, float* m2, float wd, float lr, float b1,
-                                           float b2, float eps, float bc1, float bc2, __nv_bfloat16* img)
+__device__ __forceinline__ float adamw_elem(float g, float* w, float* m1, float* m2, float wd, float lr, float b1,
+                                            float b2, float eps, float bc1, float bc2)
 {
     const float a = b1 * *m1 + (1.f - b1) * g;
     const float b = b2 * *m2 + (1.f - b2) * g * g;
@@ -875,7 +807,15 @@ __device__ __forceinline__ void adamw_elem(float g, float* w, float* m1, float* 
     float x = *w * (1.f - lr * wd);
     x -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
     *w = x;
-    *img = __float2bfloat16(x);
+    return x;
+}
+
+// the BF16 images of augmented weight (o, i): the forward slab, and W^T for i < din
+__device__ __forceinline__ void store_images(uint8_t* w_img, const LayerGeo& L, int layer, int o, int i, float x)
+{
+    const __nv_bfloat16 h = __float2bfloat16(x);
+    *reinterpret_cast<__nv_bfloat16*>(w_img + L.w_off + w_elem(L, o, i)) = h;
+    if (layer > 0 && i < L.din) *reinterpret_cast<__nv_bfloat16*>(w_img + L.wt_off + wt_elem(L, o, i)) = h;
 }
 
 __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constant__ DwArgs p)
@@ -893,8 +833,8 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
     const int t0 = static_cast<int>(rank) * tiles / static_cast<int>(nrank);
     const int t1 = (static_cast<int>(rank) + 1) * tiles / static_cast<int>(nrank);
     const int nk = t1 - t0;
-    const int cw = L.cw[T.chunk], c0 = L.c0[T.chunk];
-    const uint32_t ncol_b = static_cast<uint32_t>(cw >> 3) << 7;  // bytes of one row group of the X chunk
+    const int iw = T.iw;
+    const uint32_t ncol_b = static_cast<uint32_t>(iw >> 3) << 7;  // bytes of one row group of the staged inputs
 
     if (tid == 0) {
         for (int s = 0; s < kDwStages; ++s) {
@@ -907,7 +847,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
-                     "r"(kDwAcc * 128)
+                     "r"(256)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -923,10 +863,9 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
     const uint32_t tmem = sh->tmem;
 
     if (warp == 1) {
-        // ---- producer: per row tile, dZ of the outputs (row group by row group, the
-        // 64-output pieces side by side) and the X chunk (one contiguous block)
-        int pa = 0;
-        while (pa + 1 < L.n_pieces && L.p0[pa + 1] <= T.o0) ++pa;
+        // ---- producer: per row tile, row group g of the dZ image (the tile's
+        // outputs) by lane g, and row group g of the X image (the tile's inputs) by
+        // lane 16 + g
         for (int k = 0; k < nk; ++k) {
             const int s = k % kDwStages, round = k / kDwStages;
             bool ok = true;
@@ -934,65 +873,58 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             const uint32_t full = smem_u32(&sh->full[s]);
-            if (lane == 0) mbar_expect_tx(full, static_cast<uint32_t>(T.oh) * (kRows * 2) + static_cast<uint32_t>(cw) * (kRows * 2));
+            if (lane == 0) mbar_expect_tx(full, static_cast<uint32_t>(T.oh + iw) * (kRows * 2));
             __syncwarp();
             const int t = t0 + k;
             const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
-            const int pc = pa + (lane >> 4), g = lane & 15;
-            if (pc < L.n_pieces && L.p0[pc] < T.o0 + T.oh) {
-                const uint32_t bytes = static_cast<uint32_t>(L.ph[pc] >> 3) << 7;
-                bulk_load(a_s + g * 2048u + (static_cast<uint32_t>(L.p0[pc] - T.o0) >> 3) * 128u,
+            const int g = lane & 15;
+            if (lane < 16) {
+                const uint32_t bytes = static_cast<uint32_t>(T.oh >> 3) << 7;
+                bulk_load(a_s + g * 2048u,
                           p.scratch + L.z_off + static_cast<int64_t>(t) * L.z_tile +
-                              static_cast<int64_t>(L.p0[pc]) * (kRows * 2) + g * bytes,
+                              (static_cast<int64_t>(g) * (L.npad >> 3) + (T.o0 >> 3)) * 128,
                           bytes, full);
+            } else {
+                bulk_load(b_s + g * ncol_b,
+                          p.scratch + L.x_off + static_cast<int64_t>(t) * L.x_tile +
+                              (static_cast<int64_t>(g) * (L.kaug >> 3) + (T.i0 >> 3)) * 128,
+                          ncol_b, full);
             }
-            if (lane == 0)
-                bulk_load(b_s, p.scratch + L.x_off + static_cast<int64_t>(t) * L.x_tile + static_cast<int64_t>(c0) * (kRows * 2),
-                          static_cast<uint32_t>(cw) * (kRows * 2), full);
         }
     } else if (warp == 0 && lane == 0) {
-        // ---- MMAs: dW (outputs x inputs) += dZ^T X over the row tile, both operands
-        // MN-major; K step ks accumulates into accumulator ks % kDwAcc, so that
-        // consecutive MMAs are independent (the epilogue adds the accumulators)
-        const uint32_t idesc = instr_desc(kRows, cw, true, true);
+        // ---- MMAs: dW (outputs x inputs) += dZ^T X over the row tile, both operands MN-major
+        const uint32_t idesc = instr_desc(kRows, iw, true, true);
         for (int k = 0; k < nk; ++k) {
             const int s = k % kDwStages, round = k / kDwStages;
             const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1, abort);
             tc_after();
             const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
             for (int ks = 0; ok && ks < kRows / 16; ++ks)
-                mma_bf16(tmem + static_cast<uint32_t>((ks % kDwAcc) * 128), smem_desc(a_s + ks * 4096u, 2048u, 128u),
-                         smem_desc(b_s + ks * 2u * ncol_b, ncol_b, 128u), idesc, (k > 0 || ks >= kDwAcc) ? 1u : 0u);
+                mma_bf16(tmem, smem_desc(a_s + ks * 4096u, 2048u, 128u), smem_desc(b_s + ks * 2u * ncol_b, ncol_b, 128u),
+                         idesc, (k > 0 || ks > 0) ? 1u : 0u);
             mma_commit(smem_u32(&sh->empty[s]));
         }
         if (nk > 0) mma_commit(smem_u32(&sh->done));
     }
     __syncwarp();
 
-    // ---- this CTA's partial into its shared memory (FP32, rows of cw + 4)
+    // ---- this CTA's partial into its shared memory (FP32, rows of iw + 4)
     float* P = reinterpret_cast<float*>(smem);
-    const int pitch = cw + 4;
+    const int pitch = iw + 4;
     {
         const bool ok = __all_sync(0xffffffffu, nk > 0 && mbar_wait(smem_u32(&sh->done), 0, abort));
         tc_after();
         const int q = warp & 3, hh = warp >> 2;
         const int r = q * 32 + lane;
-        for (int u = hh; u < (cw >> 4); u += kDwThreads / 128) {
-            float a[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) a[j] = 0.f;
-            if (ok) {
-#pragma unroll
-                for (int acc = 0; acc < kDwAcc; ++acc) {  // the accumulators in order
-                    uint32_t v[16];
-                    tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * 128 + u * 16), v);
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) a[j] += __uint_as_float(v[j]);
-                }
-            }
+        for (int u = hh; u < (iw >> 4); u += kDwThreads / 128) {
+            uint32_t v[16];
+            if (ok) tmem_ld16(tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(u * 16), v);
             float4* d = reinterpret_cast<float4*>(P + r * pitch + u * 16);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) d[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
+            for (int j = 0; j < 4; ++j)
+                d[j] = ok ? make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                        __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
     tc_before();
@@ -1004,11 +936,11 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
         const int per = (T.oh + static_cast<int>(nrank) - 1) / static_cast<int>(nrank);
         const int rb = static_cast<int>(rank) * per, re = min(T.oh, rb + per);
         const uint32_t pbase = smem_u32(P);
-        const int q4 = cw >> 2;  // groups of 4 columns
+        const int q4 = iw >> 2;  // groups of 4 columns
         for (int idx = tid; idx < (re - rb) * q4; idx += kDwThreads) {
             const int ol = rb + idx / q4, i = (idx % q4) * 4;
             const int o = T.o0 + ol;
-            if (o >= L.dout || c0 + i > L.din) continue;
+            if (o >= L.dout || T.i0 + i > L.din) continue;
             const uint32_t la = pbase + static_cast<uint32_t>(ol * pitch + i) * 4u;
             float4 part[kMaxCluster];
 #pragma unroll
@@ -1026,22 +958,22 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
             const float gv[4] = {g.x, g.y, g.z, g.w};
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int ia = c0 + i + j;
+                const int ia = T.i0 + i + j;
                 if (ia > L.din) break;
                 const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
                 if (p.grad) {
                     p.grad[e] = gv[j];
                 } else {
-                    adamw_elem(gv[j], p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr, p.b1, p.b2, p.eps,
-                               p.bc1, p.bc2, reinterpret_cast<__nv_bfloat16*>(p.w_img + L.w_off + w_elem(L, o, ia)));
+                    const float x = adamw_elem(gv[j], p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr,
+                                               p.b1, p.b2, p.eps, p.bc1, p.bc2);
+                    store_images(p.w_img, L, T.layer, o, ia, x);
                 }
             }
         }
     }
     cluster_sync();
     if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDwAcc * 128) : "memory");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
 }
 
 // ---- packing and the stand-alone AdamW (data parallel) ------------------------
@@ -1065,7 +997,7 @@ __global__ void k_fused_pack(const __grid_constant__ GeoArgs a, const float* __r
         const LayerGeo& L = G.l[layer_of(G, e)];
         const int64_t el = e - L.aug_off;
         const int o = static_cast<int>(el / L.kaug), i = static_cast<int>(el - static_cast<int64_t>(o) * L.kaug);
-        *reinterpret_cast<__nv_bfloat16*>(w_img + L.w_off + w_elem(L, o, i)) = __float2bfloat16(w_aug[e]);
+        store_images(w_img, L, layer_of(G, e), o, i, w_aug[e]);
     }
 }
 
@@ -1083,8 +1015,9 @@ __global__ void k_fused_adamw(const __grid_constant__ GeoArgs a, const AdamScala
         const int64_t el = e - L.aug_off;
         const int o = static_cast<int>(el / L.kaug), i = static_cast<int>(el - static_cast<int64_t>(o) * L.kaug);
         if (o >= L.dout || i > L.din) continue;
-        adamw_elem(grad[e], w_aug + e, m1 + e, m2 + e, i < L.din ? h.wd : 0.f, h.lr, h.b1, h.b2, h.eps, h.bc1, h.bc2,
-                   reinterpret_cast<__nv_bfloat16*>(w_img + L.w_off + w_elem(L, o, i)));
+        const float x =
+            adamw_elem(grad[e], w_aug + e, m1 + e, m2 + e, i < L.din ? h.wd : 0.f, h.lr, h.b1, h.b2, h.eps, h.bc1, h.bc2);
+        store_images(w_img, L, layer_of(G, e), o, i, x);
     }
 }
 
@@ -1183,11 +1116,16 @@ int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf1
     if (cudaGetLastError() != cudaSuccess) return finish(PB_ECUDA);
 
     dw->geo = fb->geo;
+    // weight tiles: 128 outputs x at most 256 inputs (K_aug split evenly into
+    // multiples of 16)
     int nt = 0;
     for (int l = 0; l < n_layers; ++l) {
         const LayerGeo& L = dw->geo.l[l];
+        const int nr = (L.kaug + kMaxWidth - 1) / kMaxWidth;
+        const int w0 = ((L.kaug + nr - 1) / nr + 15) / 16 * 16;
         for (int o0 = 0; o0 < L.npad; o0 += kRows)
-            for (int c = 0; c < L.n_chunks; ++c) dw->t[nt++] = DwTile{l, o0, min(kRows, L.npad - o0), c};
+            for (int i0 = 0; i0 < L.kaug; i0 += w0)
+                dw->t[nt++] = DwTile{l, o0, min(kRows, L.npad - o0), i0, min(w0, L.kaug - i0)};
     }
     dw->n_tiles = nt;
     dw->M = M;

@@ -22,7 +22,9 @@ def _geometry(dims: list[int], batch: int) -> list[int]:
 
 def test_surrogate_geometry():
     """136 -> 256 x4 -> 6: inputs augmented by the ones column to 144 / 272, the
-    six classes padded to 16 rows; images and scratch sized from those."""
+    six classes padded to 16 rows; the images (the augmented weights, and W^T of
+    every layer after the first for the input gradients) and the scratch sized
+    from those."""
     dims = [136, 256, 256, 256, 256, 6]
     g = _geometry(dims, 4096)
     kaug = [g[3 + 4 * l] for l in range(5)]
@@ -31,8 +33,10 @@ def test_surrogate_geometry():
     w_off = [g[6 + 4 * l] for l in range(5)]
     assert kaug == [144, 272, 272, 272, 272] and npad == [256, 256, 256, 256, 16]
     sizes = [n * k for n, k in zip(npad, kaug)]
-    assert g[2] == sum(sizes) and g[0] == 2 * sum(sizes)
-    assert aug_off == [sum(sizes[:l]) for l in range(5)] and w_off == [2 * a for a in aug_off]
+    wt = [0] + [dims[l] * npad[l] for l in range(1, 5)]  # W^T: d_in x npad
+    assert g[2] == sum(sizes) and g[0] == 2 * (sum(sizes) + sum(wt))
+    assert aug_off == [sum(sizes[:l]) for l in range(5)]
+    assert w_off == [2 * (sum(sizes[:l]) + sum(wt[:l])) for l in range(5)]
     tiles = 4096 // 128
     per_tile = sum(128 * k * 2 + 128 * n * 2 for k, n in zip(kaug, npad)) + 4 * 128 * 256 * 2
     assert g[1] == tiles * per_tile
