@@ -452,8 +452,8 @@ C5_RANDOM = 27_778
 C5_ACTIVE = 25_000
 C5_POOL = 500_000
 C5_EPOCHS = 40
-C5_BATCH = 4096
-C5_LR = 5e-3
+C5_BATCH = 8192
+C5_LR = 1e-2
 C5_FREQ_SCALE = 0.6
 FP64_CHUNK = 500_000  # plain FP64 kernel over 10^7 ICs: chunks bound its step-record scratch
 
@@ -751,7 +751,9 @@ def profile_surrogate(args) -> None:
         torch.cuda.nvtx.range_pop()
         ts.append(e0.elapsed_time(e1))
     print(json.dumps({"only": "surrogate", "n_ic": n, "ms_per_step": statistics.mean(ts),
-                      "routed_fraction": st.routed_fraction}), flush=True)
+                      "routed_fraction": st.routed_fraction, "audit_error": st.audit_error,
+                      "training": {"epochs": C5_EPOCHS, "batch": C5_BATCH, "lr": C5_LR, "random": C5_RANDOM,
+                                   "active": C5_ACTIVE, "pool": C5_POOL}}), flush=True)
 
 
 def run_b200_arm(args) -> None:
@@ -1003,7 +1005,20 @@ def main() -> None:
     ap.add_argument("--no-studies", action="store_true", help="skip the parameter studies at full size")
     ap.add_argument("--only", default="all", choices=["all", "surrogate"],
                     help="surrogate: that workload's steps alone, NVTX-marked, for a profiler")
+    ap.add_argument("--c5-batch", type=int, default=None, help="surrogate training minibatch (rows)")
+    ap.add_argument("--c5-lr", type=float, default=None, help="surrogate training peak learning rate")
+    ap.add_argument("--c5-epochs", type=int, default=None, help="surrogate training epochs")
+    ap.add_argument("--c5-random", type=int, default=None, help="random ICs labelled for the surrogate")
+    ap.add_argument("--c5-active", type=int, default=None, help="ICs labelled by active selection")
+    ap.add_argument("--c5-pool", type=int, default=None, help="pool the active labels are chosen from")
     args = ap.parse_args()
+    global C5_BATCH, C5_LR, C5_EPOCHS, C5_RANDOM, C5_ACTIVE, C5_POOL
+    C5_BATCH = args.c5_batch or C5_BATCH
+    C5_LR = args.c5_lr or C5_LR
+    C5_EPOCHS = args.c5_epochs or C5_EPOCHS
+    C5_RANDOM = args.c5_random or C5_RANDOM
+    C5_ACTIVE = args.c5_active or C5_ACTIVE
+    C5_POOL = args.c5_pool or C5_POOL
     if args.impl == "reference":
         run_reference_arm(args)
     elif args.only == "surrogate":
