@@ -80,14 +80,15 @@ constexpr int kFbSmem = 2 * kImgBytes + kRing * kSlabBytes + kFbTail;
 
 // k_train_dw
 constexpr int kDwThreads = 256;
-constexpr int kDwStages = 2;
+constexpr int kDwStages = 3;
+constexpr int kDwMaxIn = 144;                       // inputs of a weight tile
 constexpr int kDwABytes = kRows * kRows * 2;        // 128 outputs x 128 rows
-constexpr int kDwBBytes = kRows * kMaxWidth * 2;    // 128 rows x <= 256 inputs
+constexpr int kDwBBytes = kRows * kDwMaxIn * 2;     // 128 rows x <= 144 inputs
 constexpr int kDwStageBytes = kDwABytes + kDwBBytes;
 constexpr int kDwTail = 256;
 constexpr int kDwSmem = kDwStages * kDwStageBytes + kDwTail;
 constexpr int kMaxCluster = 8;
-constexpr int kMaxDwTiles = kMaxLayers * 2 * 2;
+constexpr int kMaxDwTiles = kMaxLayers * 2 * 2;  // per layer <= 2 output tiles x 2 input ranges
 
 // ---- geometry ----------------------------------------------------------------
 
@@ -776,7 +777,7 @@ struct DwSmem {
 };
 static_assert(sizeof(DwSmem) <= kDwTail, "k_train_dw: barrier block");
 static_assert(kDwSmem <= 227 * 1024, "k_train_dw: shared memory");
-static_assert(kRows * (kMaxWidth + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
+static_assert(kRows * (kDwMaxIn + 4) * 4 <= kDwStageBytes * kDwStages, "k_train_dw: the partial fits the stages");
 
 // every thread of the cluster (non-aligned: warps may arrive diverged)
 __device__ __forceinline__ void cluster_sync()
@@ -955,18 +956,37 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
                     g.z += part[q].z;
                     g.w += part[q].w;
                 }
-            const float gv[4] = {g.x, g.y, g.z, g.w};
+            // the 4 columns are consecutive in the row-major augmented arrays (16-byte
+            // aligned: offsets, K_aug and the tile start are multiples of 4); columns
+            // past the bias are padding, whose gradient is zero and which stay zero
+            const int ia = T.i0 + i;
+            const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
+            if (p.grad) {
+                *reinterpret_cast<float4*>(p.grad + e) = g;
+            } else {
+                float4 w = *reinterpret_cast<const float4*>(p.w_aug + e);
+                float4 a = *reinterpret_cast<const float4*>(p.m1 + e);
+                float4 b = *reinterpret_cast<const float4*>(p.m2 + e);
+                float* wv = &w.x;
+                float* av = &a.x;
+                float* bv = &b.x;
+                const float gv[4] = {g.x, g.y, g.z, g.w};
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int ia = T.i0 + i + j;
-                if (ia > L.din) break;
-                const int64_t e = L.aug_off + static_cast<int64_t>(o) * L.kaug + ia;
-                if (p.grad) {
-                    p.grad[e] = gv[j];
-                } else {
-                    const float x = adamw_elem(gv[j], p.w_aug + e, p.m1 + e, p.m2 + e, ia < L.din ? p.wd : 0.f, p.lr,
-                                               p.b1, p.b2, p.eps, p.bc1, p.bc2);
-                    store_images(p.w_img, L, T.layer, o, ia, x);
+                for (int j = 0; j < 4; ++j)
+                    adamw_elem(gv[j], wv + j, av + j, bv + j, ia + j < L.din ? p.wd : 0.f, p.lr, p.b1, p.b2, p.eps,
+                               p.bc1, p.bc2);
+                *reinterpret_cast<float4*>(p.w_aug + e) = w;
+                *reinterpret_cast<float4*>(p.m1 + e) = a;
+                *reinterpret_cast<float4*>(p.m2 + e) = b;
+                // forward image: the 4 columns are 4 consecutive values of one core row
+                const uint2 h = make_uint2(pack_bf16(w.x, w.y), pack_bf16(w.z, w.w));
+                *reinterpret_cast<uint2*>(p.w_img + L.w_off + w_elem(L, o, ia)) = h;
+                if (T.layer > 0) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (ia + j < L.din)
+                            *reinterpret_cast<__nv_bfloat16*>(p.w_img + L.wt_off + wt_elem(L, o, ia + j)) =
+                                __float2bfloat16(wv[j]);
                 }
             }
         }
@@ -1116,12 +1136,12 @@ int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf1
     if (cudaGetLastError() != cudaSuccess) return finish(PB_ECUDA);
 
     dw->geo = fb->geo;
-    // weight tiles: 128 outputs x at most 256 inputs (K_aug split evenly into
+    // weight tiles: 128 outputs x at most kDwMaxIn inputs (K_aug split evenly into
     // multiples of 16)
     int nt = 0;
     for (int l = 0; l < n_layers; ++l) {
         const LayerGeo& L = dw->geo.l[l];
-        const int nr = (L.kaug + kMaxWidth - 1) / kMaxWidth;
+        const int nr = (L.kaug + kDwMaxIn - 1) / kDwMaxIn;
         const int w0 = ((L.kaug + nr - 1) / nr + 15) / 16 * 16;
         for (int o0 = 0; o0 < L.npad; o0 += kRows)
             for (int i0 = 0; i0 < L.kaug; i0 += w0)
