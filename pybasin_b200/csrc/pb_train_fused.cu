@@ -63,7 +63,6 @@ constexpr int kMaxWidth = 256;             // largest layer width
 constexpr int kMaxPieces = 4;              // 64-column pieces of a layer output (<= 256)
 constexpr int kMaxKaug = 272;
 constexpr int kMaxClasses = 32;            // the cross entropy reads one 32-column TMEM load
-constexpr int kSlab = 32;                  // columns (rows of W^T) of a weight slab
 constexpr long long kWaitPolls = 1ll << 22;
 
 // k_train_fb: 16 epilogue warps (TMEM lane quarter w % 4, output piece w / 4),
@@ -72,11 +71,11 @@ constexpr int kEpiWarps = 16;
 constexpr int kMmaWarp = kEpiWarps;
 constexpr int kLoadWarp = kEpiWarps + 1;
 constexpr int kFbThreads = (kEpiWarps + 2) * 32;
-constexpr int kRing = 5;                                 // weight-slab slots
-constexpr int kSlabBytes = kMaxWidth * kSlab * 2;        // 16 KB
+constexpr int kRing = 9;                                 // weight-slab slots
+constexpr int kSlabBytes = 16 * 1024;                    // a weight slab: all rows x as many columns as fit
 constexpr int kImgBytes = kRows * kMaxKaug * 2;          // largest activation / gradient image
 constexpr int kFbTail = 1024;                            // barriers, flags, the tile's labels
-constexpr int kFbSmem = 2 * kImgBytes + kRing * kSlabBytes + kFbTail;
+constexpr int kFbSmem = kImgBytes + kRing * kSlabBytes + kFbTail;
 
 // k_train_dw
 constexpr int kDwThreads = 256;
@@ -100,6 +99,8 @@ struct LayerGeo {
     int p0[kMaxPieces], ph[kMaxPieces];
     int n_dx;             // 64-column pieces of din (input-gradient outputs, layers >= 1)
     int d0[kMaxPieces], dw[kMaxPieces];
+    int sw;               // input columns of a W slab (all npad rows; <= kSlabBytes)
+    int tw;               // outputs of a W^T slab (all din rows; <= kSlabBytes)
     int64_t w_off;        // byte offset of this layer's W slabs in the image buffer
     int64_t wt_off;       // byte offset of its W^T slabs (layers >= 1)
     int64_t aug_off;      // element offset of this layer in the concatenated augmented (npad x kaug) arrays
@@ -142,6 +143,9 @@ inline int geo_build(int n_layers, const int32_t* dims, int batch, Geo* g)
         L.npad = (L.dout + 15) / 16 * 16;
         L.n_pieces = split64(L.npad, L.p0, L.ph);
         L.n_dx = l > 0 ? split64(L.din, L.d0, L.dw) : 0;
+        // slab widths: as many 16-column groups as fit kSlabBytes (at least one)
+        L.sw = min(L.kaug, max(16, kSlabBytes / (2 * L.npad) / 16 * 16));
+        L.tw = min(L.npad, max(16, kSlabBytes / (2 * L.din) / 16 * 16));
         L.w_off = img;
         img += static_cast<int64_t>(L.npad) * L.kaug * 2;
         L.wt_off = img;
@@ -174,18 +178,18 @@ __host__ __device__ __forceinline__ uint32_t img_off(int w, int r, int k)
 }
 
 // byte offset (relative to the layer's W slabs) of weight element (o, i): slab
-// i / 32 holds all npad rows of 32 (or the last 16) columns
+// i / sw holds all npad rows of sw (the last one fewer) columns
 __host__ __device__ inline int64_t w_elem(const LayerGeo& L, int o, int i)
 {
-    const int k0 = i / kSlab * kSlab, kw = min(kSlab, L.kaug - k0);
+    const int k0 = i / L.sw * L.sw, kw = min(L.sw, L.kaug - k0);
     return static_cast<int64_t>(L.npad) * k0 * 2 + img_off(kw, o, i - k0);
 }
 
 // byte offset (relative to the layer's W^T slabs) of weight element (o, i), i < din:
-// slab o / 32 holds all din rows of W^T for 32 (or the last 16) outputs
+// slab o / tw holds all din rows of W^T for tw (the last one fewer) outputs
 __host__ __device__ inline int64_t wt_elem(const LayerGeo& L, int o, int i)
 {
-    const int o0 = o / kSlab * kSlab, ow = min(kSlab, L.npad - o0);
+    const int o0 = o / L.tw * L.tw, ow = min(L.tw, L.npad - o0);
     return static_cast<int64_t>(L.din) * o0 * 2 + img_off(ow, i, o - o0);
 }
 
@@ -469,8 +473,9 @@ __device__ __forceinline__ void dx_cols(uint32_t tm, int ncols, int col0, int r,
 __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constant__ FbArgs p)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
-    // image buffer b at smem + b * kImgBytes, then the slab ring, then FbSmem
-    uint8_t* ring = smem + 2 * kImgBytes;
+    // the image buffer (each phase's epilogue overwrites its input in place), then
+    // the slab ring, then FbSmem
+    uint8_t* ring = smem + kImgBytes;
     FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kSlabBytes);
     volatile int* abort = &sh->abort;
     const Geo& G = p.geo;
@@ -515,15 +520,15 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             };
             for (int l = 0; l < NL && !*abort; ++l) {
                 const LayerGeo& L = G.l[l];
-                for (int k0 = 0; k0 < L.kaug; k0 += kSlab)
+                for (int k0 = 0; k0 < L.kaug; k0 += L.sw)
                     put(L.w_off + static_cast<int64_t>(L.npad) * k0 * 2,
-                        static_cast<uint32_t>(L.npad) * min(kSlab, L.kaug - k0) * 2u);
+                        static_cast<uint32_t>(L.npad) * min(L.sw, L.kaug - k0) * 2u);
             }
             for (int l = NL - 1; l >= 1 && !*abort; --l) {
                 const LayerGeo& L = G.l[l];
-                for (int o0 = 0; o0 < L.npad; o0 += kSlab)
+                for (int o0 = 0; o0 < L.npad; o0 += L.tw)
                     put(L.wt_off + static_cast<int64_t>(L.din) * o0 * 2,
-                        static_cast<uint32_t>(L.din) * min(kSlab, L.npad - o0) * 2u);
+                        static_cast<uint32_t>(L.din) * min(L.tw, L.npad - o0) * 2u);
             }
         }
         __syncwarp();
@@ -533,18 +538,22 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     }
 
     if (warp == kMmaWarp) {
-        // ---- MMAs, one phase per layer: the previous phase's epilogues are done,
-        // the image they consumed and the one they wrote are final; the MMAs read the
-        // latter, and its copy to global scratch (for the weight gradients) starts
+        // ---- MMAs, one phase per layer: the previous phase's epilogues are done and
+        // the image they wrote is final; its copy to global scratch (for the weight
+        // gradients) starts, the MMAs read it, and before the phase's epilogues may
+        // overwrite it the copy has read it (it overlaps the MMAs)
         if (lane == 0) {
             uint32_t u = 0, ep = 0;
-            int cur = 0;
+            const uint32_t a0 = smem_u32(smem);
             auto begin_phase = [&](uint8_t* dst, uint32_t bytes) {
                 mbar_wait(smem_u32(&sh->epi_done), ep++ & 1u, abort);
                 tc_after();
-                bulk_store(dst, smem_u32(smem + cur * kImgBytes), bytes);
+                bulk_store(dst, a0, bytes);
                 bulk_commit();
-                bulk_wait_read<1>();  // the copy of two phases ago has read its buffer
+            };
+            auto end_mmas = [&]() {
+                bulk_wait_read<0>();
+                mma_commit(smem_u32(&sh->mdone));
             };
             auto slab = [&](uint32_t& s) {
                 s = u % kRing;
@@ -557,45 +566,40 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             for (int l = 0; l < NL; ++l) {  // forward: Z_l (128 x npad) = X_l W_l^T, K = kaug
                 const LayerGeo& L = G.l[l];
                 begin_phase(p.scratch + L.x_off + tile * L.x_tile, static_cast<uint32_t>(L.x_tile));
-                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
                 const uint32_t sbo_a = static_cast<uint32_t>(L.kaug >> 3) << 7;
                 const uint32_t idesc = instr_desc(kRows, L.npad, false, false);
-                for (int k0 = 0; k0 < L.kaug; k0 += kSlab) {
+                for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
                     uint32_t s;
                     const bool ok = slab(s);
-                    const int kw = min(kSlab, L.kaug - k0);
+                    const int kw = min(L.sw, L.kaug - k0);
                     const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
                     for (int ks = 0; ok && ks < (kw >> 4); ++ks)
                         mma_bf16(tmem, smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
                                  smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
                     mma_commit(smem_u32(&sh->empty[s]));
                 }
-                mma_commit(smem_u32(&sh->mdone));
-                cur ^= 1;
+                end_mmas();
             }
             for (int l = NL - 1; l >= 1; --l) {  // input gradients: (128 x din) = dZ_l W_l, K = npad
                 const LayerGeo& L = G.l[l];
                 begin_phase(p.scratch + L.z_off + tile * L.z_tile, static_cast<uint32_t>(L.z_tile));
-                const uint32_t a0 = smem_u32(smem + cur * kImgBytes);
                 const uint32_t sbo_a = static_cast<uint32_t>(L.npad >> 3) << 7;
                 const uint32_t idesc = instr_desc(kRows, L.din, false, false);
-                for (int o0 = 0; o0 < L.npad; o0 += kSlab) {
+                for (int o0 = 0; o0 < L.npad; o0 += L.tw) {
                     uint32_t s;
                     const bool ok = slab(s);
-                    const int ow = min(kSlab, L.npad - o0);
+                    const int ow = min(L.tw, L.npad - o0);
                     const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(ow >> 3) << 7;
                     for (int ks = 0; ok && ks < (ow >> 4); ++ks)
                         mma_bf16(tmem, smem_desc(a0 + ((o0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
                                  smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (o0 > 0 || ks > 0) ? 1u : 0u);
                     mma_commit(smem_u32(&sh->empty[s]));
                 }
-                mma_commit(smem_u32(&sh->mdone));
-                cur ^= 1;
+                end_mmas();
             }
             // the last image written (dZ_0) to scratch once its phase is done
             mbar_wait(smem_u32(&sh->epi_done), ep++ & 1u, abort);
-            bulk_store(p.scratch + G.l[0].z_off + tile * G.l[0].z_tile, smem_u32(smem + cur * kImgBytes),
-                       static_cast<uint32_t>(G.l[0].z_tile));
+            bulk_store(p.scratch + G.l[0].z_off + tile * G.l[0].z_tile, a0, static_cast<uint32_t>(G.l[0].z_tile));
             bulk_commit();
             bulk_wait_all();
         }
@@ -632,7 +636,6 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
         const int r = quarter * 32 + lane;  // this thread's row (TMEM lane)
         const uint32_t tm_row = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
         uint32_t ph = 1;                    // this phase (the gather was phase 0)
-        int cur = 0;
         float loss = 0.f;
         int hits = 0;
         // one phase of the epilogue.  Every warp waits for the phase's MMAs (mdone
@@ -649,7 +652,6 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sh->epi_done));
             ++ph;
-            cur ^= 1;
         };
         for (int l = 0; l < NL; ++l) {
             const LayerGeo& L = G.l[l];
@@ -658,7 +660,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
             if (mine) {
                 const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone), (ph - 1) & 1u, abort));
                 tc_after();
-                uint8_t* out = smem + (cur ^ 1) * kImgBytes;
+                uint8_t* out = smem;  // in place: the phase's MMAs are done with their input
                 if (!last) {
                     const LayerGeo& Ln = G.l[l + 1];
                     const int pc = grp;
@@ -728,7 +730,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 tc_after();
                 if (ok)
                     dx_cols(tm_row + static_cast<uint32_t>(L.d0[grp]), L.dw[grp], L.d0[grp], r,
-                            smem + (cur ^ 1) * kImgBytes, Lb.npad, p.scratch + Lb.g_off + tile * Lb.g_tile);
+                            smem, Lb.npad, p.scratch + Lb.g_off + tile * Lb.g_tile);
             }
             end_phase(mine);
         }
