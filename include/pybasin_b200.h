@@ -604,6 +604,12 @@ int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf1
                         void* w_img, void* scratch, float* grad, float lr, float beta1, float beta2, float eps,
                         float weight_decay, int32_t step, float* loss_sum, int32_t* correct, int32_t* error_flag,
                         void* stream);
+/* Inference with the same BF16 weight images: logits (n x dims[n_layers], FP32) of
+ * the BF16 inputs x (n x dims[0], 16-byte aligned).  Persistent CTAs take pairs of
+ * 128-row tiles and alternate between them, so one tile's MMAs run while the other
+ * tile's activations are computed.  error_flag (optional) as for the step. */
+int pb_mlp_infer_fused(int32_t n_layers, const int32_t* dims, const void* x_bf16, int64_t n, const void* w_img,
+                       float* logits, int32_t* error_flag, void* stream);
 /* AdamW step from a gradient in the augmented layout (e.g. after a data-parallel
  * all-reduce of pb_train_fused_step's grad output), refreshing w_img. */
 int pb_train_fused_adamw(int32_t n_layers, const int32_t* dims, float* w_aug, float* m1, float* m2, const float* grad,

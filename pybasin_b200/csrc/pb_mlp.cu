@@ -250,8 +250,11 @@ __global__ void __launch_bounds__(256) k_features_in(const float* __restrict__ i
         if (n_freq > 0) {
             float turns = 0.f;
             for (int c = 0; c < d; ++c) turns = fmaf(f_s[j * d + c], z[c], turns);
+            // sin and cos of 2 pi turns: the whole turns taken off exactly (|turns| <
+            // 2^22), the rest, in [-pi, pi], to the hardware sine and cosine (absolute
+            // error about 2^-21, far below the BF16 step of the result)
             float sn, cs;
-            sincospif(2.f * turns, &sn, &cs);
+            __sincosf(6.28318530717958648f * (turns - rintf(turns)), &sn, &cs);
             o[d + j] = __float2bfloat16(sn);
             o[d + n_freq + j] = __float2bfloat16(cs);
         }
@@ -449,7 +452,11 @@ int pb_surrogate_inputs_rows(const float* ic, int32_t S, const double* params, i
     if (n_freq > 128) return PB_EINVAL;  // at least two rows per 256-thread block
     const int U = n_freq > 0 ? n_freq : 1, R = 256 / U;
     const size_t fsmem = static_cast<size_t>(n_freq + R) * (S + n_params) * sizeof(float);
-    k_features_in<<<grid_for((n + R - 1) / R, 1), 256, fsmem, static_cast<cudaStream_t>(stream)>>>(
+    // a grid of 16 blocks per SM strides over the rows (each block stages the
+    // frequencies once)
+    const int64_t blocks = (n + R - 1) / R;
+    k_features_in<<<static_cast<unsigned>(blocks < 148 * 16 ? blocks : 148 * 16), 256, fsmem,
+                    static_cast<cudaStream_t>(stream)>>>(
         ic, S, params, n_params, param_index, n_param_rows, shift, scale, freq, n_freq, n, d_pad,
         static_cast<__nv_bfloat16*>(out_bf16));
     return map_err(cudaGetLastError());

@@ -751,6 +751,230 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
 }
 
+// ---- inference: two row tiles per CTA in turn ----------------------------------
+//
+// A persistent CTA takes pairs of 128-row tiles and runs the layer chain of both,
+// alternating: the MMAs of one tile's layer run while the epilogue warps apply
+// GELU to the other tile's previous layer, so the tensor pipe and the epilogue
+// overlap.  Activations stay in shared memory (one buffer per tile, overwritten in
+// place), the accumulators in TMEM (256 columns per tile), the weights (the same
+// augmented slab images as the training step) stream through the slab ring once
+// per tile and layer.  The logits of the last layer go to global memory.
+struct InferArgs {
+    Geo geo;
+    const __nv_bfloat16* x;  // (n x dims[0]) BF16 inputs
+    int64_t n;
+    const uint8_t* w_img;
+    float* logits;           // (n x C)
+    int32_t* error;
+};
+
+constexpr int kInfRing = 5;
+constexpr int kInfSmem = 2 * kImgBytes + kInfRing * kSlabBytes + 1024;
+static_assert(kInfSmem <= 227 * 1024, "k_mlp_infer_pp: shared memory");
+
+struct InfSmem {
+    uint64_t full[kInfRing], empty[kInfRing], mdone[2], edone[2];
+    uint32_t tmem;
+    int abort;
+};
+
+// rows [row0, row0 + 128) of x into the layer-0 image at img: the ones column
+// after the inputs, zeros past n (run by the 16 epilogue warps)
+__device__ __forceinline__ void infer_stage(const InferArgs& p, const LayerGeo& L0, uint8_t* img, int64_t row0, int tid)
+{
+    const int pieces = L0.kaug >> 3;
+    for (int idx = tid; idx < kRows * pieces; idx += kEpiWarps * 32) {
+        const int r = idx & (kRows - 1), col = (idx >> 7) << 3;
+        uint8_t* dst = img + img_off(L0.kaug, r, col);
+        const int64_t row = row0 + r;
+        if (row < p.n && col < L0.din) {
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(p.x + row * L0.din + col)
+                         : "memory");
+        } else {
+            const uint32_t one = (row < p.n && col == L0.din) ? 0x3F80u : 0u;
+            *reinterpret_cast<uint4*>(dst) = make_uint4(one, 0u, 0u, 0u);
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kFbThreads, 1) k_mlp_infer_pp(const __grid_constant__ InferArgs p)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    // the activations of tile t at smem + t * kImgBytes, then the slab ring
+    uint8_t* ring = smem + 2 * kImgBytes;
+    InfSmem* sh = reinterpret_cast<InfSmem*>(ring + kInfRing * kSlabBytes);
+    volatile int* abort = &sh->abort;
+    const Geo& G = p.geo;
+    const int NL = G.n_layers;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t n_tiles = (p.n + kRows - 1) / kRows, n_pairs = (n_tiles + 1) / 2;
+
+    if (tid == 0) {
+        for (int s = 0; s < kInfRing; ++s) {
+            mbar_init(smem_u32(&sh->full[s]), 1);
+            mbar_init(smem_u32(&sh->empty[s]), 1);
+        }
+        for (int t = 0; t < 2; ++t) {
+            mbar_init(smem_u32(&sh->mdone[t]), 1);
+            mbar_init(smem_u32(&sh->edone[t]), kEpiWarps);
+        }
+        sh->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    cta_sync();
+    tc_after();
+    const uint32_t tmem = sh->tmem;
+
+    if (warp == kLoadWarp) {
+        if (lane == 0) {  // the slabs of every layer, once per tile, in the MMA order
+            uint32_t u = 0;
+            for (int64_t pr = blockIdx.x; pr < n_pairs && !*abort; pr += gridDim.x)
+                for (int l = 0; l < NL; ++l)
+                    for (int t = 0; t < 2; ++t) {
+                        const LayerGeo& L = G.l[l];
+                        for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
+                            const uint32_t s = u % kInfRing, round = u / kInfRing;
+                            ++u;
+                            if (round > 0 && !mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1u, abort)) continue;
+                            const uint32_t bytes = static_cast<uint32_t>(L.npad) * min(L.sw, L.kaug - k0) * 2u;
+                            mbar_expect_tx(smem_u32(&sh->full[s]), bytes);
+                            bulk_load(smem_u32(ring + s * kSlabBytes), p.w_img + L.w_off + static_cast<int64_t>(L.npad) * k0 * 2,
+                                      bytes, smem_u32(&sh->full[s]));
+                        }
+                    }
+        }
+        cta_sync();
+        if (tid == kLoadWarp * 32 && *abort && p.error) atomicExch(p.error, 1);
+        return;
+    }
+
+    if (warp == kMmaWarp) {
+        if (lane == 0) {
+            // each tile's barriers complete once per (pair, layer): k counts those
+            uint32_t u = 0, k = 0;
+            for (int64_t pr = blockIdx.x; pr < n_pairs; pr += gridDim.x)
+                for (int l = 0; l < NL; ++l, ++k)
+                    for (int t = 0; t < 2; ++t) {
+                        const LayerGeo& L = G.l[l];
+                        // the tile's input for this layer is written (and its TMEM read)
+                        mbar_wait(smem_u32(&sh->edone[t]), k & 1u, abort);
+                        tc_after();
+                        const uint32_t a0 = smem_u32(smem + t * kImgBytes);
+                        const uint32_t sbo_a = static_cast<uint32_t>(L.kaug >> 3) << 7;
+                        const uint32_t idesc = instr_desc(kRows, L.npad, false, false);
+                        for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
+                            const uint32_t s = u % kInfRing, round = u / kInfRing;
+                            ++u;
+                            const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
+                            tc_after();
+                            const int kw = min(L.sw, L.kaug - k0);
+                            const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
+                            for (int ks = 0; ok && ks < (kw >> 4); ++ks)
+                                mma_bf16(tmem + static_cast<uint32_t>(t * 256),
+                                         smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                         smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                            mma_commit(smem_u32(&sh->empty[s]));
+                        }
+                        mma_commit(smem_u32(&sh->mdone[t]));
+                    }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue warps: stage the first pair, then for every pair, layer and
+        // tile in the MMA order: wait for the MMAs, apply GELU in place (or write the
+        // logits and stage the tile of the next pair), arrive
+        const int quarter = warp & 3, grp = warp >> 2;
+        const int r = quarter * 32 + lane;
+        uint32_t k = 0;  // (pair, layer) steps done
+        const LayerGeo& L0 = G.l[0];
+        const int64_t first = blockIdx.x;
+        for (int t = 0; t < 2; ++t) {
+            if (first < n_pairs) infer_stage(p, L0, smem + t * kImgBytes, (2 * first + t) * kRows, tid);
+            proxy_fence();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh->edone[t]));
+        }
+        for (int64_t pr = first; pr < n_pairs; pr += gridDim.x)
+            for (int l = 0; l < NL; ++l, ++k)
+                for (int t = 0; t < 2; ++t) {
+                    const LayerGeo& L = G.l[l];
+                    uint8_t* act = smem + t * kImgBytes;
+                    const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&sh->mdone[t]), k & 1u, abort));
+                    tc_after();
+                    const uint32_t tm = tmem + static_cast<uint32_t>(t * 256) + (static_cast<uint32_t>(quarter * 32) << 16);
+                    const int64_t row = (2 * pr + t) * kRows + r;
+                    if (l + 1 < NL) {
+                        const LayerGeo& Ln = G.l[l + 1];
+                        if (grp < L.n_pieces) {
+                            const int pc = grp;
+                            for (int cc = 0; ok && cc < L.ph[pc]; cc += 32) {
+                                const int nn = L.ph[pc] - cc >= 32 ? 32 : 16;
+                                float z[32];
+                                if (nn == 32) {
+                                    uint32_t v[32];
+                                    tmem_ld32(tm + static_cast<uint32_t>(L.p0[pc] + cc), v);
+#pragma unroll
+                                    for (int j = 0; j < 32; ++j) z[j] = __uint_as_float(v[j]);
+                                } else {
+                                    uint32_t v[16];
+                                    tmem_ld16(tm + static_cast<uint32_t>(L.p0[pc] + cc), v);
+#pragma unroll
+                                    for (int j = 0; j < 16; ++j) z[j] = __uint_as_float(v[j]);
+#pragma unroll
+                                    for (int j = 16; j < 32; ++j) z[j] = 0.f;
+                                }
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    if (q * 8 >= nn) break;
+                                    uint32_t hx[4];
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k) hx[k] = pack_bf16(gelu(z[q * 8 + 2 * k]), gelu(z[q * 8 + 2 * k + 1]));
+                                    *reinterpret_cast<uint4*>(act + img_off(Ln.kaug, r, L.p0[pc] + cc + q * 8)) =
+                                        make_uint4(hx[0], hx[1], hx[2], hx[3]);
+                                }
+                            }
+                            if (pc == L.n_pieces - 1)
+                                for (int col = L.dout; col < Ln.kaug; col += 8) {
+                                    const uint32_t one = (row < p.n && col == L.dout) ? 0x3F80u : 0u;
+                                    *reinterpret_cast<uint4*>(act + img_off(Ln.kaug, r, col)) = make_uint4(one, 0u, 0u, 0u);
+                                }
+                        }
+                    } else {
+                        if (grp == 0) {
+                            uint32_t v[32];
+                            if (ok) tmem_ld32(tm, v);
+                            if (ok && row < p.n) {
+                                float* o = p.logits + row * L.dout;
+#pragma unroll
+                                for (int c = 0; c < 32; ++c)
+                                    if (c < L.dout) o[c] = __uint_as_float(v[c]);
+                            }
+                        }
+                        const int64_t nxt = pr + gridDim.x;  // this tile of the next pair
+                        if (nxt < n_pairs) infer_stage(p, L0, act, (2 * nxt + t) * kRows, tid);
+                    }
+                    proxy_fence();
+                    tc_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&sh->edone[t]));
+                }
+    }
+    tc_before();
+    cta_sync();
+    __syncwarp();
+    if (tid == 0 && *abort && p.error) atomicExch(p.error, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+}
+
 // ---- weight gradients and AdamW ---------------------------------------------
 
 struct DwTile {
@@ -1183,6 +1407,35 @@ int pb_train_fused_step(int32_t n_layers, const int32_t* dims, const void* x_bf1
     cfg.numAttrs = 1;
     if (cudaLaunchKernelEx(&cfg, k_train_dw, *dw) != cudaSuccess) return finish(PB_ECUDA);
     return finish(PB_SUCCESS);
+}
+
+int pb_mlp_infer_fused(int32_t n_layers, const int32_t* dims, const void* x_bf16, int64_t n, const void* w_img,
+                       float* logits, int32_t* error_flag, void* stream)
+{
+    InferArgs a;
+    const int rc = geo_build(n_layers, dims, 1, &a.geo);
+    if (rc != PB_SUCCESS) return rc;
+    if (n < 0 || !x_bf16 || !w_img || !logits || !aligned16h(x_bf16) || !aligned16h(w_img)) return PB_EINVAL;
+    if (n == 0) return PB_SUCCESS;
+    static int attr_done[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PB_ECUDA;
+    if (dev < 0 || dev >= 64 || !__atomic_load_n(&attr_done[dev], __ATOMIC_ACQUIRE)) {
+        if (cudaFuncSetAttribute(k_mlp_infer_pp, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem) != cudaSuccess)
+            return PB_ECUDA;
+        if (dev >= 0 && dev < 64) __atomic_store_n(&attr_done[dev], 1, __ATOMIC_RELEASE);
+    }
+    a.x = static_cast<const __nv_bfloat16*>(x_bf16);
+    a.n = n;
+    a.w_img = static_cast<const uint8_t*>(w_img);
+    a.logits = logits;
+    a.error = error_flag;
+    const int64_t pairs = ((n + kRows - 1) / kRows + 1) / 2;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = static_cast<unsigned>(pairs < sms ? pairs : sms);
+    k_mlp_infer_pp<<<grid, kFbThreads, kInfSmem, static_cast<cudaStream_t>(stream)>>>(a);
+    return cudaGetLastError() == cudaSuccess ? PB_SUCCESS : PB_ECUDA;
 }
 
 int pb_train_fused_adamw(int32_t n_layers, const int32_t* dims, float* w_aug, float* m1, float* m2, const float* grad,

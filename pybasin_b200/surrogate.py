@@ -342,10 +342,52 @@ class MLPSurrogate:
             self._tc_step = self._step
         return self._tc_cache
 
+    def fused_image(self):
+        """(BF16 weight slab images, dims) of the fused training step's layout, with
+        the bias as a column of the augmented weights (repacked after every change of
+        the weights), or None where the network is outside that step's limits."""
+        from pybasin_b200 import train as T
+
+        dims = [self.d_in] + [int(w.shape[0]) for w in self.W]
+        if not T.fused_supported(dims) or os.environ.get("PB_MLP_TC", "1") == "0":
+            return None
+        if getattr(self, "_fused_step", None) != self._step:
+            lib = T._lib()
+            nl = len(dims) - 1
+            dims_c = (ctypes.c_int32 * len(dims))(*dims)
+            geo = (ctypes.c_int64 * (3 + 4 * nl))()
+            L.check(lib.pb_train_fused_geometry(nl, dims_c, 1, geo, len(geo)), "pb_train_fused_geometry")
+            aug = torch.zeros((int(geo[2]),), dtype=torch.float32, device=self.dev)
+            for li in range(nl):
+                kaug, npad, off = int(geo[3 + 4 * li]), int(geo[4 + 4 * li]), int(geo[5 + 4 * li])
+                A = aug[off : off + npad * kaug].view(npad, kaug)
+                A[: dims[li + 1], : dims[li]].copy_(self.W[li])
+                A[: dims[li + 1], dims[li]].copy_(self.b[li])
+            img = torch.empty((int(geo[0]),), dtype=torch.uint8, device=self.dev)
+            L.check(lib.pb_train_fused_pack(nl, dims_c, _p(aug), _p(img), torch.cuda.current_stream(self.dev).cuda_stream),
+                    "pb_train_fused_pack")
+            self._fused_cache = (img, dims_c)
+            self._fused_step = self._step
+        return self._fused_cache
+
     def logits(self, x_in: torch.Tensor, chunk: int = 1 << 20) -> torch.Tensor:
-        """Inference logits: the fused tensor-core kernel when the network fits it,
-        else the layer-by-layer GEMM path of training."""
+        """Inference logits: the two-tile tensor-core kernel on the fused step's
+        weight images where the network fits it, else the one-tile tensor-core
+        kernel, else the layer-by-layer GEMM path of training."""
         n = x_in.shape[0]
+        fused = self.fused_image()
+        if fused is not None and n > 0:
+            from pybasin_b200 import train as T
+
+            lib = T._lib()
+            img, dims_c = fused
+            x = x_in.contiguous()
+            out = torch.empty((n, self.n_classes), dtype=torch.float32, device=self.dev)
+            err = torch.zeros((1,), dtype=torch.int32, device=self.dev)
+            L.check(lib.pb_mlp_infer_fused(self.n_layers, dims_c, _p(x), n, _p(img), _p(out), _p(err),
+                                           torch.cuda.current_stream(self.dev).cuda_stream), "pb_mlp_infer_fused")
+            self._fused_error = err
+            return out
         if self.tc_supported():
             packed, shapes = self.packed_tc()
             return infer_tc(x_in, packed, self.b, shapes, self.n_classes)

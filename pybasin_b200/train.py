@@ -55,8 +55,10 @@ def bind(lib: ctypes.CDLL) -> None:
     lib.pb_train_fused_step.argtypes = [i32, PI32, vp, vp, i32, vp, i32, i32, vp, vp, vp, vp, vp, vp, f32, f32, f32,
                                         f32, f32, i32, vp, vp, vp, vp]
     lib.pb_train_fused_adamw.argtypes = [i32, PI32, vp, vp, vp, vp, vp, f32, f32, f32, f32, f32, i32, vp]
+    lib.pb_mlp_infer_fused.argtypes = [i32, PI32, vp, i64, vp, vp, vp, vp]
     for name in ("pb_train_gemm", "pb_train_xent", "pb_train_xent_parts", "pb_train_adamw", "pb_train_gather",
-                 "pb_train_fused_geometry", "pb_train_fused_pack", "pb_train_fused_step", "pb_train_fused_adamw"):
+                 "pb_train_fused_geometry", "pb_train_fused_pack", "pb_train_fused_step", "pb_train_fused_adamw",
+                 "pb_mlp_infer_fused"):
         getattr(lib, name).restype = ctypes.c_int
     lib._pb_train_bound = True
 

@@ -428,3 +428,29 @@ def test_gated_pendulum_torque_sweep_matches_the_integrator_per_point():
     for q in np.nonzero(bad)[0]:
         sel = (grp == int(q))
         assert torch.equal(label[sel], ref_lab[sel])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 130, 100_003])
+def test_two_tile_inference_matches_one_tile_kernel(n):
+    """pb_mlp_infer_fused (pairs of row tiles per CTA, the bias as a BF16 column of the
+    augmented weights) against pb_mlp_infer_tc (one tile per CTA, FP32 bias added in
+    the epilogue) on the surrogate's shape: ragged last tile, an odd tile count, CTAs
+    with several pairs; the BF16 rounding of the bias and of the activations bounds
+    the difference."""
+    from pybasin_b200.surrogate import MLPSurrogate, infer_tc
+
+    dev = torch.device("cuda:0")
+    net = MLPSurrogate(2, 6, hidden=256, depth=4, seed=7, device=dev, n_freq=64, pad_inputs=True)
+    g = torch.Generator().manual_seed(n)
+    ic = (torch.rand(n, 2, generator=g) * 4 - 2).to(dev)
+    net.fit_normalisation(ic)
+    x = net.inputs(ic, None)
+    got = net.logits(x)
+    packed, shapes = net.packed_tc()
+    ref = infer_tc(x, packed, net.b, shapes, net.n_classes)
+    torch.cuda.synchronize()
+    assert int(net._fused_error.item()) == 0
+    scale = ref.abs().max().item()
+    assert (got - ref).abs().max().item() <= 2e-2 * scale
+    assert (got.argmax(1) == ref.argmax(1)).float().mean().item() >= 0.99
