@@ -26,6 +26,46 @@ __device__ __forceinline__ float gelu(float x)
     return fmaf(hx, t, hx);
 }
 
+// Two FP32 lanes in one 64-bit register for the packed FP32 instructions of sm_100
+// (fma/mul .f32x2, round to nearest, no flush): each lane rounds exactly as the
+// scalar instruction does, so a packed form of a formula is bit-identical to it.
+struct f32x2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ f32x2 f2(float a, float b)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_split(f32x2 x, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+
+// gelu of two values, the operations of gelu() lane by lane
+__device__ __forceinline__ void gelu2(float x0, float x1, float& g0, float& g1)
+{
+    const f32x2 x = f2(x0, x1);
+    float u0, u1;
+    f2_split(mul2(x, fma2(f2(kGeluB, kGeluB), mul2(x, x), f2(kGeluA, kGeluA))), u0, u1);
+    const f32x2 t = f2(tanh_approx(u0), tanh_approx(u1));
+    const f32x2 hx = mul2(f2(0.5f, 0.5f), x);
+    f2_split(fma2(hx, t, hx), g0, g1);
+}
+
 // d gelu / dx = 0.5 (1 + t) + 0.5 x (1 - t^2) du/dx, du/dx = sqrt(2/pi) (1 + 3 * 0.044715 x^2)
 __device__ __forceinline__ float gelu_grad(float x)
 {

@@ -69,13 +69,31 @@ constexpr long long kWaitPolls = 1ll << 22;
 // one MMA-issuing warp, one warp streaming the weight slabs
 constexpr int kEpiWarps = 16;
 constexpr int kMmaWarp = kEpiWarps;
-constexpr int kLoadWarp = kEpiWarps + 1;
-constexpr int kFbThreads = (kEpiWarps + 2) * 32;
-constexpr int kRing = 9;                                 // weight-slab slots
+constexpr int kLoadWarp = kEpiWarps + 1;               // the first copy-issuing warp
+// Bulk copies issued by one thread follow each other (about a microsecond each,
+// whatever the size up to ~100 KB); copies from different warps overlap, so the
+// weight copies are dealt round robin to kLoadWarps warps
+#ifndef PB_LOAD_WARPS
+#define PB_LOAD_WARPS 1
+#endif
+constexpr int kLoadWarps = PB_LOAD_WARPS;
+constexpr int kFbThreads = (kEpiWarps + 1 + kLoadWarps) * 32;
 constexpr int kSlabBytes = 16 * 1024;                    // a weight slab: all rows x as many columns as fit
+// A bulk copy costs about the same whatever its size up to tens of KB, so the
+// slabs stream in groups of consecutive slabs (contiguous in the image), one copy
+// per group, into ring slots of kGroup slabs
+#ifndef PB_FB_GROUP
+#define PB_FB_GROUP 3
+#endif
+#ifndef PB_FB_RING
+#define PB_FB_RING 3
+#endif
+constexpr int kGroup = PB_FB_GROUP;                      // slabs per copy
+constexpr int kRing = PB_FB_RING;                        // slots of the weight ring
+constexpr int kSlotBytes = kGroup * kSlabBytes;
 constexpr int kImgBytes = kRows * kMaxKaug * 2;          // largest activation / gradient image
 constexpr int kFbTail = 1024;                            // barriers, flags, the tile's labels
-constexpr int kFbSmem = kImgBytes + kRing * kSlabBytes + kFbTail;
+constexpr int kFbSmem = kImgBytes + kRing * kSlotBytes + kFbTail;
 
 // k_train_dw
 constexpr int kDwThreads = 256;
@@ -312,6 +330,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 64 columns: two loads in flight, one wait
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&v)[64])
+{
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+            "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(v[32 * h + 0]), "=r"(v[32 * h + 1]), "=r"(v[32 * h + 2]), "=r"(v[32 * h + 3]), "=r"(v[32 * h + 4]),
+              "=r"(v[32 * h + 5]), "=r"(v[32 * h + 6]), "=r"(v[32 * h + 7]), "=r"(v[32 * h + 8]), "=r"(v[32 * h + 9]),
+              "=r"(v[32 * h + 10]), "=r"(v[32 * h + 11]), "=r"(v[32 * h + 12]), "=r"(v[32 * h + 13]),
+              "=r"(v[32 * h + 14]), "=r"(v[32 * h + 15]), "=r"(v[32 * h + 16]), "=r"(v[32 * h + 17]),
+              "=r"(v[32 * h + 18]), "=r"(v[32 * h + 19]), "=r"(v[32 * h + 20]), "=r"(v[32 * h + 21]),
+              "=r"(v[32 * h + 22]), "=r"(v[32 * h + 23]), "=r"(v[32 * h + 24]), "=r"(v[32 * h + 25]),
+              "=r"(v[32 * h + 26]), "=r"(v[32 * h + 27]), "=r"(v[32 * h + 28]), "=r"(v[32 * h + 29]),
+              "=r"(v[32 * h + 30]), "=r"(v[32 * h + 31])
+            : "r"(taddr + 32u * h));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 // All threads of the CTA, in the non-aligned form (warps may arrive diverged:
 // one lane issued the MMAs or the copies)
 __device__ __forceinline__ void cta_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
@@ -476,7 +515,7 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     // the image buffer (each phase's epilogue overwrites its input in place), then
     // the slab ring, then FbSmem
     uint8_t* ring = smem + kImgBytes;
-    FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kSlabBytes);
+    FbSmem* sh = reinterpret_cast<FbSmem*>(ring + kRing * kSlotBytes);
     volatile int* abort = &sh->abort;
     const Geo& G = p.geo;
     const int NL = G.n_layers;
@@ -506,29 +545,31 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
     tc_after();
     const uint32_t tmem = sh->tmem;
 
-    if (warp == kLoadWarp) {
+    if (warp >= kLoadWarp) {
         // ---- weight slabs into the ring, in the order the MMA warp consumes them:
-        // forward W slabs of every layer, then the W^T slabs from the last layer down
+        // forward W slabs of every layer, then the W^T slabs from the last layer down;
+        // copy u is issued by load warp u % kLoadWarps
         if (lane == 0) {
+            const uint32_t lw = static_cast<uint32_t>(warp - kLoadWarp);
             uint32_t u = 0;
             auto put = [&](int64_t off, uint32_t bytes) {
                 const uint32_t s = u % kRing, round = u / kRing;
-                ++u;
+                if (u++ % kLoadWarps != lw) return;
                 if (round > 0 && !mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1u, abort)) return;
                 mbar_expect_tx(smem_u32(&sh->full[s]), bytes);
-                bulk_load(smem_u32(ring + s * kSlabBytes), p.w_img + off, bytes, smem_u32(&sh->full[s]));
+                bulk_load(smem_u32(ring + s * kSlotBytes), p.w_img + off, bytes, smem_u32(&sh->full[s]));
             };
             for (int l = 0; l < NL && !*abort; ++l) {
                 const LayerGeo& L = G.l[l];
-                for (int k0 = 0; k0 < L.kaug; k0 += L.sw)
-                    put(L.w_off + static_cast<int64_t>(L.npad) * k0 * 2,
-                        static_cast<uint32_t>(L.npad) * min(L.sw, L.kaug - k0) * 2u);
+                for (int g0 = 0; g0 < L.kaug; g0 += kGroup * L.sw)
+                    put(L.w_off + static_cast<int64_t>(L.npad) * g0 * 2,
+                        static_cast<uint32_t>(L.npad) * min(kGroup * L.sw, L.kaug - g0) * 2u);
             }
             for (int l = NL - 1; l >= 1 && !*abort; --l) {
                 const LayerGeo& L = G.l[l];
-                for (int o0 = 0; o0 < L.npad; o0 += L.tw)
-                    put(L.wt_off + static_cast<int64_t>(L.din) * o0 * 2,
-                        static_cast<uint32_t>(L.din) * min(L.tw, L.npad - o0) * 2u);
+                for (int g0 = 0; g0 < L.npad; g0 += kGroup * L.tw)
+                    put(L.wt_off + static_cast<int64_t>(L.din) * g0 * 2,
+                        static_cast<uint32_t>(L.din) * min(kGroup * L.tw, L.npad - g0) * 2u);
             }
         }
         __syncwarp();
@@ -568,14 +609,18 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 begin_phase(p.scratch + L.x_off + tile * L.x_tile, static_cast<uint32_t>(L.x_tile));
                 const uint32_t sbo_a = static_cast<uint32_t>(L.kaug >> 3) << 7;
                 const uint32_t idesc = instr_desc(kRows, L.npad, false, false);
-                for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
+                for (int g0 = 0; g0 < L.kaug; g0 += kGroup * L.sw) {
                     uint32_t s;
                     const bool ok = slab(s);
-                    const int kw = min(L.sw, L.kaug - k0);
-                    const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
-                    for (int ks = 0; ok && ks < (kw >> 4); ++ks)
-                        mma_bf16(tmem, smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
-                                 smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                    const uint32_t sb = smem_u32(ring + s * kSlotBytes);
+                    for (int k0 = g0; ok && k0 < min(g0 + kGroup * L.sw, L.kaug); k0 += L.sw) {
+                        const int kw = min(L.sw, L.kaug - k0);
+                        const uint32_t b0 = sb + static_cast<uint32_t>(L.npad * (k0 - g0) * 2);
+                        const uint32_t sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
+                        for (int ks = 0; ks < (kw >> 4); ++ks)
+                            mma_bf16(tmem, smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                     smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                    }
                     mma_commit(smem_u32(&sh->empty[s]));
                 }
                 end_mmas();
@@ -585,14 +630,18 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_train_fb(const __grid_constan
                 begin_phase(p.scratch + L.z_off + tile * L.z_tile, static_cast<uint32_t>(L.z_tile));
                 const uint32_t sbo_a = static_cast<uint32_t>(L.npad >> 3) << 7;
                 const uint32_t idesc = instr_desc(kRows, L.din, false, false);
-                for (int o0 = 0; o0 < L.npad; o0 += L.tw) {
+                for (int g0 = 0; g0 < L.npad; g0 += kGroup * L.tw) {
                     uint32_t s;
                     const bool ok = slab(s);
-                    const int ow = min(L.tw, L.npad - o0);
-                    const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(ow >> 3) << 7;
-                    for (int ks = 0; ok && ks < (ow >> 4); ++ks)
-                        mma_bf16(tmem, smem_desc(a0 + ((o0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
-                                 smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (o0 > 0 || ks > 0) ? 1u : 0u);
+                    const uint32_t sb = smem_u32(ring + s * kSlotBytes);
+                    for (int o0 = g0; ok && o0 < min(g0 + kGroup * L.tw, L.npad); o0 += L.tw) {
+                        const int ow = min(L.tw, L.npad - o0);
+                        const uint32_t b0 = sb + static_cast<uint32_t>(L.din * (o0 - g0) * 2);
+                        const uint32_t sbo_b = static_cast<uint32_t>(ow >> 3) << 7;
+                        for (int ks = 0; ks < (ow >> 4); ++ks)
+                            mma_bf16(tmem, smem_desc(a0 + ((o0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                     smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (o0 > 0 || ks > 0) ? 1u : 0u);
+                    }
                     mma_commit(smem_u32(&sh->empty[s]));
                 }
                 end_mmas();
@@ -769,8 +818,16 @@ struct InferArgs {
     int32_t* error;
 };
 
-constexpr int kInfRing = 5;
-constexpr int kInfSmem = 2 * kImgBytes + kInfRing * kSlabBytes + 1024;
+#ifndef PB_INF_GROUP
+#define PB_INF_GROUP 2
+#endif
+#ifndef PB_INF_RING
+#define PB_INF_RING 2
+#endif
+constexpr int kInfGroup = PB_INF_GROUP;  // slabs per copy
+constexpr int kInfRing = PB_INF_RING;
+constexpr int kInfSlot = kInfGroup * kSlabBytes;
+constexpr int kInfSmem = 2 * kImgBytes + kInfRing * kInfSlot + 1024;
 static_assert(kInfSmem <= 227 * 1024, "k_mlp_infer_pp: shared memory");
 
 struct InfSmem {
@@ -799,12 +856,30 @@ __device__ __forceinline__ void infer_stage(const InferArgs& p, const LayerGeo& 
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// GELU of NN accumulator columns of row r into the next layer's image (width w)
+// at columns col .. col + NN
+template <int NN>
+__device__ __forceinline__ void gelu_cols(const uint32_t (&v)[NN], uint8_t* act, int w, int r, int col)
+{
+#pragma unroll
+    for (int q = 0; q < NN / 8; ++q) {
+        uint32_t hx[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float g0, g1;
+            pb::gelu2(__uint_as_float(v[q * 8 + 2 * k]), __uint_as_float(v[q * 8 + 2 * k + 1]), g0, g1);
+            hx[k] = pack_bf16(g0, g1);
+        }
+        *reinterpret_cast<uint4*>(act + img_off(w, r, col + q * 8)) = make_uint4(hx[0], hx[1], hx[2], hx[3]);
+    }
+}
+
 __global__ void __launch_bounds__(kFbThreads, 1) k_mlp_infer_pp(const __grid_constant__ InferArgs p)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
     // the activations of tile t at smem + t * kImgBytes, then the slab ring
     uint8_t* ring = smem + 2 * kImgBytes;
-    InfSmem* sh = reinterpret_cast<InfSmem*>(ring + kInfRing * kSlabBytes);
+    InfSmem* sh = reinterpret_cast<InfSmem*>(ring + kInfRing * kInfSlot);
     volatile int* abort = &sh->abort;
     const Geo& G = p.geo;
     const int NL = G.n_layers;
@@ -834,23 +909,33 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_mlp_infer_pp(const __grid_con
     tc_after();
     const uint32_t tmem = sh->tmem;
 
-    if (warp == kLoadWarp) {
-        if (lane == 0) {  // the slabs of every layer, once per tile, in the MMA order
+    if (warp >= kLoadWarp) {
+        if (lane == 0) {  // the slabs of every layer, once per tile, in the MMA order; copy u by load warp u % kLoadWarps
+            const uint32_t lw = static_cast<uint32_t>(warp - kLoadWarp);
             uint32_t u = 0;
-            for (int64_t pr = blockIdx.x; pr < n_pairs && !*abort; pr += gridDim.x)
+            for (int64_t pr = blockIdx.x; pr < n_pairs && !*abort; pr += gridDim.x) {
+                // the next pair's input rows into L2: the epilogue stages them at the
+                // end of this pair
+                const int64_t nxt = pr + gridDim.x;
+                if (lw == 0 && nxt < n_pairs) {
+                    const int64_t r0 = 2 * nxt * kRows, r1 = min(p.n, r0 + 2 * kRows);
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p.x + r0 * G.l[0].din),
+                                 "r"(static_cast<uint32_t>((r1 - r0) * G.l[0].din * 2)) : "memory");
+                }
                 for (int l = 0; l < NL; ++l)
                     for (int t = 0; t < 2; ++t) {
                         const LayerGeo& L = G.l[l];
-                        for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
+                        for (int g0 = 0; g0 < L.kaug; g0 += kInfGroup * L.sw) {
                             const uint32_t s = u % kInfRing, round = u / kInfRing;
-                            ++u;
+                            if (u++ % kLoadWarps != lw) continue;
                             if (round > 0 && !mbar_wait(smem_u32(&sh->empty[s]), (round - 1) & 1u, abort)) continue;
-                            const uint32_t bytes = static_cast<uint32_t>(L.npad) * min(L.sw, L.kaug - k0) * 2u;
+                            const uint32_t bytes = static_cast<uint32_t>(L.npad) * min(kInfGroup * L.sw, L.kaug - g0) * 2u;
                             mbar_expect_tx(smem_u32(&sh->full[s]), bytes);
-                            bulk_load(smem_u32(ring + s * kSlabBytes), p.w_img + L.w_off + static_cast<int64_t>(L.npad) * k0 * 2,
+                            bulk_load(smem_u32(ring + s * kInfSlot), p.w_img + L.w_off + static_cast<int64_t>(L.npad) * g0 * 2,
                                       bytes, smem_u32(&sh->full[s]));
                         }
                     }
+            }
         }
         cta_sync();
         if (tid == kLoadWarp * 32 && *abort && p.error) atomicExch(p.error, 1);
@@ -871,17 +956,21 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_mlp_infer_pp(const __grid_con
                         const uint32_t a0 = smem_u32(smem + t * kImgBytes);
                         const uint32_t sbo_a = static_cast<uint32_t>(L.kaug >> 3) << 7;
                         const uint32_t idesc = instr_desc(kRows, L.npad, false, false);
-                        for (int k0 = 0; k0 < L.kaug; k0 += L.sw) {
+                        for (int g0 = 0; g0 < L.kaug; g0 += kInfGroup * L.sw) {
                             const uint32_t s = u % kInfRing, round = u / kInfRing;
                             ++u;
                             const bool ok = mbar_wait(smem_u32(&sh->full[s]), round & 1u, abort);
                             tc_after();
-                            const int kw = min(L.sw, L.kaug - k0);
-                            const uint32_t b0 = smem_u32(ring + s * kSlabBytes), sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
-                            for (int ks = 0; ok && ks < (kw >> 4); ++ks)
-                                mma_bf16(tmem + static_cast<uint32_t>(t * 256),
-                                         smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
-                                         smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                            const uint32_t sb = smem_u32(ring + s * kInfSlot);
+                            for (int k0 = g0; ok && k0 < min(g0 + kInfGroup * L.sw, L.kaug); k0 += L.sw) {
+                                const int kw = min(L.sw, L.kaug - k0);
+                                const uint32_t b0 = sb + static_cast<uint32_t>(L.npad * (k0 - g0) * 2);
+                                const uint32_t sbo_b = static_cast<uint32_t>(kw >> 3) << 7;
+                                for (int ks = 0; ks < (kw >> 4); ++ks)
+                                    mma_bf16(tmem + static_cast<uint32_t>(t * 256),
+                                             smem_desc(a0 + ((k0 >> 3) + 2 * ks) * 128u, 128u, sbo_a),
+                                             smem_desc(b0 + ks * 256u, 128u, sbo_b), idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+                            }
                             mma_commit(smem_u32(&sh->empty[s]));
                         }
                         mma_commit(smem_u32(&sh->mdone[t]));
@@ -916,30 +1005,25 @@ __global__ void __launch_bounds__(kFbThreads, 1) k_mlp_infer_pp(const __grid_con
                         const LayerGeo& Ln = G.l[l + 1];
                         if (grp < L.n_pieces) {
                             const int pc = grp;
-                            for (int cc = 0; ok && cc < L.ph[pc]; cc += 32) {
-                                const int nn = L.ph[pc] - cc >= 32 ? 32 : 16;
-                                float z[32];
-                                if (nn == 32) {
+                            for (int cc = 0; ok && cc < L.ph[pc];) {
+                                const int rem = L.ph[pc] - cc, col = L.p0[pc] + cc;
+                                const uint32_t ta = tm + static_cast<uint32_t>(col);
+                                // 64 columns per TMEM round trip where the piece has them
+                                if (rem >= 64) {
+                                    uint32_t v[64];
+                                    tmem_ld64(ta, v);
+                                    gelu_cols(v, act, Ln.kaug, r, col);
+                                    cc += 64;
+                                } else if (rem >= 32) {
                                     uint32_t v[32];
-                                    tmem_ld32(tm + static_cast<uint32_t>(L.p0[pc] + cc), v);
-#pragma unroll
-                                    for (int j = 0; j < 32; ++j) z[j] = __uint_as_float(v[j]);
+                                    tmem_ld32(ta, v);
+                                    gelu_cols(v, act, Ln.kaug, r, col);
+                                    cc += 32;
                                 } else {
                                     uint32_t v[16];
-                                    tmem_ld16(tm + static_cast<uint32_t>(L.p0[pc] + cc), v);
-#pragma unroll
-                                    for (int j = 0; j < 16; ++j) z[j] = __uint_as_float(v[j]);
-#pragma unroll
-                                    for (int j = 16; j < 32; ++j) z[j] = 0.f;
-                                }
-#pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    if (q * 8 >= nn) break;
-                                    uint32_t hx[4];
-#pragma unroll
-                                    for (int k = 0; k < 4; ++k) hx[k] = pack_bf16(gelu(z[q * 8 + 2 * k]), gelu(z[q * 8 + 2 * k + 1]));
-                                    *reinterpret_cast<uint4*>(act + img_off(Ln.kaug, r, L.p0[pc] + cc + q * 8)) =
-                                        make_uint4(hx[0], hx[1], hx[2], hx[3]);
+                                    tmem_ld16(ta, v);
+                                    gelu_cols(v, act, Ln.kaug, r, col);
+                                    cc += 16;
                                 }
                             }
                             if (pc == L.n_pieces - 1)
