@@ -96,7 +96,13 @@ constexpr int kFbTail = 1024;                            // barriers, flags, the
 constexpr int kFbSmem = kImgBytes + kRing * kSlotBytes + kFbTail;
 
 // k_train_dw
-constexpr int kDwThreads = 256;
+#ifndef PB_DW_PRODUCERS
+#define PB_DW_PRODUCERS 4
+#endif
+constexpr int kDwProducers = PB_DW_PRODUCERS;
+// the MMA warp and the producers, in whole groups of four warps (the TMEM readout
+// gives each warp a lane quarter), at least eight warps
+constexpr int kDwThreads = ((kDwProducers + 1 + 3) / 4 * 4 > 8 ? (kDwProducers + 1 + 3) / 4 * 4 : 8) * 32;
 constexpr int kDwStages = 3;
 constexpr int kDwMaxIn = 144;                       // inputs of a weight tile
 constexpr int kDwABytes = kRows * kRows * 2;        // 128 outputs x 128 rows
@@ -105,6 +111,10 @@ constexpr int kDwStageBytes = kDwABytes + kDwBBytes;
 constexpr int kDwTail = 256;
 constexpr int kDwSmem = kDwStages * kDwStageBytes + kDwTail;
 constexpr int kMaxCluster = 8;
+// warps 1 .. kDwProducers copy the row groups of a stage, 16 / kDwProducers each:
+// the lanes of one warp issue their copies together, but at about 26 B/clk for
+// 2 KB copies; copies from several warps proceed side by side
+static_assert(16 % kDwProducers == 0 && kDwProducers + 1 <= kDwThreads / 32, "k_train_dw: producer warps");
 constexpr int kMaxDwTiles = kMaxLayers * 2 * 2;  // per layer <= 2 output tiles x 2 input ranges
 
 // ---- geometry ----------------------------------------------------------------
@@ -1149,7 +1159,7 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
 
     if (tid == 0) {
         for (int s = 0; s < kDwStages; ++s) {
-            mbar_init(smem_u32(&sh->full[s]), 1);
+            mbar_init(smem_u32(&sh->full[s]), kDwProducers);
             mbar_init(smem_u32(&sh->empty[s]), 1);
         }
         mbar_init(smem_u32(&sh->done), 1);
@@ -1173,10 +1183,11 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
     tc_after();
     const uint32_t tmem = sh->tmem;
 
-    if (warp == 1) {
-        // ---- producer: per row tile, row group g of the dZ image (the tile's
-        // outputs) by lane g, and row group g of the X image (the tile's inputs) by
-        // lane 16 + g
+    if (warp >= 1 && warp <= kDwProducers) {
+        // ---- producers: per row tile, warp w takes row groups (w - 1) * G .. + G - 1
+        // (G = 16 / kDwProducers): of the dZ image (the tile's outputs) by lanes
+        // 0 .. G - 1, of the X image (the tile's inputs) by lanes G .. 2 G - 1
+        constexpr int G = 16 / kDwProducers;
         for (int k = 0; k < nk; ++k) {
             const int s = k % kDwStages, round = k / kDwStages;
             bool ok = true;
@@ -1184,18 +1195,18 @@ __global__ void __launch_bounds__(kDwThreads, 1) k_train_dw(const __grid_constan
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) break;
             const uint32_t full = smem_u32(&sh->full[s]);
-            if (lane == 0) mbar_expect_tx(full, static_cast<uint32_t>(T.oh + iw) * (kRows * 2));
+            if (lane == 0) mbar_expect_tx(full, static_cast<uint32_t>(T.oh + iw) * (kRows * 2) / kDwProducers);
             __syncwarp();
             const int t = t0 + k;
             const uint32_t a_s = smem_u32(smem + s * kDwStageBytes), b_s = a_s + kDwABytes;
-            const int g = lane & 15;
-            if (lane < 16) {
+            const int g = (warp - 1) * G + (lane % G);
+            if (lane < G) {
                 const uint32_t bytes = static_cast<uint32_t>(T.oh >> 3) << 7;
                 bulk_load(a_s + g * 2048u,
                           p.scratch + L.z_off + static_cast<int64_t>(t) * L.z_tile +
                               (static_cast<int64_t>(g) * (L.npad >> 3) + (T.o0 >> 3)) * 128,
                           bytes, full);
-            } else {
+            } else if (lane < 2 * G) {
                 bulk_load(b_s + g * ncol_b,
                           p.scratch + L.x_off + static_cast<int64_t>(t) * L.x_tile +
                               (static_cast<int64_t>(g) * (L.kaug >> 3) + (T.i0 >> 3)) * 128,
